@@ -1,0 +1,138 @@
+"""ctypes binding of libgq.so (the C ABI declared in include/gq.h).
+
+The library is built in-tree by ``gquery_b200.build_lib`` (``__graft_entry__.build``).
+There is no fallback: if the shared library is missing, loading raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libgq.so"
+
+GQ_OK = 0
+GQ_ERR_INVALID = 1
+GQ_ERR_CUDA = 2
+GQ_ERR_NOMEM = 3
+GQ_ERR_DEPTH = 4
+GQ_ERR_DEVICE = 5
+GQ_ERR_UNSUPPORTED = 6
+
+VARIANT_EXACT = 0
+VARIANT_WIDE8 = 1
+VARIANT_AUTO = 2
+
+ARRAY_BVH_NODES = 0
+ARRAY_PRIMITIVES = 1
+ARRAY_SNCH_NODES = 2
+ARRAY_SILHOUETTES = 3
+ARRAY_RAW_SILHOUETTES = 4
+ARRAY_WIDE_NODES = 5
+
+DEVERR_STACK = 1
+
+
+class BuildOpts(C.Structure):
+    _fields_ = [("max_prims_in_node", C.c_int32), ("n_threads", C.c_int32), ("build_snch", C.c_int32),
+                ("build_wide", C.c_int32), ("device", C.c_int32)]
+
+
+class SceneInfo(C.Structure):
+    _fields_ = [("dim", C.c_int32), ("n_vertices", C.c_int64), ("n_prims", C.c_int64), ("n_nodes", C.c_int64),
+                ("n_wide_nodes", C.c_int64), ("n_silhouettes", C.c_int64), ("max_depth", C.c_int32),
+                ("exact_stack", C.c_int32), ("wide_stack", C.c_int32), ("device_bytes", C.c_int64),
+                ("bbox_lo", C.c_float * 3), ("bbox_hi", C.c_float * 3)]
+
+
+class Vecs(C.Structure):
+    _fields_ = [("ptr", C.c_void_p), ("comp_stride", C.c_int64), ("elem_stride", C.c_int64)]
+
+
+class CpOut(C.Structure):
+    _fields_ = [("valid", C.c_void_p), ("p", C.c_void_p), ("n", C.c_void_p), ("t", C.c_void_p),
+                ("d", C.c_void_p), ("prim_id", C.c_void_p)]
+
+
+class RayOut(C.Structure):
+    _fields_ = [("valid", C.c_void_p), ("p", C.c_void_p), ("n", C.c_void_p), ("t", C.c_void_p),
+                ("d", C.c_void_p), ("prim_id", C.c_void_p), ("on_boundary", C.c_void_p)]
+
+
+class SilOut(C.Structure):
+    _fields_ = [("valid", C.c_void_p), ("p", C.c_void_p), ("d", C.c_void_p), ("prim_id", C.c_void_p)]
+
+
+class QueryOpts(C.Structure):
+    _fields_ = [("variant", C.c_int32), ("sort", C.c_int32), ("order", C.c_void_p), ("scratch", C.c_void_p),
+                ("scratch_bytes", C.c_int64)]
+
+
+# name -> (restype, argtypes); every exported symbol of include/gq.h
+SIGNATURES = {
+    "gq_last_error": (None, [C.c_char_p, C.c_int64]),
+    "gq_status_string": (C.c_char_p, [C.c_int32]),
+    "gq_scene_build_2d": (C.c_int32, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.POINTER(BuildOpts),
+                                      C.POINTER(C.c_void_p)]),
+    "gq_scene_build_3d": (C.c_int32, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.POINTER(BuildOpts),
+                                      C.POINTER(C.c_void_p)]),
+    "gq_scene_free": (C.c_int32, [C.c_void_p]),
+    "gq_scene_get_info": (C.c_int32, [C.c_void_p, C.POINTER(SceneInfo)]),
+    "gq_scene_ref_array": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]),
+    "gq_flat_silhouette_edges": (C.c_int32, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
+                                             C.POINTER(C.c_int64)]),
+    "gq_query_scratch_bytes": (C.c_int64, [C.c_int64]),
+    "gq_order_scratch_bytes": (C.c_int64, [C.c_int64]),
+    "gq_query_order": (C.c_int32, [C.c_void_p, Vecs, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),
+    "gq_closest_point": (C.c_int32, [C.c_void_p, Vecs, C.c_int64, C.POINTER(CpOut), C.POINTER(QueryOpts),
+                                     C.c_void_p]),
+    "gq_intersect": (C.c_int32, [C.c_void_p, Vecs, Vecs, C.c_void_p, C.c_int64, C.POINTER(RayOut),
+                                 C.POINTER(QueryOpts), C.c_void_p]),
+    "gq_closest_silhouette": (C.c_int32, [C.c_void_p, Vecs, C.c_void_p, C.c_int64, C.POINTER(SilOut),
+                                          C.POINTER(QueryOpts), C.c_void_p]),
+    "gq_closest_point_brute": (C.c_int32, [C.c_void_p, Vecs, C.c_int64, C.POINTER(CpOut), C.c_void_p]),
+    "gq_intersect_brute": (C.c_int32, [C.c_void_p, Vecs, Vecs, C.c_void_p, C.c_int64, C.POINTER(RayOut),
+                                       C.c_void_p]),
+    "gq_brute_f64": (C.c_int32, [C.c_void_p, C.c_int32, Vecs, Vecs, C.c_int64, C.c_void_p, C.c_void_p,
+                                 C.c_void_p]),
+    "gq_scene_device_error": (C.c_int32, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)]),
+}
+
+_lock = threading.Lock()
+_lib = None
+
+
+class GQError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[gq status {status}] {message}")
+        self.status = status
+
+
+def lib() -> C.CDLL:
+    """Loads libgq.so once (raises if it was never built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not LIB_PATH.exists():
+                raise ImportError(f"{LIB_PATH} is missing: run gquery_b200.build_lib.build() "
+                                  "(the engine has no non-native fallback)")
+            h = C.CDLL(str(LIB_PATH))
+            for name, (res, args) in SIGNATURES.items():
+                f = getattr(h, name)
+                f.restype = res
+                f.argtypes = args
+            _lib = h
+    return _lib
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(1024)
+    lib().gq_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(status: int) -> None:
+    if status != GQ_OK:
+        raise GQError(status, last_error())

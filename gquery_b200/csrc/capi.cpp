@@ -1,0 +1,502 @@
+// C ABI of libgq.so (declared in include/gq.h).
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/gq.h"
+#include "device/queries.cuh"
+#include "host/flatten.hpp"
+#include "host/scene_build.hpp"
+
+using namespace gqb;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+gq_status fail(gq_status s, const std::string &msg) {
+    g_last_error = msg;
+    return s;
+}
+gq_status fail_cuda(cudaError_t e, const char *what) {
+    return fail(GQ_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = true;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) ok = cudaSetDevice(dev) == cudaSuccess;
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace
+
+struct gq_scene {
+    int dim = 0;
+    int device = 0;
+    std::vector<float> verts;
+    std::vector<int32_t> index;
+    int64_t nv = 0, np = 0;
+    BvhTree<2> t2;
+    BvhTree<3> t3;
+    SnchTree<2> s2;
+    SnchTree<3> s3;
+    bool has_snch = false, has_wide = false;
+    int exact_stack = 0, wide_stack = 0;
+    int64_t n_wide = 0, n_sil = 0;
+    std::vector<float> wide_words;  // host copy of the wide nodes (host-only scenes)
+    std::vector<void *> allocs;
+    int64_t device_bytes = 0;
+    gqd::DevScene dev{};
+
+    ~gq_scene() {
+        if (device < 0 || allocs.empty()) return;
+        DeviceGuard g(device);
+        for (void *p : allocs) cudaFree(p);
+    }
+
+    template <typename T>
+    gq_status upload(const std::vector<T> &v, const void **dst) {
+        *dst = nullptr;
+        if (v.empty()) return GQ_OK;
+        void *p = nullptr;
+        const size_t bytes = v.size() * sizeof(T);
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) return fail(GQ_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        allocs.push_back(p);
+        device_bytes += (int64_t)bytes;
+        e = cudaMemcpy(p, v.data(), bytes, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpy");
+        *dst = p;
+        return GQ_OK;
+    }
+};
+
+namespace {
+
+template <int D>
+gq_status build_scene(const float *vertices, int64_t nv, const int32_t *prims, int64_t np, const gq_build_opts *opts,
+                      gq_scene **out) {
+    if (!out) return fail(GQ_ERR_INVALID, "out is null");
+    *out = nullptr;
+    if (!vertices || !prims) return fail(GQ_ERR_INVALID, "null vertex or primitive array");
+    gq_build_opts o{10, 0, 1, 1, 0};
+    if (opts) o = *opts;
+    if (o.max_prims_in_node < 1) return fail(GQ_ERR_INVALID, "max_prims_in_node must be >= 1");
+    int nt = o.n_threads > 0 ? o.n_threads : (int)std::max(1u, std::thread::hardware_concurrency());
+
+    std::unique_ptr<gq_scene> s(new (std::nothrow) gq_scene());
+    if (!s) return fail(GQ_ERR_NOMEM, "out of host memory");
+    s->dim = D;
+    s->device = o.device;
+    s->nv = nv;
+    s->np = np;
+    try {
+        s->verts.assign(vertices, vertices + nv * D);
+        s->index.assign(prims, prims + np * D);
+    } catch (const std::bad_alloc &) {
+        return fail(GQ_ERR_NOMEM, "out of host memory");
+    }
+    PrimSource<D> src{s->verts.data(), nv, s->index.data(), np};
+    std::string bad = validate_source<D>(src);
+    if (!bad.empty()) return fail(GQ_ERR_INVALID, bad);
+
+    DeviceImage<D> img;
+    try {
+        BvhTree<D> tree = build_bvh<D>(src, o.max_prims_in_node, nt);
+        flatten_bvh<D>(src, tree, img);
+        if (o.build_wide) {
+            flatten_wide<D>(tree, img);
+            s->has_wide = true;
+        }
+        if (o.build_snch) {
+            SnchTree<D> sn = build_snch<D>(src, tree, nt);
+            flatten_snch<D>(tree, sn, img);
+            s->has_snch = true;
+            if constexpr (D == 2)
+                s->s2 = std::move(sn);
+            else
+                s->s3 = std::move(sn);
+        }
+        if constexpr (D == 2)
+            s->t2 = std::move(tree);
+        else
+            s->t3 = std::move(tree);
+    } catch (const std::bad_alloc &) {
+        return fail(GQ_ERR_NOMEM, "out of host memory during the build");
+    }
+
+    s->exact_stack = img.exact_stack;
+    s->wide_stack = img.wide_stack;
+    s->n_wide = (int64_t)img.wnodes.size();
+    s->n_sil = (int64_t)img.sils.size();
+    gqd::DevScene &d = s->dev;
+    d.dim = D;
+    for (int k = 0; k < 3; ++k) {
+        d.root_lo[k] = k < D ? img.root_lo[k] : 0.f;
+        d.root_hi[k] = k < D ? img.root_hi[k] : 0.f;
+    }
+    if (o.device < 0) {  // host-only scene: reference arrays, no device copy
+        const size_t words = img.wnodes.size() * sizeof(img.wnodes[0]) / 4;
+        s->wide_words.resize(words);
+        if (words) std::memcpy(s->wide_words.data(), img.wnodes.data(), words * 4);
+        *out = s.release();
+        return GQ_OK;
+    }
+    DeviceGuard g(o.device);
+    if (!g.ok) return fail(GQ_ERR_CUDA, "cannot select the scene's CUDA device");
+    gq_status st;
+    if ((st = s->upload(img.pairs, &d.pairs)) != GQ_OK) return st;
+    if ((st = s->upload(img.prims, &d.prims)) != GQ_OK) return st;
+    if ((st = s->upload(img.wnodes, &d.wnodes)) != GQ_OK) return st;
+    if ((st = s->upload(img.spairs, &d.spairs)) != GQ_OK) return st;
+    if ((st = s->upload(img.sils, &d.sils)) != GQ_OK) return st;
+    const void *pv = nullptr, *pi = nullptr, *pe = nullptr;
+    if ((st = s->upload(s->verts, &pv)) != GQ_OK) return st;
+    if ((st = s->upload(s->index, &pi)) != GQ_OK) return st;
+    std::vector<int32_t> zero(1, 0);
+    if ((st = s->upload(zero, &pe)) != GQ_OK) return st;
+    d.verts = (const float *)pv;
+    d.index = (const int32_t *)pi;
+    d.err = (int32_t *)pe;
+    d.n_prims = np;
+    d.root_ref = img.root_ref;
+    d.wroot_ref = img.wroot_ref;
+    d.sroot_ref = img.sroot_ref;
+    *out = s.release();
+    return GQ_OK;
+}
+
+bool on_host_only(const gq_scene *s) { return s->device < 0; }
+
+int resolve_variant(const gq_scene *s, const gq_query_opts *opts) {
+    int v = opts ? opts->variant : GQ_VARIANT_AUTO;
+    if (v == GQ_VARIANT_AUTO) v = s->has_wide ? GQ_VARIANT_WIDE8 : GQ_VARIANT_EXACT;
+    return v;
+}
+
+gq_status check_variant(const gq_scene *s, int v) {
+    if (v == GQ_VARIANT_WIDE8) {
+        if (!s->has_wide) return fail(GQ_ERR_UNSUPPORTED, "scene was built without the wide BVH");
+        if (s->wide_stack > GQ_STACK_WIDE) return fail(GQ_ERR_DEPTH, "wide tree needs a deeper stack than 96");
+    } else if (v == GQ_VARIANT_EXACT) {
+        if (s->exact_stack > GQ_STACK_EXACT)
+            return fail(GQ_ERR_DEPTH, "tree deeper than gQuery's 64-entry traversal stack");
+    } else {
+        return fail(GQ_ERR_INVALID, "unknown variant");
+    }
+    return GQ_OK;
+}
+
+bool vecs_ok(const gq_vecs &v) { return v.ptr != nullptr; }
+
+size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+// Stream-ordered scratch for the Morton permutation (caller-provided or allocated).
+struct Scratch {
+    void *p = nullptr;
+    bool owned = false;
+    cudaStream_t st = nullptr;
+    ~Scratch() {
+        if (owned && p) cudaFreeAsync(p, st);
+    }
+};
+
+gq_status prepare_order(const gq_scene *s, gq_vecs keys_from, int64_t n, const gq_query_opts *opts,
+                        cudaStream_t st, Scratch &scr, const int32_t **perm) {
+    *perm = nullptr;
+    if (opts && opts->order) {
+        *perm = opts->order;
+        return GQ_OK;
+    }
+    if (!opts || !opts->sort || n < 2) return GQ_OK;
+    const size_t need = (size_t)gq_query_scratch_bytes(n);
+    if (opts->scratch) {
+        if ((size_t)opts->scratch_bytes < need) return fail(GQ_ERR_INVALID, "scratch buffer too small");
+        scr.p = opts->scratch;
+    } else {
+        cudaError_t e = cudaMallocAsync(&scr.p, need, st);
+        if (e != cudaSuccess) return fail(GQ_ERR_NOMEM, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
+        scr.owned = true;
+        scr.st = st;
+    }
+    int32_t *pp = (int32_t *)scr.p;
+    char *rest = (char *)scr.p + align256((size_t)n * 4);
+    cudaError_t e = gqd::morton_order(s->dev, keys_from, n, pp, rest, need - align256((size_t)n * 4), st);
+    if (e != cudaSuccess) return fail_cuda(e, "morton_order");
+    *perm = pp;
+    return GQ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void gq_last_error(char *buf, int64_t cap) {
+    if (!buf || cap <= 0) return;
+    std::snprintf(buf, (size_t)cap, "%s", g_last_error.c_str());
+}
+
+const char *gq_status_string(gq_status s) {
+    switch (s) {
+        case GQ_OK: return "ok";
+        case GQ_ERR_INVALID: return "invalid argument";
+        case GQ_ERR_CUDA: return "CUDA error";
+        case GQ_ERR_NOMEM: return "out of memory";
+        case GQ_ERR_DEPTH: return "tree too deep for the traversal stack";
+        case GQ_ERR_DEVICE: return "device error flag raised";
+        case GQ_ERR_UNSUPPORTED: return "unsupported";
+        default: return "unknown status";
+    }
+}
+
+gq_status gq_scene_build_2d(const float *vertices, int64_t nv, const int32_t *edges, int64_t ne,
+                            const gq_build_opts *opts, gq_scene **out) {
+    return build_scene<2>(vertices, nv, edges, ne, opts, out);
+}
+
+gq_status gq_scene_build_3d(const float *vertices, int64_t nv, const int32_t *faces, int64_t nf,
+                            const gq_build_opts *opts, gq_scene **out) {
+    return build_scene<3>(vertices, nv, faces, nf, opts, out);
+}
+
+gq_status gq_scene_free(gq_scene *scene) {
+    delete scene;
+    return GQ_OK;
+}
+
+gq_status gq_scene_get_info(const gq_scene *s, gq_scene_info *info) {
+    if (!s || !info) return fail(GQ_ERR_INVALID, "null argument");
+    std::memset(info, 0, sizeof *info);
+    info->dim = s->dim;
+    info->n_vertices = s->nv;
+    info->n_prims = s->np;
+    info->n_nodes = s->dim == 2 ? (int64_t)s->t2.nodes.size() : (int64_t)s->t3.nodes.size();
+    info->n_wide_nodes = s->n_wide;
+    info->n_silhouettes = s->n_sil;
+    info->max_depth = s->dim == 2 ? s->t2.max_depth : s->t3.max_depth;
+    info->exact_stack = s->exact_stack;
+    info->wide_stack = s->wide_stack;
+    info->device_bytes = s->device_bytes;
+    for (int k = 0; k < 3; ++k) {
+        info->bbox_lo[k] = s->dev.root_lo[k];
+        info->bbox_hi[k] = s->dev.root_hi[k];
+    }
+    return GQ_OK;
+}
+
+gq_status gq_scene_ref_array(const gq_scene *s, int32_t which, float *dst, int64_t cap, int64_t *len) {
+    if (!s || !len) return fail(GQ_ERR_INVALID, "null argument");
+    std::vector<float> v;
+    if (which == GQ_ARRAY_WIDE_NODES) {
+        if (s->device >= 0) return fail(GQ_ERR_UNSUPPORTED, "wide node dump is kept for host-only scenes");
+        *len = (int64_t)s->wide_words.size();
+        if (dst && cap > 0)
+            std::memcpy(dst, s->wide_words.data(), sizeof(float) * (size_t)std::min<int64_t>(cap, *len));
+        return GQ_OK;
+    }
+    const bool snch_needed = which == GQ_ARRAY_SNCH_NODES || which == GQ_ARRAY_SILHOUETTES ||
+                             which == GQ_ARRAY_RAW_SILHOUETTES;
+    if (snch_needed && !s->has_snch) return fail(GQ_ERR_UNSUPPORTED, "scene was built without the SNCH");
+    if (s->dim == 2) {
+        PrimSource<2> src{s->verts.data(), s->nv, s->index.data(), s->np};
+        switch (which) {
+            case GQ_ARRAY_BVH_NODES: v = ref_node_data<2>(s->t2); break;
+            case GQ_ARRAY_PRIMITIVES: v = ref_prim_data<2>(src, s->t2); break;
+            case GQ_ARRAY_SNCH_NODES: v = ref_snch_node_data<2>(s->t2, s->s2); break;
+            case GQ_ARRAY_SILHOUETTES: v = ref_silhouette_data<2>(s->s2, true); break;
+            case GQ_ARRAY_RAW_SILHOUETTES: v = ref_silhouette_data<2>(s->s2, false); break;
+            default: return fail(GQ_ERR_INVALID, "unknown array id");
+        }
+    } else {
+        PrimSource<3> src{s->verts.data(), s->nv, s->index.data(), s->np};
+        switch (which) {
+            case GQ_ARRAY_BVH_NODES: v = ref_node_data<3>(s->t3); break;
+            case GQ_ARRAY_PRIMITIVES: v = ref_prim_data<3>(src, s->t3); break;
+            case GQ_ARRAY_SNCH_NODES: v = ref_snch_node_data<3>(s->t3, s->s3); break;
+            case GQ_ARRAY_SILHOUETTES: v = ref_silhouette_data<3>(s->s3, true); break;
+            case GQ_ARRAY_RAW_SILHOUETTES: v = ref_silhouette_data<3>(s->s3, false); break;
+            default: return fail(GQ_ERR_INVALID, "unknown array id");
+        }
+    }
+    *len = (int64_t)v.size();
+    if (dst && cap > 0) std::memcpy(dst, v.data(), sizeof(float) * (size_t)std::min<int64_t>(cap, *len));
+    return GQ_OK;
+}
+
+gq_status gq_flat_silhouette_edges(const float *vertices, int64_t nv, const int32_t *faces, int64_t nf, float *dst,
+                                   int64_t cap, int64_t *len) {
+    if (!vertices || !faces || !len) return fail(GQ_ERR_INVALID, "null argument");
+    PrimSource<3> src{vertices, nv, faces, nf};
+    std::string bad = validate_source<3>(src);
+    if (!bad.empty()) return fail(GQ_ERR_INVALID, bad);
+    SnchTree<3> tmp;
+    tmp.raw = build_silhouette_edges(src, nullptr);
+    std::vector<float> v = ref_silhouette_data<3>(tmp, false);
+    *len = (int64_t)v.size();
+    if (dst && cap > 0) std::memcpy(dst, v.data(), sizeof(float) * (size_t)std::min<int64_t>(cap, *len));
+    return GQ_OK;
+}
+
+int64_t gq_query_scratch_bytes(int64_t n) {
+    if (n <= 0) return 0;
+    return (int64_t)(align256((size_t)n * 4) + gqd::morton_scratch_bytes(n));
+}
+
+int64_t gq_order_scratch_bytes(int64_t n) {
+    if (n <= 0) return 0;
+    return (int64_t)gqd::morton_scratch_bytes(n);
+}
+
+gq_status gq_query_order(const gq_scene *s, gq_vecs points, int64_t n, int32_t *order, void *scratch,
+                         int64_t scratch_bytes, void *stream) {
+    if (!s || !order) return fail(GQ_ERR_INVALID, "null scene or order");
+    if (n < 0) return fail(GQ_ERR_INVALID, "negative count");
+    if (n == 0) return GQ_OK;
+    if (!vecs_ok(points)) return fail(GQ_ERR_INVALID, "null point array");
+    if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "scene was built without a device copy");
+    DeviceGuard g(s->device);
+    cudaStream_t cs = (cudaStream_t)stream;
+    const size_t need = gqd::morton_scratch_bytes(n);
+    Scratch scr;
+    if (scratch) {
+        if ((size_t)scratch_bytes < need) return fail(GQ_ERR_INVALID, "scratch buffer too small");
+        scr.p = scratch;
+    } else {
+        cudaError_t e = cudaMallocAsync(&scr.p, need, cs);
+        if (e != cudaSuccess) return fail(GQ_ERR_NOMEM, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
+        scr.owned = true;
+        scr.st = cs;
+    }
+    cudaError_t e = gqd::morton_order(s->dev, points, n, order, scr.p, need, cs);
+    if (e != cudaSuccess) return fail_cuda(e, "morton_order");
+    return GQ_OK;
+}
+
+gq_status gq_closest_point(const gq_scene *s, gq_vecs q, int64_t n, const gq_cp_out *out, const gq_query_opts *opts,
+                           void *stream) {
+    if (!s || !out) return fail(GQ_ERR_INVALID, "null scene or output");
+    if (n < 0) return fail(GQ_ERR_INVALID, "negative query count");
+    if (n == 0) return GQ_OK;
+    if (!vecs_ok(q)) return fail(GQ_ERR_INVALID, "null query array");
+    const int v = resolve_variant(s, opts);
+    gq_status st = check_variant(s, v);
+    if (st != GQ_OK) return st;
+    if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "scene was built without a device copy");
+    DeviceGuard g(s->device);
+    cudaStream_t cs = (cudaStream_t)stream;
+    Scratch scr;
+    const int32_t *perm = nullptr;
+    if ((st = prepare_order(s, q, n, opts, cs, scr, &perm)) != GQ_OK) return st;
+    cudaError_t e = gqd::launch_cp(s->dev, v, q, n, perm, *out, cs);
+    if (e != cudaSuccess) return fail_cuda(e, "closest_point launch");
+    return GQ_OK;
+}
+
+gq_status gq_intersect(const gq_scene *s, gq_vecs origin, gq_vecs dir, const float *r_max, int64_t n,
+                       const gq_ray_out *out, const gq_query_opts *opts, void *stream) {
+    if (!s || !out) return fail(GQ_ERR_INVALID, "null scene or output");
+    if (n < 0) return fail(GQ_ERR_INVALID, "negative query count");
+    if (n == 0) return GQ_OK;
+    if (!vecs_ok(origin) || !vecs_ok(dir)) return fail(GQ_ERR_INVALID, "null ray array");
+    const int v = resolve_variant(s, opts);
+    gq_status st = check_variant(s, v);
+    if (st != GQ_OK) return st;
+    if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "scene was built without a device copy");
+    DeviceGuard g(s->device);
+    cudaStream_t cs = (cudaStream_t)stream;
+    Scratch scr;
+    const int32_t *perm = nullptr;
+    if ((st = prepare_order(s, origin, n, opts, cs, scr, &perm)) != GQ_OK) return st;
+    cudaError_t e = gqd::launch_ray(s->dev, v, origin, dir, r_max, n, perm, *out, cs);
+    if (e != cudaSuccess) return fail_cuda(e, "intersect launch");
+    return GQ_OK;
+}
+
+gq_status gq_closest_silhouette(const gq_scene *s, gq_vecs x, const float *r_max, int64_t n, const gq_sil_out *out,
+                                const gq_query_opts *opts, void *stream) {
+    if (!s || !out) return fail(GQ_ERR_INVALID, "null scene or output");
+    if (n < 0) return fail(GQ_ERR_INVALID, "negative query count");
+    if (n == 0) return GQ_OK;
+    if (!vecs_ok(x)) return fail(GQ_ERR_INVALID, "null query array");
+    if (!s->has_snch) return fail(GQ_ERR_UNSUPPORTED, "scene was built without the SNCH");
+    if (s->exact_stack > GQ_STACK_EXACT) return fail(GQ_ERR_DEPTH, "tree deeper than gQuery's 64-entry stack");
+    if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "scene was built without a device copy");
+    DeviceGuard g(s->device);
+    cudaStream_t cs = (cudaStream_t)stream;
+    Scratch scr;
+    const int32_t *perm = nullptr;
+    gq_status st;
+    if ((st = prepare_order(s, x, n, opts, cs, scr, &perm)) != GQ_OK) return st;
+    cudaError_t e = gqd::launch_sil(s->dev, x, r_max, n, perm, *out, cs);
+    if (e != cudaSuccess) return fail_cuda(e, "closest_silhouette launch");
+    return GQ_OK;
+}
+
+gq_status gq_closest_point_brute(const gq_scene *s, gq_vecs q, int64_t n, const gq_cp_out *out, void *stream) {
+    if (!s || !out) return fail(GQ_ERR_INVALID, "null scene or output");
+    if (n < 0) return fail(GQ_ERR_INVALID, "negative query count");
+    if (n == 0) return GQ_OK;
+    if (!vecs_ok(q)) return fail(GQ_ERR_INVALID, "null query array");
+    if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "scene was built without a device copy");
+    DeviceGuard g(s->device);
+    cudaError_t e = gqd::launch_cp_brute(s->dev, q, n, *out, (cudaStream_t)stream);
+    if (e != cudaSuccess) return fail_cuda(e, "closest_point_brute launch");
+    return GQ_OK;
+}
+
+gq_status gq_intersect_brute(const gq_scene *s, gq_vecs origin, gq_vecs dir, const float *r_max, int64_t n,
+                             const gq_ray_out *out, void *stream) {
+    if (!s || !out) return fail(GQ_ERR_INVALID, "null scene or output");
+    if (n < 0) return fail(GQ_ERR_INVALID, "negative query count");
+    if (n == 0) return GQ_OK;
+    if (!vecs_ok(origin) || !vecs_ok(dir)) return fail(GQ_ERR_INVALID, "null ray array");
+    if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "scene was built without a device copy");
+    DeviceGuard g(s->device);
+    cudaError_t e = gqd::launch_ray_brute(s->dev, origin, dir, r_max, n, *out, (cudaStream_t)stream);
+    if (e != cudaSuccess) return fail_cuda(e, "intersect_brute launch");
+    return GQ_OK;
+}
+
+gq_status gq_brute_f64(const gq_scene *s, int32_t kind, gq_vecs a, gq_vecs b, int64_t n, double *out_d,
+                       int32_t *out_id, void *stream) {
+    if (!s || !out_d || !out_id) return fail(GQ_ERR_INVALID, "null argument");
+    if (kind != 0 && kind != 1) return fail(GQ_ERR_INVALID, "kind must be 0 or 1");
+    if (n < 0) return fail(GQ_ERR_INVALID, "negative query count");
+    if (n == 0) return GQ_OK;
+    if (!vecs_ok(a) || (kind == 1 && !vecs_ok(b))) return fail(GQ_ERR_INVALID, "null query array");
+    if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "scene was built without a device copy");
+    DeviceGuard g(s->device);
+    cudaError_t e = gqd::launch_brute_f64(s->dev, kind, a, b, n, out_d, out_id, (cudaStream_t)stream);
+    if (e != cudaSuccess) return fail_cuda(e, "brute_f64 launch");
+    return GQ_OK;
+}
+
+gq_status gq_scene_device_error(const gq_scene *s, void *stream, int32_t *flags) {
+    if (!s || !flags) return fail(GQ_ERR_INVALID, "null argument");
+    if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "scene was built without a device copy");
+    DeviceGuard g(s->device);
+    cudaStream_t cs = (cudaStream_t)stream;
+    int32_t v = 0;
+    cudaError_t e = cudaMemcpyAsync(&v, s->dev.err, sizeof v, cudaMemcpyDeviceToHost, cs);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cs);
+    if (e == cudaSuccess && v != 0) e = cudaMemsetAsync(s->dev.err, 0, sizeof v, cs);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cs);
+    if (e != cudaSuccess) return fail_cuda(e, "device error read");
+    *flags = v;
+    return GQ_OK;
+}
+
+}  // extern "C"

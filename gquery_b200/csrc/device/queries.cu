@@ -1,0 +1,1367 @@
+// Query kernels for sm_100a: binary "exact" traversals that follow gQuery's visit
+// order step for step, quantised 8-wide traversals, brute-force scans and the
+// Morton reordering of queries.  Compiled with --fmad=false (see gq_fmath.h).
+#include <cub/cub.cuh>
+
+#include "prim.cuh"
+#include "queries.cuh"
+
+namespace gqd {
+
+namespace {
+
+constexpr int kBlock = 128;
+
+__device__ __forceinline__ float qget(const gq_vecs &v, int64_t i, int k) {
+    return v.ptr[(int64_t)k * v.comp_stride + i * v.elem_stride];
+}
+
+__device__ __forceinline__ void flag_error(int32_t *err, int bits) {
+    if (err) atomicOr(err, bits);
+}
+
+// Record writers (SoA, component stride n).  A miss writes zeros.
+__device__ __forceinline__ void put1(float *p, int64_t i, float v) {
+    if (p) p[i] = v;
+}
+__device__ __forceinline__ void put2(float *p, int64_t n, int64_t i, float a, float b) {
+    if (p) {
+        p[i] = a;
+        p[n + i] = b;
+    }
+}
+__device__ __forceinline__ void put3(float *p, int64_t n, int64_t i, float a, float b, float c) {
+    if (p) {
+        p[i] = a;
+        p[n + i] = b;
+        p[2 * n + i] = c;
+    }
+}
+
+// Batcher odd-even merge sort of 8 (key, ref) pairs, ascending keys.
+__device__ __forceinline__ void cas(float &ka, int &ra, float &kb, int &rb) {
+    const bool sw = kb < ka;
+    const float k0 = sw ? kb : ka, k1 = sw ? ka : kb;
+    const int r0 = sw ? rb : ra, r1 = sw ? ra : rb;
+    ka = k0; kb = k1; ra = r0; rb = r1;
+}
+__device__ __forceinline__ void sort8(float (&k)[8], int (&r)[8]) {
+    cas(k[0], r[0], k[1], r[1]); cas(k[2], r[2], k[3], r[3]); cas(k[4], r[4], k[5], r[5]); cas(k[6], r[6], k[7], r[7]);
+    cas(k[0], r[0], k[2], r[2]); cas(k[1], r[1], k[3], r[3]); cas(k[4], r[4], k[6], r[6]); cas(k[5], r[5], k[7], r[7]);
+    cas(k[1], r[1], k[2], r[2]); cas(k[5], r[5], k[6], r[6]);
+    cas(k[0], r[0], k[4], r[4]); cas(k[1], r[1], k[5], r[5]); cas(k[2], r[2], k[6], r[6]); cas(k[3], r[3], k[7], r[7]);
+    cas(k[2], r[2], k[4], r[4]); cas(k[3], r[3], k[5], r[5]);
+    cas(k[1], r[1], k[2], r[2]); cas(k[3], r[3], k[4], r[4]); cas(k[5], r[5], k[6], r[6]);
+}
+
+__device__ __forceinline__ float exp_scale(uint32_t meta, int ax) {
+    return __int_as_float((int)((meta >> (8 * ax)) & 0xffu) << 23);
+}
+__device__ __forceinline__ float qbyte(uint32_t lo4, uint32_t hi4, int k) {
+    const uint32_t w = (k < 4) ? lo4 : hi4;
+    return (float)((w >> (8 * (k & 3))) & 0xffu);
+}
+
+__device__ __forceinline__ int64_t query_index(const int32_t *perm, int64_t i) {
+    return perm ? (int64_t)__ldg(perm + i) : i;
+}
+
+// ===========================================================================
+// Closest point, 3D
+// ===========================================================================
+
+__device__ __forceinline__ void cp3_leaf(const void *prims, int ref, float px, float py, float pz, float &r_max,
+                                         int &idx) {
+    int j = ~ref;
+    for (;;) {
+        const float4 t0 = ldg4(prims, 3 * (int64_t)j), t1 = ldg4(prims, 3 * (int64_t)j + 1),
+                     t2 = ldg4(prims, 3 * (int64_t)j + 2);
+        const float d =
+            tri_closest<false>(px, py, pz, t0.x, t0.y, t0.z, t0.w, t1.x, t1.y, t1.z, t1.w, t2.x);
+        if (d < r_max) {
+            r_max = d;
+            idx = j;
+        }
+        if (fbits(t2.z) & GQ_ITEM_LAST) break;
+        ++j;
+    }
+}
+
+// Triangle.closest_point (triangle.py:76-81)
+__device__ __forceinline__ void cp3_record(const void *prims, int idx, bool ok, float px, float py, float pz,
+                                           const gq_cp_out &o, int64_t n, int64_t qi) {
+    float pt[3] = {0.f, 0.f, 0.f}, nx = 0.f, ny = 0.f, nz = 0.f, u = 0.f, v = 0.f, d = 0.f;
+    int pid = 0;
+    if (ok) {
+        const float4 t0 = ldg4(prims, 3 * (int64_t)idx), t1 = ldg4(prims, 3 * (int64_t)idx + 1),
+                     t2 = ldg4(prims, 3 * (int64_t)idx + 2);
+        d = tri_closest<true>(px, py, pz, t0.x, t0.y, t0.z, t0.w, t1.x, t1.y, t1.z, t1.w, t2.x, pt, &u, &v);
+        float cx, cy, cz;
+        cross3(t0.w - t0.x, t1.x - t0.y, t1.y - t0.z, t1.z - t0.x, t1.w - t0.y, t2.x - t0.z, cx, cy, cz);
+        const float inv = gq_rsqrt(gq_dot3(cx, cy, cz, cx, cy, cz));
+        nx = cx * inv;
+        ny = cy * inv;
+        nz = cz * inv;
+        pid = fbits(t2.y);
+    }
+    if (o.valid) o.valid[qi] = ok ? 1 : 0;
+    put3(o.p, n, qi, pt[0], pt[1], pt[2]);
+    put3(o.n, n, qi, nx, ny, nz);
+    put2(o.t, n, qi, u, v);
+    put1(o.d, qi, d);
+    if (o.prim_id) o.prim_id[qi] = pid;
+}
+
+// BVH3D.closest_point (bvh3d.py:108-174), same pops, pushes and tests.
+__global__ void __launch_bounds__(kBlock) k_cp3_exact(DevScene s, gq_vecs q, int64_t n, const int32_t *perm,
+                                                       gq_cp_out o) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t qi = query_index(perm, i);
+    const float px = qget(q, qi, 0), py = qget(q, qi, 1), pz = qget(q, qi, 2);
+    float r_max = kInf;
+    int idx = -1;
+    int2 stk[GQ_STACK_EXACT];
+    int sp = 0;
+    stk[0] = make_int2(s.root_ref, fbits(kInf));
+    bool ovf = false;
+    while (sp >= 0) {
+        const int2 e = stk[sp--];
+        if (!(__int_as_float(e.y) <= r_max)) continue;
+        if (e.x < 0) {
+            cp3_leaf(s.prims, e.x, px, py, pz, r_max, idx);
+            continue;
+        }
+        const float4 a = ldg4(s.pairs, 4 * (int64_t)e.x), b = ldg4(s.pairs, 4 * (int64_t)e.x + 1),
+                     c = ldg4(s.pairs, 4 * (int64_t)e.x + 2), r = ldg4(s.pairs, 4 * (int64_t)e.x + 3);
+        float dminl, dmaxl, dminr, dmaxr;
+        box_dist3(a.x, a.y, a.z, a.w, b.x, b.y, px, py, pz, dminl, dmaxl);
+        const bool hl = dminl <= r_max;
+        r_max = fminf(r_max, dmaxl);
+        box_dist3(b.z, b.w, c.x, c.y, c.z, c.w, px, py, pz, dminr, dmaxr);
+        const bool hr = dminr <= r_max;
+        r_max = fminf(r_max, dmaxr);
+        const int rl = fbits(r.x), rr = fbits(r.y);
+        if (hl & hr) {
+            if (sp + 2 >= GQ_STACK_EXACT) {
+                ovf = true;
+                break;
+            }
+            const bool sw = dminr < dminl;
+            stk[++sp] = sw ? make_int2(rl, fbits(dminl)) : make_int2(rr, fbits(dminr));
+            stk[++sp] = sw ? make_int2(rr, fbits(dminr)) : make_int2(rl, fbits(dminl));
+        } else if (hl) {
+            stk[++sp] = make_int2(rl, fbits(dminl));
+        } else if (hr) {
+            stk[++sp] = make_int2(rr, fbits(dminr));
+        }
+    }
+    if (ovf) flag_error(s.err, GQ_DEVERR_STACK);
+    cp3_record(s.prims, idx, (idx >= 0) && !ovf, px, py, pz, o, n, qi);
+}
+
+// Quantised 8-wide closest point, 3D.  All children of a node are tested at once:
+// r_max shrinks to the smallest child d_max (the farthest-corner bound of
+// bvh3d.py:141-144), children with d_min <= r_max are pushed nearest-last.
+__global__ void __launch_bounds__(kBlock) k_cp3_wide(DevScene s, gq_vecs q, int64_t n, const int32_t *perm,
+                                                      gq_cp_out o) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t qi = query_index(perm, i);
+    const float px = qget(q, qi, 0), py = qget(q, qi, 1), pz = qget(q, qi, 2);
+    float r_max = kInf;
+    int idx = -1;
+    int2 stk[GQ_STACK_WIDE];
+    int sp = 0;
+    stk[0] = make_int2(s.wroot_ref, fbits(kInf));
+    bool ovf = false;
+    while (sp >= 0) {
+        const int2 e = stk[sp--];
+        if (!(__int_as_float(e.y) <= r_max)) continue;
+        if (e.x < 0) {
+            cp3_leaf(s.prims, e.x, px, py, pz, r_max, idx);
+            continue;
+        }
+        const int64_t base = 6 * (int64_t)e.x;
+        const float4 h = ldg4(s.wnodes, base);
+        const int4 r0 = __ldg(reinterpret_cast<const int4 *>(s.wnodes) + base + 1);
+        const int4 r1 = __ldg(reinterpret_cast<const int4 *>(s.wnodes) + base + 2);
+        const uint4 q0 = __ldg(reinterpret_cast<const uint4 *>(s.wnodes) + base + 3);
+        const uint4 q1 = __ldg(reinterpret_cast<const uint4 *>(s.wnodes) + base + 4);
+        const uint4 q2 = __ldg(reinterpret_cast<const uint4 *>(s.wnodes) + base + 5);
+        const uint32_t meta = (uint32_t)fbits(h.w);
+        const int nc = (int)(meta >> 24);
+        const float sx = exp_scale(meta, 0), sy = exp_scale(meta, 1), sz = exp_scale(meta, 2);
+        float key[8], dmx[8];
+        int ref[8] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
+        float shrink = kInf;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const float lox = __fmaf_rn(qbyte(q0.x, q0.y, k), sx, h.x);
+            const float loy = __fmaf_rn(qbyte(q0.z, q0.w, k), sy, h.y);
+            const float loz = __fmaf_rn(qbyte(q1.x, q1.y, k), sz, h.z);
+            const float hix = __fmaf_rn(qbyte(q1.z, q1.w, k), sx, h.x);
+            const float hiy = __fmaf_rn(qbyte(q2.x, q2.y, k), sy, h.y);
+            const float hiz = __fmaf_rn(qbyte(q2.z, q2.w, k), sz, h.z);
+            box_dist3(lox, loy, loz, hix, hiy, hiz, px, py, pz, key[k], dmx[k]);
+            if (k < nc) shrink = fminf(shrink, dmx[k]);
+        }
+        r_max = fminf(r_max, shrink);
+        int cnt = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const bool hit = (k < nc) && (key[k] <= r_max);
+            key[k] = hit ? key[k] : kInf;
+            cnt += hit ? 1 : 0;
+        }
+        if (sp + cnt >= GQ_STACK_WIDE) {
+            ovf = true;
+            break;
+        }
+        sort8(key, ref);
+#pragma unroll
+        for (int k = 7; k >= 0; --k)
+            if (k < cnt) stk[++sp] = make_int2(ref[k], fbits(key[k]));
+    }
+    if (ovf) flag_error(s.err, GQ_DEVERR_STACK);
+    cp3_record(s.prims, idx, (idx >= 0) && !ovf, px, py, pz, o, n, qi);
+}
+
+// ===========================================================================
+// Closest point, 2D
+// ===========================================================================
+
+__device__ __forceinline__ void cp2_leaf(const void *prims, int ref, float px, float py, float &r_max, int &idx) {
+    int j = ~ref;
+    for (;;) {
+        const float4 a = ldg4(prims, 2 * (int64_t)j);
+        const int4 f = __ldg(reinterpret_cast<const int4 *>(prims) + 2 * (int64_t)j + 1);
+        const float d = seg_dist(px, py, a.x, a.y, a.z, a.w);
+        if (d < r_max) {
+            r_max = d;
+            idx = j;
+        }
+        if (f.y & GQ_ITEM_LAST) break;
+        ++j;
+    }
+}
+
+// LineSegment.closest_point (line_segment.py:64-78)
+__device__ __forceinline__ void cp2_record(const void *prims, int idx, bool ok, float px, float py,
+                                           const gq_cp_out &o, int64_t n, int64_t qi) {
+    float ix = 0.f, iy = 0.f, nx = 0.f, ny = 0.f, h = 0.f, d = 0.f;
+    int pid = 0;
+    if (ok) {
+        const float4 a = ldg4(prims, 2 * (int64_t)idx);
+        const int4 f = __ldg(reinterpret_cast<const int4 *>(prims) + 2 * (int64_t)idx + 1);
+        const float pax = px - a.x, pay = py - a.y, bax = a.z - a.x, bay = a.w - a.y;
+        const float inv = gq_rsqrt(gq_dot2(bax, bay, bax, bay));
+        const float tx = bax * inv, ty = bay * inv;
+        nx = ty;
+        ny = -tx;
+        h = gq_clamp(gq_div(gq_dot2(pax, pay, bax, bay), gq_dot2(bax, bay, bax, bay)), 0.f, 1.f);
+        ix = a.x + bax * h;
+        iy = a.y + bay * h;
+        d = gq_norm2(ix - px, iy - py);
+        pid = f.x;
+    }
+    if (o.valid) o.valid[qi] = ok ? 1 : 0;
+    put2(o.p, n, qi, ix, iy);
+    put2(o.n, n, qi, nx, ny);
+    put1(o.t, qi, h);
+    put1(o.d, qi, d);
+    if (o.prim_id) o.prim_id[qi] = pid;
+}
+
+// BVH.closest_point (bvh.py:127-198)
+__global__ void __launch_bounds__(kBlock) k_cp2_exact(DevScene s, gq_vecs q, int64_t n, const int32_t *perm,
+                                                       gq_cp_out o) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t qi = query_index(perm, i);
+    const float px = qget(q, qi, 0), py = qget(q, qi, 1);
+    float r_max = kInf;
+    int idx = -1;
+    int2 stk[GQ_STACK_EXACT];
+    int sp = 0;
+    stk[0] = make_int2(s.root_ref, fbits(kInf));
+    bool ovf = false;
+    while (sp >= 0) {
+        const int2 e = stk[sp--];
+        if (!(__int_as_float(e.y) <= r_max)) continue;
+        if (e.x < 0) {
+            cp2_leaf(s.prims, e.x, px, py, r_max, idx);
+            continue;
+        }
+        const float4 a = ldg4(s.pairs, 3 * (int64_t)e.x), b = ldg4(s.pairs, 3 * (int64_t)e.x + 1);
+        const int4 r = __ldg(reinterpret_cast<const int4 *>(s.pairs) + 3 * (int64_t)e.x + 2);
+        float dminl, dmaxl, dminr, dmaxr;
+        box_dist2(a.x, a.y, a.z, a.w, px, py, dminl, dmaxl);
+        const bool hl = dminl <= r_max;
+        r_max = fminf(r_max, dmaxl);
+        box_dist2(b.x, b.y, b.z, b.w, px, py, dminr, dmaxr);
+        const bool hr = dminr <= r_max;
+        r_max = fminf(r_max, dmaxr);
+        if (hl & hr) {
+            if (sp + 2 >= GQ_STACK_EXACT) {
+                ovf = true;
+                break;
+            }
+            const bool sw = dminr < dminl;
+            stk[++sp] = sw ? make_int2(r.x, fbits(dminl)) : make_int2(r.y, fbits(dminr));
+            stk[++sp] = sw ? make_int2(r.y, fbits(dminr)) : make_int2(r.x, fbits(dminl));
+        } else if (hl) {
+            stk[++sp] = make_int2(r.x, fbits(dminl));
+        } else if (hr) {
+            stk[++sp] = make_int2(r.y, fbits(dminr));
+        }
+    }
+    if (ovf) flag_error(s.err, GQ_DEVERR_STACK);
+    cp2_record(s.prims, idx, (idx != -1) && !ovf, px, py, o, n, qi);
+}
+
+__global__ void __launch_bounds__(kBlock) k_cp2_wide(DevScene s, gq_vecs q, int64_t n, const int32_t *perm,
+                                                      gq_cp_out o) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t qi = query_index(perm, i);
+    const float px = qget(q, qi, 0), py = qget(q, qi, 1);
+    float r_max = kInf;
+    int idx = -1;
+    int2 stk[GQ_STACK_WIDE];
+    int sp = 0;
+    stk[0] = make_int2(s.wroot_ref, fbits(kInf));
+    bool ovf = false;
+    while (sp >= 0) {
+        const int2 e = stk[sp--];
+        if (!(__int_as_float(e.y) <= r_max)) continue;
+        if (e.x < 0) {
+            cp2_leaf(s.prims, e.x, px, py, r_max, idx);
+            continue;
+        }
+        const int64_t base = 5 * (int64_t)e.x;
+        const float4 h = ldg4(s.wnodes, base);
+        const int4 r0 = __ldg(reinterpret_cast<const int4 *>(s.wnodes) + base + 1);
+        const int4 r1 = __ldg(reinterpret_cast<const int4 *>(s.wnodes) + base + 2);
+        const uint4 q0 = __ldg(reinterpret_cast<const uint4 *>(s.wnodes) + base + 3);
+        const uint4 q1 = __ldg(reinterpret_cast<const uint4 *>(s.wnodes) + base + 4);
+        const uint32_t meta = (uint32_t)fbits(h.z);
+        const int nc = (int)(meta >> 24);
+        const float sx = exp_scale(meta, 0), sy = exp_scale(meta, 1);
+        float key[8], dmx[8];
+        int ref[8] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
+        float shrink = kInf;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const float lox = __fmaf_rn(qbyte(q0.x, q0.y, k), sx, h.x);
+            const float loy = __fmaf_rn(qbyte(q0.z, q0.w, k), sy, h.y);
+            const float hix = __fmaf_rn(qbyte(q1.x, q1.y, k), sx, h.x);
+            const float hiy = __fmaf_rn(qbyte(q1.z, q1.w, k), sy, h.y);
+            box_dist2(lox, loy, hix, hiy, px, py, key[k], dmx[k]);
+            if (k < nc) shrink = fminf(shrink, dmx[k]);
+        }
+        r_max = fminf(r_max, shrink);
+        int cnt = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const bool hit = (k < nc) && (key[k] <= r_max);
+            key[k] = hit ? key[k] : kInf;
+            cnt += hit ? 1 : 0;
+        }
+        if (sp + cnt >= GQ_STACK_WIDE) {
+            ovf = true;
+            break;
+        }
+        sort8(key, ref);
+#pragma unroll
+        for (int k = 7; k >= 0; --k)
+            if (k < cnt) stk[++sp] = make_int2(ref[k], fbits(key[k]));
+    }
+    if (ovf) flag_error(s.err, GQ_DEVERR_STACK);
+    cp2_record(s.prims, idx, (idx != -1) && !ovf, px, py, o, n, qi);
+}
+
+// ===========================================================================
+// Ray intersection, 3D
+// ===========================================================================
+
+__device__ __forceinline__ void ray3_leaf(const void *prims, int ref, float xx, float xy, float xz, float vx,
+                                          float vy, float vz, float &r_max, int &idx) {
+    int j = ~ref;
+    for (;;) {
+        const float4 t0 = ldg4(prims, 3 * (int64_t)j), t1 = ldg4(prims, 3 * (int64_t)j + 1),
+                     t2 = ldg4(prims, 3 * (int64_t)j + 2);
+        const float d = tri_ray(xx, xy, xz, vx, vy, vz, t0.x, t0.y, t0.z, t0.w, t1.x, t1.y, t1.z, t1.w, t2.x, kInf);
+        if (d < r_max) {
+            r_max = d;
+            idx = j;
+        }
+        if (fbits(t2.z) & GQ_ITEM_LAST) break;
+        ++j;
+    }
+}
+
+// Triangle.ray_intersect (triangle.py:49-73) re-run on the winner with r_max = its t.
+__device__ __forceinline__ void ray3_record(const void *prims, int idx, bool found, float xx, float xy, float xz,
+                                            float vx, float vy, float vz, float r_max, const gq_ray_out &o,
+                                            int64_t n, int64_t qi) {
+    float px = 0.f, py = 0.f, pz = 0.f, nx = 0.f, ny = 0.f, nz = 0.f, u = 0.f, w0 = 0.f, d = 0.f;
+    int pid = 0;
+    bool ok = false;
+    if (found) {
+        const float4 t0 = ldg4(prims, 3 * (int64_t)idx), t1 = ldg4(prims, 3 * (int64_t)idx + 1),
+                     t2 = ldg4(prims, 3 * (int64_t)idx + 2);
+        float vv = __builtin_nanf(""), ww = 0.f;
+        const float t = tri_ray(xx, xy, xz, vx, vy, vz, t0.x, t0.y, t0.z, t0.w, t1.x, t1.y, t1.z, t1.w, t2.x, r_max,
+                                &vv, &ww);
+        ok = (vv == vv);
+        if (ok) {
+            const float v1x = t0.w - t0.x, v1y = t1.x - t0.y, v1z = t1.y - t0.z;
+            const float v2x = t1.z - t0.x, v2y = t1.w - t0.y, v2z = t2.x - t0.z;
+            px = (t0.x + v1x * vv) + v2x * ww;
+            py = (t0.y + v1y * vv) + v2y * ww;
+            pz = (t0.z + v1z * vv) + v2z * ww;
+            float cx, cy, cz;
+            cross3(v1x, v1y, v1z, v2x, v2y, v2z, cx, cy, cz);
+            const float inv = gq_rsqrt(gq_dot3(cx, cy, cz, cx, cy, cz));
+            nx = cx * inv;
+            ny = cy * inv;
+            nz = cz * inv;
+            u = 1.f - vv - ww;
+            w0 = vv;
+            d = t;
+            pid = fbits(t2.y);
+        }
+    }
+    if (o.valid) o.valid[qi] = ok ? 1 : 0;
+    put3(o.p, n, qi, px, py, pz);
+    put3(o.n, n, qi, nx, ny, nz);
+    put2(o.t, n, qi, u, w0);
+    put1(o.d, qi, d);
+    if (o.prim_id) o.prim_id[qi] = pid;
+    if (o.on_boundary) o.on_boundary[qi] = ok ? 1 : 0;
+}
+
+// BVH3D.intersect (bvh3d.py:176-239)
+__global__ void __launch_bounds__(kBlock) k_ray3_exact(DevScene s, gq_vecs x, gq_vecs v, const float *rmax_in,
+                                                        int64_t n, const int32_t *perm, gq_ray_out o) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t qi = query_index(perm, i);
+    const float xx = qget(x, qi, 0), xy = qget(x, qi, 1), xz = qget(x, qi, 2);
+    const float vx = qget(v, qi, 0), vy = qget(v, qi, 1), vz = qget(v, qi, 2);
+    float r_max = rmax_in ? rmax_in[qi] : kInf;
+    int idx = -1;
+    bool ovf = false;
+    float t_root;
+    if (box_ray3(s.root_lo[0], s.root_lo[1], s.root_lo[2], s.root_hi[0], s.root_hi[1], s.root_hi[2], xx, xy, xz, vx,
+                 vy, vz, r_max, t_root)) {
+        int2 stk[GQ_STACK_EXACT];
+        int sp = 0;
+        stk[0] = make_int2(s.root_ref, fbits(t_root));
+        while (sp >= 0) {
+            const int2 e = stk[sp--];
+            if (!(__int_as_float(e.y) <= r_max)) continue;
+            if (e.x < 0) {
+                ray3_leaf(s.prims, e.x, xx, xy, xz, vx, vy, vz, r_max, idx);
+                continue;
+            }
+            const float4 a = ldg4(s.pairs, 4 * (int64_t)e.x), b = ldg4(s.pairs, 4 * (int64_t)e.x + 1),
+                         c = ldg4(s.pairs, 4 * (int64_t)e.x + 2), r = ldg4(s.pairs, 4 * (int64_t)e.x + 3);
+            float t0, t1;
+            const bool h0 = box_ray3(a.x, a.y, a.z, a.w, b.x, b.y, xx, xy, xz, vx, vy, vz, r_max, t0);
+            const bool h1 = box_ray3(b.z, b.w, c.x, c.y, c.z, c.w, xx, xy, xz, vx, vy, vz, r_max, t1);
+            const int rl = fbits(r.x), rr = fbits(r.y);
+            if (h0 & h1) {
+                if (sp + 2 >= GQ_STACK_EXACT) {
+                    ovf = true;
+                    break;
+                }
+                const bool sw = t1 < t0;
+                stk[++sp] = sw ? make_int2(rl, fbits(t0)) : make_int2(rr, fbits(t1));
+                stk[++sp] = sw ? make_int2(rr, fbits(t1)) : make_int2(rl, fbits(t0));
+            } else if (h0) {
+                stk[++sp] = make_int2(rl, fbits(t0));
+            } else if (h1) {
+                stk[++sp] = make_int2(rr, fbits(t1));
+            }
+        }
+    }
+    if (ovf) flag_error(s.err, GQ_DEVERR_STACK);
+    ray3_record(s.prims, idx, (idx >= 0) && !ovf, xx, xy, xz, vx, vy, vz, r_max, o, n, qi);
+}
+
+// Quantised 8-wide ray traversal, 3D.  Slab tests use the reciprocal direction and
+// a far distance widened by 2^-21 so that rounding never drops a child the exact
+// test would enter.
+__global__ void __launch_bounds__(kBlock) k_ray3_wide(DevScene s, gq_vecs x, gq_vecs v, const float *rmax_in,
+                                                       int64_t n, const int32_t *perm, gq_ray_out o) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t qi = query_index(perm, i);
+    const float xx = qget(x, qi, 0), xy = qget(x, qi, 1), xz = qget(x, qi, 2);
+    const float vx = qget(v, qi, 0), vy = qget(v, qi, 1), vz = qget(v, qi, 2);
+    const float ix = gq_div(1.f, vx), iy = gq_div(1.f, vy), iz = gq_div(1.f, vz);
+    float r_max = rmax_in ? rmax_in[qi] : kInf;
+    int idx = -1;
+    bool ovf = false;
+    float t_root;
+    if (box_ray3(s.root_lo[0], s.root_lo[1], s.root_lo[2], s.root_hi[0], s.root_hi[1], s.root_hi[2], xx, xy, xz, vx,
+                 vy, vz, r_max, t_root)) {
+        int2 stk[GQ_STACK_WIDE];
+        int sp = 0;
+        stk[0] = make_int2(s.wroot_ref, fbits(t_root));
+        while (sp >= 0) {
+            const int2 e = stk[sp--];
+            if (!(__int_as_float(e.y) <= r_max)) continue;
+            if (e.x < 0) {
+                ray3_leaf(s.prims, e.x, xx, xy, xz, vx, vy, vz, r_max, idx);
+                continue;
+            }
+            const int64_t base = 6 * (int64_t)e.x;
+            const float4 h = ldg4(s.wnodes, base);
+            const int4 r0 = __ldg(reinterpret_cast<const int4 *>(s.wnodes) + base + 1);
+            const int4 r1 = __ldg(reinterpret_cast<const int4 *>(s.wnodes) + base + 2);
+            const uint4 q0 = __ldg(reinterpret_cast<const uint4 *>(s.wnodes) + base + 3);
+            const uint4 q1 = __ldg(reinterpret_cast<const uint4 *>(s.wnodes) + base + 4);
+            const uint4 q2 = __ldg(reinterpret_cast<const uint4 *>(s.wnodes) + base + 5);
+            const uint32_t meta = (uint32_t)fbits(h.w);
+            const int nc = (int)(meta >> 24);
+            const float sx = exp_scale(meta, 0), sy = exp_scale(meta, 1), sz = exp_scale(meta, 2);
+            const float far_lim = r_max * 1.000000477f;
+            float key[8];
+            int ref[8] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
+            int cnt = 0;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const float lox = __fmaf_rn(qbyte(q0.x, q0.y, k), sx, h.x);
+                const float loy = __fmaf_rn(qbyte(q0.z, q0.w, k), sy, h.y);
+                const float loz = __fmaf_rn(qbyte(q1.x, q1.y, k), sz, h.z);
+                const float hix = __fmaf_rn(qbyte(q1.z, q1.w, k), sx, h.x);
+                const float hiy = __fmaf_rn(qbyte(q2.x, q2.y, k), sy, h.y);
+                const float hiz = __fmaf_rn(qbyte(q2.z, q2.w, k), sz, h.z);
+                const float t0x = (lox - xx) * ix, t1x = (hix - xx) * ix;
+                const float t0y = (loy - xy) * iy, t1y = (hiy - xy) * iy;
+                const float t0z = (loz - xz) * iz, t1z = (hiz - xz) * iz;
+                const float tn = fmaxf(fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fminf(t0z, t1z)), 0.f);
+                const float tf =
+                    fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fmaxf(t0z, t1z)) * 1.000000477f;
+                const bool hit = (k < nc) && (tn <= fminf(tf, far_lim));
+                key[k] = hit ? tn : kInf;
+                cnt += hit ? 1 : 0;
+            }
+            if (sp + cnt >= GQ_STACK_WIDE) {
+                ovf = true;
+                break;
+            }
+            sort8(key, ref);
+#pragma unroll
+            for (int k = 7; k >= 0; --k)
+                if (k < cnt) stk[++sp] = make_int2(ref[k], fbits(key[k]));
+        }
+    }
+    if (ovf) flag_error(s.err, GQ_DEVERR_STACK);
+    ray3_record(s.prims, idx, (idx >= 0) && !ovf, xx, xy, xz, vx, vy, vz, r_max, o, n, qi);
+}
+
+// ===========================================================================
+// Ray intersection, 2D
+// ===========================================================================
+
+__device__ __forceinline__ void ray2_leaf(const void *prims, int ref, float xx, float xy, float vx, float vy,
+                                          float &d_min, int &idx) {
+    int j = ~ref;
+    for (;;) {
+        const float4 a = ldg4(prims, 2 * (int64_t)j);
+        const int4 f = __ldg(reinterpret_cast<const int4 *>(prims) + 2 * (int64_t)j + 1);
+        const float d = seg_ray(xx, xy, vx, vy, a.x, a.y, a.z, a.w);
+        if (d < d_min) {
+            d_min = d;
+            idx = j;
+        }
+        if (f.y & GQ_ITEM_LAST) break;
+        ++j;
+    }
+}
+
+// bvh.py:267-274
+__device__ __forceinline__ void ray2_record(const void *prims, int idx, bool hit, float xx, float xy, float vx,
+                                            float vy, float d_min, const gq_ray_out &o, int64_t n, int64_t qi) {
+    float px = 0.f, py = 0.f, nx = 0.f, ny = 0.f, t = 0.f, d = 0.f;
+    int pid = 0;
+    if (hit) {
+        const float4 a = ldg4(prims, 2 * (int64_t)idx);
+        const int4 f = __ldg(reinterpret_cast<const int4 *>(prims) + 2 * (int64_t)idx + 1);
+        px = xx + vx * d_min;
+        py = xy + vy * d_min;
+        const float tx = a.z - a.x, ty = a.w - a.y;  // LineSegment.normal (line_segment.py:14-16)
+        const float inv = gq_rsqrt(gq_dot2(ty, -tx, ty, -tx));
+        nx = ty * inv;
+        ny = -tx * inv;
+        t = -1.f;
+        d = d_min;
+        pid = f.x;
+    }
+    if (o.valid) o.valid[qi] = hit ? 1 : 0;
+    put2(o.p, n, qi, px, py);
+    put2(o.n, n, qi, nx, ny);
+    put1(o.t, qi, t);
+    put1(o.d, qi, d);
+    if (o.prim_id) o.prim_id[qi] = pid;
+    if (o.on_boundary) o.on_boundary[qi] = hit ? 1 : 0;
+}
+
+// BVH.intersect (bvh.py:200-276): r_max never shrinks; the best hit is tracked in d_min.
+__global__ void __launch_bounds__(kBlock) k_ray2_exact(DevScene s, gq_vecs x, gq_vecs v, const float *rmax_in,
+                                                        int64_t n, const int32_t *perm, gq_ray_out o) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t qi = query_index(perm, i);
+    const float xx = qget(x, qi, 0), xy = qget(x, qi, 1);
+    const float vx = qget(v, qi, 0), vy = qget(v, qi, 1);
+    const float r_max = rmax_in ? rmax_in[qi] : kInf;
+    float d_min = r_max;
+    int idx = -1;
+    bool ovf = false;
+    float t_root;
+    if (box_ray2(s.root_lo[0], s.root_lo[1], s.root_hi[0], s.root_hi[1], xx, xy, vx, vy, r_max, t_root)) {
+        int2 stk[GQ_STACK_EXACT];
+        int sp = 0;
+        stk[0] = make_int2(s.root_ref, fbits(t_root));
+        while (sp >= 0) {
+            const int2 e = stk[sp--];
+            if (!(__int_as_float(e.y) <= r_max)) continue;
+            if (e.x < 0) {
+                ray2_leaf(s.prims, e.x, xx, xy, vx, vy, d_min, idx);
+                continue;
+            }
+            const float4 a = ldg4(s.pairs, 3 * (int64_t)e.x), b = ldg4(s.pairs, 3 * (int64_t)e.x + 1);
+            const int4 r = __ldg(reinterpret_cast<const int4 *>(s.pairs) + 3 * (int64_t)e.x + 2);
+            float t0, t1;
+            const bool h0 = box_ray2(a.x, a.y, a.z, a.w, xx, xy, vx, vy, r_max, t0);
+            const bool h1 = box_ray2(b.x, b.y, b.z, b.w, xx, xy, vx, vy, r_max, t1);
+            if (h0 & h1) {
+                if (sp + 2 >= GQ_STACK_EXACT) {
+                    ovf = true;
+                    break;
+                }
+                const bool sw = t1 < t0;
+                stk[++sp] = sw ? make_int2(r.x, fbits(t0)) : make_int2(r.y, fbits(t1));
+                stk[++sp] = sw ? make_int2(r.y, fbits(t1)) : make_int2(r.x, fbits(t0));
+            } else if (h0) {
+                stk[++sp] = make_int2(r.x, fbits(t0));
+            } else if (h1) {
+                stk[++sp] = make_int2(r.y, fbits(t1));
+            }
+        }
+    }
+    if (ovf) flag_error(s.err, GQ_DEVERR_STACK);
+    ray2_record(s.prims, idx, (idx >= 0) && !ovf, xx, xy, vx, vy, d_min, o, n, qi);
+}
+
+// Quantised 8-wide 2D rays.  Nodes farther than the best hit so far are skipped:
+// a hit there would need a strictly smaller parameter than one already found.
+__global__ void __launch_bounds__(kBlock) k_ray2_wide(DevScene s, gq_vecs x, gq_vecs v, const float *rmax_in,
+                                                       int64_t n, const int32_t *perm, gq_ray_out o) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t qi = query_index(perm, i);
+    const float xx = qget(x, qi, 0), xy = qget(x, qi, 1);
+    const float vx = qget(v, qi, 0), vy = qget(v, qi, 1);
+    const float ix = gq_div(1.f, vx), iy = gq_div(1.f, vy);
+    const float r_max = rmax_in ? rmax_in[qi] : kInf;
+    float d_min = r_max;
+    int idx = -1;
+    bool ovf = false;
+    float t_root;
+    if (box_ray2(s.root_lo[0], s.root_lo[1], s.root_hi[0], s.root_hi[1], xx, xy, vx, vy, r_max, t_root)) {
+        int2 stk[GQ_STACK_WIDE];
+        int sp = 0;
+        stk[0] = make_int2(s.wroot_ref, fbits(t_root));
+        while (sp >= 0) {
+            const int2 e = stk[sp--];
+            if (!(__int_as_float(e.y) <= d_min)) continue;
+            if (e.x < 0) {
+                ray2_leaf(s.prims, e.x, xx, xy, vx, vy, d_min, idx);
+                continue;
+            }
+            const int64_t base = 5 * (int64_t)e.x;
+            const float4 h = ldg4(s.wnodes, base);
+            const int4 r0 = __ldg(reinterpret_cast<const int4 *>(s.wnodes) + base + 1);
+            const int4 r1 = __ldg(reinterpret_cast<const int4 *>(s.wnodes) + base + 2);
+            const uint4 q0 = __ldg(reinterpret_cast<const uint4 *>(s.wnodes) + base + 3);
+            const uint4 q1 = __ldg(reinterpret_cast<const uint4 *>(s.wnodes) + base + 4);
+            const uint32_t meta = (uint32_t)fbits(h.z);
+            const int nc = (int)(meta >> 24);
+            const float sx = exp_scale(meta, 0), sy = exp_scale(meta, 1);
+            const float far_lim = d_min * 1.000000477f;
+            float key[8];
+            int ref[8] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
+            int cnt = 0;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const float lox = __fmaf_rn(qbyte(q0.x, q0.y, k), sx, h.x);
+                const float loy = __fmaf_rn(qbyte(q0.z, q0.w, k), sy, h.y);
+                const float hix = __fmaf_rn(qbyte(q1.x, q1.y, k), sx, h.x);
+                const float hiy = __fmaf_rn(qbyte(q1.z, q1.w, k), sy, h.y);
+                const float t0x = (lox - xx) * ix, t1x = (hix - xx) * ix;
+                const float t0y = (loy - xy) * iy, t1y = (hiy - xy) * iy;
+                const float tn = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), 0.f);
+                const float tf = fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)) * 1.000000477f;
+                const bool hit = (k < nc) && (tn <= fminf(tf, far_lim));
+                key[k] = hit ? tn : kInf;
+                cnt += hit ? 1 : 0;
+            }
+            if (sp + cnt >= GQ_STACK_WIDE) {
+                ovf = true;
+                break;
+            }
+            sort8(key, ref);
+#pragma unroll
+            for (int k = 7; k >= 0; --k)
+                if (k < cnt) stk[++sp] = make_int2(ref[k], fbits(key[k]));
+        }
+    }
+    if (ovf) flag_error(s.err, GQ_DEVERR_STACK);
+    ray2_record(s.prims, idx, (idx >= 0) && !ovf, xx, xy, vx, vy, d_min, o, n, qi);
+}
+
+// ===========================================================================
+// Closest silhouette (SNCH), binary exact
+// ===========================================================================
+
+// SNCH.closest_silhouette (snch.py:106-164) and SNCH3D.closest_silhouette (snch3d.py:143-203)
+template <int D>
+__global__ void __launch_bounds__(kBlock) k_sil_exact(DevScene s, gq_vecs xq, const float *rmax_in, int64_t n,
+                                                       const int32_t *perm, gq_sil_out o) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t qi = query_index(perm, i);
+    float x[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) x[k] = qget(xq, qi, k);
+    float r_max = rmax_in ? rmax_in[qi] : kInf;
+    bool found = false, ovf = false;
+    float bp[D], bd = 0.f;
+    int bid = 0;
+#pragma unroll
+    for (int k = 0; k < D; ++k) bp[k] = 0.f;
+
+    float dmin_root, dmax_root;
+    if (D == 2)
+        box_dist2(s.root_lo[0], s.root_lo[1], s.root_hi[0], s.root_hi[1], x[0], x[1], dmin_root, dmax_root);
+    else
+        box_dist3(s.root_lo[0], s.root_lo[1], s.root_lo[2], s.root_hi[0], s.root_hi[1], s.root_hi[2], x[0], x[1],
+                  x[D - 1], dmin_root, dmax_root);
+    if (dmin_root <= r_max) {
+        int2 stk[GQ_STACK_EXACT];
+        int sp = 0;
+        stk[0] = make_int2(s.sroot_ref, fbits(dmin_root));
+        while (sp >= 0) {
+            const int2 e = stk[sp--];
+            if (!(__int_as_float(e.y) <= r_max)) continue;
+            if (e.x < 0) {
+                if (e.x == INT32_MIN) continue;  // leaf without silhouettes
+                int j = ~e.x;
+                for (;;) {
+                    bool last, ok = false;
+                    float p[D], d = 0.f;
+                    int pid;
+                    if (D == 2) {
+                        // SilhouetteVertex.closest_silhouette (silhouette_vertex.py:40-53)
+                        const float4 r0 = ldg4(s.sils, 2 * (int64_t)j);
+                        const float4 r1 = ldg4(s.sils, 2 * (int64_t)j + 1);
+                        const int flags = fbits(r1.w);
+                        last = flags & GQ_ITEM_LAST;
+                        pid = fbits(r1.z);
+                        p[0] = r0.z;
+                        p[D - 1] = r0.w;
+                        d = gq_norm2(x[0] - r0.z, x[D - 1] - r0.w);
+                        if ((flags & GQ_ITEM_VALID) && (d < r_max)) {
+                            const float c0 = (r0.z - r0.x) * (x[D - 1] - r0.y) - (r0.w - r0.y) * (x[0] - r0.x);
+                            const float c1 = (r1.x - r0.z) * (x[D - 1] - r0.w) - (r1.y - r0.w) * (x[0] - r0.z);
+                            ok = c0 * c1 < 0.f;
+                        }
+                    } else {
+                        // SilhouetteEdge.closest_silhouette (silhouette_edge.py:50-64)
+                        const float4 r0 = ldg4(s.sils, 4 * (int64_t)j), r1 = ldg4(s.sils, 4 * (int64_t)j + 1),
+                                     r2 = ldg4(s.sils, 4 * (int64_t)j + 2), r3 = ldg4(s.sils, 4 * (int64_t)j + 3);
+                        const int flags = fbits(r3.y);
+                        last = flags & GQ_ITEM_LAST;
+                        pid = fbits(r3.x);
+                        const float ax = r0.x, ay = r0.y, az = r0.z, bx = r0.w, by = r1.x, bz = r1.y;
+                        const float cx = r1.z, cy = r1.w, cz = r2.x, dx = r2.y, dy = r2.z, dz = r2.w;
+                        float qx, qy, qz;
+                        d = seg_dist3(x[0], x[1], x[D - 1], ax, ay, az, bx, by, bz, qx, qy, qz);
+                        p[0] = qx;
+                        p[1] = qy;
+                        p[D - 1] = qz;
+                        if (d < r_max) {
+                            ok = flags & GQ_ITEM_VALID;
+                            if (!ok) {
+                                float n0x, n0y, n0z, n1x, n1y, n1z;
+                                cross3(bx - ax, by - ay, bz - az, cx - ax, cy - ay, cz - az, n0x, n0y, n0z);
+                                const float i0 = gq_rsqrt(gq_dot3(n0x, n0y, n0z, n0x, n0y, n0z));
+                                n0x *= i0; n0y *= i0; n0z *= i0;
+                                cross3(dx - ax, dy - ay, dz - az, bx - ax, by - ay, bz - az, n1x, n1y, n1z);
+                                const float i1 = gq_rsqrt(gq_dot3(n1x, n1y, n1z, n1x, n1y, n1z));
+                                n1x *= i1; n1y *= i1; n1z *= i1;
+                                const float wx = qx - x[0], wy = qy - x[1], wz = qz - x[D - 1];
+                                const float dot0 = gq_dot3(wx, wy, wz, n0x, n0y, n0z);
+                                const float dot1 = gq_dot3(wx, wy, wz, n1x, n1y, n1z);
+                                ok = dot0 * dot1 < 0.f;
+                            }
+                        }
+                    }
+                    if (ok && (d < r_max)) {
+                        r_max = fminf(r_max, d);
+                        found = true;
+#pragma unroll
+                        for (int k = 0; k < D; ++k) bp[k] = p[k];
+                        bd = d;
+                        bid = pid;
+                    }
+                    if (last) break;
+                    ++j;
+                }
+                continue;
+            }
+            // interior: both children tested against the same r_max (snch.py:140-141)
+            float lo[2][D], hi[2][D], ax[2][D], half[2], rad[2];
+            int refs[2];
+            if (D == 2) {
+                const float4 a0 = ldg4(s.spairs, 5 * (int64_t)e.x), a1 = ldg4(s.spairs, 5 * (int64_t)e.x + 1),
+                             a2 = ldg4(s.spairs, 5 * (int64_t)e.x + 2), a3 = ldg4(s.spairs, 5 * (int64_t)e.x + 3);
+                const int4 rr = __ldg(reinterpret_cast<const int4 *>(s.spairs) + 5 * (int64_t)e.x + 4);
+                lo[0][0] = a0.x; lo[0][D - 1] = a0.y; hi[0][0] = a0.z; hi[0][D - 1] = a0.w;
+                ax[0][0] = a1.x; ax[0][D - 1] = a1.y; half[0] = a1.z; rad[0] = a1.w;
+                lo[1][0] = a2.x; lo[1][D - 1] = a2.y; hi[1][0] = a2.z; hi[1][D - 1] = a2.w;
+                ax[1][0] = a3.x; ax[1][D - 1] = a3.y; half[1] = a3.z; rad[1] = a3.w;
+                refs[0] = rr.x;
+                refs[1] = rr.y;
+            } else {
+                const int64_t b = 6 * (int64_t)e.x;
+                const float4 f0 = ldg4(s.spairs, b), f1 = ldg4(s.spairs, b + 1), f2 = ldg4(s.spairs, b + 2),
+                             f3 = ldg4(s.spairs, b + 3), f4 = ldg4(s.spairs, b + 4), f5 = ldg4(s.spairs, b + 5);
+                lo[0][0] = f0.x; lo[0][1] = f0.y; lo[0][D - 1] = f0.z;
+                hi[0][0] = f0.w; hi[0][1] = f1.x; hi[0][D - 1] = f1.y;
+                ax[0][0] = f1.z; ax[0][1] = f1.w; ax[0][D - 1] = f2.x;
+                half[0] = f2.y; rad[0] = f2.z;
+                lo[1][0] = f2.w; lo[1][1] = f3.x; lo[1][D - 1] = f3.y;
+                hi[1][0] = f3.z; hi[1][1] = f3.w; hi[1][D - 1] = f4.x;
+                ax[1][0] = f4.y; ax[1][1] = f4.z; ax[1][D - 1] = f4.w;
+                half[1] = f5.x; rad[1] = f5.y;
+                refs[0] = fbits(f5.z);
+                refs[1] = fbits(f5.w);
+            }
+            bool hit[2];
+            float dm[2];
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                float dmax;
+                if (D == 2)
+                    box_dist2(lo[c][0], lo[c][D - 1], hi[c][0], hi[c][D - 1], x[0], x[D - 1], dm[c], dmax);
+                else
+                    box_dist3(lo[c][0], lo[c][1], lo[c][D - 1], hi[c][0], hi[c][1], hi[c][D - 1], x[0], x[1],
+                              x[D - 1], dm[c], dmax);
+                hit[c] = dm[c] <= r_max;
+                if ((half[c] >= 0.f) & hit[c]) hit[c] = cone_overlaps<D>(lo[c], hi[c], ax[c], half[c], rad[c], x, dm[c]);
+            }
+            if (hit[0] & hit[1]) {
+                if (sp + 2 >= GQ_STACK_EXACT) {
+                    ovf = true;
+                    break;
+                }
+                const bool sw = dm[1] < dm[0];
+                stk[++sp] = sw ? make_int2(refs[0], fbits(dm[0])) : make_int2(refs[1], fbits(dm[1]));
+                stk[++sp] = sw ? make_int2(refs[1], fbits(dm[1])) : make_int2(refs[0], fbits(dm[0]));
+            } else if (hit[0]) {
+                stk[++sp] = make_int2(refs[0], fbits(dm[0]));
+            } else if (hit[1]) {
+                stk[++sp] = make_int2(refs[1], fbits(dm[1]));
+            }
+        }
+    }
+    if (ovf) {
+        flag_error(s.err, GQ_DEVERR_STACK);
+        found = false;
+    }
+    if (o.valid) o.valid[qi] = found ? 1 : 0;
+    if (o.p) {
+#pragma unroll
+        for (int k = 0; k < D; ++k) o.p[k * n + qi] = found ? bp[k] : 0.f;
+    }
+    put1(o.d, qi, found ? bd : 0.f);
+    if (o.prim_id) o.prim_id[qi] = found ? bid : 0;
+}
+
+// ===========================================================================
+// Brute force (closest_point_baseline / intersect_baseline), FP32
+// ===========================================================================
+
+template <int D>
+__device__ __forceinline__ void vtx(const DevScene &s, int64_t prim, int k, float *out) {
+    const int64_t vi = __ldg(s.index + prim * D + k);
+#pragma unroll
+    for (int c = 0; c < D; ++c) out[c] = __ldg(s.verts + vi * D + c);
+}
+
+// polyline.py:176-209 and mesh.py closest_point_baseline
+template <int D>
+__global__ void __launch_bounds__(kBlock) k_cp_brute(DevScene s, gq_vecs q, int64_t n, gq_cp_out o) {
+    const int64_t qi = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (qi >= n) return;
+    float p[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) p[k] = qget(q, qi, k);
+    float d_min = kInf;
+    int64_t idx = -1;
+    for (int64_t f = 0; f < s.n_prims; ++f) {
+        float a[D], b[D];
+        vtx<D>(s, f, 0, a);
+        vtx<D>(s, f, 1, b);
+        float d;
+        if (D == 2) {
+            const float pax = p[0] - a[0], pay = p[D - 1] - a[D - 1];
+            const float bax = b[0] - a[0], bay = b[D - 1] - a[D - 1];
+            const float h = gq_clamp(gq_div(gq_dot2(pax, pay, bax, bay), gq_dot2(bax, bay, bax, bay)), 0.f, 1.f);
+            d = gq_norm2(pax - bax * h, pay - bay * h);
+        } else {
+            float c[D];
+            vtx<D>(s, f, D - 1, c);
+            d = tri_closest<false>(p[0], p[1], p[D - 1], a[0], a[1], a[D - 1], b[0], b[1], b[D - 1], c[0], c[1],
+                                   c[D - 1]);
+        }
+        if (d < d_min) {
+            d_min = d;
+            idx = f;
+        }
+    }
+    const bool ok = idx != -1;
+    float rp[3] = {0.f, 0.f, 0.f}, rn[3] = {0.f, 0.f, 0.f}, t0 = 0.f, t1 = 0.f;
+    if (ok) {
+        float a[D], b[D];
+        vtx<D>(s, idx, 0, a);
+        vtx<D>(s, idx, 1, b);
+        if (D == 2) {
+            const float pax = p[0] - a[0], pay = p[D - 1] - a[D - 1];
+            const float bax = b[0] - a[0], bay = b[D - 1] - a[D - 1];
+            const float h = gq_clamp(gq_div(gq_dot2(pax, pay, bax, bay), gq_dot2(bax, bay, bax, bay)), 0.f, 1.f);
+            const float inv = gq_rsqrt(gq_dot2(bay, -bax, bay, -bax));
+            rn[0] = bay * inv;
+            rn[1] = -bax * inv;
+            rp[0] = gq_lerp(a[0], b[0], h);
+            rp[1] = gq_lerp(a[D - 1], b[D - 1], h);
+            t0 = h;
+        } else {
+            float c[D];
+            vtx<D>(s, idx, D - 1, c);
+            tri_closest<true>(p[0], p[1], p[D - 1], a[0], a[1], a[D - 1], b[0], b[1], b[D - 1], c[0], c[1], c[D - 1],
+                              rp, &t0, &t1);
+            float cx, cy, cz;
+            cross3(b[0] - a[0], b[1] - a[1], b[D - 1] - a[D - 1], c[0] - a[0], c[1] - a[1], c[D - 1] - a[D - 1], cx,
+                   cy, cz);
+            const float inv = gq_rsqrt(gq_dot3(cx, cy, cz, cx, cy, cz));
+            rn[0] = cx * inv;
+            rn[1] = cy * inv;
+            rn[2] = cz * inv;
+        }
+    }
+    if (o.valid) o.valid[qi] = ok ? 1 : 0;
+    if (o.p)
+        for (int k = 0; k < D; ++k) o.p[k * n + qi] = rp[k];
+    if (o.n)
+        for (int k = 0; k < D; ++k) o.n[k * n + qi] = rn[k];
+    if (D == 2)
+        put1(o.t, qi, t0);
+    else
+        put2(o.t, n, qi, t0, t1);
+    put1(o.d, qi, ok ? d_min : 0.f);
+    if (o.prim_id) o.prim_id[qi] = ok ? (int)idx : 0;
+}
+
+// polyline.py:138-169 and mesh.py intersect_baseline
+template <int D>
+__global__ void __launch_bounds__(kBlock) k_ray_brute(DevScene s, gq_vecs x, gq_vecs v, const float *rmax_in,
+                                                       int64_t n, gq_ray_out o) {
+    const int64_t qi = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (qi >= n) return;
+    float xo[D], vd[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        xo[k] = qget(x, qi, k);
+        vd[k] = qget(v, qi, k);
+    }
+    const float r_max = rmax_in ? rmax_in[qi] : kInf;
+    float d_min = r_max;
+    int64_t idx = -1;
+    for (int64_t f = 0; f < s.n_prims; ++f) {
+        float a[D], b[D];
+        vtx<D>(s, f, 0, a);
+        vtx<D>(s, f, 1, b);
+        if (D == 2) {
+            const float d = seg_ray(xo[0], xo[D - 1], vd[0], vd[D - 1], a[0], a[D - 1], b[0], b[D - 1]);
+            if (d < d_min) {
+                d_min = d;
+                idx = f;
+            }
+        } else {
+            float c[D];
+            vtx<D>(s, f, D - 1, c);
+            float vv = __builtin_nanf(""), ww;
+            const float t = tri_ray(xo[0], xo[1], xo[D - 1], vd[0], vd[1], vd[D - 1], a[0], a[1], a[D - 1], b[0],
+                                    b[1], b[D - 1], c[0], c[1], c[D - 1], r_max, &vv, &ww);
+            if ((vv == vv) && (t < d_min)) {
+                idx = f;
+                d_min = t;
+            }
+        }
+    }
+    bool ok = idx != -1;
+    float rp[3] = {0.f, 0.f, 0.f}, rn[3] = {0.f, 0.f, 0.f}, t0 = 0.f, t1 = 0.f, dd = 0.f;
+    if (ok) {
+        float a[D], b[D];
+        vtx<D>(s, idx, 0, a);
+        vtx<D>(s, idx, 1, b);
+        if (D == 2) {
+            const float bx = b[0] - a[0], by = b[D - 1] - a[D - 1];
+            const float inv = gq_rsqrt(gq_dot2(bx, by, bx, by));
+            const float abx = bx * inv, aby = by * inv;
+            rn[0] = aby;
+            rn[1] = -abx;
+            rp[0] = xo[0] + vd[0] * d_min;
+            rp[1] = xo[D - 1] + vd[D - 1] * d_min;
+            t0 = -1.f;
+            dd = d_min;
+        } else {
+            float c[D];
+            vtx<D>(s, idx, D - 1, c);
+            float vv = __builtin_nanf(""), ww = 0.f;
+            const float t = tri_ray(xo[0], xo[1], xo[D - 1], vd[0], vd[1], vd[D - 1], a[0], a[1], a[D - 1], b[0], b[1],
+                                    b[D - 1], c[0], c[1], c[D - 1], r_max, &vv, &ww);
+            ok = vv == vv;
+            if (ok) {
+                const float v1x = b[0] - a[0], v1y = b[1] - a[1], v1z = b[D - 1] - a[D - 1];
+                const float v2x = c[0] - a[0], v2y = c[1] - a[1], v2z = c[D - 1] - a[D - 1];
+                rp[0] = (a[0] + v1x * vv) + v2x * ww;
+                rp[1] = (a[1] + v1y * vv) + v2y * ww;
+                rp[2] = (a[D - 1] + v1z * vv) + v2z * ww;
+                float cx, cy, cz;
+                cross3(v1x, v1y, v1z, v2x, v2y, v2z, cx, cy, cz);
+                const float inv = gq_rsqrt(gq_dot3(cx, cy, cz, cx, cy, cz));
+                rn[0] = cx * inv;
+                rn[1] = cy * inv;
+                rn[2] = cz * inv;
+                t0 = 1.f - vv - ww;
+                t1 = vv;
+                dd = t;
+            }
+        }
+    }
+    if (o.valid) o.valid[qi] = ok ? 1 : 0;
+    if (o.p)
+        for (int k = 0; k < D; ++k) o.p[k * n + qi] = ok ? rp[k] : 0.f;
+    if (o.n)
+        for (int k = 0; k < D; ++k) o.n[k * n + qi] = ok ? rn[k] : 0.f;
+    if (D == 2)
+        put1(o.t, qi, ok ? t0 : 0.f);
+    else
+        put2(o.t, n, qi, ok ? t0 : 0.f, ok ? t1 : 0.f);
+    put1(o.d, qi, ok ? dd : 0.f);
+    if (o.prim_id) o.prim_id[qi] = ok ? (int)idx : 0;
+    if (o.on_boundary) o.on_boundary[qi] = ok ? 1 : 0;
+}
+
+// ===========================================================================
+// FP64 brute force (error reference).  Primitives are staged through shared
+// memory in tiles; one thread per query.
+// ===========================================================================
+
+constexpr int kTile = 256;
+
+__device__ double d_cp_tri(const double *p, const double *a, const double *b, const double *c) {
+    double ab[3], ac[3], ap[3], bp[3], cp[3];
+    for (int k = 0; k < 3; ++k) {
+        ab[k] = b[k] - a[k];
+        ac[k] = c[k] - a[k];
+        ap[k] = p[k] - a[k];
+        bp[k] = p[k] - b[k];
+        cp[k] = p[k] - c[k];
+    }
+    auto dot = [](const double *u, const double *v) { return u[0] * v[0] + u[1] * v[1] + u[2] * v[2]; };
+    auto dist = [&](double x, double y, double z) {
+        const double ex = p[0] - x, ey = p[1] - y, ez = p[2] - z;
+        return sqrt(ex * ex + ey * ey + ez * ez);
+    };
+    const double d1 = dot(ab, ap), d2 = dot(ac, ap);
+    if (d1 <= 0 && d2 <= 0) return dist(a[0], a[1], a[2]);
+    const double d3 = dot(ab, bp), d4 = dot(ac, bp);
+    if (d3 >= 0 && d4 <= d3) return dist(b[0], b[1], b[2]);
+    const double vc = d1 * d4 - d3 * d2;
+    if (vc <= 0 && d1 >= 0 && d3 <= 0) {
+        const double v = d1 / (d1 - d3);
+        return dist(a[0] + v * ab[0], a[1] + v * ab[1], a[2] + v * ab[2]);
+    }
+    const double d5 = dot(ab, cp), d6 = dot(ac, cp);
+    if (d6 >= 0 && d5 <= d6) return dist(c[0], c[1], c[2]);
+    const double vb = d5 * d2 - d1 * d6;
+    if (vb <= 0 && d2 >= 0 && d6 <= 0) {
+        const double w = d2 / (d2 - d6);
+        return dist(a[0] + w * ac[0], a[1] + w * ac[1], a[2] + w * ac[2]);
+    }
+    const double va = d3 * d6 - d5 * d4;
+    if (va <= 0 && (d4 - d3) >= 0 && (d5 - d6) >= 0) {
+        const double w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+        return dist(b[0] + w * (c[0] - b[0]), b[1] + w * (c[1] - b[1]), b[2] + w * (c[2] - b[2]));
+    }
+    const double den = 1.0 / (va + vb + vc);
+    const double v = vb * den, w = vc * den;
+    return dist(a[0] + ab[0] * v + ac[0] * w, a[1] + ab[1] * v + ac[1] * w, a[2] + ab[2] * v + ac[2] * w);
+}
+
+__device__ double d_ray_tri(const double *o, const double *d, const double *a, const double *b, const double *c) {
+    double e1[3], e2[3], s[3];
+    for (int k = 0; k < 3; ++k) {
+        e1[k] = b[k] - a[k];
+        e2[k] = c[k] - a[k];
+        s[k] = o[k] - a[k];
+    }
+    const double p[3] = {d[1] * e2[2] - d[2] * e2[1], d[2] * e2[0] - d[0] * e2[2], d[0] * e2[1] - d[1] * e2[0]};
+    const double det = e1[0] * p[0] + e1[1] * p[1] + e1[2] * p[2];
+    if (det == 0.0) return INFINITY;
+    const double inv = 1.0 / det;
+    const double u = (s[0] * p[0] + s[1] * p[1] + s[2] * p[2]) * inv;
+    if (u < 0 || u > 1) return INFINITY;
+    const double q[3] = {s[1] * e1[2] - s[2] * e1[1], s[2] * e1[0] - s[0] * e1[2], s[0] * e1[1] - s[1] * e1[0]};
+    const double v = (d[0] * q[0] + d[1] * q[1] + d[2] * q[2]) * inv;
+    if (v < 0 || u + v > 1) return INFINITY;
+    const double t = (e2[0] * q[0] + e2[1] * q[1] + e2[2] * q[2]) * inv;
+    return t >= 0 ? t : INFINITY;
+}
+
+template <int D>
+__global__ void __launch_bounds__(kBlock) k_brute_f64(DevScene s, int kind, gq_vecs qa, gq_vecs qb, int64_t n,
+                                                       double *out_d, int32_t *out_id) {
+    __shared__ double tile[kTile][D * D];
+    const int64_t qi = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const bool active = qi < n;
+    double a[D] = {}, b[D] = {};
+    if (active)
+        for (int k = 0; k < D; ++k) {
+            a[k] = qget(qa, qi, k);
+            if (kind == 1) b[k] = qget(qb, qi, k);
+        }
+    double best = INFINITY;
+    int64_t bid = -1;
+    for (int64_t base = 0; base < s.n_prims; base += kTile) {
+        __syncthreads();
+        for (int t = threadIdx.x; t < kTile; t += blockDim.x) {
+            const int64_t f = base + t;
+            if (f < s.n_prims)
+                for (int k = 0; k < D; ++k) {
+                    const int64_t vi = s.index[f * D + k];
+                    for (int c = 0; c < D; ++c) tile[t][k * D + c] = (double)s.verts[vi * D + c];
+                }
+        }
+        __syncthreads();
+        const int lim = (int)min((int64_t)kTile, s.n_prims - base);
+        if (active)
+            for (int t = 0; t < lim; ++t) {
+                double d;
+                const double *pv = tile[t];
+                if (D == 3) {
+                    d = (kind == 0) ? d_cp_tri(a, pv, pv + 3, pv + 6) : d_ray_tri(a, b, pv, pv + 3, pv + 6);
+                } else if (kind == 0) {
+                    const double ux = pv[2] - pv[0], uy = pv[3] - pv[1], vx = a[0] - pv[0], vy = a[D - 1] - pv[1];
+                    const double uu = ux * ux + uy * uy;
+                    double tt = uu > 0 ? (vx * ux + vy * uy) / uu : 0.0;
+                    tt = tt < 0 ? 0 : (tt > 1 ? 1 : tt);
+                    const double ex = pv[0] + tt * ux - a[0], ey = pv[1] + tt * uy - a[D - 1];
+                    d = sqrt(ex * ex + ey * ey);
+                } else {
+                    const double ux = pv[2] - pv[0], uy = pv[3] - pv[1], wx = a[0] - pv[0], wy = a[D - 1] - pv[1];
+                    const double den = b[0] * uy - b[D - 1] * ux;
+                    const double ss = (b[0] * wy - b[D - 1] * wx) / den, tt = (ux * wy - uy * wx) / den;
+                    d = (den != 0.0 && tt > 0 && ss >= 0 && ss <= 1) ? tt : INFINITY;
+                }
+                if (d < best) {
+                    best = d;
+                    bid = base + t;
+                }
+            }
+    }
+    if (active) {
+        out_d[qi] = best;
+        out_id[qi] = (int32_t)bid;
+    }
+}
+
+// ===========================================================================
+// Morton reordering
+// ===========================================================================
+
+__device__ __forceinline__ uint32_t spread3(uint32_t v) {  // 10 bits -> every third bit
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+__device__ __forceinline__ uint32_t spread2(uint32_t v) {  // 15 bits -> every second bit
+    v &= 0x7fffu;
+    v = (v | (v << 8)) & 0x00ff00ffu;
+    v = (v | (v << 4)) & 0x0f0f0f0fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    v = (v | (v << 1)) & 0x55555555u;
+    return v;
+}
+
+// Keys on a grid over the scene box grown to twice its extent about its centre.
+__global__ void k_morton_keys(int dim, float lo0, float lo1, float lo2, float sc0, float sc1, float sc2, gq_vecs q,
+                              int64_t n, uint32_t *keys, int32_t *vals) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float lo[3] = {lo0, lo1, lo2}, sc[3] = {sc0, sc1, sc2};
+    uint32_t key;
+    if (dim == 3) {
+        uint32_t c[3];
+        for (int k = 0; k < 3; ++k) {
+            float f = (qget(q, i, k) - lo[k]) * sc[k];
+            f = fminf(fmaxf(f, 0.f), 1023.f);
+            c[k] = (uint32_t)f;
+        }
+        key = (spread3(c[0]) << 2) | (spread3(c[1]) << 1) | spread3(c[2]);
+    } else {
+        uint32_t c[2];
+        for (int k = 0; k < 2; ++k) {
+            float f = (qget(q, i, k) - lo[k]) * sc[k];
+            f = fminf(fmaxf(f, 0.f), 32767.f);
+            c[k] = (uint32_t)f;
+        }
+        key = (spread2(c[0]) << 1) | spread2(c[1]);
+    }
+    keys[i] = key;
+    vals[i] = (int32_t)i;
+}
+
+inline dim3 grid_for(int64_t n) { return dim3((unsigned)((n + kBlock - 1) / kBlock)); }
+inline size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+size_t cub_temp_bytes(int64_t n) {
+    size_t tb = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, (const uint32_t *)nullptr, (uint32_t *)nullptr,
+                                    (const int32_t *)nullptr, (int32_t *)nullptr, (int)n, 0, 32);
+    return tb;
+}
+
+}  // namespace
+
+size_t morton_scratch_bytes(int64_t n) {
+    return 3 * align256((size_t)n * 4) + align256(cub_temp_bytes(n));
+}
+
+cudaError_t morton_order(const DevScene &s, gq_vecs q, int64_t n, int32_t *perm, void *scratch, size_t scratch_bytes,
+                         cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    if (scratch_bytes < morton_scratch_bytes(n)) return cudaErrorInvalidValue;
+    char *p = (char *)scratch;
+    uint32_t *k_in = (uint32_t *)p;
+    p += align256((size_t)n * 4);
+    uint32_t *k_out = (uint32_t *)p;
+    p += align256((size_t)n * 4);
+    int32_t *v_in = (int32_t *)p;
+    p += align256((size_t)n * 4);
+    size_t tb = cub_temp_bytes(n);
+    float lo[3] = {0, 0, 0}, sc[3] = {1, 1, 1};
+    const int bits = s.dim == 3 ? 1024 : 32768;
+    for (int k = 0; k < s.dim; ++k) {
+        const float c = 0.5f * (s.root_lo[k] + s.root_hi[k]);
+        float ext = s.root_hi[k] - s.root_lo[k];
+        if (!(ext > 0.f)) ext = 1.f;
+        lo[k] = c - ext;
+        sc[k] = (float)bits / (2.f * ext);
+    }
+    k_morton_keys<<<grid_for(n), kBlock, 0, st>>>(s.dim, lo[0], lo[1], lo[2], sc[0], sc[1], sc[2], q, n, k_in, v_in);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const int end_bit = s.dim == 3 ? 30 : 30;
+    return cub::DeviceRadixSort::SortPairs(p, tb, k_in, k_out, v_in, perm, (int)n, 0, end_bit, st);
+}
+
+cudaError_t launch_cp(const DevScene &s, int variant, gq_vecs q, int64_t n, const int32_t *perm, const gq_cp_out &o,
+                      cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    const bool wide = variant == GQ_VARIANT_WIDE8;
+    if (s.dim == 3) {
+        if (wide)
+            k_cp3_wide<<<grid_for(n), kBlock, 0, st>>>(s, q, n, perm, o);
+        else
+            k_cp3_exact<<<grid_for(n), kBlock, 0, st>>>(s, q, n, perm, o);
+    } else {
+        if (wide)
+            k_cp2_wide<<<grid_for(n), kBlock, 0, st>>>(s, q, n, perm, o);
+        else
+            k_cp2_exact<<<grid_for(n), kBlock, 0, st>>>(s, q, n, perm, o);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ray(const DevScene &s, int variant, gq_vecs x, gq_vecs v, const float *r_max, int64_t n,
+                       const int32_t *perm, const gq_ray_out &o, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    const bool wide = variant == GQ_VARIANT_WIDE8;
+    if (s.dim == 3) {
+        if (wide)
+            k_ray3_wide<<<grid_for(n), kBlock, 0, st>>>(s, x, v, r_max, n, perm, o);
+        else
+            k_ray3_exact<<<grid_for(n), kBlock, 0, st>>>(s, x, v, r_max, n, perm, o);
+    } else {
+        if (wide)
+            k_ray2_wide<<<grid_for(n), kBlock, 0, st>>>(s, x, v, r_max, n, perm, o);
+        else
+            k_ray2_exact<<<grid_for(n), kBlock, 0, st>>>(s, x, v, r_max, n, perm, o);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sil(const DevScene &s, gq_vecs x, const float *r_max, int64_t n, const int32_t *perm,
+                       const gq_sil_out &o, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    if (s.dim == 3)
+        k_sil_exact<3><<<grid_for(n), kBlock, 0, st>>>(s, x, r_max, n, perm, o);
+    else
+        k_sil_exact<2><<<grid_for(n), kBlock, 0, st>>>(s, x, r_max, n, perm, o);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cp_brute(const DevScene &s, gq_vecs q, int64_t n, const gq_cp_out &o, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    if (s.dim == 3)
+        k_cp_brute<3><<<grid_for(n), kBlock, 0, st>>>(s, q, n, o);
+    else
+        k_cp_brute<2><<<grid_for(n), kBlock, 0, st>>>(s, q, n, o);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ray_brute(const DevScene &s, gq_vecs x, gq_vecs v, const float *r_max, int64_t n,
+                             const gq_ray_out &o, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    if (s.dim == 3)
+        k_ray_brute<3><<<grid_for(n), kBlock, 0, st>>>(s, x, v, r_max, n, o);
+    else
+        k_ray_brute<2><<<grid_for(n), kBlock, 0, st>>>(s, x, v, r_max, n, o);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_brute_f64(const DevScene &s, int kind, gq_vecs a, gq_vecs b, int64_t n, double *out_d,
+                             int32_t *out_id, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    if (s.dim == 3)
+        k_brute_f64<3><<<grid_for(n), kBlock, 0, st>>>(s, kind, a, b, n, out_d, out_id);
+    else
+        k_brute_f64<2><<<grid_for(n), kBlock, 0, st>>>(s, kind, a, b, n, out_d, out_id);
+    return cudaGetLastError();
+}
+
+}  // namespace gqd

@@ -1,0 +1,49 @@
+// Host-side launchers of the query kernels (implemented in queries.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "../../../include/gq.h"
+#include "../layout.h"
+
+namespace gqd {
+
+// Device view of one scene.
+struct DevScene {
+    int dim;
+    const void *pairs;   // gq_pair2_t / gq_pair3_t
+    const void *prims;   // gq_seg_t / gq_tri_t
+    int32_t root_ref;
+    float root_lo[3], root_hi[3];
+    const void *wnodes;  // gq_wnode2_t / gq_wnode3_t (may be null)
+    int32_t wroot_ref;
+    const void *spairs;  // gq_spair2_t / gq_spair3_t (may be null)
+    const void *sils;    // gq_silv_t / gq_sile_t
+    int32_t sroot_ref;
+    const float *verts;  // original vertices [nv][D] (brute force)
+    const int32_t *index;  // original primitives [np][D]
+    int64_t n_prims;
+    int32_t *err;        // device error word
+};
+
+#define GQ_DEVERR_STACK 1
+
+// Morton reordering: writes perm[0..n) (a permutation of 0..n-1) using `scratch`.
+// Returns the scratch bytes needed when scratch == nullptr.
+size_t morton_scratch_bytes(int64_t n);
+cudaError_t morton_order(const DevScene &s, gq_vecs q, int64_t n, int32_t *perm, void *scratch, size_t scratch_bytes,
+                         cudaStream_t st);
+
+cudaError_t launch_cp(const DevScene &s, int variant, gq_vecs q, int64_t n, const int32_t *perm, const gq_cp_out &o,
+                      cudaStream_t st);
+cudaError_t launch_ray(const DevScene &s, int variant, gq_vecs x, gq_vecs v, const float *r_max, int64_t n,
+                       const int32_t *perm, const gq_ray_out &o, cudaStream_t st);
+cudaError_t launch_sil(const DevScene &s, gq_vecs x, const float *r_max, int64_t n, const int32_t *perm,
+                       const gq_sil_out &o, cudaStream_t st);
+cudaError_t launch_cp_brute(const DevScene &s, gq_vecs q, int64_t n, const gq_cp_out &o, cudaStream_t st);
+cudaError_t launch_ray_brute(const DevScene &s, gq_vecs x, gq_vecs v, const float *r_max, int64_t n,
+                             const gq_ray_out &o, cudaStream_t st);
+cudaError_t launch_brute_f64(const DevScene &s, int kind, gq_vecs a, gq_vecs b, int64_t n, double *out_d,
+                             int32_t *out_id, cudaStream_t st);
+
+}  // namespace gqd

@@ -1,0 +1,331 @@
+// Flattening pass (see flatten.hpp).  Compile with -ffp-contract=off.
+#include "flatten.hpp"
+
+#include <cmath>
+#include <cstring>
+
+namespace gqb {
+
+namespace {
+
+// Preorder rank of every interior node (the index of its pair record), -1 for leaves.
+template <int D>
+std::vector<int32_t> interior_ranks(const BvhTree<D> &t) {
+    std::vector<int32_t> rank(t.nodes.size(), -1);
+    int32_t r = 0;
+    for (size_t i = 0; i < t.nodes.size(); ++i)
+        if (t.nodes[i].n_prims == 0) rank[i] = r++;
+    return rank;
+}
+
+// Deepest leaf (root at depth 0).
+template <int D>
+int max_leaf_depth(const BvhTree<D> &t) {
+    std::vector<std::pair<uint32_t, int>> st{{0u, 0}};
+    int best = 0;
+    while (!st.empty()) {
+        auto [i, d] = st.back();
+        st.pop_back();
+        const auto &n = t.nodes[i];
+        if (n.n_prims > 0) {
+            best = std::max(best, d);
+        } else {
+            st.push_back({i + 1, d + 1});
+            st.push_back({i + (uint32_t)n.second_child, d + 1});
+        }
+    }
+    return best;
+}
+
+template <int D>
+void put_box(const Box<D> &b, float *lo, float *hi) {
+    for (int k = 0; k < D; ++k) {
+        lo[k] = b.lo.v[k];
+        hi[k] = b.hi.v[k];
+    }
+}
+
+}  // namespace
+
+template <int D>
+void flatten_bvh(const PrimSource<D> &src, const BvhTree<D> &t, DeviceImage<D> &img) {
+    const auto rank = interior_ranks(t);
+    auto ref_of = [&](uint32_t i) -> int32_t {
+        const auto &n = t.nodes[i];
+        return n.n_prims > 0 ? ~n.prim_offset : rank[i];
+    };
+    img.pairs.clear();
+    for (uint32_t i = 0; i < t.nodes.size(); ++i) {
+        const auto &n = t.nodes[i];
+        if (n.n_prims > 0) continue;
+        const uint32_t l = i + 1, r = i + (uint32_t)n.second_child;
+        typename DeviceImage<D>::Pair p;
+        std::memset(&p, 0, sizeof p);
+        if constexpr (D == 2) {
+            p.l_lox = t.nodes[l].box.lo.v[0];
+            p.l_loy = t.nodes[l].box.lo.v[1];
+            p.l_hix = t.nodes[l].box.hi.v[0];
+            p.l_hiy = t.nodes[l].box.hi.v[1];
+            p.r_lox = t.nodes[r].box.lo.v[0];
+            p.r_loy = t.nodes[r].box.lo.v[1];
+            p.r_hix = t.nodes[r].box.hi.v[0];
+            p.r_hiy = t.nodes[r].box.hi.v[1];
+        } else {
+            p.l_lox = t.nodes[l].box.lo.v[0];
+            p.l_loy = t.nodes[l].box.lo.v[1];
+            p.l_loz = t.nodes[l].box.lo.v[2];
+            p.l_hix = t.nodes[l].box.hi.v[0];
+            p.l_hiy = t.nodes[l].box.hi.v[1];
+            p.l_hiz = t.nodes[l].box.hi.v[2];
+            p.r_lox = t.nodes[r].box.lo.v[0];
+            p.r_loy = t.nodes[r].box.lo.v[1];
+            p.r_loz = t.nodes[r].box.lo.v[2];
+            p.r_hix = t.nodes[r].box.hi.v[0];
+            p.r_hiy = t.nodes[r].box.hi.v[1];
+            p.r_hiz = t.nodes[r].box.hi.v[2];
+        }
+        p.ref_l = ref_of(l);
+        p.ref_r = ref_of(r);
+        img.pairs.push_back(p);
+    }
+    img.root_ref = ref_of(0);
+    put_box(t.nodes[0].box, img.root_lo, img.root_hi);
+    img.exact_stack = max_leaf_depth(t) + 1;
+
+    // ordered primitives with end-of-leaf flags
+    img.prims.assign(t.order.size(), typename DeviceImage<D>::Prim{});
+    for (size_t s = 0; s < t.order.size(); ++s) {
+        const int64_t p = t.order[s];
+        auto &r = img.prims[s];
+        std::memset(&r, 0, sizeof r);
+        if constexpr (D == 2) {
+            Vec2 a = vert2(src, src.index[2 * p]), b = vert2(src, src.index[2 * p + 1]);
+            r.ax = a.v[0];
+            r.ay = a.v[1];
+            r.bx = b.v[0];
+            r.by = b.v[1];
+        } else {
+            Vec3 a = vert3(src, src.index[3 * p]), b = vert3(src, src.index[3 * p + 1]),
+                 c = vert3(src, src.index[3 * p + 2]);
+            r.ax = a.v[0];
+            r.ay = a.v[1];
+            r.az = a.v[2];
+            r.bx = b.v[0];
+            r.by = b.v[1];
+            r.bz = b.v[2];
+            r.cx = c.v[0];
+            r.cy = c.v[1];
+            r.cz = c.v[2];
+        }
+        // The reference stores the original index as a float (line_segment.h:104-108);
+        // reading it back with Int() gives the same value for every index below 2^24.
+        r.index = (int32_t)(float)p;
+        r.flags = 0;
+    }
+    for (const auto &n : t.nodes)
+        if (n.n_prims > 0) img.prims[(size_t)(n.prim_offset + n.n_prims - 1)].flags |= GQ_ITEM_LAST;
+}
+
+// ---------------------------------------------------------------------------
+// Quantised 8-wide collapse
+// ---------------------------------------------------------------------------
+
+int quant_exponent(float lo, float hi) {
+    double ext = (double)hi - (double)lo;
+    if (!(ext > 0.0)) return -126;
+    int e = (int)std::ceil(std::log2(ext / 255.0));
+    while (255.0 * std::ldexp(1.0, e) < ext) ++e;
+    while (e > -126 && 255.0 * std::ldexp(1.0, e - 1) >= ext) --e;
+    if (e < -126) e = -126;
+    if (e > 127) e = 127;
+    return e;
+}
+
+float dequant(float origin, int e, int q) {
+    float s = std::ldexp(1.0f, e);
+    return std::fma((float)q, s, origin);
+}
+
+void quantise_bounds(float origin, int e, float clo, float chi, uint8_t *qlo, uint8_t *qhi) {
+    // largest q with decode(q) <= clo
+    int a = (int)std::floor(((double)clo - (double)origin) / std::ldexp(1.0, e));
+    a = std::max(0, std::min(255, a));
+    while (a > 0 && !(dequant(origin, e, a) <= clo)) --a;
+    while (a < 255 && dequant(origin, e, a + 1) <= clo) ++a;
+    // smallest q with decode(q) >= chi
+    int b = (int)std::ceil(((double)chi - (double)origin) / std::ldexp(1.0, e));
+    b = std::max(0, std::min(255, b));
+    while (b < 255 && !(dequant(origin, e, b) >= chi)) ++b;
+    while (b > 0 && dequant(origin, e, b - 1) >= chi) --b;
+    *qlo = (uint8_t)a;
+    *qhi = (uint8_t)b;
+}
+
+namespace {
+
+template <int D>
+struct WideBuilder {
+    const BvhTree<D> &t;
+    DeviceImage<D> &img;
+
+    // Returns the stack entries a traversal of this subtree needs once its node is popped.
+    int build(uint32_t b, int32_t *ref_out) {
+        const auto &bn = t.nodes[b];
+        std::vector<uint32_t> kids{b + 1, b + (uint32_t)bn.second_child};
+        while (kids.size() < GQ_WIDTH) {
+            int pick = -1;
+            float best = -1.f;
+            for (size_t k = 0; k < kids.size(); ++k) {
+                const auto &kn = t.nodes[kids[k]];
+                if (kn.n_prims == 0) {
+                    float a = kn.box.area();
+                    if (a > best) {
+                        best = a;
+                        pick = (int)k;
+                    }
+                }
+            }
+            if (pick < 0) break;
+            uint32_t c = kids[(size_t)pick];
+            kids[(size_t)pick] = c + 1;
+            kids.insert(kids.begin() + pick + 1, c + (uint32_t)t.nodes[c].second_child);
+        }
+        const size_t me = img.wnodes.size();
+        img.wnodes.emplace_back();
+        *ref_out = (int32_t)me;
+
+        int e[D];
+        for (int k = 0; k < D; ++k) e[k] = quant_exponent(bn.box.lo.v[k], bn.box.hi.v[k]);
+        typename DeviceImage<D>::WNode w;
+        std::memset(&w, 0, sizeof w);
+        if constexpr (D == 2) {
+            w.ox = bn.box.lo.v[0];
+            w.oy = bn.box.lo.v[1];
+            w.meta = (uint32_t)(e[0] + 127) | ((uint32_t)(e[1] + 127) << 8) | ((uint32_t)kids.size() << 24);
+        } else {
+            w.ox = bn.box.lo.v[0];
+            w.oy = bn.box.lo.v[1];
+            w.oz = bn.box.lo.v[2];
+            w.meta = (uint32_t)(e[0] + 127) | ((uint32_t)(e[1] + 127) << 8) | ((uint32_t)(e[2] + 127) << 16) |
+                     ((uint32_t)kids.size() << 24);
+        }
+        for (int k = 0; k < GQ_WIDTH; ++k) w.ref[k] = kEmptyLeaf;
+        int deepest = 0;
+        for (size_t k = 0; k < kids.size(); ++k) {
+            const auto &kn = t.nodes[kids[k]];
+            for (int ax = 0; ax < D; ++ax) {
+                const float o = (ax == 0) ? w.ox : (ax == 1 ? w.oy : bn.box.lo.v[2]);
+                quantise_bounds(o, e[ax], kn.box.lo.v[ax], kn.box.hi.v[ax], &w.q[ax][k], &w.q[D + ax][k]);
+            }
+            if (kn.n_prims > 0) {
+                w.ref[k] = ~kn.prim_offset;
+            } else {
+                int32_t r;
+                int need = build(kids[k], &r);
+                w.ref[k] = r;
+                deepest = std::max(deepest, need);
+            }
+        }
+        img.wnodes[me] = w;
+        const int k = (int)kids.size();
+        return std::max(k, (k - 1) + deepest);
+    }
+};
+
+}  // namespace
+
+template <int D>
+void flatten_wide(const BvhTree<D> &t, DeviceImage<D> &img) {
+    img.wnodes.clear();
+    if (t.nodes[0].n_prims > 0) {
+        img.wroot_ref = ~t.nodes[0].prim_offset;
+        img.wide_stack = 1;
+        return;
+    }
+    WideBuilder<D> wb{t, img};
+    int32_t r;
+    img.wide_stack = wb.build(0, &r);
+    img.wroot_ref = r;
+}
+
+// ---------------------------------------------------------------------------
+// Binary SNCH
+// ---------------------------------------------------------------------------
+
+template <int D>
+void flatten_snch(const BvhTree<D> &t, const SnchTree<D> &s, DeviceImage<D> &img) {
+    const auto rank = interior_ranks(t);
+    auto ref_of = [&](uint32_t i) -> int32_t {
+        const auto &n = t.nodes[i];
+        if (n.n_prims == 0) return rank[i];
+        return s.nodes[i].n_sil > 0 ? ~s.nodes[i].sil_offset : kEmptyLeaf;
+    };
+    img.spairs.clear();
+    for (uint32_t i = 0; i < t.nodes.size(); ++i) {
+        const auto &n = t.nodes[i];
+        if (n.n_prims > 0) continue;
+        const uint32_t l = i + 1, r = i + (uint32_t)n.second_child;
+        const auto &L = t.nodes[l], &R = t.nodes[r];
+        const auto &Lc = s.nodes[l].cone, &Rc = s.nodes[r].cone;
+        typename DeviceImage<D>::SPair p;
+        std::memset(&p, 0, sizeof p);
+        if constexpr (D == 2) {
+            p.l_lox = L.box.lo.v[0]; p.l_loy = L.box.lo.v[1]; p.l_hix = L.box.hi.v[0]; p.l_hiy = L.box.hi.v[1];
+            p.l_ax = Lc.axis.v[0]; p.l_ay = Lc.axis.v[1]; p.l_half = Lc.half_angle; p.l_rad = Lc.radius;
+            p.r_lox = R.box.lo.v[0]; p.r_loy = R.box.lo.v[1]; p.r_hix = R.box.hi.v[0]; p.r_hiy = R.box.hi.v[1];
+            p.r_ax = Rc.axis.v[0]; p.r_ay = Rc.axis.v[1]; p.r_half = Rc.half_angle; p.r_rad = Rc.radius;
+        } else {
+            p.l_lox = L.box.lo.v[0]; p.l_loy = L.box.lo.v[1]; p.l_loz = L.box.lo.v[2];
+            p.l_hix = L.box.hi.v[0]; p.l_hiy = L.box.hi.v[1]; p.l_hiz = L.box.hi.v[2];
+            p.l_ax = Lc.axis.v[0]; p.l_ay = Lc.axis.v[1]; p.l_az = Lc.axis.v[2];
+            p.l_half = Lc.half_angle; p.l_rad = Lc.radius;
+            p.r_lox = R.box.lo.v[0]; p.r_loy = R.box.lo.v[1]; p.r_loz = R.box.lo.v[2];
+            p.r_hix = R.box.hi.v[0]; p.r_hiy = R.box.hi.v[1]; p.r_hiz = R.box.hi.v[2];
+            p.r_ax = Rc.axis.v[0]; p.r_ay = Rc.axis.v[1]; p.r_az = Rc.axis.v[2];
+            p.r_half = Rc.half_angle; p.r_rad = Rc.radius;
+        }
+        p.ref_l = ref_of(l);
+        p.ref_r = ref_of(r);
+        img.spairs.push_back(p);
+    }
+    img.sroot_ref = ref_of(0);
+
+    img.sils.assign(s.ordered.size(), typename DeviceImage<D>::Sil{});
+    for (size_t k = 0; k < s.ordered.size(); ++k) {
+        const auto &x = s.raw[s.ordered[k]];
+        auto &r = img.sils[k];
+        std::memset(&r, 0, sizeof r);
+        if constexpr (D == 2) {
+            r.ax = x.v[0].v[0]; r.ay = x.v[0].v[1];
+            r.bx = x.v[1].v[0]; r.by = x.v[1].v[1];
+            r.cx = x.v[2].v[0]; r.cy = x.v[2].v[1];
+            r.prim = (int32_t)(float)x.prim;
+            // silhouette_vertex.py:48: Int(Float(index)) != -1 for both neighbours
+            const bool ok = ((int64_t)(float)x.idx[0] != -1) && ((int64_t)(float)x.idx[2] != -1);
+            r.flags = ok ? GQ_ITEM_VALID : 0;
+        } else {
+            // SilhouetteEdges view (silhouette_edge.py:75-86): c = v[0], a = v[1], b = v[2], d = v[3]
+            r.ax = x.v[1].v[0]; r.ay = x.v[1].v[1]; r.az = x.v[1].v[2];
+            r.bx = x.v[2].v[0]; r.by = x.v[2].v[1]; r.bz = x.v[2].v[2];
+            r.cx = x.v[0].v[0]; r.cy = x.v[0].v[1]; r.cz = x.v[0].v[2];
+            r.dx = x.v[3].v[0]; r.dy = x.v[3].v[1]; r.dz = x.v[3].v[2];
+            r.prim = (int32_t)(float)x.prim;
+            // silhouette_edge.py:56-57: boundary marker index == -1 never occurs (size_t storage)
+            const bool boundary = ((int64_t)(float)x.idx[0] == -1) || ((int64_t)(float)x.idx[3] == -1);
+            r.flags = boundary ? GQ_ITEM_VALID : 0;  // for edges the bit means "always a silhouette"
+        }
+    }
+    for (size_t i = 0; i < t.nodes.size(); ++i) {
+        const auto &sn = s.nodes[i];
+        if (t.nodes[i].n_prims > 0 && sn.n_sil > 0) img.sils[(size_t)(sn.sil_offset + sn.n_sil - 1)].flags |= GQ_ITEM_LAST;
+    }
+}
+
+template void flatten_bvh<2>(const PrimSource<2> &, const BvhTree<2> &, DeviceImage<2> &);
+template void flatten_bvh<3>(const PrimSource<3> &, const BvhTree<3> &, DeviceImage<3> &);
+template void flatten_wide<2>(const BvhTree<2> &, DeviceImage<2> &);
+template void flatten_wide<3>(const BvhTree<3> &, DeviceImage<3> &);
+template void flatten_snch<2>(const BvhTree<2> &, const SnchTree<2> &, DeviceImage<2> &);
+template void flatten_snch<3>(const BvhTree<3> &, const SnchTree<3> &, DeviceImage<3> &);
+
+}  // namespace gqb

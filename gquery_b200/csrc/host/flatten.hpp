@@ -1,0 +1,57 @@
+// Flattening pass: turns the CPU-built binary BVH / SNCH into the device records of
+// layout.h (pair records, leaf item records, quantised 8-wide nodes).
+#pragma once
+
+#include <vector>
+
+#include "../layout.h"
+#include "scene_build.hpp"
+
+namespace gqb {
+
+template <int D>
+struct DeviceImage {
+    using Pair = std::conditional_t<D == 2, gq_pair2_t, gq_pair3_t>;
+    using Prim = std::conditional_t<D == 2, gq_seg_t, gq_tri_t>;
+    using SPair = std::conditional_t<D == 2, gq_spair2_t, gq_spair3_t>;
+    using Sil = std::conditional_t<D == 2, gq_silv_t, gq_sile_t>;
+    using WNode = std::conditional_t<D == 2, gq_wnode2_t, gq_wnode3_t>;
+
+    // binary BVH
+    std::vector<Pair> pairs;
+    std::vector<Prim> prims;
+    int32_t root_ref = 0;
+    float root_lo[D] = {}, root_hi[D] = {};
+    int exact_stack = 0;  // entries the binary traversal needs (max leaf depth + 1)
+
+    // quantised 8-wide BVH
+    std::vector<WNode> wnodes;
+    int32_t wroot_ref = 0;
+    int wide_stack = 0;
+
+    // binary SNCH
+    std::vector<SPair> spairs;
+    std::vector<Sil> sils;
+    int32_t sroot_ref = 0;
+};
+
+// Reference encoding of an empty SNCH leaf (never produced by valid inputs).
+constexpr int32_t kEmptyLeaf = INT32_MIN;
+
+template <int D>
+void flatten_bvh(const PrimSource<D> &src, const BvhTree<D> &t, DeviceImage<D> &img);
+
+template <int D>
+void flatten_wide(const BvhTree<D> &t, DeviceImage<D> &img);
+
+template <int D>
+void flatten_snch(const BvhTree<D> &t, const SnchTree<D> &s, DeviceImage<D> &img);
+
+// Smallest power-of-two exponent e with 255 * 2^e >= hi - lo (clamped to normal floats).
+int quant_exponent(float lo, float hi);
+// Outward-rounded 8-bit bounds of [clo, chi] on the grid origin + q * 2^e.
+void quantise_bounds(float origin, int e, float clo, float chi, uint8_t *qlo, uint8_t *qhi);
+// Decoding used by the kernels: origin + q * 2^e in fp32.
+float dequant(float origin, int e, int q);
+
+}  // namespace gqb

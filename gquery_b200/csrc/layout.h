@@ -1,0 +1,122 @@
+// Device-side scene layout produced by the flattening pass (host) and read by the
+// traversal kernels.  All records are 16-byte aligned and read with 128-bit loads.
+//
+// Binary layout ("exact" kernels: same visit order as gQuery's traversal)
+// -----------------------------------------------------------------------
+// gQuery pops a node, then reads both children's boxes (bvh.py:159-167).  Here the
+// two child boxes of every interior node sit together in one "pair" record, so a
+// pop costs one record read.  A child reference is
+//     ref >= 0 : interior child, index of its own pair record
+//     ref <  0 : leaf child, ~ref = first ordered primitive (or silhouette); the
+//                leaf's items run until a record whose `last` flag is set.
+// Pair records are numbered in preorder of the interior nodes.
+//
+// Wide layout ("wide" kernels: quantised 8-wide nodes)
+// ----------------------------------------------------
+// The binary tree is collapsed into nodes of up to 8 children (leaves unchanged).
+// Child boxes are stored as 8-bit offsets on a per-axis grid
+//     lo = origin + qlo * 2^e,  hi = origin + qhi * 2^e
+// rounded outward on the host so that the decoded box contains the exact child box
+// in fp32 arithmetic: a query visits a superset of the nodes it would visit with
+// exact boxes and finds the same nearest primitive.
+#pragma once
+
+#include <stdint.h>
+
+#define GQ_STACK_EXACT 64   // gQuery's traversal stack size (bvh.py:132)
+#define GQ_STACK_WIDE 96
+#define GQ_WIDTH 8
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+// Leaf item flags (the .w / last word of primitive and silhouette records).
+#define GQ_ITEM_LAST 1u      // last item of its leaf
+#define GQ_ITEM_VALID 2u     // silhouette vertex: both neighbour indices present
+
+// 2D segment: (a.x, a.y, b.x, b.y) | (orig_index, flags, 0, 0)          32 B
+typedef struct {
+    float ax, ay, bx, by;
+    int32_t index, flags, pad0, pad1;
+} gq_seg_t;
+
+// 3D triangle: (a.xyz, b.x) | (b.yz, c.xy) | (c.z, orig_index, flags, 0)  48 B
+typedef struct {
+    float ax, ay, az, bx;
+    float by, bz, cx, cy;
+    float cz;
+    int32_t index, flags, pad;
+} gq_tri_t;
+
+// 2D silhouette vertex: (a.xy, b.xy) | (c.xy, prim_id, flags)            32 B
+typedef struct {
+    float ax, ay, bx, by;
+    float cx, cy;
+    int32_t prim, flags;
+} gq_silv_t;
+
+// 3D silhouette edge (a, b end points; c, d opposite vertices)            64 B
+typedef struct {
+    float ax, ay, az, bx;
+    float by, bz, cx, cy;
+    float cz, dx, dy, dz;
+    int32_t prim, flags, pad0, pad1;
+} gq_sile_t;
+
+// Binary BVH pair records.
+typedef struct {  // 2D, 48 B: left box, right box, refs
+    float l_lox, l_loy, l_hix, l_hiy;
+    float r_lox, r_loy, r_hix, r_hiy;
+    int32_t ref_l, ref_r, pad0, pad1;
+} gq_pair2_t;
+
+typedef struct {  // 3D, 64 B
+    float l_lox, l_loy, l_loz, l_hix;
+    float l_hiy, l_hiz, r_lox, r_loy;
+    float r_loz, r_hix, r_hiy, r_hiz;
+    int32_t ref_l, ref_r, pad0, pad1;
+} gq_pair3_t;
+
+// Binary SNCH pair records: child box + cone (axis, half angle, radius).
+typedef struct {  // 2D, 80 B
+    float l_lox, l_loy, l_hix, l_hiy;
+    float l_ax, l_ay, l_half, l_rad;
+    float r_lox, r_loy, r_hix, r_hiy;
+    float r_ax, r_ay, r_half, r_rad;
+    int32_t ref_l, ref_r, pad0, pad1;
+} gq_spair2_t;
+
+typedef struct {  // 3D, 96 B
+    float l_lox, l_loy, l_loz, l_hix;
+    float l_hiy, l_hiz, l_ax, l_ay;
+    float l_az, l_half, l_rad, r_lox;
+    float r_loy, r_loz, r_hix, r_hiy;
+    float r_hiz, r_ax, r_ay, r_az;
+    float r_half, r_rad;
+    int32_t ref_l, ref_r;
+} gq_spair3_t;
+
+// Quantised 8-wide node, 3D: 96 B (three 32-byte sectors).
+//   origin.xyz, meta = exp_x | exp_y << 8 | exp_z << 16 | nchild << 24 (exps biased by 127)
+//   ref[8]      child references (same encoding as pair refs)
+//   q[6][8]     qlo_x, qlo_y, qlo_z, qhi_x, qhi_y, qhi_z (8 bits each)
+typedef struct {
+    float ox, oy, oz;
+    uint32_t meta;
+    int32_t ref[8];
+    uint8_t q[6][8];
+} gq_wnode3_t;
+
+// Quantised 8-wide node, 2D: 80 B.
+//   origin.xy, meta = exp_x | exp_y << 8 | nchild << 24
+typedef struct {
+    float ox, oy;
+    uint32_t meta, pad;
+    int32_t ref[8];
+    uint8_t q[4][8];  // qlo_x, qlo_y, qhi_x, qhi_y
+} gq_wnode2_t;
+
+#ifdef __cplusplus
+}
+#endif

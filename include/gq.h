@@ -1,0 +1,185 @@
+/* gq.h — C ABI of the B200 geometry-query engine (libgq.so).
+ *
+ * Replaces two reference interfaces:
+ *   - the nanobind builder module `gquery_ext` (src/gquery.cpp:181-250): BVH, BVH3D,
+ *     SNCH, SNCH3D, node_data(), primitive_data(), silhouette_data(),
+ *     build_flat_silhouette_edges();
+ *   - the DrJit-traced traversal methods called by Polyline / Mesh:
+ *     BVH.closest_point (gquery/shapes/bvh.py:127), BVH.intersect (bvh.py:200),
+ *     BVH3D.closest_point (bvh3d.py:108), BVH3D.intersect (bvh3d.py:176),
+ *     SNCH.closest_silhouette (snch.py:106), SNCH3D.closest_silhouette (snch3d.py:143),
+ *     and the brute-force *_baseline methods (polyline.py:137-223, mesh.py:287-362).
+ *
+ * Conventions
+ *   - Plain pointers and sizes only.  Host pointers are marked "host"; everything a
+ *     query reads or writes is device memory on the scene's device.
+ *   - Every call returns a gq_status; nothing throws across the ABI.  The text of
+ *     the last error on the calling thread is available from gq_last_error().
+ *   - Query calls are asynchronous and ordered on the CUDA stream passed as
+ *     `stream` (a cudaStream_t; NULL = legacy default stream).
+ *   - Scenes are immutable after the build and may be shared by host threads and
+ *     streams.
+ *   - Arrays of vectors are strided: component k of element i is
+ *     ptr[k * comp_stride + i * elem_stride] (SoA [D][n] -> (n, 1); AoS [n][D] -> (1, D)).
+ *   - Output records are structure-of-arrays with component stride n; a NULL field
+ *     pointer skips that field.  A miss writes an all-zero record (valid = 0).
+ */
+#ifndef GQ_H
+#define GQ_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t gq_status;
+#define GQ_OK 0
+#define GQ_ERR_INVALID 1    /* bad argument (shape, null pointer, index out of range) */
+#define GQ_ERR_CUDA 2       /* a CUDA call failed */
+#define GQ_ERR_NOMEM 3      /* allocation failed */
+#define GQ_ERR_DEPTH 4      /* tree deeper than the traversal stack of the requested variant */
+#define GQ_ERR_DEVICE 5     /* a kernel raised its error flag (see gq_scene_device_error) */
+#define GQ_ERR_UNSUPPORTED 6
+
+/* Traversal variants */
+#define GQ_VARIANT_EXACT 0  /* binary tree, gQuery's visit order: reference-identical answers */
+#define GQ_VARIANT_WIDE8 1  /* 8-wide nodes, 8-bit outward-rounded child boxes */
+#define GQ_VARIANT_AUTO 2   /* fastest available (WIDE8 for BVH queries, EXACT for SNCH) */
+
+typedef struct gq_scene gq_scene;
+
+typedef struct {
+    int32_t max_prims_in_node; /* leaf size limit of the SAH build; gQuery's default is 10 */
+    int32_t n_threads;         /* host threads for the build; 0 = all cores */
+    int32_t build_snch;        /* also build silhouettes and normal cones */
+    int32_t build_wide;        /* also build the quantised 8-wide BVH */
+    int32_t device;            /* CUDA device that holds the scene */
+} gq_build_opts;
+
+typedef struct {
+    int32_t dim;               /* 2 or 3 */
+    int64_t n_vertices, n_prims, n_nodes, n_wide_nodes, n_silhouettes;
+    int32_t max_depth;         /* deepest leaf of the binary tree (root = 0) */
+    int32_t exact_stack, wide_stack;
+    int64_t device_bytes;      /* HBM held by the scene */
+    float bbox_lo[3], bbox_hi[3];
+} gq_scene_info;
+
+typedef struct {
+    const float *ptr;
+    int64_t comp_stride;
+    int64_t elem_stride;
+} gq_vecs;
+
+typedef struct {
+    uint8_t *valid;   /* [n] */
+    float *p;         /* [D][n] closest point */
+    float *n;         /* [D][n] normal */
+    float *t;         /* 2D: [n] parameter on the segment; 3D: [2][n] barycentric uv */
+    float *d;         /* [n] distance */
+    int32_t *prim_id; /* [n] original primitive index */
+} gq_cp_out;
+
+typedef struct {
+    uint8_t *valid;
+    float *p;
+    float *n;
+    float *t;         /* 2D: [n] (gQuery stores -1 on a hit); 3D: [2][n] uv */
+    float *d;         /* [n] ray parameter of the hit */
+    int32_t *prim_id;
+    uint8_t *on_boundary;
+} gq_ray_out;
+
+typedef struct {
+    uint8_t *valid;
+    float *p;         /* [D][n] closest silhouette point */
+    float *d;
+    int32_t *prim_id; /* silhouette id: vertex index (2D) / edge index (3D) */
+} gq_sil_out;
+
+typedef struct {
+    int32_t variant;        /* GQ_VARIANT_* */
+    int32_t sort;           /* 1: reorder queries along a Morton curve before traversal */
+    const int32_t *order;   /* optional device permutation from gq_query_order(); replaces `sort` */
+    void *scratch;          /* optional device scratch (see gq_query_scratch_bytes); NULL = stream-ordered allocation */
+    int64_t scratch_bytes;
+} gq_query_opts;
+
+/* ---- errors ---- */
+/* Copies the calling thread's last error message (NUL-terminated, truncated to cap). */
+void gq_last_error(char *buf, int64_t cap);
+const char *gq_status_string(gq_status s);
+
+/* ---- scene build (replaces gquery_ext.BVH / BVH3D / SNCH / SNCH3D constructors,
+ *      src/gquery.cpp:184-185, 196-197, 227-228, 239-240) ----
+ * vertices: host [nv][D] float32; prims: host [np][D] int32 (edges in 2D, faces in 3D). */
+gq_status gq_scene_build_2d(const float *vertices, int64_t nv, const int32_t *edges, int64_t ne,
+                            const gq_build_opts *opts, gq_scene **out);
+gq_status gq_scene_build_3d(const float *vertices, int64_t nv, const int32_t *faces, int64_t nf,
+                            const gq_build_opts *opts, gq_scene **out);
+gq_status gq_scene_free(gq_scene *scene);
+gq_status gq_scene_get_info(const gq_scene *scene, gq_scene_info *info);
+
+/* Reference float layouts (gquery_ext node_data / primitive_data / silhouette_data /
+ * raw_silhouette_data, src/gquery.cpp:186-187, 229-231, 241-244).  Copies up to `cap`
+ * floats into host `dst` and stores the full length in *len (dst may be NULL to query). */
+#define GQ_ARRAY_BVH_NODES 0       /* stride 2D+3 (7 / 9) */
+#define GQ_ARRAY_PRIMITIVES 1      /* stride 5 / 10 */
+#define GQ_ARRAY_SNCH_NODES 2      /* stride 13 / 16 */
+#define GQ_ARRAY_SILHOUETTES 3     /* ordered, per-leaf lists; stride 10 / 19 */
+#define GQ_ARRAY_RAW_SILHOUETTES 4 /* one per vertex / unique edge */
+#define GQ_ARRAY_WIDE_NODES 5      /* quantised 8-wide node records as raw 32-bit words (24 / 20 per node);
+                                      host-only scenes (device < 0) only */
+gq_status gq_scene_ref_array(const gq_scene *scene, int32_t which, float *dst, int64_t cap, int64_t *len);
+
+/* build_flat_silhouette_edges (src/gquery.cpp:250, src/shapes/silhouette_edge.cpp:62-71):
+ * host in, host out (19 floats per unique edge). */
+gq_status gq_flat_silhouette_edges(const float *vertices, int64_t nv, const int32_t *faces, int64_t nf,
+                                   float *dst, int64_t cap, int64_t *len);
+
+/* ---- queries ---- */
+/* Device scratch a query of n items needs when opts->scratch is supplied. */
+int64_t gq_query_scratch_bytes(int64_t n);
+
+/* Morton order of n query points (or ray origins) over the scene's box: writes a
+ * permutation of 0..n-1 to device `order`.  `scratch` (device, gq_order_scratch_bytes(n)
+ * bytes) may be NULL for a stream-ordered allocation.  Several queries on the same
+ * points can share one order through gq_query_opts.order. */
+int64_t gq_order_scratch_bytes(int64_t n);
+gq_status gq_query_order(const gq_scene *scene, gq_vecs points, int64_t n, int32_t *order, void *scratch,
+                         int64_t scratch_bytes, void *stream);
+
+/* closest_point_bvh (Polyline: polyline.py:171 -> bvh.py:127; Mesh: mesh.py:119 -> bvh3d.py:108) */
+gq_status gq_closest_point(const gq_scene *scene, gq_vecs q, int64_t n, const gq_cp_out *out,
+                           const gq_query_opts *opts, void *stream);
+
+/* intersect_bvh (polyline.py:132 -> bvh.py:200; mesh.py:86 -> bvh3d.py:176).
+ * r_max: device [n] or NULL for +inf. */
+gq_status gq_intersect(const gq_scene *scene, gq_vecs origin, gq_vecs dir, const float *r_max, int64_t n,
+                       const gq_ray_out *out, const gq_query_opts *opts, void *stream);
+
+/* closest_silhouette_snch (polyline.py:225 -> snch.py:106; mesh.py:137 -> snch3d.py:143).
+ * r_max: device [n] or NULL for +inf.  Needs a scene built with build_snch. */
+gq_status gq_closest_silhouette(const gq_scene *scene, gq_vecs x, const float *r_max, int64_t n,
+                                const gq_sil_out *out, const gq_query_opts *opts, void *stream);
+
+/* Brute-force scans over every primitive in original order (closest_point_baseline,
+ * intersect_baseline: polyline.py:137-209, mesh.py:287-348).  FP32 like the reference. */
+gq_status gq_closest_point_brute(const gq_scene *scene, gq_vecs q, int64_t n, const gq_cp_out *out, void *stream);
+gq_status gq_intersect_brute(const gq_scene *scene, gq_vecs origin, gq_vecs dir, const float *r_max, int64_t n,
+                             const gq_ray_out *out, void *stream);
+
+/* FP64 brute force used to state the error of the FP32 paths: nearest distance
+ * (closest point) or nearest ray parameter (+inf on a miss) and its primitive. */
+gq_status gq_brute_f64(const gq_scene *scene, int32_t kind /*0 closest point, 1 ray*/, gq_vecs a, gq_vecs b,
+                       int64_t n, double *out_d, int32_t *out_id, void *stream);
+
+/* Reads and clears the scene's device error word (stack overflow etc.); synchronises `stream`. */
+gq_status gq_scene_device_error(const gq_scene *scene, void *stream, int32_t *flags);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GQ_H */

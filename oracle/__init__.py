@@ -1,0 +1,148 @@
+"""ORACLE — test infrastructure only (used by tests/, the smoke check and the
+CPU-baseline leg of bench.py; never by the product).
+
+ctypes wrapper of oracle/_build/liboracle.so, the scalar C++ restatement of the
+reference traversals (see gq_oracle.cpp for the citations and the parity status).
+Inputs are the reference float layouts (node / primitive / silhouette arrays),
+queries are [n, D] float32.  Results come back as dicts of numpy arrays with the
+record field names; misses are all-zero records like the reference's dr.zeros.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "liboracle.so"
+_lib = None
+
+
+def build(force: bool = False) -> Path:
+    srcs = [HERE / "gq_oracle.cpp", HERE.parent / "gquery_b200" / "csrc" / "gq_fmath.h"]
+    if force or not LIB.exists() or any(s.stat().st_mtime > LIB.stat().st_mtime for s in srcs):
+        subprocess.run(["make", "-C", str(HERE), "-B" if force else "all"], check=True, capture_output=True)
+    return LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        _lib = C.CDLL(str(LIB))
+    return _lib
+
+
+def n_threads() -> int:
+    return int(os.environ.get("GQ_ORACLE_THREADS", "0")) or os.cpu_count() or 1
+
+
+def _f(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _split(dim, kind, f, i):
+    """Record fields from the oracle's row layout."""
+    out = {"valid": i[:, 0] == 1, "prim_id": i[:, 1].copy(), "error": i[:, 0] < 0}
+    if kind == "cp":
+        out["p"] = f[:, 0:dim].T.copy()
+        out["n"] = f[:, dim:2 * dim].T.copy()
+        if dim == 2:
+            out["t"] = f[:, 4].copy()
+            out["d"] = f[:, 5].copy()
+        else:
+            out["uv"] = f[:, 6:8].T.copy()
+            out["d"] = f[:, 8].copy()
+    elif kind == "ray":
+        out["p"] = f[:, 0:dim].T.copy()
+        out["n"] = f[:, dim:2 * dim].T.copy()
+        if dim == 2:
+            out["t"] = f[:, 4].copy()
+            out["d"] = f[:, 5].copy()
+        else:
+            out["uv"] = f[:, 6:8].T.copy()
+            out["d"] = f[:, 8].copy()
+        out["on_boundary"] = i[:, 2] == 1
+    else:
+        out["p"] = f[:, 0:dim].T.copy()
+        out["d"] = f[:, dim].copy()
+    return out
+
+
+_KF = {("cp", 2): 6, ("cp", 3): 9, ("ray", 2): 6, ("ray", 3): 9, ("sil", 2): 3, ("sil", 3): 4}
+
+
+def _run(name, kind, dim, args, nq, counts, threads):
+    f = np.zeros((nq, _KF[(kind, dim)]), np.float32)
+    i = np.zeros((nq, 3), np.int32)
+    cnt = np.zeros((nq, 2), np.int32) if counts else None
+    fn = getattr(lib(), name)
+    fn.restype = None
+    cargs = []
+    for a in args:
+        if a is None:
+            cargs.append(C.c_void_p(None))
+        elif isinstance(a, np.ndarray):
+            cargs.append(C.c_void_p(a.ctypes.data))
+        else:
+            cargs.append(C.c_int64(a))
+    fn(*cargs, C.c_void_p(f.ctypes.data), C.c_void_p(i.ctypes.data),
+       C.c_void_p(cnt.ctypes.data) if counts else C.c_void_p(None), C.c_int(threads or n_threads()))
+    out = _split(dim, kind, f, i)
+    if counts:
+        out["interior"] = cnt[:, 0].copy()
+        out["tested"] = cnt[:, 1].copy()
+    return out
+
+
+def closest_point(dim, nodes, prims, q, counts=False, threads=0):
+    """BVH.closest_point / BVH3D.closest_point over reference arrays."""
+    nodes, prims, q = _f(nodes), _f(prims), _f(q).reshape(-1, dim)
+    return _run(f"orc_cp{dim}d", "cp", dim, [nodes, prims, q, q.shape[0]], q.shape[0], counts, threads)
+
+
+def intersect(dim, nodes, prims, x, v, r_max=None, counts=False, threads=0):
+    """BVH.intersect / BVH3D.intersect over reference arrays."""
+    nodes, prims = _f(nodes), _f(prims)
+    x, v = _f(x).reshape(-1, dim), _f(v).reshape(-1, dim)
+    rm = None if r_max is None else _f(np.broadcast_to(np.asarray(r_max, np.float32), (x.shape[0],)))
+    return _run(f"orc_ray{dim}d", "ray", dim, [nodes, prims, x, v, rm, x.shape[0]], x.shape[0], counts, threads)
+
+
+def closest_silhouette(dim, snch_nodes, silhouettes, x, r_max=None, counts=False, threads=0):
+    """SNCH.closest_silhouette / SNCH3D.closest_silhouette over reference arrays."""
+    nodes, sils = _f(snch_nodes), _f(silhouettes)
+    x = _f(x).reshape(-1, dim)
+    rm = None if r_max is None else _f(np.broadcast_to(np.asarray(r_max, np.float32), (x.shape[0],)))
+    return _run(f"orc_sil{dim}d", "sil", dim, [nodes, sils, x, rm, x.shape[0]], x.shape[0], counts, threads)
+
+
+def brute_closest_point(dim, verts, index, q, threads=0):
+    """FP64 nearest distance and primitive (original order)."""
+    verts, q = _f(verts).reshape(-1, dim), _f(q).reshape(-1, dim)
+    index = np.ascontiguousarray(index, np.int32).reshape(-1, dim)
+    d = np.zeros(q.shape[0], np.float64)
+    ids = np.zeros(q.shape[0], np.int32)
+    fn = getattr(lib(), f"orc_brute_cp{dim}d")
+    fn.restype = None
+    fn(C.c_void_p(verts.ctypes.data), C.c_void_p(index.ctypes.data), C.c_int64(index.shape[0]),
+       C.c_void_p(q.ctypes.data), C.c_int64(q.shape[0]), C.c_void_p(d.ctypes.data), C.c_void_p(ids.ctypes.data),
+       C.c_int(threads or n_threads()))
+    return d, ids
+
+
+def brute_intersect3d(verts, index, x, v, threads=0):
+    verts = _f(verts).reshape(-1, 3)
+    x, v = _f(x).reshape(-1, 3), _f(v).reshape(-1, 3)
+    index = np.ascontiguousarray(index, np.int32).reshape(-1, 3)
+    t = np.zeros(x.shape[0], np.float64)
+    ids = np.zeros(x.shape[0], np.int32)
+    fn = lib().orc_brute_ray3d
+    fn.restype = None
+    fn(C.c_void_p(verts.ctypes.data), C.c_void_p(index.ctypes.data), C.c_int64(index.shape[0]),
+       C.c_void_p(x.ctypes.data), C.c_void_p(v.ctypes.data), C.c_int64(x.shape[0]), C.c_void_p(t.ctypes.data),
+       C.c_void_p(ids.ctypes.data), C.c_int(threads or n_threads()))
+    return t, ids

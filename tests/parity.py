@@ -1,0 +1,51 @@
+"""Comparison helpers shared by the parity tests."""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+REL_TOL = 2e-6  # stated tolerance for distances and hit points across traversal orders
+
+
+def to_np(rec) -> dict:
+    out = {}
+    for k, v in vars(rec).items():
+        out[k] = v.detach().cpu().numpy() if isinstance(v, torch.Tensor) else v
+    return out
+
+
+def assert_bitwise(gpu: dict, ref: dict, fields, what=""):
+    for f in fields:
+        a, b = np.asarray(gpu[f]), np.asarray(ref[f])
+        assert a.shape == b.shape, f"{what}{f}: shape {a.shape} vs {b.shape}"
+        if a.dtype == np.bool_ or b.dtype == np.bool_:
+            bad = a.astype(bool) != b.astype(bool)
+        elif a.dtype.kind == "f":
+            bad = a.astype(np.float32).view(np.uint32) != b.astype(np.float32).view(np.uint32)
+        else:
+            bad = a.astype(np.int64) != b.astype(np.int64)
+        nbad = int(np.count_nonzero(bad))
+        if nbad:
+            idx = np.argwhere(bad)[:5]
+            raise AssertionError(f"{what}{f}: {nbad} mismatches, first at {idx.tolist()}: "
+                                 f"gpu={a[tuple(idx[0])]!r} ref={b[tuple(idx[0])]!r}")
+
+
+def tie_report(a: dict, b: dict, rel=REL_TOL) -> dict:
+    """Compares two result sets that may differ only at ties: same validity; where the
+    primitive differs, the distances agree within `rel` (relative)."""
+    va, vb = np.asarray(a["valid"]).astype(bool), np.asarray(b["valid"]).astype(bool)
+    pa, pb = np.asarray(a["prim_id"]), np.asarray(b["prim_id"])
+    da, db = np.asarray(a["d"], np.float64), np.asarray(b["d"], np.float64)
+    both = va & vb
+    scale = np.maximum(np.maximum(np.abs(da), np.abs(db)), 1e-30)
+    reldiff = np.abs(da - db) / scale
+    prim_diff = both & (pa != pb)
+    return {
+        "n": int(va.size),
+        "valid_mismatch": int(np.count_nonzero(va != vb)),
+        "prim_mismatch": int(np.count_nonzero(prim_diff)),
+        "prim_mismatch_exact_tie": int(np.count_nonzero(prim_diff & (da == db))),
+        "prim_mismatch_not_tie": int(np.count_nonzero(prim_diff & (reldiff > rel))),
+        "max_rel_d": float(reldiff[both].max()) if both.any() else 0.0,
+    }

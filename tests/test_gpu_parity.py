@@ -1,0 +1,251 @@
+"""GPU parity: the CUDA traversals (through libgq.so) against the CPU oracle.
+
+The exact kernels follow gQuery's visit order and must agree with the oracle bit
+for bit on every record field.  The quantised 8-wide kernels must give the same
+validity everywhere and the same primitive except at FP32 distance ties (distances
+within 2e-6 relative).  Sizes are chosen so the oracle finishes in seconds.
+"""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from gquery_b200 import _lib as L
+from gquery_b200 import workloads as W
+from gquery_b200.scene import Scene
+from parity import REL_TOL, assert_bitwise, tie_report, to_np
+
+pytestmark = pytest.mark.gpu
+
+CP_FIELDS_2D = ["valid", "p", "n", "t", "d", "prim_id"]
+CP_FIELDS_3D = ["valid", "p", "n", "uv", "d", "prim_id"]
+RAY_FIELDS_2D = ["valid", "p", "n", "t", "d", "prim_id", "on_boundary"]
+RAY_FIELDS_3D = ["valid", "p", "n", "uv", "d", "prim_id", "on_boundary"]
+SIL_FIELDS = ["valid", "p", "d", "prim_id"]
+ABS_TOL = 5e-7  # FP32 vs FP64 distance error: about 2 ulp of coordinates of magnitude 2
+
+
+@pytest.fixture(scope="module")
+def star():
+    v, e = W.star_polyline(4096, seed=0)
+    return Scene(v, e, 2, device=0)
+
+
+@pytest.fixture(scope="module")
+def mesh_c1():
+    v, f = W.config1_mesh()
+    return Scene(v, f, 3, device=0, build_snch=False)
+
+
+@pytest.fixture(scope="module")
+def mesh_c2():
+    v, f = W.config2_mesh()
+    return Scene(v, f, 3, device=0)
+
+
+@pytest.fixture(scope="module")
+def mesh_small():
+    v, f = W.icosphere(4, amplitude=0.3, seed=3)
+    return Scene(v, f, 3, device=0)
+
+
+def _ref(scene):
+    return (scene.ref_array(L.ARRAY_BVH_NODES), scene.ref_array(L.ARRAY_PRIMITIVES))
+
+
+def _sref(scene):
+    return (scene.ref_array(L.ARRAY_SNCH_NODES), scene.ref_array(L.ARRAY_SILHOUETTES))
+
+
+# ---------------------------------------------------------------- exact, 2D
+
+@pytest.mark.parametrize("sort", [False, True])
+def test_cp2d_exact_bitwise(star, sort):
+    q = W.uniform_points(65536 + 37, 2, seed=11)
+    got = to_np(star.closest_point(q, variant="exact", sort=sort))
+    ref = oracle.closest_point(2, *_ref(star), q)
+    assert_bitwise(got, ref, CP_FIELDS_2D, "cp2d ")
+    assert star.device_error() == 0
+
+
+def test_ray2d_exact_bitwise(star):
+    o, d = W.rays(65536, 2, seed=12)
+    got = to_np(star.intersect(o, d, variant="exact", sort=True))
+    ref = oracle.intersect(2, *_ref(star), o, d)
+    assert_bitwise(got, ref, RAY_FIELDS_2D, "ray2d ")
+    assert 0.2 < got["valid"].mean() < 1.0
+
+
+def test_ray2d_exact_finite_rmax(star):
+    o, d = W.rays(8192, 2, seed=13)
+    rmax = np.random.default_rng(5).uniform(0.0, 2.0, size=o.shape[0]).astype(np.float32)
+    got = to_np(star.intersect(o, d, torch.as_tensor(rmax), variant="exact"))
+    ref = oracle.intersect(2, *_ref(star), o, d, rmax)
+    assert_bitwise(got, ref, RAY_FIELDS_2D, "ray2d rmax ")
+
+
+def test_sil2d_exact_bitwise(star):
+    x = W.uniform_points(32768, 2, seed=14)
+    got = to_np(star.closest_silhouette(x, sort=True))
+    ref = oracle.closest_silhouette(2, *_sref(star), x)
+    assert_bitwise(got, ref, SIL_FIELDS, "sil2d ")
+
+
+def test_sil2d_exact_finite_rmax(star):
+    x = W.uniform_points(8192, 2, seed=15)
+    got = to_np(star.closest_silhouette(x, 0.25))
+    ref = oracle.closest_silhouette(2, *_sref(star), x, 0.25)
+    assert_bitwise(got, ref, SIL_FIELDS, "sil2d rmax ")
+    assert 0.0 < got["valid"].mean() < 1.0
+
+
+# ---------------------------------------------------------------- exact, 3D
+
+def test_cp3d_exact_bitwise_c1(mesh_c1):
+    q = W.uniform_points(16384, 3, seed=21)
+    got = to_np(mesh_c1.closest_point(q, variant="exact", sort=True))
+    ref = oracle.closest_point(3, *_ref(mesh_c1), q)
+    assert_bitwise(got, ref, CP_FIELDS_3D, "cp3d ")
+
+
+def test_ray3d_exact_bitwise_c1(mesh_c1):
+    o, d = W.rays(65536, 3, seed=22)
+    got = to_np(mesh_c1.intersect(o, d, variant="exact", sort=True))
+    ref = oracle.intersect(3, *_ref(mesh_c1), o, d)
+    assert_bitwise(got, ref, RAY_FIELDS_3D, "ray3d ")
+    assert got["valid"].mean() > 0.1
+
+
+def test_sil3d_exact_bitwise_c2(mesh_c2):
+    x = W.uniform_points(4096, 3, seed=23)
+    got = to_np(mesh_c2.closest_silhouette(x, sort=True))
+    ref = oracle.closest_silhouette(3, *_sref(mesh_c2), x)
+    assert_bitwise(got, ref, SIL_FIELDS, "sil3d ")
+
+
+def test_exact_small_mesh_all_queries(mesh_small):
+    q = W.uniform_points(20000, 3, seed=24)
+    o, d = W.rays(20000, 3, seed=25)
+    nodes, prims = _ref(mesh_small)
+    assert_bitwise(to_np(mesh_small.closest_point(q, variant="exact")), oracle.closest_point(3, nodes, prims, q),
+                   CP_FIELDS_3D, "cp3d small ")
+    assert_bitwise(to_np(mesh_small.intersect(o, d, variant="exact")), oracle.intersect(3, nodes, prims, o, d),
+                   RAY_FIELDS_3D, "ray3d small ")
+    assert_bitwise(to_np(mesh_small.closest_silhouette(q)), oracle.closest_silhouette(3, *_sref(mesh_small), q),
+                   SIL_FIELDS, "sil3d small ")
+
+
+# ---------------------------------------------------------------- wide vs exact
+
+def test_cp3d_wide_matches_exact(mesh_c1):
+    q = W.uniform_points(262144, 3, seed=31)
+    a = to_np(mesh_c1.closest_point(q, variant="exact", sort=True))
+    b = to_np(mesh_c1.closest_point(q, variant="wide8", sort=True))
+    rep = tie_report(a, b)
+    assert rep["valid_mismatch"] == 0, rep
+    assert rep["prim_mismatch_not_tie"] == 0, rep
+    assert rep["max_rel_d"] <= REL_TOL, rep
+    assert mesh_c1.device_error() == 0
+
+
+def test_ray3d_wide_matches_exact(mesh_c1):
+    o, d = W.rays(262144, 3, seed=32)
+    a = to_np(mesh_c1.intersect(o, d, variant="exact", sort=True))
+    b = to_np(mesh_c1.intersect(o, d, variant="wide8", sort=True))
+    rep = tie_report(a, b)
+    assert rep["valid_mismatch"] == 0, rep
+    assert rep["prim_mismatch_not_tie"] == 0, rep
+    assert rep["max_rel_d"] <= REL_TOL, rep
+
+
+def test_2d_wide_matches_exact(star):
+    q = W.uniform_points(131072, 2, seed=33)
+    rep = tie_report(to_np(star.closest_point(q, variant="exact")), to_np(star.closest_point(q, variant="wide8")))
+    assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0, rep
+    o, d = W.rays(131072, 2, seed=34)
+    rep = tie_report(to_np(star.intersect(o, d, variant="exact")), to_np(star.intersect(o, d, variant="wide8")))
+    assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0, rep
+
+
+# ---------------------------------------------------------------- layouts and edges
+
+def test_soa_aos_inputs_agree(mesh_small):
+    q = W.uniform_points(5000, 3, seed=41)
+    aos = torch.as_tensor(q).cuda()
+    soa = aos.t().contiguous()
+    a = to_np(mesh_small.closest_point(aos, variant="exact"))
+    b = to_np(mesh_small.closest_point(soa, variant="exact"))
+    assert_bitwise(a, b, CP_FIELDS_3D, "layout ")
+
+
+@pytest.mark.parametrize("n", [0, 1, 127, 128, 129])
+def test_ragged_sizes(mesh_small, n):
+    q = W.uniform_points(max(n, 1), 3, seed=42)[:n]
+    got = to_np(mesh_small.closest_point(torch.as_tensor(q).reshape(n, 3), variant="wide8"))
+    if n:
+        ref = oracle.closest_point(3, *_ref(mesh_small), q)
+        rep = tie_report(got, ref)
+        assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0, rep
+    else:
+        assert got["d"].shape == (0,)
+
+
+def test_queries_on_vertices_and_far_away(mesh_small):
+    v = mesh_small.vertices_host[:2000]
+    far = np.full((16, 3), 1e6, np.float32)
+    q = np.concatenate([v, far], axis=0)
+    nodes, prims = _ref(mesh_small)
+    assert_bitwise(to_np(mesh_small.closest_point(q, variant="exact")), oracle.closest_point(3, nodes, prims, q),
+                   CP_FIELDS_3D, "vertices ")
+    got = to_np(mesh_small.closest_point(q, variant="exact"))
+    assert (got["d"][:2000] == 0).all()
+
+
+def test_degenerate_scene_single_leaf():
+    v = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], np.float32)
+    f = np.array([[0, 1, 2], [0, 1, 3], [1, 2, 3], [0, 2, 3]], np.int32)
+    s = Scene(v, f, 3, device=0)
+    q = W.uniform_points(1000, 3, seed=43)
+    nodes, prims = _ref(s)
+    ref = oracle.closest_point(3, nodes, prims, q)
+    assert_bitwise(to_np(s.closest_point(q, variant="exact")), ref, CP_FIELDS_3D, "tetra exact ")
+    rep = tie_report(to_np(s.closest_point(q, variant="wide8")), ref)
+    assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0, rep
+
+
+# ---------------------------------------------------------------- brute force and FP64
+
+def test_brute_force_fp32_matches_fp64(mesh_small, star):
+    q = W.uniform_points(4096, 3, seed=51)
+    got = to_np(mesh_small.closest_point_brute(q))
+    d64, id64 = oracle.brute_closest_point(3, mesh_small.vertices_host, mesh_small.indices_host, q)
+    assert np.abs(got["d"] - d64).max() <= ABS_TOL
+    q2 = W.uniform_points(4096, 2, seed=52)
+    got2 = to_np(star.closest_point_brute(q2))
+    d2, id2 = oracle.brute_closest_point(2, star.vertices_host, star.indices_host, q2)
+    assert np.abs(got2["d"] - d2).max() <= ABS_TOL
+
+
+def test_brute_f64_gpu_matches_cpu(mesh_small):
+    q = W.uniform_points(2048, 3, seed=53)
+    d_gpu, id_gpu = mesh_small.brute_f64("cp", q)
+    d_cpu, id_cpu = oracle.brute_closest_point(3, mesh_small.vertices_host, mesh_small.indices_host, q)
+    assert np.allclose(d_gpu.cpu().numpy(), d_cpu, rtol=1e-12, atol=0)
+    o, d = W.rays(2048, 3, seed=54)
+    t_gpu, _ = mesh_small.brute_f64("ray", o, d)
+    t_cpu, _ = oracle.brute_intersect3d(mesh_small.vertices_host, mesh_small.indices_host, o, d)
+    t_gpu = t_gpu.cpu().numpy()
+    assert np.array_equal(np.isinf(t_gpu), np.isinf(t_cpu))
+    fin = np.isfinite(t_cpu)
+    assert np.allclose(t_gpu[fin], t_cpu[fin], rtol=1e-12)
+
+
+def test_exact_error_vs_fp64_c1_subset(mesh_c1):
+    q = W.uniform_points(8192, 3, seed=55)
+    got = to_np(mesh_c1.closest_point(q, variant="exact"))
+    d64, _ = mesh_c1.brute_f64("cp", q)
+    d64 = d64.cpu().numpy()
+    err = np.abs(got["d"].astype(np.float64) - d64)
+    assert err.max() <= ABS_TOL, err.max()
