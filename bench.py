@@ -44,7 +44,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=1 << 23, help="queries of each kind per rank")
-    ap.add_argument("--variant", default="wide8", choices=["wide8", "exact"])
+    ap.add_argument("--variant", default="auto", choices=["auto", "wide8", "coherent", "exact"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -283,12 +283,14 @@ def main():
         return res, clk
 
     plain, _ = timed("exact", max(2, args.steps // 2), 2)
+    quant, _ = timed("wide8", max(2, args.steps // 2), 2)
     main_res, clocks = timed(args.variant, args.steps, max(3, args.warmup), clocks=True)
     assert scene.device_error() == 0, "device error flag raised"
 
     total_q = 2 * n * world
     value = total_q / (main_res["step_ms"] / 1e3) / 1e6
     plain_value = total_q / (plain["step_ms"] / 1e3) / 1e6
+    quant_value = total_q / (quant["step_ms"] / 1e3) / 1e6
 
     # ---- end to end through the public API with host buffers ----
     e2e = None
@@ -348,8 +350,9 @@ def main():
             t_ms = main_res[f"{dominant}_ms"]
             achieved = b * n / (t_ms / 1e3) / 1e9
             tr = traffic_per_query().get(f"{dominant}3d_{args.variant}")
+            tuned_v = scene.get_tuning(dominant)["variant"] if args.variant == "auto" else args.variant
             roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                    "traffic": (tr * n if tr else None), "kernel": f"{dominant}3d_{args.variant}",
+                    "traffic": (tr * n if tr else None), "kernel": f"{dominant}3d_{tuned_v}",
                     "algorithmic_bytes_per_query": b, "peak_source": peak_kind,
                     "note": "achieved = reference binary-traversal bytes (oracle visit counts) / kernel time"}
         line = {
@@ -360,6 +363,10 @@ def main():
                        "parallelism": f"replicated scene, {world} query shard(s)", "l2": "flushed between steps"},
             "plain_exact": {"value": plain_value, "ms_per_step": plain["step_ms"], "cp_ms": plain["cp_ms"],
                             "ray_ms": plain["ray_ms"]},
+            "quantised_wide8": {"value": quant_value, "ms_per_step": quant["step_ms"], "cp_ms": quant["cp_ms"],
+                                "ray_ms": quant["ray_ms"], "vs_plain": quant_value / plain_value},
+            "tuned": {"cp": scene.get_tuning("cp"), "ray": scene.get_tuning("ray"),
+                      "vs_plain": value / plain_value},
             "breakdown_ms": {k: main_res[k] for k in ("order_cp_ms", "cp_ms", "order_ray_ms", "ray_ms",
                                                       "wall_ms_per_step")},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,

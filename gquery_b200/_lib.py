@@ -22,6 +22,11 @@ GQ_ERR_UNSUPPORTED = 6
 VARIANT_EXACT = 0
 VARIANT_WIDE8 = 1
 VARIANT_AUTO = 2
+VARIANT_COHERENT = 3
+
+KIND_CLOSEST_POINT = 0
+KIND_INTERSECT = 1
+KIND_SILHOUETTE = 2
 
 ARRAY_BVH_NODES = 0
 ARRAY_PRIMITIVES = 1
@@ -63,6 +68,11 @@ class SilOut(C.Structure):
     _fields_ = [("valid", C.c_void_p), ("p", C.c_void_p), ("d", C.c_void_p), ("prim_id", C.c_void_p)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("variant", C.c_int32), ("packet", C.c_int32), ("sorted", C.c_int32), ("persist", C.c_int32),
+                ("budget", C.c_int32)]
+
+
 class QueryOpts(C.Structure):
     _fields_ = [("variant", C.c_int32), ("sort", C.c_int32), ("order", C.c_void_p), ("scratch", C.c_void_p),
                 ("scratch_bytes", C.c_int64)]
@@ -78,6 +88,8 @@ SIGNATURES = {
                                       C.POINTER(C.c_void_p)]),
     "gq_scene_free": (C.c_int32, [C.c_void_p]),
     "gq_scene_get_info": (C.c_int32, [C.c_void_p, C.POINTER(SceneInfo)]),
+    "gq_scene_set_tuning": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(Tuning)]),
+    "gq_scene_get_tuning": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(Tuning)]),
     "gq_scene_ref_array": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]),
     "gq_flat_silhouette_edges": (C.c_int32, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
                                              C.POINTER(C.c_int64)]),

@@ -1,6 +1,8 @@
 // C ABI of libgq.so (declared in include/gq.h).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -60,6 +62,7 @@ struct gq_scene {
     std::vector<void *> allocs;
     int64_t device_bytes = 0;
     gqd::DevScene dev{};
+    gq_tuning tune[3] = {};
 
     ~gq_scene() {
         if (device < 0 || allocs.empty()) return;
@@ -85,6 +88,8 @@ struct gq_scene {
 };
 
 namespace {
+
+void default_tuning(gq_scene *s);
 
 template <int D>
 gq_status build_scene(const float *vertices, int64_t nv, const int32_t *prims, int64_t np, const gq_build_opts *opts,
@@ -140,6 +145,7 @@ gq_status build_scene(const float *vertices, int64_t nv, const int32_t *prims, i
 
     s->exact_stack = img.exact_stack;
     s->wide_stack = img.wide_stack;
+    default_tuning(s.get());
     s->n_wide = (int64_t)img.wnodes.size();
     s->n_sil = (int64_t)img.sils.size();
     gqd::DevScene &d = s->dev;
@@ -160,6 +166,9 @@ gq_status build_scene(const float *vertices, int64_t nv, const int32_t *prims, i
     gq_status st;
     if ((st = s->upload(img.pairs, &d.pairs)) != GQ_OK) return st;
     if ((st = s->upload(img.prims, &d.prims)) != GQ_OK) return st;
+    const void *psph = nullptr;
+    if ((st = s->upload(img.spheres, &psph)) != GQ_OK) return st;
+    d.spheres = (const gq_tsph_t *)psph;
     if ((st = s->upload(img.wnodes, &d.wnodes)) != GQ_OK) return st;
     if ((st = s->upload(img.spairs, &d.spairs)) != GQ_OK) return st;
     if ((st = s->upload(img.sils, &d.sils)) != GQ_OK) return st;
@@ -172,6 +181,8 @@ gq_status build_scene(const float *vertices, int64_t nv, const int32_t *prims, i
     d.index = (const int32_t *)pi;
     d.err = (int32_t *)pe;
     d.n_prims = np;
+    d.coord_bound = 0.f;
+    for (float x : s->verts) d.coord_bound = std::max(d.coord_bound, std::fabs(x));
     d.root_ref = img.root_ref;
     d.wroot_ref = img.wroot_ref;
     d.sroot_ref = img.sroot_ref;
@@ -181,14 +192,41 @@ gq_status build_scene(const float *vertices, int64_t nv, const int32_t *prims, i
 
 bool on_host_only(const gq_scene *s) { return s->device < 0; }
 
-int resolve_variant(const gq_scene *s, const gq_query_opts *opts) {
+// Built-in launch choices (measured on B200 for the benchmark scenes).
+void default_tuning(gq_scene *s) {
+    for (int k = 0; k < 3; ++k) s->tune[k] = gq_tuning{GQ_VARIANT_EXACT, 0, 1, 0, 32};
+    if (s->dim == 3) {
+        s->tune[GQ_KIND_CLOSEST_POINT] = gq_tuning{GQ_VARIANT_COHERENT, 1, 1, 0, 32};
+        s->tune[GQ_KIND_INTERSECT] = gq_tuning{s->has_wide ? GQ_VARIANT_WIDE8 : GQ_VARIANT_EXACT, 0, 1, 1, 32};
+    } else {
+        s->tune[GQ_KIND_CLOSEST_POINT] = gq_tuning{s->has_wide ? GQ_VARIANT_WIDE8 : GQ_VARIANT_EXACT, 0, 1, 1, 32};
+        s->tune[GQ_KIND_INTERSECT] = gq_tuning{s->has_wide ? GQ_VARIANT_WIDE8 : GQ_VARIANT_EXACT, 0, 1, 1, 32};
+    }
+}
+
+gqd::Tune to_tune(const gq_tuning &t) {
+    gqd::Tune r;
+    r.packet = t.packet;
+    r.sorted = t.sorted;
+    r.persist = t.persist;
+    r.budget = t.budget > 0 ? t.budget : 32;
+    return r;
+}
+
+int resolve_variant(const gq_scene *s, const gq_query_opts *opts, int kind) {
     int v = opts ? opts->variant : GQ_VARIANT_AUTO;
-    if (v == GQ_VARIANT_AUTO) v = s->has_wide ? GQ_VARIANT_WIDE8 : GQ_VARIANT_EXACT;
+    if (v == GQ_VARIANT_AUTO) {
+        v = s->tune[kind].variant;
+        if (v == GQ_VARIANT_WIDE8 && !s->has_wide) v = GQ_VARIANT_EXACT;
+    }
     return v;
 }
 
 gq_status check_variant(const gq_scene *s, int v) {
-    if (v == GQ_VARIANT_WIDE8) {
+    if (v == GQ_VARIANT_COHERENT) {
+        if (s->exact_stack > GQ_STACK_EXACT)
+            return fail(GQ_ERR_DEPTH, "tree deeper than the 64-entry traversal stack");
+    } else if (v == GQ_VARIANT_WIDE8) {
         if (!s->has_wide) return fail(GQ_ERR_UNSUPPORTED, "scene was built without the wide BVH");
         if (s->wide_stack > GQ_STACK_WIDE) return fail(GQ_ERR_DEPTH, "wide tree needs a deeper stack than 96");
     } else if (v == GQ_VARIANT_EXACT) {
@@ -203,6 +241,7 @@ gq_status check_variant(const gq_scene *s, int v) {
 bool vecs_ok(const gq_vecs &v) { return v.ptr != nullptr; }
 
 size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+constexpr size_t kCounterBytes = 256;
 
 // Stream-ordered scratch for the Morton permutation (caller-provided or allocated).
 struct Scratch {
@@ -214,16 +253,16 @@ struct Scratch {
     }
 };
 
+// Per-call scratch: [work counter, 256 B][permutation, n int32][Morton sort workspace].
+// The counter feeds the persistent wide kernels; the rest is used when sorting.
+
 gq_status prepare_order(const gq_scene *s, gq_vecs keys_from, int64_t n, const gq_query_opts *opts,
-                        cudaStream_t st, Scratch &scr, const int32_t **perm) {
+                        cudaStream_t st, Scratch &scr, const int32_t **perm, unsigned long long **counter) {
     *perm = nullptr;
-    if (opts && opts->order) {
-        *perm = opts->order;
-        return GQ_OK;
-    }
-    if (!opts || !opts->sort || n < 2) return GQ_OK;
-    const size_t need = (size_t)gq_query_scratch_bytes(n);
-    if (opts->scratch) {
+    *counter = nullptr;
+    const bool sorting = opts && !opts->order && opts->sort && n >= 2;
+    const size_t need = sorting ? (size_t)gq_query_scratch_bytes(n) : kCounterBytes;
+    if (opts && opts->scratch) {
         if ((size_t)opts->scratch_bytes < need) return fail(GQ_ERR_INVALID, "scratch buffer too small");
         scr.p = opts->scratch;
     } else {
@@ -232,9 +271,15 @@ gq_status prepare_order(const gq_scene *s, gq_vecs keys_from, int64_t n, const g
         scr.owned = true;
         scr.st = st;
     }
-    int32_t *pp = (int32_t *)scr.p;
-    char *rest = (char *)scr.p + align256((size_t)n * 4);
-    cudaError_t e = gqd::morton_order(s->dev, keys_from, n, pp, rest, need - align256((size_t)n * 4), st);
+    *counter = (unsigned long long *)scr.p;
+    if (opts && opts->order) {
+        *perm = opts->order;
+        return GQ_OK;
+    }
+    if (!sorting) return GQ_OK;
+    int32_t *pp = (int32_t *)((char *)scr.p + kCounterBytes);
+    char *rest = (char *)pp + align256((size_t)n * 4);
+    cudaError_t e = gqd::morton_order(s->dev, keys_from, n, pp, rest, gqd::morton_scratch_bytes(n), st);
     if (e != cudaSuccess) return fail_cuda(e, "morton_order");
     *perm = pp;
     return GQ_OK;
@@ -274,6 +319,23 @@ gq_status gq_scene_build_3d(const float *vertices, int64_t nv, const int32_t *fa
 
 gq_status gq_scene_free(gq_scene *scene) {
     delete scene;
+    return GQ_OK;
+}
+
+gq_status gq_scene_set_tuning(gq_scene *s, int32_t kind, const gq_tuning *t) {
+    if (!s || !t) return fail(GQ_ERR_INVALID, "null argument");
+    if (kind < 0 || kind > 2) return fail(GQ_ERR_INVALID, "unknown query kind");
+    if (t->variant < 0 || t->variant > 3 || t->variant == GQ_VARIANT_AUTO)
+        return fail(GQ_ERR_INVALID, "tuning variant must be EXACT, WIDE8 or COHERENT");
+    if (t->variant == GQ_VARIANT_WIDE8 && !s->has_wide) return fail(GQ_ERR_UNSUPPORTED, "scene has no wide BVH");
+    s->tune[kind] = *t;
+    return GQ_OK;
+}
+
+gq_status gq_scene_get_tuning(const gq_scene *s, int32_t kind, gq_tuning *t) {
+    if (!s || !t) return fail(GQ_ERR_INVALID, "null argument");
+    if (kind < 0 || kind > 2) return fail(GQ_ERR_INVALID, "unknown query kind");
+    *t = s->tune[kind];
     return GQ_OK;
 }
 
@@ -352,7 +414,7 @@ gq_status gq_flat_silhouette_edges(const float *vertices, int64_t nv, const int3
 
 int64_t gq_query_scratch_bytes(int64_t n) {
     if (n <= 0) return 0;
-    return (int64_t)(align256((size_t)n * 4) + gqd::morton_scratch_bytes(n));
+    return (int64_t)(kCounterBytes + align256((size_t)n * 4) + gqd::morton_scratch_bytes(n));
 }
 
 int64_t gq_order_scratch_bytes(int64_t n) {
@@ -391,7 +453,7 @@ gq_status gq_closest_point(const gq_scene *s, gq_vecs q, int64_t n, const gq_cp_
     if (n < 0) return fail(GQ_ERR_INVALID, "negative query count");
     if (n == 0) return GQ_OK;
     if (!vecs_ok(q)) return fail(GQ_ERR_INVALID, "null query array");
-    const int v = resolve_variant(s, opts);
+    const int v = resolve_variant(s, opts, GQ_KIND_CLOSEST_POINT);
     gq_status st = check_variant(s, v);
     if (st != GQ_OK) return st;
     if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "scene was built without a device copy");
@@ -399,8 +461,9 @@ gq_status gq_closest_point(const gq_scene *s, gq_vecs q, int64_t n, const gq_cp_
     cudaStream_t cs = (cudaStream_t)stream;
     Scratch scr;
     const int32_t *perm = nullptr;
-    if ((st = prepare_order(s, q, n, opts, cs, scr, &perm)) != GQ_OK) return st;
-    cudaError_t e = gqd::launch_cp(s->dev, v, q, n, perm, *out, cs);
+    unsigned long long *counter = nullptr;
+    if ((st = prepare_order(s, q, n, opts, cs, scr, &perm, &counter)) != GQ_OK) return st;
+    cudaError_t e = gqd::launch_cp(s->dev, v, to_tune(s->tune[GQ_KIND_CLOSEST_POINT]), q, n, perm, *out, counter, cs);
     if (e != cudaSuccess) return fail_cuda(e, "closest_point launch");
     return GQ_OK;
 }
@@ -411,7 +474,7 @@ gq_status gq_intersect(const gq_scene *s, gq_vecs origin, gq_vecs dir, const flo
     if (n < 0) return fail(GQ_ERR_INVALID, "negative query count");
     if (n == 0) return GQ_OK;
     if (!vecs_ok(origin) || !vecs_ok(dir)) return fail(GQ_ERR_INVALID, "null ray array");
-    const int v = resolve_variant(s, opts);
+    const int v = resolve_variant(s, opts, GQ_KIND_INTERSECT);
     gq_status st = check_variant(s, v);
     if (st != GQ_OK) return st;
     if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "scene was built without a device copy");
@@ -419,8 +482,10 @@ gq_status gq_intersect(const gq_scene *s, gq_vecs origin, gq_vecs dir, const flo
     cudaStream_t cs = (cudaStream_t)stream;
     Scratch scr;
     const int32_t *perm = nullptr;
-    if ((st = prepare_order(s, origin, n, opts, cs, scr, &perm)) != GQ_OK) return st;
-    cudaError_t e = gqd::launch_ray(s->dev, v, origin, dir, r_max, n, perm, *out, cs);
+    unsigned long long *counter = nullptr;
+    if ((st = prepare_order(s, origin, n, opts, cs, scr, &perm, &counter)) != GQ_OK) return st;
+    cudaError_t e = gqd::launch_ray(s->dev, v, to_tune(s->tune[GQ_KIND_INTERSECT]), origin, dir, r_max, n, perm,
+                                    *out, counter, cs);
     if (e != cudaSuccess) return fail_cuda(e, "intersect launch");
     return GQ_OK;
 }
@@ -438,8 +503,9 @@ gq_status gq_closest_silhouette(const gq_scene *s, gq_vecs x, const float *r_max
     cudaStream_t cs = (cudaStream_t)stream;
     Scratch scr;
     const int32_t *perm = nullptr;
+    unsigned long long *counter = nullptr;
     gq_status st;
-    if ((st = prepare_order(s, x, n, opts, cs, scr, &perm)) != GQ_OK) return st;
+    if ((st = prepare_order(s, x, n, opts, cs, scr, &perm, &counter)) != GQ_OK) return st;
     cudaError_t e = gqd::launch_sil(s->dev, x, r_max, n, perm, *out, cs);
     if (e != cudaSuccess) return fail_cuda(e, "closest_silhouette launch");
     return GQ_OK;

@@ -1,10 +1,11 @@
-// Query kernels for sm_100a: binary "exact" traversals that follow gQuery's visit
-// order step for step, quantised 8-wide traversals, brute-force scans and the
-// Morton reordering of queries.  Compiled with --fmad=false (see gq_fmath.h).
+// Query kernels for sm_100a: the binary SNCH traversal (gQuery's visit order),
+// brute-force scans and the Morton reordering of queries.  Closest-point and ray
+// traversals live in traverse.cu.  Compiled with --fmad=false (see gq_fmath.h).
 #include <cub/cub.cuh>
 
 #include "prim.cuh"
 #include "queries.cuh"
+#include "records.cuh"
 
 namespace gqd {
 
@@ -20,710 +21,8 @@ __device__ __forceinline__ void flag_error(int32_t *err, int bits) {
     if (err) atomicOr(err, bits);
 }
 
-// Record writers (SoA, component stride n).  A miss writes zeros.
-__device__ __forceinline__ void put1(float *p, int64_t i, float v) {
-    if (p) p[i] = v;
-}
-__device__ __forceinline__ void put2(float *p, int64_t n, int64_t i, float a, float b) {
-    if (p) {
-        p[i] = a;
-        p[n + i] = b;
-    }
-}
-__device__ __forceinline__ void put3(float *p, int64_t n, int64_t i, float a, float b, float c) {
-    if (p) {
-        p[i] = a;
-        p[n + i] = b;
-        p[2 * n + i] = c;
-    }
-}
-
-// Batcher odd-even merge sort of 8 (key, ref) pairs, ascending keys.
-__device__ __forceinline__ void cas(float &ka, int &ra, float &kb, int &rb) {
-    const bool sw = kb < ka;
-    const float k0 = sw ? kb : ka, k1 = sw ? ka : kb;
-    const int r0 = sw ? rb : ra, r1 = sw ? ra : rb;
-    ka = k0; kb = k1; ra = r0; rb = r1;
-}
-__device__ __forceinline__ void sort8(float (&k)[8], int (&r)[8]) {
-    cas(k[0], r[0], k[1], r[1]); cas(k[2], r[2], k[3], r[3]); cas(k[4], r[4], k[5], r[5]); cas(k[6], r[6], k[7], r[7]);
-    cas(k[0], r[0], k[2], r[2]); cas(k[1], r[1], k[3], r[3]); cas(k[4], r[4], k[6], r[6]); cas(k[5], r[5], k[7], r[7]);
-    cas(k[1], r[1], k[2], r[2]); cas(k[5], r[5], k[6], r[6]);
-    cas(k[0], r[0], k[4], r[4]); cas(k[1], r[1], k[5], r[5]); cas(k[2], r[2], k[6], r[6]); cas(k[3], r[3], k[7], r[7]);
-    cas(k[2], r[2], k[4], r[4]); cas(k[3], r[3], k[5], r[5]);
-    cas(k[1], r[1], k[2], r[2]); cas(k[3], r[3], k[4], r[4]); cas(k[5], r[5], k[6], r[6]);
-}
-
-__device__ __forceinline__ float exp_scale(uint32_t meta, int ax) {
-    return __int_as_float((int)((meta >> (8 * ax)) & 0xffu) << 23);
-}
-__device__ __forceinline__ float qbyte(uint32_t lo4, uint32_t hi4, int k) {
-    const uint32_t w = (k < 4) ? lo4 : hi4;
-    return (float)((w >> (8 * (k & 3))) & 0xffu);
-}
-
 __device__ __forceinline__ int64_t query_index(const int32_t *perm, int64_t i) {
     return perm ? (int64_t)__ldg(perm + i) : i;
-}
-
-// ===========================================================================
-// Closest point, 3D
-// ===========================================================================
-
-__device__ __forceinline__ void cp3_leaf(const void *prims, int ref, float px, float py, float pz, float &r_max,
-                                         int &idx) {
-    int j = ~ref;
-    for (;;) {
-        const float4 t0 = ldg4(prims, 3 * (int64_t)j), t1 = ldg4(prims, 3 * (int64_t)j + 1),
-                     t2 = ldg4(prims, 3 * (int64_t)j + 2);
-        const float d =
-            tri_closest<false>(px, py, pz, t0.x, t0.y, t0.z, t0.w, t1.x, t1.y, t1.z, t1.w, t2.x);
-        if (d < r_max) {
-            r_max = d;
-            idx = j;
-        }
-        if (fbits(t2.z) & GQ_ITEM_LAST) break;
-        ++j;
-    }
-}
-
-// Triangle.closest_point (triangle.py:76-81)
-__device__ __forceinline__ void cp3_record(const void *prims, int idx, bool ok, float px, float py, float pz,
-                                           const gq_cp_out &o, int64_t n, int64_t qi) {
-    float pt[3] = {0.f, 0.f, 0.f}, nx = 0.f, ny = 0.f, nz = 0.f, u = 0.f, v = 0.f, d = 0.f;
-    int pid = 0;
-    if (ok) {
-        const float4 t0 = ldg4(prims, 3 * (int64_t)idx), t1 = ldg4(prims, 3 * (int64_t)idx + 1),
-                     t2 = ldg4(prims, 3 * (int64_t)idx + 2);
-        d = tri_closest<true>(px, py, pz, t0.x, t0.y, t0.z, t0.w, t1.x, t1.y, t1.z, t1.w, t2.x, pt, &u, &v);
-        float cx, cy, cz;
-        cross3(t0.w - t0.x, t1.x - t0.y, t1.y - t0.z, t1.z - t0.x, t1.w - t0.y, t2.x - t0.z, cx, cy, cz);
-        const float inv = gq_rsqrt(gq_dot3(cx, cy, cz, cx, cy, cz));
-        nx = cx * inv;
-        ny = cy * inv;
-        nz = cz * inv;
-        pid = fbits(t2.y);
-    }
-    if (o.valid) o.valid[qi] = ok ? 1 : 0;
-    put3(o.p, n, qi, pt[0], pt[1], pt[2]);
-    put3(o.n, n, qi, nx, ny, nz);
-    put2(o.t, n, qi, u, v);
-    put1(o.d, qi, d);
-    if (o.prim_id) o.prim_id[qi] = pid;
-}
-
-// BVH3D.closest_point (bvh3d.py:108-174), same pops, pushes and tests.
-__global__ void __launch_bounds__(kBlock) k_cp3_exact(DevScene s, gq_vecs q, int64_t n, const int32_t *perm,
-                                                       gq_cp_out o) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int64_t qi = query_index(perm, i);
-    const float px = qget(q, qi, 0), py = qget(q, qi, 1), pz = qget(q, qi, 2);
-    float r_max = kInf;
-    int idx = -1;
-    int2 stk[GQ_STACK_EXACT];
-    int sp = 0;
-    stk[0] = make_int2(s.root_ref, fbits(kInf));
-    bool ovf = false;
-    while (sp >= 0) {
-        const int2 e = stk[sp--];
-        if (!(__int_as_float(e.y) <= r_max)) continue;
-        if (e.x < 0) {
-            cp3_leaf(s.prims, e.x, px, py, pz, r_max, idx);
-            continue;
-        }
-        const float4 a = ldg4(s.pairs, 4 * (int64_t)e.x), b = ldg4(s.pairs, 4 * (int64_t)e.x + 1),
-                     c = ldg4(s.pairs, 4 * (int64_t)e.x + 2), r = ldg4(s.pairs, 4 * (int64_t)e.x + 3);
-        float dminl, dmaxl, dminr, dmaxr;
-        box_dist3(a.x, a.y, a.z, a.w, b.x, b.y, px, py, pz, dminl, dmaxl);
-        const bool hl = dminl <= r_max;
-        r_max = fminf(r_max, dmaxl);
-        box_dist3(b.z, b.w, c.x, c.y, c.z, c.w, px, py, pz, dminr, dmaxr);
-        const bool hr = dminr <= r_max;
-        r_max = fminf(r_max, dmaxr);
-        const int rl = fbits(r.x), rr = fbits(r.y);
-        if (hl & hr) {
-            if (sp + 2 >= GQ_STACK_EXACT) {
-                ovf = true;
-                break;
-            }
-            const bool sw = dminr < dminl;
-            stk[++sp] = sw ? make_int2(rl, fbits(dminl)) : make_int2(rr, fbits(dminr));
-            stk[++sp] = sw ? make_int2(rr, fbits(dminr)) : make_int2(rl, fbits(dminl));
-        } else if (hl) {
-            stk[++sp] = make_int2(rl, fbits(dminl));
-        } else if (hr) {
-            stk[++sp] = make_int2(rr, fbits(dminr));
-        }
-    }
-    if (ovf) flag_error(s.err, GQ_DEVERR_STACK);
-    cp3_record(s.prims, idx, (idx >= 0) && !ovf, px, py, pz, o, n, qi);
-}
-
-// Quantised 8-wide closest point, 3D.  All children of a node are tested at once:
-// r_max shrinks to the smallest child d_max (the farthest-corner bound of
-// bvh3d.py:141-144), children with d_min <= r_max are pushed nearest-last.
-__global__ void __launch_bounds__(kBlock) k_cp3_wide(DevScene s, gq_vecs q, int64_t n, const int32_t *perm,
-                                                      gq_cp_out o) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int64_t qi = query_index(perm, i);
-    const float px = qget(q, qi, 0), py = qget(q, qi, 1), pz = qget(q, qi, 2);
-    float r_max = kInf;
-    int idx = -1;
-    int2 stk[GQ_STACK_WIDE];
-    int sp = 0;
-    stk[0] = make_int2(s.wroot_ref, fbits(kInf));
-    bool ovf = false;
-    while (sp >= 0) {
-        const int2 e = stk[sp--];
-        if (!(__int_as_float(e.y) <= r_max)) continue;
-        if (e.x < 0) {
-            cp3_leaf(s.prims, e.x, px, py, pz, r_max, idx);
-            continue;
-        }
-        const int64_t base = 6 * (int64_t)e.x;
-        const float4 h = ldg4(s.wnodes, base);
-        const int4 r0 = __ldg(reinterpret_cast<const int4 *>(s.wnodes) + base + 1);
-        const int4 r1 = __ldg(reinterpret_cast<const int4 *>(s.wnodes) + base + 2);
-        const uint4 q0 = __ldg(reinterpret_cast<const uint4 *>(s.wnodes) + base + 3);
-        const uint4 q1 = __ldg(reinterpret_cast<const uint4 *>(s.wnodes) + base + 4);
-        const uint4 q2 = __ldg(reinterpret_cast<const uint4 *>(s.wnodes) + base + 5);
-        const uint32_t meta = (uint32_t)fbits(h.w);
-        const int nc = (int)(meta >> 24);
-        const float sx = exp_scale(meta, 0), sy = exp_scale(meta, 1), sz = exp_scale(meta, 2);
-        float key[8], dmx[8];
-        int ref[8] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
-        float shrink = kInf;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const float lox = __fmaf_rn(qbyte(q0.x, q0.y, k), sx, h.x);
-            const float loy = __fmaf_rn(qbyte(q0.z, q0.w, k), sy, h.y);
-            const float loz = __fmaf_rn(qbyte(q1.x, q1.y, k), sz, h.z);
-            const float hix = __fmaf_rn(qbyte(q1.z, q1.w, k), sx, h.x);
-            const float hiy = __fmaf_rn(qbyte(q2.x, q2.y, k), sy, h.y);
-            const float hiz = __fmaf_rn(qbyte(q2.z, q2.w, k), sz, h.z);
-            box_dist3(lox, loy, loz, hix, hiy, hiz, px, py, pz, key[k], dmx[k]);
-            if (k < nc) shrink = fminf(shrink, dmx[k]);
-        }
-        r_max = fminf(r_max, shrink);
-        int cnt = 0;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const bool hit = (k < nc) && (key[k] <= r_max);
-            key[k] = hit ? key[k] : kInf;
-            cnt += hit ? 1 : 0;
-        }
-        if (sp + cnt >= GQ_STACK_WIDE) {
-            ovf = true;
-            break;
-        }
-        sort8(key, ref);
-#pragma unroll
-        for (int k = 7; k >= 0; --k)
-            if (k < cnt) stk[++sp] = make_int2(ref[k], fbits(key[k]));
-    }
-    if (ovf) flag_error(s.err, GQ_DEVERR_STACK);
-    cp3_record(s.prims, idx, (idx >= 0) && !ovf, px, py, pz, o, n, qi);
-}
-
-// ===========================================================================
-// Closest point, 2D
-// ===========================================================================
-
-__device__ __forceinline__ void cp2_leaf(const void *prims, int ref, float px, float py, float &r_max, int &idx) {
-    int j = ~ref;
-    for (;;) {
-        const float4 a = ldg4(prims, 2 * (int64_t)j);
-        const int4 f = __ldg(reinterpret_cast<const int4 *>(prims) + 2 * (int64_t)j + 1);
-        const float d = seg_dist(px, py, a.x, a.y, a.z, a.w);
-        if (d < r_max) {
-            r_max = d;
-            idx = j;
-        }
-        if (f.y & GQ_ITEM_LAST) break;
-        ++j;
-    }
-}
-
-// LineSegment.closest_point (line_segment.py:64-78)
-__device__ __forceinline__ void cp2_record(const void *prims, int idx, bool ok, float px, float py,
-                                           const gq_cp_out &o, int64_t n, int64_t qi) {
-    float ix = 0.f, iy = 0.f, nx = 0.f, ny = 0.f, h = 0.f, d = 0.f;
-    int pid = 0;
-    if (ok) {
-        const float4 a = ldg4(prims, 2 * (int64_t)idx);
-        const int4 f = __ldg(reinterpret_cast<const int4 *>(prims) + 2 * (int64_t)idx + 1);
-        const float pax = px - a.x, pay = py - a.y, bax = a.z - a.x, bay = a.w - a.y;
-        const float inv = gq_rsqrt(gq_dot2(bax, bay, bax, bay));
-        const float tx = bax * inv, ty = bay * inv;
-        nx = ty;
-        ny = -tx;
-        h = gq_clamp(gq_div(gq_dot2(pax, pay, bax, bay), gq_dot2(bax, bay, bax, bay)), 0.f, 1.f);
-        ix = a.x + bax * h;
-        iy = a.y + bay * h;
-        d = gq_norm2(ix - px, iy - py);
-        pid = f.x;
-    }
-    if (o.valid) o.valid[qi] = ok ? 1 : 0;
-    put2(o.p, n, qi, ix, iy);
-    put2(o.n, n, qi, nx, ny);
-    put1(o.t, qi, h);
-    put1(o.d, qi, d);
-    if (o.prim_id) o.prim_id[qi] = pid;
-}
-
-// BVH.closest_point (bvh.py:127-198)
-__global__ void __launch_bounds__(kBlock) k_cp2_exact(DevScene s, gq_vecs q, int64_t n, const int32_t *perm,
-                                                       gq_cp_out o) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int64_t qi = query_index(perm, i);
-    const float px = qget(q, qi, 0), py = qget(q, qi, 1);
-    float r_max = kInf;
-    int idx = -1;
-    int2 stk[GQ_STACK_EXACT];
-    int sp = 0;
-    stk[0] = make_int2(s.root_ref, fbits(kInf));
-    bool ovf = false;
-    while (sp >= 0) {
-        const int2 e = stk[sp--];
-        if (!(__int_as_float(e.y) <= r_max)) continue;
-        if (e.x < 0) {
-            cp2_leaf(s.prims, e.x, px, py, r_max, idx);
-            continue;
-        }
-        const float4 a = ldg4(s.pairs, 3 * (int64_t)e.x), b = ldg4(s.pairs, 3 * (int64_t)e.x + 1);
-        const int4 r = __ldg(reinterpret_cast<const int4 *>(s.pairs) + 3 * (int64_t)e.x + 2);
-        float dminl, dmaxl, dminr, dmaxr;
-        box_dist2(a.x, a.y, a.z, a.w, px, py, dminl, dmaxl);
-        const bool hl = dminl <= r_max;
-        r_max = fminf(r_max, dmaxl);
-        box_dist2(b.x, b.y, b.z, b.w, px, py, dminr, dmaxr);
-        const bool hr = dminr <= r_max;
-        r_max = fminf(r_max, dmaxr);
-        if (hl & hr) {
-            if (sp + 2 >= GQ_STACK_EXACT) {
-                ovf = true;
-                break;
-            }
-            const bool sw = dminr < dminl;
-            stk[++sp] = sw ? make_int2(r.x, fbits(dminl)) : make_int2(r.y, fbits(dminr));
-            stk[++sp] = sw ? make_int2(r.y, fbits(dminr)) : make_int2(r.x, fbits(dminl));
-        } else if (hl) {
-            stk[++sp] = make_int2(r.x, fbits(dminl));
-        } else if (hr) {
-            stk[++sp] = make_int2(r.y, fbits(dminr));
-        }
-    }
-    if (ovf) flag_error(s.err, GQ_DEVERR_STACK);
-    cp2_record(s.prims, idx, (idx != -1) && !ovf, px, py, o, n, qi);
-}
-
-__global__ void __launch_bounds__(kBlock) k_cp2_wide(DevScene s, gq_vecs q, int64_t n, const int32_t *perm,
-                                                      gq_cp_out o) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int64_t qi = query_index(perm, i);
-    const float px = qget(q, qi, 0), py = qget(q, qi, 1);
-    float r_max = kInf;
-    int idx = -1;
-    int2 stk[GQ_STACK_WIDE];
-    int sp = 0;
-    stk[0] = make_int2(s.wroot_ref, fbits(kInf));
-    bool ovf = false;
-    while (sp >= 0) {
-        const int2 e = stk[sp--];
-        if (!(__int_as_float(e.y) <= r_max)) continue;
-        if (e.x < 0) {
-            cp2_leaf(s.prims, e.x, px, py, r_max, idx);
-            continue;
-        }
-        const int64_t base = 5 * (int64_t)e.x;
-        const float4 h = ldg4(s.wnodes, base);
-        const int4 r0 = __ldg(reinterpret_cast<const int4 *>(s.wnodes) + base + 1);
-        const int4 r1 = __ldg(reinterpret_cast<const int4 *>(s.wnodes) + base + 2);
-        const uint4 q0 = __ldg(reinterpret_cast<const uint4 *>(s.wnodes) + base + 3);
-        const uint4 q1 = __ldg(reinterpret_cast<const uint4 *>(s.wnodes) + base + 4);
-        const uint32_t meta = (uint32_t)fbits(h.z);
-        const int nc = (int)(meta >> 24);
-        const float sx = exp_scale(meta, 0), sy = exp_scale(meta, 1);
-        float key[8], dmx[8];
-        int ref[8] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
-        float shrink = kInf;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const float lox = __fmaf_rn(qbyte(q0.x, q0.y, k), sx, h.x);
-            const float loy = __fmaf_rn(qbyte(q0.z, q0.w, k), sy, h.y);
-            const float hix = __fmaf_rn(qbyte(q1.x, q1.y, k), sx, h.x);
-            const float hiy = __fmaf_rn(qbyte(q1.z, q1.w, k), sy, h.y);
-            box_dist2(lox, loy, hix, hiy, px, py, key[k], dmx[k]);
-            if (k < nc) shrink = fminf(shrink, dmx[k]);
-        }
-        r_max = fminf(r_max, shrink);
-        int cnt = 0;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const bool hit = (k < nc) && (key[k] <= r_max);
-            key[k] = hit ? key[k] : kInf;
-            cnt += hit ? 1 : 0;
-        }
-        if (sp + cnt >= GQ_STACK_WIDE) {
-            ovf = true;
-            break;
-        }
-        sort8(key, ref);
-#pragma unroll
-        for (int k = 7; k >= 0; --k)
-            if (k < cnt) stk[++sp] = make_int2(ref[k], fbits(key[k]));
-    }
-    if (ovf) flag_error(s.err, GQ_DEVERR_STACK);
-    cp2_record(s.prims, idx, (idx != -1) && !ovf, px, py, o, n, qi);
-}
-
-// ===========================================================================
-// Ray intersection, 3D
-// ===========================================================================
-
-__device__ __forceinline__ void ray3_leaf(const void *prims, int ref, float xx, float xy, float xz, float vx,
-                                          float vy, float vz, float &r_max, int &idx) {
-    int j = ~ref;
-    for (;;) {
-        const float4 t0 = ldg4(prims, 3 * (int64_t)j), t1 = ldg4(prims, 3 * (int64_t)j + 1),
-                     t2 = ldg4(prims, 3 * (int64_t)j + 2);
-        const float d = tri_ray(xx, xy, xz, vx, vy, vz, t0.x, t0.y, t0.z, t0.w, t1.x, t1.y, t1.z, t1.w, t2.x, kInf);
-        if (d < r_max) {
-            r_max = d;
-            idx = j;
-        }
-        if (fbits(t2.z) & GQ_ITEM_LAST) break;
-        ++j;
-    }
-}
-
-// Triangle.ray_intersect (triangle.py:49-73) re-run on the winner with r_max = its t.
-__device__ __forceinline__ void ray3_record(const void *prims, int idx, bool found, float xx, float xy, float xz,
-                                            float vx, float vy, float vz, float r_max, const gq_ray_out &o,
-                                            int64_t n, int64_t qi) {
-    float px = 0.f, py = 0.f, pz = 0.f, nx = 0.f, ny = 0.f, nz = 0.f, u = 0.f, w0 = 0.f, d = 0.f;
-    int pid = 0;
-    bool ok = false;
-    if (found) {
-        const float4 t0 = ldg4(prims, 3 * (int64_t)idx), t1 = ldg4(prims, 3 * (int64_t)idx + 1),
-                     t2 = ldg4(prims, 3 * (int64_t)idx + 2);
-        float vv = __builtin_nanf(""), ww = 0.f;
-        const float t = tri_ray(xx, xy, xz, vx, vy, vz, t0.x, t0.y, t0.z, t0.w, t1.x, t1.y, t1.z, t1.w, t2.x, r_max,
-                                &vv, &ww);
-        ok = (vv == vv);
-        if (ok) {
-            const float v1x = t0.w - t0.x, v1y = t1.x - t0.y, v1z = t1.y - t0.z;
-            const float v2x = t1.z - t0.x, v2y = t1.w - t0.y, v2z = t2.x - t0.z;
-            px = (t0.x + v1x * vv) + v2x * ww;
-            py = (t0.y + v1y * vv) + v2y * ww;
-            pz = (t0.z + v1z * vv) + v2z * ww;
-            float cx, cy, cz;
-            cross3(v1x, v1y, v1z, v2x, v2y, v2z, cx, cy, cz);
-            const float inv = gq_rsqrt(gq_dot3(cx, cy, cz, cx, cy, cz));
-            nx = cx * inv;
-            ny = cy * inv;
-            nz = cz * inv;
-            u = 1.f - vv - ww;
-            w0 = vv;
-            d = t;
-            pid = fbits(t2.y);
-        }
-    }
-    if (o.valid) o.valid[qi] = ok ? 1 : 0;
-    put3(o.p, n, qi, px, py, pz);
-    put3(o.n, n, qi, nx, ny, nz);
-    put2(o.t, n, qi, u, w0);
-    put1(o.d, qi, d);
-    if (o.prim_id) o.prim_id[qi] = pid;
-    if (o.on_boundary) o.on_boundary[qi] = ok ? 1 : 0;
-}
-
-// BVH3D.intersect (bvh3d.py:176-239)
-__global__ void __launch_bounds__(kBlock) k_ray3_exact(DevScene s, gq_vecs x, gq_vecs v, const float *rmax_in,
-                                                        int64_t n, const int32_t *perm, gq_ray_out o) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int64_t qi = query_index(perm, i);
-    const float xx = qget(x, qi, 0), xy = qget(x, qi, 1), xz = qget(x, qi, 2);
-    const float vx = qget(v, qi, 0), vy = qget(v, qi, 1), vz = qget(v, qi, 2);
-    float r_max = rmax_in ? rmax_in[qi] : kInf;
-    int idx = -1;
-    bool ovf = false;
-    float t_root;
-    if (box_ray3(s.root_lo[0], s.root_lo[1], s.root_lo[2], s.root_hi[0], s.root_hi[1], s.root_hi[2], xx, xy, xz, vx,
-                 vy, vz, r_max, t_root)) {
-        int2 stk[GQ_STACK_EXACT];
-        int sp = 0;
-        stk[0] = make_int2(s.root_ref, fbits(t_root));
-        while (sp >= 0) {
-            const int2 e = stk[sp--];
-            if (!(__int_as_float(e.y) <= r_max)) continue;
-            if (e.x < 0) {
-                ray3_leaf(s.prims, e.x, xx, xy, xz, vx, vy, vz, r_max, idx);
-                continue;
-            }
-            const float4 a = ldg4(s.pairs, 4 * (int64_t)e.x), b = ldg4(s.pairs, 4 * (int64_t)e.x + 1),
-                         c = ldg4(s.pairs, 4 * (int64_t)e.x + 2), r = ldg4(s.pairs, 4 * (int64_t)e.x + 3);
-            float t0, t1;
-            const bool h0 = box_ray3(a.x, a.y, a.z, a.w, b.x, b.y, xx, xy, xz, vx, vy, vz, r_max, t0);
-            const bool h1 = box_ray3(b.z, b.w, c.x, c.y, c.z, c.w, xx, xy, xz, vx, vy, vz, r_max, t1);
-            const int rl = fbits(r.x), rr = fbits(r.y);
-            if (h0 & h1) {
-                if (sp + 2 >= GQ_STACK_EXACT) {
-                    ovf = true;
-                    break;
-                }
-                const bool sw = t1 < t0;
-                stk[++sp] = sw ? make_int2(rl, fbits(t0)) : make_int2(rr, fbits(t1));
-                stk[++sp] = sw ? make_int2(rr, fbits(t1)) : make_int2(rl, fbits(t0));
-            } else if (h0) {
-                stk[++sp] = make_int2(rl, fbits(t0));
-            } else if (h1) {
-                stk[++sp] = make_int2(rr, fbits(t1));
-            }
-        }
-    }
-    if (ovf) flag_error(s.err, GQ_DEVERR_STACK);
-    ray3_record(s.prims, idx, (idx >= 0) && !ovf, xx, xy, xz, vx, vy, vz, r_max, o, n, qi);
-}
-
-// Quantised 8-wide ray traversal, 3D.  Slab tests use the reciprocal direction and
-// a far distance widened by 2^-21 so that rounding never drops a child the exact
-// test would enter.
-__global__ void __launch_bounds__(kBlock) k_ray3_wide(DevScene s, gq_vecs x, gq_vecs v, const float *rmax_in,
-                                                       int64_t n, const int32_t *perm, gq_ray_out o) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int64_t qi = query_index(perm, i);
-    const float xx = qget(x, qi, 0), xy = qget(x, qi, 1), xz = qget(x, qi, 2);
-    const float vx = qget(v, qi, 0), vy = qget(v, qi, 1), vz = qget(v, qi, 2);
-    const float ix = gq_div(1.f, vx), iy = gq_div(1.f, vy), iz = gq_div(1.f, vz);
-    float r_max = rmax_in ? rmax_in[qi] : kInf;
-    int idx = -1;
-    bool ovf = false;
-    float t_root;
-    if (box_ray3(s.root_lo[0], s.root_lo[1], s.root_lo[2], s.root_hi[0], s.root_hi[1], s.root_hi[2], xx, xy, xz, vx,
-                 vy, vz, r_max, t_root)) {
-        int2 stk[GQ_STACK_WIDE];
-        int sp = 0;
-        stk[0] = make_int2(s.wroot_ref, fbits(t_root));
-        while (sp >= 0) {
-            const int2 e = stk[sp--];
-            if (!(__int_as_float(e.y) <= r_max)) continue;
-            if (e.x < 0) {
-                ray3_leaf(s.prims, e.x, xx, xy, xz, vx, vy, vz, r_max, idx);
-                continue;
-            }
-            const int64_t base = 6 * (int64_t)e.x;
-            const float4 h = ldg4(s.wnodes, base);
-            const int4 r0 = __ldg(reinterpret_cast<const int4 *>(s.wnodes) + base + 1);
-            const int4 r1 = __ldg(reinterpret_cast<const int4 *>(s.wnodes) + base + 2);
-            const uint4 q0 = __ldg(reinterpret_cast<const uint4 *>(s.wnodes) + base + 3);
-            const uint4 q1 = __ldg(reinterpret_cast<const uint4 *>(s.wnodes) + base + 4);
-            const uint4 q2 = __ldg(reinterpret_cast<const uint4 *>(s.wnodes) + base + 5);
-            const uint32_t meta = (uint32_t)fbits(h.w);
-            const int nc = (int)(meta >> 24);
-            const float sx = exp_scale(meta, 0), sy = exp_scale(meta, 1), sz = exp_scale(meta, 2);
-            const float far_lim = r_max * 1.000000477f;
-            float key[8];
-            int ref[8] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
-            int cnt = 0;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const float lox = __fmaf_rn(qbyte(q0.x, q0.y, k), sx, h.x);
-                const float loy = __fmaf_rn(qbyte(q0.z, q0.w, k), sy, h.y);
-                const float loz = __fmaf_rn(qbyte(q1.x, q1.y, k), sz, h.z);
-                const float hix = __fmaf_rn(qbyte(q1.z, q1.w, k), sx, h.x);
-                const float hiy = __fmaf_rn(qbyte(q2.x, q2.y, k), sy, h.y);
-                const float hiz = __fmaf_rn(qbyte(q2.z, q2.w, k), sz, h.z);
-                const float t0x = (lox - xx) * ix, t1x = (hix - xx) * ix;
-                const float t0y = (loy - xy) * iy, t1y = (hiy - xy) * iy;
-                const float t0z = (loz - xz) * iz, t1z = (hiz - xz) * iz;
-                const float tn = fmaxf(fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fminf(t0z, t1z)), 0.f);
-                const float tf =
-                    fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fmaxf(t0z, t1z)) * 1.000000477f;
-                const bool hit = (k < nc) && (tn <= fminf(tf, far_lim));
-                key[k] = hit ? tn : kInf;
-                cnt += hit ? 1 : 0;
-            }
-            if (sp + cnt >= GQ_STACK_WIDE) {
-                ovf = true;
-                break;
-            }
-            sort8(key, ref);
-#pragma unroll
-            for (int k = 7; k >= 0; --k)
-                if (k < cnt) stk[++sp] = make_int2(ref[k], fbits(key[k]));
-        }
-    }
-    if (ovf) flag_error(s.err, GQ_DEVERR_STACK);
-    ray3_record(s.prims, idx, (idx >= 0) && !ovf, xx, xy, xz, vx, vy, vz, r_max, o, n, qi);
-}
-
-// ===========================================================================
-// Ray intersection, 2D
-// ===========================================================================
-
-__device__ __forceinline__ void ray2_leaf(const void *prims, int ref, float xx, float xy, float vx, float vy,
-                                          float &d_min, int &idx) {
-    int j = ~ref;
-    for (;;) {
-        const float4 a = ldg4(prims, 2 * (int64_t)j);
-        const int4 f = __ldg(reinterpret_cast<const int4 *>(prims) + 2 * (int64_t)j + 1);
-        const float d = seg_ray(xx, xy, vx, vy, a.x, a.y, a.z, a.w);
-        if (d < d_min) {
-            d_min = d;
-            idx = j;
-        }
-        if (f.y & GQ_ITEM_LAST) break;
-        ++j;
-    }
-}
-
-// bvh.py:267-274
-__device__ __forceinline__ void ray2_record(const void *prims, int idx, bool hit, float xx, float xy, float vx,
-                                            float vy, float d_min, const gq_ray_out &o, int64_t n, int64_t qi) {
-    float px = 0.f, py = 0.f, nx = 0.f, ny = 0.f, t = 0.f, d = 0.f;
-    int pid = 0;
-    if (hit) {
-        const float4 a = ldg4(prims, 2 * (int64_t)idx);
-        const int4 f = __ldg(reinterpret_cast<const int4 *>(prims) + 2 * (int64_t)idx + 1);
-        px = xx + vx * d_min;
-        py = xy + vy * d_min;
-        const float tx = a.z - a.x, ty = a.w - a.y;  // LineSegment.normal (line_segment.py:14-16)
-        const float inv = gq_rsqrt(gq_dot2(ty, -tx, ty, -tx));
-        nx = ty * inv;
-        ny = -tx * inv;
-        t = -1.f;
-        d = d_min;
-        pid = f.x;
-    }
-    if (o.valid) o.valid[qi] = hit ? 1 : 0;
-    put2(o.p, n, qi, px, py);
-    put2(o.n, n, qi, nx, ny);
-    put1(o.t, qi, t);
-    put1(o.d, qi, d);
-    if (o.prim_id) o.prim_id[qi] = pid;
-    if (o.on_boundary) o.on_boundary[qi] = hit ? 1 : 0;
-}
-
-// BVH.intersect (bvh.py:200-276): r_max never shrinks; the best hit is tracked in d_min.
-__global__ void __launch_bounds__(kBlock) k_ray2_exact(DevScene s, gq_vecs x, gq_vecs v, const float *rmax_in,
-                                                        int64_t n, const int32_t *perm, gq_ray_out o) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int64_t qi = query_index(perm, i);
-    const float xx = qget(x, qi, 0), xy = qget(x, qi, 1);
-    const float vx = qget(v, qi, 0), vy = qget(v, qi, 1);
-    const float r_max = rmax_in ? rmax_in[qi] : kInf;
-    float d_min = r_max;
-    int idx = -1;
-    bool ovf = false;
-    float t_root;
-    if (box_ray2(s.root_lo[0], s.root_lo[1], s.root_hi[0], s.root_hi[1], xx, xy, vx, vy, r_max, t_root)) {
-        int2 stk[GQ_STACK_EXACT];
-        int sp = 0;
-        stk[0] = make_int2(s.root_ref, fbits(t_root));
-        while (sp >= 0) {
-            const int2 e = stk[sp--];
-            if (!(__int_as_float(e.y) <= r_max)) continue;
-            if (e.x < 0) {
-                ray2_leaf(s.prims, e.x, xx, xy, vx, vy, d_min, idx);
-                continue;
-            }
-            const float4 a = ldg4(s.pairs, 3 * (int64_t)e.x), b = ldg4(s.pairs, 3 * (int64_t)e.x + 1);
-            const int4 r = __ldg(reinterpret_cast<const int4 *>(s.pairs) + 3 * (int64_t)e.x + 2);
-            float t0, t1;
-            const bool h0 = box_ray2(a.x, a.y, a.z, a.w, xx, xy, vx, vy, r_max, t0);
-            const bool h1 = box_ray2(b.x, b.y, b.z, b.w, xx, xy, vx, vy, r_max, t1);
-            if (h0 & h1) {
-                if (sp + 2 >= GQ_STACK_EXACT) {
-                    ovf = true;
-                    break;
-                }
-                const bool sw = t1 < t0;
-                stk[++sp] = sw ? make_int2(r.x, fbits(t0)) : make_int2(r.y, fbits(t1));
-                stk[++sp] = sw ? make_int2(r.y, fbits(t1)) : make_int2(r.x, fbits(t0));
-            } else if (h0) {
-                stk[++sp] = make_int2(r.x, fbits(t0));
-            } else if (h1) {
-                stk[++sp] = make_int2(r.y, fbits(t1));
-            }
-        }
-    }
-    if (ovf) flag_error(s.err, GQ_DEVERR_STACK);
-    ray2_record(s.prims, idx, (idx >= 0) && !ovf, xx, xy, vx, vy, d_min, o, n, qi);
-}
-
-// Quantised 8-wide 2D rays.  Nodes farther than the best hit so far are skipped:
-// a hit there would need a strictly smaller parameter than one already found.
-__global__ void __launch_bounds__(kBlock) k_ray2_wide(DevScene s, gq_vecs x, gq_vecs v, const float *rmax_in,
-                                                       int64_t n, const int32_t *perm, gq_ray_out o) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int64_t qi = query_index(perm, i);
-    const float xx = qget(x, qi, 0), xy = qget(x, qi, 1);
-    const float vx = qget(v, qi, 0), vy = qget(v, qi, 1);
-    const float ix = gq_div(1.f, vx), iy = gq_div(1.f, vy);
-    const float r_max = rmax_in ? rmax_in[qi] : kInf;
-    float d_min = r_max;
-    int idx = -1;
-    bool ovf = false;
-    float t_root;
-    if (box_ray2(s.root_lo[0], s.root_lo[1], s.root_hi[0], s.root_hi[1], xx, xy, vx, vy, r_max, t_root)) {
-        int2 stk[GQ_STACK_WIDE];
-        int sp = 0;
-        stk[0] = make_int2(s.wroot_ref, fbits(t_root));
-        while (sp >= 0) {
-            const int2 e = stk[sp--];
-            if (!(__int_as_float(e.y) <= d_min)) continue;
-            if (e.x < 0) {
-                ray2_leaf(s.prims, e.x, xx, xy, vx, vy, d_min, idx);
-                continue;
-            }
-            const int64_t base = 5 * (int64_t)e.x;
-            const float4 h = ldg4(s.wnodes, base);
-            const int4 r0 = __ldg(reinterpret_cast<const int4 *>(s.wnodes) + base + 1);
-            const int4 r1 = __ldg(reinterpret_cast<const int4 *>(s.wnodes) + base + 2);
-            const uint4 q0 = __ldg(reinterpret_cast<const uint4 *>(s.wnodes) + base + 3);
-            const uint4 q1 = __ldg(reinterpret_cast<const uint4 *>(s.wnodes) + base + 4);
-            const uint32_t meta = (uint32_t)fbits(h.z);
-            const int nc = (int)(meta >> 24);
-            const float sx = exp_scale(meta, 0), sy = exp_scale(meta, 1);
-            const float far_lim = d_min * 1.000000477f;
-            float key[8];
-            int ref[8] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
-            int cnt = 0;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const float lox = __fmaf_rn(qbyte(q0.x, q0.y, k), sx, h.x);
-                const float loy = __fmaf_rn(qbyte(q0.z, q0.w, k), sy, h.y);
-                const float hix = __fmaf_rn(qbyte(q1.x, q1.y, k), sx, h.x);
-                const float hiy = __fmaf_rn(qbyte(q1.z, q1.w, k), sy, h.y);
-                const float t0x = (lox - xx) * ix, t1x = (hix - xx) * ix;
-                const float t0y = (loy - xy) * iy, t1y = (hiy - xy) * iy;
-                const float tn = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), 0.f);
-                const float tf = fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)) * 1.000000477f;
-                const bool hit = (k < nc) && (tn <= fminf(tf, far_lim));
-                key[k] = hit ? tn : kInf;
-                cnt += hit ? 1 : 0;
-            }
-            if (sp + cnt >= GQ_STACK_WIDE) {
-                ovf = true;
-                break;
-            }
-            sort8(key, ref);
-#pragma unroll
-            for (int k = 7; k >= 0; --k)
-                if (k < cnt) stk[++sp] = make_int2(ref[k], fbits(key[k]));
-        }
-    }
-    if (ovf) flag_error(s.err, GQ_DEVERR_STACK);
-    ray2_record(s.prims, idx, (idx >= 0) && !ovf, xx, xy, vx, vy, d_min, o, n, qi);
 }
 
 // ===========================================================================
@@ -1287,42 +586,6 @@ cudaError_t morton_order(const DevScene &s, gq_vecs q, int64_t n, int32_t *perm,
     if (e != cudaSuccess) return e;
     const int end_bit = s.dim == 3 ? 30 : 30;
     return cub::DeviceRadixSort::SortPairs(p, tb, k_in, k_out, v_in, perm, (int)n, 0, end_bit, st);
-}
-
-cudaError_t launch_cp(const DevScene &s, int variant, gq_vecs q, int64_t n, const int32_t *perm, const gq_cp_out &o,
-                      cudaStream_t st) {
-    if (n <= 0) return cudaSuccess;
-    const bool wide = variant == GQ_VARIANT_WIDE8;
-    if (s.dim == 3) {
-        if (wide)
-            k_cp3_wide<<<grid_for(n), kBlock, 0, st>>>(s, q, n, perm, o);
-        else
-            k_cp3_exact<<<grid_for(n), kBlock, 0, st>>>(s, q, n, perm, o);
-    } else {
-        if (wide)
-            k_cp2_wide<<<grid_for(n), kBlock, 0, st>>>(s, q, n, perm, o);
-        else
-            k_cp2_exact<<<grid_for(n), kBlock, 0, st>>>(s, q, n, perm, o);
-    }
-    return cudaGetLastError();
-}
-
-cudaError_t launch_ray(const DevScene &s, int variant, gq_vecs x, gq_vecs v, const float *r_max, int64_t n,
-                       const int32_t *perm, const gq_ray_out &o, cudaStream_t st) {
-    if (n <= 0) return cudaSuccess;
-    const bool wide = variant == GQ_VARIANT_WIDE8;
-    if (s.dim == 3) {
-        if (wide)
-            k_ray3_wide<<<grid_for(n), kBlock, 0, st>>>(s, x, v, r_max, n, perm, o);
-        else
-            k_ray3_exact<<<grid_for(n), kBlock, 0, st>>>(s, x, v, r_max, n, perm, o);
-    } else {
-        if (wide)
-            k_ray2_wide<<<grid_for(n), kBlock, 0, st>>>(s, x, v, r_max, n, perm, o);
-        else
-            k_ray2_exact<<<grid_for(n), kBlock, 0, st>>>(s, x, v, r_max, n, perm, o);
-    }
-    return cudaGetLastError();
 }
 
 cudaError_t launch_sil(const DevScene &s, gq_vecs x, const float *r_max, int64_t n, const int32_t *perm,

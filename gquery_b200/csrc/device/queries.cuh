@@ -13,6 +13,7 @@ struct DevScene {
     int dim;
     const void *pairs;   // gq_pair2_t / gq_pair3_t
     const void *prims;   // gq_seg_t / gq_tri_t
+    const gq_tsph_t *spheres;  // 3D: bounding sphere per ordered triangle
     int32_t root_ref;
     float root_lo[3], root_hi[3];
     const void *wnodes;  // gq_wnode2_t / gq_wnode3_t (may be null)
@@ -23,6 +24,7 @@ struct DevScene {
     const float *verts;  // original vertices [nv][D] (brute force)
     const int32_t *index;  // original primitives [np][D]
     int64_t n_prims;
+    float coord_bound;   // largest |coordinate| of any vertex
     int32_t *err;        // device error word
 };
 
@@ -34,10 +36,29 @@ size_t morton_scratch_bytes(int64_t n);
 cudaError_t morton_order(const DevScene &s, gq_vecs q, int64_t n, int32_t *perm, void *scratch, size_t scratch_bytes,
                          cudaStream_t st);
 
-cudaError_t launch_cp(const DevScene &s, int variant, gq_vecs q, int64_t n, const int32_t *perm, const gq_cp_out &o,
-                      cudaStream_t st);
-cudaError_t launch_ray(const DevScene &s, int variant, gq_vecs x, gq_vecs v, const float *r_max, int64_t n,
-                       const int32_t *perm, const gq_ray_out &o, cudaStream_t st);
+// Launch choices for one query kind (picked by the autotuner or the defaults).
+struct Tune {
+    int packet = 0;   // closest point: 1 = warp-coherent traversal
+    int sorted = 1;   // warp-coherent wide nodes: 1 = children in distance order, 0 = nearest first
+    int persist = 1;  // persistent warps with lane refill (per-thread traversal)
+    int budget = 32;  // node visits between refills
+};
+
+// `counter` is an 8-byte device word used by the persistent / warp-coherent kernels
+// (may be null: one query per thread then).
+cudaError_t launch_cp(const DevScene &s, int variant, const Tune &t, gq_vecs q, int64_t n, const int32_t *perm,
+                      const gq_cp_out &o, unsigned long long *counter, cudaStream_t st);
+cudaError_t launch_ray(const DevScene &s, int variant, const Tune &t, gq_vecs x, gq_vecs v, const float *r_max,
+                       int64_t n, const int32_t *perm, const gq_ray_out &o, unsigned long long *counter,
+                       cudaStream_t st);
+// Warp-coherent closest point, 3D; layout 0 = binary pairs, 1 = quantised 8-wide.
+cudaError_t launch_cp3_packet(const DevScene &s, int layout, gq_vecs q, int64_t n, const int32_t *perm,
+                              const gq_cp_out &o, unsigned long long *counter, cudaStream_t st);
+cudaError_t launch_cp_wide(const DevScene &s, gq_vecs q, int64_t n, const int32_t *perm, const gq_cp_out &o,
+                           unsigned long long *counter, cudaStream_t st);
+cudaError_t launch_ray_wide(const DevScene &s, gq_vecs x, gq_vecs v, const float *r_max, int64_t n,
+                            const int32_t *perm, const gq_ray_out &o, unsigned long long *counter,
+                            cudaStream_t st);
 cudaError_t launch_sil(const DevScene &s, gq_vecs x, const float *r_max, int64_t n, const int32_t *perm,
                        const gq_sil_out &o, cudaStream_t st);
 cudaError_t launch_cp_brute(const DevScene &s, gq_vecs q, int64_t n, const gq_cp_out &o, cudaStream_t st);

@@ -124,6 +124,27 @@ void flatten_bvh(const PrimSource<D> &src, const BvhTree<D> &t, DeviceImage<D> &
     }
     for (const auto &n : t.nodes)
         if (n.n_prims > 0) img.prims[(size_t)(n.prim_offset + n.n_prims - 1)].flags |= GQ_ITEM_LAST;
+
+    if constexpr (D == 3) {
+        // Bounding spheres: centre = fp32 centroid, radius = largest vertex distance in
+        // double, rounded up and widened by 2^-20 relative so the fp32 sphere contains
+        // the triangle exactly.
+        img.spheres.resize(img.prims.size());
+        for (size_t s = 0; s < img.prims.size(); ++s) {
+            const auto &r = img.prims[s];
+            const float cx = (r.ax + r.bx + r.cx) / 3.f, cy = (r.ay + r.by + r.cy) / 3.f,
+                        cz = (r.az + r.bz + r.cz) / 3.f;
+            auto dist = [&](float x, float y, float z) {
+                const double dx = (double)x - cx, dy = (double)y - cy, dz = (double)z - cz;
+                return std::sqrt(dx * dx + dy * dy + dz * dz);
+            };
+            double rad = std::max(dist(r.ax, r.ay, r.az), std::max(dist(r.bx, r.by, r.bz), dist(r.cx, r.cy, r.cz)));
+            float rf = (float)(rad * (1.0 + std::ldexp(1.0, -20)));
+            if ((double)rf < rad) rf = std::nextafter(rf, INFINITY);
+            img.spheres[s] = gq_tsph_t{cx, cy, cz, (r.flags & GQ_ITEM_LAST) ? -rf : rf};
+            if (rf == 0.f && (r.flags & GQ_ITEM_LAST)) img.spheres[s].r = -0.f;
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -141,19 +162,41 @@ int quant_exponent(float lo, float hi) {
     return e;
 }
 
-float dequant(float origin, int e, int q) {
+// Decoding used by the kernels.  `biased` is the node's stored origin
+// fma(-2^23, 2^e, lo); the kernels build the float 2^23 + q from the byte with one
+// byte-permute and decode with one fma.
+float dequant(float biased, int e, int q) {
     float s = std::ldexp(1.0f, e);
-    return std::fma((float)q, s, origin);
+    return std::fma((float)(8388608 + q), s, biased);
+}
+
+// Biased origin and exponent for the parent box [lo, hi] such that decode(0) <= lo
+// and decode(255) >= hi hold exactly in fp32.
+static void quant_axis(float lo, float hi, float *biased, int *e_out) {
+    int e = quant_exponent(lo, hi);
+    for (;;) {
+        float s = std::ldexp(1.0f, e);
+        float b = std::fma(-8388608.0f, s, lo);
+        int guard = 0;
+        while (!(dequant(b, e, 0) <= lo) && guard++ < 64) b = std::nextafter(b, -INFINITY);
+        if (dequant(b, e, 255) >= hi || e >= 127) {
+            *biased = b;
+            *e_out = e;
+            return;
+        }
+        ++e;
+    }
 }
 
 void quantise_bounds(float origin, int e, float clo, float chi, uint8_t *qlo, uint8_t *qhi) {
+    const double base = (double)dequant(origin, e, 0);
     // largest q with decode(q) <= clo
-    int a = (int)std::floor(((double)clo - (double)origin) / std::ldexp(1.0, e));
+    int a = (int)std::floor(((double)clo - base) / std::ldexp(1.0, e));
     a = std::max(0, std::min(255, a));
     while (a > 0 && !(dequant(origin, e, a) <= clo)) --a;
     while (a < 255 && dequant(origin, e, a + 1) <= clo) ++a;
     // smallest q with decode(q) >= chi
-    int b = (int)std::ceil(((double)chi - (double)origin) / std::ldexp(1.0, e));
+    int b = (int)std::ceil(((double)chi - base) / std::ldexp(1.0, e));
     b = std::max(0, std::min(255, b));
     while (b < 255 && !(dequant(origin, e, b) >= chi)) ++b;
     while (b > 0 && dequant(origin, e, b - 1) >= chi) --b;
@@ -195,17 +238,18 @@ struct WideBuilder {
         *ref_out = (int32_t)me;
 
         int e[D];
-        for (int k = 0; k < D; ++k) e[k] = quant_exponent(bn.box.lo.v[k], bn.box.hi.v[k]);
+        float org[D];
+        for (int k = 0; k < D; ++k) quant_axis(bn.box.lo.v[k], bn.box.hi.v[k], &org[k], &e[k]);
         typename DeviceImage<D>::WNode w;
         std::memset(&w, 0, sizeof w);
         if constexpr (D == 2) {
-            w.ox = bn.box.lo.v[0];
-            w.oy = bn.box.lo.v[1];
+            w.ox = org[0];
+            w.oy = org[1];
             w.meta = (uint32_t)(e[0] + 127) | ((uint32_t)(e[1] + 127) << 8) | ((uint32_t)kids.size() << 24);
         } else {
-            w.ox = bn.box.lo.v[0];
-            w.oy = bn.box.lo.v[1];
-            w.oz = bn.box.lo.v[2];
+            w.ox = org[0];
+            w.oy = org[1];
+            w.oz = org[2];
             w.meta = (uint32_t)(e[0] + 127) | ((uint32_t)(e[1] + 127) << 8) | ((uint32_t)(e[2] + 127) << 16) |
                      ((uint32_t)kids.size() << 24);
         }
@@ -213,10 +257,8 @@ struct WideBuilder {
         int deepest = 0;
         for (size_t k = 0; k < kids.size(); ++k) {
             const auto &kn = t.nodes[kids[k]];
-            for (int ax = 0; ax < D; ++ax) {
-                const float o = (ax == 0) ? w.ox : (ax == 1 ? w.oy : bn.box.lo.v[2]);
-                quantise_bounds(o, e[ax], kn.box.lo.v[ax], kn.box.hi.v[ax], &w.q[ax][k], &w.q[D + ax][k]);
-            }
+            for (int ax = 0; ax < D; ++ax)
+                quantise_bounds(org[ax], e[ax], kn.box.lo.v[ax], kn.box.hi.v[ax], &w.q[ax][k], &w.q[D + ax][k]);
             if (kn.n_prims > 0) {
                 w.ref[k] = ~kn.prim_offset;
             } else {

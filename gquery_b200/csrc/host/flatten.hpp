@@ -20,6 +20,7 @@ struct DeviceImage {
     // binary BVH
     std::vector<Pair> pairs;
     std::vector<Prim> prims;
+    std::vector<gq_tsph_t> spheres;  // 3D only: per ordered triangle
     int32_t root_ref = 0;
     float root_lo[D] = {}, root_hi[D] = {};
     int exact_stack = 0;  // entries the binary traversal needs (max leaf depth + 1)

@@ -49,6 +49,13 @@ typedef struct {
     int32_t index, flags, pad;
 } gq_tri_t;
 
+// Bounding sphere of an ordered triangle, parallel to the triangle records: centre
+// and radius, the radius rounded up so the sphere contains the triangle in exact
+// arithmetic; its sign bit repeats the triangle's end-of-leaf flag.            16 B
+typedef struct {
+    float cx, cy, cz, r;
+} gq_tsph_t;
+
 // 2D silhouette vertex: (a.xy, b.xy) | (c.xy, prim_id, flags)            32 B
 typedef struct {
     float ax, ay, bx, by;

@@ -15,7 +15,10 @@ from . import records as R
 
 ArrayLike = Union[torch.Tensor, np.ndarray, Sequence]
 
-VARIANTS = {"exact": L.VARIANT_EXACT, "wide8": L.VARIANT_WIDE8, "auto": L.VARIANT_AUTO}
+VARIANTS = {"exact": L.VARIANT_EXACT, "wide8": L.VARIANT_WIDE8, "auto": L.VARIANT_AUTO,
+            "coherent": L.VARIANT_COHERENT}
+KINDS = {"cp": L.KIND_CLOSEST_POINT, "ray": L.KIND_INTERSECT, "sil": L.KIND_SILHOUETTE}
+VARIANT_NAMES = {v: k for k, v in VARIANTS.items()}
 
 
 def _as_tensor(x) -> torch.Tensor:
@@ -160,6 +163,18 @@ class Scene:
         sp, sb = (None, 0) if scratch is None else (scratch.data_ptr(), scratch.numel() * scratch.element_size())
         L.check(L.lib().gq_query_order(self._h, vq, n, perm.data_ptr(), sp, sb, _stream_handle(stream)))
         return perm
+
+    def get_tuning(self, kind: str) -> dict:
+        t = L.Tuning()
+        L.check(L.lib().gq_scene_get_tuning(self._h, KINDS[kind], C.byref(t)))
+        d = {k: getattr(t, k) for k, _ in L.Tuning._fields_}
+        d["variant"] = VARIANT_NAMES[d["variant"]]
+        return d
+
+    def set_tuning(self, kind: str, variant: str, packet: int = 0, sorted: int = 1, persist: int = 1,
+                   budget: int = 32) -> None:
+        t = L.Tuning(VARIANTS[variant], packet, sorted, persist, budget)
+        L.check(L.lib().gq_scene_set_tuning(self._h, KINDS[kind], C.byref(t)))
 
     def scratch_bytes(self, n: int) -> int:
         return int(L.lib().gq_query_scratch_bytes(n))

@@ -43,9 +43,26 @@ typedef int32_t gq_status;
 #define GQ_ERR_UNSUPPORTED 6
 
 /* Traversal variants */
-#define GQ_VARIANT_EXACT 0  /* binary tree, gQuery's visit order: reference-identical answers */
-#define GQ_VARIANT_WIDE8 1  /* 8-wide nodes, 8-bit outward-rounded child boxes */
-#define GQ_VARIANT_AUTO 2   /* fastest available (WIDE8 for BVH queries, EXACT for SNCH) */
+#define GQ_VARIANT_EXACT 0    /* binary tree, gQuery's visit order: reference-identical answers */
+#define GQ_VARIANT_WIDE8 1    /* 8-wide nodes, 8-bit outward-rounded child boxes */
+#define GQ_VARIANT_AUTO 2     /* the scene's tuned choice for the query kind (gq_scene_set_tuning) */
+#define GQ_VARIANT_COHERENT 3 /* binary tree walked once per warp of Morton-adjacent queries (3D closest
+                                 point); other query kinds run as EXACT */
+/* All variants other than EXACT give the same answers as EXACT except at FP32 distance
+ * ties (distances within 2e-6 relative). */
+
+/* Query kinds (tuning table) */
+#define GQ_KIND_CLOSEST_POINT 0
+#define GQ_KIND_INTERSECT 1
+#define GQ_KIND_SILHOUETTE 2
+
+typedef struct {
+    int32_t variant;  /* variant used when a query asks for GQ_VARIANT_AUTO */
+    int32_t packet;   /* WIDE8 closest point (3D): warp-coherent traversal */
+    int32_t sorted;   /* warp-coherent wide nodes: children in distance order (else nearest first) */
+    int32_t persist;  /* per-thread kernels: persistent warps, finished lanes take new queries */
+    int32_t budget;   /* node visits between refills */
+} gq_tuning;
 
 typedef struct gq_scene gq_scene;
 
@@ -120,6 +137,13 @@ gq_status gq_scene_build_3d(const float *vertices, int64_t nv, const int32_t *fa
                             const gq_build_opts *opts, gq_scene **out);
 gq_status gq_scene_free(gq_scene *scene);
 gq_status gq_scene_get_info(const gq_scene *scene, gq_scene_info *info);
+
+/* Launch choices per query kind (no counterpart in the reference, whose DrJit backend
+ * picks its own launch shape).  gquery_b200.autotune measures the candidates and sets
+ * them; the built-in defaults are the measured B200 choices for the benchmark scenes.
+ * Not thread-safe against concurrent queries on the same scene. */
+gq_status gq_scene_set_tuning(gq_scene *scene, int32_t kind, const gq_tuning *tuning);
+gq_status gq_scene_get_tuning(const gq_scene *scene, int32_t kind, gq_tuning *tuning);
 
 /* Reference float layouts (gquery_ext node_data / primitive_data / silhouette_data /
  * raw_silhouette_data, src/gquery.cpp:186-187, 229-231, 241-244).  Copies up to `cap`

@@ -177,10 +177,11 @@ def _decode_wide(words, dim):
     scale = np.ldexp(np.float32(1.0), exps).astype(np.float32)
     lo = np.empty((w.shape[0], 8, dim), np.float32)
     hi = np.empty_like(lo)
-    for k in range(dim):  # decode exactly like the kernels: fma(q, 2^e, origin) in fp32
-        lo[:, :, k] = (q[:, k, :].astype(np.float64) * scale[:, k:k + 1] + origin[:, k:k + 1]).astype(np.float32)
-        hi[:, :, k] = (q[:, dim + k, :].astype(np.float64) * scale[:, k:k + 1] + origin[:, k:k + 1]).astype(
-            np.float32)
+    for k in range(dim):  # decode like the kernels: fma(2^23 + q, 2^e, biased origin) in fp32
+        s = scale[:, k:k + 1].astype(np.float64)
+        o = origin[:, k:k + 1].astype(np.float64)
+        lo[:, :, k] = ((q[:, k, :].astype(np.float64) + 8388608.0) * s + o).astype(np.float32)
+        hi[:, :, k] = ((q[:, dim + k, :].astype(np.float64) + 8388608.0) * s + o).astype(np.float32)
     return refs, nc, lo, hi
 
 

@@ -249,3 +249,46 @@ def test_exact_error_vs_fp64_c1_subset(mesh_c1):
     d64 = d64.cpu().numpy()
     err = np.abs(got["d"].astype(np.float64) - d64)
     assert err.max() <= ABS_TOL, err.max()
+
+
+# ---------------------------------------------------------------- fast variants vs exact
+
+@pytest.mark.parametrize("variant,tuning", [
+    ("coherent", None),
+    ("wide8", dict(packet=1, sorted=1)),
+    ("wide8", dict(packet=1, sorted=0)),
+    ("wide8", dict(packet=0, persist=1, budget=16)),
+    ("wide8", dict(packet=0, persist=0)),
+])
+def test_cp3d_fast_variants_match_exact(mesh_c1, variant, tuning):
+    q = W.uniform_points(131072 + 5, 3, seed=61)
+    a = to_np(mesh_c1.closest_point(q, variant="exact", sort=True))
+    saved = mesh_c1.get_tuning("cp")
+    try:
+        if tuning is not None:
+            mesh_c1.set_tuning("cp", variant, **tuning)
+        b = to_np(mesh_c1.closest_point(q, variant=variant, sort=True))
+    finally:
+        mesh_c1.set_tuning("cp", saved["variant"], saved["packet"], saved["sorted"], saved["persist"], saved["budget"])
+    rep = tie_report(a, b)
+    assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0, rep
+    assert rep["max_rel_d"] <= REL_TOL, rep
+    assert mesh_c1.device_error() == 0
+
+
+def test_auto_uses_tuning_table(mesh_small):
+    q = W.uniform_points(10000, 3, seed=62)
+    ref = to_np(mesh_small.closest_point(q, variant="exact"))
+    for variant in ("exact", "coherent", "wide8"):
+        mesh_small.set_tuning("cp", variant, packet=1)
+        assert mesh_small.get_tuning("cp")["variant"] == variant
+        rep = tie_report(ref, to_np(mesh_small.closest_point(q, variant="auto")))
+        assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0, rep
+
+
+def test_unsorted_queries_give_same_answers(mesh_c1):
+    q = W.uniform_points(50000, 3, seed=63)
+    a = to_np(mesh_c1.closest_point(q, variant="coherent", sort=False))
+    b = to_np(mesh_c1.closest_point(q, variant="coherent", sort=True))
+    rep = tie_report(a, b)
+    assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0, rep
