@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-compare", action="store_true", help="skip the exact and wide8 side-by-side runs")
     return ap.parse_args()
 
 
@@ -282,15 +283,18 @@ def main():
             res["step_ms"], res["cp_ms"], res["ray_ms"] = (float(x) for x in t.tolist())
         return res, clk
 
-    plain, _ = timed("exact", max(2, args.steps // 2), 2)
-    quant, _ = timed("wide8", max(2, args.steps // 2), 2)
+    if args.no_compare:
+        plain = quant = None
+    else:
+        plain, _ = timed("exact", max(2, args.steps // 2), 2)
+        quant, _ = timed("wide8", max(2, args.steps // 2), 2)
     main_res, clocks = timed(args.variant, args.steps, max(3, args.warmup), clocks=True)
     assert scene.device_error() == 0, "device error flag raised"
 
     total_q = 2 * n * world
     value = total_q / (main_res["step_ms"] / 1e3) / 1e6
-    plain_value = total_q / (plain["step_ms"] / 1e3) / 1e6
-    quant_value = total_q / (quant["step_ms"] / 1e3) / 1e6
+    plain_value = total_q / (plain["step_ms"] / 1e3) / 1e6 if plain else None
+    quant_value = total_q / (quant["step_ms"] / 1e3) / 1e6 if quant else None
 
     # ---- end to end through the public API with host buffers ----
     e2e = None
@@ -361,12 +365,13 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "variant": f"{args.variant}+morton", "queries_per_rank": 2 * n,
                        "parallelism": f"replicated scene, {world} query shard(s)", "l2": "flushed between steps"},
-            "plain_exact": {"value": plain_value, "ms_per_step": plain["step_ms"], "cp_ms": plain["cp_ms"],
-                            "ray_ms": plain["ray_ms"]},
-            "quantised_wide8": {"value": quant_value, "ms_per_step": quant["step_ms"], "cp_ms": quant["cp_ms"],
-                                "ray_ms": quant["ray_ms"], "vs_plain": quant_value / plain_value},
+            "plain_exact": plain and {"value": plain_value, "ms_per_step": plain["step_ms"], "cp_ms": plain["cp_ms"],
+                                      "ray_ms": plain["ray_ms"]},
+            "quantised_wide8": quant and {"value": quant_value, "ms_per_step": quant["step_ms"],
+                                          "cp_ms": quant["cp_ms"], "ray_ms": quant["ray_ms"],
+                                          "vs_plain": quant_value / plain_value},
             "tuned": {"cp": scene.get_tuning("cp"), "ray": scene.get_tuning("ray"),
-                      "vs_plain": value / plain_value},
+                      "vs_plain": value / plain_value if plain else None},
             "breakdown_ms": {k: main_res[k] for k in ("order_cp_ms", "cp_ms", "order_ray_ms", "ray_ms",
                                                       "wall_ms_per_step")},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
