@@ -98,6 +98,9 @@ SIGNATURES = {
     "gq_query_order": (C.c_int32, [C.c_void_p, Vecs, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),
     "gq_closest_point": (C.c_int32, [C.c_void_p, Vecs, C.c_int64, C.POINTER(CpOut), C.POINTER(QueryOpts),
                                      C.c_void_p]),
+    "gq_noalloc_max_queries": (C.c_int64, []),
+    "gq_closest_point_noalloc": (C.c_int32, [C.c_void_p, Vecs, C.c_int64, C.POINTER(CpOut), C.c_int32, C.c_int32,
+                                             C.c_void_p]),
     "gq_intersect": (C.c_int32, [C.c_void_p, Vecs, Vecs, C.c_void_p, C.c_int64, C.POINTER(RayOut),
                                  C.POINTER(QueryOpts), C.c_void_p]),
     "gq_closest_silhouette": (C.c_int32, [C.c_void_p, Vecs, C.c_void_p, C.c_int64, C.POINTER(SilOut),

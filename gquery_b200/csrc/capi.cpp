@@ -468,6 +468,30 @@ gq_status gq_closest_point(const gq_scene *s, gq_vecs q, int64_t n, const gq_cp_
     return GQ_OK;
 }
 
+int64_t gq_noalloc_max_queries(void) { return gqd::noalloc_max_queries(); }
+
+gq_status gq_closest_point_noalloc(const gq_scene *s, gq_vecs q, int64_t n, const gq_cp_out *out, int32_t variant,
+                                   int32_t sort, void *stream) {
+    if (!s || !out) return fail(GQ_ERR_INVALID, "null scene or output");
+    if (n < 0) return fail(GQ_ERR_INVALID, "negative query count");
+    if (n > gqd::noalloc_max_queries())
+        return fail(GQ_ERR_INVALID, "gq_closest_point_noalloc takes at most " +
+                                        std::to_string(gqd::noalloc_max_queries()) + " queries per call");
+    if (n == 0) return GQ_OK;
+    if (!vecs_ok(q)) return fail(GQ_ERR_INVALID, "null query array");
+    gq_query_opts o{};
+    o.variant = variant;
+    const int v = resolve_variant(s, &o, GQ_KIND_CLOSEST_POINT);
+    gq_status st = check_variant(s, v);
+    if (st != GQ_OK) return st;
+    if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "scene was built without a device copy");
+    DeviceGuard g(s->device);
+    cudaError_t e = gqd::noalloc_closest_point(s->dev, v, to_tune(s->tune[GQ_KIND_CLOSEST_POINT]), q, n, sort,
+                                               *out, (cudaStream_t)stream);
+    if (e != cudaSuccess) return fail_cuda(e, "closest_point_noalloc");
+    return GQ_OK;
+}
+
 gq_status gq_intersect(const gq_scene *s, gq_vecs origin, gq_vecs dir, const float *r_max, int64_t n,
                        const gq_ray_out *out, const gq_query_opts *opts, void *stream) {
     if (!s || !out) return fail(GQ_ERR_INVALID, "null scene or output");

@@ -68,3 +68,10 @@ cudaError_t launch_brute_f64(const DevScene &s, int kind, gq_vecs a, gq_vecs b, 
                              int32_t *out_id, cudaStream_t st);
 
 }  // namespace gqd
+
+namespace gqd {
+// Allocation-free closest point (noalloc.cu): scratch in a static device array.
+int64_t noalloc_max_queries();
+cudaError_t noalloc_closest_point(const DevScene &s, int variant, const Tune &t, gq_vecs q, int64_t n, int sort,
+                                  const gq_cp_out &o, cudaStream_t st);
+}  // namespace gqd

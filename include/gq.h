@@ -178,6 +178,21 @@ gq_status gq_query_order(const gq_scene *scene, gq_vecs points, int64_t n, int32
 gq_status gq_closest_point(const gq_scene *scene, gq_vecs q, int64_t n, const gq_cp_out *out,
                            const gq_query_opts *opts, void *stream);
 
+/* Closest point without any device allocation.  No counterpart in the reference: for
+ * callers that cannot allocate device memory while querying (a CUDA graph recorded with
+ * a cudaMalloc-based allocator, a plugin whose host owns all device memory, a real-time
+ * loop that must not enter an allocator).  The per-call scratch (work counter and
+ * Morton-sort buffers) comes from a fixed device array inside the library, which every
+ * device that loads the library holds until the process exits; hence at most
+ * gq_noalloc_max_queries() queries per call (larger n is rejected with GQ_ERR_INVALID).
+ * Same answers as gq_closest_point with the same variant and sort flag.  All calls on a
+ * device share that array: calls whose kernels may overlap on the GPU race and must be
+ * ordered by the caller (one stream, or events).  The first call on a device looks up
+ * the array's device address; make that first call before any stream capture. */
+int64_t gq_noalloc_max_queries(void);
+gq_status gq_closest_point_noalloc(const gq_scene *scene, gq_vecs q, int64_t n, const gq_cp_out *out,
+                                   int32_t variant, int32_t sort, void *stream);
+
 /* intersect_bvh (polyline.py:132 -> bvh.py:200; mesh.py:86 -> bvh3d.py:176).
  * r_max: device [n] or NULL for +inf. */
 gq_status gq_intersect(const gq_scene *scene, gq_vecs origin, gq_vecs dir, const float *r_max, int64_t n,
