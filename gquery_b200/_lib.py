@@ -37,6 +37,11 @@ ARRAY_WIDE_NODES = 5
 
 DEVERR_STACK = 1
 
+BATCH_CP_EXACT = 1
+BATCH_RAY_EXACT = 2
+BATCH_ERR_SCENE = 1 << 8
+BATCH_ERR_NO_SNCH = 1 << 9
+
 
 class BuildOpts(C.Structure):
     _fields_ = [("max_prims_in_node", C.c_int32), ("n_threads", C.c_int32), ("build_snch", C.c_int32),
@@ -78,6 +83,10 @@ class QueryOpts(C.Structure):
                 ("scratch_bytes", C.c_int64)]
 
 
+class BatchQueries(C.Structure):
+    _fields_ = [("n", C.c_int64), ("scene", C.c_void_p), ("a", Vecs), ("b", Vecs), ("r_max", C.c_void_p)]
+
+
 # name -> (restype, argtypes); every exported symbol of include/gq.h
 SIGNATURES = {
     "gq_last_error": (None, [C.c_char_p, C.c_int64]),
@@ -111,6 +120,12 @@ SIGNATURES = {
     "gq_brute_f64": (C.c_int32, [C.c_void_p, C.c_int32, Vecs, Vecs, C.c_int64, C.c_void_p, C.c_void_p,
                                  C.c_void_p]),
     "gq_scene_device_error": (C.c_int32, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)]),
+    "gq_batch_create": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int64, C.c_int32, C.POINTER(C.c_void_p)]),
+    "gq_batch_free": (C.c_int32, [C.c_void_p]),
+    "gq_batch_device_bytes": (C.c_int64, [C.c_void_p]),
+    "gq_batch_run": (C.c_int32, [C.c_void_p, C.POINTER(BatchQueries), C.POINTER(CpOut), C.POINTER(BatchQueries),
+                                 C.POINTER(RayOut), C.POINTER(BatchQueries), C.POINTER(SilOut), C.c_void_p]),
+    "gq_batch_device_error": (C.c_int32, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)]),
 }
 
 _lock = threading.Lock()

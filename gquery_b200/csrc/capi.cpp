@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/gq.h"
+#include "device/batch.cuh"
 #include "device/queries.cuh"
 #include "host/flatten.hpp"
 #include "host/scene_build.hpp"
@@ -286,6 +287,26 @@ gq_status prepare_order(const gq_scene *s, gq_vecs keys_from, int64_t n, const g
 }
 
 }  // namespace
+
+
+struct gq_batch {
+    int dim = 0;
+    int device = 0;
+    int flags = 0;
+    std::vector<gq_scene *> scenes;
+    int64_t max_queries = 0;
+    gqd::DevScene *dev_scenes = nullptr;
+    void *scratch = nullptr;
+    int32_t *err = nullptr;
+    int64_t device_bytes = 0;
+
+    ~gq_batch() {
+        DeviceGuard g(device);
+        if (dev_scenes) cudaFree(dev_scenes);
+        if (scratch) cudaFree(scratch);
+        if (err) cudaFree(err);
+    }
+};
 
 extern "C" {
 
@@ -586,6 +607,114 @@ gq_status gq_scene_device_error(const gq_scene *s, void *stream, int32_t *flags)
     if (e == cudaSuccess) e = cudaStreamSynchronize(cs);
     if (e != cudaSuccess) return fail_cuda(e, "device error read");
     *flags = v;
+    return GQ_OK;
+}
+
+
+gq_status gq_batch_create(gq_scene *const *scenes, int32_t n_scenes, int64_t max_queries, int32_t flags,
+                          gq_batch **out) {
+    if (!out) return fail(GQ_ERR_INVALID, "null output");
+    *out = nullptr;
+    if (!scenes || n_scenes <= 0) return fail(GQ_ERR_INVALID, "a batch needs at least one scene");
+    if (max_queries < 0 || max_queries > (int64_t)INT32_MAX) return fail(GQ_ERR_INVALID, "max_queries out of range");
+    std::unique_ptr<gq_batch> b(new (std::nothrow) gq_batch());
+    if (!b) return fail(GQ_ERR_NOMEM, "host allocation");
+    b->flags = flags;
+    b->max_queries = max_queries;
+    std::vector<gqd::DevScene> views((size_t)n_scenes);
+    for (int32_t i = 0; i < n_scenes; ++i) {
+        const gq_scene *s = scenes[i];
+        if (!s) return fail(GQ_ERR_INVALID, "null scene in batch");
+        if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "scene was built without a device copy");
+        if (i == 0) {
+            b->dim = s->dim;
+            b->device = s->device;
+        } else if (s->dim != b->dim || s->device != b->device) {
+            return fail(GQ_ERR_INVALID, "batch scenes must share dimension and device");
+        }
+        views[(size_t)i] = s->dev;
+        b->scenes.push_back(scenes[i]);
+    }
+    DeviceGuard g(b->device);
+    if (!g.ok) return fail(GQ_ERR_CUDA, "cudaSetDevice failed");
+    const size_t vb = views.size() * sizeof(gqd::DevScene);
+    const size_t sb = gqd::batch_scratch_bytes(max_queries);
+    cudaError_t e = cudaMalloc((void **)&b->dev_scenes, vb);
+    if (e == cudaSuccess) e = cudaMalloc(&b->scratch, sb);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&b->err, 256);
+    if (e != cudaSuccess) return fail(GQ_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    b->device_bytes = (int64_t)(vb + sb + 256);
+    e = cudaMemcpy(b->dev_scenes, views.data(), vb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(b->err, 0, 256);
+    if (e != cudaSuccess) return fail_cuda(e, "batch upload");
+    *out = b.release();
+    return GQ_OK;
+}
+
+gq_status gq_batch_free(gq_batch *b) {
+    delete b;
+    return GQ_OK;
+}
+
+int64_t gq_batch_device_bytes(const gq_batch *b) { return b ? b->device_bytes : 0; }
+
+gq_status gq_batch_run(gq_batch *b, const gq_batch_queries *cp, const gq_cp_out *cp_out, const gq_batch_queries *ray,
+                       const gq_ray_out *ray_out, const gq_batch_queries *sil, const gq_sil_out *sil_out,
+                       void *stream) {
+    if (!b) return fail(GQ_ERR_INVALID, "null batch");
+    gqd::BatchKind kinds[3];
+    const gq_batch_queries *in[3] = {cp, ray, sil};
+    const bool has_out[3] = {cp_out != nullptr, ray_out != nullptr, sil_out != nullptr};
+    static const char *names[3] = {"closest-point", "ray", "silhouette"};
+    for (int k = 0; k < 3; ++k) {
+        if (!in[k] || in[k]->n == 0) continue;
+        const gq_batch_queries &q = *in[k];
+        if (!has_out[k]) return fail(GQ_ERR_INVALID, std::string("null ") + names[k] + " output");
+        if (q.n < 0) return fail(GQ_ERR_INVALID, "negative query count");
+        if (q.n > b->max_queries)
+            return fail(GQ_ERR_INVALID, std::string(names[k]) + " queries exceed the batch's max_queries (" +
+                                            std::to_string(q.n) + " > " + std::to_string(b->max_queries) + ")");
+        if (!q.scene || !vecs_ok(q.a) || (k == 1 && !vecs_ok(q.b)))
+            return fail(GQ_ERR_INVALID, std::string("null ") + names[k] + " query array");
+        kinds[k].a = q.a;
+        kinds[k].b = q.b;
+        kinds[k].r_max = q.r_max;
+        kinds[k].scene = q.scene;
+        kinds[k].n = q.n;
+    }
+    if (kinds[2].n > 0) {
+        for (const gq_scene *s : b->scenes)
+            if (!s->has_snch) return fail(GQ_ERR_UNSUPPORTED, "silhouette queries need every batch scene built with SNCH");
+    }
+    DeviceGuard g(b->device);
+    const gq_cp_out co = cp_out ? *cp_out : gq_cp_out{};
+    const gq_ray_out ro = ray_out ? *ray_out : gq_ray_out{};
+    const gq_sil_out so = sil_out ? *sil_out : gq_sil_out{};
+    cudaError_t e = gqd::batch_run(b->dev_scenes, (int)b->scenes.size(), b->dim, kinds, co, ro, so,
+                                   (b->flags & GQ_BATCH_RAY_EXACT) ? 0 : 1, (b->flags & GQ_BATCH_CP_EXACT) ? 0 : 1,
+                                   b->scratch, b->max_queries, b->err, (cudaStream_t)stream);
+    if (e != cudaSuccess) return fail_cuda(e, "batch launch");
+    return GQ_OK;
+}
+
+gq_status gq_batch_device_error(gq_batch *b, void *stream, int32_t *flags) {
+    if (!b || !flags) return fail(GQ_ERR_INVALID, "null argument");
+    DeviceGuard g(b->device);
+    cudaStream_t cs = (cudaStream_t)stream;
+    int32_t v = 0;
+    cudaError_t e = cudaMemcpyAsync(&v, b->err, sizeof v, cudaMemcpyDeviceToHost, cs);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cs);
+    if (e == cudaSuccess && v != 0) e = cudaMemsetAsync(b->err, 0, sizeof v, cs);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cs);
+    if (e != cudaSuccess) return fail_cuda(e, "batch error read");
+    int32_t all = v << 8;
+    for (const gq_scene *s : b->scenes) {
+        int32_t f = 0;
+        gq_status st = gq_scene_device_error(s, stream, &f);
+        if (st != GQ_OK) return st;
+        all |= f;
+    }
+    *flags = all;
     return GQ_OK;
 }
 

@@ -1,0 +1,33 @@
+// Batched queries over many scenes in one launch (batch.cu).
+#pragma once
+
+#include "queries.cuh"
+
+namespace gqd {
+
+// Queries of one kind: query q belongs to scene[q] (an index into the batch's scenes).
+struct BatchKind {
+    gq_vecs a{};             // points / ray origins
+    gq_vecs b{};             // ray directions
+    const float *r_max = nullptr;
+    const int32_t *scene = nullptr;
+    int64_t n = 0;
+    const int32_t *perm = nullptr;  // filled by batch_run: sorted order
+};
+
+#define GQ_BATCH_SKIP (-1)       // scene index of a padding slot: no traversal, outputs untouched
+#define GQ_BATCH_ERR_SCENE 1    // a query named a scene outside the batch
+#define GQ_BATCH_ERR_NO_SNCH 2  // a silhouette query named a scene built without SNCH
+
+// Device scratch for batch_run with at most max_n queries of each kind.
+size_t batch_scratch_bytes(int64_t max_n);
+
+// kinds[0] closest point, kinds[1] rays, kinds[2] silhouettes (n = 0 to skip a kind).
+// ray_wide: rays on the quantised 8-wide BVH where a scene has one; cp_coherent:
+// warp-coherent closest point (else one exact traversal per lane).  No allocation and
+// no host synchronisation: the call can be recorded in a CUDA graph.
+cudaError_t batch_run(const DevScene *scenes_dev, int n_scenes, int dim, BatchKind kinds[3], const gq_cp_out &cp_out,
+                      const gq_ray_out &ray_out, const gq_sil_out &sil_out, int ray_wide, int cp_coherent,
+                      void *scratch, int64_t max_n, int32_t *err, cudaStream_t st);
+
+}  // namespace gqd

@@ -51,14 +51,9 @@ cudaError_t launch_cp(const DevScene &s, int variant, const Tune &t, gq_vecs q, 
 cudaError_t launch_ray(const DevScene &s, int variant, const Tune &t, gq_vecs x, gq_vecs v, const float *r_max,
                        int64_t n, const int32_t *perm, const gq_ray_out &o, unsigned long long *counter,
                        cudaStream_t st);
-// Warp-coherent closest point, 3D; layout 0 = binary pairs, 1 = quantised 8-wide.
-cudaError_t launch_cp3_packet(const DevScene &s, int layout, gq_vecs q, int64_t n, const int32_t *perm,
+// Warp-coherent closest point; layout 0 = binary pairs, 1 / 2 = quantised 8-wide (3D): sorted / nearest first.
+cudaError_t launch_cp_packet(const DevScene &s, int layout, gq_vecs q, int64_t n, const int32_t *perm,
                               const gq_cp_out &o, unsigned long long *counter, cudaStream_t st);
-cudaError_t launch_cp_wide(const DevScene &s, gq_vecs q, int64_t n, const int32_t *perm, const gq_cp_out &o,
-                           unsigned long long *counter, cudaStream_t st);
-cudaError_t launch_ray_wide(const DevScene &s, gq_vecs x, gq_vecs v, const float *r_max, int64_t n,
-                            const int32_t *perm, const gq_ray_out &o, unsigned long long *counter,
-                            cudaStream_t st);
 cudaError_t launch_sil(const DevScene &s, gq_vecs x, const float *r_max, int64_t n, const int32_t *perm,
                        const gq_sil_out &o, cudaStream_t st);
 cudaError_t launch_cp_brute(const DevScene &s, gq_vecs q, int64_t n, const gq_cp_out &o, cudaStream_t st);

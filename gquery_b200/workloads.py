@@ -107,3 +107,33 @@ def config3_scenes(n_scenes: int = 512, lo: int = 64, hi: int = 262144):
         m = int(round(math.exp(rng.uniform(math.log(lo), math.log(hi)))))
         out.append(star_polyline(m, seed=sid))
     return out
+
+
+def config3_queries(scenes, n_total: int = 1 << 24, mix=(0.5, 0.3, 0.2), seed: int = 7):
+    """Per-scene query counts proportional to segment count (summing to n_total), each
+    scene's queries uniform in its bounding box scaled 2x about its centre, split
+    closest point / ray / silhouette by `mix` (rays: directions uniform on S^1).
+
+    Returns {"cp": (ids, pts), "ray": (ids, origins, dirs), "sil": (ids, pts)} with
+    int32 [n] scene ids and float32 [n, 2] arrays, grouped by scene."""
+    rng = np.random.default_rng(seed)
+    m = np.array([e.shape[0] for _, e in scenes], dtype=np.float64)
+    counts = np.floor(n_total * m / m.sum()).astype(np.int64)
+    counts[np.argsort(-m)[: n_total - counts.sum()]] += 1  # hand out the remainder to the largest scenes
+    parts = {"cp": [], "ray": [], "sil": []}
+    for sid, ((v, _), c) in enumerate(zip(scenes, counts)):
+        lo, hi = v.min(axis=0).astype(np.float64), v.max(axis=0).astype(np.float64)
+        mid, half = 0.5 * (lo + hi), 0.5 * (hi - lo)
+        n_cp = int(round(c * mix[0]))
+        n_ray = int(round(c * mix[1]))
+        n_sil = int(c) - n_cp - n_ray
+        for kind, k in (("cp", n_cp), ("ray", n_ray), ("sil", n_sil)):
+            pts = (mid + rng.uniform(-2.0, 2.0, size=(k, 2)) * half).astype(np.float32)
+            ids = np.full(k, sid, np.int32)
+            if kind == "ray":
+                a = rng.uniform(0.0, 2.0 * np.pi, size=k)
+                dirs = np.stack([np.cos(a), np.sin(a)], axis=1).astype(np.float32)
+                parts[kind].append((ids, pts, dirs))
+            else:
+                parts[kind].append((ids, pts))
+    return {k: tuple(np.concatenate(col) for col in zip(*v)) for k, v in parts.items()}

@@ -8,7 +8,7 @@
  *     BVH.closest_point (gquery/shapes/bvh.py:127), BVH.intersect (bvh.py:200),
  *     BVH3D.closest_point (bvh3d.py:108), BVH3D.intersect (bvh3d.py:176),
  *     SNCH.closest_silhouette (snch.py:106), SNCH3D.closest_silhouette (snch3d.py:143),
- *     and the brute-force *_baseline methods (polyline.py:137-223, mesh.py:287-362).
+ *     and the brute-force *_baseline methods (polyline.py:138, 176, 212; mesh.py:61, 92, 124).
  *
  * Conventions
  *   - Plain pointers and sizes only.  Host pointers are marked "host"; everything a
@@ -204,7 +204,7 @@ gq_status gq_closest_silhouette(const gq_scene *scene, gq_vecs x, const float *r
                                 const gq_sil_out *out, const gq_query_opts *opts, void *stream);
 
 /* Brute-force scans over every primitive in original order (closest_point_baseline,
- * intersect_baseline: polyline.py:137-209, mesh.py:287-348).  FP32 like the reference. */
+ * intersect_baseline: polyline.py:138-209, mesh.py:61-118).  FP32 like the reference. */
 gq_status gq_closest_point_brute(const gq_scene *scene, gq_vecs q, int64_t n, const gq_cp_out *out, void *stream);
 gq_status gq_intersect_brute(const gq_scene *scene, gq_vecs origin, gq_vecs dir, const float *r_max, int64_t n,
                              const gq_ray_out *out, void *stream);
@@ -216,6 +216,45 @@ gq_status gq_brute_f64(const gq_scene *scene, int32_t kind /*0 closest point, 1 
 
 /* Reads and clears the scene's device error word (stack overflow etc.); synchronises `stream`. */
 gq_status gq_scene_device_error(const gq_scene *scene, void *stream, int32_t *flags);
+
+/* ---- batches: many scenes, all three query kinds, one launch ----
+ * No counterpart in the reference, which answers one scene and one query kind per call
+ * (mesh.py:86-138, polyline.py:132-226).  A batch holds device views of up to
+ * thousands of scenes of one dimension on one device (the scenes must outlive it) and
+ * a fixed scratch sized for max_queries queries of each kind, so gq_batch_run
+ * allocates nothing and never synchronises: a step can be recorded in a CUDA graph.
+ * Each query carries the index of its scene in the batch.  Results are those of the
+ * single-scene calls: closest points follow GQ_VARIANT_COHERENT (or GQ_VARIANT_EXACT
+ * with GQ_BATCH_CP_EXACT), rays GQ_VARIANT_WIDE8 where the scene has wide nodes (or
+ * GQ_VARIANT_EXACT with GQ_BATCH_RAY_EXACT), silhouettes GQ_VARIANT_EXACT. */
+typedef struct gq_batch gq_batch;
+
+#define GQ_BATCH_CP_EXACT 1  /* closest point: one exact traversal per lane, reference visit order */
+#define GQ_BATCH_RAY_EXACT 2 /* rays: binary BVH, reference visit order */
+
+typedef struct {
+    int64_t n;             /* query count (0: none of this kind) */
+    const int32_t *scene;  /* device [n]: scene index in the batch; -1 marks a padding slot
+                              (skipped, its outputs left untouched) */
+    gq_vecs a;             /* points / ray origins */
+    gq_vecs b;             /* ray directions (rays only) */
+    const float *r_max;    /* device [n] or NULL for +inf (rays, silhouettes) */
+} gq_batch_queries;
+
+gq_status gq_batch_create(gq_scene *const *scenes, int32_t n_scenes, int64_t max_queries, int32_t flags,
+                          gq_batch **out);
+gq_status gq_batch_free(gq_batch *batch);
+/* Device bytes the batch holds besides its scenes. */
+int64_t gq_batch_device_bytes(const gq_batch *batch);
+/* Any of the query / output pointers may be NULL to skip that kind. */
+gq_status gq_batch_run(gq_batch *batch, const gq_batch_queries *cp, const gq_cp_out *cp_out,
+                       const gq_batch_queries *ray, const gq_ray_out *ray_out, const gq_batch_queries *sil,
+                       const gq_sil_out *sil_out, void *stream);
+/* Reads and clears the device error words of the batch and of every member scene;
+ * synchronises `stream`.  Bits 0-7: the scenes' words or-ed together (bit 0 stack
+ * overflow); bit 8: a query named a scene outside the batch; bit 9: a silhouette query
+ * named a scene without SNCH. */
+gq_status gq_batch_device_error(gq_batch *batch, void *stream, int32_t *flags);
 
 #ifdef __cplusplus
 }
