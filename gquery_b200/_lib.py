@@ -41,6 +41,7 @@ BATCH_CP_EXACT = 1
 BATCH_RAY_EXACT = 2
 BATCH_ERR_SCENE = 1 << 8
 BATCH_ERR_NO_SNCH = 1 << 9
+SERVER_PER_REQUEST = 4
 
 
 class BuildOpts(C.Structure):
@@ -81,6 +82,28 @@ class Tuning(C.Structure):
 class QueryOpts(C.Structure):
     _fields_ = [("variant", C.c_int32), ("sort", C.c_int32), ("order", C.c_void_p), ("scratch", C.c_void_p),
                 ("scratch_bytes", C.c_int64)]
+
+
+class ServerOpts(C.Structure):
+    _fields_ = [("budget_bytes", C.c_int64), ("ring_queries", C.c_int64 * 3), ("step_queries", C.c_int64),
+                ("max_inflight", C.c_int32), ("flags", C.c_int32)]
+
+
+class Request(C.Structure):
+    _fields_ = [("scene", C.c_int32), ("kind", C.c_int32), ("n", C.c_int64), ("a", C.c_void_p), ("b", C.c_void_p),
+                ("r_max", C.c_void_p), ("cp_out", CpOut), ("ray_out", RayOut), ("sil_out", SilOut),
+                ("tag", C.c_uint64)]
+
+
+class Completion(C.Structure):
+    _fields_ = [("tag", C.c_uint64), ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_launch", C.c_double),
+                ("t_done", C.c_double), ("n", C.c_int64), ("kind", C.c_int32), ("step", C.c_int32),
+                ("status", C.c_int32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("requests_done", C.c_int64), ("queries_done", C.c_int64), ("steps", C.c_int64),
+                ("admitted_bytes_peak", C.c_int64), ("device_bytes", C.c_int64), ("device_error", C.c_int32)]
 
 
 class BatchQueries(C.Structure):
@@ -126,6 +149,15 @@ SIGNATURES = {
     "gq_batch_run": (C.c_int32, [C.c_void_p, C.POINTER(BatchQueries), C.POINTER(CpOut), C.POINTER(BatchQueries),
                                  C.POINTER(RayOut), C.POINTER(BatchQueries), C.POINTER(SilOut), C.c_void_p]),
     "gq_batch_device_error": (C.c_int32, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)]),
+    "gq_server_clock": (C.c_double, []),
+    "gq_server_create": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(ServerOpts), C.POINTER(C.c_void_p)]),
+    "gq_server_free": (C.c_int32, [C.c_void_p]),
+    "gq_server_submit": (C.c_int32, [C.c_void_p, C.POINTER(Request)]),
+    "gq_server_poll": (C.c_int32, [C.c_void_p, C.POINTER(Completion), C.c_int64, C.POINTER(C.c_int64)]),
+    "gq_server_wait_idle": (C.c_int32, [C.c_void_p, C.c_double]),
+    "gq_server_get_stats": (C.c_int32, [C.c_void_p, C.POINTER(ServerStats)]),
+    "gq_server_run_trace": (C.c_int32, [C.c_void_p, C.POINTER(Request), C.c_void_p, C.c_int64,
+                                        C.POINTER(Completion), C.c_double]),
 }
 
 _lock = threading.Lock()

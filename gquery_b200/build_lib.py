@@ -19,7 +19,7 @@ ROOT = PKG.parent
 BUILD = ROOT / "_build" / "gq"
 LIB = PKG / "lib" / "libgq.so"
 
-HOST_SOURCES = ["host/scene_build.cpp", "host/flatten.cpp", "capi.cpp"]
+HOST_SOURCES = ["host/scene_build.cpp", "host/flatten.cpp", "capi.cpp", "server.cpp"]
 DEVICE_SOURCES = ["device/queries.cu", "device/traverse.cu", "device/packet.cu", "device/noalloc.cu", "device/batch.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

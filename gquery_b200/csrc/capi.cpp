@@ -13,16 +13,15 @@
 
 #include "../../include/gq.h"
 #include "device/batch.cuh"
-#include "device/queries.cuh"
-#include "host/flatten.hpp"
-#include "host/scene_build.hpp"
+#include "internal.hpp"
 
 using namespace gqb;
 
 namespace {
-
 thread_local std::string g_last_error;
+}  // namespace
 
+namespace gqi {
 gq_status fail(gq_status s, const std::string &msg) {
     g_last_error = msg;
     return s;
@@ -30,63 +29,11 @@ gq_status fail(gq_status s, const std::string &msg) {
 gq_status fail_cuda(cudaError_t e, const char *what) {
     return fail(GQ_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
+}  // namespace gqi
 
-struct DeviceGuard {
-    int prev = -1;
-    bool ok = true;
-    explicit DeviceGuard(int dev) {
-        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-        if (prev != dev) ok = cudaSetDevice(dev) == cudaSuccess;
-    }
-    ~DeviceGuard() {
-        int cur = -1;
-        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
-    }
-};
-
-}  // namespace
-
-struct gq_scene {
-    int dim = 0;
-    int device = 0;
-    std::vector<float> verts;
-    std::vector<int32_t> index;
-    int64_t nv = 0, np = 0;
-    BvhTree<2> t2;
-    BvhTree<3> t3;
-    SnchTree<2> s2;
-    SnchTree<3> s3;
-    bool has_snch = false, has_wide = false;
-    int exact_stack = 0, wide_stack = 0;
-    int64_t n_wide = 0, n_sil = 0;
-    std::vector<float> wide_words;  // host copy of the wide nodes (host-only scenes)
-    std::vector<void *> allocs;
-    int64_t device_bytes = 0;
-    gqd::DevScene dev{};
-    gq_tuning tune[3] = {};
-
-    ~gq_scene() {
-        if (device < 0 || allocs.empty()) return;
-        DeviceGuard g(device);
-        for (void *p : allocs) cudaFree(p);
-    }
-
-    template <typename T>
-    gq_status upload(const std::vector<T> &v, const void **dst) {
-        *dst = nullptr;
-        if (v.empty()) return GQ_OK;
-        void *p = nullptr;
-        const size_t bytes = v.size() * sizeof(T);
-        cudaError_t e = cudaMalloc(&p, bytes);
-        if (e != cudaSuccess) return fail(GQ_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-        allocs.push_back(p);
-        device_bytes += (int64_t)bytes;
-        e = cudaMemcpy(p, v.data(), bytes, cudaMemcpyHostToDevice);
-        if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpy");
-        *dst = p;
-        return GQ_OK;
-    }
-};
+using gqi::DeviceGuard;
+using gqi::fail;
+using gqi::fail_cuda;
 
 namespace {
 
@@ -196,6 +143,7 @@ bool on_host_only(const gq_scene *s) { return s->device < 0; }
 // Built-in launch choices (measured on B200 for the benchmark scenes).
 void default_tuning(gq_scene *s) {
     for (int k = 0; k < 3; ++k) s->tune[k] = gq_tuning{GQ_VARIANT_EXACT, 0, 1, 0, 32};
+    s->tune[GQ_KIND_SILHOUETTE].persist = 1;
     if (s->dim == 3) {
         s->tune[GQ_KIND_CLOSEST_POINT] = gq_tuning{GQ_VARIANT_COHERENT, 1, 1, 0, 32};
         s->tune[GQ_KIND_INTERSECT] = gq_tuning{s->has_wide ? GQ_VARIANT_WIDE8 : GQ_VARIANT_EXACT, 0, 1, 1, 32};
@@ -551,7 +499,8 @@ gq_status gq_closest_silhouette(const gq_scene *s, gq_vecs x, const float *r_max
     unsigned long long *counter = nullptr;
     gq_status st;
     if ((st = prepare_order(s, x, n, opts, cs, scr, &perm, &counter)) != GQ_OK) return st;
-    cudaError_t e = gqd::launch_sil(s->dev, x, r_max, n, perm, *out, cs);
+    const gq_tuning &t = s->tune[GQ_KIND_SILHOUETTE];
+    cudaError_t e = gqd::launch_sil(s->dev, x, r_max, n, perm, *out, t.persist ? counter : nullptr, t.budget, cs);
     if (e != cudaSuccess) return fail_cuda(e, "closest_silhouette launch");
     return GQ_OK;
 }
@@ -690,8 +639,11 @@ gq_status gq_batch_run(gq_batch *b, const gq_batch_queries *cp, const gq_cp_out 
     const gq_cp_out co = cp_out ? *cp_out : gq_cp_out{};
     const gq_ray_out ro = ray_out ? *ray_out : gq_ray_out{};
     const gq_sil_out so = sil_out ? *sil_out : gq_sil_out{};
+    bool all_wide = true;
+    for (const gq_scene *s : b->scenes) all_wide &= s->has_wide;
     cudaError_t e = gqd::batch_run(b->dev_scenes, (int)b->scenes.size(), b->dim, kinds, co, ro, so,
-                                   (b->flags & GQ_BATCH_RAY_EXACT) ? 0 : 1, (b->flags & GQ_BATCH_CP_EXACT) ? 0 : 1,
+                                   (b->flags & GQ_BATCH_RAY_EXACT) || !all_wide ? 0 : 1,
+                                   (b->flags & GQ_BATCH_CP_EXACT) ? 0 : 1,
                                    b->scratch, b->max_queries, b->err, (cudaStream_t)stream);
     if (e != cudaSuccess) return fail_cuda(e, "batch launch");
     return GQ_OK;

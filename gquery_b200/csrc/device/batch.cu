@@ -1,13 +1,13 @@
 // Many scenes, three query kinds, one persistent launch.
 //
-// Queries of each kind are sorted by (scene, Morton code inside the scene's box), then
-// cut into tiles of 32.  Persistent warps take tiles from one counter in the order
-// closest point, rays, silhouettes, so a warp always runs one query kind (a
-// warp-uniform branch).  Closest-point tiles run the warp-coherent traversal once per
-// distinct scene in the tile (tiles straddle at most a scene boundary or two); ray and
-// silhouette tiles run one traversal per lane on the lane's own scene.  Every launch
-// input lives in caller- or batch-owned device memory, so a step can be captured in a
-// CUDA graph.
+// Queries of each kind are sorted by (scene, Morton code inside the scene's box).
+// Persistent warps work through the kinds in the order closest point, rays,
+// silhouettes (a warp-uniform phase).  Closest points run as tiles of 32 sorted
+// queries with the warp-coherent traversal once per distinct scene in the tile
+// (tiles straddle at most a scene boundary or two); rays and silhouettes run one
+// traversal per lane on the lane's own scene, and a lane whose query is done takes
+// the next one.  Every launch input lives in caller- or batch-owned device memory,
+// so a step can be captured in a CUDA graph.
 #include <cub/cub.cuh>
 
 #include "batch.cuh"
@@ -97,24 +97,64 @@ __device__ __forceinline__ void put_sil(const gq_sil_out &o, int64_t n, int64_t 
     if (o.prim_id) o.prim_id[qi] = found ? bid : 0;
 }
 
-// Warp tiles of 32 sorted queries: closest-point tiles first, then rays, then silhouettes.
-template <int D>
+// Lane-refill loop over the n sorted queries of one kind (persistent warps): a lane
+// without a query claims the next one through a warp-aggregated atomic on `counter`;
+// `start(i)` sets it up and says whether it needs a traversal (padding slots and bad
+// scene indices do not), `step(budget)` runs up to `budget` steps and says whether
+// the query is done, `finish()` writes its record.
+template <class Start, class Step, class Finish>
+__device__ __forceinline__ void refill(int64_t n, unsigned long long *counter, int budget, Start start, Step step,
+                                       Finish finish) {
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned below = (1u << lane) - 1u;
+    bool live = false, drained = false;
+    for (;;) {
+        if (!drained) {
+            const unsigned need = __ballot_sync(0xffffffffu, !live);
+            if (need) {
+                const int leader = __ffs(need) - 1;
+                unsigned long long base = 0;
+                if ((int)lane == leader) base = atomicAdd(counter, (unsigned long long)__popc(need));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (base + __popc(need) >= (unsigned long long)n) drained = true;
+                if (!live) {
+                    const unsigned long long mine = base + __popc(need & below);
+                    if (mine < (unsigned long long)n) live = start((int64_t)mine);
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, live)) {
+            if (drained) break;
+            continue;
+        }
+        if (live && step(budget)) {
+            finish();
+            live = false;
+        }
+    }
+}
+
+// One persistent launch per step.  Phase 1: closest points, as warp tiles of 32
+// sorted queries (warp-coherent traversal once per distinct scene in the tile) or,
+// in exact mode, one lane per query.  Phase 2: rays, phase 3: silhouettes, one lane
+// per query.  Every warp moves to the next phase when the current one has no
+// unclaimed work, so the phases' tails overlap.  counter[0..2]: claims per phase.
+template <int D, bool RAYW>
 __global__ void __launch_bounds__(kBlock) k_batch(const DevScene *scenes, int n_scenes, BatchKind cp, gq_cp_out cp_out,
                                                   BatchKind ray, gq_ray_out ray_out, BatchKind sil,
-                                                  gq_sil_out sil_out, int ray_wide, int cp_coherent,
+                                                  gq_sil_out sil_out, int cp_coherent, int budget,
                                                   unsigned long long *counter, int32_t *err) {
     const unsigned lane = threadIdx.x & 31u;
-    const int64_t t_cp = (cp.n + 31) / 32, t_ray = (ray.n + 31) / 32, t_sil = (sil.n + 31) / 32;
-    const int64_t tiles = t_cp + t_ray + t_sil;
-    for (;;) {
-        unsigned long long t = 0;
-        if (lane == 0) t = atomicAdd(counter, 1ull);
-        t = __shfl_sync(0xffffffffu, t, 0);
-        if (t >= (unsigned long long)tiles) break;
-        int64_t tt = (int64_t)t;
-        if (tt < t_cp) {
-            // ---- closest point ----
-            const int64_t i = tt * 32 + lane;
+    // ---------------- phase 1: closest points ----------------
+    if (cp_coherent) {
+        const int64_t t_cp = (cp.n + 31) / 32;
+        int2 stk[pkt::kPStack];
+        for (;;) {
+            unsigned long long t = 0;
+            if (lane == 0) t = atomicAdd(&counter[0], 1ull);
+            t = __shfl_sync(0xffffffffu, t, 0);
+            if (t >= (unsigned long long)t_cp) break;
+            const int64_t i = (int64_t)t * 32 + lane;
             const bool in = i < cp.n;
             const int64_t qi = in ? (int64_t)__ldg(cp.perm + i) : 0;
             const int sid = in ? __ldg(cp.scene + qi) : GQ_BATCH_SKIP;
@@ -126,31 +166,19 @@ __global__ void __launch_bounds__(kBlock) k_batch(const DevScene *scenes, int n_
             for (int k = 0; k < D; ++k) p[k] = alive ? qget(cp.a, qi, k) : 0.f;
             int best_idx = -1;
             bool ovf = false;
-            if (cp_coherent) {
-                int2 stk[pkt::kPStack];
-                unsigned todo = __ballot_sync(0xffffffffu, alive);
-                while (todo) {
-                    const int s0 = __shfl_sync(0xffffffffu, sid, __ffs(todo) - 1);
-                    const unsigned m = __ballot_sync(0xffffffffu, alive && sid == s0);
-                    float r = kInf;
-                    int idx = -1;
-                    bool o = false;
-                    pkt::closest_point<D, 0, false>(scenes[s0], m, p, r, idx, o, stk);
-                    if ((m >> lane) & 1u) {
-                        best_idx = idx;
-                        ovf = o;
-                    }
-                    todo &= ~m;
+            unsigned todo = __ballot_sync(0xffffffffu, alive);
+            while (todo) {
+                const int s0 = __shfl_sync(0xffffffffu, sid, __ffs(todo) - 1);
+                const unsigned m = __ballot_sync(0xffffffffu, alive && sid == s0);
+                float r = kInf;
+                int idx = -1;
+                bool o = false;
+                pkt::closest_point<D, 0, false>(scenes[s0], m, p, r, idx, o, stk);
+                if ((m >> lane) & 1u) {
+                    best_idx = idx;
+                    ovf = o;
                 }
-            } else if (alive) {
-                trav::Stack<false> stk;
-                trav::Lane<D, false, false> L;
-                const gq_vecs none{};
-                trav::lane_init(scenes[sid], L, cp.a, none, nullptr, qi);
-                while (!trav::lane_run<D, false, false, 0>(scenes[sid], L, stk, 1 << 30)) {
-                }
-                best_idx = L.idx;
-                ovf = L.ovf;
+                todo &= ~m;
             }
             if (!skip) {
                 const DevScene &s = scenes[alive ? sid : 0];
@@ -161,76 +189,111 @@ __global__ void __launch_bounds__(kBlock) k_batch(const DevScene *scenes, int n_
                 else
                     cp2_record(s.prims, best_idx, found, p[0], p[D - 1], cp_out, cp.n, qi);
             }
-            continue;
         }
-        tt -= t_cp;
-        if (tt < t_ray) {
-            // ---- rays: one traversal per lane ----
-            const int64_t i = tt * 32 + lane;
-            if (i < ray.n) {
-                const int64_t qi = (int64_t)__ldg(ray.perm + i);
+    } else if (cp.n > 0) {
+        trav::Stack<false> stk;
+        trav::Lane<D, false, false> L;
+        const DevScene *sc = scenes;
+        int64_t qi = 0;
+        const gq_vecs none{};
+        refill(
+            cp.n, &counter[0], budget,
+            [&](int64_t i) {
+                qi = (int64_t)__ldg(cp.perm + i);
+                const int sid = __ldg(cp.scene + qi);
+                if (sid == GQ_BATCH_SKIP) return false;
+                if ((unsigned)sid >= (unsigned)n_scenes) {
+                    atomicOr(err, GQ_BATCH_ERR_SCENE);
+                    if (D == 3)
+                        cp3_record(nullptr, -1, false, 0.f, 0.f, 0.f, cp_out, cp.n, qi);
+                    else
+                        cp2_record(nullptr, -1, false, 0.f, 0.f, cp_out, cp.n, qi);
+                    return false;
+                }
+                sc = scenes + sid;
+                trav::lane_init(*sc, L, cp.a, none, nullptr, qi);
+                return true;
+            },
+            [&](int b) { return trav::lane_run<D, false, false, 0>(*sc, L, stk, b); },
+            [&]() { trav::lane_write(*sc, L, qi, cp.n, cp_out, gq_ray_out{}); });
+    }
+    // ---------------- phase 2: rays ----------------
+    if (ray.n > 0) {
+        trav::Stack<RAYW> stk;
+        trav::Lane<D, true, RAYW> L;
+        const DevScene *sc = scenes;
+        int64_t qi = 0;
+        refill(
+            ray.n, &counter[1], budget,
+            [&](int64_t i) {
+                qi = (int64_t)__ldg(ray.perm + i);
                 const int sid = __ldg(ray.scene + qi);
-                if (sid == GQ_BATCH_SKIP) {
-                } else if ((unsigned)sid >= (unsigned)n_scenes) {
+                if (sid == GQ_BATCH_SKIP) return false;
+                if ((unsigned)sid >= (unsigned)n_scenes) {
                     atomicOr(err, GQ_BATCH_ERR_SCENE);
                     if (D == 3)
                         ray3_record(nullptr, -1, false, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, ray_out, ray.n, qi);
                     else
                         ray2_record(nullptr, -1, false, 0.f, 0.f, 0.f, 0.f, 0.f, ray_out, ray.n, qi);
-                } else {
-                    const DevScene &s = scenes[sid];
-                    if (ray_wide && s.wnodes) {
-                        trav::Stack<true> stk;
-                        trav::Lane<D, true, true> L;
-                        trav::lane_init(s, L, ray.a, ray.b, ray.r_max, qi);
-                        while (!trav::lane_run<D, true, true, 0>(s, L, stk, 1 << 30)) {
-                        }
-                        trav::lane_write(s, L, qi, ray.n, gq_cp_out{}, ray_out);
-                    } else {
-                        trav::Stack<false> stk;
-                        trav::Lane<D, true, false> L;
-                        trav::lane_init(s, L, ray.a, ray.b, ray.r_max, qi);
-                        while (!trav::lane_run<D, true, false, 0>(s, L, stk, 1 << 30)) {
-                        }
-                        trav::lane_write(s, L, qi, ray.n, gq_cp_out{}, ray_out);
-                    }
+                    return false;
                 }
-            }
-            continue;
-        }
-        tt -= t_ray;
-        {
-            // ---- silhouettes: one traversal per lane ----
-            const int64_t i = tt * 32 + lane;
-            if (i < sil.n) {
-                const int64_t qi = (int64_t)__ldg(sil.perm + i);
-                const int sid = __ldg(sil.scene + qi);
-                if (sid == GQ_BATCH_SKIP) continue;
-                float bp[D], bd = 0.f;
-                int bid = 0;
-                bool found = false, ovf = false;
-                if ((unsigned)sid >= (unsigned)n_scenes) {
-                    atomicOr(err, GQ_BATCH_ERR_SCENE);
-                } else {
-                    const DevScene &s = scenes[sid];
-                    float x[D];
-#pragma unroll
-                    for (int k = 0; k < D; ++k) x[k] = qget(sil.a, qi, k);
-                    const float r_max = sil.r_max ? sil.r_max[qi] : kInf;
-                    if (s.spairs) {
-                        snch::closest_silhouette<D>(s, x, r_max, found, bp, bd, bid, ovf);
-                    } else {
-                        atomicOr(err, GQ_BATCH_ERR_NO_SNCH);
-                    }
-                    if (ovf) {
-                        if (s.err) atomicOr(s.err, GQ_DEVERR_STACK);
-                        found = false;
-                    }
-                }
-                put_sil<D>(sil_out, sil.n, qi, found, bp, bd, bid);
-            }
-        }
+                sc = scenes + sid;
+                trav::lane_init(*sc, L, ray.a, ray.b, ray.r_max, qi);
+                return true;
+            },
+            [&](int b) { return trav::lane_run<D, true, RAYW, 0>(*sc, L, stk, b); },
+            [&]() { trav::lane_write(*sc, L, qi, ray.n, gq_cp_out{}, ray_out); });
     }
+    // ---------------- phase 3: silhouettes ----------------
+    if (sil.n > 0) {
+        snch::Stack stk;
+        snch::Lane<D> L;
+        const DevScene *sc = scenes;
+        int64_t qi = 0;
+        refill(
+            sil.n, &counter[2], budget,
+            [&](int64_t i) {
+                qi = (int64_t)__ldg(sil.perm + i);
+                const int sid = __ldg(sil.scene + qi);
+                if (sid == GQ_BATCH_SKIP) return false;
+                float x[D];
+#pragma unroll
+                for (int k = 0; k < D; ++k) x[k] = qget(sil.a, qi, k);
+                if ((unsigned)sid >= (unsigned)n_scenes || !scenes[sid].spairs) {
+                    atomicOr(err, (unsigned)sid >= (unsigned)n_scenes ? GQ_BATCH_ERR_SCENE : GQ_BATCH_ERR_NO_SNCH);
+                    put_sil<D>(sil_out, sil.n, qi, false, x, 0.f, 0);
+                    return false;
+                }
+                sc = scenes + sid;
+                snch::lane_init<D>(*sc, L, x, sil.r_max ? sil.r_max[qi] : kInf, stk);
+                return true;
+            },
+            [&](int b) { return snch::lane_run<D>(*sc, L, stk, b); },
+            [&]() {
+                if (L.ovf && sc->err) atomicOr(sc->err, GQ_DEVERR_STACK);
+                put_sil<D>(sil_out, sil.n, qi, L.found && !L.ovf, L.bp, L.bd, L.bid);
+            });
+    }
+}
+
+template <int D, bool RAYW>
+cudaError_t launch_batch(const DevScene *scenes_dev, int n_scenes, BatchKind kinds[3], const gq_cp_out &cp_out,
+                         const gq_ray_out &ray_out, const gq_sil_out &sil_out, int cp_coherent,
+                         unsigned long long *counter, int32_t *err, cudaStream_t st) {
+    static int bps = 0, n_sm = 0;
+    if (!bps) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_batch<D, RAYW>, kBlock, 0);
+        if (bps < 1) bps = 1;
+    }
+    const int64_t most = std::max(kinds[0].n, std::max(kinds[1].n, kinds[2].n));
+    if (most <= 0) return cudaSuccess;
+    const int64_t want = std::min<int64_t>((int64_t)bps * n_sm, (most + kBlock - 1) / kBlock);
+    k_batch<D, RAYW><<<dim3((unsigned)want), kBlock, 0, st>>>(scenes_dev, n_scenes, kinds[0], cp_out, kinds[1], ray_out,
+                                                              kinds[2], sil_out, cp_coherent, 32, counter, err);
+    return cudaGetLastError();
 }
 
 inline size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
@@ -282,30 +345,17 @@ cudaError_t batch_run(const DevScene *scenes_dev, int n_scenes, int dim, BatchKi
         e = cub::DeviceRadixSort::SortPairs(temp, tbk, k_in, k_out, v_in, perm, (int)q.n, 0, end_bit, st);
         if (e != cudaSuccess) return e;
     }
-    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
+    cudaError_t e = cudaMemsetAsync(counter, 0, 3 * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
-    static int bps[2] = {0, 0}, n_sm = 0;
-    const int di = dim == 3 ? 1 : 0;
-    if (!bps[di]) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-        if (dim == 3)
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps[1], k_batch<3>, kBlock, 0);
-        else
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps[0], k_batch<2>, kBlock, 0);
-        if (bps[di] < 1) bps[di] = 1;
-    }
-    const int64_t tiles = (kinds[0].n + 31) / 32 + (kinds[1].n + 31) / 32 + (kinds[2].n + 31) / 32;
-    if (tiles == 0) return cudaSuccess;
-    const int64_t want = std::min<int64_t>((int64_t)bps[di] * n_sm, (tiles * 32 + kBlock - 1) / kBlock);
     if (dim == 3)
-        k_batch<3><<<dim3((unsigned)want), kBlock, 0, st>>>(scenes_dev, n_scenes, kinds[0], cp_out, kinds[1], ray_out, kinds[2],
-                                                            sil_out, ray_wide, cp_coherent, counter, err);
-    else
-        k_batch<2><<<dim3((unsigned)want), kBlock, 0, st>>>(scenes_dev, n_scenes, kinds[0], cp_out, kinds[1], ray_out, kinds[2],
-                                                            sil_out, ray_wide, cp_coherent, counter, err);
-    return cudaGetLastError();
+        return ray_wide ? launch_batch<3, true>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_coherent,
+                                                counter, err, st)
+                        : launch_batch<3, false>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_coherent,
+                                                 counter, err, st);
+    return ray_wide ? launch_batch<2, true>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_coherent, counter,
+                                            err, st)
+                    : launch_batch<2, false>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_coherent, counter,
+                                             err, st);
 }
 
 }  // namespace gqd

@@ -23,7 +23,7 @@ struct BatchKind {
 size_t batch_scratch_bytes(int64_t max_n);
 
 // kinds[0] closest point, kinds[1] rays, kinds[2] silhouettes (n = 0 to skip a kind).
-// ray_wide: rays on the quantised 8-wide BVH where a scene has one; cp_coherent:
+// ray_wide: rays on the quantised 8-wide BVH (every scene must have it); cp_coherent:
 // warp-coherent closest point (else one exact traversal per lane).  No allocation and
 // no host synchronisation: the call can be recorded in a CUDA graph.
 cudaError_t batch_run(const DevScene *scenes_dev, int n_scenes, int dim, BatchKind kinds[3], const gq_cp_out &cp_out,

@@ -3,6 +3,8 @@
 // traversals live in traverse.cu.  Compiled with --fmad=false (see gq_fmath.h).
 #include <cub/cub.cuh>
 
+#include <algorithm>
+
 #include "prim.cuh"
 #include "queries.cuh"
 #include "records.cuh"
@@ -30,32 +32,83 @@ __device__ __forceinline__ int64_t query_index(const int32_t *perm, int64_t i) {
 // Closest silhouette (SNCH), binary exact
 // ===========================================================================
 
-// SNCH.closest_silhouette (snch.py:106-164) and SNCH3D.closest_silhouette (snch3d.py:143-203)
 template <int D>
-__global__ void __launch_bounds__(kBlock) k_sil_exact(DevScene s, gq_vecs xq, const float *rmax_in, int64_t n,
-                                                       const int32_t *perm, gq_sil_out o) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int64_t qi = query_index(perm, i);
-    float x[D];
-#pragma unroll
-    for (int k = 0; k < D; ++k) x[k] = qget(xq, qi, k);
-    float r_max = rmax_in ? rmax_in[qi] : kInf;
-    bool found, ovf;
-    float bp[D], bd;
-    int bid;
-    snch::closest_silhouette<D>(s, x, r_max, found, bp, bd, bid, ovf);
-    if (ovf) {
-        flag_error(s.err, GQ_DEVERR_STACK);
-        found = false;
-    }
+__device__ __forceinline__ void sil_write(const DevScene &s, const snch::Lane<D> &L, int64_t qi, int64_t n,
+                                          const gq_sil_out &o) {
+    const bool found = L.found && !L.ovf;
+    if (L.ovf) flag_error(s.err, GQ_DEVERR_STACK);
     if (o.valid) o.valid[qi] = found ? 1 : 0;
     if (o.p) {
 #pragma unroll
-        for (int k = 0; k < D; ++k) o.p[k * n + qi] = found ? bp[k] : 0.f;
+        for (int k = 0; k < D; ++k) o.p[k * n + qi] = found ? L.bp[k] : 0.f;
     }
-    put1(o.d, qi, found ? bd : 0.f);
-    if (o.prim_id) o.prim_id[qi] = found ? bid : 0;
+    put1(o.d, qi, found ? L.bd : 0.f);
+    if (o.prim_id) o.prim_id[qi] = found ? L.bid : 0;
+}
+
+template <int D>
+__device__ __forceinline__ void sil_start(const DevScene &s, snch::Lane<D> &L, int2 *stk, gq_vecs xq,
+                                          const float *rmax_in, int64_t qi) {
+    float x[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) x[k] = qget(xq, qi, k);
+    snch::lane_init<D>(s, L, x, rmax_in ? rmax_in[qi] : kInf, stk);
+}
+
+// One query per thread: SNCH.closest_silhouette (snch.py:106-164) and
+// SNCH3D.closest_silhouette (snch3d.py:143-203).
+template <int D>
+__global__ void __launch_bounds__(kBlock) k_sil_exact(DevScene s, gq_vecs xq, const float *rmax_in, int64_t n,
+                                                      const int32_t *perm, gq_sil_out o) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t qi = query_index(perm, i);
+    snch::Stack stk;
+    snch::Lane<D> L;
+    sil_start<D>(s, L, stk, xq, rmax_in, qi);
+    while (!snch::lane_run<D>(s, L, stk, 1 << 30)) {
+    }
+    sil_write<D>(s, L, qi, n, o);
+}
+
+// Persistent warps with lane refill: a lane whose query is done takes the next one
+// (warp-aggregated atomic on a per-call counter), so a warp never waits for its
+// slowest query.  Same visit order and answers as k_sil_exact.
+template <int D>
+__global__ void __launch_bounds__(kBlock) k_sil_persist(DevScene s, gq_vecs xq, const float *rmax_in, int64_t n,
+                                                        const int32_t *perm, gq_sil_out o,
+                                                        unsigned long long *counter, int budget) {
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned below = (1u << lane) - 1u;
+    snch::Stack stk;
+    snch::Lane<D> L;
+    int64_t qi = -1;
+    bool live = false, drained = false;
+    for (;;) {
+        if (!drained) {
+            const unsigned need = __ballot_sync(0xffffffffu, !live);
+            if (need) {
+                const int leader = __ffs(need) - 1;
+                unsigned long long base = 0;
+                if ((int)lane == leader) base = atomicAdd(counter, (unsigned long long)__popc(need));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (base + __popc(need) >= (unsigned long long)n) drained = true;
+                if (!live) {
+                    const unsigned long long mine = base + __popc(need & below);
+                    if (mine < (unsigned long long)n) {
+                        qi = query_index(perm, (int64_t)mine);
+                        sil_start<D>(s, L, stk, xq, rmax_in, qi);
+                        live = true;
+                    }
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, live)) break;
+        if (live && snch::lane_run<D>(s, L, stk, budget)) {
+            sil_write<D>(s, L, qi, n, o);
+            live = false;
+        }
+    }
 }
 
 // ===========================================================================
@@ -453,8 +506,31 @@ cudaError_t morton_order(const DevScene &s, gq_vecs q, int64_t n, int32_t *perm,
 }
 
 cudaError_t launch_sil(const DevScene &s, gq_vecs x, const float *r_max, int64_t n, const int32_t *perm,
-                       const gq_sil_out &o, cudaStream_t st) {
+                       const gq_sil_out &o, unsigned long long *counter, int budget, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
+    if (counter && n > 4096) {
+        static int bps[2] = {0, 0}, n_sm = 0;
+        const int di = s.dim == 3 ? 1 : 0;
+        if (!bps[di]) {
+            int dev = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+            if (s.dim == 3)
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps[1], k_sil_persist<3>, kBlock, 0);
+            else
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps[0], k_sil_persist<2>, kBlock, 0);
+            if (bps[di] < 1) bps[di] = 1;
+        }
+        const int64_t want = std::min<int64_t>((int64_t)bps[di] * n_sm, (n + kBlock - 1) / kBlock);
+        cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
+        if (e != cudaSuccess) return e;
+        const int b = budget > 0 ? budget : 32;
+        if (s.dim == 3)
+            k_sil_persist<3><<<dim3((unsigned)want), kBlock, 0, st>>>(s, x, r_max, n, perm, o, counter, b);
+        else
+            k_sil_persist<2><<<dim3((unsigned)want), kBlock, 0, st>>>(s, x, r_max, n, perm, o, counter, b);
+        return cudaGetLastError();
+    }
     if (s.dim == 3)
         k_sil_exact<3><<<grid_for(n), kBlock, 0, st>>>(s, x, r_max, n, perm, o);
     else

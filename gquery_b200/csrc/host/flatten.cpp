@@ -4,9 +4,24 @@
 #include <cmath>
 #include <cstring>
 
+#include "../gq_fmath.h"
+
 namespace gqb {
 
 namespace {
+
+// normalize(cross(u, v)) with the FP32 operations of the device's per-edge test
+// (cross in fused form, normalize = v * (1 / sqrt(dot(v, v)))), so the stored normal
+// is bit-identical to the one the traversal would compute.
+void face_normal(float ux, float uy, float uz, float vx, float vy, float vz, float &nx, float &ny, float &nz) {
+    const float cx = gq_fma(uy, vz, -(uz * vy));
+    const float cy = gq_fma(uz, vx, -(ux * vz));
+    const float cz = gq_fma(ux, vy, -(uy * vx));
+    const float inv = gq_rsqrt(gq_dot3(cx, cy, cz, cx, cy, cz));
+    nx = cx * inv;
+    ny = cy * inv;
+    nz = cz * inv;
+}
 
 // Preorder rank of every interior node (the index of its pair record), -1 for leaves.
 template <int D>
@@ -349,8 +364,11 @@ void flatten_snch(const BvhTree<D> &t, const SnchTree<D> &s, DeviceImage<D> &img
             // SilhouetteEdges view (silhouette_edge.py:75-86): c = v[0], a = v[1], b = v[2], d = v[3]
             r.ax = x.v[1].v[0]; r.ay = x.v[1].v[1]; r.az = x.v[1].v[2];
             r.bx = x.v[2].v[0]; r.by = x.v[2].v[1]; r.bz = x.v[2].v[2];
-            r.cx = x.v[0].v[0]; r.cy = x.v[0].v[1]; r.cz = x.v[0].v[2];
-            r.dx = x.v[3].v[0]; r.dy = x.v[3].v[1]; r.dz = x.v[3].v[2];
+            const float cx = x.v[0].v[0], cy = x.v[0].v[1], cz = x.v[0].v[2];
+            const float dx = x.v[3].v[0], dy = x.v[3].v[1], dz = x.v[3].v[2];
+            // n0 = normalize(cross(b - a, c - a)), n1 = normalize(cross(d - a, b - a))
+            face_normal(r.bx - r.ax, r.by - r.ay, r.bz - r.az, cx - r.ax, cy - r.ay, cz - r.az, r.n0x, r.n0y, r.n0z);
+            face_normal(dx - r.ax, dy - r.ay, dz - r.az, r.bx - r.ax, r.by - r.ay, r.bz - r.az, r.n1x, r.n1y, r.n1z);
             r.prim = (int32_t)(float)x.prim;
             // silhouette_edge.py:56-57: boundary marker index == -1 never occurs (size_t storage)
             const bool boundary = ((int64_t)(float)x.idx[0] == -1) || ((int64_t)(float)x.idx[3] == -1);

@@ -1,0 +1,77 @@
+// Internal declarations shared by the C-ABI translation units (capi.cpp, server.cpp).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/gq.h"
+#include "device/queries.cuh"
+#include "host/flatten.hpp"
+#include "host/scene_build.hpp"
+
+namespace gqi {
+
+// Records `msg` as the calling thread's last error and returns `s`.
+gq_status fail(gq_status s, const std::string &msg);
+gq_status fail_cuda(cudaError_t e, const char *what);
+
+// Selects `dev` for the lifetime of the guard and restores the previous device.
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = true;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) ok = cudaSetDevice(dev) == cudaSuccess;
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace gqi
+
+struct gq_scene {
+    int dim = 0;
+    int device = 0;
+    std::vector<float> verts;
+    std::vector<int32_t> index;
+    int64_t nv = 0, np = 0;
+    gqb::BvhTree<2> t2;
+    gqb::BvhTree<3> t3;
+    gqb::SnchTree<2> s2;
+    gqb::SnchTree<3> s3;
+    bool has_snch = false, has_wide = false;
+    int exact_stack = 0, wide_stack = 0;
+    int64_t n_wide = 0, n_sil = 0;
+    std::vector<float> wide_words;  // host copy of the wide nodes (host-only scenes)
+    std::vector<void *> allocs;
+    int64_t device_bytes = 0;
+    gqd::DevScene dev{};
+    gq_tuning tune[3] = {};
+
+    ~gq_scene() {
+        if (device < 0 || allocs.empty()) return;
+        gqi::DeviceGuard g(device);
+        for (void *p : allocs) cudaFree(p);
+    }
+
+    template <typename T>
+    gq_status upload(const std::vector<T> &v, const void **dst) {
+        *dst = nullptr;
+        if (v.empty()) return GQ_OK;
+        void *p = nullptr;
+        const size_t bytes = v.size() * sizeof(T);
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) return gqi::fail(GQ_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        allocs.push_back(p);
+        device_bytes += (int64_t)bytes;
+        e = cudaMemcpy(p, v.data(), bytes, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return gqi::fail_cuda(e, "cudaMemcpy");
+        *dst = p;
+        return GQ_OK;
+    }
+};

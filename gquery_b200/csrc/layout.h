@@ -63,11 +63,13 @@ typedef struct {
     int32_t prim, flags;
 } gq_silv_t;
 
-// 3D silhouette edge (a, b end points; c, d opposite vertices)            64 B
+// 3D silhouette edge: end points a, b and the unit normals of its two faces,
+// n0 of (a, b, c) and n1 of (a, d, b), computed once on the host with the
+// FP32 operations the reference applies per test (silhouette_edge.py:28-34).   64 B
 typedef struct {
     float ax, ay, az, bx;
-    float by, bz, cx, cy;
-    float cz, dx, dy, dz;
+    float by, bz, n0x, n0y;
+    float n0z, n1x, n1y, n1z;
     int32_t prim, flags, pad0, pad1;
 } gq_sile_t;
 

@@ -137,3 +137,14 @@ def config3_queries(scenes, n_total: int = 1 << 24, mix=(0.5, 0.3, 0.2), seed: i
             else:
                 parts[kind].append((ids, pts))
     return {k: tuple(np.concatenate(col) for col in zip(*v)) for k, v in parts.items()}
+
+
+def config4_levels(n_scenes: int = 64, lo: int = 4, hi: int = 8, seed: int = 11):
+    """Subdivision level of each served scene: uniform over lo..hi, seeded."""
+    rng = np.random.default_rng(seed)
+    return [int(x) for x in rng.integers(lo, hi + 1, size=n_scenes)]
+
+
+def config4_scene(sid: int, level: int):
+    """Served scene `sid`: icosphere of `level` displaced with amplitude 0.15 (seed = 1000 + sid)."""
+    return icosphere(level, amplitude=0.15, seed=1000 + sid)

@@ -46,7 +46,7 @@ typedef int32_t gq_status;
 #define GQ_VARIANT_EXACT 0    /* binary tree, gQuery's visit order: reference-identical answers */
 #define GQ_VARIANT_WIDE8 1    /* 8-wide nodes, 8-bit outward-rounded child boxes */
 #define GQ_VARIANT_AUTO 2     /* the scene's tuned choice for the query kind (gq_scene_set_tuning) */
-#define GQ_VARIANT_COHERENT 3 /* binary tree walked once per warp of Morton-adjacent queries (3D closest
+#define GQ_VARIANT_COHERENT 3 /* binary tree walked once per warp of Morton-adjacent queries (closest
                                  point); other query kinds run as EXACT */
 /* All variants other than EXACT give the same answers as EXACT except at FP32 distance
  * ties (distances within 2e-6 relative). */
@@ -255,6 +255,75 @@ gq_status gq_batch_run(gq_batch *batch, const gq_batch_queries *cp, const gq_cp_
  * overflow); bit 8: a query named a scene outside the batch; bit 9: a silhouette query
  * named a scene without SNCH. */
 gq_status gq_batch_device_error(gq_batch *batch, void *stream, int32_t *flags);
+
+/* ---- serving: continuous batching of requests against resident scenes ----
+ * No counterpart in the reference.  A server owns a worker thread, device rings for
+ * request data (inputs and results of each query kind) and pinned host mirrors of
+ * them.  Requests (one scene, one query kind, n queries in host memory) may be
+ * submitted from any thread at any time.  The worker admits a request when its ring
+ * has room (the rings are the admission budget: their device bytes may not exceed
+ * budget_bytes), copies its queries to the device at once on a copy stream while
+ * earlier steps compute, and launches a step over every admitted request as soon as
+ * one of max_inflight step slots is free: one gq_batch launch for all scenes and
+ * kinds (or, with GQ_SERVER_PER_REQUEST, one single-scene call per request, the
+ * scene's tuned variant).  Each slot has its own stream, so the results of one step
+ * go back to the host while the next computes.  Results are those of gq_batch_run. */
+typedef struct gq_server gq_server;
+
+#define GQ_SERVER_PER_REQUEST 4 /* one single-scene launch per request instead of batched steps */
+
+typedef struct {
+    int64_t budget_bytes;     /* device bytes the request rings may hold (0: no limit) */
+    int64_t ring_queries[3];  /* ring capacity in queries per kind (0: 1<<22) */
+    int64_t step_queries;     /* most queries of one kind in one step, and the largest request (0: 1<<19) */
+    int32_t max_inflight;     /* step slots (0: 2) */
+    int32_t flags;            /* GQ_BATCH_CP_EXACT | GQ_BATCH_RAY_EXACT | GQ_SERVER_PER_REQUEST */
+} gq_server_opts;
+
+typedef struct {
+    int32_t scene;       /* index into the server's scenes */
+    int32_t kind;        /* GQ_KIND_* */
+    int64_t n;           /* queries, 1 .. step_queries */
+    const float *a;      /* host [n][D]: points / ray origins */
+    const float *b;      /* host [n][D]: ray directions (rays only) */
+    const float *r_max;  /* host [n] or NULL for +inf (rays, silhouettes) */
+    gq_cp_out cp_out;    /* host results of a closest-point request ([D][n] fields) */
+    gq_ray_out ray_out;  /* host results of a ray request */
+    gq_sil_out sil_out;  /* host results of a silhouette request */
+    uint64_t tag;        /* returned with the completion */
+} gq_request;
+
+typedef struct {
+    uint64_t tag;
+    double t_submit, t_admit, t_launch, t_done; /* seconds on gq_server_clock() */
+    int64_t n;
+    int32_t kind;
+    int32_t step;        /* step that answered it */
+    int32_t status;      /* GQ_OK, or the error of the launch that served it */
+} gq_completion;
+
+typedef struct {
+    int64_t requests_done, queries_done, steps, admitted_bytes_peak, device_bytes;
+    int32_t device_error; /* or-ed error words of the step slots and scenes (gq_batch_device_error bits) */
+} gq_server_stats;
+
+double gq_server_clock(void);
+gq_status gq_server_create(gq_scene *const *scenes, int32_t n_scenes, const gq_server_opts *opts,
+                           gq_server **out);
+/* Stops the worker after the steps in flight; requests not yet answered are dropped. */
+gq_status gq_server_free(gq_server *server);
+/* Non-blocking; the request's host buffers must stay valid until its completion. */
+gq_status gq_server_submit(gq_server *server, const gq_request *request);
+/* Moves up to cap completions into out; *count = how many. */
+gq_status gq_server_poll(gq_server *server, gq_completion *out, int64_t cap, int64_t *count);
+/* Blocks until every submitted request has completed or timeout_s passed (GQ_ERR_DEVICE on timeout). */
+gq_status gq_server_wait_idle(gq_server *server, double timeout_s);
+gq_status gq_server_get_stats(gq_server *server, gq_server_stats *stats);
+/* Open-loop driver for an otherwise idle server: submits reqs[i] at start + t_arrival[i]
+ * seconds (start = now), waits for all, and writes each request's completion to out[i]
+ * with t_submit set to its scheduled arrival time. */
+gq_status gq_server_run_trace(gq_server *server, const gq_request *reqs, const double *t_arrival, int64_t n,
+                              gq_completion *out, double timeout_s);
 
 #ifdef __cplusplus
 }
