@@ -39,6 +39,7 @@ DEVERR_STACK = 1
 
 BATCH_CP_EXACT = 1
 BATCH_RAY_EXACT = 2
+BATCH_SIL_EXACT = 8
 BATCH_ERR_SCENE = 1 << 8
 BATCH_ERR_NO_SNCH = 1 << 9
 SERVER_PER_REQUEST = 4
@@ -86,7 +87,7 @@ class QueryOpts(C.Structure):
 
 class ServerOpts(C.Structure):
     _fields_ = [("budget_bytes", C.c_int64), ("ring_queries", C.c_int64 * 3), ("step_queries", C.c_int64),
-                ("max_inflight", C.c_int32), ("flags", C.c_int32)]
+                ("max_inflight", C.c_int32), ("flags", C.c_int32), ("sil_share", C.c_float)]
 
 
 class Request(C.Structure):

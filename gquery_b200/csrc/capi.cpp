@@ -143,7 +143,7 @@ bool on_host_only(const gq_scene *s) { return s->device < 0; }
 // Built-in launch choices (measured on B200 for the benchmark scenes).
 void default_tuning(gq_scene *s) {
     for (int k = 0; k < 3; ++k) s->tune[k] = gq_tuning{GQ_VARIANT_EXACT, 0, 1, 0, 32};
-    s->tune[GQ_KIND_SILHOUETTE].persist = 1;
+    s->tune[GQ_KIND_SILHOUETTE] = gq_tuning{GQ_VARIANT_COHERENT, 0, 1, 1, 32};
     if (s->dim == 3) {
         s->tune[GQ_KIND_CLOSEST_POINT] = gq_tuning{GQ_VARIANT_COHERENT, 1, 1, 0, 32};
         s->tune[GQ_KIND_INTERSECT] = gq_tuning{s->has_wide ? GQ_VARIANT_WIDE8 : GQ_VARIANT_EXACT, 0, 1, 1, 32};
@@ -492,6 +492,9 @@ gq_status gq_closest_silhouette(const gq_scene *s, gq_vecs x, const float *r_max
     if (!s->has_snch) return fail(GQ_ERR_UNSUPPORTED, "scene was built without the SNCH");
     if (s->exact_stack > GQ_STACK_EXACT) return fail(GQ_ERR_DEPTH, "tree deeper than gQuery's 64-entry stack");
     if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "scene was built without a device copy");
+    const int v = resolve_variant(s, opts, GQ_KIND_SILHOUETTE);
+    if (v != GQ_VARIANT_EXACT && v != GQ_VARIANT_COHERENT)
+        return fail(GQ_ERR_UNSUPPORTED, "silhouette queries run the exact or the coherent variant");
     DeviceGuard g(s->device);
     cudaStream_t cs = (cudaStream_t)stream;
     Scratch scr;
@@ -500,7 +503,7 @@ gq_status gq_closest_silhouette(const gq_scene *s, gq_vecs x, const float *r_max
     gq_status st;
     if ((st = prepare_order(s, x, n, opts, cs, scr, &perm, &counter)) != GQ_OK) return st;
     const gq_tuning &t = s->tune[GQ_KIND_SILHOUETTE];
-    cudaError_t e = gqd::launch_sil(s->dev, x, r_max, n, perm, *out, t.persist ? counter : nullptr, t.budget, cs);
+    cudaError_t e = gqd::launch_sil(s->dev, v, x, r_max, n, perm, *out, counter, t.persist, t.budget, cs);
     if (e != cudaSuccess) return fail_cuda(e, "closest_silhouette launch");
     return GQ_OK;
 }
@@ -643,7 +646,8 @@ gq_status gq_batch_run(gq_batch *b, const gq_batch_queries *cp, const gq_cp_out 
     for (const gq_scene *s : b->scenes) all_wide &= s->has_wide;
     cudaError_t e = gqd::batch_run(b->dev_scenes, (int)b->scenes.size(), b->dim, kinds, co, ro, so,
                                    (b->flags & GQ_BATCH_RAY_EXACT) || !all_wide ? 0 : 1,
-                                   (b->flags & GQ_BATCH_CP_EXACT) ? 0 : 1,
+                                   (b->flags & GQ_BATCH_CP_EXACT) ? 0 : 1, (b->flags & GQ_BATCH_SIL_EXACT) ? 0 : 1,
+                                   1.f,
                                    b->scratch, b->max_queries, b->err, (cudaStream_t)stream);
     if (e != cudaSuccess) return fail_cuda(e, "batch launch");
     return GQ_OK;

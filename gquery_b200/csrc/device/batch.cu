@@ -13,6 +13,7 @@
 #include "batch.cuh"
 #include "packet.cuh"
 #include "records.cuh"
+#include "sil_packet.cuh"
 #include "snch.cuh"
 #include "traverse.cuh"
 
@@ -136,14 +137,15 @@ __device__ __forceinline__ void refill(int64_t n, unsigned long long *counter, i
 
 // One persistent launch per step.  Phase 1: closest points, as warp tiles of 32
 // sorted queries (warp-coherent traversal once per distinct scene in the tile) or,
-// in exact mode, one lane per query.  Phase 2: rays, phase 3: silhouettes, one lane
-// per query.  Every warp moves to the next phase when the current one has no
+// in exact mode, one lane per query.  Phase 2: rays, one lane per query.  Phase 3:
+// silhouettes, as warp-coherent tiles like the closest points or, in exact mode, one
+// lane per query.  Every warp moves to the next phase when the current one has no
 // unclaimed work, so the phases' tails overlap.  counter[0..2]: claims per phase.
 template <int D, bool RAYW>
 __global__ void __launch_bounds__(kBlock) k_batch(const DevScene *scenes, int n_scenes, BatchKind cp, gq_cp_out cp_out,
                                                   BatchKind ray, gq_ray_out ray_out, BatchKind sil,
-                                                  gq_sil_out sil_out, int cp_coherent, int budget,
-                                                  unsigned long long *counter, int32_t *err) {
+                                                  gq_sil_out sil_out, int cp_coherent, int sil_coherent,
+                                                  int budget, unsigned long long *counter, int32_t *err) {
     const unsigned lane = threadIdx.x & 31u;
     // ---------------- phase 1: closest points ----------------
     if (cp_coherent) {
@@ -245,7 +247,44 @@ __global__ void __launch_bounds__(kBlock) k_batch(const DevScene *scenes, int n_
             [&]() { trav::lane_write(*sc, L, qi, ray.n, gq_cp_out{}, ray_out); });
     }
     // ---------------- phase 3: silhouettes ----------------
-    if (sil.n > 0) {
+    if (sil.n > 0 && sil_coherent) {
+        const int64_t t_sil = (sil.n + 31) / 32;
+        snch::Stack stk;
+        for (;;) {
+            unsigned long long t = 0;
+            if (lane == 0) t = atomicAdd(&counter[2], 1ull);
+            t = __shfl_sync(0xffffffffu, t, 0);
+            if (t >= (unsigned long long)t_sil) break;
+            const int64_t i = (int64_t)t * 32 + lane;
+            const bool in = i < sil.n;
+            const int64_t qi = in ? (int64_t)__ldg(sil.perm + i) : 0;
+            const int sid = in ? __ldg(sil.scene + qi) : GQ_BATCH_SKIP;
+            const bool known = in && (unsigned)sid < (unsigned)n_scenes;
+            const bool alive = known && scenes[sid].spairs != nullptr;
+            const bool skip = !in || sid == GQ_BATCH_SKIP;
+            if (!skip && !alive) atomicOr(err, known ? GQ_BATCH_ERR_NO_SNCH : GQ_BATCH_ERR_SCENE);
+            snch::Lane<D> L;
+#pragma unroll
+            for (int k = 0; k < D; ++k) L.x[k] = alive ? qget(sil.a, qi, k) : 0.f;
+            L.r = alive ? (sil.r_max ? sil.r_max[qi] : kInf) : -1.f;
+            L.found = false;
+            L.ovf = false;
+            unsigned todo = __ballot_sync(0xffffffffu, alive);
+            while (todo) {
+                const int s0 = __shfl_sync(0xffffffffu, sid, __ffs(todo) - 1);
+                const unsigned m = __ballot_sync(0xffffffffu, alive && sid == s0);
+                snch::Lane<D> M = L;
+                if (!((m >> lane) & 1u)) M.r = -1.f;
+                pkt::closest_silhouette<D>(scenes[s0], m, M, stk);
+                if ((m >> lane) & 1u) L = M;
+                todo &= ~m;
+            }
+            if (!skip) {
+                if (alive && L.ovf && scenes[sid].err) atomicOr(scenes[sid].err, GQ_DEVERR_STACK);
+                put_sil<D>(sil_out, sil.n, qi, alive && L.found && !L.ovf, L.bp, L.bd, L.bid);
+            }
+        }
+    } else if (sil.n > 0) {
         snch::Stack stk;
         snch::Lane<D> L;
         const DevScene *sc = scenes;
@@ -278,8 +317,8 @@ __global__ void __launch_bounds__(kBlock) k_batch(const DevScene *scenes, int n_
 
 template <int D, bool RAYW>
 cudaError_t launch_batch(const DevScene *scenes_dev, int n_scenes, BatchKind kinds[3], const gq_cp_out &cp_out,
-                         const gq_ray_out &ray_out, const gq_sil_out &sil_out, int cp_coherent,
-                         unsigned long long *counter, int32_t *err, cudaStream_t st) {
+                         const gq_ray_out &ray_out, const gq_sil_out &sil_out, int cp_coherent, int sil_coherent,
+                         float grid_share, unsigned long long *counter, int32_t *err, cudaStream_t st) {
     static int bps = 0, n_sm = 0;
     if (!bps) {
         int dev = 0;
@@ -290,9 +329,12 @@ cudaError_t launch_batch(const DevScene *scenes_dev, int n_scenes, BatchKind kin
     }
     const int64_t most = std::max(kinds[0].n, std::max(kinds[1].n, kinds[2].n));
     if (most <= 0) return cudaSuccess;
-    const int64_t want = std::min<int64_t>((int64_t)bps * n_sm, (most + kBlock - 1) / kBlock);
+    int64_t want = std::min<int64_t>((int64_t)bps * n_sm, (most + kBlock - 1) / kBlock);
+    if (grid_share > 0.f && grid_share < 1.f)
+        want = std::min<int64_t>(want, std::max<int64_t>(1, (int64_t)(grid_share * (float)(bps * n_sm))));
     k_batch<D, RAYW><<<dim3((unsigned)want), kBlock, 0, st>>>(scenes_dev, n_scenes, kinds[0], cp_out, kinds[1], ray_out,
-                                                              kinds[2], sil_out, cp_coherent, 32, counter, err);
+                                                              kinds[2], sil_out, cp_coherent, sil_coherent, 32, counter,
+                                                              err);
     return cudaGetLastError();
 }
 
@@ -316,7 +358,8 @@ size_t batch_scratch_bytes(int64_t max_n) {
 
 cudaError_t batch_run(const DevScene *scenes_dev, int n_scenes, int dim, BatchKind kinds[3], const gq_cp_out &cp_out,
                       const gq_ray_out &ray_out, const gq_sil_out &sil_out, int ray_wide, int cp_coherent,
-                      void *scratch, int64_t max_n, int32_t *err, cudaStream_t st) {
+                      int sil_coherent, float grid_share, void *scratch, int64_t max_n, int32_t *err,
+                      cudaStream_t st) {
     char *p = static_cast<char *>(scratch);
     unsigned long long *counter = reinterpret_cast<unsigned long long *>(p);
     p += 256;
@@ -349,13 +392,13 @@ cudaError_t batch_run(const DevScene *scenes_dev, int n_scenes, int dim, BatchKi
     if (e != cudaSuccess) return e;
     if (dim == 3)
         return ray_wide ? launch_batch<3, true>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_coherent,
-                                                counter, err, st)
+                                                sil_coherent, grid_share, counter, err, st)
                         : launch_batch<3, false>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_coherent,
-                                                 counter, err, st);
-    return ray_wide ? launch_batch<2, true>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_coherent, counter,
-                                            err, st)
-                    : launch_batch<2, false>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_coherent, counter,
-                                             err, st);
+                                                 sil_coherent, grid_share, counter, err, st);
+    return ray_wide ? launch_batch<2, true>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_coherent,
+                                            sil_coherent, grid_share, counter, err, st)
+                    : launch_batch<2, false>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_coherent,
+                                             sil_coherent, grid_share, counter, err, st);
 }
 
 }  // namespace gqd

@@ -8,6 +8,7 @@
 #include "prim.cuh"
 #include "queries.cuh"
 #include "records.cuh"
+#include "sil_packet.cuh"
 #include "snch.cuh"
 
 namespace gqd {
@@ -44,6 +45,30 @@ __device__ __forceinline__ void sil_write(const DevScene &s, const snch::Lane<D>
     }
     put1(o.d, qi, found ? L.bd : 0.f);
     if (o.prim_id) o.prim_id[qi] = found ? L.bid : 0;
+}
+
+// Warp-coherent closest silhouette (sil_packet.cuh): persistent warps take 32
+// consecutive queries of the sorted order at a time.
+template <int D>
+__global__ void __launch_bounds__(kBlock) k_sil_packet(DevScene s, gq_vecs xq, const float *rmax_in, int64_t n,
+                                                       const int32_t *perm, gq_sil_out o, unsigned long long *counter) {
+    const unsigned lane = threadIdx.x & 31u;
+    snch::Stack stk;
+    for (;;) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(counter, 32ull);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= (unsigned long long)n) break;
+        const int64_t i = (int64_t)base + lane;
+        const bool alive = i < n;
+        const int64_t qi = alive ? query_index(perm, i) : 0;
+        snch::Lane<D> L;
+#pragma unroll
+        for (int k = 0; k < D; ++k) L.x[k] = alive ? qget(xq, qi, k) : 0.f;
+        L.r = alive ? (rmax_in ? rmax_in[qi] : kInf) : -1.f;
+        pkt::closest_silhouette<D>(s, __ballot_sync(0xffffffffu, alive), L, stk);
+        if (alive) sil_write<D>(s, L, qi, n, o);
+    }
 }
 
 template <int D>
@@ -505,30 +530,47 @@ cudaError_t morton_order(const DevScene &s, gq_vecs q, int64_t n, int32_t *perm,
     return cub::DeviceRadixSort::SortPairs(p, tb, k_in, k_out, v_in, perm, (int)n, 0, end_bit, st);
 }
 
-cudaError_t launch_sil(const DevScene &s, gq_vecs x, const float *r_max, int64_t n, const int32_t *perm,
-                       const gq_sil_out &o, unsigned long long *counter, int budget, cudaStream_t st) {
+cudaError_t launch_sil(const DevScene &s, int variant, gq_vecs x, const float *r_max, int64_t n,
+                       const int32_t *perm, const gq_sil_out &o, unsigned long long *counter, int persist,
+                       int budget, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
-    if (counter && n > 4096) {
-        static int bps[2] = {0, 0}, n_sm = 0;
-        const int di = s.dim == 3 ? 1 : 0;
-        if (!bps[di]) {
+    static int bps[3][2] = {{0, 0}, {0, 0}, {0, 0}}, n_sm = 0;
+    const int di = s.dim == 3 ? 1 : 0;
+    const bool packet = variant == GQ_VARIANT_COHERENT && counter && n >= 32;
+    const bool refill = !packet && persist && counter && n > 4096;
+    if (packet || refill) {
+        const int ki = packet ? 1 : 0;
+        if (!bps[ki][di]) {
             int dev = 0;
             cudaGetDevice(&dev);
             cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-            if (s.dim == 3)
-                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps[1], k_sil_persist<3>, kBlock, 0);
+            int b = 0;
+            if (packet)
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, s.dim == 3 ? (const void *)k_sil_packet<3>
+                                                                             : (const void *)k_sil_packet<2>,
+                                                              kBlock, 0);
             else
-                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps[0], k_sil_persist<2>, kBlock, 0);
-            if (bps[di] < 1) bps[di] = 1;
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, s.dim == 3 ? (const void *)k_sil_persist<3>
+                                                                             : (const void *)k_sil_persist<2>,
+                                                              kBlock, 0);
+            bps[ki][di] = b < 1 ? 1 : b;
         }
-        const int64_t want = std::min<int64_t>((int64_t)bps[di] * n_sm, (n + kBlock - 1) / kBlock);
+        const int64_t want = std::min<int64_t>((int64_t)bps[ki][di] * n_sm, (n + kBlock - 1) / kBlock);
         cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
         if (e != cudaSuccess) return e;
-        const int b = budget > 0 ? budget : 32;
-        if (s.dim == 3)
-            k_sil_persist<3><<<dim3((unsigned)want), kBlock, 0, st>>>(s, x, r_max, n, perm, o, counter, b);
-        else
-            k_sil_persist<2><<<dim3((unsigned)want), kBlock, 0, st>>>(s, x, r_max, n, perm, o, counter, b);
+        const dim3 grid((unsigned)want);
+        if (packet) {
+            if (s.dim == 3)
+                k_sil_packet<3><<<grid, kBlock, 0, st>>>(s, x, r_max, n, perm, o, counter);
+            else
+                k_sil_packet<2><<<grid, kBlock, 0, st>>>(s, x, r_max, n, perm, o, counter);
+        } else {
+            const int b = budget > 0 ? budget : 32;
+            if (s.dim == 3)
+                k_sil_persist<3><<<grid, kBlock, 0, st>>>(s, x, r_max, n, perm, o, counter, b);
+            else
+                k_sil_persist<2><<<grid, kBlock, 0, st>>>(s, x, r_max, n, perm, o, counter, b);
+        }
         return cudaGetLastError();
     }
     if (s.dim == 3)

@@ -54,10 +54,12 @@ cudaError_t launch_ray(const DevScene &s, int variant, const Tune &t, gq_vecs x,
 // Warp-coherent closest point; layout 0 = binary pairs, 1 / 2 = quantised 8-wide (3D): sorted / nearest first.
 cudaError_t launch_cp_packet(const DevScene &s, int layout, gq_vecs q, int64_t n, const int32_t *perm,
                               const gq_cp_out &o, unsigned long long *counter, cudaStream_t st);
-// Closest silhouette; with a counter and enough queries, persistent warps with lane
-// refill (`budget` steps between refills).
-cudaError_t launch_sil(const DevScene &s, gq_vecs x, const float *r_max, int64_t n, const int32_t *perm,
-                       const gq_sil_out &o, unsigned long long *counter, int budget, cudaStream_t st);
+// Closest silhouette.  GQ_VARIANT_COHERENT (with a counter): warp-coherent traversal of
+// 32 sorted queries at a time; otherwise the reference order per lane, with persistent
+// lane refill when `persist` is set (`budget` steps between refills).
+cudaError_t launch_sil(const DevScene &s, int variant, gq_vecs x, const float *r_max, int64_t n,
+                       const int32_t *perm, const gq_sil_out &o, unsigned long long *counter, int persist,
+                       int budget, cudaStream_t st);
 cudaError_t launch_cp_brute(const DevScene &s, gq_vecs q, int64_t n, const gq_cp_out &o, cudaStream_t st);
 cudaError_t launch_ray_brute(const DevScene &s, gq_vecs x, gq_vecs v, const float *r_max, int64_t n,
                              const gq_ray_out &o, cudaStream_t st);

@@ -1,0 +1,152 @@
+// Warp-coherent ("packet") closest-silhouette traversal of the SNCH, shared by the
+// single-scene kernel (queries.cu) and the batch kernel (batch.cu).
+//
+// The lanes of a warp that hold queries on the same scene walk the tree once: the warp
+// pops one entry, every lane whose own stack key passes its own r_max takes part,
+// interior nodes are tested per lane with the reference's box and normal-cone tests
+// (SNCHNode3D.overlaps, snch3d.py:55-95; snch.py:60-97) against the lane's r_max, and
+// a child is entered when at least one lane admits it.  Leaves are scanned by all
+// participating lanes together with the reference's per-silhouette test and acceptance
+// rule (snch.py:131-134).  Each lane keeps its own r_max and best silhouette.
+//
+// Answers equal the reference's except at FP32 distance ties: the cone test does not
+// depend on r_max, so the silhouettes a lane can reach are the same in any visit
+// order, and r_max only prunes boxes that cannot hold a closer silhouette.  The order
+// (nearest lane's box first) changes only which of two equally distant silhouettes
+// wins.
+#pragma once
+
+#include "packet.cuh"
+#include "prim.cuh"
+#include "queries.cuh"
+#include "snch.cuh"
+
+namespace gqd {
+namespace pkt {
+
+constexpr int kSilNone = 0x7fffffff;
+
+// One traversal for the lanes in `mask` (warp-uniform); all 32 lanes must call it.
+// L: this lane's query state (x and r set by the caller, as snch::lane_init would);
+// on return L.found / bp / bd / bid hold its answer and L.ovf a stack overflow.
+template <int D>
+__device__ __forceinline__ void closest_silhouette(const DevScene &s, unsigned mask, snch::Lane<D> &L, int2 *stk) {
+    const unsigned lane = threadIdx.x & 31u;
+    const bool mine = (mask >> lane) & 1u;
+    L.found = false;
+    L.ovf = false;
+    L.bd = 0.f;
+    L.bid = 0;
+#pragma unroll
+    for (int k = 0; k < D; ++k) L.bp[k] = 0.f;
+    float dmin_root = kInf, dmax_root;
+    if (mine) {
+        if (D == 2)
+            box_dist2(s.root_lo[0], s.root_lo[1], s.root_hi[0], s.root_hi[1], L.x[0], L.x[1], dmin_root, dmax_root);
+        else
+            box_dist3(s.root_lo[0], s.root_lo[1], s.root_lo[2], s.root_hi[0], s.root_hi[1], s.root_hi[2], L.x[0],
+                      L.x[1], L.x[D - 1], dmin_root, dmax_root);
+    }
+    unsigned cmask = __ballot_sync(0xffffffffu, mine && dmin_root <= L.r);
+    int cur = cmask ? s.sroot_ref : kSilNone;
+    int sp = -1;
+    bool ovf = false;
+    for (;;) {
+        if (cur == kSilNone) {
+            bool got = false;
+            while (sp >= 0) {
+                const int2 e = stk[sp--];
+                // pop-time test of the reference, per lane (snch.py:118)
+                const unsigned m = __ballot_sync(0xffffffffu, mine && __int_as_float(e.y) <= L.r);
+                if (m) {
+                    cur = e.x;
+                    cmask = m;
+                    got = true;
+                    break;
+                }
+            }
+            if (!got) break;
+        }
+        const bool act = (cmask >> lane) & 1u;
+        if (cur < 0) {
+            if (cur != INT32_MIN) {  // INT32_MIN: leaf without silhouettes
+                for (int j = ~cur;; ++j) {
+                    const int flags = D == 2 ? fbits(ldg4(s.sils, 2 * (int64_t)j + 1).w)
+                                             : fbits(ldg4(s.sils, 4 * (int64_t)j + 3).y);
+                    if (act) snch::test_silhouette<D>(s, L, j);
+                    if (flags & GQ_ITEM_LAST) break;
+                }
+            }
+            cur = kSilNone;
+            continue;
+        }
+        float lo[2][D], hi[2][D], ax[2][D], half[2], rad[2];
+        int refs[2];
+        if (D == 2) {
+            const float4 a0 = ldg4(s.spairs, 5 * (int64_t)cur), a1 = ldg4(s.spairs, 5 * (int64_t)cur + 1),
+                         a2 = ldg4(s.spairs, 5 * (int64_t)cur + 2), a3 = ldg4(s.spairs, 5 * (int64_t)cur + 3);
+            const int4 rr = __ldg(reinterpret_cast<const int4 *>(s.spairs) + 5 * (int64_t)cur + 4);
+            lo[0][0] = a0.x; lo[0][D - 1] = a0.y; hi[0][0] = a0.z; hi[0][D - 1] = a0.w;
+            ax[0][0] = a1.x; ax[0][D - 1] = a1.y; half[0] = a1.z; rad[0] = a1.w;
+            lo[1][0] = a2.x; lo[1][D - 1] = a2.y; hi[1][0] = a2.z; hi[1][D - 1] = a2.w;
+            ax[1][0] = a3.x; ax[1][D - 1] = a3.y; half[1] = a3.z; rad[1] = a3.w;
+            refs[0] = rr.x;
+            refs[1] = rr.y;
+        } else {
+            const int64_t b = 6 * (int64_t)cur;
+            const float4 f0 = ldg4(s.spairs, b), f1 = ldg4(s.spairs, b + 1), f2 = ldg4(s.spairs, b + 2),
+                         f3 = ldg4(s.spairs, b + 3), f4 = ldg4(s.spairs, b + 4), f5 = ldg4(s.spairs, b + 5);
+            lo[0][0] = f0.x; lo[0][1] = f0.y; lo[0][D - 1] = f0.z;
+            hi[0][0] = f0.w; hi[0][1] = f1.x; hi[0][D - 1] = f1.y;
+            ax[0][0] = f1.z; ax[0][1] = f1.w; ax[0][D - 1] = f2.x;
+            half[0] = f2.y; rad[0] = f2.z;
+            lo[1][0] = f2.w; lo[1][1] = f3.x; lo[1][D - 1] = f3.y;
+            hi[1][0] = f3.z; hi[1][1] = f3.w; hi[1][D - 1] = f4.x;
+            ax[1][0] = f4.y; ax[1][1] = f4.z; ax[1][D - 1] = f4.w;
+            half[1] = f5.x; rad[1] = f5.y;
+            refs[0] = fbits(f5.z);
+            refs[1] = fbits(f5.w);
+        }
+        bool hit[2] = {false, false};
+        float dm[2] = {kInf, kInf};
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            if (act) {
+                float dmax;
+                if (D == 2)
+                    box_dist2(lo[c][0], lo[c][D - 1], hi[c][0], hi[c][D - 1], L.x[0], L.x[D - 1], dm[c], dmax);
+                else
+                    box_dist3(lo[c][0], lo[c][1], lo[c][D - 1], hi[c][0], hi[c][1], hi[c][D - 1], L.x[0], L.x[1],
+                              L.x[D - 1], dm[c], dmax);
+                hit[c] = dm[c] <= L.r;
+                if ((half[c] >= 0.f) & hit[c])
+                    hit[c] = cone_overlaps<D>(lo[c], hi[c], ax[c], half[c], rad[c], L.x, dm[c]);
+            }
+        }
+        const unsigned m0 = __ballot_sync(0xffffffffu, hit[0]), m1 = __ballot_sync(0xffffffffu, hit[1]);
+        if (m0 && m1) {
+            const float k0 = warp_min(hit[0] ? dm[0] : kInf), k1 = warp_min(hit[1] ? dm[1] : kInf);
+            const bool second_first = k1 < k0;  // the nearer child (over the lanes) is entered first
+            if (sp + 1 >= GQ_STACK_EXACT) {
+                ovf = true;
+                break;
+            }
+            stk[++sp] = second_first ? make_int2(refs[0], fbits(hit[0] ? dm[0] : kInf))
+                                     : make_int2(refs[1], fbits(hit[1] ? dm[1] : kInf));
+            cur = second_first ? refs[1] : refs[0];
+            cmask = second_first ? m1 : m0;
+        } else if (m0) {
+            cur = refs[0];
+            cmask = m0;
+        } else if (m1) {
+            cur = refs[1];
+            cmask = m1;
+        } else {
+            cur = kSilNone;
+        }
+    }
+    L.ovf = ovf;
+}
+
+}  // namespace pkt
+}  // namespace gqd

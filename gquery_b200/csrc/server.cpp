@@ -9,8 +9,10 @@
 // is reclaimed in allocation order, so it is first-in first-out like the admission.
 // The rings' device bytes are the admission budget.
 //
-// Step.  A step takes, for each kind, the run of admitted requests that are contiguous
-// in the ring (at most step_queries queries) and answers them with one batch launch;
+// Step.  A step takes, for each kind it serves, the run of admitted requests that are
+// contiguous in the ring (at most step_queries queries) and answers them with one
+// batch launch; closest-point and ray requests go to the general slots, silhouette
+// requests to a slot of their own whose launches hold part of the GPU only;
 // inside the step a field with C components is stored component-major with stride m
 // (the step's query count) from ring offset off * C, which is where the kernel writes
 // it and what one device-to-host copy per field brings back.
@@ -122,6 +124,7 @@ struct Slot {
     size_t scratch_bytes = 0;
     int32_t *err = nullptr;
     bool busy = false;
+    bool sil_only = false;  // batch mode: this slot answers silhouette requests only
     int step = -1;
     gq_status status = GQ_OK;
     std::vector<Req *> reqs;
@@ -133,6 +136,7 @@ struct Slot {
 struct gq_server {
     int dim = 0, device = 0, flags = 0;
     int64_t step_queries = 0, ring_bytes = 0;
+    float sil_share = 0.5f;
     std::vector<gq_scene *> scenes;
     gqd::DevScene *dev_scenes = nullptr;
     Ring ring[3];
@@ -333,8 +337,10 @@ struct gq_server {
         for (Slot &S : slots) {
             if (S.busy) continue;
             bool have = false;
-            for (int k = 0; k < 3; ++k) have |= !admitted[k].empty();
-            if (!have) break;
+            for (int k = 0; k < 3; ++k)
+                if (!(flags & GQ_SERVER_PER_REQUEST) && (k == GQ_KIND_SILHOUETTE) != S.sil_only) continue;
+                else have |= !admitted[k].empty();
+            if (!have) continue;
             S.reqs.clear();
             for (int k = 0; k < 3; ++k) S.off[k] = 0, S.m[k] = 0;
             if (flags & GQ_SERVER_PER_REQUEST) {
@@ -350,6 +356,7 @@ struct gq_server {
                 S.reqs.push_back(r);
             } else {
                 for (int k = 0; k < 3; ++k) {
+                    if ((k == GQ_KIND_SILHOUETTE) != S.sil_only) continue;
                     while (!admitted[k].empty()) {
                         Req *r = admitted[k].front();
                         if (S.m[k] == 0)
@@ -422,8 +429,8 @@ struct gq_server {
         for (const gq_scene *sc : scenes) all_wide &= sc->has_wide;
         cudaError_t e = gqd::batch_run(dev_scenes, (int)scenes.size(), D, kinds, co, ro, so,
                                        (flags & GQ_BATCH_RAY_EXACT) || !all_wide ? 0 : 1,
-                                       (flags & GQ_BATCH_CP_EXACT) ? 0 : 1,
-                                       S.scratch, step_queries, S.err, S.st);
+                                       (flags & GQ_BATCH_CP_EXACT) ? 0 : 1, (flags & GQ_BATCH_SIL_EXACT) ? 0 : 1,
+                                       S.sil_only ? sil_share : 1.f, S.scratch, step_queries, S.err, S.st);
         return e == cudaSuccess ? GQ_OK : fail_cuda(e, "server step");
     }
 
@@ -551,6 +558,7 @@ gq_status gq_server_create(gq_scene *const *scenes, int32_t n_scenes, const gq_s
     s->flags = o.flags;
     s->step_queries = o.step_queries > 0 ? o.step_queries : (1 << 19);
     const int inflight = o.max_inflight > 0 ? o.max_inflight : 2;
+    s->sil_share = o.sil_share > 0.f && o.sil_share <= 1.f ? o.sil_share : 0.5f;
     std::vector<gqd::DevScene> views((size_t)n_scenes);
     for (int32_t i = 0; i < n_scenes; ++i) {
         gq_scene *sc = scenes[i];
@@ -583,7 +591,9 @@ gq_status gq_server_create(gq_scene *const *scenes, int32_t n_scenes, const gq_s
     for (int k = 0; k < 3 && e == cudaSuccess; ++k) e = s->make_ring(s->ring[k]);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->copy_st, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->copy_evt, cudaEventDisableTiming);
-    s->slots.resize((size_t)inflight);
+    const bool per_request = (s->flags & GQ_SERVER_PER_REQUEST) != 0;
+    s->slots.resize((size_t)inflight + (per_request ? 0 : 1));
+    if (!per_request) s->slots.back().sil_only = true;
     for (Slot &S : s->slots) {
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S.st, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S.done, cudaEventDisableTiming);

@@ -233,13 +233,15 @@ class Scene:
         return L.RayOut(_ptr(rec.valid), _ptr(rec.p), _ptr(rec.n), _ptr(t), _ptr(rec.d), _ptr(rec.prim_id),
                         _ptr(rec.on_boundary))
 
-    def closest_silhouette(self, x, r_max=math.inf, *, sort=True, stream=None, scratch=None, out=None, order=None):
-        """closest_silhouette_snch (snch.py:106-164 / snch3d.py:143-203)."""
+    def closest_silhouette(self, x, r_max=math.inf, *, variant="auto", sort=True, stream=None, scratch=None,
+                           out=None, order=None):
+        """closest_silhouette_snch (snch.py:106-164 / snch3d.py:143-203); variant "exact"
+        (reference visit order) or "coherent" (warp-coherent, same answers except at ties)."""
         tx, n, vx = self._points(x)
         rm = self._rmax(r_max, n)
         rec = out or self.alloc_sil(n)
         o = L.SilOut(_ptr(rec.valid), _ptr(rec.p), _ptr(rec.d), _ptr(rec.prim_id))
-        opts = self._opts("exact", sort, scratch, order)
+        opts = self._opts(variant, sort, scratch, order)
         L.check(L.lib().gq_closest_silhouette(self._h, vx, _ptr(rm), n, C.byref(o), C.byref(opts),
                                               _stream_handle(stream)))
         return rec

@@ -47,7 +47,7 @@ typedef int32_t gq_status;
 #define GQ_VARIANT_WIDE8 1    /* 8-wide nodes, 8-bit outward-rounded child boxes */
 #define GQ_VARIANT_AUTO 2     /* the scene's tuned choice for the query kind (gq_scene_set_tuning) */
 #define GQ_VARIANT_COHERENT 3 /* binary tree walked once per warp of Morton-adjacent queries (closest
-                                 point); other query kinds run as EXACT */
+                                 point, closest silhouette); rays run as EXACT */
 /* All variants other than EXACT give the same answers as EXACT except at FP32 distance
  * ties (distances within 2e-6 relative). */
 
@@ -224,13 +224,14 @@ gq_status gq_scene_device_error(const gq_scene *scene, void *stream, int32_t *fl
  * a fixed scratch sized for max_queries queries of each kind, so gq_batch_run
  * allocates nothing and never synchronises: a step can be recorded in a CUDA graph.
  * Each query carries the index of its scene in the batch.  Results are those of the
- * single-scene calls: closest points follow GQ_VARIANT_COHERENT (or GQ_VARIANT_EXACT
- * with GQ_BATCH_CP_EXACT), rays GQ_VARIANT_WIDE8 where the scene has wide nodes (or
- * GQ_VARIANT_EXACT with GQ_BATCH_RAY_EXACT), silhouettes GQ_VARIANT_EXACT. */
+ * single-scene calls: closest points and silhouettes follow GQ_VARIANT_COHERENT (or
+ * GQ_VARIANT_EXACT with GQ_BATCH_CP_EXACT / GQ_BATCH_SIL_EXACT), rays GQ_VARIANT_WIDE8
+ * when every scene has wide nodes (or GQ_VARIANT_EXACT with GQ_BATCH_RAY_EXACT). */
 typedef struct gq_batch gq_batch;
 
 #define GQ_BATCH_CP_EXACT 1  /* closest point: one exact traversal per lane, reference visit order */
 #define GQ_BATCH_RAY_EXACT 2 /* rays: binary BVH, reference visit order */
+#define GQ_BATCH_SIL_EXACT 8 /* silhouettes: one exact traversal per lane, reference visit order */
 
 typedef struct {
     int64_t n;             /* query count (0: none of this kind) */
@@ -264,10 +265,13 @@ gq_status gq_batch_device_error(gq_batch *batch, void *stream, int32_t *flags);
  * has room (the rings are the admission budget: their device bytes may not exceed
  * budget_bytes), copies its queries to the device at once on a copy stream while
  * earlier steps compute, and launches a step over every admitted request as soon as
- * one of max_inflight step slots is free: one gq_batch launch for all scenes and
- * kinds (or, with GQ_SERVER_PER_REQUEST, one single-scene call per request, the
- * scene's tuned variant).  Each slot has its own stream, so the results of one step
- * go back to the host while the next computes.  Results are those of gq_batch_run. */
+ * a step slot is free: one gq_batch launch for all scenes (or, with
+ * GQ_SERVER_PER_REQUEST, one single-scene call per request, the scene's tuned
+ * variant).  Closest-point and ray requests share max_inflight slots; silhouette
+ * requests, whose traversals are far longer, have a slot of their own whose launches
+ * hold at most sil_share of the GPU, so the other kinds never queue behind them.
+ * Each slot has its own stream, so the results of one step go back to the host while
+ * the next computes.  Results are those of gq_batch_run. */
 typedef struct gq_server gq_server;
 
 #define GQ_SERVER_PER_REQUEST 4 /* one single-scene launch per request instead of batched steps */
@@ -276,8 +280,9 @@ typedef struct {
     int64_t budget_bytes;     /* device bytes the request rings may hold (0: no limit) */
     int64_t ring_queries[3];  /* ring capacity in queries per kind (0: 1<<22) */
     int64_t step_queries;     /* most queries of one kind in one step, and the largest request (0: 1<<19) */
-    int32_t max_inflight;     /* step slots (0: 2) */
-    int32_t flags;            /* GQ_BATCH_CP_EXACT | GQ_BATCH_RAY_EXACT | GQ_SERVER_PER_REQUEST */
+    int32_t max_inflight;     /* step slots for closest-point and ray steps (0: 2) */
+    int32_t flags;            /* GQ_BATCH_*_EXACT | GQ_SERVER_PER_REQUEST */
+    float sil_share;          /* share of the GPU's resident blocks a silhouette step may hold (0: 0.5) */
 } gq_server_opts;
 
 typedef struct {

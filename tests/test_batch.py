@@ -1,10 +1,10 @@
 """Batched queries over many uneven scenes in one launch (gq_batch_*).
 
 Every query must get the answer it gets from the single-scene call on its own scene:
-closest point (exact), rays and silhouettes bit for bit, because those traversals run
-one query per lane in the same order; warp-coherent closest points with the same
-validity and distance, and the same primitive except at FP32 distance ties, because a
-warp's visit order depends on which queries share it.  The exact mode is also checked
+rays and the exact modes bit for bit, because those traversals run one query per lane
+in the same order; warp-coherent closest points and silhouettes with the same validity
+and distance, and the same primitive except at FP32 distance ties, because a warp's
+visit order depends on which queries share it.  The exact mode is also checked
 against the CPU oracle.
 """
 import math
@@ -99,8 +99,10 @@ def test_batch_matches_single_scene_calls(dim, two_d, three_d):
     assert b.device_error() == 0
     ray_alone = _alone(scenes, ids, lambda s, sel: s.intersect(_dev(pts[sel]), _dev(dirs[sel]), variant="wide8"))
     assert_bitwise(to_np(res.ray), ray_alone, rayf, "ray ")
-    sil_alone = _alone(scenes, ids, lambda s, sel: s.closest_silhouette(_dev(pts[sel])))
-    assert_bitwise(to_np(res.sil), sil_alone, SIL, "sil ")
+    sil_alone = _alone(scenes, ids, lambda s, sel: s.closest_silhouette(_dev(pts[sel]), variant="coherent"))
+    rep = tie_report(to_np(res.sil), sil_alone)
+    assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0, rep
+    assert rep["max_rel_d"] <= REL_TOL, rep
     cp_alone = _alone(scenes, ids, lambda s, sel: s.closest_point(_dev(pts[sel]), variant="coherent"))
     rep = tie_report(to_np(res.cp), cp_alone)
     assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0, rep
@@ -116,14 +118,16 @@ def test_batch_exact_mode_bitwise(dim, two_d, three_d):
     n = 30_000
     ids, pts, dirs = _mixed_queries(n, dim, len(scenes), seed=10 + dim)
     cpf, rayf = (CP2, RAY2) if dim == 2 else (CP3, RAY3)
-    b = SceneBatch(scenes, n, cp_variant="exact", ray_variant="exact")
-    res = b.run(cp=(_dev(pts), _dev(ids)), ray=(_dev(pts), _dev(dirs), _dev(ids), 1.5))
+    b = SceneBatch(scenes, n, cp_variant="exact", ray_variant="exact", sil_variant="exact")
+    res = b.run(cp=(_dev(pts), _dev(ids)), ray=(_dev(pts), _dev(dirs), _dev(ids), 1.5), sil=(_dev(pts), _dev(ids), 0.7))
     torch.cuda.synchronize()
     cp_alone = _alone(scenes, ids, lambda s, sel: s.closest_point(_dev(pts[sel]), variant="exact"))
     assert_bitwise(to_np(res.cp), cp_alone, cpf, "cp ")
     ray_alone = _alone(scenes, ids,
                        lambda s, sel: s.intersect(_dev(pts[sel]), _dev(dirs[sel]), 1.5, variant="exact"))
     assert_bitwise(to_np(res.ray), ray_alone, rayf, "ray ")
+    sil_alone = _alone(scenes, ids, lambda s, sel: s.closest_silhouette(_dev(pts[sel]), 0.7, variant="exact"))
+    assert_bitwise(to_np(res.sil), sil_alone, SIL, "sil ")
 
 
 def test_batch_exact_mode_against_oracle(two_d):

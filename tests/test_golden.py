@@ -58,4 +58,4 @@ def test_exact_kernels_match_reference_traversal(path):
     assert_bitwise(to_np(s.closest_point(z["q"], variant="exact")), expected(z, "cp", CP[dim]), CP[dim], "cp ")
     assert_bitwise(to_np(s.intersect(z["o"], z["d"], variant="exact")), expected(z, "ray", RAY[dim]), RAY[dim],
                    "ray ")
-    assert_bitwise(to_np(s.closest_silhouette(z["q"], rmax)), expected(z, "sil", SIL), SIL, "sil ")
+    assert_bitwise(to_np(s.closest_silhouette(z["q"], rmax, variant="exact")), expected(z, "sil", SIL), SIL, "sil ")

@@ -88,14 +88,14 @@ def test_ray2d_exact_finite_rmax(star):
 
 def test_sil2d_exact_bitwise(star):
     x = W.uniform_points(32768, 2, seed=14)
-    got = to_np(star.closest_silhouette(x, sort=True))
+    got = to_np(star.closest_silhouette(x, variant="exact", sort=True))
     ref = oracle.closest_silhouette(2, *_sref(star), x)
     assert_bitwise(got, ref, SIL_FIELDS, "sil2d ")
 
 
 def test_sil2d_exact_finite_rmax(star):
     x = W.uniform_points(8192, 2, seed=15)
-    got = to_np(star.closest_silhouette(x, 0.25))
+    got = to_np(star.closest_silhouette(x, 0.25, variant="exact"))
     ref = oracle.closest_silhouette(2, *_sref(star), x, 0.25)
     assert_bitwise(got, ref, SIL_FIELDS, "sil2d rmax ")
     assert 0.0 < got["valid"].mean() < 1.0
@@ -120,7 +120,7 @@ def test_ray3d_exact_bitwise_c1(mesh_c1):
 
 def test_sil3d_exact_bitwise_c2(mesh_c2):
     x = W.uniform_points(4096, 3, seed=23)
-    got = to_np(mesh_c2.closest_silhouette(x, sort=True))
+    got = to_np(mesh_c2.closest_silhouette(x, variant="exact", sort=True))
     ref = oracle.closest_silhouette(3, *_sref(mesh_c2), x)
     assert_bitwise(got, ref, SIL_FIELDS, "sil3d ")
 
@@ -133,7 +133,7 @@ def test_exact_small_mesh_all_queries(mesh_small):
                    CP_FIELDS_3D, "cp3d small ")
     assert_bitwise(to_np(mesh_small.intersect(o, d, variant="exact")), oracle.intersect(3, nodes, prims, o, d),
                    RAY_FIELDS_3D, "ray3d small ")
-    assert_bitwise(to_np(mesh_small.closest_silhouette(q)), oracle.closest_silhouette(3, *_sref(mesh_small), q),
+    assert_bitwise(to_np(mesh_small.closest_silhouette(q, variant="exact")), oracle.closest_silhouette(3, *_sref(mesh_small), q),
                    SIL_FIELDS, "sil3d small ")
 
 
@@ -292,3 +292,38 @@ def test_unsorted_queries_give_same_answers(mesh_c1):
     b = to_np(mesh_c1.closest_point(q, variant="coherent", sort=True))
     rep = tie_report(a, b)
     assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0, rep
+
+
+# ---------------------------------------------------------------- silhouettes: refill and coherent
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_sil_refill_bitwise_and_coherent_ties(dim, star, mesh_c2):
+    scene = star if dim == 2 else mesh_c2
+    n = 40000 + 17 if dim == 2 else 12000 + 3
+    x = W.uniform_points(n, dim, seed=70 + dim)
+    saved = scene.get_tuning("sil")
+    try:
+        scene.set_tuning("sil", "exact", persist=0)
+        a = to_np(scene.closest_silhouette(x, variant="exact"))
+        scene.set_tuning("sil", "exact", persist=1, budget=7)
+        b = to_np(scene.closest_silhouette(x, variant="exact"))
+    finally:
+        scene.set_tuning("sil", saved["variant"], saved["packet"], saved["sorted"], saved["persist"], saved["budget"])
+    assert_bitwise(b, a, SIL_FIELDS, "sil refill ")
+    for r_max in (math.inf, 0.3):
+        ref = to_np(scene.closest_silhouette(x, r_max, variant="exact"))
+        got = to_np(scene.closest_silhouette(x, r_max, variant="coherent"))
+        rep = tie_report(ref, got)
+        assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0, (r_max, rep)
+        assert rep["max_rel_d"] <= REL_TOL, (r_max, rep)
+    assert scene.device_error() == 0
+
+
+def test_sil3d_coherent_against_oracle_small(mesh_small):
+    x = W.uniform_points(3000, 3, seed=75)
+    got = to_np(mesh_small.closest_silhouette(x, variant="coherent"))
+    ref = oracle.closest_silhouette(3, *_sref(mesh_small), x)
+    rep = tie_report(ref, got)
+    assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0, rep
+    with pytest.raises(L.GQError, match="exact or the coherent"):
+        mesh_small.closest_silhouette(x, variant="wide8")
