@@ -1,11 +1,17 @@
 #!/usr/bin/env python
-"""Benchmark: 3D closest point + ray intersection on the displaced icosphere of
-level 8 (1,310,720 triangles), 8,388,608 closest-point queries U[-2,2]^3 and
-8,388,608 rays (origins U[-2,2]^3, directions uniform on S^2, r_max = inf).
+"""Benchmark of the geometry-query engine on one B200 (or N, weak scaling).
 
-One step = Morton-order + closest_point over all points, then Morton-order +
-intersect over all rays, on the quantised 8-wide BVH.  The exact binary kernel
-(gQuery's visit order) is measured beside it.  Prints one JSON line (rank 0).
+Headline (the JSON line's `value`): 3D closest point + ray intersection on the
+displaced icosphere of level 8 (1,310,720 triangles), 8,388,608 closest-point queries
+U[-2,2]^3 and 8,388,608 rays (origins U[-2,2]^3, directions uniform on S^2, r_max =
+inf).  One step = Morton order + closest_point over all points, then Morton order +
+intersect over all rays, each with the scene's tuned variant; the exact binary kernel
+(gQuery's visit order) and the quantised 8-wide kernel are measured beside it.
+
+At one GPU the same line also carries (see --sections): c2 closest silhouettes on the
+level-7 mesh (plain, refill, coherent), c3 512 uneven 2D scenes answered by one
+batched launch per step (eager and CUDA graph) against one plain call per scene and
+kind, c4 the serving runtime under open-loop Poisson load against per-request launches.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Multi-GPU (weak scaling, replicated scene, disjoint query shards, no collective in
@@ -49,6 +55,13 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the exact and wide8 side-by-side runs")
+    ap.add_argument("--sections", default="c2,c3,c4",
+                    help="beside the headline (cp + rays on the level-8 mesh): c2 silhouettes on the level-7 "
+                         "mesh, c3 512 uneven 2D scenes in one batched launch, c4 serving 64 meshes; "
+                         "comma-separated or 'none' (one GPU only)")
+    ap.add_argument("--c2-n", type=int, default=1 << 22, help="silhouette queries (c2)")
+    ap.add_argument("--c3-total", type=int, default=1 << 24, help="queries per batched step (c3)")
+    ap.add_argument("--c4-requests", type=int, default=240, help="requests per serving trace (c4)")
     return ap.parse_args()
 
 
@@ -151,6 +164,197 @@ def cpu_baseline(V, F, q, o, d, seconds, counts=True):
     return {"value": 2 * done / t_total / 1e6, "unit": "Mqueries/s", "cores": threads,
             "kind": "port", "seconds": t_total,
             "sample": f"first {done} cp queries + first {done} rays of the same workload"}, means
+
+
+def dev_ms(fn, steps, warmup, flush=None):
+    """Median device time (CUDA events on the current stream) of `fn`, L2 flushed before each call."""
+    import torch
+    for _ in range(warmup):
+        if flush is not None:
+            flush.zero_()
+        fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(steps):
+        if flush is not None:
+            flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        ts.append(a.elapsed_time(b))
+    return statistics.median(ts)
+
+
+def section_c2(args, dev, flush):
+    """Closest silhouette, displaced icosphere level 7 (327,680 triangles, amplitude 0.3),
+    4,194,304 points U[-2,2]^3: the reference visit order one query per thread (plain),
+    the same with persistent lane refill, and the warp-coherent traversal."""
+    import torch
+    from gquery_b200 import workloads as W
+    from gquery_b200.scene import Scene
+    V, F = W.config2_mesh()
+    t0 = time.perf_counter()
+    sc = Scene(V, F, 3, device=dev.index or 0, build_snch=True, build_wide=False)
+    build_s = time.perf_counter() - t0
+    n = args.c2_n
+    x = torch.as_tensor(W.uniform_points(n, 3, seed=31)).to(dev)
+    order = sc.order(x)
+    out = sc.alloc_sil(n)
+    scratch = torch.empty(sc.scratch_bytes(n), dtype=torch.uint8, device=dev)
+    res = {"workload": "closest silhouette, icosphere level 7 (327,680 triangles) amplitude 0.3, "
+                       f"{n} points U[-2,2]^3", "build_s": build_s}
+    for name, variant, persist in (("plain_exact", "exact", 0), ("exact_refill", "exact", 1),
+                                   ("coherent", "coherent", 1)):
+        sc.set_tuning("sil", variant, persist=persist)
+        ms = dev_ms(lambda: sc.closest_silhouette(x, variant=variant, out=out, order=order, scratch=scratch),
+                    steps=2 if variant == "exact" else 3, warmup=1, flush=flush)
+        res[name] = {"ms": ms, "mqueries_per_s": n / ms / 1e3}
+    assert sc.device_error() == 0
+    res["coherent_vs_plain"] = res["plain_exact"]["ms"] / res["coherent"]["ms"]
+    return res
+
+
+def section_c3(args, dev, flush):
+    """512 star polylines (64 - 262,144 segments, log-uniform), 16,777,216 queries split
+    50/30/20 closest point / ray / silhouette, counts proportional to segments: one
+    batched launch per step (eager and CUDA-graph replay) against one plain single-scene
+    call per scene and kind."""
+    import torch
+    from concurrent.futures import ThreadPoolExecutor
+    from gquery_b200 import workloads as W
+    from gquery_b200.batch import SceneBatch
+    from gquery_b200.scene import Scene
+    geo = W.config3_scenes()
+    Q = W.config3_queries(geo, n_total=args.c3_total)
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(os.cpu_count() or 8) as ex:
+        scenes = list(ex.map(lambda g: Scene(g[0], g[1], 2, device=dev.index or 0, build_snch=True, n_threads=1),
+                             geo))
+    build_s = time.perf_counter() - t0
+    cp_ids, cp_pts = (torch.as_tensor(a).to(dev) for a in Q["cp"])
+    ray_ids, ray_o, ray_d = (torch.as_tensor(a).to(dev) for a in Q["ray"])
+    sil_ids, sil_pts = (torch.as_tensor(a).to(dev) for a in Q["sil"])
+    ns = (cp_ids.numel(), ray_ids.numel(), sil_ids.numel())
+    total = sum(ns)
+    b = SceneBatch(scenes, max(ns))
+    out = b.alloc(*ns)
+    eager_ms = dev_ms(lambda: b.run(cp=(cp_pts, cp_ids), ray=(ray_o, ray_d, ray_ids), sil=(sil_pts, sil_ids),
+                                    out=out), steps=5, warmup=3, flush=flush)
+    kind_ms = {k: dev_ms(lambda: b.run(out=out, **a), steps=3, warmup=1, flush=flush) for k, a in
+               (("cp", dict(cp=(cp_pts, cp_ids))), ("ray", dict(ray=(ray_o, ray_d, ray_ids))),
+                ("sil", dict(sil=(sil_pts, sil_ids))))}
+    g = b.capture(*ns)
+    g.cp_points.copy_(cp_pts.t())
+    g.cp_scene.copy_(cp_ids)
+    g.ray_origin.copy_(ray_o.t())
+    g.ray_dir.copy_(ray_d.t())
+    g.ray_scene.copy_(ray_ids)
+    g.sil_points.copy_(sil_pts.t())
+    g.sil_scene.copy_(sil_ids)
+    graph_ms = dev_ms(g.replay, steps=5, warmup=3, flush=flush)
+    assert b.device_error() == 0
+    # plain: one single-scene call per scene and kind (queries are grouped by scene)
+    bounds = [np.searchsorted(Q[k][0], np.arange(len(scenes) + 1)) for k in ("cp", "ray", "sil")]
+
+    def per_scene(variant):
+        for i, sc in enumerate(scenes):
+            a, z = bounds[0][i], bounds[0][i + 1]
+            if z > a:
+                sc.closest_point(cp_pts[a:z], variant=variant)
+            a, z = bounds[1][i], bounds[1][i + 1]
+            if z > a:
+                sc.intersect(ray_o[a:z], ray_d[a:z], variant=variant)
+            a, z = bounds[2][i], bounds[2][i + 1]
+            if z > a:
+                sc.closest_silhouette(sil_pts[a:z], variant=variant if variant == "exact" else "auto")
+    plain_ms = dev_ms(lambda: per_scene("exact"), steps=1, warmup=1, flush=flush)
+    tuned_ms = dev_ms(lambda: per_scene("auto"), steps=1, warmup=1, flush=flush)
+    mq = lambda ms: total / ms / 1e3  # noqa: E731
+    return {"workload": f"512 star polylines, {sum(e.shape[0] for _, e in geo)} segments, {total} queries "
+                        f"(cp {ns[0]}, ray {ns[1]}, sil {ns[2]})", "build_s": build_s,
+            "batched_graph": {"ms": graph_ms, "mqueries_per_s": mq(graph_ms)},
+            "batched_eager": {"ms": eager_ms, "mqueries_per_s": mq(eager_ms)},
+            "batched_kind_alone_ms": kind_ms,
+            "plain_per_scene_exact": {"ms": plain_ms, "mqueries_per_s": mq(plain_ms), "launch_calls": 3 * len(scenes)},
+            "per_scene_tuned": {"ms": tuned_ms, "mqueries_per_s": mq(tuned_ms)},
+            "batched_vs_plain": plain_ms / graph_ms}
+
+
+def section_c4(args, dev):
+    """Serving: 64 displaced icospheres (levels 4-8) resident on the device, 120 GB
+    admission budget, requests with a uniform scene, kind 50/30/20 cp/ray/silhouette and
+    log-uniform 1-262,144 queries U[-2,2]^3; open-loop Poisson arrivals at fractions of
+    the batched server's saturation rate; latency from scheduled arrival to results in
+    the request's host arrays."""
+    from concurrent.futures import ThreadPoolExecutor
+    from gquery_b200 import workloads as W
+    from gquery_b200.scene import Scene
+    from gquery_b200.serving import HostRequest, Server, poisson_arrivals, request_mix, result_fields, summarize
+    levels = W.config4_levels()
+    t0 = time.perf_counter()
+
+    def build(i):
+        v, f = W.config4_scene(i, levels[i])
+        return Scene(v, f, 3, device=dev.index or 0, build_snch=True, n_threads=1)
+    order = sorted(range(len(levels)), key=lambda i: -levels[i])
+    with ThreadPoolExecutor(os.cpu_count() or 8) as ex:
+        built = dict(zip(order, ex.map(build, order)))
+    scenes = [built[i] for i in range(len(levels))]
+    build_s = time.perf_counter() - t0
+    rng = np.random.default_rng(5)
+    pool = 1 << 22
+    pts = rng.uniform(-2.0, 2.0, size=(pool, 3)).astype(np.float32)
+    dd = rng.standard_normal((pool, 3))
+    dd = (dd / np.linalg.norm(dd, axis=1, keepdims=True)).astype(np.float32)
+    pools = {k: {nm: np.zeros(pool * c, dt) for nm, (c, dt) in result_fields(k, 3).items()} for k in ("cp", "ray", "sil")}
+    cursor = {"cp": 0, "ray": 0, "sil": 0}
+    sc_ids, kinds, counts = request_mix(args.c4_requests, len(scenes), np.random.default_rng(1))
+    reqs = []
+    for s_i, k, c in zip(sc_ids, kinds, counts):
+        kind = ("cp", "ray", "sil")[k]
+        o = int(rng.integers(0, pool - c))
+        off = cursor[kind] if cursor[kind] + c <= pool else 0
+        cursor[kind] = off + c
+        out = {nm: (pools[kind][nm][off * cc:(off + c) * cc].reshape(cc, c) if cc > 1 else pools[kind][nm][off:off + c])
+               for nm, (cc, dt) in result_fields(kind, 3).items()}
+        reqs.append(HostRequest.make(int(s_i), kind, pts[o:o + c], dd[o:o + c] if kind == "ray" else None, None,
+                                     out=out))
+    kind_of = np.array([r.kind for r in reqs])
+
+    def by_kind(res):
+        lat = (res["t_done"] - res["t_submit"]) * 1e3
+        return {k: {"p50_ms": float(np.percentile(lat[kind_of == k], 50)),
+                    "p99_ms": float(np.percentile(lat[kind_of == k], 99))} for k in ("cp", "ray", "sil")}
+
+    out = {"workload": f"64 icospheres levels 4-8 ({sum(20 * 4 ** x for x in levels)} triangles), "
+                       f"{len(reqs)} requests, {int(counts.sum())} queries", "build_s": build_s,
+           "note": "loads are fractions of the batched server's saturation arrival rate; the plain "
+                   "per-request server is run at the same arrival rate"}
+    sat_rate = None
+    for mode in ("batched", "per_request"):
+        srv = Server(scenes, budget_bytes=120 << 30, step_queries=1 << 18, max_inflight=2,
+                     per_request=(mode == "per_request"))
+        srv.run_trace(reqs[:40], np.zeros(40))  # warm-up
+        res = srv.run_trace(reqs, np.zeros(len(reqs)))
+        sat = summarize(res)
+        entry = {"saturation": {"mqueries_per_s": sat["mqueries_per_s"], "requests_per_s": sat["requests_per_s"]},
+                 "loads": []}
+        if sat_rate is None:
+            sat_rate = sat["requests_per_s"]
+        for frac in ((0.5, 0.8) if mode == "batched" else (0.8,)):
+            r = srv.run_trace(reqs, poisson_arrivals(frac * sat_rate, len(reqs), np.random.default_rng(9)))
+            sm = summarize(r)
+            entry["loads"].append({"load_of_batched_peak": frac, "arrivals_per_s": frac * sat_rate,
+                                   "mqueries_per_s": sm["mqueries_per_s"], "p50_ms": sm["p50_ms"],
+                                   "p99_ms": sm["p99_ms"], "steps": sm["steps"], "by_kind": by_kind(r)})
+        st = srv.stats()
+        assert st["device_error"] == 0
+        entry["ring_device_bytes"] = st["device_bytes"]
+        out[mode] = entry
+        srv.close()
+    return out
 
 
 def run_reference(args):
@@ -378,6 +582,15 @@ def main():
             "gpu_launches": 4 * args.steps,
             "gpu_launches_note": "own kernels per step: 2 Morton-key + 2 traversal (CUB radix-sort kernels extra)",
         }
+        sections = [x for x in args.sections.split(",") if x and x != "none"] if world == 1 else []
+        flush_buf = flush
+        for name, fn in (("c2", lambda: section_c2(args, dev, flush_buf)), ("c3", lambda: section_c3(args, dev, flush_buf)),
+                         ("c4", lambda: section_c4(args, dev))):
+            if name in sections:
+                key = {"c2": "silhouette_c2", "c3": "batched_c3", "c4": "serving_c4"}[name]
+                t_sec = time.perf_counter()
+                line[key] = fn()
+                line[key]["section_wall_s"] = time.perf_counter() - t_sec
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
