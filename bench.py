@@ -557,10 +557,12 @@ def main():
             b = b_cp if dominant == "cp" else b_ray
             t_ms = main_res[f"{dominant}_ms"]
             achieved = b * n / (t_ms / 1e3) / 1e9
-            tr = traffic_per_query().get(f"{dominant}3d_{args.variant}")
             tuned_v = scene.get_tuning(dominant)["variant"] if args.variant == "auto" else args.variant
+            tr = traffic_per_query().get(f"{dominant}3d_{tuned_v}")
             roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                     "traffic": (tr * n if tr else None), "kernel": f"{dominant}3d_{tuned_v}",
+                    "traffic_note": "DRAM bytes per query from an ncu capture at 1,048,576 queries "
+                                    "(profiles/traffic.json), scaled to the launch's query count",
                     "algorithmic_bytes_per_query": b, "peak_source": peak_kind,
                     "note": "achieved = reference binary-traversal bytes (oracle visit counts) / kernel time"}
         line = {
