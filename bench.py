@@ -409,11 +409,11 @@ def main():
     import torch
     import torch.distributed as dist
     from gquery_b200 import workloads as W
+    from gquery_b200.distributed import max_over_ranks, shard_seed
+    from gquery_b200.distributed import world as dist_world
     from gquery_b200.scene import Scene
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, world, local = dist_world()
     torch.cuda.set_device(local)
     if world > 1:
         import datetime
@@ -428,8 +428,8 @@ def main():
     V, F = W.config1_mesh()
     scene = Scene(V, F, 3, device=local, build_snch=False, build_wide=True)
     # disjoint query shards per rank (weak scaling)
-    q_h = W.uniform_points(n, 3, seed=1 + 1000 * rank)
-    o_h, d_h = W.rays(n, 3, seed=2 + 1000 * rank)
+    q_h = W.uniform_points(n, 3, seed=shard_seed(1, rank))
+    o_h, d_h = W.rays(n, 3, seed=shard_seed(2, rank))
     q = torch.as_tensor(q_h).to(dev)
     o = torch.as_tensor(o_h).to(dev)
     d = torch.as_tensor(d_h).to(dev)
@@ -482,9 +482,8 @@ def main():
                "cp_ms": statistics.mean(p[1] for p in per), "order_ray_ms": statistics.mean(p[2] for p in per),
                "ray_ms": statistics.mean(p[3] for p in per), "wall_ms_per_step": 1e3 * t_wall / steps}
         if world > 1:  # max over ranks
-            t = torch.tensor([res["step_ms"], res["cp_ms"], res["ray_ms"]], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            res["step_ms"], res["cp_ms"], res["ray_ms"] = (float(x) for x in t.tolist())
+            res["step_ms"], res["cp_ms"], res["ray_ms"] = max_over_ranks(
+                [res["step_ms"], res["cp_ms"], res["ray_ms"]], device=dev)
         return res, clk
 
     if args.no_compare:
@@ -537,9 +536,7 @@ def main():
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / ks
         if world > 1:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+            ms = max_over_ranks([ms], device=dev)[0]
         e2e = {"value": total_q / (ms / 1e3) / 1e6, "unit": "Mqueries/s", "ms_per_step": ms,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
 
