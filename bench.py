@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the exact and wide8 side-by-side runs")
+    ap.add_argument("--no-autotune", action="store_true", help="use the built-in tuning table as it is")
     ap.add_argument("--sections", default="c2,c3,c4",
                     help="beside the headline (cp + rays on the level-8 mesh): c2 silhouettes on the level-7 "
                          "mesh, c3 512 uneven 2D scenes in one batched launch, c4 serving 64 meshes; "
@@ -238,8 +239,21 @@ def section_c3(args, dev, flush):
     sil_ids, sil_pts = (torch.as_tensor(a).to(dev) for a in Q["sil"])
     ns = (cp_ids.numel(), ray_ids.numel(), sil_ids.numel())
     total = sum(ns)
-    b = SceneBatch(scenes, max(ns))
-    out = b.alloc(*ns)
+    from gquery_b200.autotune import tune_batch
+    out = None
+
+    def make(**choice):
+        return SceneBatch(scenes, max(ns), **choice)
+
+    def step(bb):
+        nonlocal out
+        if out is None:
+            out = bb.alloc(*ns)
+        bb.run(cp=(cp_pts, cp_ids), ray=(ray_o, ray_d, ray_ids), sil=(sil_pts, sil_ids), out=out)
+    t_tune = time.perf_counter()
+    tb = tune_batch(make, step)
+    tune_s = time.perf_counter() - t_tune
+    b = SceneBatch(scenes, max(ns), **tb["best"])
     eager_ms = dev_ms(lambda: b.run(cp=(cp_pts, cp_ids), ray=(ray_o, ray_d, ray_ids), sil=(sil_pts, sil_ids),
                                     out=out), steps=5, warmup=3, flush=flush)
     kind_ms = {k: dev_ms(lambda: b.run(out=out, **a), steps=3, warmup=1, flush=flush) for k, a in
@@ -279,7 +293,9 @@ def section_c3(args, dev, flush):
             "batched_kind_alone_ms": kind_ms,
             "plain_per_scene_exact": {"ms": plain_ms, "mqueries_per_s": mq(plain_ms), "launch_calls": 3 * len(scenes)},
             "per_scene_tuned": {"ms": tuned_ms, "mqueries_per_s": mq(tuned_ms)},
-            "batched_vs_plain": plain_ms / graph_ms}
+            "batched_vs_plain": plain_ms / graph_ms,
+            "autotune": {"best": tb["best"], "seconds": tune_s,
+                         "table_ms": {"/".join(t["choice"].values()): t["ms"] for t in tb["table"]}}}
 
 
 def section_c4(args, dev):
@@ -491,6 +507,19 @@ def main():
     else:
         plain, _ = timed("exact", max(2, args.steps // 2), 2)
         quant, _ = timed("wide8", max(2, args.steps // 2), 2)
+    tuning_report = None
+    if args.variant == "auto" and not args.no_autotune:
+        # the project's autotuner picks node width, stack depth and block shape on this
+        # rank's own queries before the timed run (every candidate checked against exact)
+        from gquery_b200.autotune import tune
+        t_tune = time.perf_counter()
+        r_cp = tune(scene, "cp", (q,), verify=True)
+        r_ray = tune(scene, "ray", (o, d), verify=True)
+        tuning_report = {"seconds": time.perf_counter() - t_tune,
+                         "candidates": {"cp": len(r_cp.table), "ray": len(r_ray.table)},
+                         "cp_table_ms": {f"{t['config']['variant']}/b{t['config']['block']}/k{t['config']['stack']}"
+                                         f"/p{t['config']['packet']}s{t['config']['sorted']}r{t['config']['persist']}": t["ms"]
+                                         for t in r_cp.table}}
     main_res, clocks = timed(args.variant, args.steps, max(3, args.warmup), clocks=True)
     assert scene.device_error() == 0, "device error flag raised"
 
@@ -500,45 +529,94 @@ def main():
     quant_value = total_q / (quant["step_ms"] / 1e3) / 1e6 if quant else None
 
     # ---- end to end through the public API with host buffers ----
+    # Every step copies its inputs from pinned host memory, answers them and copies every
+    # record field back to pinned host memory.  Steps alternate between two lanes (own
+    # device buffers, own streams), so one step's copies overlap another's traversals;
+    # within a step the ray inputs go up while closest points run and the closest-point
+    # records come back while rays run.
     e2e = None
     if not args.no_e2e:
         qh = torch.as_tensor(q_h).pin_memory()
         oh = torch.as_tensor(o_h).pin_memory()
         dh = torch.as_tensor(d_h).pin_memory()
-        host_cp = {k: torch.empty(v.shape, dtype=v.dtype).pin_memory() for k, v in vars(cp_out).items()}
-        host_ray = {k: torch.empty(v.shape, dtype=v.dtype).pin_memory() for k, v in vars(ray_out).items()}
-        qd, od, dd = torch.empty_like(q), torch.empty_like(o), torch.empty_like(d)
+
+        class Lane:
+            def __init__(self, first):
+                self.qd, self.od, self.dd = torch.empty_like(q), torch.empty_like(o), torch.empty_like(d)
+                self.cp = cp_out if first else scene.alloc_cp(n)
+                self.ray = ray_out if first else scene.alloc_ray(n)
+                self.scratch = scratch if first else torch.empty_like(scratch)
+                self.perm_q = torch.empty(n, dtype=torch.int32, device=dev)
+                self.perm_o = torch.empty(n, dtype=torch.int32, device=dev)
+                self.host_cp = {k: torch.empty(v.shape, dtype=v.dtype).pin_memory() for k, v in vars(self.cp).items()}
+                self.host_ray = {k: torch.empty(v.shape, dtype=v.dtype).pin_memory() for k, v in vars(self.ray).items()}
+                self.s_in, self.s_run, self.s_out = (torch.cuda.Stream(device=dev) for _ in range(3))
+                self.ev = {k: torch.cuda.Event() for k in ("q", "od", "cp", "ray", "done")}
+                self.used = False
+
+        lanes = [Lane(True), Lane(False)]
         h2d = 3 * qh.numel() * 4
-        d2h = sum(t.numel() * t.element_size() for t in host_cp.values()) + \
-            sum(t.numel() * t.element_size() for t in host_ray.values())
+        d2h = sum(t.numel() * t.element_size() for t in lanes[0].host_cp.values()) + \
+            sum(t.numel() * t.element_size() for t in lanes[0].host_ray.values())
 
-        def e2e_step():
-            qd.copy_(qh, non_blocking=True)
-            od.copy_(oh, non_blocking=True)
-            dd.copy_(dh, non_blocking=True)
-            r1 = scene.closest_point(qd, variant=args.variant, out=cp_out, scratch=scratch)
-            r2 = scene.intersect(od, dd, variant=args.variant, out=ray_out, scratch=scratch)
-            for k, v in vars(r1).items():
-                host_cp[k].copy_(v, non_blocking=True)
-            for k, v in vars(r2).items():
-                host_ray[k].copy_(v, non_blocking=True)
+        def e2e_step(ln, start_ev):
+            ev = ln.ev
+            with torch.cuda.stream(ln.s_in):
+                ln.s_in.wait_event(start_ev)
+                if ln.used:
+                    ln.s_in.wait_event(ev["ray"])  # previous step of this lane has read its inputs
+                ln.qd.copy_(qh, non_blocking=True)
+                ev["q"].record(ln.s_in)
+                ln.od.copy_(oh, non_blocking=True)
+                ln.dd.copy_(dh, non_blocking=True)
+                ev["od"].record(ln.s_in)
+            r = ln.s_run
+            r.wait_event(ev["q"])
+            if ln.used:
+                r.wait_event(ev["done"])  # previous records of this lane are back on the host
+            scene.order(ln.qd, out=ln.perm_q, scratch=ln.scratch, stream=r)
+            scene.closest_point(ln.qd, variant=args.variant, out=ln.cp, order=ln.perm_q, scratch=ln.scratch, stream=r)
+            ev["cp"].record(r)
+            r.wait_event(ev["od"])
+            scene.order(ln.od, out=ln.perm_o, scratch=ln.scratch, stream=r)
+            scene.intersect(ln.od, ln.dd, variant=args.variant, out=ln.ray, order=ln.perm_o, scratch=ln.scratch,
+                            stream=r)
+            ev["ray"].record(r)
+            with torch.cuda.stream(ln.s_out):
+                ln.s_out.wait_event(ev["cp"])
+                for k, v in vars(ln.cp).items():
+                    ln.host_cp[k].copy_(v, non_blocking=True)
+                ln.s_out.wait_event(ev["ray"])
+                for k, v in vars(ln.ray).items():
+                    ln.host_ray[k].copy_(v, non_blocking=True)
+                ev["done"].record(ln.s_out)
+            ln.used = True
 
-        for _ in range(2):
-            e2e_step()
-        torch.cuda.synchronize()
+        def e2e_run(k):
+            cur = torch.cuda.current_stream()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(cur)
+            for i in range(k):
+                e2e_step(lanes[i % 2], e0)
+            for ln in lanes:
+                if ln.used:
+                    cur.wait_event(ln.ev["done"])
+            e1.record(cur)
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1)
+
+        e2e_run(4)  # warm-up
         barrier()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        ks = max(2, args.steps)
-        for _ in range(ks):
-            e2e_step()
-        e1.record()
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / ks
+        ks = max(4, args.steps)
+        ms = e2e_run(ks) / ks
         if world > 1:
             ms = max_over_ranks([ms], device=dev)[0]
+        # the records that came back equal the device records of the timed run
+        ok = all(torch.equal(lanes[0].host_cp[k], v.cpu()) for k, v in vars(lanes[0].cp).items())
         e2e = {"value": total_q / (ms / 1e3) / 1e6, "unit": "Mqueries/s", "ms_per_step": ms,
-               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "lanes": 2, "host_records_match": ok,
+               "note": "public API (Scene.order / closest_point / intersect) on pinned host buffers; steps "
+                       "alternate between two lanes so copies overlap traversals"}
 
     line = None
     if rank == 0:
@@ -574,7 +652,7 @@ def main():
                                           "cp_ms": quant["cp_ms"], "ray_ms": quant["ray_ms"],
                                           "vs_plain": quant_value / plain_value},
             "tuned": {"cp": scene.get_tuning("cp"), "ray": scene.get_tuning("ray"),
-                      "vs_plain": value / plain_value if plain else None},
+                      "vs_plain": value / plain_value if plain else None, "autotune": tuning_report},
             "breakdown_ms": {k: main_res[k] for k in ("order_cp_ms", "cp_ms", "order_ray_ms", "ray_ms",
                                                       "wall_ms_per_step")},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,

@@ -77,7 +77,7 @@ class SilOut(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("variant", C.c_int32), ("packet", C.c_int32), ("sorted", C.c_int32), ("persist", C.c_int32),
-                ("budget", C.c_int32)]
+                ("budget", C.c_int32), ("block", C.c_int32), ("stack", C.c_int32)]
 
 
 class QueryOpts(C.Structure):

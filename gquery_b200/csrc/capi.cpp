@@ -153,12 +153,19 @@ void default_tuning(gq_scene *s) {
     }
 }
 
-gqd::Tune to_tune(const gq_tuning &t) {
+// Launch choices of one call: the tuning entry of `kind`, with the short warp-coherent
+// stack kept only when the tree fits in it (the binary walk keeps at most one entry per
+// level, the 8-wide walk up to seven).
+gqd::Tune to_tune(const gq_scene *s, int kind, int variant) {
+    const gq_tuning &t = s->tune[kind];
     gqd::Tune r;
     r.packet = t.packet;
     r.sorted = t.sorted;
     r.persist = t.persist;
     r.budget = t.budget > 0 ? t.budget : 32;
+    r.block = t.block > 0 ? t.block : 128;
+    const int need = variant == GQ_VARIANT_WIDE8 ? s->wide_stack : s->exact_stack;
+    r.stack = (t.stack == 32 && need <= 32) ? 32 : 0;
     return r;
 }
 
@@ -297,6 +304,10 @@ gq_status gq_scene_set_tuning(gq_scene *s, int32_t kind, const gq_tuning *t) {
     if (t->variant < 0 || t->variant > 3 || t->variant == GQ_VARIANT_AUTO)
         return fail(GQ_ERR_INVALID, "tuning variant must be EXACT, WIDE8 or COHERENT");
     if (t->variant == GQ_VARIANT_WIDE8 && !s->has_wide) return fail(GQ_ERR_UNSUPPORTED, "scene has no wide BVH");
+    if (t->block != 0 && t->block != 64 && t->block != 128 && t->block != 256)
+        return fail(GQ_ERR_INVALID, "block must be 0 (default), 64, 128 or 256");
+    if (t->stack != 0 && t->stack != 32) return fail(GQ_ERR_INVALID, "stack must be 0 (full depth) or 32");
+    if (t->budget < 0) return fail(GQ_ERR_INVALID, "budget must be >= 0");
     s->tune[kind] = *t;
     return GQ_OK;
 }
@@ -432,7 +443,7 @@ gq_status gq_closest_point(const gq_scene *s, gq_vecs q, int64_t n, const gq_cp_
     const int32_t *perm = nullptr;
     unsigned long long *counter = nullptr;
     if ((st = prepare_order(s, q, n, opts, cs, scr, &perm, &counter)) != GQ_OK) return st;
-    cudaError_t e = gqd::launch_cp(s->dev, v, to_tune(s->tune[GQ_KIND_CLOSEST_POINT]), q, n, perm, *out, counter, cs);
+    cudaError_t e = gqd::launch_cp(s->dev, v, to_tune(s, GQ_KIND_CLOSEST_POINT, v), q, n, perm, *out, counter, cs);
     if (e != cudaSuccess) return fail_cuda(e, "closest_point launch");
     return GQ_OK;
 }
@@ -455,7 +466,7 @@ gq_status gq_closest_point_noalloc(const gq_scene *s, gq_vecs q, int64_t n, cons
     if (st != GQ_OK) return st;
     if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "scene was built without a device copy");
     DeviceGuard g(s->device);
-    cudaError_t e = gqd::noalloc_closest_point(s->dev, v, to_tune(s->tune[GQ_KIND_CLOSEST_POINT]), q, n, sort,
+    cudaError_t e = gqd::noalloc_closest_point(s->dev, v, to_tune(s, GQ_KIND_CLOSEST_POINT, v), q, n, sort,
                                                *out, (cudaStream_t)stream);
     if (e != cudaSuccess) return fail_cuda(e, "closest_point_noalloc");
     return GQ_OK;
@@ -477,7 +488,7 @@ gq_status gq_intersect(const gq_scene *s, gq_vecs origin, gq_vecs dir, const flo
     const int32_t *perm = nullptr;
     unsigned long long *counter = nullptr;
     if ((st = prepare_order(s, origin, n, opts, cs, scr, &perm, &counter)) != GQ_OK) return st;
-    cudaError_t e = gqd::launch_ray(s->dev, v, to_tune(s->tune[GQ_KIND_INTERSECT]), origin, dir, r_max, n, perm,
+    cudaError_t e = gqd::launch_ray(s->dev, v, to_tune(s, GQ_KIND_INTERSECT, v), origin, dir, r_max, n, perm,
                                     *out, counter, cs);
     if (e != cudaSuccess) return fail_cuda(e, "intersect launch");
     return GQ_OK;
@@ -502,8 +513,8 @@ gq_status gq_closest_silhouette(const gq_scene *s, gq_vecs x, const float *r_max
     unsigned long long *counter = nullptr;
     gq_status st;
     if ((st = prepare_order(s, x, n, opts, cs, scr, &perm, &counter)) != GQ_OK) return st;
-    const gq_tuning &t = s->tune[GQ_KIND_SILHOUETTE];
-    cudaError_t e = gqd::launch_sil(s->dev, v, x, r_max, n, perm, *out, counter, t.persist, t.budget, cs);
+    cudaError_t e = gqd::launch_sil(s->dev, v, to_tune(s, GQ_KIND_SILHOUETTE, v), x, r_max, n, perm, *out, counter,
+                                    cs);
     if (e != cudaSuccess) return fail_cuda(e, "closest_silhouette launch");
     return GQ_OK;
 }

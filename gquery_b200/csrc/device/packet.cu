@@ -9,17 +9,17 @@ namespace gqd {
 
 namespace {
 
-constexpr int kBlock = 128;
+constexpr int kMaxBlock = 256;
 
 __device__ __forceinline__ float qget(const gq_vecs &v, int64_t i, int k) {
     return v.ptr[(int64_t)k * v.comp_stride + i * v.elem_stride];
 }
 
-template <int D, int LAYOUT, bool MINFIRST>
-__global__ void __launch_bounds__(kBlock) k_cp_packet(DevScene s, gq_vecs q, int64_t n, const int32_t *perm,
-                                                      gq_cp_out o, unsigned long long *counter) {
+template <int D, int LAYOUT, bool MINFIRST, int STK>
+__global__ void __launch_bounds__(kMaxBlock) k_cp_packet(DevScene s, gq_vecs q, int64_t n, const int32_t *perm,
+                                                         gq_cp_out o, unsigned long long *counter) {
     const unsigned lane = threadIdx.x & 31u;
-    int2 stk[pkt::kPStack];  // (ref, this lane's key); refs are the same in every lane
+    int2 stk[STK];  // (ref, this lane's key); refs are the same in every lane
     for (;;) {
         unsigned long long base = 0;
         if (lane == 0) base = atomicAdd(counter, 32ull);
@@ -34,7 +34,7 @@ __global__ void __launch_bounds__(kBlock) k_cp_packet(DevScene s, gq_vecs q, int
         float r = kInf;
         int idx = -1;
         bool ovf = false;
-        pkt::closest_point<D, LAYOUT, MINFIRST>(s, __ballot_sync(0xffffffffu, alive), p, r, idx, ovf, stk);
+        pkt::closest_point<D, LAYOUT, MINFIRST, STK>(s, __ballot_sync(0xffffffffu, alive), p, r, idx, ovf, stk);
         if (ovf && lane == 0 && s.err) atomicOr(s.err, GQ_DEVERR_STACK);
         if (alive) {
             if (D == 3)
@@ -45,35 +45,45 @@ __global__ void __launch_bounds__(kBlock) k_cp_packet(DevScene s, gq_vecs q, int
     }
 }
 
-template <int D, int LAYOUT, bool MINFIRST>
-cudaError_t launch(const DevScene &s, gq_vecs q, int64_t n, const int32_t *perm, const gq_cp_out &o,
+template <int D, int LAYOUT, bool MINFIRST, int STK>
+cudaError_t launch(const DevScene &s, int block, gq_vecs q, int64_t n, const int32_t *perm, const gq_cp_out &o,
                    unsigned long long *counter, cudaStream_t st) {
-    static int bps = 0, n_sm = 0;
-    if (!bps) {
+    static int bps[3] = {0, 0, 0}, n_sm = 0;
+    int slot = block_slot(block);
+    if (slot < 0) slot = 1, block = 128;
+    if (!bps[slot]) {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_cp_packet<D, LAYOUT, MINFIRST>, kBlock, 0);
-        if (bps < 1) bps = 1;
+        int b = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_cp_packet<D, LAYOUT, MINFIRST, STK>, block, 0);
+        bps[slot] = b < 1 ? 1 : b;
     }
     const int64_t warps = (n + 31) / 32;
-    const int64_t want = std::min<int64_t>((int64_t)bps * n_sm, (warps * 32 + kBlock - 1) / kBlock);
+    const int64_t want = std::min<int64_t>((int64_t)bps[slot] * n_sm, (warps * 32 + block - 1) / block);
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
-    k_cp_packet<D, LAYOUT, MINFIRST><<<dim3((unsigned)want), kBlock, 0, st>>>(s, q, n, perm, o, counter);
+    k_cp_packet<D, LAYOUT, MINFIRST, STK><<<dim3((unsigned)want), block, 0, st>>>(s, q, n, perm, o, counter);
     return cudaGetLastError();
+}
+
+template <int D, int LAYOUT, bool MINFIRST>
+cudaError_t launch_stk(const DevScene &s, const Tune &t, gq_vecs q, int64_t n, const int32_t *perm,
+                       const gq_cp_out &o, unsigned long long *counter, cudaStream_t st) {
+    if (t.stack == 32) return launch<D, LAYOUT, MINFIRST, 32>(s, t.block, q, n, perm, o, counter, st);
+    return launch<D, LAYOUT, MINFIRST, pkt::kPStack>(s, t.block, q, n, perm, o, counter, st);
 }
 
 }  // namespace
 
-cudaError_t launch_cp_packet(const DevScene &s, int layout, gq_vecs q, int64_t n, const int32_t *perm,
-                             const gq_cp_out &o, unsigned long long *counter, cudaStream_t st) {
+cudaError_t launch_cp_packet(const DevScene &s, int layout, const Tune &t, gq_vecs q, int64_t n,
+                             const int32_t *perm, const gq_cp_out &o, unsigned long long *counter, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
     // layout: 0 binary pairs, 1 quantised 8-wide (children sorted), 2 quantised 8-wide (nearest first)
-    if (s.dim == 2) return launch<2, 0, false>(s, q, n, perm, o, counter, st);
-    if (layout == 2) return launch<3, 1, true>(s, q, n, perm, o, counter, st);
-    if (layout == 1) return launch<3, 1, false>(s, q, n, perm, o, counter, st);
-    return launch<3, 0, false>(s, q, n, perm, o, counter, st);
+    if (s.dim == 2) return launch_stk<2, 0, false>(s, t, q, n, perm, o, counter, st);
+    if (layout == 2) return launch_stk<3, 1, true>(s, t, q, n, perm, o, counter, st);
+    if (layout == 1) return launch_stk<3, 1, false>(s, t, q, n, perm, o, counter, st);
+    return launch_stk<3, 0, false>(s, t, q, n, perm, o, counter, st);
 }
 
 }  // namespace gqd

@@ -107,8 +107,9 @@ __device__ __forceinline__ void leaf(const DevScene &s, int ref, bool act, const
 // One traversal for the lanes in `mask` (warp-uniform).  All 32 lanes must call it.
 // r: this lane's squared search radius (+inf to start; lanes outside `mask` are
 // ignored), idx: its best item slot (-1: none).  LAYOUT 0: binary pairs,
-// 1: quantised 8-wide nodes (3D only).
-template <int D, int LAYOUT, bool MINFIRST>
+// 1: quantised 8-wide nodes (3D only).  STK: entries of the caller's stack `stk`; the
+// warp stops with `ovf` set rather than overflow it.
+template <int D, int LAYOUT, bool MINFIRST, int STK = kPStack>
 __device__ __forceinline__ void closest_point(const DevScene &s, unsigned mask, const float *p, float &r, int &idx,
                                               bool &ovf, int2 *stk) {
     const unsigned lane = threadIdx.x & 31u;
@@ -169,7 +170,7 @@ __device__ __forceinline__ void closest_point(const DevScene &s, unsigned mask, 
             if (ml && mr) {
                 const float kl = warp_min(hl ? a2l : kInf), kr = warp_min(hr ? a2r : kInf);
                 const bool right_first = kr < kl;
-                if (sp + 1 >= kPStack) {
+                if (sp + 1 >= STK) {
                     ovf = true;
                     break;
                 }
@@ -229,7 +230,7 @@ __device__ __forceinline__ void closest_point(const DevScene &s, unsigned mask, 
                 cur = kNone;
                 continue;
             }
-            if (sp + cnt > kPStack) {
+            if (sp + cnt > STK) {
                 ovf = true;
                 break;
             }

@@ -16,6 +16,7 @@ namespace gqd {
 namespace {
 
 constexpr int kBlock = 128;
+constexpr int kMaxBlock = 256;
 
 __device__ __forceinline__ float qget(const gq_vecs &v, int64_t i, int k) {
     return v.ptr[(int64_t)k * v.comp_stride + i * v.elem_stride];
@@ -50,7 +51,7 @@ __device__ __forceinline__ void sil_write(const DevScene &s, const snch::Lane<D>
 // Warp-coherent closest silhouette (sil_packet.cuh): persistent warps take 32
 // consecutive queries of the sorted order at a time.
 template <int D>
-__global__ void __launch_bounds__(kBlock) k_sil_packet(DevScene s, gq_vecs xq, const float *rmax_in, int64_t n,
+__global__ void __launch_bounds__(kMaxBlock) k_sil_packet(DevScene s, gq_vecs xq, const float *rmax_in, int64_t n,
                                                        const int32_t *perm, gq_sil_out o, unsigned long long *counter) {
     const unsigned lane = threadIdx.x & 31u;
     snch::Stack stk;
@@ -100,7 +101,7 @@ __global__ void __launch_bounds__(kBlock) k_sil_exact(DevScene s, gq_vecs xq, co
 // (warp-aggregated atomic on a per-call counter), so a warp never waits for its
 // slowest query.  Same visit order and answers as k_sil_exact.
 template <int D>
-__global__ void __launch_bounds__(kBlock) k_sil_persist(DevScene s, gq_vecs xq, const float *rmax_in, int64_t n,
+__global__ void __launch_bounds__(kMaxBlock) k_sil_persist(DevScene s, gq_vecs xq, const float *rmax_in, int64_t n,
                                                         const int32_t *perm, gq_sil_out o,
                                                         unsigned long long *counter, int budget) {
     const unsigned lane = threadIdx.x & 31u;
@@ -530,46 +531,41 @@ cudaError_t morton_order(const DevScene &s, gq_vecs q, int64_t n, int32_t *perm,
     return cub::DeviceRadixSort::SortPairs(p, tb, k_in, k_out, v_in, perm, (int)n, 0, end_bit, st);
 }
 
-cudaError_t launch_sil(const DevScene &s, int variant, gq_vecs x, const float *r_max, int64_t n,
-                       const int32_t *perm, const gq_sil_out &o, unsigned long long *counter, int persist,
-                       int budget, cudaStream_t st) {
+cudaError_t launch_sil(const DevScene &s, int variant, const Tune &t, gq_vecs x, const float *r_max, int64_t n,
+                       const int32_t *perm, const gq_sil_out &o, unsigned long long *counter, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
-    static int bps[3][2] = {{0, 0}, {0, 0}, {0, 0}}, n_sm = 0;
+    static int bps[2][2][3] = {}, n_sm = 0;
     const int di = s.dim == 3 ? 1 : 0;
+    int slot = block_slot(t.block), block = t.block;
+    if (slot < 0) slot = 1, block = 128;
     const bool packet = variant == GQ_VARIANT_COHERENT && counter && n >= 32;
-    const bool refill = !packet && persist && counter && n > 4096;
+    const bool refill = !packet && t.persist && counter && n > 4096;
     if (packet || refill) {
         const int ki = packet ? 1 : 0;
-        if (!bps[ki][di]) {
-            int dev = 0;
+        if (!bps[ki][di][slot]) {
+            int dev = 0, b = 0;
             cudaGetDevice(&dev);
             cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-            int b = 0;
-            if (packet)
-                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, s.dim == 3 ? (const void *)k_sil_packet<3>
-                                                                             : (const void *)k_sil_packet<2>,
-                                                              kBlock, 0);
-            else
-                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, s.dim == 3 ? (const void *)k_sil_persist<3>
-                                                                             : (const void *)k_sil_persist<2>,
-                                                              kBlock, 0);
-            bps[ki][di] = b < 1 ? 1 : b;
+            const void *fn = packet ? (s.dim == 3 ? (const void *)k_sil_packet<3> : (const void *)k_sil_packet<2>)
+                                    : (s.dim == 3 ? (const void *)k_sil_persist<3> : (const void *)k_sil_persist<2>);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, block, 0);
+            bps[ki][di][slot] = b < 1 ? 1 : b;
         }
-        const int64_t want = std::min<int64_t>((int64_t)bps[ki][di] * n_sm, (n + kBlock - 1) / kBlock);
+        const int64_t want = std::min<int64_t>((int64_t)bps[ki][di][slot] * n_sm, (n + block - 1) / block);
         cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
         if (e != cudaSuccess) return e;
         const dim3 grid((unsigned)want);
         if (packet) {
             if (s.dim == 3)
-                k_sil_packet<3><<<grid, kBlock, 0, st>>>(s, x, r_max, n, perm, o, counter);
+                k_sil_packet<3><<<grid, block, 0, st>>>(s, x, r_max, n, perm, o, counter);
             else
-                k_sil_packet<2><<<grid, kBlock, 0, st>>>(s, x, r_max, n, perm, o, counter);
+                k_sil_packet<2><<<grid, block, 0, st>>>(s, x, r_max, n, perm, o, counter);
         } else {
-            const int b = budget > 0 ? budget : 32;
+            const int b = t.budget > 0 ? t.budget : 32;
             if (s.dim == 3)
-                k_sil_persist<3><<<grid, kBlock, 0, st>>>(s, x, r_max, n, perm, o, counter, b);
+                k_sil_persist<3><<<grid, block, 0, st>>>(s, x, r_max, n, perm, o, counter, b);
             else
-                k_sil_persist<2><<<grid, kBlock, 0, st>>>(s, x, r_max, n, perm, o, counter, b);
+                k_sil_persist<2><<<grid, block, 0, st>>>(s, x, r_max, n, perm, o, counter, b);
         }
         return cudaGetLastError();
     }

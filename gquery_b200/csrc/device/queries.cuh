@@ -42,7 +42,12 @@ struct Tune {
     int sorted = 1;   // warp-coherent wide nodes: 1 = children in distance order, 0 = nearest first
     int persist = 1;  // persistent warps with lane refill (per-thread traversal)
     int budget = 32;  // node visits between refills
+    int block = 128;  // threads per block: 64, 128 or 256
+    int stack = 0;    // warp-coherent closest point: 32 = short stack (trees that fit), 0 = full depth
 };
+
+// Index of a supported block size (64, 128, 256) for per-size launch caches; -1 otherwise.
+inline int block_slot(int block) { return block == 64 ? 0 : block == 128 ? 1 : block == 256 ? 2 : -1; }
 
 // `counter` is an 8-byte device word used by the persistent / warp-coherent kernels
 // (may be null: one query per thread then).
@@ -52,14 +57,13 @@ cudaError_t launch_ray(const DevScene &s, int variant, const Tune &t, gq_vecs x,
                        int64_t n, const int32_t *perm, const gq_ray_out &o, unsigned long long *counter,
                        cudaStream_t st);
 // Warp-coherent closest point; layout 0 = binary pairs, 1 / 2 = quantised 8-wide (3D): sorted / nearest first.
-cudaError_t launch_cp_packet(const DevScene &s, int layout, gq_vecs q, int64_t n, const int32_t *perm,
-                              const gq_cp_out &o, unsigned long long *counter, cudaStream_t st);
+cudaError_t launch_cp_packet(const DevScene &s, int layout, const Tune &t, gq_vecs q, int64_t n,
+                             const int32_t *perm, const gq_cp_out &o, unsigned long long *counter, cudaStream_t st);
 // Closest silhouette.  GQ_VARIANT_COHERENT (with a counter): warp-coherent traversal of
 // 32 sorted queries at a time; otherwise the reference order per lane, with persistent
-// lane refill when `persist` is set (`budget` steps between refills).
-cudaError_t launch_sil(const DevScene &s, int variant, gq_vecs x, const float *r_max, int64_t n,
-                       const int32_t *perm, const gq_sil_out &o, unsigned long long *counter, int persist,
-                       int budget, cudaStream_t st);
+// lane refill when t.persist is set (t.budget steps between refills).
+cudaError_t launch_sil(const DevScene &s, int variant, const Tune &t, gq_vecs x, const float *r_max, int64_t n,
+                       const int32_t *perm, const gq_sil_out &o, unsigned long long *counter, cudaStream_t st);
 cudaError_t launch_cp_brute(const DevScene &s, gq_vecs q, int64_t n, const gq_cp_out &o, cudaStream_t st);
 cudaError_t launch_ray_brute(const DevScene &s, gq_vecs x, gq_vecs v, const float *r_max, int64_t n,
                              const gq_ray_out &o, cudaStream_t st);

@@ -32,12 +32,12 @@ namespace gqd {
 namespace {
 
 using namespace trav;
-constexpr int kBlock = 128;
+constexpr int kMaxBlock = 256;
 
 
 // One query per thread.
 template <int D, bool RAY, bool WIDE, int CFG>
-__global__ void __launch_bounds__(kBlock) k_trav(DevScene s, gq_vecs a, gq_vecs b, const float *rmax_in, int64_t n,
+__global__ void __launch_bounds__(kMaxBlock) k_trav(DevScene s, gq_vecs a, gq_vecs b, const float *rmax_in, int64_t n,
                                                  const int32_t *perm, gq_cp_out oc, gq_ray_out orr) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(kBlock) k_trav(DevScene s, gq_vecs a, gq_vecs 
 
 // Persistent warps with lane refill.
 template <int D, bool RAY, bool WIDE, int CFG>
-__global__ void __launch_bounds__(kBlock) k_trav_persist(DevScene s, gq_vecs a, gq_vecs b, const float *rmax_in,
+__global__ void __launch_bounds__(kMaxBlock) k_trav_persist(DevScene s, gq_vecs a, gq_vecs b, const float *rmax_in,
                                                          int64_t n, const int32_t *perm, gq_cp_out oc,
                                                          gq_ray_out orr, unsigned long long *counter, int budget) {
     const unsigned lane = threadIdx.x & 31u;
@@ -93,24 +93,25 @@ cudaError_t launch_kind(const DevScene &s, const Tune &t, gq_vecs a, gq_vecs b, 
                         const int32_t *perm, const gq_cp_out &oc, const gq_ray_out &orr, unsigned long long *counter,
                         cudaStream_t st) {
     constexpr int CFG = 0;
+    int slot = block_slot(t.block), block = t.block;
+    if (slot < 0) slot = 1, block = 128;
     if (t.persist && counter && n > 4096) {
-        static int blocks_per_sm = 0, n_sm = 0;
-        if (!blocks_per_sm) {
-            int dev = 0;
+        static int blocks_per_sm[3] = {0, 0, 0}, n_sm = 0;
+        if (!blocks_per_sm[slot]) {
+            int dev = 0, b = 0;
             cudaGetDevice(&dev);
             cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_trav_persist<D, RAY, WIDE, CFG>, kBlock,
-                                                          0);
-            if (blocks_per_sm < 1) blocks_per_sm = 1;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_trav_persist<D, RAY, WIDE, CFG>, block, 0);
+            blocks_per_sm[slot] = b < 1 ? 1 : b;
         }
-        const int64_t want = std::min<int64_t>((int64_t)blocks_per_sm * n_sm, (n + kBlock - 1) / kBlock);
+        const int64_t want = std::min<int64_t>((int64_t)blocks_per_sm[slot] * n_sm, (n + block - 1) / block);
         cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
         if (e != cudaSuccess) return e;
-        k_trav_persist<D, RAY, WIDE, CFG><<<dim3((unsigned)want), kBlock, 0, st>>>(
+        k_trav_persist<D, RAY, WIDE, CFG><<<dim3((unsigned)want), block, 0, st>>>(
             s, a, b, rmax, n, perm, oc, orr, counter, std::max(1, t.budget));
     } else {
         k_trav<D, RAY, WIDE, CFG>
-            <<<dim3((unsigned)((n + kBlock - 1) / kBlock)), kBlock, 0, st>>>(s, a, b, rmax, n, perm, oc, orr);
+            <<<dim3((unsigned)((n + block - 1) / block)), block, 0, st>>>(s, a, b, rmax, n, perm, oc, orr);
     }
     return cudaGetLastError();
 }
@@ -123,9 +124,9 @@ cudaError_t launch_cp(const DevScene &s, int variant, const Tune &t, gq_vecs q, 
     const gq_ray_out none{};
     const bool wide = variant == GQ_VARIANT_WIDE8;
     if (counter && n >= 32) {
-        if (variant == GQ_VARIANT_COHERENT) return launch_cp_packet(s, 0, q, n, perm, o, counter, st);
+        if (variant == GQ_VARIANT_COHERENT) return launch_cp_packet(s, 0, t, q, n, perm, o, counter, st);
         if (wide && t.packet && s.dim == 3)
-            return launch_cp_packet(s, t.sorted ? 1 : 2, q, n, perm, o, counter, st);
+            return launch_cp_packet(s, t.sorted ? 1 : 2, t, q, n, perm, o, counter, st);
     }
     if (s.dim == 3)
         return wide ? launch_kind<3, false, true>(s, t, q, q, nullptr, n, perm, o, none, counter, st)

@@ -172,8 +172,8 @@ class Scene:
         return d
 
     def set_tuning(self, kind: str, variant: str, packet: int = 0, sorted: int = 1, persist: int = 1,
-                   budget: int = 32) -> None:
-        t = L.Tuning(VARIANTS[variant], packet, sorted, persist, budget)
+                   budget: int = 32, block: int = 0, stack: int = 0) -> None:
+        t = L.Tuning(VARIANTS[variant], packet, sorted, persist, budget, block, stack)
         L.check(L.lib().gq_scene_set_tuning(self._h, KINDS[kind], C.byref(t)))
 
     def scratch_bytes(self, n: int) -> int:

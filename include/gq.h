@@ -62,6 +62,8 @@ typedef struct {
     int32_t sorted;   /* warp-coherent wide nodes: children in distance order (else nearest first) */
     int32_t persist;  /* per-thread kernels: persistent warps, finished lanes take new queries */
     int32_t budget;   /* node visits between refills */
+    int32_t block;    /* threads per block of the persistent / warp-coherent kernels: 64, 128, 256 (0: 128) */
+    int32_t stack;    /* warp-coherent closest point: 32 = short traversal stack when the tree fits, 0 = full */
 } gq_tuning;
 
 typedef struct gq_scene gq_scene;

@@ -269,7 +269,7 @@ def test_cp3d_fast_variants_match_exact(mesh_c1, variant, tuning):
             mesh_c1.set_tuning("cp", variant, **tuning)
         b = to_np(mesh_c1.closest_point(q, variant=variant, sort=True))
     finally:
-        mesh_c1.set_tuning("cp", saved["variant"], saved["packet"], saved["sorted"], saved["persist"], saved["budget"])
+        mesh_c1.set_tuning("cp", **saved)
     rep = tie_report(a, b)
     assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0, rep
     assert rep["max_rel_d"] <= REL_TOL, rep
@@ -308,7 +308,7 @@ def test_sil_refill_bitwise_and_coherent_ties(dim, star, mesh_c2):
         scene.set_tuning("sil", "exact", persist=1, budget=7)
         b = to_np(scene.closest_silhouette(x, variant="exact"))
     finally:
-        scene.set_tuning("sil", saved["variant"], saved["packet"], saved["sorted"], saved["persist"], saved["budget"])
+        scene.set_tuning("sil", **saved)
     assert_bitwise(b, a, SIL_FIELDS, "sil refill ")
     for r_max in (math.inf, 0.3):
         ref = to_np(scene.closest_silhouette(x, r_max, variant="exact"))
