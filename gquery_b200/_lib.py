@@ -23,6 +23,7 @@ VARIANT_EXACT = 0
 VARIANT_WIDE8 = 1
 VARIANT_AUTO = 2
 VARIANT_COHERENT = 3
+VARIANT_WARP = 4
 
 KIND_CLOSEST_POINT = 0
 KIND_INTERSECT = 1
@@ -40,6 +41,7 @@ DEVERR_STACK = 1
 BATCH_CP_EXACT = 1
 BATCH_RAY_EXACT = 2
 BATCH_SIL_EXACT = 8
+BATCH_SIL_WARP = 16
 BATCH_ERR_SCENE = 1 << 8
 BATCH_ERR_NO_SNCH = 1 << 9
 SERVER_PER_REQUEST = 4
@@ -87,7 +89,8 @@ class QueryOpts(C.Structure):
 
 class ServerOpts(C.Structure):
     _fields_ = [("budget_bytes", C.c_int64), ("ring_queries", C.c_int64 * 3), ("step_queries", C.c_int64),
-                ("max_inflight", C.c_int32), ("flags", C.c_int32), ("sil_share", C.c_float)]
+                ("max_inflight", C.c_int32), ("flags", C.c_int32), ("sil_share", C.c_float),
+                ("sil_slots", C.c_int32), ("sil_step_queries", C.c_int64)]
 
 
 class Request(C.Structure):

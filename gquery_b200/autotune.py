@@ -3,8 +3,9 @@
 The reference has no launch choices to make (DrJit traces one kernel per call).  Here
 each scene carries a tuning table (``gq_scene_set_tuning``): per query kind the
 traversal variant - binary nodes in the reference order (``exact``), binary nodes walked
-once per warp of Morton-adjacent queries (``coherent``), or quantised 8-wide nodes
-(``wide8``, per lane or warp-coherent) - plus the persistent-refill budget, the threads
+once per warp of Morton-adjacent queries (``coherent``), quantised 8-wide nodes
+(``wide8``, per lane or warp-coherent) or, for silhouettes, one query per warp
+(``warp``) - plus the persistent-refill budget, the threads
 per block and, for the warp-coherent closest point, a 32-entry traversal stack when the
 tree fits in it.  :func:`tune` times every candidate on a sample of the caller's
 queries (CUDA events, median of a few launches), checks that each candidate's answers
@@ -58,6 +59,7 @@ def candidates(kind: str, dim: int, has_wide: bool, exact_stack: int, wide_stack
             return []
         for b in blocks:
             out.append(dict(variant="coherent", block=b))
+            out.append(dict(variant="warp", block=b))
             out.append(dict(variant="exact", persist=1, budget=32, block=b))
         out.append(dict(variant="exact", persist=0, block=128))
     else:
@@ -210,7 +212,7 @@ def tune(scene, kind: str, inputs: Sequence, *, cands: Optional[List[dict]] = No
 
 
 BATCH_CHOICES = [dict(cp_variant=c, ray_variant=r, sil_variant=s)
-                 for c in ("coherent", "exact") for r in ("wide8", "exact") for s in ("coherent", "exact")]
+                 for c in ("coherent", "exact") for r in ("wide8", "exact") for s in ("coherent", "warp", "exact")]
 
 
 def tune_batch(make_batch: Callable[..., object], run_step: Callable[[object], object],

@@ -5,8 +5,8 @@ mesh.py:120; Mesh.intersect_bvh, mesh.py:87; Mesh.closest_silhouette_snch,
 mesh.py:138; and the Polyline counterparts).  A :class:`SceneBatch` holds device views
 of many scenes of one dimension and answers a mixed step - closest points, rays and
 silhouette queries, each tagged with its scene - in one persistent launch, with the
-answers of the single-scene calls (closest points and silhouettes: ``coherent``; rays:
-``wide8`` when every scene has wide nodes).  ``run`` allocates nothing on the
+answers of the single-scene calls (closest points: ``coherent``; rays: ``wide8`` when
+every scene has wide nodes; silhouettes: ``warp``).  ``run`` allocates nothing on the
 device beyond the output records, so a step with fixed shapes can be recorded in a CUDA
 graph (:meth:`SceneBatch.capture`).
 """
@@ -37,21 +37,22 @@ class SceneBatch:
     fixed scratch for up to ``max_queries`` queries of each kind.
 
     ``cp_variant`` / ``sil_variant``: "coherent" (warp-coherent traversal) or "exact"
-    (reference visit order, one lane per query).  ``ray_variant``: "wide8" or "exact"."""
+    (reference visit order, one lane per query); silhouettes also "warp" (one query per
+    warp, for sparse queries).  ``ray_variant``: "wide8" or "exact"."""
 
     def __init__(self, scenes: Sequence[Scene], max_queries: int, *, cp_variant: str = "coherent",
-                 ray_variant: str = "wide8", sil_variant: str = "coherent"):
+                 ray_variant: str = "wide8", sil_variant: str = "warp"):
         if not scenes:
             raise ValueError("a batch needs at least one scene")
         if cp_variant not in ("coherent", "exact") or ray_variant not in ("wide8", "exact") or \
-                sil_variant not in ("coherent", "exact"):
-            raise ValueError("cp_variant: coherent|exact, ray_variant: wide8|exact, sil_variant: coherent|exact")
+                sil_variant not in ("coherent", "exact", "warp"):
+            raise ValueError("cp_variant: coherent|exact, ray_variant: wide8|exact, sil_variant: coherent|exact|warp")
         self.scenes = list(scenes)
         self.dim = self.scenes[0].dim
         self.torch_device = self.scenes[0].torch_device
         self.max_queries = int(max_queries)
         flags = (L.BATCH_CP_EXACT if cp_variant == "exact" else 0) | (L.BATCH_RAY_EXACT if ray_variant == "exact" else 0) | \
-            (L.BATCH_SIL_EXACT if sil_variant == "exact" else 0)
+            (L.BATCH_SIL_EXACT if sil_variant == "exact" else L.BATCH_SIL_WARP if sil_variant == "warp" else 0)
         arr = (C.c_void_p * len(self.scenes))(*[s.handle.value for s in self.scenes])
         h = C.c_void_p()
         L.check(L.lib().gq_batch_create(arr, len(self.scenes), self.max_queries, flags, C.byref(h)))

@@ -143,7 +143,7 @@ bool on_host_only(const gq_scene *s) { return s->device < 0; }
 // Built-in launch choices (measured on B200 for the benchmark scenes).
 void default_tuning(gq_scene *s) {
     for (int k = 0; k < 3; ++k) s->tune[k] = gq_tuning{GQ_VARIANT_EXACT, 0, 1, 0, 32};
-    s->tune[GQ_KIND_SILHOUETTE] = gq_tuning{GQ_VARIANT_COHERENT, 0, 1, 1, 32};
+    s->tune[GQ_KIND_SILHOUETTE] = gq_tuning{GQ_VARIANT_WARP, 0, 1, 1, 32};
     if (s->dim == 3) {
         s->tune[GQ_KIND_CLOSEST_POINT] = gq_tuning{GQ_VARIANT_COHERENT, 1, 1, 0, 32};
         s->tune[GQ_KIND_INTERSECT] = gq_tuning{s->has_wide ? GQ_VARIANT_WIDE8 : GQ_VARIANT_EXACT, 0, 1, 1, 32};
@@ -301,8 +301,10 @@ gq_status gq_scene_free(gq_scene *scene) {
 gq_status gq_scene_set_tuning(gq_scene *s, int32_t kind, const gq_tuning *t) {
     if (!s || !t) return fail(GQ_ERR_INVALID, "null argument");
     if (kind < 0 || kind > 2) return fail(GQ_ERR_INVALID, "unknown query kind");
-    if (t->variant < 0 || t->variant > 3 || t->variant == GQ_VARIANT_AUTO)
-        return fail(GQ_ERR_INVALID, "tuning variant must be EXACT, WIDE8 or COHERENT");
+    if (t->variant < 0 || t->variant > 4 || t->variant == GQ_VARIANT_AUTO)
+        return fail(GQ_ERR_INVALID, "tuning variant must be EXACT, WIDE8, COHERENT or WARP");
+    if (t->variant == GQ_VARIANT_WARP && kind != GQ_KIND_SILHOUETTE)
+        return fail(GQ_ERR_INVALID, "the WARP variant answers silhouette queries only");
     if (t->variant == GQ_VARIANT_WIDE8 && !s->has_wide) return fail(GQ_ERR_UNSUPPORTED, "scene has no wide BVH");
     if (t->block != 0 && t->block != 64 && t->block != 128 && t->block != 256)
         return fail(GQ_ERR_INVALID, "block must be 0 (default), 64, 128 or 256");
@@ -504,8 +506,8 @@ gq_status gq_closest_silhouette(const gq_scene *s, gq_vecs x, const float *r_max
     if (s->exact_stack > GQ_STACK_EXACT) return fail(GQ_ERR_DEPTH, "tree deeper than gQuery's 64-entry stack");
     if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "scene was built without a device copy");
     const int v = resolve_variant(s, opts, GQ_KIND_SILHOUETTE);
-    if (v != GQ_VARIANT_EXACT && v != GQ_VARIANT_COHERENT)
-        return fail(GQ_ERR_UNSUPPORTED, "silhouette queries run the exact or the coherent variant");
+    if (v != GQ_VARIANT_EXACT && v != GQ_VARIANT_COHERENT && v != GQ_VARIANT_WARP)
+        return fail(GQ_ERR_UNSUPPORTED, "silhouette queries run the exact, coherent or warp variant");
     DeviceGuard g(s->device);
     cudaStream_t cs = (cudaStream_t)stream;
     Scratch scr;
@@ -657,7 +659,7 @@ gq_status gq_batch_run(gq_batch *b, const gq_batch_queries *cp, const gq_cp_out 
     for (const gq_scene *s : b->scenes) all_wide &= s->has_wide;
     cudaError_t e = gqd::batch_run(b->dev_scenes, (int)b->scenes.size(), b->dim, kinds, co, ro, so,
                                    (b->flags & GQ_BATCH_RAY_EXACT) || !all_wide ? 0 : 1,
-                                   (b->flags & GQ_BATCH_CP_EXACT) ? 0 : 1, (b->flags & GQ_BATCH_SIL_EXACT) ? 0 : 1,
+                                   (b->flags & GQ_BATCH_CP_EXACT) ? 0 : 1, gqd::sil_mode_of(b->flags),
                                    1.f,
                                    b->scratch, b->max_queries, b->err, (cudaStream_t)stream);
     if (e != cudaSuccess) return fail_cuda(e, "batch launch");

@@ -14,6 +14,7 @@
 #include "packet.cuh"
 #include "records.cuh"
 #include "sil_packet.cuh"
+#include "sil_warp.cuh"
 #include "snch.cuh"
 #include "traverse.cuh"
 
@@ -138,13 +139,13 @@ __device__ __forceinline__ void refill(int64_t n, unsigned long long *counter, i
 // One persistent launch per step.  Phase 1: closest points, as warp tiles of 32
 // sorted queries (warp-coherent traversal once per distinct scene in the tile) or,
 // in exact mode, one lane per query.  Phase 2: rays, one lane per query.  Phase 3:
-// silhouettes, as warp-coherent tiles like the closest points or, in exact mode, one
-// lane per query.  Every warp moves to the next phase when the current one has no
+// silhouettes (sil_mode): 1 warp-coherent tiles like the closest points, 2 one query
+// per warp (sil_warp.cuh), 0 one lane per query in the reference order.  Every warp moves to the next phase when the current one has no
 // unclaimed work, so the phases' tails overlap.  counter[0..2]: claims per phase.
 template <int D, bool RAYW>
 __global__ void __launch_bounds__(kBlock) k_batch(const DevScene *scenes, int n_scenes, BatchKind cp, gq_cp_out cp_out,
                                                   BatchKind ray, gq_ray_out ray_out, BatchKind sil,
-                                                  gq_sil_out sil_out, int cp_coherent, int sil_coherent,
+                                                  gq_sil_out sil_out, int cp_coherent, int sil_mode,
                                                   int budget, unsigned long long *counter, int32_t *err) {
     const unsigned lane = threadIdx.x & 31u;
     // ---------------- phase 1: closest points ----------------
@@ -247,7 +248,37 @@ __global__ void __launch_bounds__(kBlock) k_batch(const DevScene *scenes, int n_
             [&]() { trav::lane_write(*sc, L, qi, ray.n, gq_cp_out{}, ray_out); });
     }
     // ---------------- phase 3: silhouettes ----------------
-    if (sil.n > 0 && sil_coherent) {
+    if (sil.n > 0 && sil_mode == 2) {
+        // one query per warp; this warp's stack in dynamic shared memory
+        extern __shared__ int2 wstk[];
+        int2 *wst = wstk + (threadIdx.x >> 5) * wsil::kWarpStack;
+        for (;;) {
+            unsigned long long t = 0;
+            if (lane == 0) t = atomicAdd(&counter[2], 1ull);
+            t = __shfl_sync(0xffffffffu, t, 0);
+            if (t >= (unsigned long long)sil.n) break;
+            const int64_t qi = (int64_t)__ldg(sil.perm + (int64_t)t);
+            const int sid = __ldg(sil.scene + qi);
+            if (sid == GQ_BATCH_SKIP) continue;
+            float x[D];
+#pragma unroll
+            for (int k = 0; k < D; ++k) x[k] = qget(sil.a, qi, k);
+            const bool known = (unsigned)sid < (unsigned)n_scenes;
+            if (!known || !scenes[sid].spairs) {
+                if (lane == 0) {
+                    atomicOr(err, known ? GQ_BATCH_ERR_NO_SNCH : GQ_BATCH_ERR_SCENE);
+                    put_sil<D>(sil_out, sil.n, qi, false, x, 0.f, 0);
+                }
+                continue;
+            }
+            snch::Lane<D> L;
+            wsil::closest_silhouette<D>(scenes[sid], x, sil.r_max ? sil.r_max[qi] : kInf, L, wst);
+            if (lane == 0) {
+                if (L.ovf && scenes[sid].err) atomicOr(scenes[sid].err, GQ_DEVERR_STACK);
+                put_sil<D>(sil_out, sil.n, qi, L.found && !L.ovf, L.bp, L.bd, L.bid);
+            }
+        }
+    } else if (sil.n > 0 && sil_mode == 1) {
         const int64_t t_sil = (sil.n + 31) / 32;
         snch::Stack stk;
         for (;;) {
@@ -317,24 +348,29 @@ __global__ void __launch_bounds__(kBlock) k_batch(const DevScene *scenes, int n_
 
 template <int D, bool RAYW>
 cudaError_t launch_batch(const DevScene *scenes_dev, int n_scenes, BatchKind kinds[3], const gq_cp_out &cp_out,
-                         const gq_ray_out &ray_out, const gq_sil_out &sil_out, int cp_coherent, int sil_coherent,
+                         const gq_ray_out &ray_out, const gq_sil_out &sil_out, int cp_coherent, int sil_mode,
                          float grid_share, unsigned long long *counter, int32_t *err, cudaStream_t st) {
-    static int bps = 0, n_sm = 0;
-    if (!bps) {
-        int dev = 0;
+    // the one-query-per-warp silhouette phase keeps its stacks in dynamic shared memory
+    const size_t smem = (sil_mode == 2 && kinds[2].n > 0) ? (size_t)(kBlock / 32) * wsil::kWarpStack * sizeof(int2) : 0;
+    const int mi = smem ? 1 : 0;
+    static int bps_m[2] = {0, 0}, n_sm = 0;
+    if (!bps_m[mi]) {
+        int dev = 0, b = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_batch<D, RAYW>, kBlock, 0);
-        if (bps < 1) bps = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch<D, RAYW>, kBlock, smem);
+        bps_m[mi] = b < 1 ? 1 : b;
     }
+    const int bps = bps_m[mi];
     const int64_t most = std::max(kinds[0].n, std::max(kinds[1].n, kinds[2].n));
     if (most <= 0) return cudaSuccess;
-    int64_t want = std::min<int64_t>((int64_t)bps * n_sm, (most + kBlock - 1) / kBlock);
+    int64_t want = std::min<int64_t>((int64_t)bps * n_sm,
+                                     std::max<int64_t>((most + kBlock - 1) / kBlock, smem ? (kinds[2].n * 32 + kBlock - 1) / kBlock : 0));
     if (grid_share > 0.f && grid_share < 1.f)
         want = std::min<int64_t>(want, std::max<int64_t>(1, (int64_t)(grid_share * (float)(bps * n_sm))));
-    k_batch<D, RAYW><<<dim3((unsigned)want), kBlock, 0, st>>>(scenes_dev, n_scenes, kinds[0], cp_out, kinds[1], ray_out,
-                                                              kinds[2], sil_out, cp_coherent, sil_coherent, 32, counter,
-                                                              err);
+    k_batch<D, RAYW><<<dim3((unsigned)want), kBlock, smem, st>>>(scenes_dev, n_scenes, kinds[0], cp_out, kinds[1],
+                                                                 ray_out, kinds[2], sil_out, cp_coherent, sil_mode, 32,
+                                                                 counter, err);
     return cudaGetLastError();
 }
 
@@ -358,7 +394,7 @@ size_t batch_scratch_bytes(int64_t max_n) {
 
 cudaError_t batch_run(const DevScene *scenes_dev, int n_scenes, int dim, BatchKind kinds[3], const gq_cp_out &cp_out,
                       const gq_ray_out &ray_out, const gq_sil_out &sil_out, int ray_wide, int cp_coherent,
-                      int sil_coherent, float grid_share, void *scratch, int64_t max_n, int32_t *err,
+                      int sil_mode, float grid_share, void *scratch, int64_t max_n, int32_t *err,
                       cudaStream_t st) {
     char *p = static_cast<char *>(scratch);
     unsigned long long *counter = reinterpret_cast<unsigned long long *>(p);
@@ -392,13 +428,13 @@ cudaError_t batch_run(const DevScene *scenes_dev, int n_scenes, int dim, BatchKi
     if (e != cudaSuccess) return e;
     if (dim == 3)
         return ray_wide ? launch_batch<3, true>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_coherent,
-                                                sil_coherent, grid_share, counter, err, st)
+                                                sil_mode, grid_share, counter, err, st)
                         : launch_batch<3, false>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_coherent,
-                                                 sil_coherent, grid_share, counter, err, st);
+                                                 sil_mode, grid_share, counter, err, st);
     return ray_wide ? launch_batch<2, true>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_coherent,
-                                            sil_coherent, grid_share, counter, err, st)
+                                            sil_mode, grid_share, counter, err, st)
                     : launch_batch<2, false>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_coherent,
-                                             sil_coherent, grid_share, counter, err, st);
+                                             sil_mode, grid_share, counter, err, st);
 }
 
 }  // namespace gqd

@@ -9,6 +9,7 @@
 #include "queries.cuh"
 #include "records.cuh"
 #include "sil_packet.cuh"
+#include "sil_warp.cuh"
 #include "snch.cuh"
 
 namespace gqd {
@@ -69,6 +70,29 @@ __global__ void __launch_bounds__(kMaxBlock) k_sil_packet(DevScene s, gq_vecs xq
         L.r = alive ? (rmax_in ? rmax_in[qi] : kInf) : -1.f;
         pkt::closest_silhouette<D>(s, __ballot_sync(0xffffffffu, alive), L, stk);
         if (alive) sil_write<D>(s, L, qi, n, o);
+    }
+}
+
+// One query per warp (sil_warp.cuh): persistent warps take the next query of the
+// sorted order; the stack lives in dynamic shared memory (kWarpStack entries per warp).
+template <int D>
+__global__ void __launch_bounds__(kMaxBlock) k_sil_warp(DevScene s, gq_vecs xq, const float *rmax_in, int64_t n,
+                                                     const int32_t *perm, gq_sil_out o, unsigned long long *counter) {
+    extern __shared__ int2 wstk[];
+    const unsigned lane = threadIdx.x & 31u;
+    int2 *stk = wstk + (threadIdx.x >> 5) * wsil::kWarpStack;
+    for (;;) {
+        unsigned long long i = 0;
+        if (lane == 0) i = atomicAdd(counter, 1ull);
+        i = __shfl_sync(0xffffffffu, i, 0);
+        if (i >= (unsigned long long)n) break;
+        const int64_t qi = query_index(perm, (int64_t)i);
+        float x[D];
+#pragma unroll
+        for (int k = 0; k < D; ++k) x[k] = qget(xq, qi, k);
+        snch::Lane<D> L;
+        wsil::closest_silhouette<D>(s, x, rmax_in ? rmax_in[qi] : kInf, L, stk);
+        if (lane == 0) sil_write<D>(s, L, qi, n, o);
     }
 }
 
@@ -538,6 +562,30 @@ cudaError_t launch_sil(const DevScene &s, int variant, const Tune &t, gq_vecs x,
     const int di = s.dim == 3 ? 1 : 0;
     int slot = block_slot(t.block), block = t.block;
     if (slot < 0) slot = 1, block = 128;
+    if (variant == GQ_VARIANT_WARP && counter) {
+        const size_t smem = (size_t)(block / 32) * wsil::kWarpStack * sizeof(int2);
+        static int wb[2][3] = {}, w_sm = 0;
+        if (!wb[di][slot]) {
+            int dev = 0, b = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&w_sm, cudaDevAttrMultiProcessorCount, dev);
+            // up to 8 warps x 8 KB of stacks: above the 48 KB a launch may take without opting in
+            const int most = (kMaxBlock / 32) * wsil::kWarpStack * (int)sizeof(int2);
+            cudaFuncSetAttribute(s.dim == 3 ? (const void *)k_sil_warp<3> : (const void *)k_sil_warp<2>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &b, s.dim == 3 ? (const void *)k_sil_warp<3> : (const void *)k_sil_warp<2>, block, smem);
+            wb[di][slot] = b < 1 ? 1 : b;
+        }
+        const int64_t want = std::min<int64_t>((int64_t)wb[di][slot] * w_sm, (n * 32 + block - 1) / block);
+        cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
+        if (e != cudaSuccess) return e;
+        if (s.dim == 3)
+            k_sil_warp<3><<<dim3((unsigned)want), block, smem, st>>>(s, x, r_max, n, perm, o, counter);
+        else
+            k_sil_warp<2><<<dim3((unsigned)want), block, smem, st>>>(s, x, r_max, n, perm, o, counter);
+        return cudaGetLastError();
+    }
     const bool packet = variant == GQ_VARIANT_COHERENT && counter && n >= 32;
     const bool refill = !packet && t.persist && counter && n > 4096;
     if (packet || refill) {

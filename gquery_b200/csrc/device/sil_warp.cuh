@@ -1,0 +1,171 @@
+// One closest-silhouette query per warp ("wide frontier"), for sparse query sets whose
+// per-query work is large and uneven: the 32 lanes expand up to 32 stack entries of
+// the same query per step, so a query that visits 10^5 nodes takes about 10^5 / 32
+// steps instead of 10^5.  Used by the single-scene kernel (queries.cu) and the server's
+// silhouette steps (batch.cu).
+//
+// Per step: the warp takes the top `take` entries of a shared-memory stack (lane l
+// gets the l-th from the top), every lane applies the reference's pop-time test
+// (snch.py:118) against the warp's current r_max, then either scans its leaf's
+// silhouettes with the reference's per-silhouette test and acceptance rule
+// (snch.py:131-134), shrinking its own copy of r_max as it goes, or tests both
+// children of its interior node with the reference's box and normal-cone tests
+// (snch3d.py:55-95, snch.py:60-97).  The warp then takes the minimum r_max over its
+// lanes and pushes the admitted children (lane 0's on top, the nearer child above the
+// farther).  Answers equal the reference's except at FP32 distance ties, for the
+// reasons given in sil_packet.cuh (the cone test does not depend on r_max).
+//
+// Stack bound: a step that takes `take` entries pushes at most 2*take, so the warp
+// takes 32 entries only while that leaves room for a depth-first descent, and one
+// entry otherwise; a depth-first descent adds at most the tree depth (<= 64, checked
+// on the host), so a stack of kWarpStack entries never overflows.  An overflow is
+// still detected and reported instead of written.
+#pragma once
+
+#include "packet.cuh"
+#include "prim.cuh"
+#include "queries.cuh"
+#include "snch.cuh"
+
+namespace gqd {
+namespace wsil {
+
+constexpr int kWarpStack = 1024;  // entries per warp (8 KB of shared memory)
+constexpr int kReserve = 2 * GQ_STACK_EXACT + 2;
+
+// min over the warp of a non-negative float (or +inf) and the lowest lane holding it
+__device__ __forceinline__ void warp_argmin(float v, float &m, int &who) {
+    m = pkt::warp_min(v);
+    const unsigned hit = __ballot_sync(0xffffffffu, v == m);
+    who = __ffs(hit) - 1;
+}
+
+// All 32 lanes call with the same query (x, r_max); stk: this warp's kWarpStack entries
+// of shared memory.  On return every lane holds the answer in L (found, bp, bd, bid, ovf).
+template <int D>
+__device__ __forceinline__ void closest_silhouette(const DevScene &s, const float *x, float r_max, snch::Lane<D> &L,
+                                                   int2 *stk) {
+    const unsigned lane = threadIdx.x & 31u;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        L.x[k] = x[k];
+        L.bp[k] = 0.f;
+    }
+    L.r = r_max;
+    L.found = false;
+    L.ovf = false;
+    L.bd = 0.f;
+    L.bid = 0;
+    float dmin_root, dmax_root;
+    if (D == 2)
+        box_dist2(s.root_lo[0], s.root_lo[1], s.root_hi[0], s.root_hi[1], x[0], x[1], dmin_root, dmax_root);
+    else
+        box_dist3(s.root_lo[0], s.root_lo[1], s.root_lo[2], s.root_hi[0], s.root_hi[1], s.root_hi[2], x[0], x[1],
+                  x[D - 1], dmin_root, dmax_root);
+    int sp = 0;  // entries on the stack (warp-uniform)
+    if (dmin_root <= r_max) {
+        if (lane == 0) stk[0] = make_int2(s.sroot_ref, fbits(dmin_root));
+        sp = 1;
+    }
+    __syncwarp();
+    float R = r_max;  // warp's r_max
+    bool ovf = false;
+    while (sp > 0) {
+        const int take = (sp + 32 <= kWarpStack - kReserve) ? min(sp, 32) : 1;
+        const bool mine = (int)lane < take;
+        int2 e = make_int2(0, 0);
+        if (mine) e = stk[sp - 1 - (int)lane];
+        __syncwarp();
+        sp -= take;
+        L.r = R;
+        int2 push[2];
+        int np = 0;
+        if (mine && __int_as_float(e.y) <= R) {
+            if (e.x < 0) {
+                if (e.x != INT32_MIN)
+                    for (int j = ~e.x;; ++j)
+                        if (snch::test_silhouette<D>(s, L, j)) break;
+            } else {
+                // interior node: both children against this lane's r_max, nearer pushed last
+                float lo[2][D], hi[2][D], ax[2][D], half[2], rad[2];
+                int refs[2];
+                if (D == 2) {
+                    const float4 a0 = ldg4(s.spairs, 5 * (int64_t)e.x), a1 = ldg4(s.spairs, 5 * (int64_t)e.x + 1),
+                                 a2 = ldg4(s.spairs, 5 * (int64_t)e.x + 2), a3 = ldg4(s.spairs, 5 * (int64_t)e.x + 3);
+                    const int4 rr = __ldg(reinterpret_cast<const int4 *>(s.spairs) + 5 * (int64_t)e.x + 4);
+                    lo[0][0] = a0.x; lo[0][D - 1] = a0.y; hi[0][0] = a0.z; hi[0][D - 1] = a0.w;
+                    ax[0][0] = a1.x; ax[0][D - 1] = a1.y; half[0] = a1.z; rad[0] = a1.w;
+                    lo[1][0] = a2.x; lo[1][D - 1] = a2.y; hi[1][0] = a2.z; hi[1][D - 1] = a2.w;
+                    ax[1][0] = a3.x; ax[1][D - 1] = a3.y; half[1] = a3.z; rad[1] = a3.w;
+                    refs[0] = rr.x;
+                    refs[1] = rr.y;
+                } else {
+                    const int64_t b = 6 * (int64_t)e.x;
+                    const float4 f0 = ldg4(s.spairs, b), f1 = ldg4(s.spairs, b + 1), f2 = ldg4(s.spairs, b + 2),
+                                 f3 = ldg4(s.spairs, b + 3), f4 = ldg4(s.spairs, b + 4), f5 = ldg4(s.spairs, b + 5);
+                    lo[0][0] = f0.x; lo[0][1] = f0.y; lo[0][D - 1] = f0.z;
+                    hi[0][0] = f0.w; hi[0][1] = f1.x; hi[0][D - 1] = f1.y;
+                    ax[0][0] = f1.z; ax[0][1] = f1.w; ax[0][D - 1] = f2.x;
+                    half[0] = f2.y; rad[0] = f2.z;
+                    lo[1][0] = f2.w; lo[1][1] = f3.x; lo[1][D - 1] = f3.y;
+                    hi[1][0] = f3.z; hi[1][1] = f3.w; hi[1][D - 1] = f4.x;
+                    ax[1][0] = f4.y; ax[1][1] = f4.z; ax[1][D - 1] = f4.w;
+                    half[1] = f5.x; rad[1] = f5.y;
+                    refs[0] = fbits(f5.z);
+                    refs[1] = fbits(f5.w);
+                }
+                bool hit[2];
+                float dm[2];
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    float dmax;
+                    if (D == 2)
+                        box_dist2(lo[c][0], lo[c][D - 1], hi[c][0], hi[c][D - 1], x[0], x[D - 1], dm[c], dmax);
+                    else
+                        box_dist3(lo[c][0], lo[c][1], lo[c][D - 1], hi[c][0], hi[c][1], hi[c][D - 1], x[0], x[1],
+                                  x[D - 1], dm[c], dmax);
+                    hit[c] = dm[c] <= L.r;
+                    if ((half[c] >= 0.f) & hit[c])
+                        hit[c] = cone_overlaps<D>(lo[c], hi[c], ax[c], half[c], rad[c], x, dm[c]);
+                }
+                const bool sw = dm[1] < dm[0];  // push the farther first so the nearer is popped first
+                const int first = sw ? 0 : 1, second = sw ? 1 : 0;
+                if (hit[first]) push[np++] = make_int2(refs[first], fbits(dm[first]));
+                if (hit[second]) push[np++] = make_int2(refs[second], fbits(dm[second]));
+            }
+        }
+        // new r_max of the warp
+        float m;
+        int who;
+        warp_argmin(L.r, m, who);
+        R = m;
+        // push: lane 31's entries at the bottom, lane 0's on top
+        const unsigned has1 = __ballot_sync(0xffffffffu, np >= 1), has2 = __ballot_sync(0xffffffffu, np >= 2);
+        const unsigned above = ~((2u << lane) - 1u);  // lanes with a higher index
+        const int before = __popc(has1 & above) + __popc(has2 & above);
+        const int total = __popc(has1) + __popc(has2);
+        if (sp + total > kWarpStack) {
+            ovf = true;
+            break;
+        }
+        if (np >= 1) stk[sp + before] = push[0];
+        if (np >= 2) stk[sp + before + 1] = push[1];
+        __syncwarp();
+        sp += total;
+    }
+    // answer: the lane with the smallest accepted distance (lowest lane on a tie)
+    const float mine_d = L.found ? L.bd : kInf;
+    float m;
+    int who;
+    warp_argmin(mine_d, m, who);
+    const bool any = m < kInf;
+    L.found = any && !ovf;
+    L.ovf = ovf;
+#pragma unroll
+    for (int k = 0; k < D; ++k) L.bp[k] = __shfl_sync(0xffffffffu, L.bp[k], who);
+    L.bd = __shfl_sync(0xffffffffu, L.bd, who);
+    L.bid = __shfl_sync(0xffffffffu, L.bid, who);
+}
+
+}  // namespace wsil
+}  // namespace gqd

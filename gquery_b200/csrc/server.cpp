@@ -12,7 +12,7 @@
 // Step.  A step takes, for each kind it serves, the run of admitted requests that are
 // contiguous in the ring (at most step_queries queries) and answers them with one
 // batch launch; closest-point and ray requests go to the general slots, silhouette
-// requests to a slot of their own whose launches hold part of the GPU only;
+// requests to slots of their own whose launches hold part of the GPU only;
 // inside the step a field with C components is stored component-major with stride m
 // (the step's query count) from ring offset off * C, which is where the kernel writes
 // it and what one device-to-host copy per field brings back.
@@ -135,8 +135,8 @@ struct Slot {
 
 struct gq_server {
     int dim = 0, device = 0, flags = 0;
-    int64_t step_queries = 0, ring_bytes = 0;
-    float sil_share = 0.5f;
+    int64_t step_queries = 0, ring_bytes = 0, sil_step_queries = 0;
+    float sil_share = 0.5f;  // per silhouette slot
     std::vector<gq_scene *> scenes;
     gqd::DevScene *dev_scenes = nullptr;
     Ring ring[3];
@@ -357,11 +357,12 @@ struct gq_server {
             } else {
                 for (int k = 0; k < 3; ++k) {
                     if ((k == GQ_KIND_SILHOUETTE) != S.sil_only) continue;
+                    const int64_t cap = S.sil_only ? sil_step_queries : step_queries;
                     while (!admitted[k].empty()) {
                         Req *r = admitted[k].front();
                         if (S.m[k] == 0)
                             S.off[k] = r->phys;
-                        else if (r->phys != S.off[k] + S.m[k] || S.m[k] + r->q.n > step_queries)
+                        else if (r->phys != S.off[k] + S.m[k] || S.m[k] + r->q.n > cap)
                             break;
                         S.m[k] += r->q.n;
                         S.reqs.push_back(r);
@@ -429,7 +430,7 @@ struct gq_server {
         for (const gq_scene *sc : scenes) all_wide &= sc->has_wide;
         cudaError_t e = gqd::batch_run(dev_scenes, (int)scenes.size(), D, kinds, co, ro, so,
                                        (flags & GQ_BATCH_RAY_EXACT) || !all_wide ? 0 : 1,
-                                       (flags & GQ_BATCH_CP_EXACT) ? 0 : 1, (flags & GQ_BATCH_SIL_EXACT) ? 0 : 1,
+                                       (flags & GQ_BATCH_CP_EXACT) ? 0 : 1, gqd::sil_mode_of(flags),
                                        S.sil_only ? sil_share : 1.f, S.scratch, step_queries, S.err, S.st);
         return e == cudaSuccess ? GQ_OK : fail_cuda(e, "server step");
     }
@@ -558,7 +559,7 @@ gq_status gq_server_create(gq_scene *const *scenes, int32_t n_scenes, const gq_s
     s->flags = o.flags;
     s->step_queries = o.step_queries > 0 ? o.step_queries : (1 << 19);
     const int inflight = o.max_inflight > 0 ? o.max_inflight : 2;
-    s->sil_share = o.sil_share > 0.f && o.sil_share <= 1.f ? o.sil_share : 0.5f;
+    s->sil_share = o.sil_share > 0.f && o.sil_share <= 1.f ? o.sil_share : 0.8f;
     std::vector<gqd::DevScene> views((size_t)n_scenes);
     for (int32_t i = 0; i < n_scenes; ++i) {
         gq_scene *sc = scenes[i];
@@ -592,8 +593,11 @@ gq_status gq_server_create(gq_scene *const *scenes, int32_t n_scenes, const gq_s
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->copy_st, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->copy_evt, cudaEventDisableTiming);
     const bool per_request = (s->flags & GQ_SERVER_PER_REQUEST) != 0;
-    s->slots.resize((size_t)inflight + (per_request ? 0 : 1));
-    if (!per_request) s->slots.back().sil_only = true;
+    const int sil_slots = per_request ? 0 : (o.sil_slots > 0 ? o.sil_slots : 2);
+    s->sil_share /= (float)std::max(sil_slots, 1);
+    s->sil_step_queries = std::min<int64_t>(s->step_queries, o.sil_step_queries > 0 ? o.sil_step_queries : (1 << 15));
+    s->slots.resize((size_t)(inflight + sil_slots));
+    for (int i = 0; i < sil_slots; ++i) s->slots[(size_t)(inflight + i)].sil_only = true;
     for (Slot &S : s->slots) {
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S.st, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S.done, cudaEventDisableTiming);

@@ -16,7 +16,7 @@ from . import records as R
 ArrayLike = Union[torch.Tensor, np.ndarray, Sequence]
 
 VARIANTS = {"exact": L.VARIANT_EXACT, "wide8": L.VARIANT_WIDE8, "auto": L.VARIANT_AUTO,
-            "coherent": L.VARIANT_COHERENT}
+            "coherent": L.VARIANT_COHERENT, "warp": L.VARIANT_WARP}
 KINDS = {"cp": L.KIND_CLOSEST_POINT, "ray": L.KIND_INTERSECT, "sil": L.KIND_SILHOUETTE}
 VARIANT_NAMES = {v: k for k, v in VARIANTS.items()}
 
@@ -236,7 +236,9 @@ class Scene:
     def closest_silhouette(self, x, r_max=math.inf, *, variant="auto", sort=True, stream=None, scratch=None,
                            out=None, order=None):
         """closest_silhouette_snch (snch.py:106-164 / snch3d.py:143-203); variant "exact"
-        (reference visit order) or "coherent" (warp-coherent, same answers except at ties)."""
+        (reference visit order), "coherent" (one traversal per warp of neighbouring
+        queries) or "warp" (one query per warp); the last two give the same answers
+        except at FP32 distance ties."""
         tx, n, vx = self._points(x)
         rm = self._rmax(r_max, n)
         rec = out or self.alloc_sil(n)

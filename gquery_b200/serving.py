@@ -99,21 +99,22 @@ class Server:
     budget_bytes: device bytes the request rings may hold (the admission budget);
     ring_queries: ring capacity per kind (cp, ray, sil); step_queries: most queries of
     one kind per step and the largest request; max_inflight: closest-point / ray step
-    slots (streams); silhouette steps have a slot of their own holding at most
-    sil_share of the GPU."""
+    slots (streams); silhouette steps have sil_slots slots of their own holding at most
+    sil_share of the GPU together, sil_step_queries queries per step.  Silhouettes default to one query per warp ("warp"): served
+    requests are sparse, and a warp per query bounds the latency of far-reaching ones."""
 
     def __init__(self, scenes: Sequence[Scene], *, budget_bytes: int = 0, ring_queries=(1 << 22,) * 3,
                  step_queries: int = 1 << 19, max_inflight: int = 2, per_request: bool = False,
-                 cp_variant: str = "coherent", ray_variant: str = "wide8", sil_variant: str = "coherent",
-                 sil_share: float = 0.5):
+                 cp_variant: str = "coherent", ray_variant: str = "wide8", sil_variant: str = "warp",
+                 sil_share: float = 0.8, sil_slots: int = 2, sil_step_queries: int = 1 << 15):
         self.scenes = list(scenes)
         self.dim = self.scenes[0].dim
         flags = (L.SERVER_PER_REQUEST if per_request else 0) | \
             (L.BATCH_CP_EXACT if cp_variant == "exact" else 0) | (L.BATCH_RAY_EXACT if ray_variant == "exact" else 0) | \
-            (L.BATCH_SIL_EXACT if sil_variant == "exact" else 0)
+            (L.BATCH_SIL_EXACT if sil_variant == "exact" else L.BATCH_SIL_WARP if sil_variant == "warp" else 0)
         rq = [int(ring_queries)] * 3 if isinstance(ring_queries, int) else [int(x) for x in ring_queries]
         opts = L.ServerOpts(int(budget_bytes), (C.c_int64 * 3)(*rq), int(step_queries), int(max_inflight), flags,
-                            float(sil_share))
+                            float(sil_share), int(sil_slots), int(sil_step_queries))
         arr = (C.c_void_p * len(self.scenes))(*[s.handle.value for s in self.scenes])
         h = C.c_void_p()
         L.check(L.lib().gq_server_create(arr, len(self.scenes), C.byref(opts), C.byref(h)))

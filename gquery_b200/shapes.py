@@ -39,7 +39,7 @@ class _Shape:
         return self.scene.intersect(p, v, r_max, variant=self.variant, sort=self.sort_queries)
 
     def closest_silhouette_snch(self, x, r_max=math.inf):
-        variant = self.variant if self.variant in ("exact", "coherent") else "auto"  # no wide silhouette traversal
+        variant = self.variant if self.variant in ("exact", "coherent", "warp") else "auto"  # no wide silhouettes
         return self.scene.closest_silhouette(x, r_max, variant=variant, sort=self.sort_queries)
 
     # ---- brute-force scans (the reference's *_baseline methods) ----

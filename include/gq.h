@@ -48,6 +48,8 @@ typedef int32_t gq_status;
 #define GQ_VARIANT_AUTO 2     /* the scene's tuned choice for the query kind (gq_scene_set_tuning) */
 #define GQ_VARIANT_COHERENT 3 /* binary tree walked once per warp of Morton-adjacent queries (closest
                                  point, closest silhouette); rays run as EXACT */
+#define GQ_VARIANT_WARP 4     /* closest silhouette only: one query per warp, its 32 lanes expanding up to
+                                 32 tree nodes per step (for few, far-reaching queries) */
 /* All variants other than EXACT give the same answers as EXACT except at FP32 distance
  * ties (distances within 2e-6 relative). */
 
@@ -227,13 +229,15 @@ gq_status gq_scene_device_error(const gq_scene *scene, void *stream, int32_t *fl
  * allocates nothing and never synchronises: a step can be recorded in a CUDA graph.
  * Each query carries the index of its scene in the batch.  Results are those of the
  * single-scene calls: closest points and silhouettes follow GQ_VARIANT_COHERENT (or
- * GQ_VARIANT_EXACT with GQ_BATCH_CP_EXACT / GQ_BATCH_SIL_EXACT), rays GQ_VARIANT_WIDE8
- * when every scene has wide nodes (or GQ_VARIANT_EXACT with GQ_BATCH_RAY_EXACT). */
+ * GQ_VARIANT_EXACT with GQ_BATCH_CP_EXACT / GQ_BATCH_SIL_EXACT, GQ_VARIANT_WARP with
+ * GQ_BATCH_SIL_WARP), rays GQ_VARIANT_WIDE8 when every scene has wide nodes (or
+ * GQ_VARIANT_EXACT with GQ_BATCH_RAY_EXACT). */
 typedef struct gq_batch gq_batch;
 
 #define GQ_BATCH_CP_EXACT 1  /* closest point: one exact traversal per lane, reference visit order */
 #define GQ_BATCH_RAY_EXACT 2 /* rays: binary BVH, reference visit order */
 #define GQ_BATCH_SIL_EXACT 8 /* silhouettes: one exact traversal per lane, reference visit order */
+#define GQ_BATCH_SIL_WARP 16 /* silhouettes: one query per warp (GQ_VARIANT_WARP), for sparse queries */
 
 typedef struct {
     int64_t n;             /* query count (0: none of this kind) */
@@ -270,8 +274,10 @@ gq_status gq_batch_device_error(gq_batch *batch, void *stream, int32_t *flags);
  * a step slot is free: one gq_batch launch for all scenes (or, with
  * GQ_SERVER_PER_REQUEST, one single-scene call per request, the scene's tuned
  * variant).  Closest-point and ray requests share max_inflight slots; silhouette
- * requests, whose traversals are far longer, have a slot of their own whose launches
- * hold at most sil_share of the GPU, so the other kinds never queue behind them.
+ * requests, whose traversals are far longer, have sil_slots slots of their own whose
+ * launches together hold at most sil_share of the GPU and take at most
+ * sil_step_queries queries each, so the other kinds never queue behind them and a
+ * small silhouette request does not wait for a large one.
  * Each slot has its own stream, so the results of one step go back to the host while
  * the next computes.  Results are those of gq_batch_run. */
 typedef struct gq_server gq_server;
@@ -284,7 +290,9 @@ typedef struct {
     int64_t step_queries;     /* most queries of one kind in one step, and the largest request (0: 1<<19) */
     int32_t max_inflight;     /* step slots for closest-point and ray steps (0: 2) */
     int32_t flags;            /* GQ_BATCH_*_EXACT | GQ_SERVER_PER_REQUEST */
-    float sil_share;          /* share of the GPU's resident blocks a silhouette step may hold (0: 0.5) */
+    float sil_share;          /* share of the GPU's resident blocks all silhouette steps together may hold (0: 0.8) */
+    int32_t sil_slots;        /* silhouette step slots (0: 2) */
+    int64_t sil_step_queries; /* most silhouette queries in one step, unless one request is larger (0: 1<<15) */
 } gq_server_opts;
 
 typedef struct {

@@ -19,7 +19,7 @@ def test_candidates_cover_width_stack_and_block():
     assert not any(x["stack"] == 32 for x in candidates("cp", 3, True, 40, 60))
     assert all(x["variant"] != "wide8" for x in candidates("cp", 3, False, 24, 0))
     assert candidates("sil", 3, True, 24, 40, has_snch=False) == []
-    assert {x["variant"] for x in candidates("sil", 2, True, 20, 20)} == {"coherent", "exact"}
+    assert {x["variant"] for x in candidates("sil", 2, True, 20, 20)} == {"coherent", "exact", "warp"}
 
 
 class FakeScene:
@@ -85,4 +85,4 @@ def test_tune_batch_picks_fastest_choice():
     t = {("coherent", "wide8", "coherent"): 1.0}
     res = tune_batch(make, lambda b: None, timer=lambda fn: t.get(tuple(made[-1].values()), 2.0))
     assert res["best"] == dict(cp_variant="coherent", ray_variant="wide8", sil_variant="coherent")
-    assert len(res["table"]) == 8
+    assert len(res["table"]) == 12

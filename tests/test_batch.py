@@ -232,3 +232,24 @@ def test_batch_single_kind_and_tiny(three_d):
         alone = _alone(scenes, ids, lambda s, sel: s.intersect(_dev(pts[sel]), _dev(dirs[sel]), variant="wide8"))
         assert_bitwise(to_np(res.ray), alone, RAY3, f"n={n} ")
     assert b.run().cp is None
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_batch_silhouettes_one_query_per_warp(dim, two_d, three_d):
+    scenes, _ = two_d if dim == 2 else three_d
+    n = 6000
+    ids, pts, _ = _mixed_queries(n, dim, len(scenes), seed=50 + dim)
+    ids[::11] = SKIP
+    b = SceneBatch(scenes, n, sil_variant="warp")
+    out = b.alloc(0, 0, n)
+    out.sil.prim_id.fill_(-7)
+    res = b.run(sil=(_dev(pts), _dev(ids), 0.9), out=out)
+    torch.cuda.synchronize()
+    assert b.device_error() == 0
+    got = to_np(res.sil)
+    live = ids != SKIP
+    assert np.all(got["prim_id"][~live] == -7)
+    ref = _alone(scenes, np.where(live, ids, -1),
+                 lambda s, sel: s.closest_silhouette(_dev(pts[sel]), 0.9, variant="exact"))
+    rep = tie_report({k: v[..., live] for k, v in got.items()}, {k: v[..., live] for k, v in ref.items()})
+    assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0 and rep["max_rel_d"] <= REL_TOL, rep

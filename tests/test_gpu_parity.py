@@ -312,18 +312,20 @@ def test_sil_refill_bitwise_and_coherent_ties(dim, star, mesh_c2):
     assert_bitwise(b, a, SIL_FIELDS, "sil refill ")
     for r_max in (math.inf, 0.3):
         ref = to_np(scene.closest_silhouette(x, r_max, variant="exact"))
-        got = to_np(scene.closest_silhouette(x, r_max, variant="coherent"))
-        rep = tie_report(ref, got)
-        assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0, (r_max, rep)
-        assert rep["max_rel_d"] <= REL_TOL, (r_max, rep)
+        for variant in ("coherent", "warp"):
+            got = to_np(scene.closest_silhouette(x, r_max, variant=variant))
+            rep = tie_report(ref, got)
+            assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0, (variant, r_max, rep)
+            assert rep["max_rel_d"] <= REL_TOL, (variant, r_max, rep)
     assert scene.device_error() == 0
 
 
-def test_sil3d_coherent_against_oracle_small(mesh_small):
+@pytest.mark.parametrize("variant", ["coherent", "warp"])
+def test_sil3d_fast_variants_against_oracle_small(mesh_small, variant):
     x = W.uniform_points(3000, 3, seed=75)
-    got = to_np(mesh_small.closest_silhouette(x, variant="coherent"))
+    got = to_np(mesh_small.closest_silhouette(x, variant=variant))
     ref = oracle.closest_silhouette(3, *_sref(mesh_small), x)
     rep = tie_report(ref, got)
     assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0, rep
-    with pytest.raises(L.GQError, match="exact or the coherent"):
+    with pytest.raises(L.GQError, match="exact, coherent or warp"):
         mesh_small.closest_silhouette(x, variant="wide8")
