@@ -191,7 +191,8 @@ def dev_ms(fn, steps, warmup, flush=None):
 def section_c2(args, dev, flush):
     """Closest silhouette, displaced icosphere level 7 (327,680 triangles, amplitude 0.3),
     4,194,304 points U[-2,2]^3: the reference visit order one query per thread (plain),
-    the same with persistent lane refill, and the warp-coherent traversal."""
+    the same with persistent lane refill, the warp-coherent traversal and one query per
+    warp."""
     import torch
     from gquery_b200 import workloads as W
     from gquery_b200.scene import Scene
@@ -207,13 +208,14 @@ def section_c2(args, dev, flush):
     res = {"workload": "closest silhouette, icosphere level 7 (327,680 triangles) amplitude 0.3, "
                        f"{n} points U[-2,2]^3", "build_s": build_s}
     for name, variant, persist in (("plain_exact", "exact", 0), ("exact_refill", "exact", 1),
-                                   ("coherent", "coherent", 1)):
+                                   ("coherent", "coherent", 1), ("warp", "warp", 1)):
         sc.set_tuning("sil", variant, persist=persist)
         ms = dev_ms(lambda: sc.closest_silhouette(x, variant=variant, out=out, order=order, scratch=scratch),
                     steps=2 if variant == "exact" else 3, warmup=1, flush=flush)
         res[name] = {"ms": ms, "mqueries_per_s": n / ms / 1e3}
     assert sc.device_error() == 0
     res["coherent_vs_plain"] = res["plain_exact"]["ms"] / res["coherent"]["ms"]
+    res["warp_vs_plain"] = res["plain_exact"]["ms"] / res["warp"]["ms"]
     return res
 
 
