@@ -8,7 +8,8 @@ inf).  One step = Morton order + closest_point over all points, then Morton orde
 intersect over all rays, each with the scene's tuned variant; the exact binary kernel
 (gQuery's visit order) and the quantised 8-wide kernel are measured beside it.
 
-At one GPU the same line also carries (see --sections): c2 closest silhouettes on the
+At one GPU the same line also carries (see --sections): c0 2D closest point on the
+4,096-vertex star (every GPU variant and the CPU oracle), c2 closest silhouettes on the
 level-7 mesh (plain, refill, coherent), c3 512 uneven 2D scenes answered by one
 batched launch per step (eager and CUDA graph) against one plain call per scene and
 kind, c4 the serving runtime under open-loop Poisson load against per-request launches.
@@ -56,8 +57,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the exact and wide8 side-by-side runs")
     ap.add_argument("--no-autotune", action="store_true", help="use the built-in tuning table as it is")
-    ap.add_argument("--sections", default="c2,c3,c4",
-                    help="beside the headline (cp + rays on the level-8 mesh): c2 silhouettes on the level-7 "
+    ap.add_argument("--sections", default="c0,c2,c3,c4",
+                    help="beside the headline (cp + rays on the level-8 mesh): c0 2D closest point on the "
+                         "4,096-vertex star (GPU and CPU), c2 silhouettes on the level-7 "
                          "mesh, c3 512 uneven 2D scenes in one batched launch, c4 serving 64 meshes; "
                          "comma-separated or 'none' (one GPU only)")
     ap.add_argument("--c2-n", type=int, default=1 << 22, help="silhouette queries (c2)")
@@ -186,6 +188,39 @@ def dev_ms(fn, steps, warmup, flush=None):
         torch.cuda.synchronize()
         ts.append(a.elapsed_time(b))
     return statistics.median(ts)
+
+
+def section_c0(args, dev, flush):
+    """2D closest point: 4,096-vertex star polyline, 1,048,576 points U[-2,2]^2 - the
+    configuration that also runs on the CPU: every GPU variant and the CPU oracle port
+    on all host cores over the same points."""
+    import torch
+    import oracle
+    from gquery_b200 import _lib as L
+    from gquery_b200 import workloads as W
+    from gquery_b200.scene import Scene
+    V, E, Q = W.config0()
+    sc = Scene(V, E, 2, device=dev.index or 0, build_snch=False)
+    n = Q.shape[0]
+    q = torch.as_tensor(Q).to(dev)
+    order = sc.order(q)
+    out = sc.alloc_cp(n)
+    scratch = torch.empty(sc.scratch_bytes(n), dtype=torch.uint8, device=dev)
+    res = {"workload": f"2D closest point, star polyline {E.shape[0]} segments, {n} points U[-2,2]^2"}
+    for variant in ("exact", "wide8", "coherent", "auto"):
+        ms = dev_ms(lambda: sc.closest_point(q, variant=variant, out=out, order=order, scratch=scratch),
+                    steps=5, warmup=3, flush=flush)
+        res[variant] = {"ms": ms, "mqueries_per_s": n / ms / 1e3}
+    res["auto_variant"] = sc.get_tuning("cp")["variant"]
+    host = Scene(V, E, 2, device=None, build_snch=False, build_wide=False)
+    nodes, prims = host.ref_array(L.ARRAY_BVH_NODES), host.ref_array(L.ARRAY_PRIMITIVES)
+    threads = oracle.n_threads()
+    t0 = time.perf_counter()
+    oracle.closest_point(2, nodes, prims, Q, threads=threads)
+    cpu_s = time.perf_counter() - t0
+    res["cpu_oracle"] = {"seconds": cpu_s, "mqueries_per_s": n / cpu_s / 1e6, "cores": threads, "kind": "port"}
+    assert sc.device_error() == 0
+    return res
 
 
 def section_c2(args, dev, flush):
@@ -663,10 +698,12 @@ def main():
         }
         sections = [x for x in args.sections.split(",") if x and x != "none"] if world == 1 else []
         flush_buf = flush
-        for name, fn in (("c2", lambda: section_c2(args, dev, flush_buf)), ("c3", lambda: section_c3(args, dev, flush_buf)),
+        for name, fn in (("c0", lambda: section_c0(args, dev, flush_buf)),
+                         ("c2", lambda: section_c2(args, dev, flush_buf)), ("c3", lambda: section_c3(args, dev, flush_buf)),
                          ("c4", lambda: section_c4(args, dev))):
             if name in sections:
-                key = {"c2": "silhouette_c2", "c3": "batched_c3", "c4": "serving_c4"}[name]
+                key = {"c0": "closest_point_2d_c0", "c2": "silhouette_c2", "c3": "batched_c3",
+                       "c4": "serving_c4"}[name]
                 t_sec = time.perf_counter()
                 line[key] = fn()
                 line[key]["section_wall_s"] = time.perf_counter() - t_sec
