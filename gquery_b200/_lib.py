@@ -123,6 +123,8 @@ SIGNATURES = {
     "gq_scene_build_3d": (C.c_int32, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.POINTER(BuildOpts),
                                       C.POINTER(C.c_void_p)]),
     "gq_scene_free": (C.c_int32, [C.c_void_p]),
+    "gq_scene_save": (C.c_int32, [C.c_void_p, C.c_char_p]),
+    "gq_scene_load": (C.c_int32, [C.c_char_p, C.c_int32, C.POINTER(C.c_void_p)]),
     "gq_scene_get_info": (C.c_int32, [C.c_void_p, C.POINTER(SceneInfo)]),
     "gq_scene_set_tuning": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(Tuning)]),
     "gq_scene_get_tuning": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(Tuning)]),

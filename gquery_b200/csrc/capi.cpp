@@ -93,6 +93,15 @@ gq_status build_scene(const float *vertices, int64_t nv, const int32_t *prims, i
 
     s->exact_stack = img.exact_stack;
     s->wide_stack = img.wide_stack;
+    s->max_prims_in_node = o.max_prims_in_node;
+    s->n_nodes = D == 2 ? (int64_t)s->t2.nodes.size() : (int64_t)s->t3.nodes.size();
+    s->max_depth = D == 2 ? s->t2.max_depth : s->t3.max_depth;
+    s->image_bytes[0] = img.pairs.size() * sizeof(img.pairs[0]);
+    s->image_bytes[1] = img.prims.size() * sizeof(img.prims[0]);
+    s->image_bytes[2] = img.spheres.size() * sizeof(gq_tsph_t);
+    s->image_bytes[3] = img.wnodes.size() * sizeof(img.wnodes[0]);
+    s->image_bytes[4] = img.spairs.size() * sizeof(img.spairs[0]);
+    s->image_bytes[5] = img.sils.size() * sizeof(img.sils[0]);
     default_tuning(s.get());
     s->n_wide = (int64_t)img.wnodes.size();
     s->n_sil = (int64_t)img.sils.size();
@@ -139,6 +148,29 @@ gq_status build_scene(const float *vertices, int64_t nv, const int32_t *prims, i
 }
 
 bool on_host_only(const gq_scene *s) { return s->device < 0; }
+
+// Host trees of a loaded scene, rebuilt on first use: the build is deterministic, so
+// they are the trees the saved device image was flattened from.
+gq_status ensure_trees(gq_scene *s) {
+    std::lock_guard<std::mutex> lk(s->tree_mu);
+    if (s->trees_ready) return GQ_OK;
+    const int nt = (int)std::max(1u, std::thread::hardware_concurrency());
+    try {
+        if (s->dim == 2) {
+            PrimSource<2> src{s->verts.data(), s->nv, s->index.data(), s->np};
+            s->t2 = build_bvh<2>(src, s->max_prims_in_node, nt);
+            if (s->has_snch) s->s2 = build_snch<2>(src, s->t2, nt);
+        } else {
+            PrimSource<3> src{s->verts.data(), s->nv, s->index.data(), s->np};
+            s->t3 = build_bvh<3>(src, s->max_prims_in_node, nt);
+            if (s->has_snch) s->s3 = build_snch<3>(src, s->t3, nt);
+        }
+    } catch (const std::bad_alloc &) {
+        return fail(GQ_ERR_NOMEM, "out of host memory rebuilding the trees");
+    }
+    s->trees_ready = true;
+    return GQ_OK;
+}
 
 // Built-in launch choices (measured on B200 for the benchmark scenes).
 void default_tuning(gq_scene *s) {
@@ -327,10 +359,10 @@ gq_status gq_scene_get_info(const gq_scene *s, gq_scene_info *info) {
     info->dim = s->dim;
     info->n_vertices = s->nv;
     info->n_prims = s->np;
-    info->n_nodes = s->dim == 2 ? (int64_t)s->t2.nodes.size() : (int64_t)s->t3.nodes.size();
+    info->n_nodes = s->n_nodes;
     info->n_wide_nodes = s->n_wide;
     info->n_silhouettes = s->n_sil;
-    info->max_depth = s->dim == 2 ? s->t2.max_depth : s->t3.max_depth;
+    info->max_depth = s->max_depth;
     info->exact_stack = s->exact_stack;
     info->wide_stack = s->wide_stack;
     info->device_bytes = s->device_bytes;
@@ -354,6 +386,8 @@ gq_status gq_scene_ref_array(const gq_scene *s, int32_t which, float *dst, int64
     const bool snch_needed = which == GQ_ARRAY_SNCH_NODES || which == GQ_ARRAY_SILHOUETTES ||
                              which == GQ_ARRAY_RAW_SILHOUETTES;
     if (snch_needed && !s->has_snch) return fail(GQ_ERR_UNSUPPORTED, "scene was built without the SNCH");
+    gq_status tst = ensure_trees(const_cast<gq_scene *>(s));
+    if (tst != GQ_OK) return tst;
     if (s->dim == 2) {
         PrimSource<2> src{s->verts.data(), s->nv, s->index.data(), s->np};
         switch (which) {
@@ -557,6 +591,150 @@ gq_status gq_brute_f64(const gq_scene *s, int32_t kind, gq_vecs a, gq_vecs b, in
     DeviceGuard g(s->device);
     cudaError_t e = gqd::launch_brute_f64(s->dev, kind, a, b, n, out_d, out_id, (cudaStream_t)stream);
     if (e != cudaSuccess) return fail_cuda(e, "brute_f64 launch");
+    return GQ_OK;
+}
+
+namespace {
+
+// Saved scene: header, then the input geometry and the six device arrays, raw.
+struct SceneFileHeader {
+    char magic[8];
+    int32_t version, dim;
+    int64_t nv, np;
+    int32_t max_prims_in_node, has_snch, has_wide, exact_stack, wide_stack, max_depth;
+    int64_t n_nodes, n_wide, n_sil;
+    int32_t root_ref, wroot_ref, sroot_ref, pad;
+    float root_lo[3], root_hi[3], coord_bound, pad2;
+    uint64_t image_bytes[6];
+};
+constexpr char kSceneMagic[8] = {'G', 'Q', 'S', 'C', 'E', 'N', 'E', '1'};
+
+struct File {
+    FILE *f = nullptr;
+    ~File() {
+        if (f) std::fclose(f);
+    }
+};
+
+}  // namespace
+
+gq_status gq_scene_save(const gq_scene *s, const char *path) {
+    if (!s || !path) return fail(GQ_ERR_INVALID, "null argument");
+    if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "only scenes with a device copy can be saved");
+    SceneFileHeader h{};
+    std::memcpy(h.magic, kSceneMagic, 8);
+    h.version = 1;
+    h.dim = s->dim;
+    h.nv = s->nv;
+    h.np = s->np;
+    h.max_prims_in_node = s->max_prims_in_node;
+    h.has_snch = s->has_snch;
+    h.has_wide = s->has_wide;
+    h.exact_stack = s->exact_stack;
+    h.wide_stack = s->wide_stack;
+    h.max_depth = s->max_depth;
+    h.n_nodes = s->n_nodes;
+    h.n_wide = s->n_wide;
+    h.n_sil = s->n_sil;
+    h.root_ref = s->dev.root_ref;
+    h.wroot_ref = s->dev.wroot_ref;
+    h.sroot_ref = s->dev.sroot_ref;
+    for (int k = 0; k < 3; ++k) h.root_lo[k] = s->dev.root_lo[k], h.root_hi[k] = s->dev.root_hi[k];
+    h.coord_bound = s->dev.coord_bound;
+    for (int k = 0; k < 6; ++k) h.image_bytes[k] = s->image_bytes[k];
+    const void *dev_arrays[6] = {s->dev.pairs, s->dev.prims, s->dev.spheres, s->dev.wnodes, s->dev.spairs,
+                                 s->dev.sils};
+    File out;
+    out.f = std::fopen(path, "wb");
+    if (!out.f) return fail(GQ_ERR_INVALID, std::string("cannot open ") + path + " for writing");
+    bool ok = std::fwrite(&h, sizeof h, 1, out.f) == 1;
+    ok = ok && std::fwrite(s->verts.data(), sizeof(float), s->verts.size(), out.f) == s->verts.size();
+    ok = ok && std::fwrite(s->index.data(), sizeof(int32_t), s->index.size(), out.f) == s->index.size();
+    DeviceGuard g(s->device);
+    std::vector<char> buf;
+    for (int k = 0; k < 6 && ok; ++k) {
+        if (!h.image_bytes[k]) continue;
+        buf.resize(h.image_bytes[k]);
+        cudaError_t e = cudaMemcpy(buf.data(), dev_arrays[k], buf.size(), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return fail_cuda(e, "scene save");
+        ok = std::fwrite(buf.data(), 1, buf.size(), out.f) == buf.size();
+    }
+    if (!ok || std::fflush(out.f) != 0) return fail(GQ_ERR_INVALID, std::string("write failed: ") + path);
+    return GQ_OK;
+}
+
+gq_status gq_scene_load(const char *path, int32_t device, gq_scene **out) {
+    if (!path || !out) return fail(GQ_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (device < 0) return fail(GQ_ERR_INVALID, "a loaded scene lives on a device");
+    File in;
+    in.f = std::fopen(path, "rb");
+    if (!in.f) return fail(GQ_ERR_INVALID, std::string("cannot open ") + path);
+    SceneFileHeader h{};
+    if (std::fread(&h, sizeof h, 1, in.f) != 1 || std::memcmp(h.magic, kSceneMagic, 8) != 0 || h.version != 1 ||
+        (h.dim != 2 && h.dim != 3) || h.nv < 0 || h.np < 0)
+        return fail(GQ_ERR_INVALID, std::string(path) + " is not a saved scene of this version");
+    std::unique_ptr<gq_scene> s(new (std::nothrow) gq_scene());
+    if (!s) return fail(GQ_ERR_NOMEM, "out of host memory");
+    s->dim = h.dim;
+    s->device = device;
+    s->nv = h.nv;
+    s->np = h.np;
+    s->max_prims_in_node = h.max_prims_in_node;
+    s->has_snch = h.has_snch != 0;
+    s->has_wide = h.has_wide != 0;
+    s->exact_stack = h.exact_stack;
+    s->wide_stack = h.wide_stack;
+    s->max_depth = h.max_depth;
+    s->n_nodes = h.n_nodes;
+    s->n_wide = h.n_wide;
+    s->n_sil = h.n_sil;
+    s->trees_ready = false;
+    try {
+        s->verts.resize((size_t)(h.nv * h.dim));
+        s->index.resize((size_t)(h.np * h.dim));
+    } catch (const std::bad_alloc &) {
+        return fail(GQ_ERR_NOMEM, "out of host memory");
+    }
+    bool ok = std::fread(s->verts.data(), sizeof(float), s->verts.size(), in.f) == s->verts.size() &&
+              std::fread(s->index.data(), sizeof(int32_t), s->index.size(), in.f) == s->index.size();
+    std::vector<char> arrays[6];
+    for (int k = 0; k < 6 && ok; ++k) {
+        s->image_bytes[k] = (size_t)h.image_bytes[k];
+        arrays[k].resize(s->image_bytes[k]);
+        ok = std::fread(arrays[k].data(), 1, arrays[k].size(), in.f) == arrays[k].size();
+    }
+    if (!ok) return fail(GQ_ERR_INVALID, std::string(path) + " is truncated");
+    default_tuning(s.get());
+    gqd::DevScene &d = s->dev;
+    d.dim = h.dim;
+    for (int k = 0; k < 3; ++k) d.root_lo[k] = h.root_lo[k], d.root_hi[k] = h.root_hi[k];
+    DeviceGuard g(device);
+    if (!g.ok) return fail(GQ_ERR_CUDA, "cannot select the scene's CUDA device");
+    const void *ptrs[6] = {};
+    gq_status st;
+    for (int k = 0; k < 6; ++k)
+        if ((st = s->upload(arrays[k], &ptrs[k])) != GQ_OK) return st;
+    d.pairs = ptrs[0];
+    d.prims = ptrs[1];
+    d.spheres = (const gq_tsph_t *)ptrs[2];
+    d.wnodes = ptrs[3];
+    d.spairs = ptrs[4];
+    d.sils = ptrs[5];
+    const void *pv = nullptr, *pi = nullptr, *pe = nullptr;
+    if ((st = s->upload(s->verts, &pv)) != GQ_OK) return st;
+    if ((st = s->upload(s->index, &pi)) != GQ_OK) return st;
+    std::vector<int32_t> zero(1, 0);
+    if ((st = s->upload(zero, &pe)) != GQ_OK) return st;
+    d.verts = (const float *)pv;
+    d.index = (const int32_t *)pi;
+    d.err = (int32_t *)pe;
+    d.n_prims = h.np;
+    d.coord_bound = h.coord_bound;
+    d.root_ref = h.root_ref;
+    d.wroot_ref = h.wroot_ref;
+    d.sroot_ref = h.sroot_ref;
+    *out = s.release();
     return GQ_OK;
 }
 

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -52,6 +53,14 @@ struct gq_scene {
     int64_t device_bytes = 0;
     gqd::DevScene dev{};
     gq_tuning tune[3] = {};
+    // what a saved scene needs besides the device arrays
+    size_t image_bytes[6] = {};  // pairs, prims, spheres, wide nodes, SNCH pairs, silhouettes
+    int max_prims_in_node = 10;
+    int64_t n_nodes = 0;
+    int max_depth = 0;
+    // host trees (reference arrays): absent in a loaded scene until first asked for
+    bool trees_ready = true;
+    std::mutex tree_mu;
 
     ~gq_scene() {
         if (device < 0 || allocs.empty()) return;

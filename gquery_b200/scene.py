@@ -100,6 +100,30 @@ class Scene:
         self.has_wide = build_wide
         self.torch_device = torch.device("cuda", self.device) if self.device >= 0 else None
 
+    def save(self, path: str) -> None:
+        """Writes the scene (geometry and flattened device arrays) for :meth:`load`."""
+        L.check(L.lib().gq_scene_save(self._h, str(path).encode()))
+
+    @classmethod
+    def load(cls, path: str, *, device: int = 0) -> "Scene":
+        """A scene saved by :meth:`save`, uploaded to `device` without rebuilding its
+        trees (the reference arrays rebuild them on first use)."""
+        h = C.c_void_p()
+        L.check(L.lib().gq_scene_load(str(path).encode(), int(device), C.byref(h)))
+        self = cls.__new__(cls)
+        self._h = h
+        info = L.SceneInfo()
+        L.check(L.lib().gq_scene_get_info(self._h, C.byref(info)))
+        self.info = {k: (list(getattr(info, k)) if k.startswith("bbox") else getattr(info, k))
+                     for k, _ in L.SceneInfo._fields_}
+        self.dim = self.info["dim"]
+        self.vertices_host = self.indices_host = None
+        self.device = int(device)
+        self.has_snch = self.info["n_silhouettes"] > 0
+        self.has_wide = self.info["n_wide_nodes"] > 0
+        self.torch_device = torch.device("cuda", self.device)
+        return self
+
     def close(self):
         if getattr(self, "_h", None) and self._h.value:
             L.lib().gq_scene_free(self._h)

@@ -100,12 +100,15 @@ class Server:
     ring_queries: ring capacity per kind (cp, ray, sil); step_queries: most queries of
     one kind per step and the largest request; max_inflight: closest-point / ray step
     slots (streams); silhouette steps have sil_slots slots of their own holding at most
-    sil_share of the GPU together, sil_step_queries queries per step.  Silhouettes default to one query per warp ("warp"): served
-    requests are sparse, and a warp per query bounds the latency of far-reaching ones."""
+    sil_share of the GPU together, sil_step_queries queries per step.  Served requests
+    are sparse (few queries per scene per step), so closest points default to one lane
+    per query in the reference order ("exact": cheaper than a warp-coherent walk when
+    neighbours are far apart) and silhouettes to one query per warp ("warp": bounds the
+    latency of far-reaching ones)."""
 
     def __init__(self, scenes: Sequence[Scene], *, budget_bytes: int = 0, ring_queries=(1 << 22,) * 3,
                  step_queries: int = 1 << 19, max_inflight: int = 2, per_request: bool = False,
-                 cp_variant: str = "coherent", ray_variant: str = "wide8", sil_variant: str = "warp",
+                 cp_variant: str = "exact", ray_variant: str = "wide8", sil_variant: str = "warp",
                  sil_share: float = 0.8, sil_slots: int = 2, sil_step_queries: int = 1 << 15):
         self.scenes = list(scenes)
         self.dim = self.scenes[0].dim

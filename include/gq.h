@@ -140,6 +140,14 @@ gq_status gq_scene_build_2d(const float *vertices, int64_t nv, const int32_t *ed
 gq_status gq_scene_build_3d(const float *vertices, int64_t nv, const int32_t *faces, int64_t nf,
                             const gq_build_opts *opts, gq_scene **out);
 gq_status gq_scene_free(gq_scene *scene);
+
+/* Scene files (no counterpart in the reference, which rebuilds its trees whenever a
+ * Mesh / Polyline is constructed): save writes the input geometry and the flattened
+ * device arrays of a scene that has a device copy; load uploads them to `device` without
+ * building anything.  The host trees behind gq_scene_ref_array are rebuilt on first use
+ * (the build is deterministic).  The format is native-endian and versioned. */
+gq_status gq_scene_save(const gq_scene *scene, const char *path);
+gq_status gq_scene_load(const char *path, int32_t device, gq_scene **out);
 gq_status gq_scene_get_info(const gq_scene *scene, gq_scene_info *info);
 
 /* Launch choices per query kind (no counterpart in the reference, whose DrJit backend
