@@ -59,7 +59,7 @@ def candidates(kind: str, dim: int, has_wide: bool, exact_stack: int, wide_stack
             return []
         for b in blocks:
             out.append(dict(variant="coherent", block=b))
-            out.append(dict(variant="warp", block=b))
+            out.append(dict(variant="warp", packet=0, block=b))
             out.append(dict(variant="exact", persist=1, budget=32, block=b))
         out.append(dict(variant="exact", persist=0, block=128))
     else:

@@ -5,8 +5,8 @@ mesh.py:120; Mesh.intersect_bvh, mesh.py:87; Mesh.closest_silhouette_snch,
 mesh.py:138; and the Polyline counterparts).  A :class:`SceneBatch` holds device views
 of many scenes of one dimension and answers a mixed step - closest points, rays and
 silhouette queries, each tagged with its scene - in one persistent launch, with the
-answers of the single-scene calls (closest points: ``coherent``; rays: ``wide8`` when
-every scene has wide nodes; silhouettes: ``warp``).  ``run`` allocates nothing on the
+answers of the single-scene calls (closest points and silhouettes: ``coherent``; rays:
+``wide8`` when every scene has wide nodes).  ``run`` allocates nothing on the
 device beyond the output records, so a step with fixed shapes can be recorded in a CUDA
 graph (:meth:`SceneBatch.capture`).
 """
@@ -41,7 +41,7 @@ class SceneBatch:
     warp, for sparse queries).  ``ray_variant``: "wide8" or "exact"."""
 
     def __init__(self, scenes: Sequence[Scene], max_queries: int, *, cp_variant: str = "coherent",
-                 ray_variant: str = "wide8", sil_variant: str = "warp"):
+                 ray_variant: str = "wide8", sil_variant: str = "coherent"):
         if not scenes:
             raise ValueError("a batch needs at least one scene")
         if cp_variant not in ("coherent", "exact") or ray_variant not in ("wide8", "exact") or \

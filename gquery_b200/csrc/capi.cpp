@@ -149,6 +149,11 @@ gq_status build_scene(const float *vertices, int64_t nv, const int32_t *prims, i
 
 bool on_host_only(const gq_scene *s) { return s->device < 0; }
 
+// Silhouette queries tuned to the WARP variant with `packet` set switch to the coherent
+// traversal from this many queries on (measured crossover on B200: ~2^20 for the
+// level-7 benchmark mesh, below it for smaller scenes).
+constexpr int64_t kSilCoherentFrom = 1 << 18;
+
 // Host trees of a loaded scene, rebuilt on first use: the build is deterministic, so
 // they are the trees the saved device image was flattened from.
 gq_status ensure_trees(gq_scene *s) {
@@ -175,7 +180,8 @@ gq_status ensure_trees(gq_scene *s) {
 // Built-in launch choices (measured on B200 for the benchmark scenes).
 void default_tuning(gq_scene *s) {
     for (int k = 0; k < 3; ++k) s->tune[k] = gq_tuning{GQ_VARIANT_EXACT, 0, 1, 0, 32};
-    s->tune[GQ_KIND_SILHOUETTE] = gq_tuning{GQ_VARIANT_WARP, 0, 1, 1, 32};
+    // one query per warp for few queries, warp-coherent from 2^18 on (packet = 1)
+    s->tune[GQ_KIND_SILHOUETTE] = gq_tuning{GQ_VARIANT_WARP, 1, 1, 1, 32};
     if (s->dim == 3) {
         s->tune[GQ_KIND_CLOSEST_POINT] = gq_tuning{GQ_VARIANT_COHERENT, 1, 1, 0, 32};
         s->tune[GQ_KIND_INTERSECT] = gq_tuning{s->has_wide ? GQ_VARIANT_WIDE8 : GQ_VARIANT_EXACT, 0, 1, 1, 32};
@@ -539,7 +545,10 @@ gq_status gq_closest_silhouette(const gq_scene *s, gq_vecs x, const float *r_max
     if (!s->has_snch) return fail(GQ_ERR_UNSUPPORTED, "scene was built without the SNCH");
     if (s->exact_stack > GQ_STACK_EXACT) return fail(GQ_ERR_DEPTH, "tree deeper than gQuery's 64-entry stack");
     if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "scene was built without a device copy");
-    const int v = resolve_variant(s, opts, GQ_KIND_SILHOUETTE);
+    int v = resolve_variant(s, opts, GQ_KIND_SILHOUETTE);
+    if ((!opts || opts->variant == GQ_VARIANT_AUTO) && v == GQ_VARIANT_WARP && s->tune[GQ_KIND_SILHOUETTE].packet &&
+        n >= kSilCoherentFrom)
+        v = GQ_VARIANT_COHERENT;  // many queries: neighbours share their walks
     if (v != GQ_VARIANT_EXACT && v != GQ_VARIANT_COHERENT && v != GQ_VARIANT_WARP)
         return fail(GQ_ERR_UNSUPPORTED, "silhouette queries run the exact, coherent or warp variant");
     DeviceGuard g(s->device);

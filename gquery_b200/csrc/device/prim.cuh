@@ -246,4 +246,75 @@ __device__ __forceinline__ bool cone_overlaps(const float *lo, const float *hi, 
     return (hs > GQ_PIO2_F) | in_range(GQ_PIO2_F, dA - hs, dA + hs);
 }
 
+// The normal-cone test of cone_overlaps restated without inverse trigonometry, for the
+// traversals that promise the reference's answers up to FP32 ties (not its exact visit
+// order).  With dA the angle between the cone axis and the view direction v and h_v
+// the view cone's half angle, the reference accepts when h + h_v >= pi/2 or
+// |dA - pi/2| <= h + h_v, i.e. when |cos dA| = |axis . v| <= sin(h + h_v); the sine and
+// cosine of h + h_v follow from sin h, cos h (hardware approximations) and those of h_v,
+// which are ratios of lengths the reference already forms (radius / l, or d and s of
+// its atan2).  Both comparisons carry a margin of kConeSlack, far above the few-ulp
+// error of either form, so every node the reference admits is admitted here; a node it
+// rejects by less than the margin may be visited too, which cannot change a correct
+// answer.
+constexpr float kConeSlack = 1e-5f;
+
+template <int D>
+__device__ __forceinline__ bool cone_overlaps_fast(const float *lo, const float *hi, const float *axis, float half,
+                                                   float radius, const float *x, float dmin) {
+    if (half >= GQ_PIO2_F) return true;  // |dA - pi/2| <= pi/2 <= h always holds
+    float c[D], v[D], l2 = 0.f;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        c[k] = 0.5f * (lo[k] + hi[k]);
+        v[k] = c[k] - x[k];
+        l2 = __fmaf_rn(v[k], v[k], l2);
+    }
+    if (!(l2 > 1e-30f)) return true;
+    const float il = rsqrtf(l2), l = l2 * il;
+    float dt = 0.f;
+#pragma unroll
+    for (int k = 0; k < D; ++k) dt = __fmaf_rn(axis[k], v[k], dt);
+    dt = fabsf(dt * il);
+    float sv, cv;  // sine and cosine of the view cone's half angle
+    if (l > radius) {
+        sv = radius * il;
+        cv = sqrtf(fmaxf(0.f, 1.f - sv * sv));
+    } else {
+        float e[D], u[D], dd = 0.f;
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+            e[k] = hi[k] - c[k];
+            u[k] = v[k] * il;
+            dd = __fmaf_rn(e[k], fabsf(u[k]), dd);
+        }
+        const float s = l - dd;
+        if (s < kConeSlack * l) return true;
+        float pd;
+        if (D == 2) {
+            pd = fabsf(__fmaf_rn(e[0], fabsf(u[D - 1]), e[D - 1] * fabsf(u[0])));
+        } else {
+            // project_to_plane_3D (snch3d.py:26-30) with the same orthonormal basis
+            const float nx = u[0], ny = u[1], nz = u[D - 1];
+            const float sign = copysignf(1.f, nz);
+            const float a = -1.f / (sign + nz);
+            const float b = nx * ny * a;
+            const float r1 = __fmaf_rn(e[D - 1], fabsf(-sign * nx),
+                                       __fmaf_rn(e[1], fabsf(sign * b), e[0] * fabsf(1.f + sign * nx * nx * a)));
+            const float r2 = __fmaf_rn(e[D - 1], fabsf(-ny), __fmaf_rn(e[1], fabsf(sign + ny * ny * a), e[0] * fabsf(b)));
+            pd = sqrtf(__fmaf_rn(r1, r1, r2 * r2));
+        }
+        const float ih = rsqrtf(__fmaf_rn(pd, pd, s * s));
+        sv = pd * ih;
+        cv = s * ih;
+    }
+    float sh, ch;
+    __sincosf(half, &sh, &ch);
+    const float cos_sum = ch * cv - sh * sv;  // cos(h + h_v)
+    if (cos_sum <= kConeSlack) return true;   // h + h_v >= pi/2
+    const float sin_sum = sh * cv + ch * sv;  // sin(h + h_v), h + h_v in [0, pi/2)
+    (void)dmin;
+    return dt <= sin_sum + kConeSlack;
+}
+
 }  // namespace gqd

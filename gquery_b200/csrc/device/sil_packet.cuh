@@ -3,7 +3,7 @@
 //
 // The lanes of a warp that hold queries on the same scene walk the tree once: the warp
 // pops one entry, every lane whose own stack key passes its own r_max takes part,
-// interior nodes are tested per lane with the reference's box and normal-cone tests
+// interior nodes are tested per lane with the reference's box test and normal-cone test
 // (SNCHNode3D.overlaps, snch3d.py:55-95; snch.py:60-97) against the lane's r_max, and
 // a child is entered when at least one lane admits it.  Leaves are scanned by all
 // participating lanes together with the reference's per-silhouette test and acceptance
@@ -13,7 +13,8 @@
 // depend on r_max, so the silhouettes a lane can reach are the same in any visit
 // order, and r_max only prunes boxes that cannot hold a closer silhouette.  The order
 // (nearest lane's box first) changes only which of two equally distant silhouettes
-// wins.
+// wins.  The cone test is the trigonometry-free restatement cone_overlaps_fast, which
+// admits every node the reference's test admits.
 #pragma once
 
 #include "packet.cuh"
@@ -120,7 +121,7 @@ __device__ __forceinline__ void closest_silhouette(const DevScene &s, unsigned m
                               L.x[D - 1], dm[c], dmax);
                 hit[c] = dm[c] <= L.r;
                 if ((half[c] >= 0.f) & hit[c])
-                    hit[c] = cone_overlaps<D>(lo[c], hi[c], ax[c], half[c], rad[c], L.x, dm[c]);
+                    hit[c] = cone_overlaps_fast<D>(lo[c], hi[c], ax[c], half[c], rad[c], L.x, dm[c]);
             }
         }
         const unsigned m0 = __ballot_sync(0xffffffffu, hit[0]), m1 = __ballot_sync(0xffffffffu, hit[1]);

@@ -13,7 +13,8 @@
 // (snch3d.py:55-95, snch.py:60-97).  The warp then takes the minimum r_max over its
 // lanes and pushes the admitted children (lane 0's on top, the nearer child above the
 // farther).  Answers equal the reference's except at FP32 distance ties, for the
-// reasons given in sil_packet.cuh (the cone test does not depend on r_max).
+// reasons given in sil_packet.cuh (the cone test does not depend on r_max; its
+// trigonometry-free form cone_overlaps_fast admits every node the reference admits).
 //
 // Stack bound: a step that takes `take` entries pushes at most 2*take, so the warp
 // takes 32 entries only while that leaves room for a depth-first descent, and one
@@ -126,7 +127,7 @@ __device__ __forceinline__ void closest_silhouette(const DevScene &s, const floa
                                   x[D - 1], dm[c], dmax);
                     hit[c] = dm[c] <= L.r;
                     if ((half[c] >= 0.f) & hit[c])
-                        hit[c] = cone_overlaps<D>(lo[c], hi[c], ax[c], half[c], rad[c], x, dm[c]);
+                        hit[c] = cone_overlaps_fast<D>(lo[c], hi[c], ax[c], half[c], rad[c], x, dm[c]);
                 }
                 const bool sw = dm[1] < dm[0];  // push the farther first so the nearer is popped first
                 const int first = sw ? 0 : 1, second = sw ? 1 : 0;
