@@ -57,9 +57,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the exact and wide8 side-by-side runs")
     ap.add_argument("--no-autotune", action="store_true", help="use the built-in tuning table as it is")
-    ap.add_argument("--sections", default="c0,c2,c3,c4",
+    ap.add_argument("--sections", default="c0,build,c2,c3,c4",
                     help="beside the headline (cp + rays on the level-8 mesh): c0 2D closest point on the "
-                         "4,096-vertex star (GPU and CPU), c2 silhouettes on the level-7 "
+                         "4,096-vertex star (GPU and CPU), build host SAH vs device build of the "
+                         "level-8 mesh, c2 silhouettes on the level-7 "
                          "mesh, c3 512 uneven 2D scenes in one batched launch, c4 serving 64 meshes; "
                          "comma-separated or 'none' (one GPU only)")
     ap.add_argument("--c2-n", type=int, default=1 << 22, help="silhouette queries (c2)")
@@ -220,6 +221,41 @@ def section_c0(args, dev, flush):
     cpu_s = time.perf_counter() - t0
     res["cpu_oracle"] = {"seconds": cpu_s, "mqueries_per_s": n / cpu_s / 1e6, "cores": threads, "kind": "port"}
     assert sc.device_error() == 0
+    return res
+
+
+def section_build(args, dev, flush):
+    """Scene build for the level-8 mesh: the host SAH build (the reference's builder
+    algorithm) against the linear BVH built on the device, and closest-point / ray
+    throughput on each tree."""
+    import torch
+    from gquery_b200 import workloads as W
+    from gquery_b200.scene import Scene
+    V, F = W.config1_mesh()
+    res = {"workload": f"icosphere level 8, {F.shape[0]} triangles; 1,048,576 cp queries + rays"}
+    t0 = time.perf_counter()
+    host = Scene(V, F, 3, device=dev.index or 0, build_snch=False, build_wide=False)
+    res["host_sah_build_s"] = time.perf_counter() - t0
+    torch.cuda.synchronize()
+    Scene(V, F, 3, device=dev.index or 0, gpu_build=True)  # warm-up (module load, pool growth)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    devb = Scene(V, F, 3, device=dev.index or 0, gpu_build=True)
+    torch.cuda.synchronize()
+    res["device_build_s"] = time.perf_counter() - t0
+    res["device_tree_depth"] = devb.info["max_depth"]
+    res["host_tree_depth"] = host.info["max_depth"]
+    n = 1 << 20
+    q = torch.as_tensor(W.uniform_points(n, 3, seed=41)).to(dev)
+    o, d = (torch.as_tensor(a).to(dev) for a in W.rays(n, 3, seed=42))
+    for name, sc in (("host_tree", host), ("device_tree", devb)):
+        row = {}
+        for variant in ("exact", "coherent"):
+            ms = dev_ms(lambda: sc.closest_point(q, variant=variant), steps=3, warmup=2, flush=flush)
+            row[f"cp_{variant}_mqueries_per_s"] = n / ms / 1e3
+        ms = dev_ms(lambda: sc.intersect(o, d, variant="exact"), steps=3, warmup=2, flush=flush)
+        row["ray_exact_mqueries_per_s"] = n / ms / 1e3
+        res[name] = row
     return res
 
 
@@ -699,11 +735,12 @@ def main():
         sections = [x for x in args.sections.split(",") if x and x != "none"] if world == 1 else []
         flush_buf = flush
         for name, fn in (("c0", lambda: section_c0(args, dev, flush_buf)),
+                         ("build", lambda: section_build(args, dev, flush_buf)),
                          ("c2", lambda: section_c2(args, dev, flush_buf)), ("c3", lambda: section_c3(args, dev, flush_buf)),
                          ("c4", lambda: section_c4(args, dev))):
             if name in sections:
-                key = {"c0": "closest_point_2d_c0", "c2": "silhouette_c2", "c3": "batched_c3",
-                       "c4": "serving_c4"}[name]
+                key = {"c0": "closest_point_2d_c0", "build": "scene_build", "c2": "silhouette_c2",
+                       "c3": "batched_c3", "c4": "serving_c4"}[name]
                 t_sec = time.perf_counter()
                 line[key] = fn()
                 line[key]["section_wall_s"] = time.perf_counter() - t_sec

@@ -49,7 +49,7 @@ SERVER_PER_REQUEST = 4
 
 class BuildOpts(C.Structure):
     _fields_ = [("max_prims_in_node", C.c_int32), ("n_threads", C.c_int32), ("build_snch", C.c_int32),
-                ("build_wide", C.c_int32), ("device", C.c_int32)]
+                ("build_wide", C.c_int32), ("device", C.c_int32), ("gpu_build", C.c_int32)]
 
 
 class SceneInfo(C.Structure):

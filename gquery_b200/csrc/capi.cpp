@@ -13,6 +13,7 @@
 
 #include "../../include/gq.h"
 #include "device/batch.cuh"
+#include "device/gpu_build.cuh"
 #include "internal.hpp"
 
 using namespace gqb;
@@ -39,13 +40,64 @@ namespace {
 
 void default_tuning(gq_scene *s);
 
+// Linear BVH on the device (device/gpu_build.cu) straight into the traversal records.
+template <int D>
+gq_status build_on_device(gq_scene *s, const gq_build_opts &o) {
+    if (o.device < 0) return fail(GQ_ERR_INVALID, "a device build needs a device");
+    if (o.build_snch) return fail(GQ_ERR_UNSUPPORTED, "the device build has no SNCH (build_snch must be 0)");
+    if (s->np < 1) return fail(GQ_ERR_INVALID, "a device build needs at least one primitive");
+    DeviceGuard g(o.device);
+    if (!g.ok) return fail(GQ_ERR_CUDA, "cannot select the scene's CUDA device");
+    gqd::DevScene &d = s->dev;
+    const void *pv = nullptr, *pi = nullptr, *pe = nullptr;
+    gq_status st;
+    if ((st = s->upload(s->verts, &pv)) != GQ_OK) return st;
+    if ((st = s->upload(s->index, &pi)) != GQ_OK) return st;
+    std::vector<int32_t> zero(1, 0);
+    if ((st = s->upload(zero, &pe)) != GQ_OK) return st;
+    using Pair = std::conditional_t<D == 2, gq_pair2_t, gq_pair3_t>;
+    using Prim = std::conditional_t<D == 2, gq_seg_t, gq_tri_t>;
+    const size_t pair_bytes = sizeof(Pair) * (size_t)std::max<int64_t>(s->np - 1, 1);
+    const size_t prim_bytes = sizeof(Prim) * (size_t)s->np;
+    void *pairs = nullptr, *prims = nullptr;
+    cudaError_t e = cudaMalloc(&pairs, pair_bytes);
+    if (e == cudaSuccess) s->allocs.push_back(pairs), e = cudaMalloc(&prims, prim_bytes);
+    if (e == cudaSuccess) s->allocs.push_back(prims);
+    if (e != cudaSuccess) return fail(GQ_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    s->device_bytes += (int64_t)(pair_bytes + prim_bytes);
+    gqd::GpuBuildResult r;
+    e = gqd::gpu_build_bvh(D, (const float *)pv, (const int32_t *)pi, s->np, pairs, prims, r, nullptr);
+    if (e != cudaSuccess) return fail_cuda(e, "device build");
+    d.dim = D;
+    d.pairs = pairs;
+    d.prims = prims;
+    d.verts = (const float *)pv;
+    d.index = (const int32_t *)pi;
+    d.err = (int32_t *)pe;
+    d.n_prims = s->np;
+    d.coord_bound = 0.f;
+    for (float x : s->verts) d.coord_bound = std::max(d.coord_bound, std::fabs(x));
+    d.root_ref = r.root_ref;
+    for (int k = 0; k < 3; ++k) d.root_lo[k] = r.root_lo[k], d.root_hi[k] = r.root_hi[k];
+    s->gpu_built = true;
+    s->trees_ready = false;
+    s->max_prims_in_node = 1;
+    s->max_depth = r.max_depth;
+    s->exact_stack = r.max_depth + 1;
+    s->n_nodes = 2 * s->np - 1;
+    s->image_bytes[0] = s->np > 1 ? pair_bytes : 0;
+    s->image_bytes[1] = prim_bytes;
+    default_tuning(s);
+    return GQ_OK;
+}
+
 template <int D>
 gq_status build_scene(const float *vertices, int64_t nv, const int32_t *prims, int64_t np, const gq_build_opts *opts,
                       gq_scene **out) {
     if (!out) return fail(GQ_ERR_INVALID, "out is null");
     *out = nullptr;
     if (!vertices || !prims) return fail(GQ_ERR_INVALID, "null vertex or primitive array");
-    gq_build_opts o{10, 0, 1, 1, 0};
+    gq_build_opts o{10, 0, 1, 1, 0, 0};
     if (opts) o = *opts;
     if (o.max_prims_in_node < 1) return fail(GQ_ERR_INVALID, "max_prims_in_node must be >= 1");
     int nt = o.n_threads > 0 ? o.n_threads : (int)std::max(1u, std::thread::hardware_concurrency());
@@ -65,6 +117,12 @@ gq_status build_scene(const float *vertices, int64_t nv, const int32_t *prims, i
     PrimSource<D> src{s->verts.data(), nv, s->index.data(), np};
     std::string bad = validate_source<D>(src);
     if (!bad.empty()) return fail(GQ_ERR_INVALID, bad);
+    if (o.gpu_build) {
+        gq_status st = build_on_device<D>(s.get(), o);
+        if (st != GQ_OK) return st;
+        *out = s.release();
+        return GQ_OK;
+    }
 
     DeviceImage<D> img;
     try {
@@ -392,6 +450,8 @@ gq_status gq_scene_ref_array(const gq_scene *s, int32_t which, float *dst, int64
     const bool snch_needed = which == GQ_ARRAY_SNCH_NODES || which == GQ_ARRAY_SILHOUETTES ||
                              which == GQ_ARRAY_RAW_SILHOUETTES;
     if (snch_needed && !s->has_snch) return fail(GQ_ERR_UNSUPPORTED, "scene was built without the SNCH");
+    if (s->gpu_built)
+        return fail(GQ_ERR_UNSUPPORTED, "scene was built on the device; the reference arrays describe the host SAH build");
     gq_status tst = ensure_trees(const_cast<gq_scene *>(s));
     if (tst != GQ_OK) return tst;
     if (s->dim == 2) {
@@ -612,7 +672,7 @@ struct SceneFileHeader {
     int64_t nv, np;
     int32_t max_prims_in_node, has_snch, has_wide, exact_stack, wide_stack, max_depth;
     int64_t n_nodes, n_wide, n_sil;
-    int32_t root_ref, wroot_ref, sroot_ref, pad;
+    int32_t root_ref, wroot_ref, sroot_ref, gpu_built;
     float root_lo[3], root_hi[3], coord_bound, pad2;
     uint64_t image_bytes[6];
 };
@@ -648,6 +708,7 @@ gq_status gq_scene_save(const gq_scene *s, const char *path) {
     h.root_ref = s->dev.root_ref;
     h.wroot_ref = s->dev.wroot_ref;
     h.sroot_ref = s->dev.sroot_ref;
+    h.gpu_built = s->gpu_built;
     for (int k = 0; k < 3; ++k) h.root_lo[k] = s->dev.root_lo[k], h.root_hi[k] = s->dev.root_hi[k];
     h.coord_bound = s->dev.coord_bound;
     for (int k = 0; k < 6; ++k) h.image_bytes[k] = s->image_bytes[k];
@@ -699,6 +760,7 @@ gq_status gq_scene_load(const char *path, int32_t device, gq_scene **out) {
     s->n_wide = h.n_wide;
     s->n_sil = h.n_sil;
     s->trees_ready = false;
+    s->gpu_built = h.gpu_built != 0;
     try {
         s->verts.resize((size_t)(h.nv * h.dim));
         s->index.resize((size_t)(h.np * h.dim));

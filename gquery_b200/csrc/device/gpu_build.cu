@@ -1,0 +1,325 @@
+// Binary BVH built on the device (linear BVH): for scenes that must be admitted in
+// milliseconds rather than after the host SAH build.  Primitive centroids get 30-bit
+// Morton codes over the centroid bounds; (code << 32 | primitive) keys are radix-sorted;
+// the hierarchy over the sorted keys follows Karras, "Maximizing parallelism in the
+// construction of BVHs, octrees, and k-d trees" (HPG 2012): internal node i covers the
+// key range found from the longest common prefixes around i and splits where the
+// prefix changes; boxes are formed bottom-up, the second child to arrive at a node
+// forming its box.  The result is written straight into the traversal's records: pair
+// record i for internal node i (both child boxes and references), one primitive per
+// leaf in sorted order with its end-of-leaf flag.  The tree differs from the host SAH
+// tree, so queries on it give the reference's answers up to FP32 distance ties.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <vector>
+
+#include "gpu_build.cuh"
+
+namespace gqd {
+
+namespace {
+
+constexpr int kBlock = 256;
+
+inline dim3 grid_of(int64_t n) { return dim3((unsigned)((n + kBlock - 1) / kBlock)); }
+
+__device__ __forceinline__ void atomic_min_f(float *a, float v) {
+    if (v >= 0.f)
+        atomicMin(reinterpret_cast<int *>(a), __float_as_int(v));
+    else
+        atomicMax(reinterpret_cast<unsigned *>(a), __float_as_uint(v));
+}
+__device__ __forceinline__ void atomic_max_f(float *a, float v) {
+    if (v >= 0.f)
+        atomicMax(reinterpret_cast<int *>(a), __float_as_int(v));
+    else
+        atomicMin(reinterpret_cast<unsigned *>(a), __float_as_uint(v));
+}
+
+template <int D>
+__device__ __forceinline__ void prim_box(const float *v, const int32_t *idx, int64_t p, float *lo, float *hi) {
+#pragma unroll
+    for (int k = 0; k < D; ++k) lo[k] = __int_as_float(0x7f800000), hi[k] = -__int_as_float(0x7f800000);
+#pragma unroll
+    for (int c = 0; c < D; ++c) {
+        const int64_t vi = idx[p * D + c];
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+            const float x = v[vi * D + k];
+            lo[k] = fminf(lo[k], x);
+            hi[k] = fmaxf(hi[k], x);
+        }
+    }
+}
+
+// centroid bounds: bounds[0..D) min, bounds[3..3+D) max
+template <int D>
+__global__ void k_centroid_bounds(const float *v, const int32_t *idx, int64_t n, float *bounds) {
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    float c[D];
+    if (p < n) {
+        float lo[D], hi[D];
+        prim_box<D>(v, idx, p, lo, hi);
+#pragma unroll
+        for (int k = 0; k < D; ++k) c[k] = 0.5f * (lo[k] + hi[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        float mn = p < n ? c[k] : __int_as_float(0x7f800000), mx = p < n ? c[k] : -__int_as_float(0x7f800000);
+        for (int o = 16; o > 0; o >>= 1) {
+            mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+            mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomic_min_f(&bounds[k], mn);
+            atomic_max_f(&bounds[3 + k], mx);
+        }
+    }
+}
+
+__device__ __forceinline__ uint32_t spread3(uint32_t v) {
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+__device__ __forceinline__ uint32_t spread2(uint32_t v) {
+    v &= 0x7fffu;
+    v = (v | (v << 8)) & 0x00ff00ffu;
+    v = (v | (v << 4)) & 0x0f0f0f0fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    v = (v | (v << 1)) & 0x55555555u;
+    return v;
+}
+
+template <int D>
+__global__ void k_keys(const float *v, const int32_t *idx, int64_t n, const float *bounds, uint64_t *keys,
+                       int32_t *vals) {
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    float lo[D], hi[D];
+    prim_box<D>(v, idx, p, lo, hi);
+    uint32_t q[D];
+    const float cells = D == 3 ? 1024.f : 32768.f;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        const float ext = bounds[3 + k] - bounds[k];
+        const float f = ext > 0.f ? (0.5f * (lo[k] + hi[k]) - bounds[k]) * (cells / ext) : 0.f;
+        q[k] = (uint32_t)fminf(fmaxf(f, 0.f), cells - 1.f);
+    }
+    const uint32_t code = D == 3 ? ((spread3(q[0]) << 2) | (spread3(q[1]) << 1) | spread3(q[D - 1]))
+                                 : ((spread2(q[0]) << 1) | spread2(q[D - 1]));
+    keys[p] = ((uint64_t)code << 32) | (uint64_t)p;
+    vals[p] = (int32_t)p;
+}
+
+__device__ __forceinline__ int delta(const uint64_t *k, int64_t n, int64_t i, int64_t j) {
+    if (j < 0 || j >= n) return -1;
+    return __clzll(k[i] ^ k[j]);  // keys are unique (primitive index in the low bits)
+}
+
+// Karras 2012, internal node i of n - 1; child references: internal >= 0, leaf = ~slot.
+__global__ void k_hierarchy(const uint64_t *k, int64_t n, int2 *child, int32_t *parent_int, int32_t *parent_leaf) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    const int d = (delta(k, n, i, i + 1) - delta(k, n, i, i - 1)) >= 0 ? 1 : -1;
+    const int dmin = delta(k, n, i, i - d);
+    int64_t lmax = 2;
+    while (delta(k, n, i, i + lmax * d) > dmin) lmax *= 2;
+    int64_t l = 0;
+    for (int64_t t = lmax / 2; t >= 1; t /= 2)
+        if (delta(k, n, i, i + (l + t) * d) > dmin) l += t;
+    const int64_t j = i + l * d;
+    const int dnode = delta(k, n, i, j);
+    int64_t s = 0, t = l;
+    do {
+        t = (t + 1) / 2;
+        if (delta(k, n, i, i + (s + t) * d) > dnode) s += t;
+    } while (t > 1);
+    const int64_t gamma = i + s * d + min(d, 0);
+    const int64_t lo = min(i, j), hi = max(i, j);
+    const int left = lo == gamma ? ~(int)gamma : (int)gamma;
+    const int right = hi == gamma + 1 ? ~(int)(gamma + 1) : (int)(gamma + 1);
+    child[i] = make_int2(left, right);
+    if (left < 0)
+        parent_leaf[~left] = (int32_t)i;
+    else
+        parent_int[left] = (int32_t)i;
+    if (right < 0)
+        parent_leaf[~right] = (int32_t)i;
+    else
+        parent_int[right] = (int32_t)i;
+}
+
+template <int D>
+struct NodeBox {
+    float lo[D], hi[D];
+};
+
+// Leaf records in sorted order (one primitive per leaf) and their boxes.
+template <int D>
+__global__ void k_leaves(const float *v, const int32_t *idx, int64_t n, const int32_t *order, void *prims,
+                         NodeBox<D> *leafbox) {
+    const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int64_t p = order[s];
+    NodeBox<D> b;
+    prim_box<D>(v, idx, p, b.lo, b.hi);
+    leafbox[s] = b;
+    if (D == 3) {
+        gq_tri_t r{};
+        const int64_t a = idx[p * 3], bb = idx[p * 3 + 1], c = idx[p * 3 + 2];
+        r.ax = v[a * 3]; r.ay = v[a * 3 + 1]; r.az = v[a * 3 + 2];
+        r.bx = v[bb * 3]; r.by = v[bb * 3 + 1]; r.bz = v[bb * 3 + 2];
+        r.cx = v[c * 3]; r.cy = v[c * 3 + 1]; r.cz = v[c * 3 + 2];
+        r.index = (int32_t)(float)p;  // as the host flattening stores it
+        r.flags = GQ_ITEM_LAST;
+        static_cast<gq_tri_t *>(prims)[s] = r;
+    } else {
+        gq_seg_t r{};
+        const int64_t a = idx[p * 2], bb = idx[p * 2 + 1];
+        r.ax = v[a * 2]; r.ay = v[a * 2 + 1];
+        r.bx = v[bb * 2]; r.by = v[bb * 2 + 1];
+        r.index = (int32_t)(float)p;
+        r.flags = GQ_ITEM_LAST;
+        static_cast<gq_seg_t *>(prims)[s] = r;
+    }
+}
+
+template <int D>
+__device__ __forceinline__ NodeBox<D> box_of(int ref, const NodeBox<D> *leafbox, const NodeBox<D> *nodebox) {
+    if (ref < 0) return leafbox[~ref];
+    NodeBox<D> b;
+    const volatile float *q = reinterpret_cast<const volatile float *>(nodebox + ref);
+#pragma unroll
+    for (int k = 0; k < D; ++k) b.lo[k] = q[k], b.hi[k] = q[D + k];
+    return b;
+}
+
+// Bottom-up boxes: the second child to reach a node forms its box and its pair record.
+template <int D>
+__global__ void k_boxes(int64_t n, const int2 *child, const int32_t *parent_int, const int32_t *parent_leaf,
+                        const NodeBox<D> *leafbox, NodeBox<D> *nodebox, int32_t *arrivals, void *pairs,
+                        int32_t *max_depth) {
+    const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    // depth of this leaf: internal ancestors up to the root
+    int depth = 0;
+    for (int32_t q = parent_leaf[s]; q >= 0; q = parent_int[q]) ++depth;
+    atomicMax(max_depth, depth);
+    int32_t node = parent_leaf[s];
+    while (node >= 0) {
+        __threadfence();
+        if (atomicAdd(&arrivals[node], 1) == 0) return;  // the other child forms this node
+        const int2 c = child[node];
+        const NodeBox<D> l = box_of<D>(c.x, leafbox, nodebox), r = box_of<D>(c.y, leafbox, nodebox);
+        NodeBox<D> u;
+#pragma unroll
+        for (int k = 0; k < D; ++k) u.lo[k] = fminf(l.lo[k], r.lo[k]), u.hi[k] = fmaxf(l.hi[k], r.hi[k]);
+        volatile float *q = reinterpret_cast<volatile float *>(nodebox + node);
+#pragma unroll
+        for (int k = 0; k < D; ++k) q[k] = u.lo[k], q[D + k] = u.hi[k];
+        if (D == 3) {
+            gq_pair3_t p{};
+            p.l_lox = l.lo[0]; p.l_loy = l.lo[1]; p.l_loz = l.lo[D - 1];
+            p.l_hix = l.hi[0]; p.l_hiy = l.hi[1]; p.l_hiz = l.hi[D - 1];
+            p.r_lox = r.lo[0]; p.r_loy = r.lo[1]; p.r_loz = r.lo[D - 1];
+            p.r_hix = r.hi[0]; p.r_hiy = r.hi[1]; p.r_hiz = r.hi[D - 1];
+            p.ref_l = c.x;
+            p.ref_r = c.y;
+            static_cast<gq_pair3_t *>(pairs)[node] = p;
+        } else {
+            gq_pair2_t p{};
+            p.l_lox = l.lo[0]; p.l_loy = l.lo[D - 1]; p.l_hix = l.hi[0]; p.l_hiy = l.hi[D - 1];
+            p.r_lox = r.lo[0]; p.r_loy = r.lo[D - 1]; p.r_hix = r.hi[0]; p.r_hiy = r.hi[D - 1];
+            p.ref_l = c.x;
+            p.ref_r = c.y;
+            static_cast<gq_pair2_t *>(pairs)[node] = p;
+        }
+        node = parent_int[node];
+    }
+}
+
+template <int D>
+cudaError_t build(const float *v, const int32_t *idx, int64_t n, void *pairs, void *prims, GpuBuildResult &res,
+                  cudaStream_t st) {
+    cudaError_t e = cudaSuccess;
+    std::vector<void *> tmp;
+    auto grab = [&](size_t bytes) -> void * {
+        void *p = nullptr;
+        if (e == cudaSuccess) e = cudaMallocAsync(&p, std::max<size_t>(bytes, 256), st);
+        if (e == cudaSuccess) tmp.push_back(p);
+        return p;
+    };
+    float *bounds = (float *)grab(6 * sizeof(float));
+    uint64_t *k_in = (uint64_t *)grab((size_t)n * 8), *k_out = (uint64_t *)grab((size_t)n * 8);
+    int32_t *v_in = (int32_t *)grab((size_t)n * 4), *order = (int32_t *)grab((size_t)n * 4);
+    int2 *child = (int2 *)grab((size_t)n * sizeof(int2));
+    int32_t *parent_int = (int32_t *)grab((size_t)n * 4), *parent_leaf = (int32_t *)grab((size_t)n * 4);
+    int32_t *arrivals = (int32_t *)grab((size_t)n * 4), *depth = (int32_t *)grab(4);
+    NodeBox<D> *leafbox = (NodeBox<D> *)grab((size_t)n * sizeof(NodeBox<D>));
+    NodeBox<D> *nodebox = (NodeBox<D> *)grab((size_t)n * sizeof(NodeBox<D>));
+    size_t tb = 0;
+    if (e == cudaSuccess)
+        e = cub::DeviceRadixSort::SortPairs(nullptr, tb, k_in, k_out, v_in, order, (int)n, 0, 64, st);
+    void *temp = grab(tb);
+    if (e == cudaSuccess) {
+        const float init[6] = {__builtin_inff(), __builtin_inff(), __builtin_inff(), -__builtin_inff(),
+                               -__builtin_inff(), -__builtin_inff()};
+        e = cudaMemcpyAsync(bounds, init, sizeof init, cudaMemcpyHostToDevice, st);
+    }
+    if (e == cudaSuccess) e = cudaMemsetAsync(parent_int, 0xff, (size_t)n * 4, st);  // root's parent = -1
+    if (e == cudaSuccess) e = cudaMemsetAsync(arrivals, 0, (size_t)n * 4, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(depth, 0, 4, st);
+    if (e == cudaSuccess) {
+        k_centroid_bounds<D><<<grid_of(n), kBlock, 0, st>>>(v, idx, n, bounds);
+        k_keys<D><<<grid_of(n), kBlock, 0, st>>>(v, idx, n, bounds, k_in, v_in);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortPairs(temp, tb, k_in, k_out, v_in, order, (int)n, 0, 64, st);
+    if (e == cudaSuccess) {
+        if (n == 1) {
+            int32_t minus1 = -1;
+            e = cudaMemcpyAsync(parent_leaf, &minus1, 4, cudaMemcpyHostToDevice, st);
+        } else {
+            k_hierarchy<<<grid_of(n - 1), kBlock, 0, st>>>(k_out, n, child, parent_int, parent_leaf);
+        }
+    }
+    if (e == cudaSuccess) {
+        k_leaves<D><<<grid_of(n), kBlock, 0, st>>>(v, idx, n, order, prims, leafbox);
+        k_boxes<D><<<grid_of(n), kBlock, 0, st>>>(n, child, parent_int, parent_leaf, leafbox, nodebox, arrivals, pairs,
+                                                  depth);
+        e = cudaGetLastError();
+    }
+    NodeBox<D> root{};
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(&root, n == 1 ? (const void *)leafbox : (const void *)nodebox, sizeof root,
+                            cudaMemcpyDeviceToHost, st);
+    int32_t dmax = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&dmax, depth, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    for (void *p : tmp) cudaFreeAsync(p, st);
+    cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return e;
+    for (int k = 0; k < 3; ++k) {
+        res.root_lo[k] = k < D ? root.lo[k] : 0.f;
+        res.root_hi[k] = k < D ? root.hi[k] : 0.f;
+    }
+    res.root_ref = n == 1 ? ~0 : 0;
+    res.max_depth = dmax;
+    return cudaSuccess;
+}
+
+}  // namespace
+
+cudaError_t gpu_build_bvh(int dim, const float *verts, const int32_t *index, int64_t n_prims, void *pairs,
+                          void *prims, GpuBuildResult &res, cudaStream_t st) {
+    if (n_prims <= 0) return cudaErrorInvalidValue;
+    return dim == 3 ? build<3>(verts, index, n_prims, pairs, prims, res, st)
+                    : build<2>(verts, index, n_prims, pairs, prims, res, st);
+}
+
+}  // namespace gqd

@@ -60,6 +60,7 @@ struct gq_scene {
     int max_depth = 0;
     // host trees (reference arrays): absent in a loaded scene until first asked for
     bool trees_ready = true;
+    bool gpu_built = false;  // tree built on the device: no host SAH trees to describe it
     std::mutex tree_mu;
 
     ~gq_scene() {

@@ -77,6 +77,8 @@ typedef struct {
     int32_t build_snch;        /* also build silhouettes and normal cones */
     int32_t build_wide;        /* also build the quantised 8-wide BVH */
     int32_t device;            /* CUDA device that holds the scene */
+    int32_t gpu_build;         /* build a linear BVH on the device instead (milliseconds; no SNCH, no wide
+                                  nodes, no reference arrays; answers equal up to FP32 ties) */
 } gq_build_opts;
 
 typedef struct {

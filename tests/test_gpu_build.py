@@ -1,0 +1,64 @@
+"""Linear BVH built on the device: queries on it give the host-built scene's answers
+(same validity and distances, same primitive except at FP32 ties), for every variant
+that runs without the SNCH or wide nodes."""
+import time
+
+import numpy as np
+import pytest
+
+from gquery_b200 import _lib as L
+from gquery_b200 import workloads as W
+from gquery_b200.scene import Scene
+from parity import REL_TOL, tie_report, to_np
+
+pytestmark = pytest.mark.gpu
+
+
+def _check(a, b, what):
+    rep = tie_report(to_np(a), to_np(b))
+    assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0 and rep["max_rel_d"] <= REL_TOL, (what, rep)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_device_build_matches_host_build(dim):
+    if dim == 2:
+        v, f = W.star_polyline(20000, seed=2)
+    else:
+        v, f = W.icosphere(6, amplitude=0.2, seed=5)
+    host = Scene(v, f, dim, device=0, build_snch=False)
+    t0 = time.perf_counter()
+    dev = Scene(v, f, dim, device=0, gpu_build=True)
+    assert time.perf_counter() - t0 < 30.0
+    assert dev.info["n_nodes"] == 2 * f.shape[0] - 1 and dev.info["n_wide_nodes"] == 0
+    assert 1 <= dev.info["max_depth"] <= 64
+    q = W.uniform_points(50000, dim, seed=3)
+    o, d = W.rays(50000, dim, seed=4)
+    ref_cp = host.closest_point(q, variant="exact")
+    ref_ray = host.intersect(o, d, variant="exact")
+    for variant in ("exact", "coherent", "auto"):
+        _check(ref_cp, dev.closest_point(q, variant=variant), f"cp {variant}")
+    _check(ref_ray, dev.intersect(o, d, variant="exact"), "ray exact")
+    _check(host.intersect(o, d, 0.7, variant="exact"), dev.intersect(o, d, 0.7, variant="auto"), "ray r_max")
+    assert dev.device_error() == 0
+
+
+def test_device_build_limits_and_files(tmp_path):
+    v, f = W.icosphere(3, seed=1)
+    dev = Scene(v, f, 3, device=0, gpu_build=True)
+    with pytest.raises(L.GQError, match="built on the device"):
+        dev.ref_array(L.ARRAY_BVH_NODES)
+    with pytest.raises(L.GQError, match="wide"):
+        dev.closest_point(W.uniform_points(10, 3, seed=0), variant="wide8")
+    path = tmp_path / "dev.gqs"
+    dev.save(path)
+    back = Scene.load(path, device=0)
+    q = W.uniform_points(5000, 3, seed=9)
+    a, b = to_np(dev.closest_point(q, variant="exact")), to_np(back.closest_point(q, variant="exact"))
+    for k in ("valid", "d", "prim_id"):
+        assert np.array_equal(np.asarray(a[k]), np.asarray(b[k]))
+    with pytest.raises(L.GQError, match="built on the device"):
+        back.ref_array(L.ARRAY_PRIMITIVES)
+    one = Scene(np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32), np.array([[0, 1, 2]], np.int32), 3,
+                device=0, gpu_build=True)
+    r = to_np(one.closest_point(np.array([[0.2, 0.2, 1.0]], np.float32), variant="exact"))
+    assert r["valid"][0] and abs(float(r["d"][0]) - 1.0) < 1e-6
