@@ -131,6 +131,8 @@ SIGNATURES = {
     "gq_scene_ref_array": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]),
     "gq_flat_silhouette_edges": (C.c_int32, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
                                              C.POINTER(C.c_int64)]),
+    "gq_flat_silhouette_edges_device": (C.c_int32, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p,
+                                                    C.c_int64, C.POINTER(C.c_int64), C.c_int32, C.c_void_p]),
     "gq_query_scratch_bytes": (C.c_int64, [C.c_int64]),
     "gq_order_scratch_bytes": (C.c_int64, [C.c_int64]),
     "gq_query_order": (C.c_int32, [C.c_void_p, Vecs, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),

@@ -244,7 +244,7 @@ void default_tuning(gq_scene *s) {
         s->tune[GQ_KIND_CLOSEST_POINT] = gq_tuning{GQ_VARIANT_COHERENT, 1, 1, 0, 32};
         s->tune[GQ_KIND_INTERSECT] = gq_tuning{s->has_wide ? GQ_VARIANT_WIDE8 : GQ_VARIANT_EXACT, 0, 1, 1, 32};
     } else {
-        s->tune[GQ_KIND_CLOSEST_POINT] = gq_tuning{s->has_wide ? GQ_VARIANT_WIDE8 : GQ_VARIANT_EXACT, 0, 1, 1, 32};
+        s->tune[GQ_KIND_CLOSEST_POINT] = gq_tuning{GQ_VARIANT_COHERENT, 1, 1, 0, 32};
         s->tune[GQ_KIND_INTERSECT] = gq_tuning{s->has_wide ? GQ_VARIANT_WIDE8 : GQ_VARIANT_EXACT, 0, 1, 1, 32};
     }
 }
@@ -491,6 +491,24 @@ gq_status gq_flat_silhouette_edges(const float *vertices, int64_t nv, const int3
     std::vector<float> v = ref_silhouette_data<3>(tmp, false);
     *len = (int64_t)v.size();
     if (dst && cap > 0) std::memcpy(dst, v.data(), sizeof(float) * (size_t)std::min<int64_t>(cap, *len));
+    return GQ_OK;
+}
+
+gq_status gq_flat_silhouette_edges_device(const float *vertices, int64_t nv, const int32_t *faces, int64_t nf,
+                                          float *dst, int64_t cap, int64_t *len, int32_t device, void *stream) {
+    if (!len || (nf > 0 && (!vertices || !faces))) return fail(GQ_ERR_INVALID, "null argument");
+    if (nv < 0 || nf < 0 || nf > (int64_t)(INT32_MAX / 3)) return fail(GQ_ERR_INVALID, "bad vertex or face count");
+    DeviceGuard g(device);
+    if (!g.ok) return fail(GQ_ERR_CUDA, "cannot select the device");
+    int64_t n_edges = 0;
+    int bad = 0;
+    const int64_t cap_edges = dst ? cap / 19 : 0;
+    cudaError_t e = gqd::gpu_silhouette_edges(vertices, nv, faces, nf, dst, cap_edges, &n_edges, &bad,
+                                              (cudaStream_t)stream);
+    if (e != cudaSuccess) return fail_cuda(e, "device silhouette edges");
+    if (bad) return fail(GQ_ERR_INVALID, "face index out of range");
+    *len = n_edges * 19;
+    if (dst && cap_edges < n_edges) return fail(GQ_ERR_INVALID, "destination holds fewer floats than *len");
     return GQ_OK;
 }
 

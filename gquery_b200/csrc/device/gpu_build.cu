@@ -313,6 +313,87 @@ cudaError_t build(const float *v, const int32_t *idx, int64_t n, void *pairs, vo
     return cudaSuccess;
 }
 
+// ---- silhouette edges on the device (build_flat_silhouette_edges) ----
+
+__global__ void k_check_faces(const int32_t *faces, int64_t nf, int64_t nv, int32_t *bad) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < nf * 3 && (faces[i] < 0 || (int64_t)faces[i] >= nv)) atomicOr(bad, 1);
+}
+
+__global__ void k_half_edges(const int32_t *faces, int64_t nh, uint64_t *keys, uint32_t *vals) {
+    const int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (h >= nh) return;
+    const int64_t f = h / 3, k = h % 3;
+    uint64_t i0 = (uint32_t)faces[f * 3 + k], i1 = (uint32_t)faces[f * 3 + (k + 1) % 3];
+    if (i0 > i1) {
+        const uint64_t t = i0;
+        i0 = i1;
+        i1 = t;
+    }
+    keys[h] = (i0 << 32) | i1;
+    vals[h] = (uint32_t)h;
+}
+
+// head[i] = 1 where a run of equal keys starts
+__global__ void k_heads(const uint64_t *keys, int64_t nh, uint32_t *head) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < nh) head[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1u : 0u;
+}
+
+// per run g (its index = inclusive head scan - 1): start position and first half-edge
+__global__ void k_runs(const uint32_t *head, const uint32_t *run_of, const uint32_t *vals, int64_t nh,
+                       uint32_t *run_start, uint32_t *run_first, uint32_t *run_id) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= nh || !head[i]) return;
+    const uint32_t g = run_of[i] - 1;
+    run_start[g] = (uint32_t)i;
+    run_first[g] = vals[i];
+    run_id[g] = g;
+}
+
+// edge e (runs ordered by first appearance): replays its half-edges in face order with
+// the host's last-writer rule and writes the 19 floats of silhouette_data().
+__global__ void k_edges(const float *v, const int32_t *faces, const uint64_t *keys, const uint32_t *vals, int64_t nh,
+                        const uint32_t *run_start, const uint32_t *run_by_first, int64_t n_edges, float *out) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= n_edges) return;
+    const uint32_t g = run_by_first[e];
+    int64_t i = run_start[g];
+    const uint64_t key = keys[i];
+    float pv[4][3] = {};
+    uint64_t idx[4] = {0, 0, 0, 0}, face[2] = {0, 0};
+    for (; i < nh && keys[i] == key; ++i) {
+        const int64_t h = vals[i], f = h / 3, k = h % 3;
+        uint64_t i0 = (uint32_t)faces[f * 3 + k], i1 = (uint32_t)faces[f * 3 + (k + 1) % 3];
+        const uint64_t i2 = (uint32_t)faces[f * 3 + (k + 2) % 3];
+        const uint64_t o0 = i0, o1 = i1;
+        bool swapped = false;
+        if (i0 > i1) {
+            const uint64_t t = i0;
+            i0 = i1;
+            i1 = t;
+            swapped = true;
+        }
+        const int slot = swapped ? 3 : 0;
+        for (int c = 0; c < 3; ++c) {
+            pv[1][c] = v[o0 * 3 + c];
+            pv[2][c] = v[o1 * 3 + c];
+            pv[slot][c] = v[i2 * 3 + c];
+        }
+        idx[1] = i0;
+        idx[2] = i1;
+        idx[slot] = i2;
+        face[swapped ? 1 : 0] = (uint64_t)f;
+    }
+    float *r = out + e * 19;
+    for (int a = 0; a < 4; ++a)
+        for (int c = 0; c < 3; ++c) r[a * 3 + c] = pv[a][c];
+    for (int a = 0; a < 4; ++a) r[12 + a] = (float)idx[a];
+    r[16] = (float)face[0];
+    r[17] = (float)face[1];
+    r[18] = (float)(uint64_t)e;
+}
+
 }  // namespace
 
 cudaError_t gpu_build_bvh(int dim, const float *verts, const int32_t *index, int64_t n_prims, void *pairs,
@@ -320,6 +401,87 @@ cudaError_t gpu_build_bvh(int dim, const float *verts, const int32_t *index, int
     if (n_prims <= 0) return cudaErrorInvalidValue;
     return dim == 3 ? build<3>(verts, index, n_prims, pairs, prims, res, st)
                     : build<2>(verts, index, n_prims, pairs, prims, res, st);
+}
+
+cudaError_t gpu_silhouette_edges(const float *verts, int64_t nv, const int32_t *faces, int64_t nf, float *out,
+                                 int64_t cap_edges, int64_t *n_edges, int *bad_input, cudaStream_t st) {
+    *n_edges = 0;
+    *bad_input = 0;
+    if (nf <= 0) return cudaSuccess;
+    const int64_t nh = nf * 3;
+    cudaError_t e = cudaSuccess;
+    std::vector<void *> tmp;
+    auto grab = [&](size_t bytes) -> void * {
+        void *p = nullptr;
+        if (e == cudaSuccess) e = cudaMallocAsync(&p, std::max<size_t>(bytes, 256), st);
+        if (e == cudaSuccess) tmp.push_back(p);
+        return p;
+    };
+    auto done = [&](cudaError_t r) {
+        for (void *p : tmp) cudaFreeAsync(p, st);
+        cudaStreamSynchronize(st);
+        return r;
+    };
+    int32_t *bad = (int32_t *)grab(4);
+    if (e == cudaSuccess) e = cudaMemsetAsync(bad, 0, 4, st);
+    if (e == cudaSuccess) {
+        k_check_faces<<<grid_of(nh), kBlock, 0, st>>>(faces, nf, nv, bad);
+        e = cudaGetLastError();
+    }
+    int32_t hbad = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return done(e);
+    if (hbad) {
+        *bad_input = 1;
+        return done(cudaSuccess);
+    }
+    uint64_t *k_in = (uint64_t *)grab((size_t)nh * 8), *k_out = (uint64_t *)grab((size_t)nh * 8);
+    uint32_t *v_in = (uint32_t *)grab((size_t)nh * 4), *v_out = (uint32_t *)grab((size_t)nh * 4);
+    uint32_t *head = (uint32_t *)grab((size_t)nh * 4), *run_of = (uint32_t *)grab((size_t)nh * 4);
+    uint32_t *run_start = (uint32_t *)grab((size_t)nh * 4), *run_first = (uint32_t *)grab((size_t)nh * 4);
+    uint32_t *run_id = (uint32_t *)grab((size_t)nh * 4), *first_sorted = (uint32_t *)grab((size_t)nh * 4);
+    uint32_t *run_by_first = (uint32_t *)grab((size_t)nh * 4);
+    size_t tb_sort = 0, tb_scan = 0, tb_first = 0;
+    if (e == cudaSuccess)
+        e = cub::DeviceRadixSort::SortPairs(nullptr, tb_sort, k_in, k_out, v_in, v_out, (int)nh, 0, 64, st);
+    if (e == cudaSuccess) e = cub::DeviceScan::InclusiveSum(nullptr, tb_scan, head, run_of, (int)nh, st);
+    if (e == cudaSuccess)
+        e = cub::DeviceRadixSort::SortPairs(nullptr, tb_first, run_first, first_sorted, run_id, run_by_first, (int)nh, 0,
+                                            32, st);
+    void *temp = grab(std::max(tb_sort, std::max(tb_scan, tb_first)));
+    if (e == cudaSuccess) {
+        k_half_edges<<<grid_of(nh), kBlock, 0, st>>>(faces, nh, k_in, v_in);
+        e = cudaGetLastError();
+    }
+    size_t tb = tb_sort;
+    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortPairs(temp, tb, k_in, k_out, v_in, v_out, (int)nh, 0, 64, st);
+    if (e == cudaSuccess) {
+        k_heads<<<grid_of(nh), kBlock, 0, st>>>(k_out, nh, head);
+        e = cudaGetLastError();
+    }
+    tb = tb_scan;
+    if (e == cudaSuccess) e = cub::DeviceScan::InclusiveSum(temp, tb, head, run_of, (int)nh, st);
+    uint32_t runs = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&runs, run_of + nh - 1, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return done(e);
+    *n_edges = runs;
+    if (!out || cap_edges < (int64_t)runs) return done(cudaSuccess);  // size query, or too small
+    if (e == cudaSuccess) {
+        k_runs<<<grid_of(nh), kBlock, 0, st>>>(head, run_of, v_out, nh, run_start, run_first, run_id);
+        e = cudaGetLastError();
+    }
+    tb = tb_first;
+    // runs in order of first appearance (first half-edges are distinct)
+    if (e == cudaSuccess)
+        e = cub::DeviceRadixSort::SortPairs(temp, tb, run_first, first_sorted, run_id, run_by_first, (int)runs, 0, 32,
+                                            st);
+    if (e == cudaSuccess) {
+        k_edges<<<grid_of(runs), kBlock, 0, st>>>(verts, faces, k_out, v_out, nh, run_start, run_by_first, runs, out);
+        e = cudaGetLastError();
+    }
+    return done(e);
 }
 
 }  // namespace gqd

@@ -22,4 +22,12 @@ struct GpuBuildResult {
 cudaError_t gpu_build_bvh(int dim, const float *verts, const int32_t *index, int64_t n_prims, void *pairs,
                           void *prims, GpuBuildResult &res, cudaStream_t st);
 
+// Unique edges of a triangle mesh in the reference's flat layout (19 floats each, the
+// layout of build_flat_silhouette_edges / silhouette_data()), in order of first
+// appearance, on the device.  *n_edges receives the count; nothing is written unless
+// `out` holds cap_edges >= *n_edges records.  *bad_input = 1 (and nothing else done)
+// when a face index is outside [0, nv).  Synchronises `st`.
+cudaError_t gpu_silhouette_edges(const float *verts, int64_t nv, const int32_t *faces, int64_t nf, float *out,
+                                 int64_t cap_edges, int64_t *n_edges, int *bad_input, cudaStream_t st);
+
 }  // namespace gqd

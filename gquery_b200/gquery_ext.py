@@ -79,3 +79,27 @@ def build_flat_silhouette_edges(vertices, indices) -> np.ndarray:  # gquery.cpp:
     L.check(L.lib().gq_flat_silhouette_edges(v.ctypes.data, v.shape[0], f.ctypes.data, f.shape[0],
                                              out.ctypes.data, n.value, C.byref(n)))
     return out
+
+
+def build_flat_silhouette_edges_device(vertices, indices, *, device: int = 0):
+    """build_flat_silhouette_edges on the GPU: device torch tensors in ([V, 3] float32,
+    [F, 3] int32, or anything torch can move there), a device float32 tensor out with
+    the same values and order as the host function."""
+    import torch
+    dev = torch.device("cuda", device)
+    v = torch.as_tensor(vertices).to(dev, torch.float32).contiguous()
+    f = torch.as_tensor(indices).to(dev, torch.int32).contiguous()
+    if v.dim() != 2 or f.dim() != 2:
+        raise ValueError("vertices and indices must be 2-D")
+    if v.shape[1] != 3 and v.shape[0] == 3:
+        v = v.t().contiguous()
+    if f.shape[1] != 3 and f.shape[0] == 3:
+        f = f.t().contiguous()
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    n = C.c_int64()
+    L.check(L.lib().gq_flat_silhouette_edges_device(v.data_ptr(), v.shape[0], f.data_ptr(), f.shape[0], None, 0,
+                                                    C.byref(n), device, stream))
+    out = torch.empty(n.value, dtype=torch.float32, device=dev)
+    L.check(L.lib().gq_flat_silhouette_edges_device(v.data_ptr(), v.shape[0], f.data_ptr(), f.shape[0],
+                                                    out.data_ptr(), n.value, C.byref(n), device, stream))
+    return out

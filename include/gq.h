@@ -177,6 +177,13 @@ gq_status gq_scene_ref_array(const gq_scene *scene, int32_t which, float *dst, i
 gq_status gq_flat_silhouette_edges(const float *vertices, int64_t nv, const int32_t *faces, int64_t nf,
                                    float *dst, int64_t cap, int64_t *len);
 
+/* The same on the device: vertices [nv][3] float and faces [nf][3] int32 in device
+ * memory of `device`, the 19-float records written to device `dst` (cap floats; with
+ * dst = NULL only *len is set).  Ordered, valued and encoded exactly as
+ * gq_flat_silhouette_edges; synchronises `stream`. */
+gq_status gq_flat_silhouette_edges_device(const float *vertices, int64_t nv, const int32_t *faces, int64_t nf,
+                                          float *dst, int64_t cap, int64_t *len, int32_t device, void *stream);
+
 /* ---- queries ---- */
 /* Device scratch a query of n items needs when opts->scratch is supplied. */
 int64_t gq_query_scratch_bytes(int64_t n);

@@ -62,3 +62,27 @@ def test_device_build_limits_and_files(tmp_path):
                 device=0, gpu_build=True)
     r = to_np(one.closest_point(np.array([[0.2, 0.2, 1.0]], np.float32), variant="exact"))
     assert r["valid"][0] and abs(float(r["d"][0]) - 1.0) < 1e-6
+
+
+@pytest.mark.parametrize("level,amp", [(1, 0.0), (4, 0.3), (6, 0.15)])
+def test_device_silhouette_edges_equal_host(level, amp):
+    from gquery_b200.gquery_ext import build_flat_silhouette_edges, build_flat_silhouette_edges_device
+    v, f = W.icosphere(level, amplitude=amp, seed=level)
+    host = build_flat_silhouette_edges(v, f)
+    dev = build_flat_silhouette_edges_device(v, f).cpu().numpy()
+    assert host.shape == dev.shape
+    assert np.array_equal(host.view(np.uint32), dev.view(np.uint32))
+
+
+def test_device_silhouette_edges_open_and_bad_meshes():
+    import torch
+    from gquery_b200.gquery_ext import build_flat_silhouette_edges, build_flat_silhouette_edges_device
+    v, f = W.icosphere(2, seed=1)
+    f_open = f[: len(f) // 2]  # boundary edges and unused vertices
+    assert np.array_equal(build_flat_silhouette_edges(v, f_open).view(np.uint32),
+                          build_flat_silhouette_edges_device(v, f_open).cpu().numpy().view(np.uint32))
+    bad = f.copy()
+    bad[5, 1] = len(v) + 7
+    with pytest.raises(L.GQError, match="out of range"):
+        build_flat_silhouette_edges_device(v, bad)
+    assert build_flat_silhouette_edges_device(v, f[:0]).numel() == 0
