@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--c2-n", type=int, default=1 << 22, help="silhouette queries (c2)")
     ap.add_argument("--c3-total", type=int, default=1 << 24, help="queries per batched step (c3)")
     ap.add_argument("--c4-requests", type=int, default=240, help="requests per serving trace (c4)")
+    ap.add_argument("--c3-quick", action="store_true",
+                    help="c3: batched launch only (no variant tuning, no per-scene comparison)")
     return ap.parse_args()
 
 
@@ -324,9 +326,12 @@ def section_c3(args, dev, flush):
             out = bb.alloc(*ns)
         bb.run(cp=(cp_pts, cp_ids), ray=(ray_o, ray_d, ray_ids), sil=(sil_pts, sil_ids), out=out)
     t_tune = time.perf_counter()
-    tb = tune_batch(make, step)
+    tb = {"best": dict(cp_variant="coherent", ray_variant="wide8", sil_variant="coherent"), "table": []} \
+        if args.c3_quick else tune_batch(make, step)
     tune_s = time.perf_counter() - t_tune
     b = SceneBatch(scenes, max(ns), **tb["best"])
+    if out is None:
+        out = b.alloc(*ns)
     eager_ms = dev_ms(lambda: b.run(cp=(cp_pts, cp_ids), ray=(ray_o, ray_d, ray_ids), sil=(sil_pts, sil_ids),
                                     out=out), steps=5, warmup=3, flush=flush)
     kind_ms = {k: dev_ms(lambda: b.run(out=out, **a), steps=3, warmup=1, flush=flush) for k, a in
@@ -356,9 +361,12 @@ def section_c3(args, dev, flush):
             a, z = bounds[2][i], bounds[2][i + 1]
             if z > a:
                 sc.closest_silhouette(sil_pts[a:z], variant=variant if variant == "exact" else "auto")
-    plain_ms = dev_ms(lambda: per_scene("exact"), steps=1, warmup=1, flush=flush)
-    tuned_ms = dev_ms(lambda: per_scene("auto"), steps=1, warmup=1, flush=flush)
-    mq = lambda ms: total / ms / 1e3  # noqa: E731
+    if args.c3_quick:
+        plain_ms = tuned_ms = None
+    else:
+        plain_ms = dev_ms(lambda: per_scene("exact"), steps=1, warmup=1, flush=flush)
+        tuned_ms = dev_ms(lambda: per_scene("auto"), steps=1, warmup=1, flush=flush)
+    mq = lambda ms: total / ms / 1e3 if ms else None  # noqa: E731
     return {"workload": f"512 star polylines, {sum(e.shape[0] for _, e in geo)} segments, {total} queries "
                         f"(cp {ns[0]}, ray {ns[1]}, sil {ns[2]})", "build_s": build_s,
             "batched_graph": {"ms": graph_ms, "mqueries_per_s": mq(graph_ms)},
@@ -366,7 +374,7 @@ def section_c3(args, dev, flush):
             "batched_kind_alone_ms": kind_ms,
             "plain_per_scene_exact": {"ms": plain_ms, "mqueries_per_s": mq(plain_ms), "launch_calls": 3 * len(scenes)},
             "per_scene_tuned": {"ms": tuned_ms, "mqueries_per_s": mq(tuned_ms)},
-            "batched_vs_plain": plain_ms / graph_ms,
+            "batched_vs_plain": plain_ms / graph_ms if plain_ms else None,
             "autotune": {"best": tb["best"], "seconds": tune_s,
                          "table_ms": {"/".join(t["choice"].values()): t["ms"] for t in tb["table"]}}}
 
