@@ -65,7 +65,7 @@ def parse():
                          "comma-separated or 'none' (one GPU only)")
     ap.add_argument("--c2-n", type=int, default=1 << 22, help="silhouette queries (c2)")
     ap.add_argument("--c3-total", type=int, default=1 << 24, help="queries per batched step (c3)")
-    ap.add_argument("--c4-requests", type=int, default=240, help="requests per serving trace (c4)")
+    ap.add_argument("--c4-requests", type=int, default=800, help="requests per serving trace (c4)")
     ap.add_argument("--c3-quick", action="store_true",
                     help="c3: batched launch only (no variant tuning, no per-scene comparison)")
     return ap.parse_args()
