@@ -219,3 +219,62 @@ def summarize(res: dict) -> dict:
             "mqueries_per_s": q / span / 1e6 if span > 0 else float("inf"),
             "requests_per_s": lat.size / span if span > 0 else float("inf"),
             "steps": int(np.unique(res["step"]).size)}
+
+
+# ---------------------------------------------------------------- several GPUs
+
+def place_scenes(scene_bytes: Sequence[int], budgets: Sequence[int]) -> List[int]:
+    """Scene affinity for serving on several GPUs: device index of every scene, chosen so
+    that each device's scenes fit its budget (largest scene first, onto the device with
+    the most room left; ties to the lower index).  Raises ValueError when a scene fits
+    on no device."""
+    room = [int(b) for b in budgets]
+    if not room:
+        raise ValueError("no devices")
+    place = [-1] * len(scene_bytes)
+    for i in sorted(range(len(scene_bytes)), key=lambda k: (-int(scene_bytes[k]), k)):
+        d = max(range(len(room)), key=lambda k: (room[k], -k))
+        if room[d] < int(scene_bytes[i]):
+            raise ValueError(f"scene {i} ({int(scene_bytes[i])} bytes) fits on no device")
+        room[d] -= int(scene_bytes[i])
+        place[i] = d
+    return place
+
+
+class Router:
+    """Requests to the GPU that holds their scene: one :class:`Server` per device over that
+    device's scenes (each scene built or loaded on its device, e.g. placed by
+    :func:`place_scenes`).  `scenes_by_device[d]` lists the global scene indices on
+    device d; requests name global scene indices."""
+
+    def __init__(self, scenes: Sequence[Scene], **server_kw):
+        by_dev: Dict[int, List[int]] = {}
+        for i, s in enumerate(scenes):
+            by_dev.setdefault(int(s.device), []).append(i)
+        self.route: Dict[int, tuple] = {}
+        self.servers: Dict[int, Server] = {}
+        for d, idx in sorted(by_dev.items()):
+            self.servers[d] = Server([scenes[i] for i in idx], **server_kw)
+            for local, g in enumerate(idx):
+                self.route[g] = (d, local)
+
+    def submit(self, req: HostRequest) -> tuple:
+        if req.scene not in self.route:
+            raise ValueError(f"scene index {req.scene} is not served")
+        d, local = self.route[req.scene]
+        global_scene = req.scene
+        req.scene = local
+        try:
+            return d, self.servers[d].submit(req)
+        finally:
+            req.scene = global_scene
+
+    def wait_idle(self, timeout: float = 120.0) -> List[HostRequest]:
+        done: List[HostRequest] = []
+        for srv in self.servers.values():
+            done += srv.wait_idle(timeout)
+        return done
+
+    def close(self):
+        for srv in self.servers.values():
+            srv.close()

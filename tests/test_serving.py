@@ -150,3 +150,19 @@ def test_summary_of_a_short_open_loop_run(scenes):
     s = summarize(res)
     assert s["requests"] == len(reqs) and s["p99_ms"] >= s["p50_ms"] > 0
     assert s["queries"] == sum(r.n for r in reqs)
+
+
+def test_router_sends_requests_to_their_scene(scenes):
+    from gquery_b200.serving import Router, place_scenes
+    assert place_scenes([s.info["device_bytes"] for s in scenes], [1 << 40]) == [0] * len(scenes)
+    router = Router(scenes, ring_queries=(1 << 15,) * 3, step_queries=1 << 13)
+    reqs = _requests(30, len(scenes), seed=11)
+    for r in reqs:
+        d, _ = router.submit(r)
+        assert d == 0
+    done = router.wait_idle(60.0)
+    assert len(done) == len(reqs) and all(r.completion["status"] == 0 for r in done)
+    _check_same_as_alone(scenes, reqs)
+    with pytest.raises(ValueError):
+        router.submit(HostRequest.make(len(scenes) + 1, "cp", np.zeros((4, 3), np.float32)))
+    router.close()

@@ -55,3 +55,18 @@ def test_summarize_percentiles_and_throughput():
     assert abs(s["p50_ms"] - 2.0) < 1e-9 and s["max_ms"] > 9.99
     assert abs(s["mqueries_per_s"] - 1e6 / 1.010 / 1e6) < 1e-9
     assert s["steps"] == 250
+
+
+def test_place_scenes_respects_budgets_and_balances():
+    from gquery_b200.serving import place_scenes
+    sizes = [50, 40, 30, 20, 10, 10]
+    place = place_scenes(sizes, [80, 100])
+    used = [sum(s for s, p in zip(sizes, place) if p == d) for d in range(2)]
+    assert used[0] <= 80 and used[1] <= 100 and sum(used) == sum(sizes)
+    assert place[0] != place[1]  # the two largest go to different devices
+    assert place_scenes([5, 5], [10]) == [0, 0]
+    import pytest
+    with pytest.raises(ValueError, match="fits on no device"):
+        place_scenes([60, 60], [50, 100])
+    with pytest.raises(ValueError):
+        place_scenes([1], [])
