@@ -62,7 +62,16 @@ GQ_HD float gq_div(float a, float b) {
     return a / b;
 #endif
 }
-GQ_HD float gq_clamp(float x, float lo, float hi) { return gq_max(gq_min(x, hi), lo); }
+// max(min(x, hi), lo): a NaN x gives hi (fminf returns the other operand).  On the
+// device a [0, 1] clamp may be folded into a saturate, which maps NaN to 0, so the NaN
+// case is spelled out there (t of a zero-length segment is 0/0).
+GQ_HD float gq_clamp(float x, float lo, float hi) {
+#if defined(__CUDA_ARCH__)
+    return x != x ? hi : gq_max(gq_min(x, hi), lo);
+#else
+    return gq_max(gq_min(x, hi), lo);
+#endif
+}
 
 GQ_HD float gq_dot2(float ax, float ay, float bx, float by) { return gq_fma(ay, by, ax * bx); }
 GQ_HD float gq_dot3(float ax, float ay, float az, float bx, float by, float bz) {
