@@ -695,6 +695,8 @@ struct SceneFileHeader {
     uint64_t image_bytes[6];
 };
 constexpr char kSceneMagic[8] = {'G', 'Q', 'S', 'C', 'E', 'N', 'E', '1'};
+// 2: 3D silhouette edges carry the pre-test spans (gq_sile_t.span0 / span1)
+constexpr int32_t kSceneFileVersion = 2;
 
 struct File {
     FILE *f = nullptr;
@@ -710,7 +712,7 @@ gq_status gq_scene_save(const gq_scene *s, const char *path) {
     if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "only scenes with a device copy can be saved");
     SceneFileHeader h{};
     std::memcpy(h.magic, kSceneMagic, 8);
-    h.version = 1;
+    h.version = kSceneFileVersion;
     h.dim = s->dim;
     h.nv = s->nv;
     h.np = s->np;
@@ -759,7 +761,7 @@ gq_status gq_scene_load(const char *path, int32_t device, gq_scene **out) {
     in.f = std::fopen(path, "rb");
     if (!in.f) return fail(GQ_ERR_INVALID, std::string("cannot open ") + path);
     SceneFileHeader h{};
-    if (std::fread(&h, sizeof h, 1, in.f) != 1 || std::memcmp(h.magic, kSceneMagic, 8) != 0 || h.version != 1 ||
+    if (std::fread(&h, sizeof h, 1, in.f) != 1 || std::memcmp(h.magic, kSceneMagic, 8) != 0 || h.version != kSceneFileVersion ||
         (h.dim != 2 && h.dim != 3) || h.nv < 0 || h.np < 0)
         return fail(GQ_ERR_INVALID, std::string(path) + " is not a saved scene of this version");
     std::unique_ptr<gq_scene> s(new (std::nothrow) gq_scene());

@@ -11,6 +11,7 @@
 // computed on the host with the same FP32 operations the reference applies per test.
 #pragma once
 
+#include "../sil_filter.h"
 #include "prim.cuh"
 #include "queries.cuh"
 
@@ -74,32 +75,41 @@ __device__ __forceinline__ bool test_silhouette(const DevScene &s, Lane<D> &L, i
         pid = fbits(r1.z);
         p[0] = r0.z;
         p[D - 1] = r0.w;
-        d = gq_norm2(x[0] - r0.z, x[D - 1] - r0.w);
-        if ((flags & GQ_ITEM_VALID) && (d < L.r)) {
+        // the reference tests d < r_max first; the silhouette test is independent of
+        // d, so it goes first here and the square root only follows for silhouettes
+        if (flags & GQ_ITEM_VALID) {
             const float c0 = (r0.z - r0.x) * (x[D - 1] - r0.y) - (r0.w - r0.y) * (x[0] - r0.x);
             const float c1 = (r1.x - r0.z) * (x[D - 1] - r0.w) - (r1.y - r0.w) * (x[0] - r0.z);
             ok = c0 * c1 < 0.f;
+            if (ok) d = gq_norm2(x[0] - r0.z, x[D - 1] - r0.w);
         }
     } else {
         const float4 r0 = ldg4(s.sils, 4 * (int64_t)j), r1 = ldg4(s.sils, 4 * (int64_t)j + 1);
-        const float4 r3 = ldg4(s.sils, 4 * (int64_t)j + 3);
+        const float4 r2 = ldg4(s.sils, 4 * (int64_t)j + 2), r3 = ldg4(s.sils, 4 * (int64_t)j + 3);
         const int flags = fbits(r3.y);
         last = flags & GQ_ITEM_LAST;
         pid = fbits(r3.x);
-        float qx, qy, qz;
-        d = seg_dist3(x[0], x[1], x[D - 1], r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, qx, qy, qz);
-        p[0] = qx;
-        p[1] = qy;
-        p[D - 1] = qz;
-        if (d < L.r) {
-            ok = flags & GQ_ITEM_VALID;  // boundary edge: always a silhouette
-            if (!ok) {
-                // is_silhouette_edge (silhouette_edge.py:7-12) with the stored face normals
-                const float4 r2 = ldg4(s.sils, 4 * (int64_t)j + 2);
-                const float wx = qx - x[0], wy = qy - x[1], wz = qz - x[D - 1];
-                const float dot0 = gq_dot3(wx, wy, wz, r1.z, r1.w, r2.x);
-                const float dot1 = gq_dot3(wx, wy, wz, r2.y, r2.z, r2.w);
-                ok = dot0 * dot1 < 0.f;
+        // pre-test (sil_filter.h): skips only edges that are certainly no silhouette
+        const bool skip = ((flags & (GQ_ITEM_VALID | GQ_SIL_FILTER)) == GQ_SIL_FILTER) &&
+                          sil_edge_excluded(r0.x, r0.y, r0.z, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w, r3.z, r3.w, x[0],
+                                            x[1], x[D - 1],
+                                            sil_margin(fmaxf(fmaxf(fabsf(x[0]), fabsf(x[1])), fabsf(x[D - 1])),
+                                                       s.coord_bound));
+        if (!skip) {
+            float qx, qy, qz;
+            d = seg_dist3(x[0], x[1], x[D - 1], r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, qx, qy, qz);
+            p[0] = qx;
+            p[1] = qy;
+            p[D - 1] = qz;
+            if (d < L.r) {
+                ok = flags & GQ_ITEM_VALID;  // boundary edge: always a silhouette
+                if (!ok) {
+                    // is_silhouette_edge (silhouette_edge.py:7-12) with the stored face normals
+                    const float wx = qx - x[0], wy = qy - x[1], wz = qz - x[D - 1];
+                    const float dot0 = gq_dot3(wx, wy, wz, r1.z, r1.w, r2.x);
+                    const float dot1 = gq_dot3(wx, wy, wz, r2.y, r2.z, r2.w);
+                    ok = dot0 * dot1 < 0.f;
+                }
             }
         }
     }

@@ -5,23 +5,11 @@
 #include <cstring>
 
 #include "../gq_fmath.h"
+#include "../sil_filter.h"
 
 namespace gqb {
 
 namespace {
-
-// normalize(cross(u, v)) with the FP32 operations of the device's per-edge test
-// (cross in fused form, normalize = v * (1 / sqrt(dot(v, v)))), so the stored normal
-// is bit-identical to the one the traversal would compute.
-void face_normal(float ux, float uy, float uz, float vx, float vy, float vz, float &nx, float &ny, float &nz) {
-    const float cx = gq_fma(uy, vz, -(uz * vy));
-    const float cy = gq_fma(uz, vx, -(ux * vz));
-    const float cz = gq_fma(ux, vy, -(uy * vx));
-    const float inv = gq_rsqrt(gq_dot3(cx, cy, cz, cx, cy, cz));
-    nx = cx * inv;
-    ny = cy * inv;
-    nz = cz * inv;
-}
 
 // Preorder rank of every interior node (the index of its pair record), -1 for leaves.
 template <int D>
@@ -367,12 +355,19 @@ void flatten_snch(const BvhTree<D> &t, const SnchTree<D> &s, DeviceImage<D> &img
             const float cx = x.v[0].v[0], cy = x.v[0].v[1], cz = x.v[0].v[2];
             const float dx = x.v[3].v[0], dy = x.v[3].v[1], dz = x.v[3].v[2];
             // n0 = normalize(cross(b - a, c - a)), n1 = normalize(cross(d - a, b - a))
-            face_normal(r.bx - r.ax, r.by - r.ay, r.bz - r.az, cx - r.ax, cy - r.ay, cz - r.az, r.n0x, r.n0y, r.n0z);
-            face_normal(dx - r.ax, dy - r.ay, dz - r.az, r.bx - r.ax, r.by - r.ay, r.bz - r.az, r.n1x, r.n1y, r.n1z);
+            sil_face_normal(r.bx - r.ax, r.by - r.ay, r.bz - r.az, cx - r.ax, cy - r.ay, cz - r.az, r.n0x, r.n0y,
+                            r.n0z);
+            sil_face_normal(dx - r.ax, dy - r.ay, dz - r.az, r.bx - r.ax, r.by - r.ay, r.bz - r.az, r.n1x, r.n1y,
+                            r.n1z);
             r.prim = (int32_t)(float)x.prim;
             // silhouette_edge.py:56-57: boundary marker index == -1 never occurs (size_t storage)
             const bool boundary = ((int64_t)(float)x.idx[0] == -1) || ((int64_t)(float)x.idx[3] == -1);
             r.flags = boundary ? GQ_ITEM_VALID : 0;  // for edges the bit means "always a silhouette"
+            // spans of the pre-test that skips edges which are certainly no silhouette
+            r.span0 = sil_span(r.n0x, r.n0y, r.n0z, r.ax, r.ay, r.az, r.bx, r.by, r.bz);
+            r.span1 = sil_span(r.n1x, r.n1y, r.n1z, r.ax, r.ay, r.az, r.bx, r.by, r.bz);
+            if (!boundary && sil_filter_usable(r.n0x, r.n0y, r.n0z, r.n1x, r.n1y, r.n1z, r.span0, r.span1))
+                r.flags |= GQ_SIL_FILTER;
         }
     }
     for (size_t i = 0; i < t.nodes.size(); ++i) {

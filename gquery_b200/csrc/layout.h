@@ -65,12 +65,15 @@ typedef struct {
 
 // 3D silhouette edge: end points a, b and the unit normals of its two faces,
 // n0 of (a, b, c) and n1 of (a, d, b), computed once on the host with the
-// FP32 operations the reference applies per test (silhouette_edge.py:28-34).   64 B
+// FP32 operations the reference applies per test (silhouette_edge.py:28-34), and
+// span0 = n0 . (b - a), span1 = n1 . (b - a) for the pre-test of sil_filter.h
+// (valid when flags has GQ_SIL_FILTER).                                       64 B
 typedef struct {
     float ax, ay, az, bx;
     float by, bz, n0x, n0y;
     float n0z, n1x, n1y, n1z;
-    int32_t prim, flags, pad0, pad1;
+    int32_t prim, flags;
+    float span0, span1;
 } gq_sile_t;
 
 // Binary BVH pair records.
