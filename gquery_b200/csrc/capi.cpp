@@ -134,7 +134,7 @@ gq_status build_scene(const float *vertices, int64_t nv, const int32_t *prims, i
         }
         if (o.build_snch) {
             SnchTree<D> sn = build_snch<D>(src, tree, nt);
-            flatten_snch<D>(tree, sn, img);
+            flatten_snch<D>(tree, sn, img, nt);
             s->has_snch = true;
             if constexpr (D == 2)
                 s->s2 = std::move(sn);
@@ -696,7 +696,8 @@ struct SceneFileHeader {
 };
 constexpr char kSceneMagic[8] = {'G', 'Q', 'S', 'C', 'E', 'N', 'E', '1'};
 // 2: 3D silhouette edges carry the pre-test spans (gq_sile_t.span0 / span1)
-constexpr int32_t kSceneFileVersion = 2;
+// 3: 3D SNCH pairs carry the node bounds of both children (gq_spair3_t.l_b / r_b)
+constexpr int32_t kSceneFileVersion = 3;
 
 struct File {
     FILE *f = nullptr;

@@ -81,33 +81,8 @@ __device__ __forceinline__ void closest_silhouette(const DevScene &s, unsigned m
             cur = kSilNone;
             continue;
         }
-        float lo[2][D], hi[2][D], ax[2][D], half[2], rad[2];
-        int refs[2];
-        if (D == 2) {
-            const float4 a0 = ldg4(s.spairs, 5 * (int64_t)cur), a1 = ldg4(s.spairs, 5 * (int64_t)cur + 1),
-                         a2 = ldg4(s.spairs, 5 * (int64_t)cur + 2), a3 = ldg4(s.spairs, 5 * (int64_t)cur + 3);
-            const int4 rr = __ldg(reinterpret_cast<const int4 *>(s.spairs) + 5 * (int64_t)cur + 4);
-            lo[0][0] = a0.x; lo[0][D - 1] = a0.y; hi[0][0] = a0.z; hi[0][D - 1] = a0.w;
-            ax[0][0] = a1.x; ax[0][D - 1] = a1.y; half[0] = a1.z; rad[0] = a1.w;
-            lo[1][0] = a2.x; lo[1][D - 1] = a2.y; hi[1][0] = a2.z; hi[1][D - 1] = a2.w;
-            ax[1][0] = a3.x; ax[1][D - 1] = a3.y; half[1] = a3.z; rad[1] = a3.w;
-            refs[0] = rr.x;
-            refs[1] = rr.y;
-        } else {
-            const int64_t b = 6 * (int64_t)cur;
-            const float4 f0 = ldg4(s.spairs, b), f1 = ldg4(s.spairs, b + 1), f2 = ldg4(s.spairs, b + 2),
-                         f3 = ldg4(s.spairs, b + 3), f4 = ldg4(s.spairs, b + 4), f5 = ldg4(s.spairs, b + 5);
-            lo[0][0] = f0.x; lo[0][1] = f0.y; lo[0][D - 1] = f0.z;
-            hi[0][0] = f0.w; hi[0][1] = f1.x; hi[0][D - 1] = f1.y;
-            ax[0][0] = f1.z; ax[0][1] = f1.w; ax[0][D - 1] = f2.x;
-            half[0] = f2.y; rad[0] = f2.z;
-            lo[1][0] = f2.w; lo[1][1] = f3.x; lo[1][D - 1] = f3.y;
-            hi[1][0] = f3.z; hi[1][1] = f3.w; hi[1][D - 1] = f4.x;
-            ax[1][0] = f4.y; ax[1][1] = f4.z; ax[1][D - 1] = f4.w;
-            half[1] = f5.x; rad[1] = f5.y;
-            refs[0] = fbits(f5.z);
-            refs[1] = fbits(f5.w);
-        }
+        snch::PairView<D> P;
+        snch::load_pair<D>(s, cur, P);
         bool hit[2] = {false, false};
         float dm[2] = {kInf, kInf};
 #pragma unroll
@@ -115,13 +90,15 @@ __device__ __forceinline__ void closest_silhouette(const DevScene &s, unsigned m
             if (act) {
                 float dmax;
                 if (D == 2)
-                    box_dist2(lo[c][0], lo[c][D - 1], hi[c][0], hi[c][D - 1], L.x[0], L.x[D - 1], dm[c], dmax);
+                    box_dist2(P.lo[c][0], P.lo[c][D - 1], P.hi[c][0], P.hi[c][D - 1], L.x[0], L.x[D - 1], dm[c],
+                              dmax);
                 else
-                    box_dist3(lo[c][0], lo[c][1], lo[c][D - 1], hi[c][0], hi[c][1], hi[c][D - 1], L.x[0], L.x[1],
-                              L.x[D - 1], dm[c], dmax);
+                    box_dist3(P.lo[c][0], P.lo[c][1], P.lo[c][D - 1], P.hi[c][0], P.hi[c][1], P.hi[c][D - 1], L.x[0],
+                              L.x[1], L.x[D - 1], dm[c], dmax);
                 hit[c] = dm[c] <= L.r;
-                if ((half[c] >= 0.f) & hit[c])
-                    hit[c] = cone_overlaps_fast<D>(lo[c], hi[c], ax[c], half[c], rad[c], L.x, dm[c]);
+                if ((P.half[c] >= 0.f) & hit[c])
+                    hit[c] = cone_overlaps_fast<D>(P.lo[c], P.hi[c], P.ax[c], P.half[c], P.rad[c], L.x, dm[c]);
+                if (hit[c]) hit[c] = !snch::child_free<D>(s, P, c, L.x);
             }
         }
         const unsigned m0 = __ballot_sync(0xffffffffu, hit[0]), m1 = __ballot_sync(0xffffffffu, hit[1]);
@@ -132,15 +109,15 @@ __device__ __forceinline__ void closest_silhouette(const DevScene &s, unsigned m
                 ovf = true;
                 break;
             }
-            stk[++sp] = second_first ? make_int2(refs[0], fbits(hit[0] ? dm[0] : kInf))
-                                     : make_int2(refs[1], fbits(hit[1] ? dm[1] : kInf));
-            cur = second_first ? refs[1] : refs[0];
+            stk[++sp] = second_first ? make_int2(P.refs[0], fbits(hit[0] ? dm[0] : kInf))
+                                     : make_int2(P.refs[1], fbits(hit[1] ? dm[1] : kInf));
+            cur = second_first ? P.refs[1] : P.refs[0];
             cmask = second_first ? m1 : m0;
         } else if (m0) {
-            cur = refs[0];
+            cur = P.refs[0];
             cmask = m0;
         } else if (m1) {
-            cur = refs[1];
+            cur = P.refs[1];
             cmask = m1;
         } else {
             cur = kSilNone;

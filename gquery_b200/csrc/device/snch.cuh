@@ -124,48 +124,85 @@ __device__ __forceinline__ bool test_silhouette(const DevScene &s, Lane<D> &L, i
     return last;
 }
 
-// Interior node `ref`: both children against the current r_max, closer pushed last.
+constexpr int kSPair3Vec = 11;  // float4s per gq_spair3_t
+
+// One pair record: both children's boxes and normal cones (the reference's), their
+// references and, in 3D, their node bounds (sil_filter.h).
 template <int D>
-__device__ __forceinline__ void visit_interior(const DevScene &s, Lane<D> &L, int2 *stk, int ref) {
+struct PairView {
     float lo[2][D], hi[2][D], ax[2][D], half[2], rad[2];
     int refs[2];
+    float nb[2][D == 3 ? 9 : 1];
+};
+
+template <int D>
+__device__ __forceinline__ void load_pair(const DevScene &s, int ref, PairView<D> &P) {
     if (D == 2) {
         const float4 a0 = ldg4(s.spairs, 5 * (int64_t)ref), a1 = ldg4(s.spairs, 5 * (int64_t)ref + 1),
                      a2 = ldg4(s.spairs, 5 * (int64_t)ref + 2), a3 = ldg4(s.spairs, 5 * (int64_t)ref + 3);
         const int4 rr = __ldg(reinterpret_cast<const int4 *>(s.spairs) + 5 * (int64_t)ref + 4);
-        lo[0][0] = a0.x; lo[0][D - 1] = a0.y; hi[0][0] = a0.z; hi[0][D - 1] = a0.w;
-        ax[0][0] = a1.x; ax[0][D - 1] = a1.y; half[0] = a1.z; rad[0] = a1.w;
-        lo[1][0] = a2.x; lo[1][D - 1] = a2.y; hi[1][0] = a2.z; hi[1][D - 1] = a2.w;
-        ax[1][0] = a3.x; ax[1][D - 1] = a3.y; half[1] = a3.z; rad[1] = a3.w;
-        refs[0] = rr.x;
-        refs[1] = rr.y;
+        P.lo[0][0] = a0.x; P.lo[0][D - 1] = a0.y; P.hi[0][0] = a0.z; P.hi[0][D - 1] = a0.w;
+        P.ax[0][0] = a1.x; P.ax[0][D - 1] = a1.y; P.half[0] = a1.z; P.rad[0] = a1.w;
+        P.lo[1][0] = a2.x; P.lo[1][D - 1] = a2.y; P.hi[1][0] = a2.z; P.hi[1][D - 1] = a2.w;
+        P.ax[1][0] = a3.x; P.ax[1][D - 1] = a3.y; P.half[1] = a3.z; P.rad[1] = a3.w;
+        P.refs[0] = rr.x;
+        P.refs[1] = rr.y;
     } else {
-        const int64_t b = 6 * (int64_t)ref;
+        const int64_t b = kSPair3Vec * (int64_t)ref;
         const float4 f0 = ldg4(s.spairs, b), f1 = ldg4(s.spairs, b + 1), f2 = ldg4(s.spairs, b + 2),
                      f3 = ldg4(s.spairs, b + 3), f4 = ldg4(s.spairs, b + 4), f5 = ldg4(s.spairs, b + 5);
-        lo[0][0] = f0.x; lo[0][1] = f0.y; lo[0][D - 1] = f0.z;
-        hi[0][0] = f0.w; hi[0][1] = f1.x; hi[0][D - 1] = f1.y;
-        ax[0][0] = f1.z; ax[0][1] = f1.w; ax[0][D - 1] = f2.x;
-        half[0] = f2.y; rad[0] = f2.z;
-        lo[1][0] = f2.w; lo[1][1] = f3.x; lo[1][D - 1] = f3.y;
-        hi[1][0] = f3.z; hi[1][1] = f3.w; hi[1][D - 1] = f4.x;
-        ax[1][0] = f4.y; ax[1][1] = f4.z; ax[1][D - 1] = f4.w;
-        half[1] = f5.x; rad[1] = f5.y;
-        refs[0] = fbits(f5.z);
-        refs[1] = fbits(f5.w);
+        const float4 f6 = ldg4(s.spairs, b + 6), f7 = ldg4(s.spairs, b + 7), f8 = ldg4(s.spairs, b + 8),
+                     f9 = ldg4(s.spairs, b + 9), f10 = ldg4(s.spairs, b + 10);
+        P.lo[0][0] = f0.x; P.lo[0][1] = f0.y; P.lo[0][D - 1] = f0.z;
+        P.hi[0][0] = f0.w; P.hi[0][1] = f1.x; P.hi[0][D - 1] = f1.y;
+        P.ax[0][0] = f1.z; P.ax[0][1] = f1.w; P.ax[0][D - 1] = f2.x;
+        P.half[0] = f2.y; P.rad[0] = f2.z;
+        P.lo[1][0] = f2.w; P.lo[1][1] = f3.x; P.lo[1][D - 1] = f3.y;
+        P.hi[1][0] = f3.z; P.hi[1][1] = f3.w; P.hi[1][D - 1] = f4.x;
+        P.ax[1][0] = f4.y; P.ax[1][1] = f4.z; P.ax[1][D - 1] = f4.w;
+        P.half[1] = f5.x; P.rad[1] = f5.y;
+        P.refs[0] = fbits(f5.z);
+        P.refs[1] = fbits(f5.w);
+        float *n0 = P.nb[0], *n1 = P.nb[D == 3 ? 1 : 0];
+        if (D == 3) {
+            n0[0] = f6.x; n0[1] = f6.y; n0[2] = f6.z; n0[3] = f6.w; n0[4] = f7.x;
+            n0[5] = f7.y; n0[6] = f7.z; n0[7] = f7.w; n0[8] = f8.x;
+            n1[0] = f8.y; n1[1] = f8.z; n1[2] = f8.w; n1[3] = f9.x; n1[4] = f9.y;
+            n1[5] = f9.z; n1[6] = f9.w; n1[7] = f10.x; n1[8] = f10.y;
+        }
     }
+}
+
+// Child c of the pair certainly holds no silhouette for x (3D node bound, sil_filter.h;
+// skipping it leaves the reference's answers and the order of its other visits as
+// they are).  Always false in 2D.
+template <int D>
+__device__ __forceinline__ bool child_free(const DevScene &s, const PairView<D> &P, int c, const float *x) {
+    if (D == 2) return false;
+    const float *b = P.nb[D == 3 ? c : 0];
+    const float m = sil_node_margin(fmaxf(fmaxf(fabsf(x[0]), fabsf(x[1])), fabsf(x[D - 1])), s.coord_bound);
+    return sil_node_excluded(b[0], b[1], b[2], b[3], b[4], b[5], b[6], b[7], b[8], x[0], x[1], x[D - 1], m);
+}
+
+// Interior node `ref`: both children against the current r_max, closer pushed last.
+template <int D>
+__device__ __forceinline__ void visit_interior(const DevScene &s, Lane<D> &L, int2 *stk, int ref) {
+    PairView<D> P;
+    load_pair<D>(s, ref, P);
     bool hit[2];
     float dm[2];
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
         float dmax;
         if (D == 2)
-            box_dist2(lo[c][0], lo[c][D - 1], hi[c][0], hi[c][D - 1], L.x[0], L.x[D - 1], dm[c], dmax);
+            box_dist2(P.lo[c][0], P.lo[c][D - 1], P.hi[c][0], P.hi[c][D - 1], L.x[0], L.x[D - 1], dm[c], dmax);
         else
-            box_dist3(lo[c][0], lo[c][1], lo[c][D - 1], hi[c][0], hi[c][1], hi[c][D - 1], L.x[0], L.x[1],
-                      L.x[D - 1], dm[c], dmax);
+            box_dist3(P.lo[c][0], P.lo[c][1], P.lo[c][D - 1], P.hi[c][0], P.hi[c][1], P.hi[c][D - 1], L.x[0],
+                      L.x[1], L.x[D - 1], dm[c], dmax);
         hit[c] = dm[c] <= L.r;
-        if ((half[c] >= 0.f) & hit[c]) hit[c] = cone_overlaps<D>(lo[c], hi[c], ax[c], half[c], rad[c], L.x, dm[c]);
+        if ((P.half[c] >= 0.f) & hit[c])
+            hit[c] = cone_overlaps<D>(P.lo[c], P.hi[c], P.ax[c], P.half[c], P.rad[c], L.x, dm[c]);
+        if (hit[c]) hit[c] = !child_free<D>(s, P, c, L.x);
     }
     if (hit[0] & hit[1]) {
         if (L.sp + 2 >= GQ_STACK_EXACT) {
@@ -175,12 +212,12 @@ __device__ __forceinline__ void visit_interior(const DevScene &s, Lane<D> &L, in
             return;
         }
         const bool sw = dm[1] < dm[0];
-        stk[++L.sp] = sw ? make_int2(refs[0], fbits(dm[0])) : make_int2(refs[1], fbits(dm[1]));
-        stk[++L.sp] = sw ? make_int2(refs[1], fbits(dm[1])) : make_int2(refs[0], fbits(dm[0]));
+        stk[++L.sp] = sw ? make_int2(P.refs[0], fbits(dm[0])) : make_int2(P.refs[1], fbits(dm[1]));
+        stk[++L.sp] = sw ? make_int2(P.refs[1], fbits(dm[1])) : make_int2(P.refs[0], fbits(dm[0]));
     } else if (hit[0]) {
-        stk[++L.sp] = make_int2(refs[0], fbits(dm[0]));
+        stk[++L.sp] = make_int2(P.refs[0], fbits(dm[0]));
     } else if (hit[1]) {
-        stk[++L.sp] = make_int2(refs[1], fbits(dm[1]));
+        stk[++L.sp] = make_int2(P.refs[1], fbits(dm[1]));
     }
 }
 

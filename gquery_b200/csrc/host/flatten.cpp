@@ -1,8 +1,11 @@
 // Flattening pass (see flatten.hpp).  Compile with -ffp-contract=off.
 #include "flatten.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <thread>
+#include <vector>
 
 #include "../gq_fmath.h"
 #include "../sil_filter.h"
@@ -297,8 +300,92 @@ void flatten_wide(const BvhTree<D> &t, DeviceImage<D> &img) {
 // Binary SNCH
 // ---------------------------------------------------------------------------
 
+namespace {
+
+// Node bounds of sil_filter.h for both children of every 3D pair.  The silhouettes of
+// a subtree are one contiguous run of the leaf-ordered list (depth-first layout); a
+// subtree whose run is not contiguous gets a bound that never skips it.
 template <int D>
-void flatten_snch(const BvhTree<D> &t, const SnchTree<D> &s, DeviceImage<D> &img) {
+void snch_node_bounds(const BvhTree<D> &t, const SnchTree<D> &s, DeviceImage<D> &img, int n_threads) {
+    const size_t nn = t.nodes.size();
+    std::vector<int64_t> beg(nn, 0), end(nn, 0);
+    std::vector<uint8_t> split(nn, 0);  // 1: run not contiguous
+    for (size_t i = nn; i-- > 0;) {
+        const auto &n = t.nodes[i];
+        if (n.n_prims > 0) {
+            beg[i] = s.nodes[i].n_sil > 0 ? s.nodes[i].sil_offset : 0;
+            end[i] = s.nodes[i].n_sil > 0 ? s.nodes[i].sil_offset + s.nodes[i].n_sil : 0;
+            continue;
+        }
+        const size_t l = i + 1, r = i + (size_t)n.second_child;
+        const bool el = beg[l] == end[l], er = beg[r] == end[r];
+        split[i] = split[l] | split[r];
+        if (el) {
+            beg[i] = beg[r];
+            end[i] = end[r];
+        } else if (er) {
+            beg[i] = beg[l];
+            end[i] = end[l];
+        } else if (end[l] == beg[r]) {
+            beg[i] = beg[l];
+            end[i] = end[r];
+        } else if (end[r] == beg[l]) {
+            beg[i] = beg[r];
+            end[i] = end[l];
+        } else {
+            beg[i] = std::min(beg[l], beg[r]);
+            end[i] = std::max(end[l], end[r]);
+            split[i] = 1;
+        }
+    }
+    auto edge = [&](long long j) {
+        const gq_sile_t &r = img.sils[(size_t)j];
+        SilEdgeGeom g;
+        g.a[0] = r.ax; g.a[1] = r.ay; g.a[2] = r.az;
+        g.b[0] = r.bx; g.b[1] = r.by; g.b[2] = r.bz;
+        g.n0[0] = r.n0x; g.n0[1] = r.n0y; g.n0[2] = r.n0z;
+        g.n1[0] = r.n1x; g.n1[1] = r.n1y; g.n1[2] = r.n1z;
+        g.orient = (float)s.raw[s.ordered[(size_t)j]].orient;
+        g.usable = (r.flags & (GQ_ITEM_VALID | GQ_SIL_FILTER)) == GQ_SIL_FILTER;
+        return g;
+    };
+    auto bound = [&](size_t i, float out[9]) {
+        const auto &bx = t.nodes[i].box;
+        const float cx = 0.5f * (bx.lo.v[0] + bx.hi.v[0]), cy = 0.5f * (bx.lo.v[1] + bx.hi.v[1]),
+                    cz = 0.5f * (bx.lo.v[2] + bx.hi.v[2]);
+        if (split[i]) {
+            const float open[9] = {cx, cy, cz, 0.f, 0.f, 0.f, __builtin_inff(), 0.f, 0.f};
+            std::memcpy(out, open, sizeof open);
+        } else {
+            sil_node_bound(cx, cy, cz, beg[i], end[i], edge, out);
+        }
+    };
+    std::vector<uint32_t> interior;  // pair k belongs to interior node interior[k]
+    for (size_t i = 0; i < nn; ++i)
+        if (t.nodes[i].n_prims == 0) interior.push_back((uint32_t)i);
+    auto pair_bounds = [&](size_t k) {
+        const size_t i = interior[k];
+        auto &p = img.spairs[k];
+        bound(i + 1, p.l_b);
+        bound(i + (size_t)t.nodes[i].second_child, p.r_b);
+    };
+    const int nt = std::max(1, n_threads);
+    if (nt == 1 || interior.size() < 4096) {
+        for (size_t k = 0; k < interior.size(); ++k) pair_bounds(k);
+    } else {  // each pair is independent: the result does not depend on the thread count
+        std::vector<std::thread> pool;
+        for (int th = 0; th < nt; ++th)
+            pool.emplace_back([&, th]() {
+                for (size_t k = (size_t)th; k < interior.size(); k += (size_t)nt) pair_bounds(k);
+            });
+        for (auto &th : pool) th.join();
+    }
+}
+
+}  // namespace
+
+template <int D>
+void flatten_snch(const BvhTree<D> &t, const SnchTree<D> &s, DeviceImage<D> &img, int n_threads) {
     const auto rank = interior_ranks(t);
     auto ref_of = [&](uint32_t i) -> int32_t {
         const auto &n = t.nodes[i];
@@ -374,13 +461,14 @@ void flatten_snch(const BvhTree<D> &t, const SnchTree<D> &s, DeviceImage<D> &img
         const auto &sn = s.nodes[i];
         if (t.nodes[i].n_prims > 0 && sn.n_sil > 0) img.sils[(size_t)(sn.sil_offset + sn.n_sil - 1)].flags |= GQ_ITEM_LAST;
     }
+    if constexpr (D == 3) snch_node_bounds(t, s, img, n_threads);
 }
 
 template void flatten_bvh<2>(const PrimSource<2> &, const BvhTree<2> &, DeviceImage<2> &);
 template void flatten_bvh<3>(const PrimSource<3> &, const BvhTree<3> &, DeviceImage<3> &);
 template void flatten_wide<2>(const BvhTree<2> &, DeviceImage<2> &);
 template void flatten_wide<3>(const BvhTree<3> &, DeviceImage<3> &);
-template void flatten_snch<2>(const BvhTree<2> &, const SnchTree<2> &, DeviceImage<2> &);
-template void flatten_snch<3>(const BvhTree<3> &, const SnchTree<3> &, DeviceImage<3> &);
+template void flatten_snch<2>(const BvhTree<2> &, const SnchTree<2> &, DeviceImage<2> &, int);
+template void flatten_snch<3>(const BvhTree<3> &, const SnchTree<3> &, DeviceImage<3> &, int);
 
 }  // namespace gqb

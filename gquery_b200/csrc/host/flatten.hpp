@@ -46,7 +46,7 @@ template <int D>
 void flatten_wide(const BvhTree<D> &t, DeviceImage<D> &img);
 
 template <int D>
-void flatten_snch(const BvhTree<D> &t, const SnchTree<D> &s, DeviceImage<D> &img);
+void flatten_snch(const BvhTree<D> &t, const SnchTree<D> &s, DeviceImage<D> &img, int n_threads = 1);
 
 // Smallest power-of-two exponent e with 255 * 2^e >= hi - lo (clamped to normal floats).
 int quant_exponent(float lo, float hi);

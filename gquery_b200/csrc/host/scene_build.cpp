@@ -275,6 +275,7 @@ std::vector<SilEdge> build_silhouette_edges(const PrimSource<3> &src,
             s.idx[2] = i1;
             s.idx[swapped ? 3 : 0] = i2;
             s.face[swapped ? 1 : 0] = (uint64_t)f;
+            s.orient = swapped ? -1 : 1;
             s.prim = e;
         }
     }

@@ -54,6 +54,11 @@ struct SilEdge {
     uint64_t idx[4] = {0, 0, 0, 0};
     uint64_t face[2] = {0, 0};
     uint64_t prim = 0;
+    // +1 when the stored end points v[1] -> v[2] follow the winding of the face that
+    // wrote them last with its index pair in ascending order, -1 otherwise: on a
+    // consistently wound mesh the face normals of the record point outward exactly
+    // when this is +1 (used only to orient the node bounds of the flattening pass)
+    int8_t orient = 1;
 };
 
 template <int D>

@@ -66,3 +66,107 @@ GQ_HD bool sil_edge_excluded(float ax, float ay, float az, float n0x, float n0y,
     const float lo1 = a1 + fminf(0.f, s1), hi1 = a1 + fmaxf(0.f, s1);
     return ((lo0 > margin) & (lo1 > margin)) | ((hi0 < -margin) & (hi1 < -margin));
 }
+
+// ---------------------------------------------------------------- node bound
+//
+// The same argument one level up.  For a node (a child of an SNCH pair) with box
+// centre c, every silhouette edge of its subtree and each of its two faces, take the
+// face normal n with the edge's orientation sign s (both normals of an edge may flip
+// together: the test above is unchanged), and the points q of the edge.  Then
+//   s n . (q - x) = s n . (q - c) + A . (c - x) + (s n - A) . (c - x)
+// lies in [g + lo - delta l, g + hi + delta l], with g = A . (c - x), l = |c - x|,
+// [lo, hi] the range of s n . (q - c) over the subtree (from the end points and the
+// spans) and delta = max |s n - A|, both computed on the host in double and rounded
+// outward to FP32.  When that interval lies beyond a margin on one side of zero, both
+// dot products of every edge have the sign of that side and none is a silhouette for
+// x, so the traversal may skip the child: the reference's visit order of the other
+// nodes and its answers stay as they are.  With the orientation signs of a
+// consistently wound mesh the axis A gathers outward normals only, so delta measures
+// how much the surface bends inside the node rather than the pi of a cone that holds
+// both orientations.
+//
+// Margin.  Besides the reference's rounding of each dot product (at most
+// 1.75 eps (6 M + 4 X), see above), the FP32 evaluation of g (c - x, the fused dot
+// product), of l and delta l and of the two sums moves the interval by at most about
+// eps (37 M + 30 X); the margin 2e-5 (2 M + X) is nine times the total.  Nodes whose
+// subtree holds a boundary edge or an edge without GQ_SIL_FILTER get delta = +inf
+// (never skipped); nodes without silhouettes get lo = hi = +inf (always skipped).
+
+// Geometry of one 3D silhouette edge for the node bound: end points, stored face
+// normals, orientation sign and whether the pre-test may be used on it.
+struct SilEdgeGeom {
+    float a[3], b[3], n0[3], n1[3];
+    float orient;
+    bool usable;
+};
+
+GQ_HD float sil_node_margin(float x_inf, float coord_bound) { return 2.f * sil_margin(x_inf, coord_bound); }
+
+// True when the node with bound (c, axis, delta, lo, hi) holds no silhouette for x.
+GQ_HD bool sil_node_excluded(float cx, float cy, float cz, float ax, float ay, float az, float delta, float lo,
+                             float hi, float xx, float xy, float xz, float margin) {
+    const float vx = cx - xx, vy = cy - xy, vz = cz - xz;
+    const float g = gq_dot3(ax, ay, az, vx, vy, vz);
+    const float dl = delta * gq_norm3(vx, vy, vz);
+    return (g + lo - dl > margin) | (g + hi + dl < -margin);
+}
+
+#if !defined(__CUDA_ARCH__)
+// Node bound over the edges begin..end-1 (edge(j) returns their SilEdgeGeom), for a
+// node whose box centre is c: out = c[3], axis[3], delta, lo, hi.
+template <class EdgeAt>
+inline void sil_node_bound(float cx, float cy, float cz, long long begin, long long end, EdgeAt edge,
+                           float out[9]) {
+    out[0] = cx;
+    out[1] = cy;
+    out[2] = cz;
+    out[3] = out[4] = out[5] = 0.f;
+    if (begin >= end) {  // no silhouettes: always skipped
+        out[6] = 0.f;
+        out[7] = out[8] = __builtin_inff();
+        return;
+    }
+    double m[3] = {0.0, 0.0, 0.0};
+    bool ok = true;
+    for (long long j = begin; j < end && ok; ++j) {
+        const SilEdgeGeom e = edge(j);
+        ok = e.usable;
+        for (int k = 0; k < 3; ++k) m[k] += (double)e.orient * ((double)e.n0[k] + (double)e.n1[k]);
+    }
+    const double ml = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+    if (!ok || !(ml > 1e-30)) {  // never skipped
+        out[6] = __builtin_inff();
+        out[7] = out[8] = 0.f;
+        return;
+    }
+    float A[3];
+    for (int k = 0; k < 3; ++k) A[k] = out[3 + k] = (float)(m[k] / ml);
+    const double c[3] = {cx, cy, cz};
+    double dmax = 0.0, lo = __builtin_inf(), hi = -__builtin_inf();
+    for (long long j = begin; j < end; ++j) {
+        const SilEdgeGeom e = edge(j);
+        for (int f = 0; f < 2; ++f) {
+            const float *n = f ? e.n1 : e.n0;
+            double d2 = 0.0, ac = 0.0, sp = 0.0;
+            for (int k = 0; k < 3; ++k) {
+                const double sn = (double)e.orient * (double)n[k];
+                d2 += (sn - A[k]) * (sn - A[k]);
+                ac += sn * ((double)e.a[k] - c[k]);
+                sp += sn * ((double)e.b[k] - (double)e.a[k]);
+            }
+            dmax = fmax(dmax, sqrt(d2));
+            lo = fmin(lo, ac + fmin(0.0, sp));
+            hi = fmax(hi, ac + fmax(0.0, sp));
+        }
+    }
+    // outward to FP32, with room for the double rounding above
+    const double pad = 1e-12 * (fabs(lo) + fabs(hi) + 1.0);
+    float fd = (float)(dmax * (1.0 + 1e-12)), fl = (float)(lo - pad), fh = (float)(hi + pad);
+    if ((double)fd < dmax) fd = nextafterf(fd, __builtin_inff());
+    if ((double)fl > lo - pad) fl = nextafterf(fl, -__builtin_inff());
+    if ((double)fh < hi + pad) fh = nextafterf(fh, __builtin_inff());
+    out[6] = fd;
+    out[7] = fl;
+    out[8] = fh;
+}
+#endif

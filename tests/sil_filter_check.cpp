@@ -2,7 +2,8 @@
 // over random and adversarial edges and query points, the pre-test must never
 // exclude an edge that the reference's test (silhouette_edge.py:7-12, 50-64, in the
 // FP32 operations the kernels use) calls a silhouette.  Prints one JSON line with the
-// counts per regime; a non-zero "unsound" is a failure.  An optional second argument
+// counts per regime; a non-zero "unsound" is a failure.  The node regimes check the
+// node bound the same way over whole patches of edges.  An optional second argument
 // scales the margin (0 removes it: the check must then find unsound exclusions, which
 // shows that its cases reach the rounding boundary the margin covers).
 //
@@ -11,6 +12,8 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <utility>
+#include <vector>
 
 #include "gq_fmath.h"
 #include "sil_filter.h"
@@ -95,6 +98,124 @@ void print(const char *name, const Count &k, bool last) {
                 name, k.cases, k.usable, k.excluded, k.silhouettes, k.unsound, last ? "" : ", ");
 }
 
+
+// Node bound: a patch of a height field z = h(x, y) (smooth waves plus noise of a
+// chosen amplitude), triangulated consistently; every interior edge is a silhouette
+// record whose end points are stored in winding order (orientation +1) or swapped
+// (both stored normals point the other way, orientation -1), as the reference's
+// records come.  The patch is placed with a random rotation, scale and offset.
+struct Patch {
+    std::vector<SilEdgeGeom> edges;
+    float c[3];
+    float bound;  // largest |coordinate|
+};
+
+V rot(V v, const float R[9]) {
+    return {R[0] * v.x + R[1] * v.y + R[2] * v.z, R[3] * v.x + R[4] * v.y + R[5] * v.z,
+            R[6] * v.x + R[7] * v.y + R[8] * v.z};
+}
+
+Patch make_patch(Rng &r, int g, float rough) {
+    // random rotation from a random unit quaternion
+    float q0 = r.uni(-1, 1), q1 = r.uni(-1, 1), q2 = r.uni(-1, 1), q3 = r.uni(-1, 1);
+    const float qn = std::sqrt(q0 * q0 + q1 * q1 + q2 * q2 + q3 * q3);
+    q0 /= qn; q1 /= qn; q2 /= qn; q3 /= qn;
+    const float R[9] = {1 - 2 * (q2 * q2 + q3 * q3), 2 * (q1 * q2 - q0 * q3), 2 * (q1 * q3 + q0 * q2),
+                        2 * (q1 * q2 + q0 * q3), 1 - 2 * (q1 * q1 + q3 * q3), 2 * (q2 * q3 - q0 * q1),
+                        2 * (q1 * q3 - q0 * q2), 2 * (q2 * q3 + q0 * q1), 1 - 2 * (q1 * q1 + q2 * q2)};
+    const float s = r.logu(1e-2f, 1e2f);
+    const V off = mul(rand_in(r, 1.f), s * r.uni(0.f, 3.f));
+    const float w1 = r.uni(0.5f, 4.f), w2 = r.uni(0.5f, 4.f), amp = r.uni(0.f, 0.3f);
+    std::vector<V> p((size_t)(g + 1) * (g + 1));
+    for (int i = 0; i <= g; ++i)
+        for (int j = 0; j <= g; ++j) {
+            const float u = (float)i / g, v = (float)j / g;
+            const float z = amp * std::sin(w1 * u + 1.3f) * std::cos(w2 * v) + rough * r.uni(-1.f, 1.f) / g;
+            p[(size_t)i * (g + 1) + j] = add(mul(rot({u - 0.5f, v - 0.5f, z}, R), s), off);
+        }
+    auto at = [&](int i, int j) { return p[(size_t)i * (g + 1) + j]; };
+    Patch P;
+    // triangles (i,j),(i+1,j),(i+1,j+1) and (i,j),(i+1,j+1),(i,j+1); interior diagonal and
+    // grid edges with their two faces in winding order: edge a->b of face (a, b, c), the
+    // other face (b, a, d)
+    auto add_edge = [&](V a, V b, V c, V d) {
+        SilEdgeGeom e;
+        const bool swap = r.next() & 1;
+        if (swap) std::swap(a, b);
+        e.a[0] = a.x; e.a[1] = a.y; e.a[2] = a.z;
+        e.b[0] = b.x; e.b[1] = b.y; e.b[2] = b.z;
+        sil_face_normal(b.x - a.x, b.y - a.y, b.z - a.z, c.x - a.x, c.y - a.y, c.z - a.z, e.n0[0], e.n0[1], e.n0[2]);
+        sil_face_normal(d.x - a.x, d.y - a.y, d.z - a.z, b.x - a.x, b.y - a.y, b.z - a.z, e.n1[0], e.n1[1], e.n1[2]);
+        e.orient = swap ? -1.f : 1.f;
+        const float s0 = sil_span(e.n0[0], e.n0[1], e.n0[2], a.x, a.y, a.z, b.x, b.y, b.z);
+        const float s1 = sil_span(e.n1[0], e.n1[1], e.n1[2], a.x, a.y, a.z, b.x, b.y, b.z);
+        e.usable = sil_filter_usable(e.n0[0], e.n0[1], e.n0[2], e.n1[0], e.n1[1], e.n1[2], s0, s1);
+        P.edges.push_back(e);
+    };
+    for (int i = 0; i < g; ++i)
+        for (int j = 0; j < g; ++j) {
+            // diagonal (i,j)-(i+1,j+1) between the two triangles of the cell
+            add_edge(at(i, j), at(i + 1, j + 1), at(i, j + 1), at(i + 1, j));
+            if (i + 1 < g) add_edge(at(i + 1, j), at(i + 1, j + 1), at(i, j), at(i + 2, j + 1));
+            if (j + 1 < g) add_edge(at(i, j + 1), at(i + 1, j + 1), at(i + 1, j + 2), at(i, j));
+        }
+    float lo[3] = {1e30f, 1e30f, 1e30f}, hi[3] = {-1e30f, -1e30f, -1e30f};
+    P.bound = 0.f;
+    for (const V &v : p) {
+        const float w[3] = {v.x, v.y, v.z};
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = std::fmin(lo[k], w[k]);
+            hi[k] = std::fmax(hi[k], w[k]);
+        }
+        P.bound = std::fmax(P.bound, amax(v));
+    }
+    for (int k = 0; k < 3; ++k) P.c[k] = 0.5f * (lo[k] + hi[k]);
+    return P;
+}
+
+struct NodeCount {
+    long long cases = 0, excluded = 0, unsound = 0;
+};
+
+void check_node(Rng &r, int g, float rough, NodeCount &k) {
+    Patch P = make_patch(r, g, rough);
+    float b[9];
+    sil_node_bound(P.c[0], P.c[1], P.c[2], 0, (long long)P.edges.size(),
+                   [&](long long j) { return P.edges[(size_t)j]; }, b);
+    const float s = std::fmax(P.bound, 1e-6f);
+    for (int t = 0; t < 64; ++t) {
+        // queries: near the patch (within 1e-6 .. 2 of its size), and far
+        V x;
+        const V c{P.c[0], P.c[1], P.c[2]};
+        const int kind = (int)(r.next() % 3);
+        if (kind == 0) {
+            const SilEdgeGeom &e = P.edges[r.next() % P.edges.size()];
+            x = add(V{e.a[0], e.a[1], e.a[2]}, mul(unit(rand_in(r, 1.f)), r.logu(1e-7f, 1.f) * s));
+        } else if (kind == 1) {
+            x = add(c, rand_in(r, 2.f * s));
+        } else {
+            x = add(c, mul(unit(rand_in(r, 1.f)), r.logu(2.f, 1e3f) * s));
+        }
+        const float m = g_margin_scale * sil_node_margin(amax(x), P.bound);
+        const bool ex = sil_node_excluded(b[0], b[1], b[2], b[3], b[4], b[5], b[6], b[7], b[8], x.x, x.y, x.z, m);
+        ++k.cases;
+        if (!ex) continue;
+        ++k.excluded;
+        for (const SilEdgeGeom &e : P.edges)
+            if (reference_silhouette(V{e.a[0], e.a[1], e.a[2]}, V{e.b[0], e.b[1], e.b[2]},
+                                     V{e.n0[0], e.n0[1], e.n0[2]}, V{e.n1[0], e.n1[1], e.n1[2]}, x)) {
+                ++k.unsound;
+                break;
+            }
+    }
+}
+
+void print_node(const char *name, const NodeCount &k, bool last) {
+    std::printf("\"%s\": {\"cases\": %lld, \"usable\": %lld, \"excluded\": %lld, \"silhouettes\": 0, "
+                "\"unsound\": %lld}%s",
+                name, k.cases, k.cases, k.excluded, k.unsound, last ? "" : ", ");
+}
+
 }  // namespace
 
 int main(int argc, char **argv) {
@@ -153,6 +274,12 @@ int main(int argc, char **argv) {
             check(a, b, c, d, x, bound_of(a, b, c, d), on_edge);
         }
     }
+    NodeCount smooth, rough, flat;
+    for (long long i = 0; i < n / 200; ++i) {
+        check_node(r, 2 + (int)(r.next() % 7), 0.f, smooth);
+        check_node(r, 2 + (int)(r.next() % 7), r.logu(1e-3f, 2.f), rough);
+        check_node(r, 2 + (int)(r.next() % 7), 1e-6f, flat);
+    }
     std::printf("{");
     print("generic", generic, false);
     print("coplanar", coplanar, false);
@@ -160,9 +287,13 @@ int main(int argc, char **argv) {
     print("sliver", sliver, false);
     print("zero_length", zero_len, false);
     print("far", far, false);
-    print("on_edge", on_edge, true);
+    print("on_edge", on_edge, false);
+    print_node("node_smooth", smooth, false);
+    print_node("node_rough", rough, false);
+    print_node("node_flat", flat, true);
     std::printf("}\n");
     const long long bad = generic.unsound + coplanar.unsound + near_plane.unsound + sliver.unsound +
-                          zero_len.unsound + far.unsound + on_edge.unsound;
+                          zero_len.unsound + far.unsound + on_edge.unsound + smooth.unsound + rough.unsound +
+                          flat.unsound;
     return bad ? 1 : 0;
 }

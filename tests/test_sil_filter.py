@@ -1,6 +1,8 @@
 """The silhouette-edge pre-test never excludes an edge the reference's test calls a
 silhouette (random, nearly coplanar, sliver, zero-length, far and on-edge cases), and
-without its margin it would: the cases reach the rounding boundary the margin covers."""
+without its margin it would: the cases reach the rounding boundary the margin covers.
+The node bound never excludes a patch of edges (smooth, rough or flat height fields
+whose records come in either orientation) that holds a silhouette for the query."""
 import json
 import shutil
 import subprocess
@@ -34,6 +36,9 @@ def test_pre_test_is_sound(checker):
     assert res["generic"]["excluded"] > 0.3 * res["generic"]["cases"]
     # degenerate faces never use it
     assert res["zero_length"]["usable"] == 0
+    # the node bound skips patches, and with mixed record orientations too
+    for k in ("node_smooth", "node_rough", "node_flat"):
+        assert res[k]["excluded"] > 0.2 * res[k]["cases"], (k, res[k])
 
 
 def test_margin_is_needed(checker):
