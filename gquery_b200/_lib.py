@@ -42,6 +42,8 @@ BATCH_CP_EXACT = 1
 BATCH_RAY_EXACT = 2
 BATCH_SIL_EXACT = 8
 BATCH_SIL_WARP = 16
+BATCH_CP_SPLIT = 32
+BATCH_SIL_SPLIT = 64
 BATCH_ERR_SCENE = 1 << 8
 BATCH_ERR_NO_SNCH = 1 << 9
 SERVER_PER_REQUEST = 4

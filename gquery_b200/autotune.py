@@ -212,7 +212,8 @@ def tune(scene, kind: str, inputs: Sequence, *, cands: Optional[List[dict]] = No
 
 
 BATCH_CHOICES = [dict(cp_variant=c, ray_variant=r, sil_variant=s)
-                 for c in ("coherent", "exact") for r in ("wide8", "exact") for s in ("coherent", "warp", "exact")]
+                 for c in ("coherent", "exact", "split") for r in ("wide8", "exact")
+                 for s in ("coherent", "warp", "exact")]
 
 
 def tune_batch(make_batch: Callable[..., object], run_step: Callable[[object], object],

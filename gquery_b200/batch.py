@@ -44,15 +44,18 @@ class SceneBatch:
                  ray_variant: str = "wide8", sil_variant: str = "coherent"):
         if not scenes:
             raise ValueError("a batch needs at least one scene")
-        if cp_variant not in ("coherent", "exact") or ray_variant not in ("wide8", "exact") or \
-                sil_variant not in ("coherent", "exact", "warp"):
-            raise ValueError("cp_variant: coherent|exact, ray_variant: wide8|exact, sil_variant: coherent|exact|warp")
+        if cp_variant not in ("coherent", "exact", "split") or ray_variant not in ("wide8", "exact") or \
+                sil_variant not in ("coherent", "exact", "warp", "split"):
+            raise ValueError("cp_variant: coherent|exact|split, ray_variant: wide8|exact, "
+                             "sil_variant: coherent|exact|warp|split")
         self.scenes = list(scenes)
         self.dim = self.scenes[0].dim
         self.torch_device = self.scenes[0].torch_device
         self.max_queries = int(max_queries)
-        flags = (L.BATCH_CP_EXACT if cp_variant == "exact" else 0) | (L.BATCH_RAY_EXACT if ray_variant == "exact" else 0) | \
-            (L.BATCH_SIL_EXACT if sil_variant == "exact" else L.BATCH_SIL_WARP if sil_variant == "warp" else 0)
+        flags = (L.BATCH_CP_EXACT if cp_variant == "exact" else L.BATCH_CP_SPLIT if cp_variant == "split" else 0) | \
+            (L.BATCH_RAY_EXACT if ray_variant == "exact" else 0) | \
+            (L.BATCH_SIL_EXACT if sil_variant == "exact" else L.BATCH_SIL_WARP if sil_variant == "warp" else
+             L.BATCH_SIL_SPLIT if sil_variant == "split" else 0)
         arr = (C.c_void_p * len(self.scenes))(*[s.handle.value for s in self.scenes])
         h = C.c_void_p()
         L.check(L.lib().gq_batch_create(arr, len(self.scenes), self.max_queries, flags, C.byref(h)))

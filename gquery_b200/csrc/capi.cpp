@@ -929,7 +929,7 @@ gq_status gq_batch_run(gq_batch *b, const gq_batch_queries *cp, const gq_cp_out 
     for (const gq_scene *s : b->scenes) all_wide &= s->has_wide;
     cudaError_t e = gqd::batch_run(b->dev_scenes, (int)b->scenes.size(), b->dim, kinds, co, ro, so,
                                    (b->flags & GQ_BATCH_RAY_EXACT) || !all_wide ? 0 : 1,
-                                   (b->flags & GQ_BATCH_CP_EXACT) ? 0 : 1, gqd::sil_mode_of(b->flags),
+                                   gqd::cp_mode_of(b->flags), gqd::sil_mode_of(b->flags),
                                    1.f,
                                    b->scratch, b->max_queries, b->err, (cudaStream_t)stream);
     if (e != cudaSuccess) return fail_cuda(e, "batch launch");

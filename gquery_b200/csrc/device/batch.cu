@@ -11,6 +11,7 @@
 #include <cub/cub.cuh>
 
 #include "batch.cuh"
+#include "cp_warp.cuh"
 #include "packet.cuh"
 #include "records.cuh"
 #include "sil_packet.cuh"
@@ -136,20 +137,32 @@ __device__ __forceinline__ void refill(int64_t n, unsigned long long *counter, i
     }
 }
 
+// Closest-point queries whose per-lane traversal passes this many node visits are
+// handed to k_cp_heavy (cp_mode 2).
+constexpr int kHeavyVisits = 1024;
+// Silhouette queries whose per-lane traversal passes this many steps (node visits and
+// silhouette tests) are handed to k_sil_heavy (sil_mode 3).
+constexpr int kHeavySilSteps = 2048;
+
 // One persistent launch per step.  Phase 1: closest points, as warp tiles of 32
-// sorted queries (warp-coherent traversal once per distinct scene in the tile) or,
-// in exact mode, one lane per query.  Phase 2: rays, one lane per query.  Phase 3:
-// silhouettes (sil_mode): 1 warp-coherent tiles like the closest points, 2 one query
-// per warp (sil_warp.cuh), 0 one lane per query in the reference order.  Every warp moves to the next phase when the current one has no
-// unclaimed work, so the phases' tails overlap.  counter[0..2]: claims per phase.
+// sorted queries (warp-coherent traversal once per distinct scene in the tile) or
+// one lane per query (cp_mode 0; in cp_mode 2 a query past kHeavyVisits node visits
+// is appended to `heavy` and left to k_cp_heavy).  Phase 2: rays, one lane per query.
+// Phase 3: silhouettes (sil_mode): 1 warp-coherent tiles like the closest points, 2
+// one query per warp (sil_warp.cuh), 0 one lane per query in the reference order, 3
+// the same with queries past kHeavySilSteps handed to k_sil_heavy.  Every warp moves
+// to the next phase when the current one has no unclaimed work, so the phases' tails
+// overlap.  counter[0..2]: claims per phase, counter[3] / [5]: closest points /
+// silhouettes handed over.
 template <int D, bool RAYW>
 __global__ void __launch_bounds__(kBlock) k_batch(const DevScene *scenes, int n_scenes, BatchKind cp, gq_cp_out cp_out,
                                                   BatchKind ray, gq_ray_out ray_out, BatchKind sil,
-                                                  gq_sil_out sil_out, int cp_coherent, int sil_mode,
-                                                  int budget, unsigned long long *counter, int32_t *err) {
+                                                  gq_sil_out sil_out, int cp_mode, int sil_mode,
+                                                  int budget, unsigned long long *counter, int32_t *heavy,
+                                                  int2 *heavy_r, int32_t *sheavy, int2 *sheavy_r, int32_t *err) {
     const unsigned lane = threadIdx.x & 31u;
     // ---------------- phase 1: closest points ----------------
-    if (cp_coherent) {
+    if (cp_mode == 1) {
         const int64_t t_cp = (cp.n + 31) / 32;
         int2 stk[pkt::kPStack];
         for (;;) {
@@ -198,10 +211,15 @@ __global__ void __launch_bounds__(kBlock) k_batch(const DevScene *scenes, int n_
         trav::Lane<D, false, false> L;
         const DevScene *sc = scenes;
         int64_t qi = 0;
+        int visits = 0;
+        bool handed = false;
+        const bool split = cp_mode == 2;
         const gq_vecs none{};
         refill(
             cp.n, &counter[0], budget,
             [&](int64_t i) {
+                visits = 0;
+                handed = false;
                 qi = (int64_t)__ldg(cp.perm + i);
                 const int sid = __ldg(cp.scene + qi);
                 if (sid == GQ_BATCH_SKIP) return false;
@@ -217,8 +235,21 @@ __global__ void __launch_bounds__(kBlock) k_batch(const DevScene *scenes, int n_
                 trav::lane_init(*sc, L, cp.a, none, nullptr, qi);
                 return true;
             },
-            [&](int b) { return trav::lane_run<D, false, false, 0>(*sc, L, stk, b); },
-            [&]() { trav::lane_write(*sc, L, qi, cp.n, cp_out, gq_ray_out{}); });
+            [&](int b) {
+                if (trav::lane_run<D, false, false, 0>(*sc, L, stk, b)) return true;
+                visits += b;
+                if (split && visits >= kHeavyVisits) {  // long traversal: one warp takes it over
+                    const unsigned long long h = atomicAdd(&counter[3], 1ull);
+                    heavy[h] = (int32_t)qi;
+                    heavy_r[h] = make_int2(L.idx, fbits(L.r));
+                    handed = true;
+                    return true;
+                }
+                return false;
+            },
+            [&]() {
+                if (!handed) trav::lane_write(*sc, L, qi, cp.n, cp_out, gq_ray_out{});
+            });
     }
     // ---------------- phase 2: rays ----------------
     if (ray.n > 0) {
@@ -320,9 +351,14 @@ __global__ void __launch_bounds__(kBlock) k_batch(const DevScene *scenes, int n_
         snch::Lane<D> L;
         const DevScene *sc = scenes;
         int64_t qi = 0;
+        int steps = 0;
+        bool handed = false;
+        const bool split = sil_mode == 3;
         refill(
             sil.n, &counter[2], budget,
             [&](int64_t i) {
+                steps = 0;
+                handed = false;
                 qi = (int64_t)__ldg(sil.perm + i);
                 const int sid = __ldg(sil.scene + qi);
                 if (sid == GQ_BATCH_SKIP) return false;
@@ -338,18 +374,112 @@ __global__ void __launch_bounds__(kBlock) k_batch(const DevScene *scenes, int n_
                 snch::lane_init<D>(*sc, L, x, sil.r_max ? sil.r_max[qi] : kInf, stk);
                 return true;
             },
-            [&](int b) { return snch::lane_run<D>(*sc, L, stk, b); },
+            [&](int b) {
+                if (snch::lane_run<D>(*sc, L, stk, b)) return true;
+                steps += b;
+                if (split && steps >= kHeavySilSteps) {  // long traversal: one warp takes it over
+                    const unsigned long long h = atomicAdd(&counter[5], 1ull);
+                    sheavy[h] = (int32_t)qi;
+                    // the silhouette accepted so far (its position in the leaf order) and r_max
+                    sheavy_r[h] = make_int2(L.found ? L.bj : -1, fbits(L.r));
+                    handed = true;
+                    return true;
+                }
+                return false;
+            },
             [&]() {
+                if (handed) return;
                 if (L.ovf && sc->err) atomicOr(sc->err, GQ_DEVERR_STACK);
                 put_sil<D>(sil_out, sil.n, qi, L.found && !L.ovf, L.bp, L.bd, L.bid);
             });
     }
 }
 
+// Closest points handed over by k_batch (cp_mode 2): one query per warp (cp_warp.cuh),
+// `heavy[0 .. counter[3])` their query indices, heavy_r the (best primitive, r_max) each
+// lane had reached, counter[4] the claims.  Runs after k_batch on the same stream, so
+// the list is complete.
+template <int D>
+__global__ void __launch_bounds__(kBlock) k_cp_heavy(const DevScene *scenes, BatchKind cp, gq_cp_out cp_out,
+                                                     const int32_t *heavy, const int2 *heavy_r,
+                                                     unsigned long long *counter) {
+    extern __shared__ int2 hstk[];
+    int2 *wst = hstk + (threadIdx.x >> 5) * wcp::kWarpStack;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned long long n_heavy = counter[3];
+    for (;;) {
+        unsigned long long t = 0;
+        if (lane == 0) t = atomicAdd(&counter[4], 1ull);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= n_heavy) break;
+        const int64_t qi = __ldg(heavy + t);
+        const DevScene &s = scenes[__ldg(cp.scene + qi)];  // checked by k_batch before the hand-over
+        float p[D];
+#pragma unroll
+        for (int k = 0; k < D; ++k) p[k] = qget(cp.a, qi, k);
+        const int2 carried = __ldg(heavy_r + t);
+        int idx;
+        bool ovf;
+        wcp::closest_point<D>(s, p, __int_as_float(carried.y), carried.x, wst, idx, ovf);
+        if (lane == 0) {
+            if (ovf && s.err) atomicOr(s.err, GQ_DEVERR_STACK);
+            const bool found = idx >= 0 && !ovf;
+            if (D == 3)
+                cp3_record(s.prims, idx, found, p[0], p[1], p[D - 1], cp_out, cp.n, qi);
+            else
+                cp2_record(s.prims, idx, found, p[0], p[D - 1], cp_out, cp.n, qi);
+        }
+    }
+}
+
+// Silhouettes handed over by k_batch (sil_mode 3): one query per warp (sil_warp.cuh)
+// from the lane's r_max; the silhouette the lane had accepted, if any, stands unless a
+// nearer one turns up.  sheavy[0 .. counter[5]) the query indices, sheavy_r the
+// (accepted silhouette, r_max) pairs, counter[6] the claims.
+template <int D>
+__global__ void __launch_bounds__(kBlock) k_sil_heavy(const DevScene *scenes, BatchKind sil, gq_sil_out sil_out,
+                                                      const int32_t *sheavy, const int2 *sheavy_r,
+                                                      unsigned long long *counter) {
+    extern __shared__ int2 hstk[];
+    int2 *wst = hstk + (threadIdx.x >> 5) * wsil::kWarpStack;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned long long n_heavy = counter[5];
+    for (;;) {
+        unsigned long long t = 0;
+        if (lane == 0) t = atomicAdd(&counter[6], 1ull);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= n_heavy) break;
+        const int64_t qi = __ldg(sheavy + t);
+        const DevScene &s = scenes[__ldg(sil.scene + qi)];  // checked by k_batch before the hand-over
+        const int2 carried = __ldg(sheavy_r + t);
+        float x[D];
+#pragma unroll
+        for (int k = 0; k < D; ++k) x[k] = qget(sil.a, qi, k);
+        snch::Lane<D> L;
+        wsil::closest_silhouette<D>(s, x, __int_as_float(carried.y), L, wst);
+        if (lane == 0) {
+            if (L.ovf && s.err) atomicOr(s.err, GQ_DEVERR_STACK);
+            if (!L.found && !L.ovf && carried.x >= 0) {
+                // nothing nearer: the carried silhouette, its record recomputed by the same test
+                snch::Lane<D> C;
+#pragma unroll
+                for (int k = 0; k < D; ++k) C.x[k] = x[k];
+                C.r = kInf;
+                C.found = false;
+                snch::test_silhouette<D>(s, C, carried.x);
+                put_sil<D>(sil_out, sil.n, qi, C.found, C.bp, C.bd, C.bid);
+            } else {
+                put_sil<D>(sil_out, sil.n, qi, L.found && !L.ovf, L.bp, L.bd, L.bid);
+            }
+        }
+    }
+}
+
 template <int D, bool RAYW>
 cudaError_t launch_batch(const DevScene *scenes_dev, int n_scenes, BatchKind kinds[3], const gq_cp_out &cp_out,
-                         const gq_ray_out &ray_out, const gq_sil_out &sil_out, int cp_coherent, int sil_mode,
-                         float grid_share, unsigned long long *counter, int32_t *err, cudaStream_t st) {
+                         const gq_ray_out &ray_out, const gq_sil_out &sil_out, int cp_mode, int sil_mode,
+                         float grid_share, unsigned long long *counter, int32_t *heavy, int2 *heavy_r,
+                         int32_t *sheavy, int2 *sheavy_r, int32_t *err, cudaStream_t st) {
     // the one-query-per-warp silhouette phase keeps its stacks in dynamic shared memory
     const size_t smem = (sil_mode == 2 && kinds[2].n > 0) ? (size_t)(kBlock / 32) * wsil::kWarpStack * sizeof(int2) : 0;
     const int mi = smem ? 1 : 0;
@@ -369,9 +499,37 @@ cudaError_t launch_batch(const DevScene *scenes_dev, int n_scenes, BatchKind kin
     if (grid_share > 0.f && grid_share < 1.f)
         want = std::min<int64_t>(want, std::max<int64_t>(1, (int64_t)(grid_share * (float)(bps * n_sm))));
     k_batch<D, RAYW><<<dim3((unsigned)want), kBlock, smem, st>>>(scenes_dev, n_scenes, kinds[0], cp_out, kinds[1],
-                                                                 ray_out, kinds[2], sil_out, cp_coherent, sil_mode, 32,
-                                                                 counter, err);
-    return cudaGetLastError();
+                                                                 ray_out, kinds[2], sil_out, cp_mode, sil_mode, 32,
+                                                                 counter, heavy, heavy_r, sheavy, sheavy_r, err);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    // the handed-over queries: persistent grids of one query per warp
+    const size_t hsmem = (size_t)(kBlock / 32) * wcp::kWarpStack * sizeof(int2);
+    static int hbps[2] = {0, 0};
+    if (!hbps[0]) {
+        int b = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_cp_heavy<D>, kBlock, hsmem);
+        hbps[0] = b < 1 ? 1 : b;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sil_heavy<D>, kBlock, hsmem);
+        hbps[1] = b < 1 ? 1 : b;
+    }
+    auto hgrid = [&](int which, int64_t n) {
+        int64_t g = std::min<int64_t>((int64_t)hbps[which] * n_sm, (n * 32 + kBlock - 1) / kBlock);
+        if (grid_share > 0.f && grid_share < 1.f)
+            g = std::min<int64_t>(g, std::max<int64_t>(1, (int64_t)(grid_share * (float)(hbps[which] * n_sm))));
+        return dim3((unsigned)g);
+    };
+    if (cp_mode == 2 && kinds[0].n > 0) {
+        k_cp_heavy<D><<<hgrid(0, kinds[0].n), kBlock, hsmem, st>>>(scenes_dev, kinds[0], cp_out, heavy, heavy_r,
+                                                                   counter);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    if (sil_mode == 3 && kinds[2].n > 0) {
+        k_sil_heavy<D><<<hgrid(1, kinds[2].n), kBlock, hsmem, st>>>(scenes_dev, kinds[2], sil_out, sheavy, sheavy_r,
+                                                                    counter);
+        e = cudaGetLastError();
+    }
+    return e;
 }
 
 inline size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
@@ -393,7 +551,7 @@ size_t batch_scratch_bytes(int64_t max_n) {
 }
 
 cudaError_t batch_run(const DevScene *scenes_dev, int n_scenes, int dim, BatchKind kinds[3], const gq_cp_out &cp_out,
-                      const gq_ray_out &ray_out, const gq_sil_out &sil_out, int ray_wide, int cp_coherent,
+                      const gq_ray_out &ray_out, const gq_sil_out &sil_out, int ray_wide, int cp_mode,
                       int sil_mode, float grid_share, void *scratch, int64_t max_n, int32_t *err,
                       cudaStream_t st) {
     char *p = static_cast<char *>(scratch);
@@ -402,6 +560,9 @@ cudaError_t batch_run(const DevScene *scenes_dev, int n_scenes, int dim, BatchKi
     int end_bit = 32;
     while ((1ll << (end_bit - 32)) < (long long)n_scenes + 1) ++end_bit;  // padding keys sort last
     const size_t tb = sort_temp_bytes(max_n);
+    // closest points handed to k_cp_heavy: the cp kind's sort inputs, free after the sort
+    int32_t *heavy = nullptr, *sheavy = nullptr;
+    int2 *heavy_r = nullptr, *sheavy_r = nullptr;
     for (int k = 0; k < 3; ++k) {
         BatchKind &q = kinds[k];
         uint64_t *k_in = reinterpret_cast<uint64_t *>(p);
@@ -415,6 +576,13 @@ cudaError_t batch_run(const DevScene *scenes_dev, int n_scenes, int dim, BatchKi
         void *temp = p;
         p += align256(tb);
         q.perm = perm;
+        if (k == 0) {
+            heavy = v_in;
+            heavy_r = reinterpret_cast<int2 *>(k_in);
+        } else if (k == 2) {
+            sheavy = v_in;
+            sheavy_r = reinterpret_cast<int2 *>(k_in);
+        }
         if (q.n <= 0) continue;
         k_batch_keys<<<dim3((unsigned)((q.n + kBlock - 1) / kBlock)), kBlock, 0, st>>>(scenes_dev, n_scenes, q, q.n,
                                                                                         k_in, v_in, err);
@@ -424,17 +592,18 @@ cudaError_t batch_run(const DevScene *scenes_dev, int n_scenes, int dim, BatchKi
         e = cub::DeviceRadixSort::SortPairs(temp, tbk, k_in, k_out, v_in, perm, (int)q.n, 0, end_bit, st);
         if (e != cudaSuccess) return e;
     }
-    cudaError_t e = cudaMemsetAsync(counter, 0, 3 * sizeof(unsigned long long), st);
+    // claims per phase; closest points handed over, their claims; silhouettes the same
+    cudaError_t e = cudaMemsetAsync(counter, 0, 7 * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
     if (dim == 3)
-        return ray_wide ? launch_batch<3, true>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_coherent,
-                                                sil_mode, grid_share, counter, err, st)
-                        : launch_batch<3, false>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_coherent,
-                                                 sil_mode, grid_share, counter, err, st);
-    return ray_wide ? launch_batch<2, true>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_coherent,
-                                            sil_mode, grid_share, counter, err, st)
-                    : launch_batch<2, false>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_coherent,
-                                             sil_mode, grid_share, counter, err, st);
+        return ray_wide ? launch_batch<3, true>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_mode,
+                                                sil_mode, grid_share, counter, heavy, heavy_r, sheavy, sheavy_r, err, st)
+                        : launch_batch<3, false>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_mode,
+                                                 sil_mode, grid_share, counter, heavy, heavy_r, sheavy, sheavy_r, err, st);
+    return ray_wide ? launch_batch<2, true>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_mode,
+                                            sil_mode, grid_share, counter, heavy, heavy_r, sheavy, sheavy_r, err, st)
+                    : launch_batch<2, false>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_mode,
+                                             sil_mode, grid_share, counter, heavy, heavy_r, sheavy, sheavy_r, err, st);
 }
 
 }  // namespace gqd

@@ -25,6 +25,7 @@ struct Lane {
     float bp[D];    // best silhouette point
     float bd;
     int bid;
+    int bj;         // position of the best silhouette in the leaf order (valid when found)
     int j;          // next silhouette of the current leaf, -1 when not in a leaf
     int sp;         // stack top, -1 when empty
     bool found, ovf;
@@ -120,6 +121,7 @@ __device__ __forceinline__ bool test_silhouette(const DevScene &s, Lane<D> &L, i
         for (int k = 0; k < D; ++k) L.bp[k] = p[k];
         L.bd = d;
         L.bid = pid;
+        L.bj = j;
     }
     return last;
 }

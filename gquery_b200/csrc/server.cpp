@@ -430,7 +430,7 @@ struct gq_server {
         for (const gq_scene *sc : scenes) all_wide &= sc->has_wide;
         cudaError_t e = gqd::batch_run(dev_scenes, (int)scenes.size(), D, kinds, co, ro, so,
                                        (flags & GQ_BATCH_RAY_EXACT) || !all_wide ? 0 : 1,
-                                       (flags & GQ_BATCH_CP_EXACT) ? 0 : 1, gqd::sil_mode_of(flags),
+                                       gqd::cp_mode_of(flags), gqd::sil_mode_of(flags),
                                        S.sil_only ? sil_share : 1.f, S.scratch, step_queries, S.err, S.st);
         return e == cudaSuccess ? GQ_OK : fail_cuda(e, "server step");
     }

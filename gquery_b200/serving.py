@@ -108,13 +108,15 @@ class Server:
 
     def __init__(self, scenes: Sequence[Scene], *, budget_bytes: int = 0, ring_queries=(1 << 22,) * 3,
                  step_queries: int = 1 << 19, max_inflight: int = 2, per_request: bool = False,
-                 cp_variant: str = "exact", ray_variant: str = "wide8", sil_variant: str = "warp",
+                 cp_variant: str = "split", ray_variant: str = "wide8", sil_variant: str = "warp",
                  sil_share: float = 0.8, sil_slots: int = 2, sil_step_queries: int = 1 << 15):
         self.scenes = list(scenes)
         self.dim = self.scenes[0].dim
         flags = (L.SERVER_PER_REQUEST if per_request else 0) | \
-            (L.BATCH_CP_EXACT if cp_variant == "exact" else 0) | (L.BATCH_RAY_EXACT if ray_variant == "exact" else 0) | \
-            (L.BATCH_SIL_EXACT if sil_variant == "exact" else L.BATCH_SIL_WARP if sil_variant == "warp" else 0)
+            (L.BATCH_CP_EXACT if cp_variant == "exact" else L.BATCH_CP_SPLIT if cp_variant == "split" else 0) | \
+            (L.BATCH_RAY_EXACT if ray_variant == "exact" else 0) | \
+            (L.BATCH_SIL_EXACT if sil_variant == "exact" else L.BATCH_SIL_WARP if sil_variant == "warp" else
+             L.BATCH_SIL_SPLIT if sil_variant == "split" else 0)
         rq = [int(ring_queries)] * 3 if isinstance(ring_queries, int) else [int(x) for x in ring_queries]
         opts = L.ServerOpts(int(budget_bytes), (C.c_int64 * 3)(*rq), int(step_queries), int(max_inflight), flags,
                             float(sil_share), int(sil_slots), int(sil_step_queries))

@@ -256,6 +256,12 @@ typedef struct gq_batch gq_batch;
 #define GQ_BATCH_RAY_EXACT 2 /* rays: binary BVH, reference visit order */
 #define GQ_BATCH_SIL_EXACT 8 /* silhouettes: one exact traversal per lane, reference visit order */
 #define GQ_BATCH_SIL_WARP 16 /* silhouettes: one query per warp (GQ_VARIANT_WARP), for sparse queries */
+#define GQ_BATCH_CP_SPLIT 32 /* closest point: one lane per query in the reference order; a query past
+                                1024 node visits is restarted with one warp for it (answers equal up to
+                                FP32 distance ties): bounds the tail of sparse, uneven query sets */
+#define GQ_BATCH_SIL_SPLIT 64 /* silhouettes: one lane per query in the reference order; a query past 2048
+                                 steps is taken over by one warp from the r_max it reached (answers equal up
+                                 to FP32 distance ties) */
 
 typedef struct {
     int64_t n;             /* query count (0: none of this kind) */

@@ -6,7 +6,7 @@ import types
 import numpy as np
 import pytest
 
-from gquery_b200.autotune import TuneCache, candidates, config_key, full_config, tune, tune_batch
+from gquery_b200.autotune import BATCH_CHOICES, TuneCache, candidates, config_key, full_config, tune, tune_batch
 
 
 def test_candidates_cover_width_stack_and_block():
@@ -85,4 +85,4 @@ def test_tune_batch_picks_fastest_choice():
     t = {("coherent", "wide8", "coherent"): 1.0}
     res = tune_batch(make, lambda b: None, timer=lambda fn: t.get(tuple(made[-1].values()), 2.0))
     assert res["best"] == dict(cp_variant="coherent", ray_variant="wide8", sil_variant="coherent")
-    assert len(res["table"]) == 12
+    assert len(res["table"]) == len(BATCH_CHOICES) == 18

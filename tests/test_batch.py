@@ -253,3 +253,68 @@ def test_batch_silhouettes_one_query_per_warp(dim, two_d, three_d):
                  lambda s, sel: s.closest_silhouette(_dev(pts[sel]), 0.9, variant="exact"))
     rep = tie_report({k: v[..., live] for k, v in got.items()}, {k: v[..., live] for k, v in ref.items()})
     assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0 and rep["max_rel_d"] <= REL_TOL, rep
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_batch_split_closest_points(dim, two_d, three_d):
+    """cp_variant "split": one lane per query, long traversals restarted one per warp.
+    An undisplaced sphere (circle) queried near its centre makes every primitive almost
+    equally far, so those traversals pass the visit budget and take the warp path."""
+    scenes, _ = two_d if dim == 2 else three_d
+    if dim == 3:
+        v, f = W.icosphere(5)
+    else:
+        t = np.linspace(0.0, 2.0 * np.pi, 20000, endpoint=False)
+        v = np.stack([np.cos(t), np.sin(t)], 1).astype(np.float32)
+        f = np.stack([np.arange(20000), (np.arange(20000) + 1) % 20000], 1).astype(np.int32)
+    scenes = scenes + [Scene(v, f, dim, device=0, build_snch=False)]
+    n = 6000
+    ids, pts, _ = _mixed_queries(n, dim, len(scenes), seed=60 + dim)
+    rng = np.random.default_rng(61)
+    centre = slice(0, 1500)  # near the centre of the sphere / circle
+    ids[centre] = len(scenes) - 1
+    pts[centre] = rng.uniform(-0.02, 0.02, size=(1500, dim)).astype(np.float32)
+    ids[::13] = SKIP
+    b = SceneBatch(scenes, n, cp_variant="split")
+    out = b.alloc(n, 0, 0)
+    out.cp.prim_id.fill_(-7)
+    res = b.run(cp=(_dev(pts), _dev(ids)), out=out)
+    torch.cuda.synchronize()
+    assert b.device_error() == 0
+    got = to_np(res.cp)
+    live = ids != SKIP
+    assert np.all(got["prim_id"][~live] == -7)
+    ref = _alone(scenes, np.where(live, ids, -1), lambda s, sel: s.closest_point(_dev(pts[sel]), variant="exact"))
+    rep = tie_report({k: v[..., live] for k, v in got.items()}, {k: v[..., live] for k, v in ref.items()})
+    assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0 and rep["max_rel_d"] <= REL_TOL, rep
+    # a second run gives the same answers (the hand-over list and its counters restart)
+    again = to_np(b.run(cp=(_dev(pts), _dev(ids))).cp)
+    for k in ("valid", "d", "prim_id"):
+        assert np.array_equal(again[k][..., live], got[k][..., live]), k
+
+
+def test_batch_split_silhouettes():
+    """sil_variant "split": one lane per query, traversals past 2048 steps taken over by
+    one warp from the r_max they reached.  On this level-6 mesh about one uniform query
+    in a thousand runs that long."""
+    v, f = W.icosphere(6, amplitude=0.15, seed=5)
+    scenes = [Scene(v, f, 3, device=0, build_snch=True)]
+    n = 8000
+    pts = W.uniform_points(n, 3, seed=3)
+    ids = np.zeros(n, np.int32)
+    ids[::17] = SKIP
+    b = SceneBatch(scenes, n, sil_variant="split")
+    out = b.alloc(0, 0, n)
+    out.sil.prim_id.fill_(-7)
+    res = b.run(sil=(_dev(pts), _dev(ids)), out=out)
+    torch.cuda.synchronize()
+    assert b.device_error() == 0
+    got = to_np(res.sil)
+    live = ids != SKIP
+    assert np.all(got["prim_id"][~live] == -7)
+    ref = to_np(scenes[0].closest_silhouette(_dev(pts[live]), variant="exact"))
+    rep = tie_report({k: v[..., live] for k, v in got.items()}, ref)
+    assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0 and rep["max_rel_d"] <= REL_TOL, rep
+    again = to_np(b.run(sil=(_dev(pts), _dev(ids))).sil)
+    for k in ("valid", "d", "prim_id"):
+        assert np.array_equal(again[k][..., live], got[k][..., live]), k
