@@ -590,7 +590,12 @@ gq_status gq_server_create(gq_scene *const *scenes, int32_t n_scenes, const gq_s
     if (e == cudaSuccess)
         e = cudaMemcpy(s->dev_scenes, views.data(), views.size() * sizeof(gqd::DevScene), cudaMemcpyHostToDevice);
     for (int k = 0; k < 3 && e == cudaSuccess; ++k) e = s->make_ring(s->ring[k]);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->copy_st, cudaStreamNonBlocking);
+    // closest-point / ray steps and the copies on the highest stream priority, silhouette
+    // steps (long, persistent launches) on the lowest: when both wait for SMs, the short
+    // kinds' blocks are scheduled first
+    int prio_low = 0, prio_high = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&s->copy_st, cudaStreamNonBlocking, prio_high);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->copy_evt, cudaEventDisableTiming);
     const bool per_request = (s->flags & GQ_SERVER_PER_REQUEST) != 0;
     const int sil_slots = per_request ? 0 : (o.sil_slots > 0 ? o.sil_slots : 2);
@@ -599,7 +604,8 @@ gq_status gq_server_create(gq_scene *const *scenes, int32_t n_scenes, const gq_s
     s->slots.resize((size_t)(inflight + sil_slots));
     for (int i = 0; i < sil_slots; ++i) s->slots[(size_t)(inflight + i)].sil_only = true;
     for (Slot &S : s->slots) {
-        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S.st, cudaStreamNonBlocking);
+        if (e == cudaSuccess)
+            e = cudaStreamCreateWithPriority(&S.st, cudaStreamNonBlocking, S.sil_only ? prio_low : prio_high);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S.done, cudaEventDisableTiming);
         S.scratch_bytes = (s->flags & GQ_SERVER_PER_REQUEST) ? (size_t)gq_query_scratch_bytes(s->step_queries)
                                                              : gqd::batch_scratch_bytes(s->step_queries);
