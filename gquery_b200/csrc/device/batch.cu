@@ -137,6 +137,44 @@ __device__ __forceinline__ void refill(int64_t n, unsigned long long *counter, i
     }
 }
 
+// Phase 3, sil_mode 2: one silhouette query per warp (sil_warp.cuh), the warp's stack in
+// dynamic shared memory; counter[2] counts the claims.
+template <int D>
+__device__ __forceinline__ void sil_warp_phase(const DevScene *scenes, int n_scenes, const BatchKind &sil,
+                                               const gq_sil_out &sil_out, unsigned long long *counter,
+                                               int32_t *err) {
+    const unsigned lane = threadIdx.x & 31u;
+    // one query per warp; this warp's stack in dynamic shared memory
+    extern __shared__ int2 wstk[];
+    int2 *wst = wstk + (threadIdx.x >> 5) * wsil::kWarpStack;
+    for (;;) {
+        unsigned long long t = 0;
+        if (lane == 0) t = atomicAdd(&counter[2], 1ull);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= (unsigned long long)sil.n) break;
+        const int64_t qi = (int64_t)__ldg(sil.perm + (int64_t)t);
+        const int sid = __ldg(sil.scene + qi);
+        if (sid == GQ_BATCH_SKIP) continue;
+        float x[D];
+#pragma unroll
+        for (int k = 0; k < D; ++k) x[k] = qget(sil.a, qi, k);
+        const bool known = (unsigned)sid < (unsigned)n_scenes;
+        if (!known || !scenes[sid].spairs) {
+            if (lane == 0) {
+                atomicOr(err, known ? GQ_BATCH_ERR_NO_SNCH : GQ_BATCH_ERR_SCENE);
+                put_sil<D>(sil_out, sil.n, qi, false, x, 0.f, 0);
+            }
+            continue;
+        }
+        snch::Lane<D> L;
+        wsil::closest_silhouette<D>(scenes[sid], x, sil.r_max ? sil.r_max[qi] : kInf, L, wst);
+        if (lane == 0) {
+            if (L.ovf && scenes[sid].err) atomicOr(scenes[sid].err, GQ_DEVERR_STACK);
+            put_sil<D>(sil_out, sil.n, qi, L.found && !L.ovf, L.bp, L.bd, L.bid);
+        }
+    }
+}
+
 // Closest-point queries whose per-lane traversal passes this many node visits are
 // handed to k_cp_heavy (cp_mode 2).
 constexpr int kHeavyVisits = 1024;
@@ -280,35 +318,7 @@ __global__ void __launch_bounds__(kBlock) k_batch(const DevScene *scenes, int n_
     }
     // ---------------- phase 3: silhouettes ----------------
     if (sil.n > 0 && sil_mode == 2) {
-        // one query per warp; this warp's stack in dynamic shared memory
-        extern __shared__ int2 wstk[];
-        int2 *wst = wstk + (threadIdx.x >> 5) * wsil::kWarpStack;
-        for (;;) {
-            unsigned long long t = 0;
-            if (lane == 0) t = atomicAdd(&counter[2], 1ull);
-            t = __shfl_sync(0xffffffffu, t, 0);
-            if (t >= (unsigned long long)sil.n) break;
-            const int64_t qi = (int64_t)__ldg(sil.perm + (int64_t)t);
-            const int sid = __ldg(sil.scene + qi);
-            if (sid == GQ_BATCH_SKIP) continue;
-            float x[D];
-#pragma unroll
-            for (int k = 0; k < D; ++k) x[k] = qget(sil.a, qi, k);
-            const bool known = (unsigned)sid < (unsigned)n_scenes;
-            if (!known || !scenes[sid].spairs) {
-                if (lane == 0) {
-                    atomicOr(err, known ? GQ_BATCH_ERR_NO_SNCH : GQ_BATCH_ERR_SCENE);
-                    put_sil<D>(sil_out, sil.n, qi, false, x, 0.f, 0);
-                }
-                continue;
-            }
-            snch::Lane<D> L;
-            wsil::closest_silhouette<D>(scenes[sid], x, sil.r_max ? sil.r_max[qi] : kInf, L, wst);
-            if (lane == 0) {
-                if (L.ovf && scenes[sid].err) atomicOr(scenes[sid].err, GQ_DEVERR_STACK);
-                put_sil<D>(sil_out, sil.n, qi, L.found && !L.ovf, L.bp, L.bd, L.bid);
-            }
-        }
+        sil_warp_phase<D>(scenes, n_scenes, sil, sil_out, counter, err);
     } else if (sil.n > 0 && sil_mode == 1) {
         const int64_t t_sil = (sil.n + 31) / 32;
         snch::Stack stk;
@@ -475,6 +485,15 @@ __global__ void __launch_bounds__(kBlock) k_sil_heavy(const DevScene *scenes, Ba
     }
 }
 
+// A step with silhouettes only, one query per warp (the server's silhouette slots): the
+// phase alone, so that its register count, not k_batch's, sets the residency.
+template <int D>
+__global__ void __launch_bounds__(kBlock, 8) k_batch_silw(const DevScene *scenes, int n_scenes, BatchKind sil,
+                                                          gq_sil_out sil_out, unsigned long long *counter,
+                                                          int32_t *err) {
+    sil_warp_phase<D>(scenes, n_scenes, sil, sil_out, counter, err);
+}
+
 template <int D, bool RAYW>
 cudaError_t launch_batch(const DevScene *scenes_dev, int n_scenes, BatchKind kinds[3], const gq_cp_out &cp_out,
                          const gq_ray_out &ray_out, const gq_sil_out &sil_out, int cp_mode, int sil_mode,
@@ -482,6 +501,22 @@ cudaError_t launch_batch(const DevScene *scenes_dev, int n_scenes, BatchKind kin
                          int32_t *sheavy, int2 *sheavy_r, int32_t *err, cudaStream_t st) {
     // the one-query-per-warp silhouette phase keeps its stacks in dynamic shared memory
     const size_t smem = (sil_mode == 2 && kinds[2].n > 0) ? (size_t)(kBlock / 32) * wsil::kWarpStack * sizeof(int2) : 0;
+    if (smem && kinds[0].n <= 0 && kinds[1].n <= 0) {  // silhouettes only: the phase's own kernel
+        static int wbps = 0, w_sm = 0;
+        if (!wbps) {
+            int dev = 0, b = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&w_sm, cudaDevAttrMultiProcessorCount, dev);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_silw<D>, kBlock, smem);
+            wbps = b < 1 ? 1 : b;
+        }
+        int64_t want = std::min<int64_t>((int64_t)wbps * w_sm, (kinds[2].n * 32 + kBlock - 1) / kBlock);
+        if (grid_share > 0.f && grid_share < 1.f)
+            want = std::min<int64_t>(want, std::max<int64_t>(1, (int64_t)(grid_share * (float)(wbps * w_sm))));
+        k_batch_silw<D><<<dim3((unsigned)want), kBlock, smem, st>>>(scenes_dev, n_scenes, kinds[2], sil_out, counter,
+                                                                    err);
+        return cudaGetLastError();
+    }
     const int mi = smem ? 1 : 0;
     static int bps_m[2] = {0, 0}, n_sm = 0;
     if (!bps_m[mi]) {

@@ -68,7 +68,7 @@ __device__ __forceinline__ void closest_point(const DevScene &s, const float *p,
         __syncwarp();
         sp -= take;
         r = R;
-        int2 push[2];
+        int2 push0 = make_int2(0, 0), push1 = make_int2(0, 0);  // the lane's entries, push1 on top
         int np = 0;
         if (mine && __int_as_float(e.y) <= r) {
             if (e.x < 0) {
@@ -148,15 +148,14 @@ __device__ __forceinline__ void closest_point(const DevScene &s, const float *p,
                 trav::child_cp<D, 0>(lo[1], hi[1], p, r, h1, k1);
                 h0 = h0 && k0 <= r;
                 h1 = h1 && k1 <= r;
-                const bool sw = k1 < k0;  // push the farther first so the nearer is taken first
-                if (h0 && h1) {
-                    push[np++] = sw ? make_int2(rl, fbits(k0)) : make_int2(rr, fbits(k1));
-                    push[np++] = sw ? make_int2(rr, fbits(k1)) : make_int2(rl, fbits(k0));
-                } else if (h0) {
-                    push[np++] = make_int2(rl, fbits(k0));
-                } else if (h1) {
-                    push[np++] = make_int2(rr, fbits(k1));
-                }
+                // push the farther first so the nearer is taken first
+                const bool sw = k1 < k0;
+                const bool hf = sw ? h0 : h1, hn = sw ? h1 : h0;
+                const int2 ef = sw ? make_int2(rl, fbits(k0)) : make_int2(rr, fbits(k1));
+                const int2 en = sw ? make_int2(rr, fbits(k1)) : make_int2(rl, fbits(k0));
+                np = (int)hf + (int)hn;
+                push0 = hf ? ef : en;
+                push1 = en;
             }
         }
         R = pkt::warp_min(r);
@@ -168,8 +167,8 @@ __device__ __forceinline__ void closest_point(const DevScene &s, const float *p,
             ovf = true;
             break;
         }
-        if (np >= 1) stk[sp + before] = push[0];
-        if (np >= 2) stk[sp + before + 1] = push[1];
+        if (np >= 1) stk[sp + before] = push0;
+        if (np >= 2) stk[sp + before + 1] = push1;
         __syncwarp();
         sp += total;
     }

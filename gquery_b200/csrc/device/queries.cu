@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_sil_packet(DevScene s, gq_vecs xq
 // One query per warp (sil_warp.cuh): persistent warps take the next query of the
 // sorted order; the stack lives in dynamic shared memory (kWarpStack entries per warp).
 template <int D>
-__global__ void __launch_bounds__(kMaxBlock) k_sil_warp(DevScene s, gq_vecs xq, const float *rmax_in, int64_t n,
+__global__ void __launch_bounds__(kMaxBlock, 4) k_sil_warp(DevScene s, gq_vecs xq, const float *rmax_in, int64_t n,
                                                      const int32_t *perm, gq_sil_out o, unsigned long long *counter) {
     extern __shared__ int2 wstk[];
     const unsigned lane = threadIdx.x & 31u;
@@ -569,7 +569,7 @@ cudaError_t launch_sil(const DevScene &s, int variant, const Tune &t, gq_vecs x,
             int dev = 0, b = 0;
             cudaGetDevice(&dev);
             cudaDeviceGetAttribute(&w_sm, cudaDevAttrMultiProcessorCount, dev);
-            // up to 8 warps x 8 KB of stacks: above the 48 KB a launch may take without opting in
+            // up to 8 warps x 4 KB of stacks (the opt-in keeps larger stacks possible)
             const int most = (kMaxBlock / 32) * wsil::kWarpStack * (int)sizeof(int2);
             cudaFuncSetAttribute(s.dim == 3 ? (const void *)k_sil_warp<3> : (const void *)k_sil_warp<2>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, most);

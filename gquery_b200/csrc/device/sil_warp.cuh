@@ -31,7 +31,7 @@
 namespace gqd {
 namespace wsil {
 
-constexpr int kWarpStack = 1024;  // entries per warp (8 KB of shared memory)
+constexpr int kWarpStack = 512;  // entries per warp (4 KB of shared memory)
 constexpr int kReserve = 2 * GQ_STACK_EXACT + 2;
 
 // min over the warp of a non-negative float (or +inf) and the lowest lane holding it
@@ -79,7 +79,7 @@ __device__ __forceinline__ void closest_silhouette(const DevScene &s, const floa
         __syncwarp();
         sp -= take;
         L.r = R;
-        int2 push[2];
+        int2 push0 = make_int2(0, 0), push1 = make_int2(0, 0);  // the lane's entries, push1 on top
         int np = 0;
         if (mine && __int_as_float(e.y) <= R) {
             if (e.x < 0) {
@@ -106,10 +106,15 @@ __device__ __forceinline__ void closest_silhouette(const DevScene &s, const floa
                         hit[c] = cone_overlaps_fast<D>(P.lo[c], P.hi[c], P.ax[c], P.half[c], P.rad[c], x, dm[c]);
                     if (hit[c]) hit[c] = !snch::child_free<D>(s, P, c, x);
                 }
-                const bool sw = dm[1] < dm[0];  // push the farther first so the nearer is popped first
-                const int first = sw ? 0 : 1, second = sw ? 1 : 0;
-                if (hit[first]) push[np++] = make_int2(P.refs[first], fbits(dm[first]));
-                if (hit[second]) push[np++] = make_int2(P.refs[second], fbits(dm[second]));
+                // push the farther first so the nearer is taken first (selects, not indexed
+                // arrays, so that nothing here lives in local memory)
+                const bool sw = dm[1] < dm[0];
+                const bool hf = sw ? hit[0] : hit[1], hn = sw ? hit[1] : hit[0];
+                const int2 ef = sw ? make_int2(P.refs[0], fbits(dm[0])) : make_int2(P.refs[1], fbits(dm[1]));
+                const int2 en = sw ? make_int2(P.refs[1], fbits(dm[1])) : make_int2(P.refs[0], fbits(dm[0]));
+                np = (int)hf + (int)hn;
+                push0 = hf ? ef : en;
+                push1 = en;
             }
         }
         // new r_max of the warp
@@ -126,8 +131,8 @@ __device__ __forceinline__ void closest_silhouette(const DevScene &s, const floa
             ovf = true;
             break;
         }
-        if (np >= 1) stk[sp + before] = push[0];
-        if (np >= 2) stk[sp + before + 1] = push[1];
+        if (np >= 1) stk[sp + before] = push0;
+        if (np >= 2) stk[sp + before + 1] = push1;
         __syncwarp();
         sp += total;
     }
