@@ -136,7 +136,7 @@ struct Slot {
 struct gq_server {
     int dim = 0, device = 0, flags = 0;
     int64_t step_queries = 0, ring_bytes = 0, sil_step_queries = 0;
-    float sil_share = 0.5f;  // per silhouette slot
+    float sil_share = 0.8f;  // per silhouette slot
     std::vector<gq_scene *> scenes;
     gqd::DevScene *dev_scenes = nullptr;
     Ring ring[3];
@@ -559,7 +559,7 @@ gq_status gq_server_create(gq_scene *const *scenes, int32_t n_scenes, const gq_s
     s->flags = o.flags;
     s->step_queries = o.step_queries > 0 ? o.step_queries : (1 << 19);
     const int inflight = o.max_inflight > 0 ? o.max_inflight : 2;
-    s->sil_share = o.sil_share > 0.f && o.sil_share <= 1.f ? o.sil_share : 0.8f;
+    s->sil_share = o.sil_share > 0.f ? o.sil_share : 2.4f;  // above 1: the slots may oversubscribe
     std::vector<gqd::DevScene> views((size_t)n_scenes);
     for (int32_t i = 0; i < n_scenes; ++i) {
         gq_scene *sc = scenes[i];
@@ -598,8 +598,8 @@ gq_status gq_server_create(gq_scene *const *scenes, int32_t n_scenes, const gq_s
     if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&s->copy_st, cudaStreamNonBlocking, prio_high);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->copy_evt, cudaEventDisableTiming);
     const bool per_request = (s->flags & GQ_SERVER_PER_REQUEST) != 0;
-    const int sil_slots = per_request ? 0 : (o.sil_slots > 0 ? o.sil_slots : 2);
-    s->sil_share /= (float)std::max(sil_slots, 1);
+    const int sil_slots = per_request ? 0 : (o.sil_slots > 0 ? o.sil_slots : 3);
+    s->sil_share = std::min(1.f, s->sil_share / (float)std::max(sil_slots, 1));
     s->sil_step_queries = std::min<int64_t>(s->step_queries, o.sil_step_queries > 0 ? o.sil_step_queries : (1 << 15));
     s->slots.resize((size_t)(inflight + sil_slots));
     for (int i = 0; i < sil_slots; ++i) s->slots[(size_t)(inflight + i)].sil_only = true;

@@ -100,16 +100,18 @@ class Server:
     ring_queries: ring capacity per kind (cp, ray, sil); step_queries: most queries of
     one kind per step and the largest request; max_inflight: closest-point / ray step
     slots (streams); silhouette steps have sil_slots slots of their own holding at most
-    sil_share of the GPU together, sil_step_queries queries per step.  Served requests
-    are sparse (few queries per scene per step), so closest points default to one lane
-    per query in the reference order ("exact": cheaper than a warp-coherent walk when
-    neighbours are far apart) and silhouettes to one query per warp ("warp": bounds the
+    sil_share of the GPU together (above 1 they may oversubscribe it; each slot at most
+    all of it), sil_step_queries queries per step.  Served requests are sparse (few
+    queries per scene per step), so closest points default to one lane per query in the
+    reference order with long traversals taken over one per warp ("split": cheaper than
+    a warp-coherent walk when neighbours are far apart, and the slowest query no longer
+    sets the step time) and silhouettes to one query per warp ("warp": bounds the
     latency of far-reaching ones)."""
 
     def __init__(self, scenes: Sequence[Scene], *, budget_bytes: int = 0, ring_queries=(1 << 22,) * 3,
                  step_queries: int = 1 << 19, max_inflight: int = 2, per_request: bool = False,
                  cp_variant: str = "split", ray_variant: str = "wide8", sil_variant: str = "warp",
-                 sil_share: float = 0.8, sil_slots: int = 2, sil_step_queries: int = 1 << 15):
+                 sil_share: float = 2.4, sil_slots: int = 3, sil_step_queries: int = 1 << 15):
         self.scenes = list(scenes)
         self.dim = self.scenes[0].dim
         flags = (L.SERVER_PER_REQUEST if per_request else 0) | \
