@@ -178,6 +178,8 @@ __device__ __forceinline__ void sil_warp_phase(const DevScene *scenes, int n_sce
 // Closest-point queries whose per-lane traversal passes this many node visits are
 // handed to k_cp_heavy (cp_mode 2).
 constexpr int kHeavyVisits = 1024;
+// Node visits (closest points, rays) or steps (silhouettes) between refills in k_batch.
+constexpr int kBudget = 32;
 // Silhouette queries whose per-lane traversal passes this many steps (node visits and
 // silhouette tests) are handed to k_sil_heavy (sil_mode 3).
 constexpr int kHeavySilSteps = 2048;
@@ -192,7 +194,10 @@ constexpr int kHeavySilSteps = 2048;
 // to the next phase when the current one has no unclaimed work, so the phases' tails
 // overlap.  counter[0..2]: claims per phase, counter[3] / [5]: closest points /
 // silhouettes handed over.
-template <int D, bool RAYW>
+// SPLIT: compiled with the hand-over of cp_mode 2 / sil_mode 3 (its state costs
+// registers that the other modes need not carry); SIL: compiled with the silhouette
+// phase (steps without silhouettes, such as the server's general ones, leave it out).
+template <int D, bool RAYW, bool SPLIT, bool SIL>
 __global__ void __launch_bounds__(kBlock) k_batch(const DevScene *scenes, int n_scenes, BatchKind cp, gq_cp_out cp_out,
                                                   BatchKind ray, gq_ray_out ray_out, BatchKind sil,
                                                   gq_sil_out sil_out, int cp_mode, int sil_mode,
@@ -251,7 +256,7 @@ __global__ void __launch_bounds__(kBlock) k_batch(const DevScene *scenes, int n_
         int64_t qi = 0;
         int visits = 0;
         bool handed = false;
-        const bool split = cp_mode == 2;
+        const bool split = SPLIT && cp_mode == 2;
         const gq_vecs none{};
         refill(
             cp.n, &counter[0], budget,
@@ -317,6 +322,7 @@ __global__ void __launch_bounds__(kBlock) k_batch(const DevScene *scenes, int n_
             [&]() { trav::lane_write(*sc, L, qi, ray.n, gq_cp_out{}, ray_out); });
     }
     // ---------------- phase 3: silhouettes ----------------
+    if (!SIL) return;
     if (sil.n > 0 && sil_mode == 2) {
         sil_warp_phase<D>(scenes, n_scenes, sil, sil_out, counter, err);
     } else if (sil.n > 0 && sil_mode == 1) {
@@ -363,7 +369,7 @@ __global__ void __launch_bounds__(kBlock) k_batch(const DevScene *scenes, int n_
         int64_t qi = 0;
         int steps = 0;
         bool handed = false;
-        const bool split = sil_mode == 3;
+        const bool split = SPLIT && sil_mode == 3;
         refill(
             sil.n, &counter[2], budget,
             [&](int64_t i) {
@@ -518,24 +524,32 @@ cudaError_t launch_batch(const DevScene *scenes_dev, int n_scenes, BatchKind kin
         return cudaGetLastError();
     }
     const int mi = smem ? 1 : 0;
-    static int bps_m[2] = {0, 0}, n_sm = 0;
-    if (!bps_m[mi]) {
+    const bool split = cp_mode == 2 || sil_mode == 3, sil = kinds[2].n > 0;
+    const int si = (split ? 1 : 0) + (sil ? 2 : 0);
+    const void *kern = split ? (sil ? (const void *)k_batch<D, RAYW, true, true>
+                                    : (const void *)k_batch<D, RAYW, true, false>)
+                             : (sil ? (const void *)k_batch<D, RAYW, false, true>
+                                    : (const void *)k_batch<D, RAYW, false, false>);
+    static int bps_m[2][4] = {}, n_sm = 0;
+    if (!bps_m[mi][si]) {
         int dev = 0, b = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch<D, RAYW>, kBlock, smem);
-        bps_m[mi] = b < 1 ? 1 : b;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, kBlock, smem);
+        bps_m[mi][si] = b < 1 ? 1 : b;
     }
-    const int bps = bps_m[mi];
+    const int bps = bps_m[mi][si];
     const int64_t most = std::max(kinds[0].n, std::max(kinds[1].n, kinds[2].n));
     if (most <= 0) return cudaSuccess;
     int64_t want = std::min<int64_t>((int64_t)bps * n_sm,
                                      std::max<int64_t>((most + kBlock - 1) / kBlock, smem ? (kinds[2].n * 32 + kBlock - 1) / kBlock : 0));
     if (grid_share > 0.f && grid_share < 1.f)
         want = std::min<int64_t>(want, std::max<int64_t>(1, (int64_t)(grid_share * (float)(bps * n_sm))));
-    k_batch<D, RAYW><<<dim3((unsigned)want), kBlock, smem, st>>>(scenes_dev, n_scenes, kinds[0], cp_out, kinds[1],
-                                                                 ray_out, kinds[2], sil_out, cp_mode, sil_mode, 32,
-                                                                 counter, heavy, heavy_r, sheavy, sheavy_r, err);
+    void *args[] = {(void *)&scenes_dev, (void *)&n_scenes, (void *)&kinds[0], (void *)&cp_out, (void *)&kinds[1],
+                    (void *)&ray_out,    (void *)&kinds[2], (void *)&sil_out, (void *)&cp_mode, (void *)&sil_mode,
+                    (void *)&kBudget,    (void *)&counter, (void *)&heavy,    (void *)&heavy_r, (void *)&sheavy,
+                    (void *)&sheavy_r,   (void *)&err};
+    cudaLaunchKernel(kern, dim3((unsigned)want), dim3(kBlock), args, smem, st);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     // the handed-over queries: persistent grids of one query per warp
