@@ -52,7 +52,7 @@ __device__ __forceinline__ void sil_write(const DevScene &s, const snch::Lane<D>
 // Warp-coherent closest silhouette (sil_packet.cuh): persistent warps take 32
 // consecutive queries of the sorted order at a time.
 template <int D>
-__global__ void __launch_bounds__(kMaxBlock) k_sil_packet(DevScene s, gq_vecs xq, const float *rmax_in, int64_t n,
+__global__ void __launch_bounds__(kMaxBlock, 4) k_sil_packet(DevScene s, gq_vecs xq, const float *rmax_in, int64_t n,
                                                        const int32_t *perm, gq_sil_out o, unsigned long long *counter) {
     const unsigned lane = threadIdx.x & 31u;
     snch::Stack stk;
