@@ -150,6 +150,8 @@ SIGNATURES = {
     "gq_closest_point_brute": (C.c_int32, [C.c_void_p, Vecs, C.c_int64, C.POINTER(CpOut), C.c_void_p]),
     "gq_intersect_brute": (C.c_int32, [C.c_void_p, Vecs, Vecs, C.c_void_p, C.c_int64, C.POINTER(RayOut),
                                        C.c_void_p]),
+    "gq_closest_silhouette_brute": (C.c_int32, [C.c_void_p, Vecs, C.c_void_p, C.c_int64, C.POINTER(SilOut),
+                                                C.c_void_p]),
     "gq_brute_f64": (C.c_int32, [C.c_void_p, C.c_int32, Vecs, Vecs, C.c_int64, C.c_void_p, C.c_void_p,
                                  C.c_void_p]),
     "gq_scene_device_error": (C.c_int32, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)]),

@@ -667,6 +667,51 @@ gq_status gq_intersect_brute(const gq_scene *s, gq_vecs origin, gq_vecs dir, con
     return GQ_OK;
 }
 
+// Uploads (once) the list closest_silhouette_baseline scans: a Mesh's unique edges in
+// first-appearance order (build_flat_silhouette_edges), a Polyline's silhouette
+// vertices (Polyline.configure_silhouette).
+static gq_status ensure_base_sils(gq_scene *s) {
+    std::lock_guard<std::mutex> lk(s->base_mu);
+    if (s->n_base_sils >= 0) return GQ_OK;
+    try {
+        gq_status st = GQ_OK;
+        if (s->dim == 2) {
+            PrimSource<2> src{s->verts.data(), s->nv, s->index.data(), s->np};
+            const std::vector<gqb::SilVertex> raw = gqb::build_polyline_silhouettes(src);
+            std::vector<gq_silv_t> rec(raw.size());
+            for (size_t k = 0; k < raw.size(); ++k) gqb::device_silhouette(raw[k], rec[k]);
+            if (!rec.empty()) st = s->upload(rec, &s->base_sils);
+            if (st == GQ_OK) s->n_base_sils = (int64_t)rec.size();
+        } else {
+            PrimSource<3> src{s->verts.data(), s->nv, s->index.data(), s->np};
+            const std::vector<gqb::SilEdge> raw = gqb::build_silhouette_edges(src, nullptr);
+            std::vector<gq_sile_t> rec(raw.size());
+            for (size_t k = 0; k < raw.size(); ++k) gqb::device_silhouette(raw[k], rec[k]);
+            if (!rec.empty()) st = s->upload(rec, &s->base_sils);
+            if (st == GQ_OK) s->n_base_sils = (int64_t)rec.size();
+        }
+        return st;
+    } catch (const std::bad_alloc &) {
+        return fail(GQ_ERR_NOMEM, "out of host memory building the silhouette list");
+    }
+}
+
+gq_status gq_closest_silhouette_brute(const gq_scene *s, gq_vecs x, const float *r_max, int64_t n,
+                                      const gq_sil_out *out, void *stream) {
+    if (!s || !out) return fail(GQ_ERR_INVALID, "null scene or output");
+    if (n < 0) return fail(GQ_ERR_INVALID, "negative query count");
+    if (n == 0) return GQ_OK;
+    if (!vecs_ok(x)) return fail(GQ_ERR_INVALID, "null query array");
+    if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "scene was built without a device copy");
+    DeviceGuard g(s->device);
+    if (!g.ok) return fail(GQ_ERR_CUDA, "cannot select the scene's device");
+    gq_status st = ensure_base_sils(const_cast<gq_scene *>(s));
+    if (st != GQ_OK) return st;
+    cudaError_t e = gqd::launch_sil_brute(s->dev, s->base_sils, s->n_base_sils, x, r_max, n, *out, (cudaStream_t)stream);
+    if (e != cudaSuccess) return fail_cuda(e, "closest_silhouette_brute launch");
+    return GQ_OK;
+}
+
 gq_status gq_brute_f64(const gq_scene *s, int32_t kind, gq_vecs a, gq_vecs b, int64_t n, double *out_d,
                        int32_t *out_id, void *stream) {
     if (!s || !out_d || !out_id) return fail(GQ_ERR_INVALID, "null argument");

@@ -339,6 +339,30 @@ __global__ void __launch_bounds__(kBlock) k_ray_brute(DevScene s, gq_vecs x, gq_
 }
 
 // ===========================================================================
+// closest_silhouette_baseline (mesh.py:124-135, polyline.py:212-223): every query
+// tests the scene's silhouette list in order and keeps the first strictly nearest
+// silhouette (the same per-silhouette test and acceptance as the SNCH traversal, so
+// snch::test_silhouette does it; s.sils points at the baseline list here).
+template <int D>
+__global__ void __launch_bounds__(kBlock) k_sil_brute(DevScene s, int64_t n_sil, gq_vecs x, const float *rmax_in,
+                                                      int64_t n, gq_sil_out o) {
+    const int64_t qi = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (qi >= n) return;
+    snch::Lane<D> L;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        L.x[k] = qget(x, qi, k);
+        L.bp[k] = 0.f;
+    }
+    L.r = rmax_in ? rmax_in[qi] : kInf;
+    L.found = false;
+    L.ovf = false;
+    L.bd = 0.f;
+    L.bid = 0;
+    for (int64_t j = 0; j < n_sil; ++j) snch::test_silhouette<D>(s, L, (int)j);
+    sil_write<D>(s, L, qi, n, o);
+}
+
 // FP64 brute force (error reference).  Primitives are staged through shared
 // memory in tiles; one thread per query.
 // ===========================================================================
@@ -640,6 +664,17 @@ cudaError_t launch_ray_brute(const DevScene &s, gq_vecs x, gq_vecs v, const floa
         k_ray_brute<3><<<grid_for(n), kBlock, 0, st>>>(s, x, v, r_max, n, o);
     else
         k_ray_brute<2><<<grid_for(n), kBlock, 0, st>>>(s, x, v, r_max, n, o);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sil_brute(const DevScene &s, const void *sils, int64_t n_sil, gq_vecs x, const float *r_max,
+                             int64_t n, const gq_sil_out &o, cudaStream_t st) {
+    DevScene b = s;
+    b.sils = sils;
+    if (s.dim == 3)
+        k_sil_brute<3><<<grid_for(n), kBlock, 0, st>>>(b, n_sil, x, r_max, n, o);
+    else
+        k_sil_brute<2><<<grid_for(n), kBlock, 0, st>>>(b, n_sil, x, r_max, n, o);
     return cudaGetLastError();
 }
 

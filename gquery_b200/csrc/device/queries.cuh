@@ -65,6 +65,10 @@ cudaError_t launch_cp_packet(const DevScene &s, int layout, const Tune &t, gq_ve
 cudaError_t launch_sil(const DevScene &s, int variant, const Tune &t, gq_vecs x, const float *r_max, int64_t n,
                        const int32_t *perm, const gq_sil_out &o, unsigned long long *counter, cudaStream_t st);
 cudaError_t launch_cp_brute(const DevScene &s, gq_vecs q, int64_t n, const gq_cp_out &o, cudaStream_t st);
+// closest_silhouette_baseline over `sils` (n_sil records of the scene's silhouette
+// layout, in the reference's list order) instead of the SNCH leaf lists.
+cudaError_t launch_sil_brute(const DevScene &s, const void *sils, int64_t n_sil, gq_vecs x, const float *r_max,
+                             int64_t n, const gq_sil_out &o, cudaStream_t st);
 cudaError_t launch_ray_brute(const DevScene &s, gq_vecs x, gq_vecs v, const float *r_max, int64_t n,
                              const gq_ray_out &o, cudaStream_t st);
 cudaError_t launch_brute_f64(const DevScene &s, int kind, gq_vecs a, gq_vecs b, int64_t n, double *out_d,

@@ -384,6 +384,38 @@ void snch_node_bounds(const BvhTree<D> &t, const SnchTree<D> &s, DeviceImage<D> 
 
 }  // namespace
 
+void device_silhouette(const SilVertex &x, gq_silv_t &r) {
+    std::memset(&r, 0, sizeof r);
+    r.ax = x.v[0].v[0]; r.ay = x.v[0].v[1];
+    r.bx = x.v[1].v[0]; r.by = x.v[1].v[1];
+    r.cx = x.v[2].v[0]; r.cy = x.v[2].v[1];
+    r.prim = (int32_t)(float)x.prim;
+    // silhouette_vertex.py:48: Int(Float(index)) != -1 for both neighbours
+    const bool ok = ((int64_t)(float)x.idx[0] != -1) && ((int64_t)(float)x.idx[2] != -1);
+    r.flags = ok ? GQ_ITEM_VALID : 0;
+}
+
+void device_silhouette(const SilEdge &x, gq_sile_t &r) {
+    std::memset(&r, 0, sizeof r);
+    // SilhouetteEdges view (silhouette_edge.py:75-86): c = v[0], a = v[1], b = v[2], d = v[3]
+    r.ax = x.v[1].v[0]; r.ay = x.v[1].v[1]; r.az = x.v[1].v[2];
+    r.bx = x.v[2].v[0]; r.by = x.v[2].v[1]; r.bz = x.v[2].v[2];
+    const float cx = x.v[0].v[0], cy = x.v[0].v[1], cz = x.v[0].v[2];
+    const float dx = x.v[3].v[0], dy = x.v[3].v[1], dz = x.v[3].v[2];
+    // n0 = normalize(cross(b - a, c - a)), n1 = normalize(cross(d - a, b - a))
+    sil_face_normal(r.bx - r.ax, r.by - r.ay, r.bz - r.az, cx - r.ax, cy - r.ay, cz - r.az, r.n0x, r.n0y, r.n0z);
+    sil_face_normal(dx - r.ax, dy - r.ay, dz - r.az, r.bx - r.ax, r.by - r.ay, r.bz - r.az, r.n1x, r.n1y, r.n1z);
+    r.prim = (int32_t)(float)x.prim;
+    // silhouette_edge.py:56-57: boundary marker index == -1 never occurs (size_t storage)
+    const bool boundary = ((int64_t)(float)x.idx[0] == -1) || ((int64_t)(float)x.idx[3] == -1);
+    r.flags = boundary ? GQ_ITEM_VALID : 0;  // for edges the bit means "always a silhouette"
+    // spans of the pre-test that skips edges which are certainly no silhouette
+    r.span0 = sil_span(r.n0x, r.n0y, r.n0z, r.ax, r.ay, r.az, r.bx, r.by, r.bz);
+    r.span1 = sil_span(r.n1x, r.n1y, r.n1z, r.ax, r.ay, r.az, r.bx, r.by, r.bz);
+    if (!boundary && sil_filter_usable(r.n0x, r.n0y, r.n0z, r.n1x, r.n1y, r.n1z, r.span0, r.span1))
+        r.flags |= GQ_SIL_FILTER;
+}
+
 template <int D>
 void flatten_snch(const BvhTree<D> &t, const SnchTree<D> &s, DeviceImage<D> &img, int n_threads) {
     const auto rank = interior_ranks(t);
@@ -423,40 +455,7 @@ void flatten_snch(const BvhTree<D> &t, const SnchTree<D> &s, DeviceImage<D> &img
     img.sroot_ref = ref_of(0);
 
     img.sils.assign(s.ordered.size(), typename DeviceImage<D>::Sil{});
-    for (size_t k = 0; k < s.ordered.size(); ++k) {
-        const auto &x = s.raw[s.ordered[k]];
-        auto &r = img.sils[k];
-        std::memset(&r, 0, sizeof r);
-        if constexpr (D == 2) {
-            r.ax = x.v[0].v[0]; r.ay = x.v[0].v[1];
-            r.bx = x.v[1].v[0]; r.by = x.v[1].v[1];
-            r.cx = x.v[2].v[0]; r.cy = x.v[2].v[1];
-            r.prim = (int32_t)(float)x.prim;
-            // silhouette_vertex.py:48: Int(Float(index)) != -1 for both neighbours
-            const bool ok = ((int64_t)(float)x.idx[0] != -1) && ((int64_t)(float)x.idx[2] != -1);
-            r.flags = ok ? GQ_ITEM_VALID : 0;
-        } else {
-            // SilhouetteEdges view (silhouette_edge.py:75-86): c = v[0], a = v[1], b = v[2], d = v[3]
-            r.ax = x.v[1].v[0]; r.ay = x.v[1].v[1]; r.az = x.v[1].v[2];
-            r.bx = x.v[2].v[0]; r.by = x.v[2].v[1]; r.bz = x.v[2].v[2];
-            const float cx = x.v[0].v[0], cy = x.v[0].v[1], cz = x.v[0].v[2];
-            const float dx = x.v[3].v[0], dy = x.v[3].v[1], dz = x.v[3].v[2];
-            // n0 = normalize(cross(b - a, c - a)), n1 = normalize(cross(d - a, b - a))
-            sil_face_normal(r.bx - r.ax, r.by - r.ay, r.bz - r.az, cx - r.ax, cy - r.ay, cz - r.az, r.n0x, r.n0y,
-                            r.n0z);
-            sil_face_normal(dx - r.ax, dy - r.ay, dz - r.az, r.bx - r.ax, r.by - r.ay, r.bz - r.az, r.n1x, r.n1y,
-                            r.n1z);
-            r.prim = (int32_t)(float)x.prim;
-            // silhouette_edge.py:56-57: boundary marker index == -1 never occurs (size_t storage)
-            const bool boundary = ((int64_t)(float)x.idx[0] == -1) || ((int64_t)(float)x.idx[3] == -1);
-            r.flags = boundary ? GQ_ITEM_VALID : 0;  // for edges the bit means "always a silhouette"
-            // spans of the pre-test that skips edges which are certainly no silhouette
-            r.span0 = sil_span(r.n0x, r.n0y, r.n0z, r.ax, r.ay, r.az, r.bx, r.by, r.bz);
-            r.span1 = sil_span(r.n1x, r.n1y, r.n1z, r.ax, r.ay, r.az, r.bx, r.by, r.bz);
-            if (!boundary && sil_filter_usable(r.n0x, r.n0y, r.n0z, r.n1x, r.n1y, r.n1z, r.span0, r.span1))
-                r.flags |= GQ_SIL_FILTER;
-        }
-    }
+    for (size_t k = 0; k < s.ordered.size(); ++k) device_silhouette(s.raw[s.ordered[k]], img.sils[k]);
     for (size_t i = 0; i < t.nodes.size(); ++i) {
         const auto &sn = s.nodes[i];
         if (t.nodes[i].n_prims > 0 && sn.n_sil > 0) img.sils[(size_t)(sn.sil_offset + sn.n_sil - 1)].flags |= GQ_ITEM_LAST;

@@ -45,6 +45,10 @@ void flatten_bvh(const PrimSource<D> &src, const BvhTree<D> &t, DeviceImage<D> &
 template <int D>
 void flatten_wide(const BvhTree<D> &t, DeviceImage<D> &img);
 
+// One silhouette in the device layout (also used for the brute-force silhouette list).
+void device_silhouette(const SilVertex &x, gq_silv_t &r);
+void device_silhouette(const SilEdge &x, gq_sile_t &r);
+
 template <int D>
 void flatten_snch(const BvhTree<D> &t, const SnchTree<D> &s, DeviceImage<D> &img, int n_threads = 1);
 

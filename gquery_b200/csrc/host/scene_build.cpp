@@ -2,9 +2,12 @@
 #include "scene_build.hpp"
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <thread>
 #include <unordered_set>
+
+#include "../gq_fmath.h"
 
 namespace gqb {
 
@@ -227,6 +230,45 @@ BvhTree<D> build_bvh(const PrimSource<D> &src, int max_prims_in_node, int n_thre
 // ---------------------------------------------------------------------------
 // Silhouettes and normal cones (src/shapes/snch.cpp, silhouette_edge.cpp)
 // ---------------------------------------------------------------------------
+
+std::vector<SilVertex> build_polyline_silhouettes(const PrimSource<2> &src) {
+    const int64_t nv = src.nv;
+    std::vector<int64_t> prev((size_t)nv, -1), next((size_t)nv, -1), order;
+    std::vector<uint8_t> seen((size_t)nv, 0);
+    auto visit = [&](int64_t v) {
+        if (!seen[(size_t)v]) {
+            seen[(size_t)v] = 1;
+            order.push_back(v);
+        }
+    };
+    for (int64_t e = 0; e < src.np; ++e) {  // polyline.py:60-73
+        const int64_t a = src.index[2 * e], b = src.index[2 * e + 1];
+        visit(a);
+        visit(b);
+        next[(size_t)a] = b;
+        prev[(size_t)b] = a;
+    }
+    std::vector<SilVertex> out;
+    for (size_t i = 0; i < order.size(); ++i) {  // polyline.py:82-97
+        const int64_t cur = order[i], p = prev[(size_t)cur], n = next[(size_t)cur];
+        if (p == -1 || n == -1) continue;
+        SilVertex s;
+        s.v[0] = vert2(src, p);
+        s.v[1] = vert2(src, cur);
+        s.v[2] = vert2(src, n);
+        s.idx[0] = (uint64_t)p;
+        s.idx[1] = (uint64_t)cur;
+        s.idx[2] = (uint64_t)n;
+        s.prim = (uint64_t)i;
+        // polyline.py:111-118: drop nearly collinear vertices (normalize = v / |v| in FP32)
+        const float e1x = s.v[1].v[0] - s.v[0].v[0], e1y = s.v[1].v[1] - s.v[0].v[1];
+        const float e2x = s.v[2].v[0] - s.v[1].v[0], e2y = s.v[2].v[1] - s.v[1].v[1];
+        const float i1 = gq_rsqrt(gq_dot2(e1x, e1y, e1x, e1y)), i2 = gq_rsqrt(gq_dot2(e2x, e2y, e2x, e2y));
+        const float col = std::fabs(gq_dot2(e1x * i1, e1y * i1, e2x * i2, e2y * i2));
+        if (col < 0.99999f) out.push_back(s);
+    }
+    return out;
+}
 
 std::vector<SilEdge> build_silhouette_edges(const PrimSource<3> &src,
                                             std::vector<uint32_t> *face_edge_out) {

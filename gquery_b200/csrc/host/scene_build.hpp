@@ -108,6 +108,13 @@ BvhTree<D> build_bvh(const PrimSource<D> &src, int max_prims_in_node, int n_thre
 template <int D>
 SnchTree<D> build_snch(const PrimSource<D> &src, const BvhTree<D> &bvh, int n_threads);
 
+// The silhouette list of a Polyline (Polyline.configure_silhouette, polyline.py:44-122):
+// vertices in order of first appearance in the edge list that have both a predecessor
+// and a successor, without those whose two edges are nearly collinear
+// (|normalize(b - a) . normalize(c - b)| >= 1 - 1e-5 in FP32); prim = position in the
+// first-appearance order.  closest_silhouette_baseline scans this list.
+std::vector<SilVertex> build_polyline_silhouettes(const PrimSource<2> &src);
+
 // Raw silhouette edges in first-appearance edge order (silhouette_edge.cpp:5-60).
 // face_edge[3*f + k] receives the edge index of face f's k-th edge (k -> k+1).
 std::vector<SilEdge> build_silhouette_edges(const PrimSource<3> &src,

@@ -62,6 +62,10 @@ struct gq_scene {
     bool trees_ready = true;
     bool gpu_built = false;  // tree built on the device: no host SAH trees to describe it
     std::mutex tree_mu;
+    // closest_silhouette_baseline's list (Mesh / Polyline .silhouettes), uploaded on first use
+    const void *base_sils = nullptr;
+    int64_t n_base_sils = -1;
+    std::mutex base_mu;
 
     ~gq_scene() {
         if (device < 0 || allocs.empty()) return;

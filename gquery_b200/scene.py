@@ -301,6 +301,16 @@ class Scene:
         L.check(L.lib().gq_intersect_brute(self._h, vx, vv, _ptr(rm), n, C.byref(o), _stream_handle(stream)))
         return rec
 
+    def closest_silhouette_brute(self, x, r_max=math.inf, *, stream=None):
+        """closest_silhouette_baseline (polyline.py:212-223, mesh.py:124-135): every
+        silhouette of the shape's list in order, the first strictly nearest kept."""
+        tx, n, vx = self._points(x)
+        rm = self._rmax(r_max, n)
+        rec = self.alloc_sil(n)
+        o = L.SilOut(_ptr(rec.valid), _ptr(rec.p), _ptr(rec.d), _ptr(rec.prim_id))
+        L.check(L.lib().gq_closest_silhouette_brute(self._h, vx, _ptr(rm), n, C.byref(o), _stream_handle(stream)))
+        return rec
+
     def brute_f64(self, kind: str, a, b=None, *, stream=None):
         """FP64 brute force: (distance or ray parameter [float64], primitive id [int32])."""
         ta, n, va = self._points(a)

@@ -49,6 +49,9 @@ class _Shape:
     def intersect_baseline(self, p, v, r_max=math.inf):
         return self.scene.intersect_brute(p, v, r_max)
 
+    def closest_silhouette_baseline(self, x, r_max=math.inf):
+        return self.scene.closest_silhouette_brute(x, r_max)
+
 
 class Polyline(_Shape):
     """2D polyline: ``Polyline(vertices [2, V] float32, indices [2, E] int32)`` (polyline.py:20)."""

@@ -230,6 +230,13 @@ gq_status gq_closest_silhouette(const gq_scene *scene, gq_vecs x, const float *r
 gq_status gq_closest_point_brute(const gq_scene *scene, gq_vecs q, int64_t n, const gq_cp_out *out, void *stream);
 gq_status gq_intersect_brute(const gq_scene *scene, gq_vecs origin, gq_vecs dir, const float *r_max, int64_t n,
                              const gq_ray_out *out, void *stream);
+/* closest_silhouette_baseline (mesh.py:124-135, polyline.py:212-223): every query scans
+ * the shape's silhouette list in order (a Mesh's unique edges as build_flat_silhouette_edges
+ * lists them; a Polyline's silhouette vertices as Polyline.configure_silhouette keeps them,
+ * polyline.py:44-122) and keeps the first strictly nearest silhouette.  r_max: device [n]
+ * or NULL for +inf.  The list is built and uploaded on the scene's first call. */
+gq_status gq_closest_silhouette_brute(const gq_scene *scene, gq_vecs x, const float *r_max, int64_t n,
+                                      const gq_sil_out *out, void *stream);
 
 /* FP64 brute force used to state the error of the FP32 paths: nearest distance
  * (closest point) or nearest ray parameter (+inf on a miss) and its primitive. */

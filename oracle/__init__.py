@@ -146,3 +146,29 @@ def brute_intersect3d(verts, index, x, v, threads=0):
        C.c_void_p(x.ctypes.data), C.c_void_p(v.ctypes.data), C.c_int64(x.shape[0]), C.c_void_p(t.ctypes.data),
        C.c_void_p(ids.ctypes.data), C.c_int(threads or n_threads()))
     return t, ids
+
+
+def closest_silhouette_brute(dim, x, r_max=None, threads=0, *, vertices=None, indices=None, raw_silhouettes=None):
+    """closest_silhouette_baseline: the first strictly nearest silhouette of the shape's
+    list.  2D: the Polyline list built from vertices [nv, 2] / indices [ne, 2]
+    (Polyline.configure_silhouette); 3D: the raw edges in the reference's flat layout
+    (build_flat_silhouette_edges, 19 floats per edge)."""
+    x = _f(x).reshape(-1, dim)
+    rm = None if r_max is None else _f(np.broadcast_to(np.asarray(r_max, np.float32), (x.shape[0],)))
+    nq = x.shape[0]
+    f = np.zeros((nq, _KF[("sil", dim)]), np.float32)
+    i = np.zeros((nq, 3), np.int32)
+    if dim == 2:
+        v = _f(vertices).reshape(-1, 2)
+        e = np.ascontiguousarray(indices, dtype=np.int32).reshape(-1, 2)
+        fn = lib().orc_sil_brute2d
+        args = [v, v.shape[0], e, e.shape[0], x, rm, nq]
+    else:
+        s = _f(raw_silhouettes).reshape(-1)
+        fn = lib().orc_sil_brute3d
+        args = [s, s.size // 19, x, rm, nq]
+    fn.restype = None
+    cargs = [C.c_void_p(None) if a is None else C.c_void_p(a.ctypes.data) if isinstance(a, np.ndarray)
+             else C.c_int64(a) for a in args]
+    fn(*cargs, C.c_void_p(f.ctypes.data), C.c_void_p(i.ctypes.data), C.c_int(threads or n_threads()))
+    return _split(dim, "sil", f, i)

@@ -868,6 +868,75 @@ static double d_cp_triangle(D3 p, D3 a, D3 b, D3 c) {
 
 }  // namespace
 
+// closest_silhouette_baseline (mesh.py:124-135, polyline.py:212-223): the shape's
+// silhouette list in order, the first strictly nearest silhouette kept.  The per-
+// silhouette test is called with the current minimum as its r_max, which accepts
+// exactly what "valid and d < d_min" accepts.
+template <int D>
+static void sil_brute_one(const float *S, int64_t n_sil, const float *xq, float r_max, Out o, int64_t q) {
+    using V = std::conditional_t<D == 2, V2, V3>;
+    V x;
+    memcpy(&x, xq, sizeof(V));
+    float d_min = r_max;
+    bool found = false;
+    V best_p;
+    memset(&best_p, 0, sizeof best_p);
+    float best_d = 0.f;
+    int best_id = 0;
+    for (int64_t j = 0; j < n_sil; ++j) {
+        V p;
+        float d;
+        bool ok;
+        if constexpr (D == 2)
+            ok = sil_vertex(S + 10 * j, x, d_min, &p, &d);
+        else
+            ok = sil_edge(S + 19 * j, x, d_min, &p, &d);
+        if (ok && d < d_min) {
+            d_min = d;
+            found = true;
+            best_p = p;
+            best_d = d;
+            best_id = (D == 2) ? I(S[10 * j + 9]) : I(S[19 * j + 18]);
+        }
+    }
+    float *f = o.f + q * o.kf;
+    int32_t *ii = o.i + q * 3;
+    memset(f, 0, sizeof(float) * o.kf);
+    ii[0] = ii[1] = ii[2] = 0;
+    if (found) {
+        memcpy(f, &best_p, sizeof(V));
+        f[D] = best_d;
+        ii[0] = 1;
+        ii[1] = best_id;
+    }
+}
+
+// Polyline.configure_silhouette (polyline.py:44-122) as 10-float SilhouetteVertex
+// records (a, b, c, indices, index): vertices in order of first appearance in the edge
+// list with both a predecessor and a successor, nearly collinear ones dropped.
+static std::vector<float> polyline_silhouettes(const float *V, int64_t nv, const int32_t *E, int64_t ne) {
+    std::vector<int64_t> prev((size_t)nv, -1), next((size_t)nv, -1), order;
+    std::vector<char> seen((size_t)nv, 0);
+    for (int64_t e = 0; e < ne; ++e) {
+        const int64_t a = E[2 * e], b = E[2 * e + 1];
+        if (!seen[(size_t)a]) seen[(size_t)a] = 1, order.push_back(a);
+        if (!seen[(size_t)b]) seen[(size_t)b] = 1, order.push_back(b);
+        next[(size_t)a] = b;
+        prev[(size_t)b] = a;
+    }
+    std::vector<float> r;
+    for (size_t i = 0; i < order.size(); ++i) {
+        const int64_t c = order[i], p = prev[(size_t)c], n = next[(size_t)c];
+        if (p == -1 || n == -1) continue;
+        const V2 p0{V[2 * p], V[2 * p + 1]}, p1{V[2 * c], V[2 * c + 1]}, p2{V[2 * n], V[2 * n + 1]};
+        const float col = fabsf(dot(normalize(sub(p1, p0)), normalize(sub(p2, p1))));
+        if (!(col < 0.99999f)) continue;
+        const float rec[10] = {p0.x, p0.y, p1.x, p1.y, p2.x, p2.y, (float)p, (float)c, (float)n, (float)i};
+        r.insert(r.end(), rec, rec + 10);
+    }
+    return r;
+}
+
 extern "C" {
 
 int orc_version(void) { return 1; }
@@ -922,6 +991,20 @@ void orc_sil3d(const float *N, const float *S, const float *x, const float *rmax
                int32_t *i_out, int32_t *counts, int nthreads) {
     Out o{f_out, i_out, counts, 4};
     parallel_for(nq, nthreads, [&](int64_t i) { sil_one<3>(N, S, x + 3 * i, rmax ? rmax[i] : INF, o, i); });
+}
+
+void orc_sil_brute2d(const float *V, int64_t nv, const int32_t *E, int64_t ne, const float *x, const float *rmax,
+                     int64_t nq, float *f_out, int32_t *i_out, int nthreads) {
+    const std::vector<float> S = polyline_silhouettes(V, nv, E, ne);
+    const int64_t n_sil = (int64_t)S.size() / 10;
+    Out o{f_out, i_out, nullptr, 3};
+    parallel_for(nq, nthreads,
+                 [&](int64_t i) { sil_brute_one<2>(S.data(), n_sil, x + 2 * i, rmax ? rmax[i] : INF, o, i); });
+}
+void orc_sil_brute3d(const float *S, int64_t n_sil, const float *x, const float *rmax, int64_t nq, float *f_out,
+                     int32_t *i_out, int nthreads) {
+    Out o{f_out, i_out, nullptr, 4};
+    parallel_for(nq, nthreads, [&](int64_t i) { sil_brute_one<3>(S, n_sil, x + 3 * i, rmax ? rmax[i] : INF, o, i); });
 }
 
 // FP64 brute force over the raw (unordered) primitives.  verts [nv][D], idx [np][D].
