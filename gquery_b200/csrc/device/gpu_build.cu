@@ -16,6 +16,8 @@
 
 #include "gpu_build.cuh"
 
+#include "../sil_filter.h"
+
 namespace gqd {
 
 namespace {
@@ -122,7 +124,8 @@ __device__ __forceinline__ int delta(const uint64_t *k, int64_t n, int64_t i, in
 }
 
 // Karras 2012, internal node i of n - 1; child references: internal >= 0, leaf = ~slot.
-__global__ void k_hierarchy(const uint64_t *k, int64_t n, int2 *child, int32_t *parent_int, int32_t *parent_leaf) {
+__global__ void k_hierarchy(const uint64_t *k, int64_t n, int2 *child, int32_t *parent_int, int32_t *parent_leaf,
+                            int2 *range) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n - 1) return;
     const int d = (delta(k, n, i, i + 1) - delta(k, n, i, i - 1)) >= 0 ? 1 : -1;
@@ -144,6 +147,7 @@ __global__ void k_hierarchy(const uint64_t *k, int64_t n, int2 *child, int32_t *
     const int left = lo == gamma ? ~(int)gamma : (int)gamma;
     const int right = hi == gamma + 1 ? ~(int)(gamma + 1) : (int)(gamma + 1);
     child[i] = make_int2(left, right);
+    if (range) range[i] = make_int2((int)lo, (int)hi);  // the leaves below node i
     if (left < 0)
         parent_leaf[~left] = (int32_t)i;
     else
@@ -243,9 +247,180 @@ __global__ void k_boxes(int64_t n, const int2 *child, const int32_t *parent_int,
     }
 }
 
+// ---- SNCH on the device-built tree (3D) ----
+//
+// Leaf s (one triangle, order[s]) lists its three edges as silhouette records 3s..3s+2
+// (gq_sile_t, converted from the 19-float records exactly as the host flattening does).
+// Each child of each pair gets a normal cone and a node bound over the records of its
+// leaves.  The cones are built from the geometry (both face normals of every edge with
+// its orientation sign, radius from the box centre to the edge end points), not with
+// the reference's midpoint radius, so the walk finds what closest_silhouette_baseline
+// finds up to FP32 distance ties; half angle and radius carry a small outward margin.
+
+__device__ gq_sile_t edge_record(const float *s) {
+    gq_sile_t r;
+    r.ax = s[3]; r.ay = s[4]; r.az = s[5];
+    r.bx = s[6]; r.by = s[7]; r.bz = s[8];
+    const float cx = s[0], cy = s[1], cz = s[2], dx = s[9], dy = s[10], dz = s[11];
+    sil_face_normal(r.bx - r.ax, r.by - r.ay, r.bz - r.az, cx - r.ax, cy - r.ay, cz - r.az, r.n0x, r.n0y, r.n0z);
+    sil_face_normal(dx - r.ax, dy - r.ay, dz - r.az, r.bx - r.ax, r.by - r.ay, r.bz - r.az, r.n1x, r.n1y, r.n1z);
+    r.prim = (int32_t)s[18];
+    const bool boundary = ((int64_t)s[12] == -1) || ((int64_t)s[15] == -1);
+    r.flags = boundary ? GQ_ITEM_VALID : 0;
+    r.span0 = sil_span(r.n0x, r.n0y, r.n0z, r.ax, r.ay, r.az, r.bx, r.by, r.bz);
+    r.span1 = sil_span(r.n1x, r.n1y, r.n1z, r.ax, r.ay, r.az, r.bx, r.by, r.bz);
+    if (!boundary && sil_filter_usable(r.n0x, r.n0y, r.n0z, r.n1x, r.n1y, r.n1z, r.span0, r.span1))
+        r.flags |= GQ_SIL_FILTER;
+    return r;
+}
+
+__global__ void k_snch_sils(int64_t n, const int32_t *order, const uint32_t *face_edge, const float *edges19,
+                            const float *edge_orient, gq_sile_t *sils, float *rec_orient) {
+    const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int64_t t = order[s];
+    for (int k = 0; k < 3; ++k) {
+        const uint32_t e = face_edge[3 * t + k];
+        gq_sile_t r = edge_record(edges19 + 19 * (int64_t)e);
+        if (k == 2) r.flags |= GQ_ITEM_LAST;
+        sils[3 * s + k] = r;
+        rec_orient[3 * s + k] = edge_orient[e];
+    }
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ double warp_min(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ float up(double x) {
+    float f = (float)x;
+    return (double)f < x ? nextafterf(f, __builtin_inff()) : f;
+}
+__device__ __forceinline__ float down(double x) {
+    float f = (float)x;
+    return (double)f > x ? nextafterf(f, -__builtin_inff()) : f;
+}
+
+// One warp per child of a pair (2 (n - 1) warps): cone and node bound over its records.
+__global__ void k_snch_pairs(int64_t n, const int2 *child, const int2 *range, const gq_pair3_t *pairs,
+                             const gq_sile_t *sils, const float *rec_orient, gq_spair3_t *spairs) {
+    const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= 2 * (n - 1)) return;  // warp-uniform
+    const int64_t p = w >> 1;
+    const int c = (int)(w & 1);
+    const int ref = c ? child[p].y : child[p].x;
+    const gq_pair3_t &P = pairs[p];
+    const float lo[3] = {c ? P.r_lox : P.l_lox, c ? P.r_loy : P.l_loy, c ? P.r_loz : P.l_loz};
+    const float hi[3] = {c ? P.r_hix : P.l_hix, c ? P.r_hiy : P.l_hiy, c ? P.r_hiz : P.l_hiz};
+    float ctr[3];
+    for (int k = 0; k < 3; ++k) ctr[k] = 0.5f * (lo[k] + hi[k]);
+    int64_t b0, b1;
+    if (ref < 0) {
+        b0 = 3 * (int64_t)~ref;
+        b1 = b0 + 3;
+    } else {
+        const int2 rr = range[ref];
+        b0 = 3 * (int64_t)rr.x;
+        b1 = 3 * (int64_t)rr.y + 3;
+    }
+    // pass 1: oriented normal sum, usability
+    double m[3] = {0.0, 0.0, 0.0};
+    bool bad = false;
+    for (int64_t j = b0 + lane; j < b1; j += 32) {
+        const gq_sile_t &r = sils[j];
+        const double o = rec_orient[j];
+        bad |= (r.flags & (GQ_ITEM_VALID | GQ_SIL_FILTER)) != GQ_SIL_FILTER;
+        m[0] += o * ((double)r.n0x + (double)r.n1x);
+        m[1] += o * ((double)r.n0y + (double)r.n1y);
+        m[2] += o * ((double)r.n0z + (double)r.n1z);
+    }
+    for (int k = 0; k < 3; ++k) m[k] = warp_sum(m[k]);
+    bad = __any_sync(0xffffffffu, bad);
+    const double ml = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+    const bool open = bad || !(ml > 1e-30);
+    float A[3] = {0.f, 0.f, 0.f};
+    if (!open)
+        for (int k = 0; k < 3; ++k) A[k] = (float)(m[k] / ml);
+    // pass 2: spread of the oriented normals around A, plane offsets, cone, radius
+    double dmax = 0.0, mlo = __builtin_inf(), mhi = -__builtin_inf(), cmin = 1.0, rmax = 0.0;
+    for (int64_t j = b0 + lane; j < b1; j += 32) {
+        const gq_sile_t &r = sils[j];
+        const double o = rec_orient[j];
+        const double a[3] = {r.ax, r.ay, r.az}, b[3] = {r.bx, r.by, r.bz};
+        double ra = 0.0, rb = 0.0;
+        for (int k = 0; k < 3; ++k) {
+            ra += (a[k] - ctr[k]) * (a[k] - ctr[k]);
+            rb += (b[k] - ctr[k]) * (b[k] - ctr[k]);
+        }
+        rmax = fmax(rmax, sqrt(fmax(ra, rb)));
+        for (int f = 0; f < 2; ++f) {
+            const double nn[3] = {o * (f ? r.n1x : r.n0x), o * (f ? r.n1y : r.n0y), o * (f ? r.n1z : r.n0z)};
+            double d2 = 0.0, ac = 0.0, sp = 0.0, cs = 0.0;
+            for (int k = 0; k < 3; ++k) {
+                d2 += (nn[k] - A[k]) * (nn[k] - A[k]);
+                ac += nn[k] * (a[k] - ctr[k]);
+                sp += nn[k] * (b[k] - a[k]);
+                cs += nn[k] * A[k];
+            }
+            dmax = fmax(dmax, sqrt(d2));
+            mlo = fmin(mlo, ac + fmin(0.0, sp));
+            mhi = fmax(mhi, ac + fmax(0.0, sp));
+            cmin = fmin(cmin, cs);
+        }
+    }
+    dmax = warp_max(dmax);
+    mlo = warp_min(mlo);
+    mhi = warp_max(mhi);
+    cmin = warp_min(cmin);
+    rmax = warp_max(rmax);
+    if (lane != 0) return;
+    // cone: the largest angle to A (normals are unit up to rounding: clamp), widened
+    const double half = open ? 3.14159265358979 : acos(fmax(-1.0, fmin(1.0, cmin))) + 1e-5;
+    const float rad = up(rmax * (1.0 + 1e-6) + 1e-30);
+    float nb[9] = {ctr[0], ctr[1], ctr[2], A[0], A[1], A[2], __builtin_inff(), 0.f, 0.f};
+    if (!open) {
+        const double pad = 1e-12 * (fabs(mlo) + fabs(mhi) + 1.0);
+        nb[6] = up(dmax * (1.0 + 1e-12));
+        nb[7] = down(mlo - pad);
+        nb[8] = up(mhi + pad);
+    }
+    gq_spair3_t &S = spairs[p];
+    const int out_ref = ref < 0 ? ~(3 * ~ref) : ref;  // leaf: its first silhouette record
+    if (c == 0) {
+        S.l_lox = lo[0]; S.l_loy = lo[1]; S.l_loz = lo[2];
+        S.l_hix = hi[0]; S.l_hiy = hi[1]; S.l_hiz = hi[2];
+        S.l_ax = A[0]; S.l_ay = A[1]; S.l_az = A[2];
+        S.l_half = up(half);
+        S.l_rad = rad;
+        S.ref_l = out_ref;
+        for (int k = 0; k < 9; ++k) S.l_b[k] = nb[k];
+    } else {
+        S.r_lox = lo[0]; S.r_loy = lo[1]; S.r_loz = lo[2];
+        S.r_hix = hi[0]; S.r_hiy = hi[1]; S.r_hiz = hi[2];
+        S.r_ax = A[0]; S.r_ay = A[1]; S.r_az = A[2];
+        S.r_half = up(half);
+        S.r_rad = rad;
+        S.ref_r = out_ref;
+        for (int k = 0; k < 9; ++k) S.r_b[k] = nb[k];
+        S.pad0 = S.pad1 = 0.f;
+    }
+}
+
 template <int D>
 cudaError_t build(const float *v, const int32_t *idx, int64_t n, void *pairs, void *prims, GpuBuildResult &res,
-                  cudaStream_t st) {
+                  const GpuSnchBuild *snch, cudaStream_t st) {
     cudaError_t e = cudaSuccess;
     std::vector<void *> tmp;
     auto grab = [&](size_t bytes) -> void * {
@@ -262,6 +437,9 @@ cudaError_t build(const float *v, const int32_t *idx, int64_t n, void *pairs, vo
     int32_t *arrivals = (int32_t *)grab((size_t)n * 4), *depth = (int32_t *)grab(4);
     NodeBox<D> *leafbox = (NodeBox<D> *)grab((size_t)n * sizeof(NodeBox<D>));
     NodeBox<D> *nodebox = (NodeBox<D> *)grab((size_t)n * sizeof(NodeBox<D>));
+    const bool with_snch = D == 3 && snch != nullptr;
+    int2 *range = with_snch ? (int2 *)grab((size_t)n * sizeof(int2)) : nullptr;
+    float *rec_orient = with_snch ? (float *)grab((size_t)n * 3 * sizeof(float)) : nullptr;
     size_t tb = 0;
     if (e == cudaSuccess)
         e = cub::DeviceRadixSort::SortPairs(nullptr, tb, k_in, k_out, v_in, order, (int)n, 0, 64, st);
@@ -285,13 +463,24 @@ cudaError_t build(const float *v, const int32_t *idx, int64_t n, void *pairs, vo
             int32_t minus1 = -1;
             e = cudaMemcpyAsync(parent_leaf, &minus1, 4, cudaMemcpyHostToDevice, st);
         } else {
-            k_hierarchy<<<grid_of(n - 1), kBlock, 0, st>>>(k_out, n, child, parent_int, parent_leaf);
+            k_hierarchy<<<grid_of(n - 1), kBlock, 0, st>>>(k_out, n, child, parent_int, parent_leaf, range);
         }
     }
     if (e == cudaSuccess) {
         k_leaves<D><<<grid_of(n), kBlock, 0, st>>>(v, idx, n, order, prims, leafbox);
         k_boxes<D><<<grid_of(n), kBlock, 0, st>>>(n, child, parent_int, parent_leaf, leafbox, nodebox, arrivals, pairs,
                                                   depth);
+        e = cudaGetLastError();
+    }
+    if (with_snch && e == cudaSuccess) {
+        k_snch_sils<<<grid_of(n), kBlock, 0, st>>>(n, order, snch->face_edge, snch->edges19, snch->edge_orient,
+                                                   static_cast<gq_sile_t *>(snch->sils), rec_orient);
+        if (n > 1) {
+            const int64_t threads = 2 * (n - 1) * 32;
+            k_snch_pairs<<<dim3((unsigned)((threads + kBlock - 1) / kBlock)), kBlock, 0, st>>>(
+                n, child, range, static_cast<const gq_pair3_t *>(pairs), static_cast<const gq_sile_t *>(snch->sils),
+                rec_orient, static_cast<gq_spair3_t *>(snch->spairs));
+        }
         e = cudaGetLastError();
     }
     NodeBox<D> root{};
@@ -354,7 +543,8 @@ __global__ void k_runs(const uint32_t *head, const uint32_t *run_of, const uint3
 // edge e (runs ordered by first appearance): replays its half-edges in face order with
 // the host's last-writer rule and writes the 19 floats of silhouette_data().
 __global__ void k_edges(const float *v, const int32_t *faces, const uint64_t *keys, const uint32_t *vals, int64_t nh,
-                        const uint32_t *run_start, const uint32_t *run_by_first, int64_t n_edges, float *out) {
+                        const uint32_t *run_start, const uint32_t *run_by_first, int64_t n_edges, float *out,
+                        float *orient) {
     const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (e >= n_edges) return;
     const uint32_t g = run_by_first[e];
@@ -362,6 +552,7 @@ __global__ void k_edges(const float *v, const int32_t *faces, const uint64_t *ke
     const uint64_t key = keys[i];
     float pv[4][3] = {};
     uint64_t idx[4] = {0, 0, 0, 0}, face[2] = {0, 0};
+    bool last_swapped = false;
     for (; i < nh && keys[i] == key; ++i) {
         const int64_t h = vals[i], f = h / 3, k = h % 3;
         uint64_t i0 = (uint32_t)faces[f * 3 + k], i1 = (uint32_t)faces[f * 3 + (k + 1) % 3];
@@ -384,7 +575,11 @@ __global__ void k_edges(const float *v, const int32_t *faces, const uint64_t *ke
         idx[2] = i1;
         idx[slot] = i2;
         face[swapped ? 1 : 0] = (uint64_t)f;
+        last_swapped = swapped;
     }
+    // the stored end points follow the last writer's winding: its normals point
+    // outward on a consistently wound mesh unless its index pair was swapped
+    if (orient) orient[e] = last_swapped ? -1.f : 1.f;
     float *r = out + e * 19;
     for (int a = 0; a < 4; ++a)
         for (int c = 0; c < 3; ++c) r[a * 3 + c] = pv[a][c];
@@ -394,17 +589,29 @@ __global__ void k_edges(const float *v, const int32_t *faces, const uint64_t *ke
     r[18] = (float)(uint64_t)e;
 }
 
+// face_edge[h] = edge index of half-edge h: runs are numbered by first appearance
+__global__ void k_edge_of_run(const uint32_t *run_by_first, int64_t runs, uint32_t *edge_of_run) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e < runs) edge_of_run[run_by_first[e]] = (uint32_t)e;
+}
+__global__ void k_face_edge(const uint32_t *vals, const uint32_t *run_of, int64_t nh, const uint32_t *edge_of_run,
+                            uint32_t *face_edge) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < nh) face_edge[vals[i]] = edge_of_run[run_of[i] - 1];
+}
+
 }  // namespace
 
 cudaError_t gpu_build_bvh(int dim, const float *verts, const int32_t *index, int64_t n_prims, void *pairs,
-                          void *prims, GpuBuildResult &res, cudaStream_t st) {
+                          void *prims, GpuBuildResult &res, cudaStream_t st, const GpuSnchBuild *snch) {
     if (n_prims <= 0) return cudaErrorInvalidValue;
-    return dim == 3 ? build<3>(verts, index, n_prims, pairs, prims, res, st)
-                    : build<2>(verts, index, n_prims, pairs, prims, res, st);
+    return dim == 3 ? build<3>(verts, index, n_prims, pairs, prims, res, snch, st)
+                    : build<2>(verts, index, n_prims, pairs, prims, res, nullptr, st);
 }
 
 cudaError_t gpu_silhouette_edges(const float *verts, int64_t nv, const int32_t *faces, int64_t nf, float *out,
-                                 int64_t cap_edges, int64_t *n_edges, int *bad_input, cudaStream_t st) {
+                                 int64_t cap_edges, int64_t *n_edges, int *bad_input, cudaStream_t st,
+                                 uint32_t *face_edge, float *orient) {
     *n_edges = 0;
     *bad_input = 0;
     if (nf <= 0) return cudaSuccess;
@@ -478,7 +685,14 @@ cudaError_t gpu_silhouette_edges(const float *verts, int64_t nv, const int32_t *
         e = cub::DeviceRadixSort::SortPairs(temp, tb, run_first, first_sorted, run_id, run_by_first, (int)runs, 0, 32,
                                             st);
     if (e == cudaSuccess) {
-        k_edges<<<grid_of(runs), kBlock, 0, st>>>(verts, faces, k_out, v_out, nh, run_start, run_by_first, runs, out);
+        k_edges<<<grid_of(runs), kBlock, 0, st>>>(verts, faces, k_out, v_out, nh, run_start, run_by_first, runs, out,
+                                                  orient);
+        e = cudaGetLastError();
+    }
+    if (face_edge && e == cudaSuccess) {
+        uint32_t *edge_of_run = run_start;  // free now: k_edges has read it
+        k_edge_of_run<<<grid_of(runs), kBlock, 0, st>>>(run_by_first, runs, edge_of_run);
+        k_face_edge<<<grid_of(nh), kBlock, 0, st>>>(v_out, run_of, nh, edge_of_run, face_edge);
         e = cudaGetLastError();
     }
     return done(e);

@@ -86,3 +86,37 @@ def test_device_silhouette_edges_open_and_bad_meshes():
     with pytest.raises(L.GQError, match="out of range"):
         build_flat_silhouette_edges_device(v, bad)
     assert build_flat_silhouette_edges_device(v, f[:0]).numel() == 0
+
+
+@pytest.mark.parametrize("open_mesh", [False, True])
+def test_device_snch_matches_the_baseline(open_mesh):
+    """The SNCH built on the device tree (cones from the geometry) answers silhouette
+    queries like closest_silhouette_baseline, up to FP32 ties, in every variant."""
+    v, f = W.icosphere(5, amplitude=0.3, seed=6)
+    if open_mesh:
+        f = f[v[f[:, 0], 2] > -0.4]  # boundary edges
+    dev = Scene(v, f, 3, device=0, gpu_build=True)
+    assert dev.info["n_silhouettes"] == 3 * f.shape[0]
+    q = W.uniform_points(20000, 3, seed=7)
+    for r_max in (np.inf, 0.3):
+        base = dev.closest_silhouette_brute(q, r_max)
+        for variant in ("exact", "coherent", "warp"):
+            _check(base, dev.closest_silhouette(q, r_max, variant=variant), f"sil {variant} r_max={r_max}")
+    assert dev.device_error() == 0
+
+
+def test_device_snch_scene_file(tmp_path):
+    v, f = W.icosphere(4, amplitude=0.2, seed=8)
+    dev = Scene(v, f, 3, device=0, gpu_build=True)
+    path = tmp_path / "dev_snch.gqs"
+    dev.save(path)
+    back = Scene.load(path, device=0)
+    q = W.uniform_points(5000, 3, seed=10)
+    a = to_np(dev.closest_silhouette(q, variant="exact"))
+    b = to_np(back.closest_silhouette(q, variant="exact"))
+    for k in ("valid", "d", "prim_id"):
+        assert np.array_equal(np.asarray(a[k]), np.asarray(b[k]))
+    one = Scene(np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32), np.array([[0, 1, 2]], np.int32), 3,
+                device=0, gpu_build=True)
+    x = np.array([[0.3, 0.3, 1.0], [2.0, 2.0, 0.0]], np.float32)
+    _check(one.closest_silhouette_brute(x), one.closest_silhouette(x, variant="exact"), "single triangle")
