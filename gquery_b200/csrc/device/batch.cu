@@ -180,6 +180,15 @@ __device__ __forceinline__ void sil_warp_phase(const DevScene *scenes, int n_sce
 constexpr int kHeavyVisits = 1024;
 // Node visits (closest points, rays) or steps (silhouettes) between refills in k_batch.
 constexpr int kBudget = 32;
+
+// Hand-over lists of the split modes (in the kinds' sort scratch): query index, and
+// (best primitive or silhouette, r_max bits) the lane had reached.
+struct Handover {
+    int32_t *cp_q = nullptr;
+    int2 *cp_r = nullptr;
+    int32_t *sil_q = nullptr;
+    int2 *sil_r = nullptr;
+};
 // Silhouette queries whose per-lane traversal passes this many steps (node visits and
 // silhouette tests) are handed to k_sil_heavy (sil_mode 3).
 constexpr int kHeavySilSteps = 2048;
@@ -187,8 +196,8 @@ constexpr int kHeavySilSteps = 2048;
 // One persistent launch per step.  Phase 1: closest points, as warp tiles of 32
 // sorted queries (warp-coherent traversal once per distinct scene in the tile) or
 // one lane per query (cp_mode 0; in cp_mode 2 a query past kHeavyVisits node visits
-// is appended to `heavy` and left to k_cp_heavy).  Phase 2: rays, one lane per query.
-// Phase 3: silhouettes (sil_mode): 1 warp-coherent tiles like the closest points, 2
+// is appended to the hand-over list and left to k_cp_heavy).  Phase 2: rays, one lane
+// per query.  Phase 3: silhouettes (sil_mode): 1 warp-coherent tiles like the closest points, 2
 // one query per warp (sil_warp.cuh), 0 one lane per query in the reference order, 3
 // the same with queries past kHeavySilSteps handed to k_sil_heavy.  Every warp moves
 // to the next phase when the current one has no unclaimed work, so the phases' tails
@@ -201,8 +210,8 @@ template <int D, bool RAYW, bool SPLIT, bool SIL>
 __global__ void __launch_bounds__(kBlock) k_batch(const DevScene *scenes, int n_scenes, BatchKind cp, gq_cp_out cp_out,
                                                   BatchKind ray, gq_ray_out ray_out, BatchKind sil,
                                                   gq_sil_out sil_out, int cp_mode, int sil_mode,
-                                                  int budget, unsigned long long *counter, int32_t *heavy,
-                                                  int2 *heavy_r, int32_t *sheavy, int2 *sheavy_r, int32_t *err) {
+                                                  int budget, unsigned long long *counter, Handover ho,
+                                                  int32_t *err) {
     const unsigned lane = threadIdx.x & 31u;
     // ---------------- phase 1: closest points ----------------
     if (cp_mode == 1) {
@@ -283,8 +292,8 @@ __global__ void __launch_bounds__(kBlock) k_batch(const DevScene *scenes, int n_
                 visits += b;
                 if (split && visits >= kHeavyVisits) {  // long traversal: one warp takes it over
                     const unsigned long long h = atomicAdd(&counter[3], 1ull);
-                    heavy[h] = (int32_t)qi;
-                    heavy_r[h] = make_int2(L.idx, fbits(L.r));
+                    ho.cp_q[h] = (int32_t)qi;
+                    ho.cp_r[h] = make_int2(L.idx, fbits(L.r));
                     handed = true;
                     return true;
                 }
@@ -395,9 +404,9 @@ __global__ void __launch_bounds__(kBlock) k_batch(const DevScene *scenes, int n_
                 steps += b;
                 if (split && steps >= kHeavySilSteps) {  // long traversal: one warp takes it over
                     const unsigned long long h = atomicAdd(&counter[5], 1ull);
-                    sheavy[h] = (int32_t)qi;
+                    ho.sil_q[h] = (int32_t)qi;
                     // the silhouette accepted so far (its position in the leaf order) and r_max
-                    sheavy_r[h] = make_int2(L.found ? L.bj : -1, fbits(L.r));
+                    ho.sil_r[h] = make_int2(L.found ? L.bj : -1, fbits(L.r));
                     handed = true;
                     return true;
                 }
@@ -503,8 +512,8 @@ __global__ void __launch_bounds__(kBlock, 8) k_batch_silw(const DevScene *scenes
 template <int D, bool RAYW>
 cudaError_t launch_batch(const DevScene *scenes_dev, int n_scenes, BatchKind kinds[3], const gq_cp_out &cp_out,
                          const gq_ray_out &ray_out, const gq_sil_out &sil_out, int cp_mode, int sil_mode,
-                         float grid_share, unsigned long long *counter, int32_t *heavy, int2 *heavy_r,
-                         int32_t *sheavy, int2 *sheavy_r, int32_t *err, cudaStream_t st) {
+                         float grid_share, unsigned long long *counter, Handover ho, int32_t *err,
+                         cudaStream_t st) {
     // the one-query-per-warp silhouette phase keeps its stacks in dynamic shared memory
     const size_t smem = (sil_mode == 2 && kinds[2].n > 0) ? (size_t)(kBlock / 32) * wsil::kWarpStack * sizeof(int2) : 0;
     if (smem && kinds[0].n <= 0 && kinds[1].n <= 0) {  // silhouettes only: the phase's own kernel
@@ -545,10 +554,10 @@ cudaError_t launch_batch(const DevScene *scenes_dev, int n_scenes, BatchKind kin
                                      std::max<int64_t>((most + kBlock - 1) / kBlock, smem ? (kinds[2].n * 32 + kBlock - 1) / kBlock : 0));
     if (grid_share > 0.f && grid_share < 1.f)
         want = std::min<int64_t>(want, std::max<int64_t>(1, (int64_t)(grid_share * (float)(bps * n_sm))));
-    void *args[] = {(void *)&scenes_dev, (void *)&n_scenes, (void *)&kinds[0], (void *)&cp_out, (void *)&kinds[1],
-                    (void *)&ray_out,    (void *)&kinds[2], (void *)&sil_out, (void *)&cp_mode, (void *)&sil_mode,
-                    (void *)&kBudget,    (void *)&counter, (void *)&heavy,    (void *)&heavy_r, (void *)&sheavy,
-                    (void *)&sheavy_r,   (void *)&err};
+    void *args[] = {(void *)&scenes_dev, (void *)&n_scenes, (void *)&kinds[0], (void *)&cp_out,
+                    (void *)&kinds[1],   (void *)&ray_out,  (void *)&kinds[2], (void *)&sil_out,
+                    (void *)&cp_mode,    (void *)&sil_mode, (void *)&kBudget,  (void *)&counter,
+                    (void *)&ho,         (void *)&err};
     cudaLaunchKernel(kern, dim3((unsigned)want), dim3(kBlock), args, smem, st);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -569,13 +578,13 @@ cudaError_t launch_batch(const DevScene *scenes_dev, int n_scenes, BatchKind kin
         return dim3((unsigned)g);
     };
     if (cp_mode == 2 && kinds[0].n > 0) {
-        k_cp_heavy<D><<<hgrid(0, kinds[0].n), kBlock, hsmem, st>>>(scenes_dev, kinds[0], cp_out, heavy, heavy_r,
+        k_cp_heavy<D><<<hgrid(0, kinds[0].n), kBlock, hsmem, st>>>(scenes_dev, kinds[0], cp_out, ho.cp_q, ho.cp_r,
                                                                    counter);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     if (sil_mode == 3 && kinds[2].n > 0) {
-        k_sil_heavy<D><<<hgrid(1, kinds[2].n), kBlock, hsmem, st>>>(scenes_dev, kinds[2], sil_out, sheavy, sheavy_r,
-                                                                    counter);
+        k_sil_heavy<D><<<hgrid(1, kinds[2].n), kBlock, hsmem, st>>>(scenes_dev, kinds[2], sil_out, ho.sil_q,
+                                                                    ho.sil_r, counter);
         e = cudaGetLastError();
     }
     return e;
@@ -610,8 +619,7 @@ cudaError_t batch_run(const DevScene *scenes_dev, int n_scenes, int dim, BatchKi
     while ((1ll << (end_bit - 32)) < (long long)n_scenes + 1) ++end_bit;  // padding keys sort last
     const size_t tb = sort_temp_bytes(max_n);
     // closest points handed to k_cp_heavy: the cp kind's sort inputs, free after the sort
-    int32_t *heavy = nullptr, *sheavy = nullptr;
-    int2 *heavy_r = nullptr, *sheavy_r = nullptr;
+    Handover ho;
     for (int k = 0; k < 3; ++k) {
         BatchKind &q = kinds[k];
         uint64_t *k_in = reinterpret_cast<uint64_t *>(p);
@@ -626,11 +634,11 @@ cudaError_t batch_run(const DevScene *scenes_dev, int n_scenes, int dim, BatchKi
         p += align256(tb);
         q.perm = perm;
         if (k == 0) {
-            heavy = v_in;
-            heavy_r = reinterpret_cast<int2 *>(k_in);
+            ho.cp_q = v_in;
+            ho.cp_r = reinterpret_cast<int2 *>(k_in);
         } else if (k == 2) {
-            sheavy = v_in;
-            sheavy_r = reinterpret_cast<int2 *>(k_in);
+            ho.sil_q = v_in;
+            ho.sil_r = reinterpret_cast<int2 *>(k_in);
         }
         if (q.n <= 0) continue;
         k_batch_keys<<<dim3((unsigned)((q.n + kBlock - 1) / kBlock)), kBlock, 0, st>>>(scenes_dev, n_scenes, q, q.n,
@@ -646,13 +654,13 @@ cudaError_t batch_run(const DevScene *scenes_dev, int n_scenes, int dim, BatchKi
     if (e != cudaSuccess) return e;
     if (dim == 3)
         return ray_wide ? launch_batch<3, true>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_mode,
-                                                sil_mode, grid_share, counter, heavy, heavy_r, sheavy, sheavy_r, err, st)
+                                                sil_mode, grid_share, counter, ho, err, st)
                         : launch_batch<3, false>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_mode,
-                                                 sil_mode, grid_share, counter, heavy, heavy_r, sheavy, sheavy_r, err, st);
+                                                 sil_mode, grid_share, counter, ho, err, st);
     return ray_wide ? launch_batch<2, true>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_mode,
-                                            sil_mode, grid_share, counter, heavy, heavy_r, sheavy, sheavy_r, err, st)
+                                            sil_mode, grid_share, counter, ho, err, st)
                     : launch_batch<2, false>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_mode,
-                                             sil_mode, grid_share, counter, heavy, heavy_r, sheavy, sheavy_r, err, st);
+                                             sil_mode, grid_share, counter, ho, err, st);
 }
 
 }  // namespace gqd

@@ -37,10 +37,10 @@ size_t batch_scratch_bytes(int64_t max_n);
 // kinds[0] closest point, kinds[1] rays, kinds[2] silhouettes (n = 0 to skip a kind).
 // ray_wide: rays on the quantised 8-wide BVH (every scene must have it); cp_mode:
 // closest points as cp_mode_of; sil_mode: silhouettes 1 warp-coherent, 2 one query per
-// warp, 0 reference order per lane, 3 the same with long traversals handed to a warp; grid_share in (0, 1) caps the persistent grid at
-// that share of the GPU's resident blocks, so a launch on another stream can run
-// beside it.  No allocation and no host synchronisation: the call can be recorded in
-// a CUDA graph.
+// warp, 0 reference order per lane, 3 the same with long traversals handed to a warp;
+// grid_share in (0, 1) caps the persistent grid at that share of the GPU's resident
+// blocks, so a launch on another stream can run beside it.  No allocation and no host
+// synchronisation: the call can be recorded in a CUDA graph.
 cudaError_t batch_run(const DevScene *scenes_dev, int n_scenes, int dim, BatchKind kinds[3], const gq_cp_out &cp_out,
                       const gq_ray_out &ray_out, const gq_sil_out &sil_out, int ray_wide, int cp_mode,
                       int sil_mode, float grid_share, void *scratch, int64_t max_n, int32_t *err,
