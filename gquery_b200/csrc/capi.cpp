@@ -44,8 +44,6 @@ void default_tuning(gq_scene *s);
 template <int D>
 gq_status build_on_device(gq_scene *s, const gq_build_opts &o) {
     if (o.device < 0) return fail(GQ_ERR_INVALID, "a device build needs a device");
-    if (o.build_snch && D == 2)
-        return fail(GQ_ERR_UNSUPPORTED, "the device build makes an SNCH for meshes only (build_snch must be 0 in 2D)");
     if (s->np < 1) return fail(GQ_ERR_INVALID, "a device build needs at least one primitive");
     DeviceGuard g(o.device);
     if (!g.ok) return fail(GQ_ERR_CUDA, "cannot select the scene's CUDA device");
@@ -68,21 +66,25 @@ gq_status build_on_device(gq_scene *s, const gq_build_opts &o) {
     s->device_bytes += (int64_t)(pair_bytes + prim_bytes);
     gqd::GpuBuildResult r;
     gqd::GpuSnchBuild sb;
-    const bool with_snch = D == 3 && o.build_snch;
+    const bool with_snch = o.build_snch != 0;
     std::vector<void *> tmp;  // the unique edges, freed after the build
     auto free_tmp = [&]() {
         for (void *p : tmp) cudaFree(p);
     };
     size_t spair_bytes = 0, sil_bytes = 0;
     if (with_snch) {
-        const int64_t nh = 3 * s->np;
+        using SPair = std::conditional_t<D == 2, gq_spair2_t, gq_spair3_t>;
+        using Sil = std::conditional_t<D == 2, gq_silv_t, gq_sile_t>;
+        const int64_t nh = 3 * s->np, n_rec = D * s->np;  // 3D: half-edges; records: D per leaf
         void *edges = nullptr, *face_edge = nullptr, *orient = nullptr, *spairs = nullptr, *sils = nullptr;
-        e = cudaMalloc(&edges, (size_t)nh * 19 * sizeof(float));
-        if (e == cudaSuccess) tmp.push_back(edges), e = cudaMalloc(&face_edge, (size_t)nh * sizeof(uint32_t));
-        if (e == cudaSuccess) tmp.push_back(face_edge), e = cudaMalloc(&orient, (size_t)nh * sizeof(float));
-        if (e == cudaSuccess) tmp.push_back(orient);
-        spair_bytes = sizeof(gq_spair3_t) * (size_t)std::max<int64_t>(s->np - 1, 1);
-        sil_bytes = sizeof(gq_sile_t) * (size_t)nh;
+        if (D == 3) {
+            e = cudaMalloc(&edges, (size_t)nh * 19 * sizeof(float));
+            if (e == cudaSuccess) tmp.push_back(edges), e = cudaMalloc(&face_edge, (size_t)nh * sizeof(uint32_t));
+            if (e == cudaSuccess) tmp.push_back(face_edge), e = cudaMalloc(&orient, (size_t)nh * sizeof(float));
+            if (e == cudaSuccess) tmp.push_back(orient);
+        }
+        spair_bytes = sizeof(SPair) * (size_t)std::max<int64_t>(s->np - 1, 1);
+        sil_bytes = sizeof(Sil) * (size_t)n_rec;
         if (e == cudaSuccess) e = cudaMalloc(&spairs, spair_bytes);
         if (e == cudaSuccess) s->allocs.push_back(spairs), e = cudaMalloc(&sils, sil_bytes);
         if (e == cudaSuccess) s->allocs.push_back(sils);
@@ -91,18 +93,21 @@ gq_status build_on_device(gq_scene *s, const gq_build_opts &o) {
             return fail(GQ_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
         }
         s->device_bytes += (int64_t)(spair_bytes + sil_bytes);
-        int64_t n_edges = 0;
-        int bad = 0;
-        e = gqd::gpu_silhouette_edges((const float *)pv, s->nv, (const int32_t *)pi, s->np, (float *)edges, nh,
-                                      &n_edges, &bad, nullptr, (uint32_t *)face_edge, (float *)orient);
-        if (e != cudaSuccess || bad) {
-            free_tmp();
-            if (e != cudaSuccess) return fail_cuda(e, "device silhouette edges");
-            return fail(GQ_ERR_INVALID, "face index out of range");
+        if (D == 3) {
+            int64_t n_edges = 0;
+            int bad = 0;
+            e = gqd::gpu_silhouette_edges((const float *)pv, s->nv, (const int32_t *)pi, s->np, (float *)edges, nh,
+                                          &n_edges, &bad, nullptr, (uint32_t *)face_edge, (float *)orient);
+            if (e != cudaSuccess || bad) {
+                free_tmp();
+                if (e != cudaSuccess) return fail_cuda(e, "device silhouette edges");
+                return fail(GQ_ERR_INVALID, "face index out of range");
+            }
         }
         sb.edges19 = (const float *)edges;
         sb.face_edge = (const uint32_t *)face_edge;
         sb.edge_orient = (const float *)orient;
+        sb.n_verts = s->nv;
         sb.spairs = spairs;
         sb.sils = sils;
     }
@@ -113,9 +118,9 @@ gq_status build_on_device(gq_scene *s, const gq_build_opts &o) {
     if (with_snch) {
         d.spairs = sb.spairs;
         d.sils = sb.sils;
-        d.sroot_ref = s->np > 1 ? 0 : ~0;  // a single triangle: its leaf, records 0..2
+        d.sroot_ref = s->np > 1 ? 0 : ~0;  // a single primitive: its leaf, records 0..D-1
         s->has_snch = true;
-        s->n_sil = 3 * s->np;
+        s->n_sil = D * s->np;
         s->image_bytes[4] = s->np > 1 ? spair_bytes : 0;
         s->image_bytes[5] = sil_bytes;
     }

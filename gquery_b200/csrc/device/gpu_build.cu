@@ -418,6 +418,122 @@ __global__ void k_snch_pairs(int64_t n, const int2 *child, const int2 *range, co
     }
 }
 
+// ---- SNCH on the device-built tree (2D) ----
+//
+// The raw silhouette of vertex v (snch.cpp:157-184): its own position, the previous
+// vertex from the last edge that ends at v and the next vertex from the last edge that
+// starts at v (zero where there is none, like the reference's value-initialised
+// records).  Leaf s (segment order[s]) lists its two vertices as records 2s, 2s+1.
+
+__global__ void k_sil_roles(const int32_t *idx, int64_t ne, int32_t *prev_e, int32_t *next_e) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    atomicMax(&next_e[idx[2 * e]], (int32_t)e);
+    atomicMax(&prev_e[idx[2 * e + 1]], (int32_t)e);
+}
+
+__global__ void k_snch2_sils(int64_t n, const int32_t *order, const float *v, const int32_t *idx,
+                             const int32_t *prev_e, const int32_t *next_e, gq_silv_t *sils) {
+    const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int64_t t = order[s];
+    for (int k = 0; k < 2; ++k) {
+        const int64_t u = idx[2 * t + k];
+        const int32_t pe = prev_e[u], ne = next_e[u];
+        gq_silv_t r;
+        r.ax = pe >= 0 ? v[2 * (int64_t)idx[2 * (int64_t)pe]] : 0.f;
+        r.ay = pe >= 0 ? v[2 * (int64_t)idx[2 * (int64_t)pe] + 1] : 0.f;
+        r.bx = v[2 * u];
+        r.by = v[2 * u + 1];
+        r.cx = ne >= 0 ? v[2 * (int64_t)idx[2 * (int64_t)ne + 1]] : 0.f;
+        r.cy = ne >= 0 ? v[2 * (int64_t)idx[2 * (int64_t)ne + 1] + 1] : 0.f;
+        r.prim = (int32_t)(float)u;
+        // silhouette_vertex.py:48: both neighbour indices != -1, which stored indices always are
+        r.flags = GQ_ITEM_VALID | (k == 1 ? GQ_ITEM_LAST : 0);
+        sils[2 * s + k] = r;
+    }
+}
+
+// unit perpendicular of d, (d.y, -d.x) / |d| (NaN for d = 0)
+__device__ __forceinline__ void perp_unit(double dx, double dy, double &nx, double &ny) {
+    const double l = sqrt(dx * dx + dy * dy);
+    nx = dy / l;
+    ny = -dx / l;
+}
+
+// One warp per child of a pair: the cone of the vertex records below it.  The test of a
+// record is sign(n0 . (b - x)) != sign(n1 . (b - x)) with n0, n1 the unit normals of its
+// two segments, so a cone holding every n0, n1 and a radius reaching every b is enough.
+__global__ void k_snch2_pairs(int64_t n, const int2 *child, const int2 *range, const gq_pair2_t *pairs,
+                              const gq_silv_t *sils, gq_spair2_t *spairs) {
+    const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= 2 * (n - 1)) return;  // warp-uniform
+    const int64_t p = w >> 1;
+    const int c = (int)(w & 1);
+    const int ref = c ? child[p].y : child[p].x;
+    const gq_pair2_t &P = pairs[p];
+    const float lo[2] = {c ? P.r_lox : P.l_lox, c ? P.r_loy : P.l_loy};
+    const float hi[2] = {c ? P.r_hix : P.l_hix, c ? P.r_hiy : P.l_hiy};
+    const float ctr[2] = {0.5f * (lo[0] + hi[0]), 0.5f * (lo[1] + hi[1])};
+    int64_t b0, b1;
+    if (ref < 0) {
+        b0 = 2 * (int64_t)~ref;
+        b1 = b0 + 2;
+    } else {
+        const int2 rr = range[ref];
+        b0 = 2 * (int64_t)rr.x;
+        b1 = 2 * (int64_t)rr.y + 2;
+    }
+    double m[2] = {0.0, 0.0};
+    bool bad = false;
+    for (int64_t j = b0 + lane; j < b1; j += 32) {
+        const gq_silv_t &r = sils[j];
+        double n0x, n0y, n1x, n1y;
+        perp_unit((double)r.bx - r.ax, (double)r.by - r.ay, n0x, n0y);
+        perp_unit((double)r.cx - r.bx, (double)r.cy - r.by, n1x, n1y);
+        bad |= !(isfinite(n0x) && isfinite(n0y) && isfinite(n1x) && isfinite(n1y));
+        m[0] += n0x + n1x;
+        m[1] += n0y + n1y;
+    }
+    m[0] = warp_sum(m[0]);
+    m[1] = warp_sum(m[1]);
+    bad = __any_sync(0xffffffffu, bad);
+    const double ml = sqrt(m[0] * m[0] + m[1] * m[1]);
+    const bool open = bad || !(ml > 1e-30);
+    float A[2] = {0.f, 0.f};
+    if (!open) A[0] = (float)(m[0] / ml), A[1] = (float)(m[1] / ml);
+    double cmin = 1.0, rmax = 0.0;
+    for (int64_t j = b0 + lane; j < b1; j += 32) {
+        const gq_silv_t &r = sils[j];
+        const double dx = (double)r.bx - ctr[0], dy = (double)r.by - ctr[1];
+        rmax = fmax(rmax, sqrt(dx * dx + dy * dy));
+        if (!open) {
+            double n0x, n0y, n1x, n1y;
+            perp_unit((double)r.bx - r.ax, (double)r.by - r.ay, n0x, n0y);
+            perp_unit((double)r.cx - r.bx, (double)r.cy - r.by, n1x, n1y);
+            cmin = fmin(cmin, fmin(n0x * A[0] + n0y * A[1], n1x * A[0] + n1y * A[1]));
+        }
+    }
+    cmin = warp_min(cmin);
+    rmax = warp_max(rmax);
+    if (lane != 0) return;
+    const double half = open ? 3.14159265358979 : acos(fmax(-1.0, fmin(1.0, cmin))) + 1e-5;
+    const float rad = up(rmax * (1.0 + 1e-6) + 1e-30);
+    gq_spair2_t &S = spairs[p];
+    const int out_ref = ref < 0 ? ~(2 * ~ref) : ref;  // leaf: its first silhouette record
+    if (c == 0) {
+        S.l_lox = lo[0]; S.l_loy = lo[1]; S.l_hix = hi[0]; S.l_hiy = hi[1];
+        S.l_ax = A[0]; S.l_ay = A[1]; S.l_half = up(half); S.l_rad = rad;
+        S.ref_l = out_ref;
+    } else {
+        S.r_lox = lo[0]; S.r_loy = lo[1]; S.r_hix = hi[0]; S.r_hiy = hi[1];
+        S.r_ax = A[0]; S.r_ay = A[1]; S.r_half = up(half); S.r_rad = rad;
+        S.ref_r = out_ref;
+        S.pad0 = S.pad1 = 0;
+    }
+}
+
 template <int D>
 cudaError_t build(const float *v, const int32_t *idx, int64_t n, void *pairs, void *prims, GpuBuildResult &res,
                   const GpuSnchBuild *snch, cudaStream_t st) {
@@ -437,9 +553,12 @@ cudaError_t build(const float *v, const int32_t *idx, int64_t n, void *pairs, vo
     int32_t *arrivals = (int32_t *)grab((size_t)n * 4), *depth = (int32_t *)grab(4);
     NodeBox<D> *leafbox = (NodeBox<D> *)grab((size_t)n * sizeof(NodeBox<D>));
     NodeBox<D> *nodebox = (NodeBox<D> *)grab((size_t)n * sizeof(NodeBox<D>));
-    const bool with_snch = D == 3 && snch != nullptr;
+    const bool with_snch = snch != nullptr;
     int2 *range = with_snch ? (int2 *)grab((size_t)n * sizeof(int2)) : nullptr;
-    float *rec_orient = with_snch ? (float *)grab((size_t)n * 3 * sizeof(float)) : nullptr;
+    float *rec_orient = with_snch && D == 3 ? (float *)grab((size_t)n * 3 * sizeof(float)) : nullptr;
+    // 2D: per vertex the last edges ending / starting at it
+    int32_t *prev_e = with_snch && D == 2 ? (int32_t *)grab((size_t)snch->n_verts * 4) : nullptr;
+    int32_t *next_e = with_snch && D == 2 ? (int32_t *)grab((size_t)snch->n_verts * 4) : nullptr;
     size_t tb = 0;
     if (e == cudaSuccess)
         e = cub::DeviceRadixSort::SortPairs(nullptr, tb, k_in, k_out, v_in, order, (int)n, 0, 64, st);
@@ -473,15 +592,29 @@ cudaError_t build(const float *v, const int32_t *idx, int64_t n, void *pairs, vo
         e = cudaGetLastError();
     }
     if (with_snch && e == cudaSuccess) {
-        k_snch_sils<<<grid_of(n), kBlock, 0, st>>>(n, order, snch->face_edge, snch->edges19, snch->edge_orient,
-                                                   static_cast<gq_sile_t *>(snch->sils), rec_orient);
-        if (n > 1) {
-            const int64_t threads = 2 * (n - 1) * 32;
-            k_snch_pairs<<<dim3((unsigned)((threads + kBlock - 1) / kBlock)), kBlock, 0, st>>>(
-                n, child, range, static_cast<const gq_pair3_t *>(pairs), static_cast<const gq_sile_t *>(snch->sils),
-                rec_orient, static_cast<gq_spair3_t *>(snch->spairs));
+        const int64_t threads = 2 * (n - 1) * 32;
+        const dim3 pgrid((unsigned)((threads + kBlock - 1) / kBlock));
+        if (D == 3) {
+            k_snch_sils<<<grid_of(n), kBlock, 0, st>>>(n, order, snch->face_edge, snch->edges19, snch->edge_orient,
+                                                       static_cast<gq_sile_t *>(snch->sils), rec_orient);
+            if (n > 1)
+                k_snch_pairs<<<pgrid, kBlock, 0, st>>>(n, child, range, static_cast<const gq_pair3_t *>(pairs),
+                                                       static_cast<const gq_sile_t *>(snch->sils), rec_orient,
+                                                       static_cast<gq_spair3_t *>(snch->spairs));
+        } else {
+            e = cudaMemsetAsync(prev_e, 0xff, (size_t)snch->n_verts * 4, st);
+            if (e == cudaSuccess) e = cudaMemsetAsync(next_e, 0xff, (size_t)snch->n_verts * 4, st);
+            if (e == cudaSuccess) {
+                k_sil_roles<<<grid_of(n), kBlock, 0, st>>>(idx, n, prev_e, next_e);
+                k_snch2_sils<<<grid_of(n), kBlock, 0, st>>>(n, order, v, idx, prev_e, next_e,
+                                                            static_cast<gq_silv_t *>(snch->sils));
+                if (n > 1)
+                    k_snch2_pairs<<<pgrid, kBlock, 0, st>>>(n, child, range, static_cast<const gq_pair2_t *>(pairs),
+                                                            static_cast<const gq_silv_t *>(snch->sils),
+                                                            static_cast<gq_spair2_t *>(snch->spairs));
+            }
         }
-        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaGetLastError();
     }
     NodeBox<D> root{};
     if (e == cudaSuccess)
@@ -606,7 +739,7 @@ cudaError_t gpu_build_bvh(int dim, const float *verts, const int32_t *index, int
                           void *prims, GpuBuildResult &res, cudaStream_t st, const GpuSnchBuild *snch) {
     if (n_prims <= 0) return cudaErrorInvalidValue;
     return dim == 3 ? build<3>(verts, index, n_prims, pairs, prims, res, snch, st)
-                    : build<2>(verts, index, n_prims, pairs, prims, res, nullptr, st);
+                    : build<2>(verts, index, n_prims, pairs, prims, res, snch, st);
 }
 
 cudaError_t gpu_silhouette_edges(const float *verts, int64_t nv, const int32_t *faces, int64_t nf, float *out,

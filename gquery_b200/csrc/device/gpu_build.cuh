@@ -16,20 +16,22 @@ struct GpuBuildResult {
     int32_t max_depth = 0;  // internal ancestors of the deepest leaf
 };
 
-// SNCH of a device-built triangle mesh: the unique edges (gpu_silhouette_edges with its
-// face_edge and orient outputs) in, the SNCH pair records (max(n_prims - 1, 1) of them)
-// and 3 n_prims silhouette records (three per leaf) out.
+// SNCH on the device-built tree.  A triangle mesh: the unique edges (gpu_silhouette_edges
+// with its face_edge and orient outputs) in, 3 n_prims silhouette records (three per
+// leaf) out.  A polyline: n_verts in, 2 n_prims vertex records (two per leaf) out.
+// Both: max(n_prims - 1, 1) SNCH pair records out.
 struct GpuSnchBuild {
-    const float *edges19 = nullptr;       // unique edges, 19 floats each
-    const uint32_t *face_edge = nullptr;  // [3 n_prims] edge of half-edge 3 f + k
-    const float *edge_orient = nullptr;   // [edges] +1 / -1, see gpu_silhouette_edges
-    void *spairs = nullptr;               // gq_spair3_t
-    void *sils = nullptr;                 // gq_sile_t
+    const float *edges19 = nullptr;       // 3D: unique edges, 19 floats each
+    const uint32_t *face_edge = nullptr;  // 3D: [3 n_prims] edge of half-edge 3 f + k
+    const float *edge_orient = nullptr;   // 3D: [edges] +1 / -1, see gpu_silhouette_edges
+    int64_t n_verts = 0;                  // 2D: vertex count
+    void *spairs = nullptr;               // gq_spair3_t / gq_spair2_t
+    void *sils = nullptr;                 // gq_sile_t / gq_silv_t
 };
 
 // verts [nv][dim], index [n_prims][dim] on the device (indices already validated);
 // pairs: room for max(n_prims - 1, 1) pair records, prims: n_prims primitive records;
-// snch (3D only, may be null): the SNCH on the same tree.  Synchronises `st` before
+// snch (may be null): the SNCH on the same tree.  Synchronises `st` before
 // returning.
 cudaError_t gpu_build_bvh(int dim, const float *verts, const int32_t *index, int64_t n_prims, void *pairs,
                           void *prims, GpuBuildResult &res, cudaStream_t st, const GpuSnchBuild *snch = nullptr);

@@ -120,3 +120,25 @@ def test_device_snch_scene_file(tmp_path):
                 device=0, gpu_build=True)
     x = np.array([[0.3, 0.3, 1.0], [2.0, 2.0, 0.0]], np.float32)
     _check(one.closest_silhouette_brute(x), one.closest_silhouette(x, variant="exact"), "single triangle")
+
+
+@pytest.mark.parametrize("closed", [True, False])
+def test_device_snch_polyline_matches_host(closed):
+    """2D: the device SNCH (vertex records with the reference's last-writer neighbours,
+    cones from the geometry) answers like the host-built SNCH, up to FP32 ties."""
+    if closed:
+        v, e = W.star_polyline(20000, seed=3)
+    else:
+        rng = np.random.default_rng(4)
+        v = np.cumsum(rng.normal(0, 0.01, (5000, 2)), axis=0).astype(np.float32)
+        e = np.stack([np.arange(4999), np.arange(1, 5000)], 1).astype(np.int32)  # open chain
+    host = Scene(v, e, 2, device=0, build_snch=True, build_wide=False)
+    dev = Scene(v, e, 2, device=0, gpu_build=True)
+    assert dev.info["n_silhouettes"] == 2 * e.shape[0]
+    lo, hi = v.min(0), v.max(0)
+    q = (lo + (hi - lo) * np.random.default_rng(5).uniform(-0.5, 1.5, (20000, 2))).astype(np.float32)
+    for r_max in (np.inf, 0.05):
+        ref = host.closest_silhouette(q, r_max, variant="exact")
+        for variant in ("exact", "coherent", "warp"):
+            _check(ref, dev.closest_silhouette(q, r_max, variant=variant), f"sil2 {variant} r_max={r_max}")
+    assert dev.device_error() == 0
