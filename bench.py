@@ -228,8 +228,9 @@ def section_c0(args, dev, flush):
 
 def section_build(args, dev, flush):
     """Scene build for the level-8 mesh: the host SAH build (the reference's builder
-    algorithm) against the linear BVH built on the device, each without and with the
-    SNCH, and closest-point / ray / silhouette throughput on each tree."""
+    algorithm) against the linear BVH built on the device, each as the binary BVH alone
+    and in full (quantised 8-wide nodes and SNCH too), and closest-point / ray /
+    silhouette throughput on each full scene."""
     import torch
     from gquery_b200 import workloads as W
     from gquery_b200.scene import Scene
@@ -238,35 +239,35 @@ def section_build(args, dev, flush):
     res = {"workload": f"icosphere level 8, {F.shape[0]} triangles; 1,048,576 cp queries + rays + "
                        "silhouette points"}
     t0 = time.perf_counter()
-    host = Scene(V, F, 3, device=dv, build_snch=False, build_wide=False)
+    Scene(V, F, 3, device=dv, build_snch=False, build_wide=False)
     res["host_sah_build_s"] = time.perf_counter() - t0
     t0 = time.perf_counter()
-    host_s = Scene(V, F, 3, device=dv, build_snch=True, build_wide=False)
-    res["host_sah_snch_build_s"] = time.perf_counter() - t0
-    del host
+    host = Scene(V, F, 3, device=dv)
+    res["host_full_build_s"] = time.perf_counter() - t0
     torch.cuda.synchronize()
     Scene(V, F, 3, device=dv, gpu_build=True)  # warm-up (module load, pool growth)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    Scene(V, F, 3, device=dv, gpu_build=True, build_snch=False)
+    Scene(V, F, 3, device=dv, gpu_build=True, build_snch=False, build_wide=False)
     torch.cuda.synchronize()
     res["device_build_s"] = time.perf_counter() - t0
     t0 = time.perf_counter()
     devb = Scene(V, F, 3, device=dv, gpu_build=True)
     torch.cuda.synchronize()
-    res["device_snch_build_s"] = time.perf_counter() - t0
+    res["device_full_build_s"] = time.perf_counter() - t0
     res["device_tree_depth"] = devb.info["max_depth"]
-    res["host_tree_depth"] = host_s.info["max_depth"]
+    res["host_tree_depth"] = host.info["max_depth"]
     n = 1 << 20
     q = torch.as_tensor(W.uniform_points(n, 3, seed=41)).to(dev)
     o, d = (torch.as_tensor(a).to(dev) for a in W.rays(n, 3, seed=42))
-    for name, sc in (("host_tree", host_s), ("device_tree", devb)):
+    for name, sc in (("host_tree", host), ("device_tree", devb)):
         row = {}
         for variant in ("exact", "coherent"):
             ms = dev_ms(lambda: sc.closest_point(q, variant=variant), steps=3, warmup=2, flush=flush)
             row[f"cp_{variant}_mqueries_per_s"] = n / ms / 1e3
-        ms = dev_ms(lambda: sc.intersect(o, d, variant="exact"), steps=3, warmup=2, flush=flush)
-        row["ray_exact_mqueries_per_s"] = n / ms / 1e3
+        for variant in ("exact", "wide8"):
+            ms = dev_ms(lambda: sc.intersect(o, d, variant=variant), steps=3, warmup=2, flush=flush)
+            row[f"ray_{variant}_mqueries_per_s"] = n / ms / 1e3
         ms = dev_ms(lambda: sc.closest_silhouette(q, variant="coherent"), steps=2, warmup=1, flush=flush)
         row["sil_coherent_mqueries_per_s"] = n / ms / 1e3
         res[name] = row

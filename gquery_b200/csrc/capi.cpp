@@ -115,6 +115,27 @@ gq_status build_on_device(gq_scene *s, const gq_build_opts &o) {
                            with_snch ? &sb : nullptr);
     free_tmp();
     if (e != cudaSuccess) return fail_cuda(e, "device build");
+    if (o.build_wide) {
+        // the collapse into quantised 8-wide nodes runs on the host over the pair records
+        using WPair = std::conditional_t<D == 2, gq_pair2_t, gq_pair3_t>;
+        DeviceImage<D> wimg;
+        std::vector<WPair> hp((size_t)std::max<int64_t>(s->np - 1, 0));
+        if (!hp.empty()) {
+            e = cudaMemcpy(hp.data(), pairs, hp.size() * sizeof(WPair), cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) return fail_cuda(e, "device build: pair download");
+        }
+        try {
+            flatten_wide_from_pairs<D>(hp, r.root_ref, r.root_lo, r.root_hi, wimg);
+        } catch (const std::bad_alloc &) {
+            return fail(GQ_ERR_NOMEM, "out of host memory collapsing the device-built tree");
+        }
+        if (!wimg.wnodes.empty() && (st = s->upload(wimg.wnodes, &d.wnodes)) != GQ_OK) return st;
+        d.wroot_ref = wimg.wroot_ref;
+        s->has_wide = true;
+        s->wide_stack = wimg.wide_stack;
+        s->n_wide = (int64_t)wimg.wnodes.size();
+        s->image_bytes[3] = wimg.wnodes.size() * sizeof(wimg.wnodes[0]);
+    }
     if (with_snch) {
         d.spairs = sb.spairs;
         d.sils = sb.sils;

@@ -463,10 +463,114 @@ void flatten_snch(const BvhTree<D> &t, const SnchTree<D> &s, DeviceImage<D> &img
     if constexpr (D == 3) snch_node_bounds(t, s, img, n_threads);
 }
 
+// The same collapse over a binary tree given as pair records (a device-built tree: pair
+// i holds both child boxes of interior node i and their references, leaf = ~record).
+template <int D>
+struct PairWideBuilder {
+    using Pair = typename DeviceImage<D>::Pair;
+    const std::vector<Pair> &pairs;
+    DeviceImage<D> &img;
+
+    struct Kid {
+        int32_t ref;
+        Box<D> box;
+    };
+    static Box<D> child_box(const Pair &p, int c) {
+        Box<D> b;
+        if constexpr (D == 2) {
+            b.lo.v[0] = c ? p.r_lox : p.l_lox; b.lo.v[1] = c ? p.r_loy : p.l_loy;
+            b.hi.v[0] = c ? p.r_hix : p.l_hix; b.hi.v[1] = c ? p.r_hiy : p.l_hiy;
+        } else {
+            b.lo.v[0] = c ? p.r_lox : p.l_lox; b.lo.v[1] = c ? p.r_loy : p.l_loy; b.lo.v[2] = c ? p.r_loz : p.l_loz;
+            b.hi.v[0] = c ? p.r_hix : p.l_hix; b.hi.v[1] = c ? p.r_hiy : p.l_hiy; b.hi.v[2] = c ? p.r_hiz : p.l_hiz;
+        }
+        return b;
+    }
+
+    int build(int32_t node, const Box<D> &box, int32_t *ref_out) {
+        const Pair &pn = pairs[(size_t)node];
+        std::vector<Kid> kids{{pn.ref_l, child_box(pn, 0)}, {pn.ref_r, child_box(pn, 1)}};
+        while (kids.size() < GQ_WIDTH) {  // open the interior child with the largest area
+            int pick = -1;
+            float best = -1.f;
+            for (size_t k = 0; k < kids.size(); ++k) {
+                if (kids[k].ref >= 0) {
+                    const float a = kids[k].box.area();
+                    if (a > best) {
+                        best = a;
+                        pick = (int)k;
+                    }
+                }
+            }
+            if (pick < 0) break;
+            const Pair &pc = pairs[(size_t)kids[(size_t)pick].ref];
+            kids[(size_t)pick] = Kid{pc.ref_l, child_box(pc, 0)};
+            kids.insert(kids.begin() + pick + 1, Kid{pc.ref_r, child_box(pc, 1)});
+        }
+        const size_t me = img.wnodes.size();
+        img.wnodes.emplace_back();
+        *ref_out = (int32_t)me;
+        int e[D];
+        float org[D];
+        for (int k = 0; k < D; ++k) quant_axis(box.lo.v[k], box.hi.v[k], &org[k], &e[k]);
+        typename DeviceImage<D>::WNode w;
+        std::memset(&w, 0, sizeof w);
+        if constexpr (D == 2) {
+            w.ox = org[0];
+            w.oy = org[1];
+            w.meta = (uint32_t)(e[0] + 127) | ((uint32_t)(e[1] + 127) << 8) | ((uint32_t)kids.size() << 24);
+        } else {
+            w.ox = org[0];
+            w.oy = org[1];
+            w.oz = org[2];
+            w.meta = (uint32_t)(e[0] + 127) | ((uint32_t)(e[1] + 127) << 8) | ((uint32_t)(e[2] + 127) << 16) |
+                     ((uint32_t)kids.size() << 24);
+        }
+        for (int k = 0; k < GQ_WIDTH; ++k) w.ref[k] = kEmptyLeaf;
+        int deepest = 0;
+        for (size_t k = 0; k < kids.size(); ++k) {
+            for (int ax = 0; ax < D; ++ax)
+                quantise_bounds(org[ax], e[ax], kids[k].box.lo.v[ax], kids[k].box.hi.v[ax], &w.q[ax][k],
+                                &w.q[D + ax][k]);
+            if (kids[k].ref < 0) {
+                w.ref[k] = kids[k].ref;  // one primitive per leaf: ~record
+            } else {
+                int32_t r;
+                deepest = std::max(deepest, build(kids[k].ref, kids[k].box, &r));
+                w.ref[k] = r;
+            }
+        }
+        img.wnodes[me] = w;
+        const int k = (int)kids.size();
+        return std::max(k, (k - 1) + deepest);
+    }
+};
+
+template <int D>
+void flatten_wide_from_pairs(const std::vector<typename DeviceImage<D>::Pair> &pairs, int32_t root_ref,
+                             const float *root_lo, const float *root_hi, DeviceImage<D> &img) {
+    img.wnodes.clear();
+    if (root_ref < 0) {
+        img.wroot_ref = root_ref;
+        img.wide_stack = 1;
+        return;
+    }
+    Box<D> box;
+    for (int k = 0; k < D; ++k) box.lo.v[k] = root_lo[k], box.hi.v[k] = root_hi[k];
+    PairWideBuilder<D> wb{pairs, img};
+    int32_t r;
+    img.wide_stack = wb.build(root_ref, box, &r);
+    img.wroot_ref = r;
+}
+
 template void flatten_bvh<2>(const PrimSource<2> &, const BvhTree<2> &, DeviceImage<2> &);
 template void flatten_bvh<3>(const PrimSource<3> &, const BvhTree<3> &, DeviceImage<3> &);
 template void flatten_wide<2>(const BvhTree<2> &, DeviceImage<2> &);
 template void flatten_wide<3>(const BvhTree<3> &, DeviceImage<3> &);
+template void flatten_wide_from_pairs<2>(const std::vector<gq_pair2_t> &, int32_t, const float *, const float *,
+                                         DeviceImage<2> &);
+template void flatten_wide_from_pairs<3>(const std::vector<gq_pair3_t> &, int32_t, const float *, const float *,
+                                         DeviceImage<3> &);
 template void flatten_snch<2>(const BvhTree<2> &, const SnchTree<2> &, DeviceImage<2> &, int);
 template void flatten_snch<3>(const BvhTree<3> &, const SnchTree<3> &, DeviceImage<3> &, int);
 

@@ -45,6 +45,13 @@ void flatten_bvh(const PrimSource<D> &src, const BvhTree<D> &t, DeviceImage<D> &
 template <int D>
 void flatten_wide(const BvhTree<D> &t, DeviceImage<D> &img);
 
+// flatten_wide over a binary tree given as pair records (pair i: both child boxes of
+// interior node i and their references, leaf = ~primitive record), e.g. one built on
+// the device; root box and reference given.
+template <int D>
+void flatten_wide_from_pairs(const std::vector<typename DeviceImage<D>::Pair> &pairs, int32_t root_ref,
+                             const float *root_lo, const float *root_hi, DeviceImage<D> &img);
+
 // One silhouette in the device layout (also used for the brute-force silhouette list).
 void device_silhouette(const SilVertex &x, gq_silv_t &r);
 void device_silhouette(const SilEdge &x, gq_sile_t &r);

@@ -76,11 +76,12 @@ class Scene:
     """One polyline (dim 2) or triangle mesh (dim 3) with its acceleration structures.
 
     ``device=None`` builds on the host only (reference arrays, no queries);
-    ``gpu_build=True`` builds a linear BVH on the device in milliseconds (no wide
-    nodes, no reference arrays; answers equal to the host build's up to FP32 ties) and
-    an SNCH on the same tree whose cones are taken from the geometry (mesh silhouette
-    answers equal to closest_silhouette_baseline's, polyline ones to the host-built
-    SNCH's, up to FP32 ties)."""
+    ``gpu_build=True`` builds a linear BVH on the device in milliseconds (no reference
+    arrays; answers equal to the host build's up to FP32 ties), its collapse into
+    quantised 8-wide nodes (on the host, from the device-built pair records) and an SNCH
+    on the same tree whose cones are taken from the geometry (mesh silhouette answers
+    equal to closest_silhouette_baseline's, polyline ones to the host-built SNCH's, up
+    to FP32 ties)."""
 
     def __init__(self, vertices: ArrayLike, indices: ArrayLike, dim: int, *, device: Optional[int] = 0,
                  build_snch: bool = True, build_wide: bool = True, max_prims_in_node: int = 10,
@@ -92,8 +93,7 @@ class Scene:
         self.vertices_host = v
         self.indices_host = f
         self.device = -1 if device is None else int(device)
-        if gpu_build:
-            build_wide = False  # the device build makes the binary BVH and the SNCH
+
         opts = L.BuildOpts(max_prims_in_node, n_threads, int(build_snch), int(build_wide), self.device,
                            int(gpu_build))
         h = C.c_void_p()

@@ -1,6 +1,6 @@
-"""Linear BVH built on the device: queries on it give the host-built scene's answers
-(same validity and distances, same primitive except at FP32 ties), for every variant
-that runs without the SNCH or wide nodes."""
+"""Scenes built on the device (linear BVH, its collapse into quantised 8-wide nodes, the
+SNCH): queries on them give the host-built scene's answers (same validity and
+distances, same primitive except at FP32 ties) in every variant."""
 import time
 
 import numpy as np
@@ -29,15 +29,16 @@ def test_device_build_matches_host_build(dim):
     t0 = time.perf_counter()
     dev = Scene(v, f, dim, device=0, gpu_build=True)
     assert time.perf_counter() - t0 < 30.0
-    assert dev.info["n_nodes"] == 2 * f.shape[0] - 1 and dev.info["n_wide_nodes"] == 0
+    assert dev.info["n_nodes"] == 2 * f.shape[0] - 1 and dev.info["n_wide_nodes"] > 0
     assert 1 <= dev.info["max_depth"] <= 64
     q = W.uniform_points(50000, dim, seed=3)
     o, d = W.rays(50000, dim, seed=4)
     ref_cp = host.closest_point(q, variant="exact")
     ref_ray = host.intersect(o, d, variant="exact")
-    for variant in ("exact", "coherent", "auto"):
+    for variant in ("exact", "coherent", "wide8", "auto"):
         _check(ref_cp, dev.closest_point(q, variant=variant), f"cp {variant}")
-    _check(ref_ray, dev.intersect(o, d, variant="exact"), "ray exact")
+    for variant in ("exact", "wide8"):
+        _check(ref_ray, dev.intersect(o, d, variant=variant), f"ray {variant}")
     _check(host.intersect(o, d, 0.7, variant="exact"), dev.intersect(o, d, 0.7, variant="auto"), "ray r_max")
     assert dev.device_error() == 0
 
@@ -47,13 +48,17 @@ def test_device_build_limits_and_files(tmp_path):
     dev = Scene(v, f, 3, device=0, gpu_build=True)
     with pytest.raises(L.GQError, match="built on the device"):
         dev.ref_array(L.ARRAY_BVH_NODES)
+    nowide = Scene(v, f, 3, device=0, gpu_build=True, build_wide=False)
     with pytest.raises(L.GQError, match="wide"):
-        dev.closest_point(W.uniform_points(10, 3, seed=0), variant="wide8")
+        nowide.closest_point(W.uniform_points(10, 3, seed=0), variant="wide8")
     path = tmp_path / "dev.gqs"
     dev.save(path)
     back = Scene.load(path, device=0)
     q = W.uniform_points(5000, 3, seed=9)
     a, b = to_np(dev.closest_point(q, variant="exact")), to_np(back.closest_point(q, variant="exact"))
+    for k in ("valid", "d", "prim_id"):
+        assert np.array_equal(np.asarray(a[k]), np.asarray(b[k]))
+    a, b = to_np(dev.closest_point(q, variant="wide8")), to_np(back.closest_point(q, variant="wide8"))
     for k in ("valid", "d", "prim_id"):
         assert np.array_equal(np.asarray(a[k]), np.asarray(b[k]))
     with pytest.raises(L.GQError, match="built on the device"):
