@@ -102,9 +102,11 @@ __device__ __forceinline__ void closest_silhouette(const DevScene &s, const floa
                         box_dist3(P.lo[c][0], P.lo[c][1], P.lo[c][D - 1], P.hi[c][0], P.hi[c][1], P.hi[c][D - 1],
                                   x[0], x[1], x[D - 1], dm[c], dmax);
                     hit[c] = dm[c] <= L.r;
+                    // the node bound first: it rejects most of what the cone test rejects, for less
+                    // (both must admit a child, so the order changes no decision)
+                    if (hit[c]) hit[c] = !snch::child_free<D>(s, P, c, x);
                     if ((P.half[c] >= 0.f) & hit[c])
                         hit[c] = cone_overlaps_fast<D>(P.lo[c], P.hi[c], P.ax[c], P.half[c], P.rad[c], x, dm[c]);
-                    if (hit[c]) hit[c] = !snch::child_free<D>(s, P, c, x);
                 }
                 // push the farther first so the nearer is taken first (selects, not indexed
                 // arrays, so that nothing here lives in local memory)

@@ -202,9 +202,11 @@ __device__ __forceinline__ void visit_interior(const DevScene &s, Lane<D> &L, in
             box_dist3(P.lo[c][0], P.lo[c][1], P.lo[c][D - 1], P.hi[c][0], P.hi[c][1], P.hi[c][D - 1], L.x[0],
                       L.x[1], L.x[D - 1], dm[c], dmax);
         hit[c] = dm[c] <= L.r;
+        // the node bound first: it rejects most of what the cone test rejects, for less
+        // (both must admit a child, so the order changes no decision)
+        if (hit[c]) hit[c] = !child_free<D>(s, P, c, L.x);
         if ((P.half[c] >= 0.f) & hit[c])
             hit[c] = cone_overlaps<D>(P.lo[c], P.hi[c], P.ax[c], P.half[c], P.rad[c], L.x, dm[c]);
-        if (hit[c]) hit[c] = !child_free<D>(s, P, c, L.x);
     }
     if (hit[0] & hit[1]) {
         if (L.sp + 2 >= GQ_STACK_EXACT) {
