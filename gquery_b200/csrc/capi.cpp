@@ -125,7 +125,8 @@ gq_status build_on_device(gq_scene *s, const gq_build_opts &o) {
             if (e != cudaSuccess) return fail_cuda(e, "device build: pair download");
         }
         try {
-            flatten_wide_from_pairs<D>(hp, r.root_ref, r.root_lo, r.root_hi, wimg);
+            flatten_wide_from_pairs<D>(hp, r.root_ref, r.root_lo, r.root_hi, wimg,
+                                       o.n_threads > 0 ? o.n_threads : (int)std::max(1u, std::thread::hardware_concurrency()));
         } catch (const std::bad_alloc &) {
             return fail(GQ_ERR_NOMEM, "out of host memory collapsing the device-built tree");
         }

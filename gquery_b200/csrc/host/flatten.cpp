@@ -2,6 +2,7 @@
 #include "flatten.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <thread>
@@ -465,16 +466,23 @@ void flatten_snch(const BvhTree<D> &t, const SnchTree<D> &s, DeviceImage<D> &img
 
 // The same collapse over a binary tree given as pair records (a device-built tree: pair
 // i holds both child boxes of interior node i and their references, leaf = ~record).
+// The top levels are built first; the interior children found at depth kDeferDepth are
+// built as separate subtrees on threads and appended with their indices shifted.
 template <int D>
 struct PairWideBuilder {
     using Pair = typename DeviceImage<D>::Pair;
-    const std::vector<Pair> &pairs;
-    DeviceImage<D> &img;
-
-    struct Kid {
-        int32_t ref;
+    using WNode = typename DeviceImage<D>::WNode;
+    struct Deferred {
+        int32_t node;
         Box<D> box;
+        size_t wnode;
+        int slot;
     };
+    const std::vector<Pair> &pairs;
+    std::vector<WNode> &out;
+    int defer_depth;                   // < 0: build everything here
+    std::vector<Deferred> *deferred;
+
     static Box<D> child_box(const Pair &p, int c) {
         Box<D> b;
         if constexpr (D == 2) {
@@ -487,7 +495,11 @@ struct PairWideBuilder {
         return b;
     }
 
-    int build(int32_t node, const Box<D> &box, int32_t *ref_out) {
+    int32_t build(int32_t node, const Box<D> &box, int depth) {
+        struct Kid {
+            int32_t ref;
+            Box<D> box;
+        };
         const Pair &pn = pairs[(size_t)node];
         std::vector<Kid> kids{{pn.ref_l, child_box(pn, 0)}, {pn.ref_r, child_box(pn, 1)}};
         while (kids.size() < GQ_WIDTH) {  // open the interior child with the largest area
@@ -507,13 +519,12 @@ struct PairWideBuilder {
             kids[(size_t)pick] = Kid{pc.ref_l, child_box(pc, 0)};
             kids.insert(kids.begin() + pick + 1, Kid{pc.ref_r, child_box(pc, 1)});
         }
-        const size_t me = img.wnodes.size();
-        img.wnodes.emplace_back();
-        *ref_out = (int32_t)me;
+        const size_t me = out.size();
+        out.emplace_back();
         int e[D];
         float org[D];
         for (int k = 0; k < D; ++k) quant_axis(box.lo.v[k], box.hi.v[k], &org[k], &e[k]);
-        typename DeviceImage<D>::WNode w;
+        WNode w;
         std::memset(&w, 0, sizeof w);
         if constexpr (D == 2) {
             w.ox = org[0];
@@ -527,28 +538,40 @@ struct PairWideBuilder {
                      ((uint32_t)kids.size() << 24);
         }
         for (int k = 0; k < GQ_WIDTH; ++k) w.ref[k] = kEmptyLeaf;
-        int deepest = 0;
-        for (size_t k = 0; k < kids.size(); ++k) {
+        for (size_t k = 0; k < kids.size(); ++k)
             for (int ax = 0; ax < D; ++ax)
                 quantise_bounds(org[ax], e[ax], kids[k].box.lo.v[ax], kids[k].box.hi.v[ax], &w.q[ax][k],
                                 &w.q[D + ax][k]);
+        out[me] = w;
+        for (size_t k = 0; k < kids.size(); ++k) {
             if (kids[k].ref < 0) {
-                w.ref[k] = kids[k].ref;  // one primitive per leaf: ~record
+                out[me].ref[k] = kids[k].ref;  // one primitive per leaf: ~record
+            } else if (defer_depth >= 0 && depth + 1 >= defer_depth) {
+                deferred->push_back(Deferred{kids[k].ref, kids[k].box, me, (int)k});
             } else {
-                int32_t r;
-                deepest = std::max(deepest, build(kids[k].ref, kids[k].box, &r));
-                w.ref[k] = r;
+                const int32_t r = build(kids[k].ref, kids[k].box, depth + 1);
+                out[me].ref[k] = r;
             }
         }
-        img.wnodes[me] = w;
-        const int k = (int)kids.size();
-        return std::max(k, (k - 1) + deepest);
+        return (int32_t)me;
     }
 };
 
+// Stack entries a traversal of wide node w needs once it is popped (as flatten_wide
+// computes while building).
+template <int D>
+static int wide_need(const std::vector<typename DeviceImage<D>::WNode> &w, int32_t i) {
+    const int k = (int)(w[(size_t)i].meta >> 24);
+    int deepest = 0;
+    for (int c = 0; c < k; ++c)
+        if (w[(size_t)i].ref[c] >= 0) deepest = std::max(deepest, wide_need<D>(w, w[(size_t)i].ref[c]));
+    return std::max(k, (k - 1) + deepest);
+}
+
 template <int D>
 void flatten_wide_from_pairs(const std::vector<typename DeviceImage<D>::Pair> &pairs, int32_t root_ref,
-                             const float *root_lo, const float *root_hi, DeviceImage<D> &img) {
+                             const float *root_lo, const float *root_hi, DeviceImage<D> &img, int n_threads) {
+    using WNode = typename DeviceImage<D>::WNode;
     img.wnodes.clear();
     if (root_ref < 0) {
         img.wroot_ref = root_ref;
@@ -557,10 +580,32 @@ void flatten_wide_from_pairs(const std::vector<typename DeviceImage<D>::Pair> &p
     }
     Box<D> box;
     for (int k = 0; k < D; ++k) box.lo.v[k] = root_lo[k], box.hi.v[k] = root_hi[k];
-    PairWideBuilder<D> wb{pairs, img};
-    int32_t r;
-    img.wide_stack = wb.build(root_ref, box, &r);
-    img.wroot_ref = r;
+    constexpr int kDeferDepth = 3;  // up to 8^3 subtrees for the threads
+    std::vector<typename PairWideBuilder<D>::Deferred> deferred;
+    PairWideBuilder<D> top{pairs, img.wnodes, kDeferDepth, &deferred};
+    img.wroot_ref = top.build(root_ref, box, 0);
+    std::vector<std::vector<WNode>> parts(deferred.size());
+    std::atomic<size_t> next{0};
+    auto work = [&]() {
+        for (size_t i; (i = next.fetch_add(1)) < deferred.size();) {
+            PairWideBuilder<D> sub{pairs, parts[i], -1, nullptr};
+            sub.build(deferred[i].node, deferred[i].box, 0);
+        }
+    };
+    const int nt = std::max(1, std::min<int>(n_threads, (int)deferred.size()));
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) pool.emplace_back(work);
+    work();
+    for (auto &th : pool) th.join();
+    for (size_t i = 0; i < deferred.size(); ++i) {  // append, shifting the subtree's own indices
+        const int32_t base = (int32_t)img.wnodes.size();
+        for (WNode &w : parts[i])
+            for (int k = 0; k < GQ_WIDTH; ++k)
+                if (w.ref[k] >= 0) w.ref[k] += base;
+        img.wnodes.insert(img.wnodes.end(), parts[i].begin(), parts[i].end());
+        img.wnodes[deferred[i].wnode].ref[deferred[i].slot] = base;
+    }
+    img.wide_stack = wide_need<D>(img.wnodes, img.wroot_ref);
 }
 
 template void flatten_bvh<2>(const PrimSource<2> &, const BvhTree<2> &, DeviceImage<2> &);
@@ -568,9 +613,9 @@ template void flatten_bvh<3>(const PrimSource<3> &, const BvhTree<3> &, DeviceIm
 template void flatten_wide<2>(const BvhTree<2> &, DeviceImage<2> &);
 template void flatten_wide<3>(const BvhTree<3> &, DeviceImage<3> &);
 template void flatten_wide_from_pairs<2>(const std::vector<gq_pair2_t> &, int32_t, const float *, const float *,
-                                         DeviceImage<2> &);
+                                         DeviceImage<2> &, int);
 template void flatten_wide_from_pairs<3>(const std::vector<gq_pair3_t> &, int32_t, const float *, const float *,
-                                         DeviceImage<3> &);
+                                         DeviceImage<3> &, int);
 template void flatten_snch<2>(const BvhTree<2> &, const SnchTree<2> &, DeviceImage<2> &, int);
 template void flatten_snch<3>(const BvhTree<3> &, const SnchTree<3> &, DeviceImage<3> &, int);
 

@@ -47,10 +47,11 @@ void flatten_wide(const BvhTree<D> &t, DeviceImage<D> &img);
 
 // flatten_wide over a binary tree given as pair records (pair i: both child boxes of
 // interior node i and their references, leaf = ~primitive record), e.g. one built on
-// the device; root box and reference given.
+// the device; root box and reference given; deep subtrees on n_threads threads (the
+// nodes are the same for any thread count, their numbering not).
 template <int D>
 void flatten_wide_from_pairs(const std::vector<typename DeviceImage<D>::Pair> &pairs, int32_t root_ref,
-                             const float *root_lo, const float *root_hi, DeviceImage<D> &img);
+                             const float *root_lo, const float *root_hi, DeviceImage<D> &img, int n_threads = 1);
 
 // One silhouette in the device layout (also used for the brute-force silhouette list).
 void device_silhouette(const SilVertex &x, gq_silv_t &r);
