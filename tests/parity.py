@@ -52,3 +52,32 @@ def tie_report(a: dict, b: dict, rel=REL_TOL) -> dict:
         "prim_mismatch_not_tie": int(np.count_nonzero(prim_diff & (reldiff > rel))),
         "max_rel_d": float(reldiff[both].max()) if both.any() else 0.0,
     }
+
+
+def sil_variant_report(exact: dict, variant: dict, brute: dict, rel=REL_TOL) -> dict:
+    """Like tie_report for a fast silhouette variant against the exact one, with one more
+    allowance: the reference's normal-cone test may reject a node that holds the true
+    nearest silhouette (its cones reuse face 0's normal and measure their radius from edge
+    midpoints), while the fast variants' cone test admits every node the reference admits
+    and sometimes more.  A variant answer that is strictly nearer than the exact one and
+    equals the brute-force nearest silhouette is counted in `nearer_true`, not as a
+    mismatch; every other differing primitive must be a tie."""
+    va, vv = np.asarray(exact["valid"]).astype(bool), np.asarray(variant["valid"]).astype(bool)
+    de, dv = np.asarray(exact["d"], np.float64), np.asarray(variant["d"], np.float64)
+    db = np.asarray(brute["d"], np.float64)
+    vb = np.asarray(brute["valid"]).astype(bool)
+    scale = np.maximum(np.maximum(np.abs(de), np.abs(dv)), 1e-30)
+    nearer_true = va & vv & vb & (dv < de) & (np.abs(dv - db) <= rel * np.maximum(np.abs(db), 1e-30))
+    keep = ~nearer_true
+    rep = tie_report({k: np.asarray(exact[k])[keep] for k in ("valid", "prim_id", "d")},
+                     {k: np.asarray(variant[k])[keep] for k in ("valid", "prim_id", "d")}, rel)
+    rep["nearer_true"] = int(np.count_nonzero(nearer_true))
+    rep["max_rel_gain"] = float(((de - dv) / scale)[nearer_true].max()) if nearer_true.any() else 0.0
+    return rep
+
+
+def assert_sil_variant(exact: dict, variant: dict, brute: dict, what="", max_nearer=0.01):
+    rep = sil_variant_report(exact, variant, brute)
+    ok = (rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0 and rep["max_rel_d"] <= REL_TOL
+          and rep["nearer_true"] <= max_nearer * rep["n"])
+    assert ok, (what, rep)
