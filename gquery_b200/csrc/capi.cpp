@@ -820,7 +820,7 @@ struct SceneFileHeader {
 constexpr char kSceneMagic[8] = {'G', 'Q', 'S', 'C', 'E', 'N', 'E', '1'};
 // 2: 3D silhouette edges carry the pre-test spans (gq_sile_t.span0 / span1)
 // 3: 3D SNCH pairs carry the node bounds of both children (gq_spair3_t.l_b / r_b)
-constexpr int32_t kSceneFileVersion = 3;
+constexpr int32_t kSceneFileVersion = 4;
 
 struct File {
     FILE *f = nullptr;

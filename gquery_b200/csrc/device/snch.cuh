@@ -134,7 +134,7 @@ template <int D>
 struct PairView {
     float lo[2][D], hi[2][D], ax[2][D], half[2], rad[2];
     int refs[2];
-    float nb[2][D == 3 ? 9 : 1];
+    float nb[2][D == 3 ? 10 : 1];
 };
 
 template <int D>
@@ -168,9 +168,9 @@ __device__ __forceinline__ void load_pair(const DevScene &s, int ref, PairView<D
         float *n0 = P.nb[0], *n1 = P.nb[D == 3 ? 1 : 0];
         if (D == 3) {
             n0[0] = f6.x; n0[1] = f6.y; n0[2] = f6.z; n0[3] = f6.w; n0[4] = f7.x;
-            n0[5] = f7.y; n0[6] = f7.z; n0[7] = f7.w; n0[8] = f8.x;
-            n1[0] = f8.y; n1[1] = f8.z; n1[2] = f8.w; n1[3] = f9.x; n1[4] = f9.y;
-            n1[5] = f9.z; n1[6] = f9.w; n1[7] = f10.x; n1[8] = f10.y;
+            n0[5] = f7.y; n0[6] = f7.z; n0[7] = f7.w; n0[8] = f8.x; n0[9] = f8.y;
+            n1[0] = f8.z; n1[1] = f8.w; n1[2] = f9.x; n1[3] = f9.y; n1[4] = f9.z;
+            n1[5] = f9.w; n1[6] = f10.x; n1[7] = f10.y; n1[8] = f10.z; n1[9] = f10.w;
         }
     }
 }
@@ -183,7 +183,7 @@ __device__ __forceinline__ bool child_free(const DevScene &s, const PairView<D> 
     if (D == 2) return false;
     const float *b = P.nb[D == 3 ? c : 0];
     const float m = sil_node_margin(fmaxf(fmaxf(fabsf(x[0]), fabsf(x[1])), fabsf(x[D - 1])), s.coord_bound);
-    return sil_node_excluded(b[0], b[1], b[2], b[3], b[4], b[5], b[6], b[7], b[8], x[0], x[1], x[D - 1], m);
+    return sil_node_excluded(b[0], b[1], b[2], b[3], b[4], b[5], b[6], b[7], b[8], b[9], x[0], x[1], x[D - 1], m);
 }
 
 // Interior node `ref`: both children against the current r_max, closer pushed last.

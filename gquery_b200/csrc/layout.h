@@ -100,8 +100,8 @@ typedef struct {  // 2D, 80 B
 } gq_spair2_t;
 
 // 3D, 176 B: the reference's boxes and cones of both children (96 B), then per child
-// the node bound of sil_filter.h (box centre, axis, delta, lo, hi) that proves a child
-// free of silhouettes for a query point.
+// the node bound of sil_filter.h (box centre, axis, cos and sin of the normal cone's
+// half-angle, lo, hi) that proves a child free of silhouettes for a query point.
 typedef struct {
     float l_lox, l_loy, l_loz, l_hix;
     float l_hiy, l_hiz, l_ax, l_ay;
@@ -110,8 +110,7 @@ typedef struct {
     float r_hiz, r_ax, r_ay, r_az;
     float r_half, r_rad;
     int32_t ref_l, ref_r;
-    float l_b[9], r_b[9];
-    float pad0, pad1;
+    float l_b[10], r_b[10];
 } gq_spair3_t;
 
 // Quantised 8-wide node, 3D: 96 B (three 32-byte sectors).

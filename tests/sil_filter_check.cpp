@@ -100,7 +100,8 @@ void print(const char *name, const Count &k, bool last) {
 
 
 // Node bound: a patch of a height field z = h(x, y) (smooth waves plus noise of a
-// chosen amplitude), triangulated consistently; every interior edge is a silhouette
+// chosen amplitude) or a spherical cap (normals spread up to `cap` radians from its
+// axis), triangulated consistently; every interior edge is a silhouette
 // record whose end points are stored in winding order (orientation +1) or swapped
 // (both stored normals point the other way, orientation -1), as the reference's
 // records come.  The patch is placed with a random rotation, scale and offset.
@@ -108,6 +109,7 @@ struct Patch {
     std::vector<SilEdgeGeom> edges;
     float c[3];
     float bound;  // largest |coordinate|
+    V sphere;     // centre of the cap's sphere (cap patches)
 };
 
 V rot(V v, const float R[9]) {
@@ -115,7 +117,7 @@ V rot(V v, const float R[9]) {
             R[6] * v.x + R[7] * v.y + R[8] * v.z};
 }
 
-Patch make_patch(Rng &r, int g, float rough) {
+Patch make_patch(Rng &r, int g, float rough, float cap = 0.f) {
     // random rotation from a random unit quaternion
     float q0 = r.uni(-1, 1), q1 = r.uni(-1, 1), q2 = r.uni(-1, 1), q3 = r.uni(-1, 1);
     const float qn = std::sqrt(q0 * q0 + q1 * q1 + q2 * q2 + q3 * q3);
@@ -127,14 +129,22 @@ Patch make_patch(Rng &r, int g, float rough) {
     const V off = mul(rand_in(r, 1.f), s * r.uni(0.f, 3.f));
     const float w1 = r.uni(0.5f, 4.f), w2 = r.uni(0.5f, 4.f), amp = r.uni(0.f, 0.3f);
     std::vector<V> p((size_t)(g + 1) * (g + 1));
+    const float tc = std::tan(cap) / std::sqrt(2.f);  // the cap's corners lie `cap` off its axis
     for (int i = 0; i <= g; ++i)
         for (int j = 0; j <= g; ++j) {
             const float u = (float)i / g, v = (float)j / g;
-            const float z = amp * std::sin(w1 * u + 1.3f) * std::cos(w2 * v) + rough * r.uni(-1.f, 1.f) / g;
-            p[(size_t)i * (g + 1) + j] = add(mul(rot({u - 0.5f, v - 0.5f, z}, R), s), off);
+            V q;
+            if (cap > 0.f) {
+                q = unit(V{2.f * (u - 0.5f) * tc, 2.f * (v - 0.5f) * tc, 1.f});
+            } else {
+                const float z = amp * std::sin(w1 * u + 1.3f) * std::cos(w2 * v) + rough * r.uni(-1.f, 1.f) / g;
+                q = V{u - 0.5f, v - 0.5f, z};
+            }
+            p[(size_t)i * (g + 1) + j] = add(mul(rot(q, R), s), off);
         }
     auto at = [&](int i, int j) { return p[(size_t)i * (g + 1) + j]; };
     Patch P;
+    P.sphere = off;
     // triangles (i,j),(i+1,j),(i+1,j+1) and (i,j),(i+1,j+1),(i,j+1); interior diagonal and
     // grid edges with their two faces in winding order: edge a->b of face (a, b, c), the
     // other face (b, a, d)
@@ -177,9 +187,9 @@ struct NodeCount {
     long long cases = 0, excluded = 0, unsound = 0;
 };
 
-void check_node(Rng &r, int g, float rough, NodeCount &k) {
-    Patch P = make_patch(r, g, rough);
-    float b[9];
+void check_node(Rng &r, int g, float rough, NodeCount &k, float cap = 0.f) {
+    Patch P = make_patch(r, g, rough, cap);
+    float b[10];
     sil_node_bound(P.c[0], P.c[1], P.c[2], 0, (long long)P.edges.size(),
                    [&](long long j) { return P.edges[(size_t)j]; }, b);
     const float s = std::fmax(P.bound, 1e-6f);
@@ -187,8 +197,10 @@ void check_node(Rng &r, int g, float rough, NodeCount &k) {
         // queries: near the patch (within 1e-6 .. 2 of its size), and far
         V x;
         const V c{P.c[0], P.c[1], P.c[2]};
-        const int kind = (int)(r.next() % 3);
-        if (kind == 0) {
+        const int kind = (int)(r.next() % (cap > 0.f ? 4 : 3));
+        if (kind == 3) {  // near the centre of the cap's sphere
+            x = add(P.sphere, mul(unit(rand_in(r, 1.f)), r.logu(1e-4f, 0.3f) * s));
+        } else if (kind == 0) {
             const SilEdgeGeom &e = P.edges[r.next() % P.edges.size()];
             x = add(V{e.a[0], e.a[1], e.a[2]}, mul(unit(rand_in(r, 1.f)), r.logu(1e-7f, 1.f) * s));
         } else if (kind == 1) {
@@ -197,7 +209,7 @@ void check_node(Rng &r, int g, float rough, NodeCount &k) {
             x = add(c, mul(unit(rand_in(r, 1.f)), r.logu(2.f, 1e3f) * s));
         }
         const float m = g_margin_scale * sil_node_margin(amax(x), P.bound);
-        const bool ex = sil_node_excluded(b[0], b[1], b[2], b[3], b[4], b[5], b[6], b[7], b[8], x.x, x.y, x.z, m);
+        const bool ex = sil_node_excluded(b[0], b[1], b[2], b[3], b[4], b[5], b[6], b[7], b[8], b[9], x.x, x.y, x.z, m);
         ++k.cases;
         if (!ex) continue;
         ++k.excluded;
@@ -274,11 +286,12 @@ int main(int argc, char **argv) {
             check(a, b, c, d, x, bound_of(a, b, c, d), on_edge);
         }
     }
-    NodeCount smooth, rough, flat;
+    NodeCount smooth, rough, flat, capn;
     for (long long i = 0; i < n / 200; ++i) {
         check_node(r, 2 + (int)(r.next() % 7), 0.f, smooth);
         check_node(r, 2 + (int)(r.next() % 7), r.logu(1e-3f, 2.f), rough);
         check_node(r, 2 + (int)(r.next() % 7), 1e-6f, flat);
+        check_node(r, 2 + (int)(r.next() % 7), 0.f, capn, r.uni(0.35f, 1.48f));  // 20 .. 85 degrees
     }
     std::printf("{");
     print("generic", generic, false);
@@ -290,10 +303,11 @@ int main(int argc, char **argv) {
     print("on_edge", on_edge, false);
     print_node("node_smooth", smooth, false);
     print_node("node_rough", rough, false);
-    print_node("node_flat", flat, true);
+    print_node("node_flat", flat, false);
+    print_node("node_cap", capn, true);
     std::printf("}\n");
     const long long bad = generic.unsound + coplanar.unsound + near_plane.unsound + sliver.unsound +
                           zero_len.unsound + far.unsound + on_edge.unsound + smooth.unsound + rough.unsound +
-                          flat.unsound;
+                          flat.unsound + capn.unsound;
     return bad ? 1 : 0;
 }

@@ -1,8 +1,9 @@
 """The silhouette-edge pre-test never excludes an edge the reference's test calls a
 silhouette (random, nearly coplanar, sliver, zero-length, far and on-edge cases), and
 without its margin it would: the cases reach the rounding boundary the margin covers.
-The node bound never excludes a patch of edges (smooth, rough or flat height fields
-whose records come in either orientation) that holds a silhouette for the query."""
+The node bound never excludes a patch of edges (smooth, rough or flat height fields and
+spherical caps, whose records come in either orientation) that holds a silhouette for
+the query."""
 import json
 import shutil
 import subprocess
@@ -39,6 +40,9 @@ def test_pre_test_is_sound(checker):
     # the node bound skips patches, and with mixed record orientations too
     for k in ("node_smooth", "node_rough", "node_flat"):
         assert res[k]["excluded"] > 0.2 * res[k]["cases"], (k, res[k])
+    # caps seen from near their sphere's centre: the normal-cone form skips them for
+    # spreads up to 85 degrees (a bound by |s n - A| alone stops near 60)
+    assert res["node_cap"]["excluded"] > 0.3 * res["node_cap"]["cases"], res["node_cap"]
 
 
 def test_margin_is_needed(checker):
