@@ -820,7 +820,8 @@ struct SceneFileHeader {
 constexpr char kSceneMagic[8] = {'G', 'Q', 'S', 'C', 'E', 'N', 'E', '1'};
 // 2: 3D silhouette edges carry the pre-test spans (gq_sile_t.span0 / span1)
 // 3: 3D SNCH pairs carry the node bounds of both children (gq_spair3_t.l_b / r_b)
-constexpr int32_t kSceneFileVersion = 4;
+// 5: the node bounds hold the delta and cone forms and the pair record is 160 B
+constexpr int32_t kSceneFileVersion = 5;
 
 struct File {
     FILE *f = nullptr;

@@ -325,7 +325,7 @@ __global__ void k_snch_pairs(int64_t n, const int2 *child, const int2 *range, co
     const float lo[3] = {c ? P.r_lox : P.l_lox, c ? P.r_loy : P.l_loy, c ? P.r_loz : P.l_loz};
     const float hi[3] = {c ? P.r_hix : P.l_hix, c ? P.r_hiy : P.l_hiy, c ? P.r_hiz : P.l_hiz};
     float ctr[3];
-    for (int k = 0; k < 3; ++k) ctr[k] = 0.5f * (lo[k] + hi[k]);
+    for (int k = 0; k < 3; ++k) ctr[k] = sil_node_centre(lo[k], hi[k]);
     int64_t b0, b1;
     if (ref < 0) {
         b0 = 3 * (int64_t)~ref;
@@ -354,7 +354,7 @@ __global__ void k_snch_pairs(int64_t n, const int2 *child, const int2 *range, co
     if (!open)
         for (int k = 0; k < 3; ++k) A[k] = (float)(m[k] / ml);
     // pass 2: spread of the oriented normals around A, plane offsets, cone, radius
-    double mlo = __builtin_inf(), mhi = -__builtin_inf(), cmin = 1.0, cnode = 1.0, rmax = 0.0;
+    double dmax = 0.0, mlo = __builtin_inf(), mhi = -__builtin_inf(), cmin = 1.0, cnode = 1.0, rmax = 0.0;
     const double al = sqrt((double)A[0] * A[0] + (double)A[1] * A[1] + (double)A[2] * A[2]);
     for (int64_t j = b0 + lane; j < b1; j += 32) {
         const gq_sile_t &r = sils[j];
@@ -368,19 +368,22 @@ __global__ void k_snch_pairs(int64_t n, const int2 *child, const int2 *range, co
         rmax = fmax(rmax, sqrt(fmax(ra, rb)));
         for (int f = 0; f < 2; ++f) {
             const double nn[3] = {o * (f ? r.n1x : r.n0x), o * (f ? r.n1y : r.n0y), o * (f ? r.n1z : r.n0z)};
-            double nl = 0.0, ac = 0.0, sp = 0.0, cs = 0.0;
+            double d2 = 0.0, nl = 0.0, ac = 0.0, sp = 0.0, cs = 0.0;
             for (int k = 0; k < 3; ++k) {
+                d2 += (nn[k] - A[k]) * (nn[k] - A[k]);
                 nl += nn[k] * nn[k];
                 ac += nn[k] * (a[k] - ctr[k]);
                 sp += nn[k] * (b[k] - a[k]);
                 cs += nn[k] * A[k];
             }
+            dmax = fmax(dmax, sqrt(d2));
             mlo = fmin(mlo, ac + fmin(0.0, sp));
             mhi = fmax(mhi, ac + fmax(0.0, sp));
             cmin = fmin(cmin, cs);
             if (!open) cnode = fmin(cnode, cs / (sqrt(nl) * al));
         }
     }
+    dmax = warp_max(dmax);
     cnode = warp_min(cnode);
     mlo = warp_min(mlo);
     mhi = warp_max(mhi);
@@ -390,13 +393,14 @@ __global__ void k_snch_pairs(int64_t n, const int2 *child, const int2 *range, co
     // cone: the largest angle to A (normals are unit up to rounding: clamp), widened
     const double half = open ? 3.14159265358979 : acos(fmax(-1.0, fmin(1.0, cmin))) + 1e-5;
     const float rad = up(rmax * (1.0 + 1e-6) + 1e-30);
-    // node bound of sil_filter.h: never skipped when open (lo = -inf, hi = +inf)
-    float nb[10] = {ctr[0], ctr[1], ctr[2], A[0], A[1], A[2], 1.f, 0.f, -__builtin_inff(), __builtin_inff()};
+    // node bound of sil_filter.h: never skipped when open (delta = +inf, lo = -inf, hi = +inf)
+    float nb[kSilNodeBound] = {A[0], A[1], A[2], __builtin_inff(), 1.f, 0.f, -__builtin_inff(), __builtin_inff()};
     if (!open) {
         const double pad = 1e-12 * (fabs(mlo) + fabs(mhi) + 1.0);
-        sil_cone_of(cnode, nb[6], nb[7]);
-        nb[8] = down(mlo - pad);
-        nb[9] = up(mhi + pad);
+        nb[3] = up(dmax * (1.0 + 1e-12));
+        sil_cone_of(cnode, nb[4], nb[5]);
+        nb[6] = down(mlo - pad);
+        nb[7] = up(mhi + pad);
     }
     gq_spair3_t &S = spairs[p];
     const int out_ref = ref < 0 ? ~(3 * ~ref) : ref;  // leaf: its first silhouette record
@@ -407,7 +411,7 @@ __global__ void k_snch_pairs(int64_t n, const int2 *child, const int2 *range, co
         S.l_half = up(half);
         S.l_rad = rad;
         S.ref_l = out_ref;
-        for (int k = 0; k < 10; ++k) S.l_b[k] = nb[k];
+        for (int k = 0; k < kSilNodeBound; ++k) S.l_b[k] = nb[k];
     } else {
         S.r_lox = lo[0]; S.r_loy = lo[1]; S.r_loz = lo[2];
         S.r_hix = hi[0]; S.r_hiy = hi[1]; S.r_hiz = hi[2];
@@ -415,7 +419,7 @@ __global__ void k_snch_pairs(int64_t n, const int2 *child, const int2 *range, co
         S.r_half = up(half);
         S.r_rad = rad;
         S.ref_r = out_ref;
-        for (int k = 0; k < 10; ++k) S.r_b[k] = nb[k];
+        for (int k = 0; k < kSilNodeBound; ++k) S.r_b[k] = nb[k];
     }
 }
 

@@ -26,6 +26,10 @@ namespace gqd {
 namespace pkt {
 
 constexpr int kSilNone = 0x7fffffff;
+// The packet form tests the node bound in its delta form only: its queries are dense
+// and rarely see a node head-on, where the cone form would skip more for twice the
+// arithmetic.
+constexpr bool kPacketCone = false;
 
 // One traversal for the lanes in `mask` (warp-uniform); all 32 lanes must call it.
 // L: this lane's query state (x and r set by the caller, as snch::lane_init would);
@@ -98,7 +102,7 @@ __device__ __forceinline__ void closest_silhouette(const DevScene &s, unsigned m
                 hit[c] = dm[c] <= L.r;
                 // the node bound first: it rejects most of what the cone test rejects, for less
                 // (both must admit a child, so the order changes no decision)
-                if (hit[c]) hit[c] = !snch::child_free<D>(s, P, c, L.x);
+                if (hit[c]) hit[c] = !snch::child_free<D, kPacketCone>(s, P, c, L.x);
                 if ((P.half[c] >= 0.f) & hit[c])
                     hit[c] = cone_overlaps_fast<D>(P.lo[c], P.hi[c], P.ax[c], P.half[c], P.rad[c], L.x, dm[c]);
             }

@@ -126,7 +126,7 @@ __device__ __forceinline__ bool test_silhouette(const DevScene &s, Lane<D> &L, i
     return last;
 }
 
-constexpr int kSPair3Vec = 11;  // float4s per gq_spair3_t
+constexpr int kSPair3Vec = 10;  // float4s per gq_spair3_t
 
 // One pair record: both children's boxes and normal cones (the reference's), their
 // references and, in 3D, their node bounds (sil_filter.h).
@@ -134,7 +134,7 @@ template <int D>
 struct PairView {
     float lo[2][D], hi[2][D], ax[2][D], half[2], rad[2];
     int refs[2];
-    float nb[2][D == 3 ? 10 : 1];
+    float nb[2][D == 3 ? kSilNodeBound : 1];
 };
 
 template <int D>
@@ -154,7 +154,7 @@ __device__ __forceinline__ void load_pair(const DevScene &s, int ref, PairView<D
         const float4 f0 = ldg4(s.spairs, b), f1 = ldg4(s.spairs, b + 1), f2 = ldg4(s.spairs, b + 2),
                      f3 = ldg4(s.spairs, b + 3), f4 = ldg4(s.spairs, b + 4), f5 = ldg4(s.spairs, b + 5);
         const float4 f6 = ldg4(s.spairs, b + 6), f7 = ldg4(s.spairs, b + 7), f8 = ldg4(s.spairs, b + 8),
-                     f9 = ldg4(s.spairs, b + 9), f10 = ldg4(s.spairs, b + 10);
+                     f9 = ldg4(s.spairs, b + 9);
         P.lo[0][0] = f0.x; P.lo[0][1] = f0.y; P.lo[0][D - 1] = f0.z;
         P.hi[0][0] = f0.w; P.hi[0][1] = f1.x; P.hi[0][D - 1] = f1.y;
         P.ax[0][0] = f1.z; P.ax[0][1] = f1.w; P.ax[0][D - 1] = f2.x;
@@ -167,23 +167,28 @@ __device__ __forceinline__ void load_pair(const DevScene &s, int ref, PairView<D
         P.refs[1] = fbits(f5.w);
         float *n0 = P.nb[0], *n1 = P.nb[D == 3 ? 1 : 0];
         if (D == 3) {
-            n0[0] = f6.x; n0[1] = f6.y; n0[2] = f6.z; n0[3] = f6.w; n0[4] = f7.x;
-            n0[5] = f7.y; n0[6] = f7.z; n0[7] = f7.w; n0[8] = f8.x; n0[9] = f8.y;
-            n1[0] = f8.z; n1[1] = f8.w; n1[2] = f9.x; n1[3] = f9.y; n1[4] = f9.z;
-            n1[5] = f9.w; n1[6] = f10.x; n1[7] = f10.y; n1[8] = f10.z; n1[9] = f10.w;
+            n0[0] = f6.x; n0[1] = f6.y; n0[2] = f6.z; n0[3] = f6.w;
+            n0[4] = f7.x; n0[5] = f7.y; n0[6] = f7.z; n0[7] = f7.w;
+            n1[0] = f8.x; n1[1] = f8.y; n1[2] = f8.z; n1[3] = f8.w;
+            n1[4] = f9.x; n1[5] = f9.y; n1[6] = f9.z; n1[7] = f9.w;
         }
     }
 }
 
 // Child c of the pair certainly holds no silhouette for x (3D node bound, sil_filter.h;
 // skipping it leaves the reference's answers and the order of its other visits as
-// they are).  Always false in 2D.
-template <int D>
+// they are).  The delta form first; with CONE the cone form where it does not decide
+// (it is never wider, and skips nodes seen head-on with larger normal spreads).
+// Always false in 2D.
+template <int D, bool CONE = true>
 __device__ __forceinline__ bool child_free(const DevScene &s, const PairView<D> &P, int c, const float *x) {
     if (D == 2) return false;
     const float *b = P.nb[D == 3 ? c : 0];
     const float m = sil_node_margin(fmaxf(fmaxf(fabsf(x[0]), fabsf(x[1])), fabsf(x[D - 1])), s.coord_bound);
-    return sil_node_excluded(b[0], b[1], b[2], b[3], b[4], b[5], b[6], b[7], b[8], b[9], x[0], x[1], x[D - 1], m);
+    const float cx = sil_node_centre(P.lo[c][0], P.hi[c][0]), cy = sil_node_centre(P.lo[c][1], P.hi[c][1]),
+                cz = sil_node_centre(P.lo[c][D - 1], P.hi[c][D - 1]);
+    if (sil_node_excluded_delta(cx, cy, cz, b, x[0], x[1], x[D - 1], m)) return true;
+    return CONE && sil_node_excluded_cone(cx, cy, cz, b, x[0], x[1], x[D - 1], m);
 }
 
 // Interior node `ref`: both children against the current r_max, closer pushed last.

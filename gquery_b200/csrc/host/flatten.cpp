@@ -350,13 +350,14 @@ void snch_node_bounds(const BvhTree<D> &t, const SnchTree<D> &s, DeviceImage<D> 
         g.usable = (r.flags & (GQ_ITEM_VALID | GQ_SIL_FILTER)) == GQ_SIL_FILTER;
         return g;
     };
-    auto bound = [&](size_t i, float out[10]) {
+    auto bound = [&](size_t i, float out[kSilNodeBound]) {
         const auto &bx = t.nodes[i].box;
-        const float cx = 0.5f * (bx.lo.v[0] + bx.hi.v[0]), cy = 0.5f * (bx.lo.v[1] + bx.hi.v[1]),
-                    cz = 0.5f * (bx.lo.v[2] + bx.hi.v[2]);
+        const float cx = sil_node_centre(bx.lo.v[0], bx.hi.v[0]), cy = sil_node_centre(bx.lo.v[1], bx.hi.v[1]),
+                    cz = sil_node_centre(bx.lo.v[2], bx.hi.v[2]);
         if (split[i]) {
-            // never skipped (lo = -inf, hi = +inf)
-            const float open[10] = {cx, cy, cz, 0.f, 0.f, 0.f, 1.f, 0.f, -__builtin_inff(), __builtin_inff()};
+            // never skipped (delta = +inf, lo = -inf, hi = +inf)
+            const float open[kSilNodeBound] = {0.f, 0.f, 0.f, __builtin_inff(), 1.f, 0.f, -__builtin_inff(),
+                                               __builtin_inff()};
             std::memcpy(out, open, sizeof open);
         } else {
             sil_node_bound(cx, cy, cz, beg[i], end[i], edge, out);

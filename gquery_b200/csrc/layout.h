@@ -99,9 +99,10 @@ typedef struct {  // 2D, 80 B
     int32_t ref_l, ref_r, pad0, pad1;
 } gq_spair2_t;
 
-// 3D, 176 B: the reference's boxes and cones of both children (96 B), then per child
-// the node bound of sil_filter.h (box centre, axis, cos and sin of the normal cone's
-// half-angle, lo, hi) that proves a child free of silhouettes for a query point.
+// 3D, 160 B (five 32-byte sectors): the reference's boxes and cones of both children
+// (96 B), then per child the node bound of sil_filter.h (axis, delta, cos and sin of the
+// normal cone's half-angle, lo, hi; the centre is the child box's) that proves a child
+// free of silhouettes for a query point.
 typedef struct {
     float l_lox, l_loy, l_loz, l_hix;
     float l_hiy, l_hiz, l_ax, l_ay;
@@ -110,8 +111,11 @@ typedef struct {
     float r_hiz, r_ax, r_ay, r_az;
     float r_half, r_rad;
     int32_t ref_l, ref_r;
-    float l_b[10], r_b[10];
+    float l_b[8], r_b[8];
 } gq_spair3_t;
+#ifdef __cplusplus
+static_assert(sizeof(gq_spair3_t) == 160, "gq_spair3_t is five 32-byte sectors");
+#endif
 
 // Quantised 8-wide node, 3D: 96 B (three 32-byte sectors).
 //   origin.xyz, meta = exp_x | exp_y << 8 | exp_z << 16 | nchild << 24 (exps biased by 127)

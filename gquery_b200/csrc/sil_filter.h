@@ -74,29 +74,34 @@ GQ_HD bool sil_edge_excluded(float ax, float ay, float az, float n0x, float n0y,
 // face normal n with the edge's orientation sign s (both normals of an edge may flip
 // together: the test above is unchanged), and the points q of the edge.  Then
 //   s n . (q - x) = s n . (q - c) + s n . (c - x),
-// where s n . (q - c) lies in [lo, hi] (from the end points and the spans) and the
-// unit vectors s n lie in the cone of half-angle theta around the unit axis A, so that
-// with v = c - x, l = |v| and phi the angle between A and v,
-//   s n . v  in  [l cos(min(phi + theta, pi)), l cos(max(phi - theta, 0))],
-// l cos phi = A . v and l sin phi = |A x v| (no trigonometry, no cancellation near
-// phi = 0).  The host computes lo, hi and theta in double (theta widened by 1e-6 rad,
-// lo and hi rounded outward) and stores (c, A, cos theta, sin theta, lo, hi).  When the
-// interval lies beyond a margin on one side of zero, both dot products of every edge
-// have the sign of that side and none is a silhouette for x, so the traversal may skip
-// the child: the reference's visit order of the other nodes and its answers stay as
-// they are.  With the orientation signs of a consistently wound mesh the axis gathers
-// outward normals only, so theta measures how much the surface bends inside the node
-// rather than the pi of a cone that holds both orientations; a node seen head-on is
-// skipped for any theta below about 90 degrees.
+// where s n . (q - c) lies in [lo, hi] (from the end points and the spans).  With
+// v = c - x and l = |v|, the second term is bounded two ways from the spread of the
+// unit vectors s n around the unit axis A:
+//   delta form: s n . v in [A . v - delta l, A . v + delta l], delta = max |s n - A|;
+//   cone form:  s n . v in [l cos(min(phi + theta, pi)), l cos(max(phi - theta, 0))],
+//               theta the largest angle between s n and A, phi that between A and v,
+//               from l cos phi = A . v and l sin phi = |A x v| (no trigonometry and no
+//               cancellation near phi = 0).
+// The cone form is never wider (l (cos(phi - theta) - cos phi) <= 2 sin(theta / 2) l =
+// delta l) and skips a node seen head-on for spreads up to about 90 degrees where the
+// delta form stops near 60; the delta form is about half the arithmetic.  The host
+// computes lo, hi, delta and theta in double (delta rounded up, theta widened by
+// 1e-6 rad, lo and hi rounded outward) and stores (A, delta, cos theta, sin theta, lo,
+// hi).  When the interval lies beyond a margin on one side of zero, both dot products
+// of every edge have the sign of that side and none is a silhouette for x, so the
+// traversal may skip the child: the reference's visit order of the other nodes and its
+// answers stay as they are.  With the orientation signs of a consistently wound mesh
+// the axis gathers outward normals only, so the spread measures how much the surface
+// bends inside the node rather than the pi of a cone that holds both orientations.
 //
 // Margin.  Besides the reference's rounding of each dot product (at most
-// 1.75 eps (6 M + 4 X), see above), the FP32 evaluation of A . v, |A x v|, l, the two
-// products with cos theta and sin theta, the sums, the rounding of the stored cosine
-// and sine and of A and n to unit length move the interval by at most about
-// eps (40 M + 30 X); the margin 2e-5 (2 M + X) is eight times the total.  Nodes whose
-// subtree holds a boundary edge or an edge without GQ_SIL_FILTER get lo = -inf,
-// hi = +inf (never skipped); nodes without silhouettes get lo = hi = +inf (always
-// skipped).
+// 1.75 eps (6 M + 4 X), see above), the FP32 evaluation of either form (c from the box,
+// c - x, the dot and cross products, l, the products with delta or with the stored
+// cosine and sine, the sums), and the rounding of A and n to unit length move the
+// interval by at most about eps (40 M + 30 X); the margin 2e-5 (2 M + X) is eight times
+// the total.  Nodes whose subtree holds a boundary edge or an edge without
+// GQ_SIL_FILTER get lo = -inf, hi = +inf (never skipped); nodes without silhouettes get
+// lo = hi = +inf (always skipped).
 
 // Geometry of one 3D silhouette edge for the node bound: end points, stored face
 // normals, orientation sign and whether the pre-test may be used on it.
@@ -106,7 +111,14 @@ struct SilEdgeGeom {
     bool usable;
 };
 
+// Stored bound of a node: b[0..2] = A, b[3] = delta, b[4] = cos theta, b[5] = sin theta,
+// b[6] = lo, b[7] = hi.
+constexpr int kSilNodeBound = 8;
+
 GQ_HD float sil_node_margin(float x_inf, float coord_bound) { return 2.f * sil_margin(x_inf, coord_bound); }
+
+// The node's centre as the bound was computed with it: the middle of its box.
+GQ_HD float sil_node_centre(float lo, float hi) { return 0.5f * (lo + hi); }
 
 // cos and sin of the cone half-angle theta + 1e-6 (at most pi) from cmin = cos theta.
 GQ_HD void sil_cone_of(double cmin, float &ct, float &st) {
@@ -122,34 +134,41 @@ GQ_HD void sil_cone_of(double cmin, float &ct, float &st) {
     st = (float)s2;
 }
 
-// True when the node with bound (c, A, cos theta, sin theta, lo, hi) holds no
-// silhouette for x.
-GQ_HD bool sil_node_excluded(float cx, float cy, float cz, float ax, float ay, float az, float ct, float st,
-                             float lo, float hi, float xx, float xy, float xz, float margin) {
+// Delta form: true when the node (centre c, bound b) certainly holds no silhouette for x.
+GQ_HD bool sil_node_excluded_delta(float cx, float cy, float cz, const float *b, float xx, float xy, float xz,
+                                   float margin) {
     const float vx = cx - xx, vy = cy - xy, vz = cz - xz;
+    const float g = gq_dot3(b[0], b[1], b[2], vx, vy, vz);
+    const float dl = b[3] * gq_norm3(vx, vy, vz);
+    return (g + b[6] - dl > margin) | (g + b[7] + dl < -margin);
+}
+
+// Cone form of the same test.
+GQ_HD bool sil_node_excluded_cone(float cx, float cy, float cz, const float *b, float xx, float xy, float xz,
+                                  float margin) {
+    const float vx = cx - xx, vy = cy - xy, vz = cz - xz;
+    const float ax = b[0], ay = b[1], az = b[2], ct = b[4], st = b[5];
     const float g = gq_dot3(ax, ay, az, vx, vy, vz);  // l cos phi
     const float wx = gq_fma(ay, vz, -(az * vy)), wy = gq_fma(az, vx, -(ax * vz)), wz = gq_fma(ax, vy, -(ay * vx));
     const float h = gq_norm3(wx, wy, wz);  // l sin phi
     const float l = gq_norm3(vx, vy, vz);
-    const float up = g >= l * ct ? l : gq_fma(g, ct, h * st);       // phi <= theta: v inside the cone
+    const float up = g >= l * ct ? l : gq_fma(g, ct, h * st);         // phi <= theta: v inside the cone
     const float dn = g <= -(l * ct) ? -l : gq_fma(g, ct, -(h * st));  // phi >= pi - theta
-    return (dn + lo > margin) | (up + hi < -margin);
+    return (dn + b[6] > margin) | (up + b[7] < -margin);
 }
 
 #if !defined(__CUDA_ARCH__)
-// Node bound over the edges begin..end-1 (edge(j) returns their SilEdgeGeom), for a
-// node whose box centre is c: out = c[3], axis[3], cos theta, sin theta, lo, hi.
+// Node bound over the edges begin..end-1 (edge(j) returns their SilEdgeGeom) for a node
+// whose box centre is c: out[kSilNodeBound] as above.
 template <class EdgeAt>
 inline void sil_node_bound(float cx, float cy, float cz, long long begin, long long end, EdgeAt edge,
-                           float out[10]) {
-    out[0] = cx;
-    out[1] = cy;
-    out[2] = cz;
-    out[3] = out[4] = out[5] = 0.f;
-    out[6] = 1.f;
-    out[7] = 0.f;
+                           float out[kSilNodeBound]) {
+    out[0] = out[1] = out[2] = 0.f;
+    out[3] = 0.f;
+    out[4] = 1.f;
+    out[5] = 0.f;
     if (begin >= end) {  // no silhouettes: always skipped
-        out[8] = out[9] = __builtin_inff();
+        out[6] = out[7] = __builtin_inff();
         return;
     }
     double m[3] = {0.0, 0.0, 0.0};
@@ -161,39 +180,45 @@ inline void sil_node_bound(float cx, float cy, float cz, long long begin, long l
     }
     const double ml = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
     if (!ok || !(ml > 1e-30)) {  // never skipped
-        out[8] = -__builtin_inff();
-        out[9] = __builtin_inff();
+        out[3] = __builtin_inff();
+        out[6] = -__builtin_inff();
+        out[7] = __builtin_inff();
         return;
     }
     float A[3];
-    for (int k = 0; k < 3; ++k) A[k] = out[3 + k] = (float)(m[k] / ml);
+    for (int k = 0; k < 3; ++k) A[k] = out[k] = (float)(m[k] / ml);
     const double al = sqrt((double)A[0] * A[0] + (double)A[1] * A[1] + (double)A[2] * A[2]);
     const double c[3] = {cx, cy, cz};
-    double cmin = 1.0, lo = __builtin_inf(), hi = -__builtin_inf();
+    double dmax = 0.0, cmin = 1.0, lo = __builtin_inf(), hi = -__builtin_inf();
     for (long long j = begin; j < end; ++j) {
         const SilEdgeGeom e = edge(j);
         for (int f = 0; f < 2; ++f) {
             const float *n = f ? e.n1 : e.n0;
-            double cs = 0.0, nl = 0.0, ac = 0.0, sp = 0.0;
+            double d2 = 0.0, cs = 0.0, nl = 0.0, ac = 0.0, sp = 0.0;
             for (int k = 0; k < 3; ++k) {
                 const double sn = (double)e.orient * (double)n[k];
+                d2 += (sn - A[k]) * (sn - A[k]);
                 cs += sn * A[k];
                 nl += sn * sn;
                 ac += sn * ((double)e.a[k] - c[k]);
                 sp += sn * ((double)e.b[k] - (double)e.a[k]);
             }
+            dmax = fmax(dmax, sqrt(d2));
             cmin = fmin(cmin, cs / (sqrt(nl) * al));  // the angle between the directions
             lo = fmin(lo, ac + fmin(0.0, sp));
             hi = fmax(hi, ac + fmax(0.0, sp));
         }
     }
-    sil_cone_of(cmin, out[6], out[7]);
+    float fd = (float)(dmax * (1.0 + 1e-12));
+    if ((double)fd < dmax) fd = nextafterf(fd, __builtin_inff());
+    out[3] = fd;
+    sil_cone_of(cmin, out[4], out[5]);
     // outward to FP32, with room for the double rounding above
     const double pad = 1e-12 * (fabs(lo) + fabs(hi) + 1.0);
     float fl = (float)(lo - pad), fh = (float)(hi + pad);
     if ((double)fl > lo - pad) fl = nextafterf(fl, -__builtin_inff());
     if ((double)fh < hi + pad) fh = nextafterf(fh, __builtin_inff());
-    out[8] = fl;
-    out[9] = fh;
+    out[6] = fl;
+    out[7] = fh;
 }
 #endif

@@ -100,8 +100,8 @@ void print(const char *name, const Count &k, bool last) {
 
 
 // Node bound: a patch of a height field z = h(x, y) (smooth waves plus noise of a
-// chosen amplitude) or a spherical cap (normals spread up to `cap` radians from its
-// axis), triangulated consistently; every interior edge is a silhouette
+// chosen amplitude, or steep waves whose slopes reach `steep` radians), or a spherical
+// cap (normals spread up to `cap` radians from its axis), triangulated consistently; every interior edge is a silhouette
 // record whose end points are stored in winding order (orientation +1) or swapped
 // (both stored normals point the other way, orientation -1), as the reference's
 // records come.  The patch is placed with a random rotation, scale and offset.
@@ -110,6 +110,7 @@ struct Patch {
     float c[3];
     float bound;  // largest |coordinate|
     V sphere;     // centre of the cap's sphere (cap patches)
+    V axis;       // the patch's unit z axis
 };
 
 V rot(V v, const float R[9]) {
@@ -117,7 +118,7 @@ V rot(V v, const float R[9]) {
             R[6] * v.x + R[7] * v.y + R[8] * v.z};
 }
 
-Patch make_patch(Rng &r, int g, float rough, float cap = 0.f) {
+Patch make_patch(Rng &r, int g, float rough, float cap = 0.f, float steep = 0.f) {
     // random rotation from a random unit quaternion
     float q0 = r.uni(-1, 1), q1 = r.uni(-1, 1), q2 = r.uni(-1, 1), q3 = r.uni(-1, 1);
     const float qn = std::sqrt(q0 * q0 + q1 * q1 + q2 * q2 + q3 * q3);
@@ -136,6 +137,9 @@ Patch make_patch(Rng &r, int g, float rough, float cap = 0.f) {
             V q;
             if (cap > 0.f) {
                 q = unit(V{2.f * (u - 0.5f) * tc, 2.f * (v - 0.5f) * tc, 1.f});
+            } else if (steep > 0.f) {  // slope up to tan(steep) along u
+                const float w = 2.f * (float)g;
+                q = V{u - 0.5f, v - 0.5f, std::tan(steep) / w * std::sin(w * u + 1.3f)};
             } else {
                 const float z = amp * std::sin(w1 * u + 1.3f) * std::cos(w2 * v) + rough * r.uni(-1.f, 1.f) / g;
                 q = V{u - 0.5f, v - 0.5f, z};
@@ -145,6 +149,7 @@ Patch make_patch(Rng &r, int g, float rough, float cap = 0.f) {
     auto at = [&](int i, int j) { return p[(size_t)i * (g + 1) + j]; };
     Patch P;
     P.sphere = off;
+    P.axis = rot(V{0.f, 0.f, 1.f}, R);
     // triangles (i,j),(i+1,j),(i+1,j+1) and (i,j),(i+1,j+1),(i,j+1); interior diagonal and
     // grid edges with their two faces in winding order: edge a->b of face (a, b, c), the
     // other face (b, a, d)
@@ -179,17 +184,17 @@ Patch make_patch(Rng &r, int g, float rough, float cap = 0.f) {
         }
         P.bound = std::fmax(P.bound, amax(v));
     }
-    for (int k = 0; k < 3; ++k) P.c[k] = 0.5f * (lo[k] + hi[k]);
+    for (int k = 0; k < 3; ++k) P.c[k] = sil_node_centre(lo[k], hi[k]);
     return P;
 }
 
 struct NodeCount {
-    long long cases = 0, excluded = 0, unsound = 0;
+    long long cases = 0, excluded = 0, unsound = 0, delta = 0, cone = 0;  // excluded by either / each form
 };
 
-void check_node(Rng &r, int g, float rough, NodeCount &k, float cap = 0.f) {
-    Patch P = make_patch(r, g, rough, cap);
-    float b[10];
+void check_node(Rng &r, int g, float rough, NodeCount &k, float cap = 0.f, float steep = 0.f) {
+    Patch P = make_patch(r, g, rough, cap, steep);
+    float b[kSilNodeBound];
     sil_node_bound(P.c[0], P.c[1], P.c[2], 0, (long long)P.edges.size(),
                    [&](long long j) { return P.edges[(size_t)j]; }, b);
     const float s = std::fmax(P.bound, 1e-6f);
@@ -197,8 +202,10 @@ void check_node(Rng &r, int g, float rough, NodeCount &k, float cap = 0.f) {
         // queries: near the patch (within 1e-6 .. 2 of its size), and far
         V x;
         const V c{P.c[0], P.c[1], P.c[2]};
-        const int kind = (int)(r.next() % (cap > 0.f ? 4 : 3));
-        if (kind == 3) {  // near the centre of the cap's sphere
+        const int kind = (int)(r.next() % (cap > 0.f || steep > 0.f ? 4 : 3));
+        if (kind == 3 && steep > 0.f) {  // head-on, far along the patch's axis (either side)
+            x = add(add(c, mul(P.axis, r.sgn() * r.logu(3.f, 100.f) * s)), mul(rand_in(r, 1.f), 0.05f * s));
+        } else if (kind == 3) {  // near the centre of the cap's sphere
             x = add(P.sphere, mul(unit(rand_in(r, 1.f)), r.logu(1e-4f, 0.3f) * s));
         } else if (kind == 0) {
             const SilEdgeGeom &e = P.edges[r.next() % P.edges.size()];
@@ -209,9 +216,12 @@ void check_node(Rng &r, int g, float rough, NodeCount &k, float cap = 0.f) {
             x = add(c, mul(unit(rand_in(r, 1.f)), r.logu(2.f, 1e3f) * s));
         }
         const float m = g_margin_scale * sil_node_margin(amax(x), P.bound);
-        const bool ex = sil_node_excluded(b[0], b[1], b[2], b[3], b[4], b[5], b[6], b[7], b[8], b[9], x.x, x.y, x.z, m);
+        const bool ed = sil_node_excluded_delta(P.c[0], P.c[1], P.c[2], b, x.x, x.y, x.z, m);
+        const bool ec = sil_node_excluded_cone(P.c[0], P.c[1], P.c[2], b, x.x, x.y, x.z, m);
         ++k.cases;
-        if (!ex) continue;
+        k.delta += ed;
+        k.cone += ec;
+        if (!(ed || ec)) continue;
         ++k.excluded;
         for (const SilEdgeGeom &e : P.edges)
             if (reference_silhouette(V{e.a[0], e.a[1], e.a[2]}, V{e.b[0], e.b[1], e.b[2]},
@@ -224,8 +234,8 @@ void check_node(Rng &r, int g, float rough, NodeCount &k, float cap = 0.f) {
 
 void print_node(const char *name, const NodeCount &k, bool last) {
     std::printf("\"%s\": {\"cases\": %lld, \"usable\": %lld, \"excluded\": %lld, \"silhouettes\": 0, "
-                "\"unsound\": %lld}%s",
-                name, k.cases, k.cases, k.excluded, k.unsound, last ? "" : ", ");
+                "\"unsound\": %lld, \"delta\": %lld, \"cone\": %lld}%s",
+                name, k.cases, k.cases, k.excluded, k.unsound, k.delta, k.cone, last ? "" : ", ");
 }
 
 }  // namespace
@@ -286,12 +296,13 @@ int main(int argc, char **argv) {
             check(a, b, c, d, x, bound_of(a, b, c, d), on_edge);
         }
     }
-    NodeCount smooth, rough, flat, capn;
+    NodeCount smooth, rough, flat, capn, steepn;
     for (long long i = 0; i < n / 200; ++i) {
         check_node(r, 2 + (int)(r.next() % 7), 0.f, smooth);
         check_node(r, 2 + (int)(r.next() % 7), r.logu(1e-3f, 2.f), rough);
         check_node(r, 2 + (int)(r.next() % 7), 1e-6f, flat);
         check_node(r, 2 + (int)(r.next() % 7), 0.f, capn, r.uni(0.35f, 1.48f));  // 20 .. 85 degrees
+        check_node(r, 3 + (int)(r.next() % 6), 0.f, steepn, 0.f, r.uni(1.05f, 1.48f));  // 60 .. 85 degrees
     }
     std::printf("{");
     print("generic", generic, false);
@@ -304,10 +315,11 @@ int main(int argc, char **argv) {
     print_node("node_smooth", smooth, false);
     print_node("node_rough", rough, false);
     print_node("node_flat", flat, false);
-    print_node("node_cap", capn, true);
+    print_node("node_cap", capn, false);
+    print_node("node_steep", steepn, true);
     std::printf("}\n");
     const long long bad = generic.unsound + coplanar.unsound + near_plane.unsound + sliver.unsound +
                           zero_len.unsound + far.unsound + on_edge.unsound + smooth.unsound + rough.unsound +
-                          flat.unsound + capn.unsound;
+                          flat.unsound + capn.unsound + steepn.unsound;
     return bad ? 1 : 0;
 }

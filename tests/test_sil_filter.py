@@ -1,9 +1,9 @@
 """The silhouette-edge pre-test never excludes an edge the reference's test calls a
 silhouette (random, nearly coplanar, sliver, zero-length, far and on-edge cases), and
 without its margin it would: the cases reach the rounding boundary the margin covers.
-The node bound never excludes a patch of edges (smooth, rough or flat height fields and
-spherical caps, whose records come in either orientation) that holds a silhouette for
-the query."""
+The node bound never excludes a patch of edges (smooth, rough, flat or steep height
+fields and spherical caps, whose records come in either orientation) that holds a
+silhouette for the query."""
 import json
 import shutil
 import subprocess
@@ -40,9 +40,14 @@ def test_pre_test_is_sound(checker):
     # the node bound skips patches, and with mixed record orientations too
     for k in ("node_smooth", "node_rough", "node_flat"):
         assert res[k]["excluded"] > 0.2 * res[k]["cases"], (k, res[k])
-    # caps seen from near their sphere's centre: the normal-cone form skips them for
-    # spreads up to 85 degrees (a bound by |s n - A| alone stops near 60)
-    assert res["node_cap"]["excluded"] > 0.3 * res["node_cap"]["cases"], res["node_cap"]
+    # the cone form is never wider than the delta form (rounding aside) ...
+    for k in ("node_smooth", "node_rough", "node_flat", "node_cap", "node_steep"):
+        assert res[k]["cone"] >= 0.999 * res[k]["delta"], (k, res[k])
+    assert res["node_cap"]["cone"] > 0.3 * res["node_cap"]["cases"], res["node_cap"]
+    # ... and skips patches whose normals spread 60 to 85 degrees when they are seen
+    # head-on, where the delta form stops near 60
+    w = res["node_steep"]
+    assert w["cone"] > w["delta"] + 0.02 * w["cases"], w
 
 
 def test_margin_is_needed(checker):
