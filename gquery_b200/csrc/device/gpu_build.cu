@@ -351,8 +351,60 @@ __global__ void k_snch_pairs(int64_t n, const int2 *child, const int2 *range, co
     const double ml = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
     const bool open = bad || !(ml > 1e-30);
     float A[3] = {0.f, 0.f, 0.f};
-    if (!open)
-        for (int k = 0; k < 3; ++k) A[k] = (float)(m[k] / ml);
+    if (!open) {
+        // axis: the mean direction, then steps toward the farthest normal (as the host's
+        // sil_node_bound, in FP32 here: the axis only has to be good, the spread around it
+        // is measured in double below); the axis with the smallest spread wins
+        float ax[3] = {(float)(m[0] / ml), (float)(m[1] / ml), (float)(m[2] / ml)};
+        double best[3] = {m[0] / ml, m[1] / ml, m[2] / ml};
+        float best_c = -2.f;
+        const int steps = b1 - b0 <= kSilAxisMaxRecords ? kSilAxisSteps : 0;
+        for (int it = 0; it <= steps; ++it) {
+            float cmin_it = 2.f, far[3] = {0.f, 0.f, 0.f};
+            for (int64_t j = b0 + lane; j < b1; j += 32) {
+                const gq_sile_t &r = sils[j];
+                const float o = rec_orient[j];
+                for (int f = 0; f < 2; ++f) {
+                    const float sn[3] = {o * (f ? r.n1x : r.n0x), o * (f ? r.n1y : r.n0y), o * (f ? r.n1z : r.n0z)};
+                    const float cs = sn[0] * ax[0] + sn[1] * ax[1] + sn[2] * ax[2];  // stored normals are unit
+                    if (cs < cmin_it) {
+                        cmin_it = cs;
+                        for (int k = 0; k < 3; ++k) far[k] = sn[k];
+                    }
+                }
+            }
+            // the warp's farthest normal (lowest lane on a tie), the same on every lane
+            int who = lane;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const float oc = __shfl_xor_sync(0xffffffffu, cmin_it, o);
+                const int ow = __shfl_xor_sync(0xffffffffu, who, o);
+                const float of0 = __shfl_xor_sync(0xffffffffu, far[0], o), of1 = __shfl_xor_sync(0xffffffffu, far[1], o),
+                            of2 = __shfl_xor_sync(0xffffffffu, far[2], o);
+                if (oc < cmin_it || (oc == cmin_it && ow < who)) {
+                    cmin_it = oc;
+                    who = ow;
+                    far[0] = of0;
+                    far[1] = of1;
+                    far[2] = of2;
+                }
+            }
+            if (cmin_it > best_c) {
+                best_c = cmin_it;
+                for (int k = 0; k < 3; ++k) best[k] = ax[k];
+            }
+            const float w = 1.f / (float)(it + 2);
+            float nx[3], nn = 0.f;
+            for (int k = 0; k < 3; ++k) {
+                nx[k] = ax[k] + w * (far[k] - ax[k]);
+                nn += nx[k] * nx[k];
+            }
+            nn = sqrtf(nn);
+            if (!(nn > 1e-6f)) break;
+            for (int k = 0; k < 3; ++k) ax[k] = nx[k] / nn;
+        }
+        for (int k = 0; k < 3; ++k) A[k] = (float)best[k];
+    }
     // pass 2: spread of the oriented normals around A, plane offsets, cone, radius
     double dmax = 0.0, mlo = __builtin_inf(), mhi = -__builtin_inf(), cmin = 1.0, cnode = 1.0, rmax = 0.0;
     const double al = sqrt((double)A[0] * A[0] + (double)A[1] * A[1] + (double)A[2] * A[2]);

@@ -111,6 +111,12 @@ struct SilEdgeGeom {
     bool usable;
 };
 
+// Steps of the search for a narrow cone axis, and the largest node (in silhouette
+// records) it runs on: above that the normals of a closed surface spread about pi
+// around any axis.
+constexpr int kSilAxisSteps = 8;
+constexpr long long kSilAxisMaxRecords = 8192;
+
 // Stored bound of a node: b[0..2] = A, b[3] = delta, b[4] = cos theta, b[5] = sin theta,
 // b[6] = lo, b[7] = hi.
 constexpr int kSilNodeBound = 8;
@@ -185,8 +191,41 @@ inline void sil_node_bound(float cx, float cy, float cz, long long begin, long l
         out[7] = __builtin_inff();
         return;
     }
+    // axis: the mean direction, then steps toward the farthest normal (Badoiu-Clarkson
+    // iterations for the smallest enclosing cone); the axis with the smallest spread wins
+    double ax[3] = {m[0] / ml, m[1] / ml, m[2] / ml}, best[3] = {ax[0], ax[1], ax[2]}, best_c = -2.0;
+    const int steps = end - begin <= kSilAxisMaxRecords ? kSilAxisSteps : 0;
+    for (int it = 0; it <= steps; ++it) {
+        double cmin_it = 2.0, far[3] = {0.0, 0.0, 0.0};
+        for (long long j = begin; j < end; ++j) {
+            const SilEdgeGeom e = edge(j);
+            for (int f = 0; f < 2; ++f) {
+                const float *n = f ? e.n1 : e.n0;
+                const double sn[3] = {(double)e.orient * n[0], (double)e.orient * n[1], (double)e.orient * n[2]};
+                const double nl = sqrt(sn[0] * sn[0] + sn[1] * sn[1] + sn[2] * sn[2]);
+                const double cs = (sn[0] * ax[0] + sn[1] * ax[1] + sn[2] * ax[2]) / nl;
+                if (cs < cmin_it) {
+                    cmin_it = cs;
+                    for (int k = 0; k < 3; ++k) far[k] = sn[k] / nl;
+                }
+            }
+        }
+        if (cmin_it > best_c) {
+            best_c = cmin_it;
+            for (int k = 0; k < 3; ++k) best[k] = ax[k];
+        }
+        const double w = 1.0 / (it + 2);
+        double nx[3], nn = 0.0;
+        for (int k = 0; k < 3; ++k) {
+            nx[k] = ax[k] + w * (far[k] - ax[k]);
+            nn += nx[k] * nx[k];
+        }
+        nn = sqrt(nn);
+        if (!(nn > 1e-12)) break;
+        for (int k = 0; k < 3; ++k) ax[k] = nx[k] / nn;
+    }
     float A[3];
-    for (int k = 0; k < 3; ++k) A[k] = out[k] = (float)(m[k] / ml);
+    for (int k = 0; k < 3; ++k) A[k] = out[k] = (float)best[k];
     const double al = sqrt((double)A[0] * A[0] + (double)A[1] * A[1] + (double)A[2] * A[2]);
     const double c[3] = {cx, cy, cz};
     double dmax = 0.0, cmin = 1.0, lo = __builtin_inf(), hi = -__builtin_inf();
