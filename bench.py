@@ -444,7 +444,7 @@ def section_c4(args, dev):
                    "per-request server is run at the same arrival rate"}
     sat_rate = None
     for mode in ("batched", "per_request"):
-        srv = Server(scenes, budget_bytes=120 << 30, step_queries=1 << 18, max_inflight=2,
+        srv = Server(scenes, budget_bytes=120 << 30, step_queries=1 << 18, max_inflight=3,
                      per_request=(mode == "per_request"))
         srv.run_trace(reqs[:40], np.zeros(40))  # warm-up
         res = srv.run_trace(reqs, np.zeros(len(reqs)))

@@ -558,8 +558,8 @@ gq_status gq_server_create(gq_scene *const *scenes, int32_t n_scenes, const gq_s
     if (!s) return fail(GQ_ERR_NOMEM, "host allocation");
     s->flags = o.flags;
     s->step_queries = o.step_queries > 0 ? o.step_queries : (1 << 19);
-    const int inflight = o.max_inflight > 0 ? o.max_inflight : 2;
-    s->sil_share = o.sil_share > 0.f ? o.sil_share : 2.4f;  // above 1: the slots may oversubscribe
+    const int inflight = o.max_inflight > 0 ? o.max_inflight : 3;
+    s->sil_share = o.sil_share > 0.f ? o.sil_share : 1.5f;  // above 1: the slots may oversubscribe
     std::vector<gqd::DevScene> views((size_t)n_scenes);
     for (int32_t i = 0; i < n_scenes; ++i) {
         gq_scene *sc = scenes[i];

@@ -109,9 +109,9 @@ class Server:
     latency of far-reaching ones)."""
 
     def __init__(self, scenes: Sequence[Scene], *, budget_bytes: int = 0, ring_queries=(1 << 22,) * 3,
-                 step_queries: int = 1 << 19, max_inflight: int = 2, per_request: bool = False,
+                 step_queries: int = 1 << 19, max_inflight: int = 3, per_request: bool = False,
                  cp_variant: str = "split", ray_variant: str = "wide8", sil_variant: str = "warp",
-                 sil_share: float = 2.4, sil_slots: int = 3, sil_step_queries: int = 1 << 15):
+                 sil_share: float = 1.5, sil_slots: int = 3, sil_step_queries: int = 1 << 15):
         self.scenes = list(scenes)
         self.dim = self.scenes[0].dim
         flags = (L.SERVER_PER_REQUEST if per_request else 0) | \

@@ -319,9 +319,9 @@ typedef struct {
     int64_t budget_bytes;     /* device bytes the request rings may hold (0: no limit) */
     int64_t ring_queries[3];  /* ring capacity in queries per kind (0: 1<<22) */
     int64_t step_queries;     /* most queries of one kind in one step, and the largest request (0: 1<<19) */
-    int32_t max_inflight;     /* step slots for closest-point and ray steps (0: 2) */
+    int32_t max_inflight;     /* step slots for closest-point and ray steps (0: 3) */
     int32_t flags;            /* GQ_BATCH_*_EXACT | GQ_SERVER_PER_REQUEST */
-    float sil_share;          /* share of the GPU's resident blocks all silhouette steps together may hold (0: 2.4;
+    float sil_share;          /* share of the GPU's resident blocks all silhouette steps together may hold (0: 1.5;
                                  above 1 they may oversubscribe it, each slot capped at 1) */
     int32_t sil_slots;        /* silhouette step slots (0: 3) */
     int64_t sil_step_queries; /* most silhouette queries in one step, unless one request is larger (0: 1<<15) */
