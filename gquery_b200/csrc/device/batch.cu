@@ -137,14 +137,41 @@ __device__ __forceinline__ void refill(int64_t n, unsigned long long *counter, i
     }
 }
 
-// Phase 3, sil_mode 2: one silhouette query per warp (sil_warp.cuh), the warp's stack in
-// dynamic shared memory; counter[2] counts the claims.
+// One silhouette query (sorted position t) on one warp (sil_warp.cuh), the warp's stack
+// at wst.
+template <int D>
+__device__ __forceinline__ void sil_warp_query(const DevScene *scenes, int n_scenes, const BatchKind &sil,
+                                               const gq_sil_out &sil_out, int32_t *err, int64_t t, int2 *wst) {
+    const unsigned lane = threadIdx.x & 31u;
+    const int64_t qi = (int64_t)__ldg(sil.perm + t);
+    const int sid = __ldg(sil.scene + qi);
+    if (sid == GQ_BATCH_SKIP) return;
+    float x[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) x[k] = qget(sil.a, qi, k);
+    const bool known = (unsigned)sid < (unsigned)n_scenes;
+    if (!known || !scenes[sid].spairs) {
+        if (lane == 0) {
+            atomicOr(err, known ? GQ_BATCH_ERR_NO_SNCH : GQ_BATCH_ERR_SCENE);
+            put_sil<D>(sil_out, sil.n, qi, false, x, 0.f, 0);
+        }
+        return;
+    }
+    snch::Lane<D> L;
+    wsil::closest_silhouette<D>(scenes[sid], x, sil.r_max ? sil.r_max[qi] : kInf, L, wst);
+    if (lane == 0) {
+        if (L.ovf && scenes[sid].err) atomicOr(scenes[sid].err, GQ_DEVERR_STACK);
+        put_sil<D>(sil_out, sil.n, qi, L.found && !L.ovf, L.bp, L.bd, L.bid);
+    }
+}
+
+// Phase 3, sil_mode 2: one silhouette query per warp, persistent warps claiming the
+// next one (counter[2]); the warp's stack in dynamic shared memory.
 template <int D>
 __device__ __forceinline__ void sil_warp_phase(const DevScene *scenes, int n_scenes, const BatchKind &sil,
                                                const gq_sil_out &sil_out, unsigned long long *counter,
                                                int32_t *err) {
     const unsigned lane = threadIdx.x & 31u;
-    // one query per warp; this warp's stack in dynamic shared memory
     extern __shared__ int2 wstk[];
     int2 *wst = wstk + (threadIdx.x >> 5) * wsil::kWarpStack;
     for (;;) {
@@ -152,26 +179,7 @@ __device__ __forceinline__ void sil_warp_phase(const DevScene *scenes, int n_sce
         if (lane == 0) t = atomicAdd(&counter[2], 1ull);
         t = __shfl_sync(0xffffffffu, t, 0);
         if (t >= (unsigned long long)sil.n) break;
-        const int64_t qi = (int64_t)__ldg(sil.perm + (int64_t)t);
-        const int sid = __ldg(sil.scene + qi);
-        if (sid == GQ_BATCH_SKIP) continue;
-        float x[D];
-#pragma unroll
-        for (int k = 0; k < D; ++k) x[k] = qget(sil.a, qi, k);
-        const bool known = (unsigned)sid < (unsigned)n_scenes;
-        if (!known || !scenes[sid].spairs) {
-            if (lane == 0) {
-                atomicOr(err, known ? GQ_BATCH_ERR_NO_SNCH : GQ_BATCH_ERR_SCENE);
-                put_sil<D>(sil_out, sil.n, qi, false, x, 0.f, 0);
-            }
-            continue;
-        }
-        snch::Lane<D> L;
-        wsil::closest_silhouette<D>(scenes[sid], x, sil.r_max ? sil.r_max[qi] : kInf, L, wst);
-        if (lane == 0) {
-            if (L.ovf && scenes[sid].err) atomicOr(scenes[sid].err, GQ_DEVERR_STACK);
-            put_sil<D>(sil_out, sil.n, qi, L.found && !L.ovf, L.bp, L.bd, L.bid);
-        }
+        sil_warp_query<D>(scenes, n_scenes, sil, sil_out, err, (int64_t)t, wst);
     }
 }
 
@@ -500,13 +508,18 @@ __global__ void __launch_bounds__(kBlock) k_sil_heavy(const DevScene *scenes, Ba
     }
 }
 
-// A step with silhouettes only, one query per warp (the server's silhouette slots): the
-// phase alone, so that its register count, not k_batch's, sets the residency.
+// A step with silhouettes only (the server's silhouette slots): one block of one warp
+// per query, which answers it and exits.  Blocks end all the time, so the block
+// scheduler places the pending blocks of higher-priority streams (the server's closest
+// points and rays) first and fills the rest of the GPU with silhouettes: no share of the
+// GPU has to be set aside, and a large step uses all of it when nothing else waits.  One
+// warp per block, so a heavy query holds no idle warps; 32 blocks of 64 registers a
+// thread fill the register file as the persistent form does.
 template <int D>
-__global__ void __launch_bounds__(kBlock, 8) k_batch_silw(const DevScene *scenes, int n_scenes, BatchKind sil,
-                                                          gq_sil_out sil_out, unsigned long long *counter,
-                                                          int32_t *err) {
-    sil_warp_phase<D>(scenes, n_scenes, sil, sil_out, counter, err);
+__global__ void __launch_bounds__(32, 32) k_batch_silw(const DevScene *scenes, int n_scenes, BatchKind sil,
+                                                       gq_sil_out sil_out, int32_t *err) {
+    __shared__ int2 wst[wsil::kWarpStack];
+    sil_warp_query<D>(scenes, n_scenes, sil, sil_out, err, (int64_t)blockIdx.x, wst);
 }
 
 template <int D, bool RAYW>
@@ -516,20 +529,9 @@ cudaError_t launch_batch(const DevScene *scenes_dev, int n_scenes, BatchKind kin
                          cudaStream_t st) {
     // the one-query-per-warp silhouette phase keeps its stacks in dynamic shared memory
     const size_t smem = (sil_mode == 2 && kinds[2].n > 0) ? (size_t)(kBlock / 32) * wsil::kWarpStack * sizeof(int2) : 0;
-    if (smem && kinds[0].n <= 0 && kinds[1].n <= 0) {  // silhouettes only: the phase's own kernel
-        static int wbps = 0, w_sm = 0;
-        if (!wbps) {
-            int dev = 0, b = 0;
-            cudaGetDevice(&dev);
-            cudaDeviceGetAttribute(&w_sm, cudaDevAttrMultiProcessorCount, dev);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_silw<D>, kBlock, smem);
-            wbps = b < 1 ? 1 : b;
-        }
-        int64_t want = std::min<int64_t>((int64_t)wbps * w_sm, (kinds[2].n * 32 + kBlock - 1) / kBlock);
-        if (grid_share > 0.f && grid_share < 1.f)
-            want = std::min<int64_t>(want, std::max<int64_t>(1, (int64_t)(grid_share * (float)(wbps * w_sm))));
-        k_batch_silw<D><<<dim3((unsigned)want), kBlock, smem, st>>>(scenes_dev, n_scenes, kinds[2], sil_out, counter,
-                                                                    err);
+    if (smem && kinds[0].n <= 0 && kinds[1].n <= 0) {  // silhouettes only: one block per query
+        if (kinds[2].n > 0x7fffffff) return cudaErrorInvalidValue;
+        k_batch_silw<D><<<dim3((unsigned)kinds[2].n), 32, 0, st>>>(scenes_dev, n_scenes, kinds[2], sil_out, err);
         return cudaGetLastError();
     }
     const int mi = smem ? 1 : 0;

@@ -99,9 +99,12 @@ class Server:
     budget_bytes: device bytes the request rings may hold (the admission budget);
     ring_queries: ring capacity per kind (cp, ray, sil); step_queries: most queries of
     one kind per step and the largest request; max_inflight: closest-point / ray step
-    slots (streams); silhouette steps have sil_slots slots of their own holding at most
-    sil_share of the GPU together (above 1 they may oversubscribe it; each slot at most
-    all of it), sil_step_queries queries per step.  Served requests are sparse (few
+    slots (streams); silhouette steps have sil_slots slots of their own on the lowest
+    stream priority, sil_step_queries queries per step; in the default "warp" form each
+    query is a block that exits when answered, so closest-point / ray blocks are placed
+    first and silhouettes fill the rest of the GPU, while the persistent forms hold at
+    most sil_share of the GPU together (above 1 they may oversubscribe it; each slot at
+    most all of it).  Served requests are sparse (few
     queries per scene per step), so closest points default to one lane per query in the
     reference order with long traversals taken over one per warp ("split": cheaper than
     a warp-coherent walk when neighbours are far apart, and the slowest query no longer

@@ -305,10 +305,14 @@ gq_status gq_batch_device_error(gq_batch *batch, void *stream, int32_t *flags);
  * a step slot is free: one gq_batch launch for all scenes (or, with
  * GQ_SERVER_PER_REQUEST, one single-scene call per request, the scene's tuned
  * variant).  Closest-point and ray requests share max_inflight slots; silhouette
- * requests, whose traversals are far longer, have sil_slots slots of their own whose
- * launches together hold at most sil_share of the GPU and take at most
- * sil_step_queries queries each, so the other kinds never queue behind them and a
- * small silhouette request does not wait for a large one.
+ * requests, whose traversals are far longer, have sil_slots slots of their own on the
+ * lowest stream priority, taking at most sil_step_queries queries each, so the other
+ * kinds never queue behind them and a small silhouette request does not wait for a
+ * large one.  Silhouette steps in the default one-query-per-warp form launch one block
+ * per query that exits when its query is answered, so the blocks of the higher-priority
+ * closest-point / ray steps are placed first and silhouettes fill the rest of the GPU;
+ * the other silhouette forms run persistent launches that together hold at most
+ * sil_share of the GPU.
  * Each slot has its own stream, so the results of one step go back to the host while
  * the next computes.  Results are those of gq_batch_run. */
 typedef struct gq_server gq_server;
@@ -321,7 +325,7 @@ typedef struct {
     int64_t step_queries;     /* most queries of one kind in one step, and the largest request (0: 1<<19) */
     int32_t max_inflight;     /* step slots for closest-point and ray steps (0: 3) */
     int32_t flags;            /* GQ_BATCH_*_EXACT | GQ_SERVER_PER_REQUEST */
-    float sil_share;          /* share of the GPU's resident blocks all silhouette steps together may hold (0: 1.5;
+    float sil_share;          /* share of the GPU's resident blocks all persistent silhouette steps together may hold (0: 1.5;
                                  above 1 they may oversubscribe it, each slot capped at 1) */
     int32_t sil_slots;        /* silhouette step slots (0: 3) */
     int64_t sil_step_queries; /* most silhouette queries in one step, unless one request is larger (0: 1<<15) */
