@@ -35,6 +35,8 @@ ARRAY_SNCH_NODES = 2
 ARRAY_SILHOUETTES = 3
 ARRAY_RAW_SILHOUETTES = 4
 ARRAY_WIDE_NODES = 5
+ARRAY_SNCH_PAIRS = 6
+ARRAY_SIL_RECORDS = 7
 
 DEVERR_STACK = 1
 

@@ -248,9 +248,13 @@ gq_status build_scene(const float *vertices, int64_t nv, const int32_t *prims, i
         d.root_hi[k] = k < D ? img.root_hi[k] : 0.f;
     }
     if (o.device < 0) {  // host-only scene: reference arrays, no device copy
-        const size_t words = img.wnodes.size() * sizeof(img.wnodes[0]) / 4;
-        s->wide_words.resize(words);
-        if (words) std::memcpy(s->wide_words.data(), img.wnodes.data(), words * 4);
+        auto keep = [](std::vector<float> &dst, const void *src, size_t bytes) {
+            dst.resize(bytes / 4);
+            if (bytes) std::memcpy(dst.data(), src, bytes);
+        };
+        keep(s->wide_words, img.wnodes.data(), img.wnodes.size() * sizeof(img.wnodes[0]));
+        keep(s->spair_words, img.spairs.data(), img.spairs.size() * sizeof(img.spairs[0]));
+        keep(s->sil_words, img.sils.data(), img.sils.size() * sizeof(img.sils[0]));
         *out = s.release();
         return GQ_OK;
     }
@@ -518,11 +522,13 @@ gq_status gq_scene_get_info(const gq_scene *s, gq_scene_info *info) {
 gq_status gq_scene_ref_array(const gq_scene *s, int32_t which, float *dst, int64_t cap, int64_t *len) {
     if (!s || !len) return fail(GQ_ERR_INVALID, "null argument");
     std::vector<float> v;
-    if (which == GQ_ARRAY_WIDE_NODES) {
-        if (s->device >= 0) return fail(GQ_ERR_UNSUPPORTED, "wide node dump is kept for host-only scenes");
-        *len = (int64_t)s->wide_words.size();
-        if (dst && cap > 0)
-            std::memcpy(dst, s->wide_words.data(), sizeof(float) * (size_t)std::min<int64_t>(cap, *len));
+    if (which == GQ_ARRAY_WIDE_NODES || which == GQ_ARRAY_SNCH_PAIRS || which == GQ_ARRAY_SIL_RECORDS) {
+        if (s->device >= 0) return fail(GQ_ERR_UNSUPPORTED, "device record dumps are kept for host-only scenes");
+        const std::vector<float> &w = which == GQ_ARRAY_WIDE_NODES   ? s->wide_words
+                                      : which == GQ_ARRAY_SNCH_PAIRS ? s->spair_words
+                                                                     : s->sil_words;
+        *len = (int64_t)w.size();
+        if (dst && cap > 0) std::memcpy(dst, w.data(), sizeof(float) * (size_t)std::min<int64_t>(cap, *len));
         return GQ_OK;
     }
     const bool snch_needed = which == GQ_ARRAY_SNCH_NODES || which == GQ_ARRAY_SILHOUETTES ||

@@ -49,6 +49,7 @@ struct gq_scene {
     int exact_stack = 0, wide_stack = 0;
     int64_t n_wide = 0, n_sil = 0;
     std::vector<float> wide_words;  // host copy of the wide nodes (host-only scenes)
+    std::vector<float> spair_words, sil_words;  // host copies of the SNCH pairs and silhouette records (idem)
     std::vector<void *> allocs;
     int64_t device_bytes = 0;
     gqd::DevScene dev{};

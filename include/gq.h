@@ -170,6 +170,10 @@ gq_status gq_scene_get_tuning(const gq_scene *scene, int32_t kind, gq_tuning *tu
 #define GQ_ARRAY_RAW_SILHOUETTES 4 /* one per vertex / unique edge */
 #define GQ_ARRAY_WIDE_NODES 5      /* quantised 8-wide node records as raw 32-bit words (24 / 20 per node);
                                       host-only scenes (device < 0) only */
+#define GQ_ARRAY_SNCH_PAIRS 6      /* SNCH pair records (gq_spair2_t / gq_spair3_t) as raw 32-bit words
+                                      (20 / 40 per pair; pair 0 is the root's); host-only scenes only */
+#define GQ_ARRAY_SIL_RECORDS 7     /* silhouette records (gq_silv_t / gq_sile_t) as raw 32-bit words
+                                      (8 / 16 per record, in leaf order); host-only scenes only */
 gq_status gq_scene_ref_array(const gq_scene *scene, int32_t which, float *dst, int64_t cap, int64_t *len);
 
 /* build_flat_silhouette_edges (src/gquery.cpp:250, src/shapes/silhouette_edge.cpp:62-71):

@@ -17,6 +17,7 @@
 
 #include "gq_fmath.h"
 #include "sil_filter.h"
+#include "sil_ref.h"
 
 namespace {
 
@@ -33,9 +34,6 @@ struct Rng {
     float sgn() { return (next() & 1) ? 1.f : -1.f; }
 };
 
-struct V {
-    float x, y, z;
-};
 V add(V a, V b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
 V sub(V a, V b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
 V mul(V a, float s) { return {a.x * s, a.y * s, a.z * s}; }
@@ -46,19 +44,6 @@ V unit(V a) {
     return {(float)(a.x / l), (float)(a.y / l), (float)(a.z / l)};
 }
 V cross(V a, V b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
-
-// The kernels' per-edge test: closest point q (closest_point_line_segment, math.py),
-// w = q - x, silhouette when (w . n0) * (w . n1) < 0.
-bool reference_silhouette(V a, V b, V n0, V n1, V x) {
-    const float ux = b.x - a.x, uy = b.y - a.y, uz = b.z - a.z;
-    const float vx = x.x - a.x, vy = x.y - a.y, vz = x.z - a.z;
-    const float t = gq_clamp(gq_div(gq_dot3(vx, vy, vz, ux, uy, uz), gq_dot3(ux, uy, uz, ux, uy, uz)), 0.f, 1.f);
-    const float qx = gq_lerp(a.x, b.x, t), qy = gq_lerp(a.y, b.y, t), qz = gq_lerp(a.z, b.z, t);
-    const float wx = qx - x.x, wy = qy - x.y, wz = qz - x.z;
-    const float d0 = gq_dot3(wx, wy, wz, n0.x, n0.y, n0.z);
-    const float d1 = gq_dot3(wx, wy, wz, n1.x, n1.y, n1.z);
-    return d0 * d1 < 0.f;
-}
 
 struct Count {
     long long cases = 0, usable = 0, excluded = 0, silhouettes = 0, unsound = 0;
