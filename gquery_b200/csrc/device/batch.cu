@@ -508,16 +508,26 @@ __global__ void __launch_bounds__(kBlock) k_sil_heavy(const DevScene *scenes, Ba
     }
 }
 
-// A step with silhouettes only (the server's silhouette slots): one block of one warp
-// per query, which answers it and exits.  Blocks end all the time, so the block
-// scheduler places the pending blocks of higher-priority streams (the server's closest
-// points and rays) first and fills the rest of the GPU with silhouettes: no share of the
-// GPU has to be set aside, and a large step uses all of it when nothing else waits.  One
-// warp per block, so a heavy query holds no idle warps; 32 blocks of 64 registers a
-// thread fill the register file as the persistent form does.
+// A step with silhouettes only on the whole GPU: the phase alone, so that its register
+// count, not k_batch's, sets the residency; persistent warps.
 template <int D>
-__global__ void __launch_bounds__(32, 32) k_batch_silw(const DevScene *scenes, int n_scenes, BatchKind sil,
-                                                       gq_sil_out sil_out, int32_t *err) {
+__global__ void __launch_bounds__(kBlock, 8) k_batch_silw(const DevScene *scenes, int n_scenes, BatchKind sil,
+                                                          gq_sil_out sil_out, unsigned long long *counter,
+                                                          int32_t *err) {
+    sil_warp_phase<D>(scenes, n_scenes, sil, sil_out, counter, err);
+}
+
+// A step with silhouettes only beside other work (the server's silhouette slots, which
+// pass a share of the GPU): one block of one warp per query, which answers it and exits.
+// Blocks end all the time, so the block scheduler places the pending blocks of
+// higher-priority streams (the server's closest points and rays) first and fills the
+// rest of the GPU with silhouettes: no share has to be set aside, and a large step uses
+// all of the GPU when nothing else waits.  One warp per block, so a heavy query holds no
+// idle warps; 32 blocks of 64 registers a thread fill the register file as the
+// persistent form does.
+template <int D>
+__global__ void __launch_bounds__(32, 32) k_batch_silw1(const DevScene *scenes, int n_scenes, BatchKind sil,
+                                                        gq_sil_out sil_out, int32_t *err) {
     __shared__ int2 wst[wsil::kWarpStack];
     sil_warp_query<D>(scenes, n_scenes, sil, sil_out, err, (int64_t)blockIdx.x, wst);
 }
@@ -529,9 +539,24 @@ cudaError_t launch_batch(const DevScene *scenes_dev, int n_scenes, BatchKind kin
                          cudaStream_t st) {
     // the one-query-per-warp silhouette phase keeps its stacks in dynamic shared memory
     const size_t smem = (sil_mode == 2 && kinds[2].n > 0) ? (size_t)(kBlock / 32) * wsil::kWarpStack * sizeof(int2) : 0;
-    if (smem && kinds[0].n <= 0 && kinds[1].n <= 0) {  // silhouettes only: one block per query
-        if (kinds[2].n > 0x7fffffff) return cudaErrorInvalidValue;
-        k_batch_silw<D><<<dim3((unsigned)kinds[2].n), 32, 0, st>>>(scenes_dev, n_scenes, kinds[2], sil_out, err);
+    if (smem && kinds[0].n <= 0 && kinds[1].n <= 0) {  // silhouettes only: the phase's own kernel
+        if (grid_share > 0.f && grid_share < 1.f) {      // beside other work: one block per query
+            if (kinds[2].n > 0x7fffffff) return cudaErrorInvalidValue;
+            k_batch_silw1<D><<<dim3((unsigned)kinds[2].n), 32, 0, st>>>(scenes_dev, n_scenes, kinds[2], sil_out,
+                                                                        err);
+            return cudaGetLastError();
+        }
+        static int wbps = 0, w_sm = 0;
+        if (!wbps) {
+            int dev = 0, b = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&w_sm, cudaDevAttrMultiProcessorCount, dev);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_silw<D>, kBlock, smem);
+            wbps = b < 1 ? 1 : b;
+        }
+        const int64_t want = std::min<int64_t>((int64_t)wbps * w_sm, (kinds[2].n * 32 + kBlock - 1) / kBlock);
+        k_batch_silw<D><<<dim3((unsigned)want), kBlock, smem, st>>>(scenes_dev, n_scenes, kinds[2], sil_out, counter,
+                                                                    err);
         return cudaGetLastError();
     }
     const int mi = smem ? 1 : 0;
