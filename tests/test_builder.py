@@ -71,7 +71,10 @@ def test_build_deterministic_and_thread_count_independent():
     a = _host(v, f, 3, n_threads=1)
     b = _host(v, f, 3, n_threads=8)
     c = _host(v, f, 3, n_threads=3)
-    for which in (L.ARRAY_BVH_NODES, L.ARRAY_PRIMITIVES, L.ARRAY_SNCH_NODES, L.ARRAY_SILHOUETTES):
+    # the reference layouts, and the device records built from them (wide nodes, SNCH
+    # pairs with their node bounds and searched cone axes, silhouette records)
+    for which in (L.ARRAY_BVH_NODES, L.ARRAY_PRIMITIVES, L.ARRAY_SNCH_NODES, L.ARRAY_SILHOUETTES,
+                  L.ARRAY_WIDE_NODES, L.ARRAY_SNCH_PAIRS, L.ARRAY_SIL_RECORDS):
         ra, rb, rc = a.ref_array(which), b.ref_array(which), c.ref_array(which)
         assert np.array_equal(ra.view(np.uint32), rb.view(np.uint32)), which
         assert np.array_equal(ra.view(np.uint32), rc.view(np.uint32)), which
