@@ -53,12 +53,15 @@ def parse():
     ap.add_argument("--n", type=int, default=1 << 23, help="queries of each kind per rank")
     ap.add_argument("--variant", default="auto", choices=["auto", "wide8", "coherent", "exact"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--ref-n", type=int, default=1 << 20,
+                    help="reference arm: closest points and rays per step (a prefix of the workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the exact and wide8 side-by-side runs")
     ap.add_argument("--no-autotune", action="store_true", help="use the built-in tuning table as it is")
-    ap.add_argument("--sections", default="c0,build,c2,c3,c4",
-                    help="beside the headline (cp + rays on the level-8 mesh): c0 2D closest point on the "
+    ap.add_argument("--sections", default="fp64,c0,build,c2,c3,c4",
+                    help="beside the headline (cp + rays on the level-8 mesh): fp64 FP32-vs-FP64 error on "
+                         "65,536 of the headline's closest points and rays, c0 2D closest point on the "
                          "4,096-vertex star (GPU and CPU), build host SAH vs device build of the "
                          "level-8 mesh, c2 silhouettes on the level-7 "
                          "mesh, c3 512 uneven 2D scenes in one batched launch, c4 serving 64 meshes; "
@@ -193,6 +196,67 @@ def dev_ms(fn, steps, warmup, flush=None):
     return statistics.median(ts)
 
 
+def l2_copy_gbs(dev):
+    """Copy bandwidth of a working set that stays in L2 (2 x 16 MB of the 126 MB):
+    read + write bytes over CUDA-event time, best of three runs of 50 copies."""
+    import torch
+    a = torch.empty(16 << 20, dtype=torch.uint8, device=dev)
+    b = torch.empty_like(a)
+    for _ in range(10):
+        b.copy_(a)
+    best = 0.0
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(50):
+            b.copy_(a)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2 * a.numel() * 50 / (e0.elapsed_time(e1) / 1e3) / 1e9)
+    return best
+
+
+def fp64_error(kind, valid, d, d64):
+    """FP32 answers against the FP64 brute force: validity that differs, and the error of
+    the distance (closest point, silhouette: absolute; ray: relative to max(t, 1)) where
+    both found one.  Silhouettes also count answers farther than the FP64 nearest by more
+    than 5e-7 (the reference's cone test may skip the nearest silhouette)."""
+    import torch
+    v = valid.bool()
+    h = torch.isfinite(d64)
+    both = v & h
+    diff = d.double() - d64
+    err = diff.abs() / d64.clamp(min=1.0) if kind == "ray" else diff.abs()
+    e = err[both]
+    out = {"n": int(v.numel()), "found": int(both.sum()), "valid_differs": int((v != h).sum())}
+    if e.numel():
+        out.update({"max": float(e.max()), "median": float(e.median()),
+                    "p99_9": float(torch.quantile(e.float(), 0.999)),
+                    "unit": "relative to max(t, 1)" if kind == "ray" else "absolute"})
+    if kind == "sil":
+        out["farther_than_fp64"] = int((diff[both] > 5e-7).sum())
+        out["nearer_than_fp64"] = int((diff[both] < -5e-7).sum())
+    return out
+
+
+def tie_stats(a, b, rel=2e-6):
+    """Answers of a fast variant `a` against the exact traversal `b` (records of device
+    tensors): validity mismatches, differing primitives split into exact ties (the same
+    FP32 distance bit for bit), loose ties (distances within `rel` relative) and the rest."""
+    import torch
+    va, vb = a.valid.bool(), b.valid.bool()
+    both = va & vb
+    da, db = a.d.double(), b.d.double()
+    reld = (da - db).abs() / torch.maximum(torch.maximum(da.abs(), db.abs()), torch.full_like(da, 1e-30))
+    diff = both & (a.prim_id != b.prim_id)
+    exact = diff & (a.d == b.d)
+    return {"n": int(va.numel()), "valid_mismatch": int((va != vb).sum()), "prim_mismatch": int(diff.sum()),
+            "prim_mismatch_exact_tie": int(exact.sum()),
+            "prim_mismatch_loose_tie": int((diff & ~exact & (reld <= rel)).sum()),
+            "prim_mismatch_not_tie": int((diff & (reld > rel)).sum()),
+            "max_rel_d": float(reld[both].max()) if bool(both.any()) else 0.0}
+
+
 def section_c0(args, dev, flush):
     """2D closest point: 4,096-vertex star polyline, 1,048,576 points U[-2,2]^2 - the
     configuration that also runs on the CPU: every GPU variant and the CPU oracle port
@@ -223,6 +287,20 @@ def section_c0(args, dev, flush):
     cpu_s = time.perf_counter() - t0
     res["cpu_oracle"] = {"seconds": cpu_s, "mqueries_per_s": n / cpu_s / 1e6, "cores": threads, "kind": "port"}
     assert sc.device_error() == 0
+    # FP32 (the exact traversal, equal to the reference's) against FP64 brute force on the
+    # first 65,536 points, 65,536 rays and 65,536 silhouette points of this star
+    snch = Scene(V, E, 2, device=dev.index or 0, build_snch=True)
+    m = 1 << 16
+    qs = q[:m]
+    ro, rd = (torch.as_tensor(a).to(dev) for a in W.rays(m, 2, seed=3))
+    cp = snch.closest_point(qs, variant="exact")
+    ray = snch.intersect(ro, rd, variant="exact")
+    sil = snch.closest_silhouette(qs, variant="exact")
+    res["fp64_error"] = {
+        "cp2d": fp64_error("cp", cp.valid, cp.d, snch.brute_f64("cp", qs)[0]),
+        "ray2d": fp64_error("ray", ray.valid, ray.d, snch.brute_f64("ray", ro, rd)[0]),
+        "sil2d": fp64_error("sil", sil.valid, sil.d, snch.brute_f64("sil", qs)[0])}
+    assert snch.device_error() == 0
     return res
 
 
@@ -299,6 +377,14 @@ def section_c2(args, dev, flush):
         ms = dev_ms(lambda: sc.closest_silhouette(x, variant=variant, out=out, order=order, scratch=scratch),
                     steps=2 if variant == "exact" else 3, warmup=1, flush=flush)
         res[name] = {"ms": ms, "mqueries_per_s": n / ms / 1e3}
+    assert sc.device_error() == 0
+    # FP32 against FP64 brute force over every silhouette edge, first 65,536 points
+    xs = x[:1 << 16]
+    d64 = sc.brute_f64("sil", xs)[0]
+    res["fp64_error"] = {}
+    for variant in ("exact", "coherent"):
+        r = sc.closest_silhouette(xs, variant=variant)
+        res["fp64_error"][f"sil3d_{variant}"] = fp64_error("sil", r.valid, r.d, d64)
     assert sc.device_error() == 0
     res["coherent_vs_plain"] = res["plain_exact"]["ms"] / res["coherent"]["ms"]
     res["warp_vs_plain"] = res["plain_exact"]["ms"] / res["warp"]["ms"]
@@ -382,6 +468,7 @@ def section_c3(args, dev, flush):
     mq = lambda ms: total / ms / 1e3 if ms else None  # noqa: E731
     return {"workload": f"512 star polylines, {sum(e.shape[0] for _, e in geo)} segments, {total} queries "
                         f"(cp {ns[0]}, ray {ns[1]}, sil {ns[2]})", "build_s": build_s,
+            "batched_vs_tuned_per_scene": tuned_ms / graph_ms if tuned_ms else None,
             "batched_graph": {"ms": graph_ms, "mqueries_per_s": mq(graph_ms)},
             "batched_eager": {"ms": eager_ms, "mqueries_per_s": mq(eager_ms)},
             "batched_kind_alone_ms": kind_ms,
@@ -475,7 +562,7 @@ def run_reference(args):
         return 0
     from gquery_b200 import workloads as W
     V, F = W.config1_mesh()
-    per_step = 16384
+    per_step = args.ref_n  # a prefix of the workload's queries of each kind
     q = W.uniform_points(per_step, 3, seed=1)
     o, d = W.rays(per_step, 3, seed=2)
     import oracle
@@ -509,6 +596,37 @@ def run_reference(args):
             "e2e": {"value": value, "unit": "Mqueries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def summary(line):
+    """The figures the north star names, side by side, at the end of the line."""
+    def get(*path):
+        x = line
+        for k in path:
+            if not isinstance(x, dict) or x.get(k) is None:
+                return None
+            x = x[k]
+        return x
+    s = {"mqps": {"plain_exact": line.get("plain_exact_mqps"), "quantised_wide8": line.get("quantised_wide8_mqps"),
+                  "tuned": line.get("value"), "e2e": get("e2e", "value"),
+                  "cpu_port": get("cpu_baseline", "value")},
+         "quantised_wide8_vs_plain": line.get("quantised_wide8_vs_plain"), "tuned_vs_plain": line.get("tuned_vs_plain"),
+         "roofline_frac_hbm": get("roofline", "frac"), "roofline_frac_l2": get("roofline", "l2", "frac"),
+         "ties_tuned_cp": {k: get("parity", "tuned", "cp", k) for k in
+                           ("prim_mismatch", "prim_mismatch_exact_tie", "prim_mismatch_loose_tie",
+                            "prim_mismatch_not_tie", "valid_mismatch")},
+         "fp64_max_err": {k: get("fp64_error", k, "max") for k in ("cp3d_exact", "ray3d_exact")},
+         "c2_coherent_mqps": get("silhouette_c2", "coherent", "mqueries_per_s"),
+         "c3_batched_mqps": get("batched_c3", "batched_graph", "mqueries_per_s"),
+         "c3_batched_vs_tuned_per_scene": get("batched_c3", "batched_vs_tuned_per_scene")}
+    for k in ("cp2d", "ray2d", "sil2d"):
+        s["fp64_max_err"][k] = get("closest_point_2d_c0", "fp64_error", k, "max")
+    s["fp64_max_err"]["sil3d_exact"] = get("silhouette_c2", "fp64_error", "sil3d_exact", "max")
+    loads = get("serving_c4", "batched", "loads") or []
+    for ld in loads:
+        if abs(ld.get("load_of_batched_peak", 0) - 0.8) < 1e-9:
+            s["c4_p50_p99_ms_at_80pct"] = [ld.get("p50_ms"), ld.get("p99_ms")]
+    return s
 
 
 def main():
@@ -617,6 +735,36 @@ def main():
     main_res, clocks = timed(args.variant, args.steps, max(3, args.warmup), clocks=True)
     assert scene.device_error() == 0, "device error flag raised"
 
+    # ---- parity at full size: the quantised and tuned answers against the exact ones ----
+    parity = None
+    if not args.no_compare:
+        ex_cp, ex_ray = scene.alloc_cp(n), scene.alloc_ray(n)
+        scene.closest_point(q, variant="exact", out=ex_cp)
+        scene.intersect(o, d, variant="exact", out=ex_ray)
+        parity = {"note": "answers on all queries of this rank against the exact traversal (gQuery's visit "
+                          "order); ties: exact = the same FP32 distance, loose = within 2e-6 relative"}
+        for name, variant in (("quantised_wide8", "wide8"), ("tuned", args.variant)):
+            scene.closest_point(q, variant=variant, out=cp_out)
+            scene.intersect(o, d, variant=variant, out=ray_out)
+            parity[name] = {"cp": tie_stats(cp_out, ex_cp), "ray": tie_stats(ray_out, ex_ray)}
+        del ex_cp, ex_ray
+        assert scene.device_error() == 0
+    fp64 = None
+    sections_on = [x for x in args.sections.split(",") if x and x != "none"] if world == 1 else []
+    if "fp64" in sections_on:
+        m = 1 << 16
+        qs, os_, ds = q[:m], o[:m], d[:m]
+        d64 = scene.brute_f64("cp", qs)[0]
+        t64 = scene.brute_f64("ray", os_, ds)[0]
+        fp64 = {"workload": f"first {m} closest points and rays of the headline workload, FP64 brute force over "
+                            "all 1,310,720 triangles"}
+        for variant in ("exact", args.variant):
+            rc = scene.closest_point(qs, variant=variant)
+            rr = scene.intersect(os_, ds, variant=variant)
+            fp64[f"cp3d_{variant}"] = fp64_error("cp", rc.valid, rc.d, d64)
+            fp64[f"ray3d_{variant}"] = fp64_error("ray", rr.valid, rr.d, t64)
+        assert scene.device_error() == 0
+
     total_q = 2 * n * world
     value = total_q / (main_res["step_ms"] / 1e3) / 1e6
     plain_value = total_q / (plain["step_ms"] / 1e3) / 1e6 if plain else None
@@ -668,6 +816,8 @@ def main():
             r.wait_event(ev["q"])
             if ln.used:
                 r.wait_event(ev["done"])  # previous records of this lane are back on the host
+            with torch.cuda.stream(r):
+                flush.zero_()  # L2 flushed before every step, as in the device-timed run
             scene.order(ln.qd, out=ln.perm_q, scratch=ln.scratch, stream=r)
             scene.closest_point(ln.qd, variant=args.variant, out=ln.cp, order=ln.perm_q, scratch=ln.scratch, stream=r)
             ev["cp"].record(r)
@@ -709,6 +859,7 @@ def main():
         ok = all(torch.equal(lanes[0].host_cp[k], v.cpu()) for k, v in vars(lanes[0].cp).items())
         e2e = {"value": total_q / (ms / 1e3) / 1e6, "unit": "Mqueries/s", "ms_per_step": ms,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "lanes": 2, "host_records_match": ok,
+               "l2": "flushed before every step (a 256 MB write on the step's stream, inside the timed region)",
                "note": "public API (Scene.order / closest_point / intersect) on pinned host buffers; steps "
                        "alternate between two lanes so copies overlap traversals"}
 
@@ -728,12 +879,20 @@ def main():
             achieved = b * n / (t_ms / 1e3) / 1e9
             tuned_v = scene.get_tuning(dominant)["variant"] if args.variant == "auto" else args.variant
             tr = traffic_per_query().get(f"{dominant}3d_{tuned_v}")
+            l2_peak = l2_copy_gbs(dev)
+            prof = traffic_per_query().get(f"{dominant}3d_{tuned_v}_counters", {})
             roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                     "traffic": (tr * n if tr else None), "kernel": f"{dominant}3d_{tuned_v}",
                     "traffic_note": "DRAM bytes per query from an ncu capture at 1,048,576 queries "
                                     "(profiles/traffic.json), scaled to the launch's query count",
                     "algorithmic_bytes_per_query": b, "peak_source": peak_kind,
-                    "note": "achieved = reference binary-traversal bytes (oracle visit counts) / kernel time"}
+                    "note": "achieved = reference binary-traversal bytes (oracle visit counts) / kernel time; "
+                            "those bytes are served from L2 and L1, so the level that serves them is below",
+                    "l2": {"peak": l2_peak, "peak_source": "measured in this run: L2-resident copy, 2 x 16 MB",
+                           "frac": achieved / l2_peak},
+                    "dram": {"achieved": (tr * n / (t_ms / 1e3) / 1e9) if tr else None,
+                             "frac": (tr * n / (t_ms / 1e3) / 1e9 / peak) if tr else None},
+                    "binding": prof or None}
         line = {
             "metric": METRIC, "value": value, "unit": "Mqueries/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": main_res["step_ms"], "higher_is_better": True,
@@ -749,11 +908,15 @@ def main():
                       "vs_plain": value / plain_value if plain else None, "autotune": tuning_report},
             "breakdown_ms": {k: main_res[k] for k in ("order_cp_ms", "cp_ms", "order_ray_ms", "ray_ms",
                                                       "wall_ms_per_step")},
+            "plain_exact_mqps": plain_value, "quantised_wide8_mqps": quant_value,
+            "quantised_wide8_vs_plain": quant_value / plain_value if plain else None,
+            "tuned_vs_plain": value / plain_value if plain else None,
+            "parity": parity, "fp64_error": fp64,
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
             "gpu_launches": 4 * args.steps,
             "gpu_launches_note": "own kernels per step: 2 Morton-key + 2 traversal (CUB radix-sort kernels extra)",
         }
-        sections = [x for x in args.sections.split(",") if x and x != "none"] if world == 1 else []
+        sections = sections_on
         flush_buf = flush
         for name, fn in (("c0", lambda: section_c0(args, dev, flush_buf)),
                          ("build", lambda: section_build(args, dev, flush_buf)),
@@ -765,6 +928,7 @@ def main():
                 t_sec = time.perf_counter()
                 line[key] = fn()
                 line[key]["section_wall_s"] = time.perf_counter() - t_sec
+        line["summary"] = summary(line)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

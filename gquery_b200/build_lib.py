@@ -66,20 +66,24 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
     nvcc = cuda / "bin" / "nvcc"
     BUILD.mkdir(parents=True, exist_ok=True)
     LIB.parent.mkdir(parents=True, exist_ok=True)
-    objs = []
+    jobs = []
     for src in HOST_SOURCES:
         obj = BUILD / (src.replace("/", "_") + ".o")
-        _run(["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall",
-              "-Wno-unused-function", f"-I{cuda / 'include'}", "-c", CSRC / src, "-o", obj], verbose)
-        objs.append(obj)
+        jobs.append((["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall",
+                      "-Wno-unused-function", f"-I{cuda / 'include'}", "-c", CSRC / src, "-o", obj], verbose, obj))
     for src in DEVICE_SOURCES:
         obj = BUILD / (src.replace("/", "_") + ".o")
         flags = ["-O3", "-std=c++17", "--fmad=false", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
                  "-ffp-contract=off", *ARCH]
         if ptxas_verbose:
             flags += ["-Xptxas", "-v"]
-        _run([nvcc, *flags, "-c", CSRC / src, "-o", obj], verbose or ptxas_verbose)
-        objs.append(obj)
+        jobs.append(([nvcc, *flags, "-c", CSRC / src, "-o", obj], verbose or ptxas_verbose, obj))
+    # the translation units are independent: compile them side by side
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 1)) as pool:
+        for f in [pool.submit(_run, cmd, vb) for cmd, vb, _ in jobs]:
+            f.result()
+    objs = [obj for _, _, obj in jobs]
     tmp = LIB.with_suffix(".so.tmp")
     _run([nvcc, "-shared", *ARCH, "-cudart", "static", "-o", tmp, *objs, "-lpthread"], verbose)
     os.replace(tmp, LIB)

@@ -614,6 +614,7 @@ gq_status gq_query_order(const gq_scene *s, gq_vecs points, int64_t n, int32_t *
     if (!vecs_ok(points)) return fail(GQ_ERR_INVALID, "null point array");
     if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "scene was built without a device copy");
     DeviceGuard g(s->device);
+    if (!g.ok) return fail(GQ_ERR_CUDA, "cannot select the scene's CUDA device");
     cudaStream_t cs = (cudaStream_t)stream;
     const size_t need = gqd::morton_scratch_bytes(n);
     Scratch scr;
@@ -642,6 +643,7 @@ gq_status gq_closest_point(const gq_scene *s, gq_vecs q, int64_t n, const gq_cp_
     if (st != GQ_OK) return st;
     if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "scene was built without a device copy");
     DeviceGuard g(s->device);
+    if (!g.ok) return fail(GQ_ERR_CUDA, "cannot select the scene's CUDA device");
     cudaStream_t cs = (cudaStream_t)stream;
     Scratch scr;
     const int32_t *perm = nullptr;
@@ -670,6 +672,7 @@ gq_status gq_closest_point_noalloc(const gq_scene *s, gq_vecs q, int64_t n, cons
     if (st != GQ_OK) return st;
     if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "scene was built without a device copy");
     DeviceGuard g(s->device);
+    if (!g.ok) return fail(GQ_ERR_CUDA, "cannot select the scene's CUDA device");
     cudaError_t e = gqd::noalloc_closest_point(s->dev, v, to_tune(s, GQ_KIND_CLOSEST_POINT, v), q, n, sort,
                                                *out, (cudaStream_t)stream);
     if (e != cudaSuccess) return fail_cuda(e, "closest_point_noalloc");
@@ -687,6 +690,7 @@ gq_status gq_intersect(const gq_scene *s, gq_vecs origin, gq_vecs dir, const flo
     if (st != GQ_OK) return st;
     if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "scene was built without a device copy");
     DeviceGuard g(s->device);
+    if (!g.ok) return fail(GQ_ERR_CUDA, "cannot select the scene's CUDA device");
     cudaStream_t cs = (cudaStream_t)stream;
     Scratch scr;
     const int32_t *perm = nullptr;
@@ -714,6 +718,7 @@ gq_status gq_closest_silhouette(const gq_scene *s, gq_vecs x, const float *r_max
     if (v != GQ_VARIANT_EXACT && v != GQ_VARIANT_COHERENT && v != GQ_VARIANT_WARP)
         return fail(GQ_ERR_UNSUPPORTED, "silhouette queries run the exact, coherent or warp variant");
     DeviceGuard g(s->device);
+    if (!g.ok) return fail(GQ_ERR_CUDA, "cannot select the scene's CUDA device");
     cudaStream_t cs = (cudaStream_t)stream;
     Scratch scr;
     const int32_t *perm = nullptr;
@@ -733,6 +738,7 @@ gq_status gq_closest_point_brute(const gq_scene *s, gq_vecs q, int64_t n, const 
     if (!vecs_ok(q)) return fail(GQ_ERR_INVALID, "null query array");
     if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "scene was built without a device copy");
     DeviceGuard g(s->device);
+    if (!g.ok) return fail(GQ_ERR_CUDA, "cannot select the scene's CUDA device");
     cudaError_t e = gqd::launch_cp_brute(s->dev, q, n, *out, (cudaStream_t)stream);
     if (e != cudaSuccess) return fail_cuda(e, "closest_point_brute launch");
     return GQ_OK;
@@ -746,6 +752,7 @@ gq_status gq_intersect_brute(const gq_scene *s, gq_vecs origin, gq_vecs dir, con
     if (!vecs_ok(origin) || !vecs_ok(dir)) return fail(GQ_ERR_INVALID, "null ray array");
     if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "scene was built without a device copy");
     DeviceGuard g(s->device);
+    if (!g.ok) return fail(GQ_ERR_CUDA, "cannot select the scene's CUDA device");
     cudaError_t e = gqd::launch_ray_brute(s->dev, origin, dir, r_max, n, *out, (cudaStream_t)stream);
     if (e != cudaSuccess) return fail_cuda(e, "intersect_brute launch");
     return GQ_OK;
@@ -796,15 +803,72 @@ gq_status gq_closest_silhouette_brute(const gq_scene *s, gq_vecs x, const float 
     return GQ_OK;
 }
 
+// Uploads (once) the SNCH's raw silhouette list (one record per polyline vertex, one per
+// unique mesh edge) as float positions for the FP64 silhouette scan: 2D a, b, c, flag
+// (1 = both neighbours exist), 3D a, b, c, d, flag (1 = boundary edge, always a
+// silhouette; the reference's size_t indices never hold -1, so this stays 0).
+static gq_status ensure_f64_sils(gq_scene *s) {
+    std::lock_guard<std::mutex> lk(s->base_mu);
+    if (s->n_f64_sils >= 0) return GQ_OK;
+    gq_status st = ensure_trees(s);
+    if (st != GQ_OK) return st;
+    try {
+        std::vector<float> rec;
+        int64_t n = 0;
+        if (s->dim == 2) {
+            for (const gqb::SilVertex &x : s->s2.raw) {
+                const bool ok = ((int64_t)(float)x.idx[0] != -1) && ((int64_t)(float)x.idx[2] != -1);
+                const float r[8] = {x.v[0].v[0], x.v[0].v[1], x.v[1].v[0], x.v[1].v[1],
+                                    x.v[2].v[0], x.v[2].v[1], ok ? 1.f : 0.f, 0.f};
+                rec.insert(rec.end(), r, r + 8);
+                ++n;
+            }
+        } else {
+            for (const gqb::SilEdge &x : s->s3.raw) {
+                const bool boundary = ((int64_t)(float)x.idx[0] == -1) || ((int64_t)(float)x.idx[3] == -1);
+                float r[16] = {};
+                const int order[4] = {1, 2, 0, 3};  // a, b, c, d of silhouette_edge.py:75-86
+                for (int k = 0; k < 4; ++k)
+                    for (int c = 0; c < 3; ++c) r[3 * k + c] = x.v[order[k]].v[c];
+                r[12] = boundary ? 1.f : 0.f;
+                rec.insert(rec.end(), r, r + 16);
+                ++n;
+            }
+        }
+        if (!rec.empty()) st = s->upload(rec, &s->f64_sils);
+        if (st == GQ_OK) s->n_f64_sils = n;
+        return st;
+    } catch (const std::bad_alloc &) {
+        return fail(GQ_ERR_NOMEM, "out of host memory building the FP64 silhouette list");
+    }
+}
+
 gq_status gq_brute_f64(const gq_scene *s, int32_t kind, gq_vecs a, gq_vecs b, int64_t n, double *out_d,
                        int32_t *out_id, void *stream) {
     if (!s || !out_d || !out_id) return fail(GQ_ERR_INVALID, "null argument");
-    if (kind != 0 && kind != 1) return fail(GQ_ERR_INVALID, "kind must be 0 or 1");
+    if (kind == 2) {
+        if (n < 0) return fail(GQ_ERR_INVALID, "negative query count");
+        if (n == 0) return GQ_OK;
+        if (!vecs_ok(a)) return fail(GQ_ERR_INVALID, "null query array");
+        if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "scene was built without a device copy");
+        if (!s->has_snch) return fail(GQ_ERR_UNSUPPORTED, "scene was built without the SNCH");
+        if (s->gpu_built) return fail(GQ_ERR_UNSUPPORTED, "scene was built on the device: no host silhouette list");
+        DeviceGuard g(s->device);
+        if (!g.ok) return fail(GQ_ERR_CUDA, "cannot select the scene's CUDA device");
+        gq_status st = ensure_f64_sils(const_cast<gq_scene *>(s));
+        if (st != GQ_OK) return st;
+        cudaError_t e = gqd::launch_sil_f64(s->dim, (const float *)s->f64_sils, s->n_f64_sils, a, n, out_d, out_id,
+                                            (cudaStream_t)stream);
+        if (e != cudaSuccess) return fail_cuda(e, "brute_f64 silhouette launch");
+        return GQ_OK;
+    }
+    if (kind != 0 && kind != 1) return fail(GQ_ERR_INVALID, "kind must be 0, 1 or 2");
     if (n < 0) return fail(GQ_ERR_INVALID, "negative query count");
     if (n == 0) return GQ_OK;
     if (!vecs_ok(a) || (kind == 1 && !vecs_ok(b))) return fail(GQ_ERR_INVALID, "null query array");
     if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "scene was built without a device copy");
     DeviceGuard g(s->device);
+    if (!g.ok) return fail(GQ_ERR_CUDA, "cannot select the scene's CUDA device");
     cudaError_t e = gqd::launch_brute_f64(s->dev, kind, a, b, n, out_d, out_id, (cudaStream_t)stream);
     if (e != cudaSuccess) return fail_cuda(e, "brute_f64 launch");
     return GQ_OK;
@@ -872,6 +936,7 @@ gq_status gq_scene_save(const gq_scene *s, const char *path) {
     ok = ok && std::fwrite(s->verts.data(), sizeof(float), s->verts.size(), out.f) == s->verts.size();
     ok = ok && std::fwrite(s->index.data(), sizeof(int32_t), s->index.size(), out.f) == s->index.size();
     DeviceGuard g(s->device);
+    if (!g.ok) return fail(GQ_ERR_CUDA, "cannot select the scene's CUDA device");
     std::vector<char> buf;
     for (int k = 0; k < 6 && ok; ++k) {
         if (!h.image_bytes[k]) continue;
@@ -960,10 +1025,18 @@ gq_status gq_scene_load(const char *path, int32_t device, gq_scene **out) {
     return GQ_OK;
 }
 
+gq_status gq_scene_set_stack_limit(gq_scene *s, int32_t entries) {
+    if (!s) return fail(GQ_ERR_INVALID, "null scene");
+    if (entries < 0) return fail(GQ_ERR_INVALID, "stack limit must be >= 0");
+    s->dev.stack_cap = entries > 0 ? entries : (1 << 30);
+    return GQ_OK;
+}
+
 gq_status gq_scene_device_error(const gq_scene *s, void *stream, int32_t *flags) {
     if (!s || !flags) return fail(GQ_ERR_INVALID, "null argument");
     if (on_host_only(s)) return fail(GQ_ERR_UNSUPPORTED, "scene was built without a device copy");
     DeviceGuard g(s->device);
+    if (!g.ok) return fail(GQ_ERR_CUDA, "cannot select the scene's CUDA device");
     cudaStream_t cs = (cudaStream_t)stream;
     int32_t v = 0;
     cudaError_t e = cudaMemcpyAsync(&v, s->dev.err, sizeof v, cudaMemcpyDeviceToHost, cs);
@@ -1052,6 +1125,7 @@ gq_status gq_batch_run(gq_batch *b, const gq_batch_queries *cp, const gq_cp_out 
             if (!s->has_snch) return fail(GQ_ERR_UNSUPPORTED, "silhouette queries need every batch scene built with SNCH");
     }
     DeviceGuard g(b->device);
+    if (!g.ok) return fail(GQ_ERR_CUDA, "cannot select the batch's CUDA device");
     const gq_cp_out co = cp_out ? *cp_out : gq_cp_out{};
     const gq_ray_out ro = ray_out ? *ray_out : gq_ray_out{};
     const gq_sil_out so = sil_out ? *sil_out : gq_sil_out{};
@@ -1069,6 +1143,7 @@ gq_status gq_batch_run(gq_batch *b, const gq_batch_queries *cp, const gq_cp_out 
 gq_status gq_batch_device_error(gq_batch *b, void *stream, int32_t *flags) {
     if (!b || !flags) return fail(GQ_ERR_INVALID, "null argument");
     DeviceGuard g(b->device);
+    if (!g.ok) return fail(GQ_ERR_CUDA, "cannot select the batch's CUDA device");
     cudaStream_t cs = (cudaStream_t)stream;
     int32_t v = 0;
     cudaError_t e = cudaMemcpyAsync(&v, b->err, sizeof v, cudaMemcpyDeviceToHost, cs);

@@ -1,8 +1,9 @@
 // Closest-point queries that allocate no device memory.
 //
-// Some callers cannot allocate device memory while they query: code recorded into
-// a CUDA graph with a plain cudaMalloc-based allocator, plugins whose host owns every
-// device allocation, or real-time loops that must not touch an allocator at all.  For
+// Some callers cannot allocate device memory while they query: plugins whose host
+// application owns every device allocation and passes in only input and output
+// buffers, or real-time loops that must not touch an allocator at all (cudaMalloc can
+// synchronise the device and take unbounded time).  For
 // them the per-call scratch of a closest-point query (the work counter of the
 // warp-coherent / persistent kernels and the Morton-sort workspace) lives in a
 // file-scope device array of fixed size, so at most kNoAllocMaxQueries queries fit
@@ -37,7 +38,9 @@ void *g_addr[kMaxDevices] = {};
 
 // Device address of the scratch on the current device, looked up once per device with
 // that device current.  The first call on a device does this lookup, so it should not
-// happen while a stream is being captured.
+// happen while a stream is being captured.  The address belongs to the device's primary
+// context: after cudaDeviceReset, or from another context, it is not valid (the header
+// says so to callers).
 cudaError_t device_scratch(void **out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);

@@ -170,7 +170,7 @@ __device__ __forceinline__ void closest_point(const DevScene &s, unsigned mask, 
             if (ml && mr) {
                 const float kl = warp_min(hl ? a2l : kInf), kr = warp_min(hr ? a2r : kInf);
                 const bool right_first = kr < kl;
-                if (sp + 1 >= STK) {
+                if (sp + 1 >= min(STK, s.stack_cap)) {
                     ovf = true;
                     break;
                 }
@@ -230,7 +230,7 @@ __device__ __forceinline__ void closest_point(const DevScene &s, unsigned mask, 
                 cur = kNone;
                 continue;
             }
-            if (sp + cnt > STK) {
+            if (sp + cnt > min(STK, s.stack_cap)) {
                 ovf = true;
                 break;
             }

@@ -486,6 +486,75 @@ __global__ void __launch_bounds__(kBlock) k_brute_f64(DevScene s, int kind, gq_v
     }
 }
 
+// FP64 nearest silhouette over the scene's raw silhouette list (the reference's
+// SNCH list: one record per polyline vertex, one per unique mesh edge), the records as
+// float positions: 2D a, b, c, flag (8 floats; flag 1 = both neighbours exist,
+// silhouette_vertex.py:48), 3D a, b, c, d, flag (16 floats; flag 1 = boundary edge,
+// always a silhouette, silhouette_edge.py:56-57).  The silhouette conditions of
+// silhouette_vertex.py:27-28 and silhouette_edge.py:7-12 in double: the face normals
+// are left unnormalised (the sign test does not depend on their length).  The first
+// strictly nearest silhouette in list order is kept.
+template <int D>
+__global__ void __launch_bounds__(kBlock) k_sil_f64(const float *recs, int64_t n_sil, gq_vecs qx, int64_t n,
+                                                    double *out_d, int32_t *out_id) {
+    constexpr int W = (D == 3) ? 16 : 8;
+    __shared__ double tile[kTile][W];
+    const int64_t qi = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const bool active = qi < n;
+    double x[D] = {};
+    if (active)
+        for (int k = 0; k < D; ++k) x[k] = qget(qx, qi, k);
+    double best = INFINITY;
+    int64_t bid = -1;
+    for (int64_t base = 0; base < n_sil; base += kTile) {
+        __syncthreads();
+        for (int t = threadIdx.x; t < kTile * W; t += blockDim.x) {
+            const int64_t f = base + t / W;
+            tile[t / W][t % W] = f < n_sil ? (double)recs[base * W + t] : 0.0;
+        }
+        __syncthreads();
+        const int lim = (int)min((int64_t)kTile, n_sil - base);
+        if (!active) continue;
+        for (int t = 0; t < lim; ++t) {
+            const double *r = tile[t];
+            double d;
+            bool sil;
+            if (D == 3) {
+                const double ux = r[3] - r[0], uy = r[4] - r[1], uz = r[5] - r[2];
+                const double uu = ux * ux + uy * uy + uz * uz;
+                double tt = uu > 0 ? ((x[0] - r[0]) * ux + (x[1] - r[1]) * uy + (x[D - 1] - r[2]) * uz) / uu : 0.0;
+                tt = tt < 0 ? 0 : (tt > 1 ? 1 : tt);
+                const double wx = r[0] + tt * ux - x[0], wy = r[1] + tt * uy - x[1], wz = r[2] + tt * uz - x[D - 1];
+                d = sqrt(wx * wx + wy * wy + wz * wz);
+                if (!(d < best)) continue;
+                // n0 = (b - a) x (c - a), n1 = (d - a) x (b - a)
+                const double cx = r[6] - r[0], cy = r[7] - r[1], cz = r[8] - r[2];
+                const double ex = r[9] - r[0], ey = r[10] - r[1], ez = r[11] - r[2];
+                const double n0x = uy * cz - uz * cy, n0y = uz * cx - ux * cz, n0z = ux * cy - uy * cx;
+                const double n1x = ey * uz - ez * uy, n1y = ez * ux - ex * uz, n1z = ex * uy - ey * ux;
+                sil = (r[12] != 0.0) ||
+                      ((wx * n0x + wy * n0y + wz * n0z) * (wx * n1x + wy * n1y + wz * n1z) < 0.0);
+            } else {
+                const double bx = r[2] - x[0], by = r[3] - x[D - 1];
+                d = sqrt(bx * bx + by * by);
+                if (!(d < best) || r[6] == 0.0) continue;
+                // cross(b - a, x - a) * cross(c - b, x - b) < 0
+                const double c0 = (r[2] - r[0]) * (x[D - 1] - r[1]) - (r[3] - r[1]) * (x[0] - r[0]);
+                const double c1 = (r[4] - r[2]) * (x[D - 1] - r[3]) - (r[5] - r[3]) * (x[0] - r[2]);
+                sil = c0 * c1 < 0.0;
+            }
+            if (sil) {
+                best = d;
+                bid = base + t;
+            }
+        }
+    }
+    if (active) {
+        out_d[qi] = best;
+        out_id[qi] = (int32_t)bid;
+    }
+}
+
 // ===========================================================================
 // Morton reordering
 // ===========================================================================
@@ -675,6 +744,16 @@ cudaError_t launch_sil_brute(const DevScene &s, const void *sils, int64_t n_sil,
         k_sil_brute<3><<<grid_for(n), kBlock, 0, st>>>(b, n_sil, x, r_max, n, o);
     else
         k_sil_brute<2><<<grid_for(n), kBlock, 0, st>>>(b, n_sil, x, r_max, n, o);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sil_f64(int dim, const float *recs, int64_t n_sil, gq_vecs x, int64_t n, double *out_d,
+                           int32_t *out_id, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    if (dim == 3)
+        k_sil_f64<3><<<grid_for(n), kBlock, 0, st>>>(recs, n_sil, x, n, out_d, out_id);
+    else
+        k_sil_f64<2><<<grid_for(n), kBlock, 0, st>>>(recs, n_sil, x, n, out_d, out_id);
     return cudaGetLastError();
 }
 

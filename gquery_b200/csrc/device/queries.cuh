@@ -26,6 +26,8 @@ struct DevScene {
     int64_t n_prims;
     float coord_bound;   // largest |coordinate| of any vertex
     int32_t *err;        // device error word
+    int32_t stack_cap = 1 << 30;  // entries a traversal stack may hold (the compiled sizes when larger); a walk
+                                  // that needs more stops, its query is a miss and GQ_DEVERR_STACK is raised
 };
 
 #define GQ_DEVERR_STACK 1
@@ -71,6 +73,9 @@ cudaError_t launch_sil_brute(const DevScene &s, const void *sils, int64_t n_sil,
                              int64_t n, const gq_sil_out &o, cudaStream_t st);
 cudaError_t launch_ray_brute(const DevScene &s, gq_vecs x, gq_vecs v, const float *r_max, int64_t n,
                              const gq_ray_out &o, cudaStream_t st);
+// FP64 nearest silhouette over raw records (2D: 8 floats, 3D: 16 floats each).
+cudaError_t launch_sil_f64(int dim, const float *recs, int64_t n_sil, gq_vecs x, int64_t n, double *out_d,
+                           int32_t *out_id, cudaStream_t st);
 cudaError_t launch_brute_f64(const DevScene &s, int kind, gq_vecs a, gq_vecs b, int64_t n, double *out_d,
                              int32_t *out_id, cudaStream_t st);
 

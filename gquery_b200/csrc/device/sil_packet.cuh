@@ -111,7 +111,7 @@ __device__ __forceinline__ void closest_silhouette(const DevScene &s, unsigned m
         if (m0 && m1) {
             const float k0 = warp_min(hit[0] ? dm[0] : kInf), k1 = warp_min(hit[1] ? dm[1] : kInf);
             const bool second_first = k1 < k0;  // the nearer child (over the lanes) is entered first
-            if (sp + 1 >= GQ_STACK_EXACT) {
+            if (sp + 1 >= min(GQ_STACK_EXACT, s.stack_cap)) {
                 ovf = true;
                 break;
             }

@@ -214,7 +214,7 @@ __device__ __forceinline__ void visit_interior(const DevScene &s, Lane<D> &L, in
             hit[c] = cone_overlaps<D>(P.lo[c], P.hi[c], P.ax[c], P.half[c], P.rad[c], L.x, dm[c]);
     }
     if (hit[0] & hit[1]) {
-        if (L.sp + 2 >= GQ_STACK_EXACT) {
+        if (L.sp + 2 >= min(GQ_STACK_EXACT, s.stack_cap)) {
             L.ovf = true;
             L.sp = -1;
             L.j = -1;

@@ -230,7 +230,7 @@ __device__ __forceinline__ void visit_pair(const DevScene &s, Lane<D, RAY, false
     // The reference pushes (other, closer) and pops `closer` at once under
     // dist <= r_max; here `closer` continues directly under the same test.
     if (h0 & h1) {
-        if (L.sp + 1 >= GQ_STACK_EXACT) {
+        if (L.sp + 1 >= min(GQ_STACK_EXACT, s.stack_cap)) {
             L.ovf = true;
             L.cur = kNone;
             L.sp = -1;
@@ -325,7 +325,7 @@ __device__ __forceinline__ void visit_wide(const DevScene &s, Lane<D, RAY, true>
         L.cur = kNone;
         return;
     }
-    if (L.sp + cnt > GQ_STACK_WIDE) {
+    if (L.sp + cnt > min(GQ_STACK_WIDE, s.stack_cap)) {
         L.ovf = true;
         L.cur = kNone;
         L.sp = -1;

@@ -67,6 +67,9 @@ struct gq_scene {
     const void *base_sils = nullptr;
     int64_t n_base_sils = -1;
     std::mutex base_mu;
+    // the SNCH's raw silhouette list as float positions for the FP64 scan, uploaded on first use
+    const void *f64_sils = nullptr;
+    int64_t n_f64_sils = -1;
 
     ~gq_scene() {
         if (device < 0 || allocs.empty()) return;

@@ -668,6 +668,7 @@ gq_status gq_server_get_stats(gq_server *s, gq_server_stats *st) {
     st->device_bytes = s->ring_bytes;
     if (s->outstanding.load() == 0) {  // error words are read only while nothing runs
         DeviceGuard g(s->device);
+        if (!g.ok) return fail(GQ_ERR_CUDA, "cannot select the server's CUDA device");
         int32_t all = 0;
         for (Slot &S : s->slots) {
             int32_t v = 0;

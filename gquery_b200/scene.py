@@ -314,16 +314,22 @@ class Scene:
         return rec
 
     def brute_f64(self, kind: str, a, b=None, *, stream=None):
-        """FP64 brute force: (distance or ray parameter [float64], primitive id [int32])."""
+        """FP64 brute force, kind "cp" / "ray" / "sil": (distance, ray parameter or silhouette
+        distance [float64, +inf when none], primitive or silhouette record id [int32])."""
         ta, n, va = self._points(a)
         vb = L.Vecs(None, 0, 0)
         if kind == "ray":
             tb, _, vb = self._points(b)
         d = torch.empty(n, dtype=torch.float64, device=self.torch_device)
         idx = torch.empty(n, dtype=torch.int32, device=self.torch_device)
-        L.check(L.lib().gq_brute_f64(self._h, 0 if kind == "cp" else 1, va, vb, n, d.data_ptr(), idx.data_ptr(),
+        L.check(L.lib().gq_brute_f64(self._h, {"cp": 0, "ray": 1, "sil": 2}[kind], va, vb, n, d.data_ptr(), idx.data_ptr(),
                                      _stream_handle(stream)))
         return d, idx
+
+    def set_stack_limit(self, entries: int) -> None:
+        """Caps the traversal stacks at `entries` (0: the compiled sizes).  Queries whose
+        walk needs more come back as misses and raise the stack bit of device_error()."""
+        L.check(L.lib().gq_scene_set_stack_limit(self._h, int(entries)))
 
     def device_error(self, stream=None) -> int:
         v = C.c_int32()

@@ -205,16 +205,20 @@ gq_status gq_closest_point(const gq_scene *scene, gq_vecs q, int64_t n, const gq
                            const gq_query_opts *opts, void *stream);
 
 /* Closest point without any device allocation.  No counterpart in the reference: for
- * callers that cannot allocate device memory while querying (a CUDA graph recorded with
- * a cudaMalloc-based allocator, a plugin whose host owns all device memory, a real-time
- * loop that must not enter an allocator).  The per-call scratch (work counter and
+ * callers that cannot allocate device memory while querying (a plugin whose host
+ * application owns every device allocation and hands it only input and output buffers,
+ * a real-time loop that must not enter an allocator, since cudaMalloc may synchronise the
+ * device and take unbounded time).  The per-call scratch (work counter and
  * Morton-sort buffers) comes from a fixed device array inside the library, which every
  * device that loads the library holds until the process exits; hence at most
  * gq_noalloc_max_queries() queries per call (larger n is rejected with GQ_ERR_INVALID).
  * Same answers as gq_closest_point with the same variant and sort flag.  All calls on a
  * device share that array: calls whose kernels may overlap on the GPU race and must be
  * ordered by the caller (one stream, or events).  The first call on a device looks up
- * the array's device address; make that first call before any stream capture. */
+ * the array's device address; make that first call before any stream capture.  The
+ * address is kept for the process's primary context of each device: call this entry
+ * point from the primary context only, and not after cudaDeviceReset (which frees the
+ * array the kept address points to). */
 int64_t gq_noalloc_max_queries(void);
 gq_status gq_closest_point_noalloc(const gq_scene *scene, gq_vecs q, int64_t n, const gq_cp_out *out,
                                    int32_t variant, int32_t sort, void *stream);
@@ -243,12 +247,24 @@ gq_status gq_closest_silhouette_brute(const gq_scene *scene, gq_vecs x, const fl
                                       const gq_sil_out *out, void *stream);
 
 /* FP64 brute force used to state the error of the FP32 paths: nearest distance
- * (closest point) or nearest ray parameter (+inf on a miss) and its primitive. */
-gq_status gq_brute_f64(const gq_scene *scene, int32_t kind /*0 closest point, 1 ray*/, gq_vecs a, gq_vecs b,
-                       int64_t n, double *out_d, int32_t *out_id, void *stream);
+ * (closest point), nearest ray parameter (ray) or nearest silhouette distance (silhouette,
+ * over the SNCH's raw silhouette list; host-built scenes with build_snch), +inf when there
+ * is none, and the primitive (silhouette record) it belongs to (-1 when none).  b: ray
+ * directions (kind 1 only). */
+gq_status gq_brute_f64(const gq_scene *scene, int32_t kind /*0 closest point, 1 ray, 2 silhouette*/, gq_vecs a,
+                       gq_vecs b, int64_t n, double *out_d, int32_t *out_id, void *stream);
 
 /* Reads and clears the scene's device error word (stack overflow etc.); synchronises `stream`. */
 gq_status gq_scene_device_error(const gq_scene *scene, void *stream, int32_t *flags);
+
+/* Caps the entries of this scene's traversal stacks below their compiled sizes (64 binary,
+ * 96 wide / warp-coherent); 0 restores the compiled sizes.  A walk that would push past the
+ * cap stops: its query comes back as a zeroed miss and GQ_DEVERR_STACK (bit 0) is raised in
+ * the scene's device error word.  For bounding per-thread stack memory on trees known to be
+ * shallow, and for exercising the overflow path.  Batches and servers copy the cap when they
+ * are created.  No counterpart in the reference, whose 64-entry stack (bvh.py:132) has no
+ * overflow check. */
+gq_status gq_scene_set_stack_limit(gq_scene *scene, int32_t entries);
 
 /* ---- batches: many scenes, all three query kinds, one launch ----
  * No counterpart in the reference, which answers one scene and one query kind per call

@@ -75,7 +75,7 @@ def _split(dim, kind, f, i):
 _KF = {("cp", 2): 6, ("cp", 3): 9, ("ray", 2): 6, ("ray", 3): 9, ("sil", 2): 3, ("sil", 3): 4}
 
 
-def _run(name, kind, dim, args, nq, counts, threads):
+def _run(name, kind, dim, args, nq, counts, threads, with_counts=True):
     f = np.zeros((nq, _KF[(kind, dim)]), np.float32)
     i = np.zeros((nq, 3), np.int32)
     cnt = np.zeros((nq, 2), np.int32) if counts else None
@@ -89,8 +89,8 @@ def _run(name, kind, dim, args, nq, counts, threads):
             cargs.append(C.c_void_p(a.ctypes.data))
         else:
             cargs.append(C.c_int64(a))
-    fn(*cargs, C.c_void_p(f.ctypes.data), C.c_void_p(i.ctypes.data),
-       C.c_void_p(cnt.ctypes.data) if counts else C.c_void_p(None), C.c_int(threads or n_threads()))
+    tail = [C.c_void_p(cnt.ctypes.data) if counts else C.c_void_p(None)] if with_counts else []
+    fn(*cargs, C.c_void_p(f.ctypes.data), C.c_void_p(i.ctypes.data), *tail, C.c_int(threads or n_threads()))
     out = _split(dim, kind, f, i)
     if counts:
         out["interior"] = cnt[:, 0].copy()
@@ -118,6 +118,29 @@ def closest_silhouette(dim, snch_nodes, silhouettes, x, r_max=None, counts=False
     x = _f(x).reshape(-1, dim)
     rm = None if r_max is None else _f(np.broadcast_to(np.asarray(r_max, np.float32), (x.shape[0],)))
     return _run(f"orc_sil{dim}d", "sil", dim, [nodes, sils, x, rm, x.shape[0]], x.shape[0], counts, threads)
+
+
+def _raw(dim, verts, index):
+    return _f(verts).reshape(-1, dim), np.ascontiguousarray(index, np.int32).reshape(-1, dim)
+
+
+def closest_point_baseline(dim, verts, index, q, threads=0):
+    """closest_point_baseline (polyline.py:175-209, mesh.py:91-117) in FP32: the first
+    strictly nearest primitive of the raw list, its record as the traversals'."""
+    verts, index = _raw(dim, verts, index)
+    q = _f(q).reshape(-1, dim)
+    return _run(f"orc_cp_brute{dim}d", "cp", dim, [verts, index, index.shape[0], q, q.shape[0]], q.shape[0], False,
+                threads, with_counts=False)
+
+
+def intersect_baseline(dim, verts, index, x, v, r_max=None, threads=0):
+    """intersect_baseline (polyline.py:137-169, mesh.py:60-84) in FP32: the first
+    strictly nearest hit within r_max; on_boundary is set on every hit."""
+    verts, index = _raw(dim, verts, index)
+    x, v = _f(x).reshape(-1, dim), _f(v).reshape(-1, dim)
+    rm = None if r_max is None else _f(np.broadcast_to(np.asarray(r_max, np.float32), (x.shape[0],)))
+    return _run(f"orc_ray_brute{dim}d", "ray", dim, [verts, index, index.shape[0], x, v, rm, x.shape[0]], x.shape[0],
+                False, threads, with_counts=False)
 
 
 def brute_closest_point(dim, verts, index, q, threads=0):

@@ -866,6 +866,154 @@ static double d_cp_triangle(D3 p, D3 a, D3 b, D3 c) {
     return dist(D3{a.x + ab.x * v + ac.x * w, a.y + ab.y * v + ac.y * w, a.z + ab.z * v + ac.z * w});
 }
 
+// ---- FP32 brute force: the reference's *_baseline scans over the raw primitives ----
+// Records are written in the row layout of the traversals (Out.kf floats, 3 ints);
+// a scan that keeps no primitive leaves the zeroed record.
+static inline V2 vtx2(const float *V, const int32_t *E, int64_t e, int k) {
+    const int64_t i = E[2 * e + k];
+    return V2{V[2 * i], V[2 * i + 1]};
+}
+static inline V3 vtx3(const float *V, const int32_t *F, int64_t f, int k) {
+    const int64_t i = F[3 * f + k];
+    return V3{V[3 * i], V[3 * i + 1], V[3 * i + 2]};
+}
+
+// Polyline.closest_point_baseline, polyline.py:175-209
+static void cp_brute2d_one(const float *V, const int32_t *E, int64_t ne, V2 p, Out o, int64_t q) {
+    float d_min = INF;
+    int64_t idx = -1;
+    for (int64_t i = 0; i < ne; ++i) {
+        const V2 a = vtx2(V, E, i, 0), b = vtx2(V, E, i, 1);
+        const V2 pa = sub(p, a), ba = sub(b, a);
+        const float h = gq_clamp(gq_div(dot(pa, ba), dot(ba, ba)), 0.f, 1.f);
+        const float d = norm(sub(pa, mul(ba, h)));
+        if (d < d_min) {
+            d_min = d;
+            idx = i;
+        }
+    }
+    float *f = o.f + q * o.kf;
+    int32_t *ii = o.i + q * 3;
+    memset(f, 0, sizeof(float) * o.kf);
+    ii[0] = ii[1] = ii[2] = 0;
+    if (idx == -1) return;
+    const V2 a = vtx2(V, E, idx, 0), b = vtx2(V, E, idx, 1);
+    const V2 pa = sub(p, a), ba = sub(b, a);
+    const float h = gq_clamp(gq_div(dot(pa, ba), dot(ba, ba)), 0.f, 1.f);  // dr.clip
+    const V2 n = normalize(V2{ba.y, -ba.x});
+    f[0] = gq_lerp(a.x, b.x, h);
+    f[1] = gq_lerp(a.y, b.y, h);
+    f[2] = n.x;
+    f[3] = n.y;
+    f[4] = h;
+    f[5] = d_min;
+    ii[0] = 1;
+    ii[1] = (int32_t)idx;
+}
+
+// Mesh.closest_point_baseline, mesh.py:91-117; the normal is the face normal of
+// Mesh.configure_normal (mesh.py:35-40), normalize(cross(b - a, c - a)).
+static void cp_brute3d_one(const float *V, const int32_t *F, int64_t nf, V3 x, Out o, int64_t q) {
+    float d_min = INF;
+    int64_t idx = -1;
+    for (int64_t i = 0; i < nf; ++i) {
+        const float d = cp_triangle(x, vtx3(V, F, i, 0), vtx3(V, F, i, 1), vtx3(V, F, i, 2), nullptr, nullptr, nullptr);
+        if (d < d_min) {
+            d_min = d;
+            idx = i;
+        }
+    }
+    float *f = o.f + q * o.kf;
+    int32_t *ii = o.i + q * 3;
+    memset(f, 0, sizeof(float) * o.kf);
+    ii[0] = ii[1] = ii[2] = 0;
+    if (idx == -1) return;
+    const V3 a = vtx3(V, F, idx, 0), b = vtx3(V, F, idx, 1), c = vtx3(V, F, idx, 2);
+    V3 pt;
+    float u, v;
+    cp_triangle(x, a, b, c, &pt, &u, &v);
+    const V3 n = normalize(cross(sub(b, a), sub(c, a)));
+    f[0] = pt.x, f[1] = pt.y, f[2] = pt.z;
+    f[3] = n.x, f[4] = n.y, f[5] = n.z;
+    f[6] = u, f[7] = v;
+    f[8] = d_min;
+    ii[0] = 1;
+    ii[1] = (int32_t)idx;
+}
+
+// Polyline.intersect_baseline, polyline.py:137-169: d_min starts at r_max, the first
+// strictly nearest hit is kept; the record has p = x + v d, t = -1, on_boundary set.
+static void ray_brute2d_one(const float *V, const int32_t *E, int64_t ne, V2 x, V2 v, float r_max, Out o, int64_t q) {
+    float d_min = r_max;
+    int64_t idx = -1;
+    for (int64_t i = 0; i < ne; ++i) {
+        const float d = ray_segment(x, v, vtx2(V, E, i, 0), vtx2(V, E, i, 1));
+        if (d < d_min) {
+            d_min = d;
+            idx = i;
+        }
+    }
+    float *f = o.f + q * o.kf;
+    int32_t *ii = o.i + q * 3;
+    memset(f, 0, sizeof(float) * o.kf);
+    ii[0] = ii[1] = ii[2] = 0;
+    if (idx == -1) return;
+    const V2 a = vtx2(V, E, idx, 0), b = vtx2(V, E, idx, 1);
+    const V2 ab = normalize(sub(b, a));
+    const V2 p = add(x, mul(v, d_min));
+    f[0] = p.x, f[1] = p.y;
+    f[2] = ab.y, f[3] = -ab.x;
+    f[4] = -1.f;
+    f[5] = d_min;
+    ii[0] = 1;
+    ii[1] = (int32_t)idx;
+    ii[2] = 1;
+}
+
+// Triangle.ray_intersect, triangle.py:48-73: whether the ray hits within [0, r_max],
+// with the barycentric v, w and the parameter t of the hit.
+static inline bool tri_hit(V3 x, V3 d, V3 a, V3 b, V3 c, float r_max, float *t, float *v, float *w) {
+    float vv = NAN, ww = 0.f;
+    const float tt = ray_triangle(x, d, a, b, c, r_max, &vv, &ww);
+    if (vv != vv) return false;
+    *t = tt, *v = vv, *w = ww;
+    return true;
+}
+
+// Mesh.intersect_baseline, mesh.py:60-84: every triangle is tested against the
+// caller's r_max, a hit is kept when nearer than the best so far, and the record is
+// the kept triangle's ray_intersect at the caller's r_max again.
+static void ray_brute3d_one(const float *V, const int32_t *F, int64_t nf, V3 x, V3 dir, float r_max, Out o,
+                            int64_t q) {
+    float d_min = r_max;
+    int64_t idx = -1;
+    for (int64_t i = 0; i < nf; ++i) {
+        float t, v, w;
+        if (tri_hit(x, dir, vtx3(V, F, i, 0), vtx3(V, F, i, 1), vtx3(V, F, i, 2), r_max, &t, &v, &w) && t < d_min) {
+            idx = i;
+            d_min = t;
+        }
+    }
+    float *f = o.f + q * o.kf;
+    int32_t *ii = o.i + q * 3;
+    memset(f, 0, sizeof(float) * o.kf);
+    ii[0] = ii[1] = ii[2] = 0;
+    if (idx == -1) return;
+    const V3 a = vtx3(V, F, idx, 0), b = vtx3(V, F, idx, 1), c = vtx3(V, F, idx, 2);
+    float t, v, w;
+    if (!tri_hit(x, dir, a, b, c, r_max, &t, &v, &w)) return;
+    const V3 v1 = sub(b, a), v2 = sub(c, a);
+    const V3 p = add(add(a, mul(v1, v)), mul(v2, w));
+    const V3 n = normalize(cross(v1, v2));
+    f[0] = p.x, f[1] = p.y, f[2] = p.z;
+    f[3] = n.x, f[4] = n.y, f[5] = n.z;
+    f[6] = 1.f - v - w, f[7] = v;
+    f[8] = t;
+    ii[0] = 1;
+    ii[1] = (int32_t)idx;
+    ii[2] = 1;
+}
+
 }  // namespace
 
 // closest_silhouette_baseline (mesh.py:124-135, polyline.py:212-223): the shape's
@@ -1005,6 +1153,37 @@ void orc_sil_brute3d(const float *S, int64_t n_sil, const float *x, const float 
                      int32_t *i_out, int nthreads) {
     Out o{f_out, i_out, nullptr, 4};
     parallel_for(nq, nthreads, [&](int64_t i) { sil_brute_one<3>(S, n_sil, x + 3 * i, rmax ? rmax[i] : INF, o, i); });
+}
+
+// FP32 *_baseline scans over the raw primitives (verts [nv][D], idx [np][D]), records in
+// the traversal row layout.  rmax: nullable (+inf).
+void orc_cp_brute2d(const float *verts, const int32_t *idx, int64_t np, const float *q, int64_t nq, float *f_out,
+                    int32_t *i_out, int nthreads) {
+    Out o{f_out, i_out, nullptr, 6};
+    parallel_for(nq, nthreads, [&](int64_t i) { cp_brute2d_one(verts, idx, np, V2{q[2 * i], q[2 * i + 1]}, o, i); });
+}
+void orc_cp_brute3d(const float *verts, const int32_t *idx, int64_t np, const float *q, int64_t nq, float *f_out,
+                    int32_t *i_out, int nthreads) {
+    Out o{f_out, i_out, nullptr, 9};
+    parallel_for(nq, nthreads, [&](int64_t i) {
+        cp_brute3d_one(verts, idx, np, V3{q[3 * i], q[3 * i + 1], q[3 * i + 2]}, o, i);
+    });
+}
+void orc_ray_brute2d(const float *verts, const int32_t *idx, int64_t np, const float *x, const float *v,
+                     const float *rmax, int64_t nq, float *f_out, int32_t *i_out, int nthreads) {
+    Out o{f_out, i_out, nullptr, 6};
+    parallel_for(nq, nthreads, [&](int64_t i) {
+        ray_brute2d_one(verts, idx, np, V2{x[2 * i], x[2 * i + 1]}, V2{v[2 * i], v[2 * i + 1]}, rmax ? rmax[i] : INF,
+                        o, i);
+    });
+}
+void orc_ray_brute3d(const float *verts, const int32_t *idx, int64_t np, const float *x, const float *v,
+                     const float *rmax, int64_t nq, float *f_out, int32_t *i_out, int nthreads) {
+    Out o{f_out, i_out, nullptr, 9};
+    parallel_for(nq, nthreads, [&](int64_t i) {
+        ray_brute3d_one(verts, idx, np, V3{x[3 * i], x[3 * i + 1], x[3 * i + 2]},
+                        V3{v[3 * i], v[3 * i + 1], v[3 * i + 2]}, rmax ? rmax[i] : INF, o, i);
+    });
 }
 
 // FP64 brute force over the raw (unordered) primitives.  verts [nv][D], idx [np][D].

@@ -251,6 +251,13 @@ def arange(T, n):
 
 
 def gather(T, data, idx):
+    if isinstance(T, type) and issubclass(T, ArrayN):
+        if isinstance(data, ArrayN):  # SoA source: one gather per component
+            return T(*[gather(T.ELEM, c, idx) for c in data.c])
+        # flat source: element k of item i sits at N * i + k
+        i = np.asarray(_v(idx))
+        flat = np.asarray(data.v)
+        return T(*[T.ELEM(flat[T.N * i + k]) for k in range(T.N)])
     return T(np.asarray(data.v)[np.asarray(_v(idx))])
 
 

@@ -7,12 +7,15 @@ available).  What this pins: the traversal control flow, pruning and tie rules o
 reference, statement for statement.  What it cannot pin: DrJit's own rounding (the
 stand-in applies this project's fixed rules, the same as the kernels and the oracle).
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py <gQuery checkout>      (or GQ_REFERENCE=<checkout>)
 
-Writes golden_<case>.npz: scene, queries and the reference's record fields.
+Writes golden_<case>.npz: scene, queries and the reference's record fields, and
+baseline_<case>.npz: the records of the reference's brute-force methods
+(Polyline/Mesh closest_point_baseline and intersect_baseline, Polyline.intersect).
 """
 from __future__ import annotations
 
+import os
 import sys
 import types
 from pathlib import Path
@@ -21,7 +24,10 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent.parent
-REF = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+_ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GQ_REFERENCE")
+if not _ref:
+    sys.exit("usage: make_golden.py <path of a gQuery checkout>  (or set GQ_REFERENCE)")
+REF = Path(_ref)
 sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(HERE))
 
@@ -105,7 +111,78 @@ def case_3d(name, v, f, q, o, d, rmax_sil):
     print(name, "cp valid", cp["valid"].mean(), "ray valid", ray["valid"].mean(), "sil valid", sil["valid"].mean())
 
 
+def baseline_2d(name, v, e, q, o, d, rmax, nrm, onb):
+    """The reference's Polyline brute-force methods on a Polyline whose flat vertex and
+    index buffers are set as Polyline.__init__ sets them (polyline.py:20-33); the
+    constructor itself is not run (it would build trees through the nanobind module)."""
+    from drjit_scalar import Bool, Int
+    from gquery.shapes.polyline import Polyline
+    pl = object.__new__(Polyline)
+    pl._vertices = Float(np.ascontiguousarray(v, np.float32).reshape(-1))
+    pl._indices = Int(np.ascontiguousarray(e, np.int32).reshape(-1))
+    cp = run(pl.closest_point_baseline, [(vec(p),) for p in q], ["valid", "p", "n", "t", "d", "prim_id"])
+    fields = ["valid", "p", "n", "t", "d", "prim_id", "on_boundary"]
+    ray = run(pl.intersect_baseline, [(vec(a), vec(b), Float(r)) for a, b, r in zip(o, d, rmax)], fields)
+    off = run(pl.intersect, [(vec(a), vec(b), vec(n), Bool(bool(ob)), Float(r))
+                             for a, b, n, ob, r in zip(o, d, nrm, onb, rmax)], fields)
+    np.savez_compressed(HERE / f"baseline_{name}.npz", dim=2, vertices=v, indices=e, q=q, o=o, d=d, rmax=rmax,
+                        n=nrm, on_boundary=onb, **{f"cp_{k}": x for k, x in cp.items()},
+                        **{f"ray_{k}": x for k, x in ray.items()}, **{f"off_{k}": x for k, x in off.items()})
+    print("baseline", name, "cp valid", cp["valid"].mean(), "ray valid", ray["valid"].mean())
+
+
+def baseline_3d(name, v, f, q, o, d, rmax):
+    """The reference's Mesh brute-force methods on a Mesh holding the vertex and index
+    arrays and the face normals of Mesh.configure_normal (mesh.py:35-40), computed face by
+    face with the same operations; the constructor itself is not run."""
+    from drjit_scalar import Array3i
+    from gquery.shapes.mesh import Mesh
+    m = object.__new__(Mesh)
+    m.vertices = soa(v, Array3)
+    m.indices = soa(f, Array3i)
+    fn = []
+    for tri in f:
+        a, b, c = (vec(v[k]) for k in tri)
+        fn.append(dr.normalize(dr.cross(b - a, c - a)).numpy())
+    m.face_normals = soa(np.stack(fn).astype(np.float32), Array3)
+    cp = run(m.closest_point_baseline, [(vec(p),) for p in q], ["valid", "p", "n", "uv", "d", "prim_id"])
+    ray = run(m.intersect_baseline, [(vec(a), vec(b), Float(r)) for a, b, r in zip(o, d, rmax)],
+              ["valid", "p", "n", "uv", "d", "prim_id", "on_boundary"])
+    np.savez_compressed(HERE / f"baseline_{name}.npz", dim=3, vertices=v, indices=f, q=q, o=o, d=d, rmax=rmax,
+                        **{f"cp_{k}": x for k, x in cp.items()}, **{f"ray_{k}": x for k, x in ray.items()})
+    print("baseline", name, "cp valid", cp["valid"].mean(), "ray valid", ray["valid"].mean())
+
+
+def _rmax(n, seed):
+    """+inf for even queries, a finite radius in [0.2, 2] for odd ones."""
+    r = np.random.default_rng(seed).uniform(0.2, 2.0, n).astype(np.float32)
+    r[0::2] = np.inf
+    return r
+
+
+def baselines():
+    pv = np.array([[0.0, 0.0], [1.0, 0.0], [1.5, 1.0], [0.5, 1.5], [-0.5, 1.0]], np.float32)
+    pe = np.array([[0, 1], [1, 2], [2, 3], [3, 4], [4, 0]], np.int32)
+    for name, (v, e) in (("pentagon", (pv, pe)), ("star300", W.star_polyline(300, seed=7))):
+        q = W.uniform_points(96, 2, seed=601)
+        o, d = W.rays(96, 2, seed=602)
+        rng = np.random.default_rng(603)
+        ang = rng.uniform(0, 2 * np.pi, 96)
+        nrm = np.stack([np.cos(ang), np.sin(ang)], 1).astype(np.float32)
+        onb = rng.random(96) < 0.5
+        baseline_2d(name, v, e, q, o, d, _rmax(96, 604), nrm, onb)
+    tv = np.array([[0, 0, 0], [1, 0, 0], [0.5, 1, 0], [0.5, 0.5, 1]], np.float32)
+    tf = np.array([[0, 1, 2], [0, 1, 3], [1, 2, 3], [0, 2, 3]], np.int32)
+    for name, (v, f) in (("tetrahedron", (tv, tf)), ("icosphere2", W.icosphere(2, amplitude=0.3, seed=11))):
+        q = W.uniform_points(96, 3, seed=605)
+        o, d = W.rays(96, 3, seed=606)
+        baseline_3d(name, v, f, q, o, d, _rmax(96, 607))
+
+
 def main():
+    if "--baselines-only" in sys.argv:
+        baselines()
+        return
     # README pentagon (examples/example_2d.py) and tetrahedron (examples/example_3d.py)
     pv = np.array([[0.0, 0.0], [1.0, 0.0], [1.5, 1.0], [0.5, 1.5], [-0.5, 1.0]], np.float32)
     pe = np.array([[0, 1], [1, 2], [2, 3], [3, 4], [4, 0]], np.int32)
@@ -132,6 +209,7 @@ def main():
     q = W.uniform_points(200, 3, seed=507)
     o, d = W.rays(300, 3, seed=508)
     case_3d("icosphere2", iv, iff, q, o, d, np.inf)
+    baselines()
 
 
 if __name__ == "__main__":

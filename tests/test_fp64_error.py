@@ -4,6 +4,7 @@ FP32 traversal is the measured side (the exact GPU kernels equal it bit for bit)
 FP64 side is a numpy scan over every primitive or silhouette.  Closest points and 3D rays
 are measured the same way in test_oracle_kat.py and test_gpu_parity.py."""
 import numpy as np
+import pytest
 
 import oracle
 from gquery_b200 import gquery_ext as gx
@@ -122,3 +123,33 @@ def test_sil3d_error_vs_fp64():
     # few queries end on a farther one (err > 0), never on a nearer one
     assert err.min() > -ABS_TOL, err.min()
     assert np.mean(np.abs(err) <= ABS_TOL) > 0.99, np.sort(err)[-5:]
+
+
+# ---------------------------------------------------------------- the GPU FP64 silhouette scan
+
+@pytest.mark.gpu
+def test_gpu_fp64_silhouette_scan_matches_numpy():
+    """gq_brute_f64 kind 2 (the FP64 silhouette reference the bench uses at full size)
+    against the numpy FP64 scans above on the same raw silhouette lists."""
+    from gquery_b200 import _lib as L
+    from gquery_b200.scene import Scene
+    v, e = W.star_polyline(2000, seed=4)
+    s = Scene(v, e, 2, device=0)
+    x = W.uniform_points(3000, 2, seed=8)
+    d, ids = s.brute_f64("sil", x)
+    d = d.cpu().numpy()
+    d_np = _sil2d_fp64(v, e, x)
+    assert np.array_equal(np.isinf(d), np.isinf(d_np))
+    fin = np.isfinite(d_np)
+    assert np.allclose(d[fin], d_np[fin], rtol=1e-12, atol=0)
+    assert np.all(ids.cpu().numpy()[~fin] == -1)
+
+    v3, f3 = W.icosphere(3, amplitude=0.3, seed=3)
+    s3 = Scene(v3, f3, 3, device=0)
+    x3 = W.uniform_points(3000, 3, seed=12)
+    d3, _ = s3.brute_f64("sil", x3)
+    d3 = d3.cpu().numpy()
+    d3_np = _sil3d_fp64(_raw_f32_view(s3.ref_array(L.ARRAY_RAW_SILHOUETTES)), x3)
+    assert np.array_equal(np.isinf(d3), np.isinf(d3_np))
+    fin = np.isfinite(d3_np)
+    assert np.allclose(d3[fin], d3_np[fin], rtol=1e-12, atol=0)

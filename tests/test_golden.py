@@ -59,3 +59,51 @@ def test_exact_kernels_match_reference_traversal(path):
     assert_bitwise(to_np(s.intersect(z["o"], z["d"], variant="exact")), expected(z, "ray", RAY[dim]), RAY[dim],
                    "ray ")
     assert_bitwise(to_np(s.closest_silhouette(z["q"], rmax, variant="exact")), expected(z, "sil", SIL), SIL, "sil ")
+
+
+# ---------------------------------------------------------------- brute-force baselines
+
+BASELINES = sorted((Path(__file__).resolve().parent / "golden").glob("baseline_*.npz"))
+
+
+def _offset(z):
+    """Polyline.intersect's origin (polyline.py:124-130): x - 1e-5 n where on_boundary."""
+    return np.where(z["on_boundary"][:, None], z["o"] - np.float32(1e-5) * z["n"], z["o"]).astype(np.float32)
+
+
+def test_baseline_fixtures_exist():
+    names = {p.stem for p in BASELINES}
+    assert {"baseline_pentagon", "baseline_star300", "baseline_tetrahedron", "baseline_icosphere2"} <= names
+
+
+@pytest.mark.parametrize("path", BASELINES, ids=[p.stem for p in BASELINES])
+def test_oracle_matches_reference_baselines(path):
+    dim, z = load(path)
+    v, ix = z["vertices"], z["indices"]
+    assert_bitwise(oracle.closest_point_baseline(dim, v, ix, z["q"]), expected(z, "cp", CP[dim]), CP[dim], "cp ")
+    assert_bitwise(oracle.intersect_baseline(dim, v, ix, z["o"], z["d"], z["rmax"]), expected(z, "ray", RAY[dim]),
+                   RAY[dim], "ray ")
+    if dim == 2:
+        assert_bitwise(oracle.intersect_baseline(dim, v, ix, _offset(z), z["d"], z["rmax"]),
+                       expected(z, "off", RAY[dim]), RAY[dim], "offset ray ")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", BASELINES, ids=[p.stem for p in BASELINES])
+def test_brute_kernels_match_reference_baselines(path):
+    import torch
+    from gquery_b200.shapes import Mesh, Polyline
+    dim, z = load(path)
+    s = Scene(z["vertices"], z["indices"], dim, device=0, build_snch=False)
+    assert_bitwise(to_np(s.closest_point_brute(z["q"])), expected(z, "cp", CP[dim]), CP[dim], "cp ")
+    assert_bitwise(to_np(s.intersect_brute(z["o"], z["d"], torch.as_tensor(z["rmax"]))), expected(z, "ray", RAY[dim]),
+                   RAY[dim], "ray ")
+    shape = (Polyline if dim == 2 else Mesh)(torch.as_tensor(z["vertices"]), torch.as_tensor(z["indices"]))
+    assert_bitwise(to_np(shape.closest_point_baseline(torch.as_tensor(z["q"]).cuda())), expected(z, "cp", CP[dim]),
+                   CP[dim], "facade cp ")
+    assert_bitwise(to_np(shape.intersect_baseline(z["o"], z["d"], torch.as_tensor(z["rmax"]))),
+                   expected(z, "ray", RAY[dim]), RAY[dim], "facade ray ")
+    if dim == 2:
+        got = shape.intersect(torch.as_tensor(z["o"]).cuda(), z["d"], torch.as_tensor(z["n"]).cuda(),
+                              torch.as_tensor(z["on_boundary"]).cuda(), torch.as_tensor(z["rmax"]))
+        assert_bitwise(to_np(got), expected(z, "off", RAY[dim]), RAY[dim], "Polyline.intersect ")

@@ -1,7 +1,7 @@
 """gq_closest_point_noalloc: closest point without device allocation, for callers that
-cannot allocate while they query (graph capture with a cudaMalloc-based allocator, a
-host that owns all device memory, a real-time loop).  Its scratch is a fixed array in
-the library, shared by all calls on a device.
+cannot allocate while they query (a plugin whose host application owns all device
+memory, a real-time loop that must not enter an allocator).  Its scratch is a fixed
+array in the library, shared by all calls on a device.
 
 Checked through the C ABI against gq_closest_point on the same inputs, for two calls in
 a row (the second call must not see leftovers of the first), plus the size limit.
@@ -22,7 +22,7 @@ REL_TOL = 2e-6
 
 
 def _call_noalloc(scene, q, variant, sort):
-    t, n, cs, es = points_layout(q, 3)
+    t, n, cs, es = points_layout(q, scene.dim)
     rec = scene.alloc_cp(n)
     out = scene.cp_out_struct(rec)
     st = L.lib().gq_closest_point_noalloc(scene.handle, L.Vecs(t.data_ptr(), cs, es), n, C.byref(out), variant,
@@ -41,6 +41,19 @@ def scene():
     return Scene(v, f, 3, device=0, build_snch=False)
 
 
+@pytest.fixture(scope="module")
+def polyline():
+    v, e = W.star_polyline(4096, seed=0)
+    return Scene(v, e, 2, device=0, build_snch=False)
+
+
+def _compare(got, ref, fields):
+    assert np.array_equal(got["valid"], ref["valid"])
+    assert np.array_equal(got["prim_id"], ref["prim_id"])
+    for f in fields:
+        np.testing.assert_allclose(got[f], ref[f], rtol=REL_TOL, atol=0)
+
+
 @pytest.mark.parametrize("variant", [L.VARIANT_COHERENT, L.VARIANT_WIDE8, L.VARIANT_EXACT])
 def test_noalloc_matches_allocating_entry_point_twice(scene, variant):
     cap = L.lib().gq_noalloc_max_queries()
@@ -50,11 +63,21 @@ def test_noalloc_matches_allocating_entry_point_twice(scene, variant):
         q = torch.as_tensor(W.uniform_points(n, 3, seed=100 + call)).cuda()
         got = _np(_call_noalloc(scene, q, variant, sort=True))
         ref = _np(scene.closest_point(q, variant=name, sort=True))
-        assert np.array_equal(got["valid"], ref["valid"])
-        assert np.array_equal(got["prim_id"], ref["prim_id"])
-        for f in ("p", "n", "uv", "d"):
-            np.testing.assert_allclose(got[f], ref[f], rtol=REL_TOL, atol=0)
+        _compare(got, ref, ("p", "n", "uv", "d"))
     assert scene.device_error() == 0
+
+
+@pytest.mark.parametrize("sort", [False, True])
+@pytest.mark.parametrize("variant", [L.VARIANT_COHERENT, L.VARIANT_EXACT])
+def test_noalloc_polyline_sorted_and_unsorted(polyline, variant, sort):
+    cap = L.lib().gq_noalloc_max_queries()
+    name = {L.VARIANT_COHERENT: "coherent", L.VARIANT_EXACT: "exact"}[variant]
+    for call, n in enumerate((cap, 777)):
+        q = torch.as_tensor(W.uniform_points(n, 2, seed=200 + call)).cuda()
+        got = _np(_call_noalloc(polyline, q, variant, sort=sort))
+        ref = _np(polyline.closest_point(q, variant=name, sort=sort))
+        _compare(got, ref, ("p", "n", "t", "d"))
+    assert polyline.device_error() == 0
 
 
 def test_noalloc_rejects_oversized_batches(scene):
