@@ -432,7 +432,15 @@ SnchTree<D> build_snch(const PrimSource<D> &src, const BvhTree<D> &bvh, int n_th
         sn.n_sil = (int32_t)(out.ordered.size() - start);
     }
 
-    // Subtree extents: node i covers [i, end[i]) in preorder.
+    // The node range each cone is computed over, [i, end[i]) in preorder, as the
+    // reference's recursion passes it (snch.cpp:151-152): the root gets [0, n); an
+    // interior node's right child inherits the node's end, but its left child gets the
+    // node's RELATIVE second-child offset as its end.  That end is short of the left
+    // subtree's true end by the node's own index, so deeper left subtrees see a
+    // truncated range, or an empty one (end <= start): no silhouette is found there and
+    // the cone stays invalid (half angle -pi, which the traversal treats as "no cone
+    // test").  Kept as the reference builds it, so that node_data() and the traversal's
+    // pruning are the reference's.
     std::vector<uint32_t> end(nn);
     {
         std::vector<std::pair<uint32_t, uint32_t>> st;  // (node, end)
@@ -443,9 +451,9 @@ SnchTree<D> build_snch(const PrimSource<D> &src, const BvhTree<D> &bvh, int n_th
             end[i] = e;
             const FlatNode<D> &bn = bvh.nodes[i];
             if (bn.n_prims == 0) {
-                uint32_t r = i + (uint32_t)bn.second_child;
-                st.push_back({i + 1, r});
-                st.push_back({r, e});
+                const uint32_t off = (uint32_t)bn.second_child;
+                st.push_back({i + 1, off});
+                st.push_back({i + off, e});
             }
         }
     }

@@ -195,3 +195,76 @@ def closest_silhouette_brute(dim, x, r_max=None, threads=0, *, vertices=None, in
              else C.c_int64(a) for a in args]
     fn(*cargs, C.c_void_p(f.ctypes.data), C.c_void_p(i.ctypes.data), C.c_int(threads or n_threads()))
     return _split(dim, "sil", f, i)
+
+
+# ---- the reference's own builder (oracle/_ref, built by `make -C oracle ref`) ----
+
+REF_LIB = HERE / "_ref" / "libgqref.so"
+_ref_lib = None
+REF_ARRAYS = {"bvh_nodes": 0, "primitives": 1, "snch_nodes": 2, "silhouettes": 3, "raw_silhouettes": 4}
+
+
+def build_ref(reference=None):
+    """Compiles gQuery's own builder sources from a checkout (GQ_REFERENCE, or the
+    default below) into oracle/_ref/libgqref.so.  Returns the library path, or None when
+    neither a checkout nor a built library is at hand."""
+    ref = Path(reference or os.environ.get("GQ_REFERENCE") or "/root/reference")
+    deps = [HERE / "ref_builder.cpp", HERE / "eigen_subset" / "Eigen" / "Dense", HERE / "Makefile"]
+    if not (ref / "src" / "shapes" / "bvh.cpp").exists():
+        return REF_LIB if REF_LIB.exists() else None
+    if not REF_LIB.exists() or any(d.stat().st_mtime > REF_LIB.stat().st_mtime for d in deps):
+        subprocess.run(["make", "-C", str(HERE), "ref", f"REF={ref}"], check=True, capture_output=True)
+    return REF_LIB
+
+
+def ref_lib():
+    global _ref_lib
+    if _ref_lib is None:
+        if build_ref() is None:
+            raise FileNotFoundError("oracle/_ref/libgqref.so is not built and no gQuery checkout was found")
+        _ref_lib = C.CDLL(str(REF_LIB))
+        _ref_lib.gqref_build.restype = C.c_void_p
+        _ref_lib.gqref_array.restype = C.c_int64
+        _ref_lib.gqref_array.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int64]
+        _ref_lib.gqref_free.argtypes = [C.c_void_p]
+        _ref_lib.gqref_error.restype = C.c_char_p
+        _ref_lib.gqref_flat_silhouette_edges.restype = C.c_int64
+    return _ref_lib
+
+
+def reference_build(dim, vertices, indices, snch=True, max_prims_in_node=10):
+    """The reference's BVH / SNCH (src/shapes/bvh.cpp, snch.cpp) built from its own
+    sources: a dict of its flat float arrays (node_data, primitive_data, silhouette_data,
+    raw_silhouette_data) under the names of REF_ARRAYS."""
+    lib = ref_lib()
+    v = _f(vertices).reshape(-1, dim)
+    ix = np.ascontiguousarray(indices, np.int32).reshape(-1, dim)
+    h = lib.gqref_build(C.c_int(dim), C.c_void_p(v.ctypes.data), C.c_int64(v.shape[0]), C.c_void_p(ix.ctypes.data),
+                        C.c_int64(ix.shape[0]), C.c_int(max_prims_in_node), C.c_int(1 if snch else 0))
+    if not h:
+        raise RuntimeError(lib.gqref_error().decode())
+    try:
+        out = {}
+        for name, which in REF_ARRAYS.items():
+            n = lib.gqref_array(h, which, None, 0)
+            if n < 0:
+                continue
+            a = np.empty(n, np.float32)
+            lib.gqref_array(h, which, C.c_void_p(a.ctypes.data), n)
+            out[name] = a
+        return out
+    finally:
+        lib.gqref_free(h)
+
+
+def reference_flat_silhouette_edges(vertices, indices):
+    """build_flat_silhouette_edges (src/shapes/silhouette_edge.cpp:62-71) from the
+    reference's own source."""
+    lib = ref_lib()
+    v = _f(vertices).reshape(-1, 3)
+    ix = np.ascontiguousarray(indices, np.int32).reshape(-1, 3)
+    args = [C.c_void_p(v.ctypes.data), C.c_int64(v.shape[0]), C.c_void_p(ix.ctypes.data), C.c_int64(ix.shape[0])]
+    n = lib.gqref_flat_silhouette_edges(*args, None, C.c_int64(0))
+    a = np.empty(n, np.float32)
+    lib.gqref_flat_silhouette_edges(*args, C.c_void_p(a.ctypes.data), C.c_int64(n))
+    return a

@@ -141,17 +141,34 @@ def test_silhouette_edge_boundary_keeps_zero_vertex():
 
 
 def test_snch_cones_reference_rules():
+    """Cones follow snch.cpp:103-154 over the node ranges the reference's recursion
+    passes (snch.cpp:151-152): the root gets [0, n), a right child its parent's end, a
+    left child its parent's RELATIVE second-child offset as its end.  A range without
+    silhouettes leaves the invalid cone (half angle -pi, zero axis and radius); valid
+    cones have unit axes (or the half angle pi)."""
     v, e = W.star_polyline(2048, seed=4)
     s = gx.SNCH(v, e)
     N = s.node_data().reshape(-1, 13)
-    half, rad = N[:, 6], N[:, 7]
-    axis = N[:, 4:6]
-    # every node owns silhouettes below it -> valid cone with unit axis or pi (degenerate axis)
-    assert ((half >= 0) & (half <= np.float32(math.pi))).all()
+    half, rad, axis = N[:, 6], N[:, 7], N[:, 4:6]
+    second, nprim, nsil = N[:, 9].astype(np.int64), N[:, 10].astype(np.int64), N[:, 12].astype(np.int64)
+    n = N.shape[0]
+    end = np.zeros(n, np.int64)
+    stack = [(0, n)]
+    while stack:
+        i, e_ = stack.pop()
+        end[i] = e_
+        if nprim[i] == 0:
+            stack += [(i + 1, second[i]), (i + second[i], e_)]
+    expect_valid = np.array([nsil[i:max(i, end[i])].sum() > 0 for i in range(n)])
+    valid = half >= 0
+    assert np.array_equal(valid, expect_valid)
+    assert valid[0] and not valid.all()
+    assert np.all(half[~valid] == np.float32(-math.pi))
+    assert np.all(axis[~valid] == 0) and np.all(rad[~valid] == 0)
     norm = np.linalg.norm(axis, axis=1)
-    assert np.allclose(norm[half < np.float32(math.pi)], 1.0, atol=1e-5)
+    assert np.allclose(norm[valid & (half < np.float32(math.pi))], 1.0, atol=1e-5)
     assert (rad >= 0).all()
-    # root cone half angle covers all silhouette normals of a closed star: pi (axis ~ 0)
+    # the root's cone covers all silhouette normals of a closed star
     assert half[0] == np.float32(math.pi) or half[0] > 1.5
 
 
