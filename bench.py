@@ -566,10 +566,19 @@ def run_reference(args):
     q = W.uniform_points(per_step, 3, seed=1)
     o, d = W.rays(per_step, 3, seed=2)
     import oracle
-    from gquery_b200 import _lib as L
-    from gquery_b200.scene import Scene
-    s = Scene(V, F, 3, device=None, build_snch=False, build_wide=False)
-    nodes, prims = s.ref_array(L.ARRAY_BVH_NODES), s.ref_array(L.ARRAY_PRIMITIVES)
+    # the tree: gQuery's own builder code (oracle/_ref, compiled from its sources) when it
+    # is at hand, else this project's builder, whose arrays equal it bit for bit
+    # (tests/test_ref_builder.py)
+    if oracle.build_ref() is not None:
+        arrays = oracle.reference_build(3, V, F, snch=False)
+        nodes, prims = arrays["bvh_nodes"], arrays["primitives"]
+        tree = "gQuery's own builder sources (oracle/_ref/libgqref.so)"
+    else:
+        from gquery_b200 import _lib as L
+        from gquery_b200.scene import Scene
+        s = Scene(V, F, 3, device=None, build_snch=False, build_wide=False)
+        nodes, prims = s.ref_array(L.ARRAY_BVH_NODES), s.ref_array(L.ARRAY_PRIMITIVES)
+        tree = "this project's builder (arrays bit-identical to the reference builder's)"
     threads = oracle.n_threads()
 
     def step():
@@ -590,7 +599,7 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "engine": "CPU restatement of gQuery's traversal (oracle port)",
-                       "sample": sample},
+                       "tree": tree, "sample": sample},
             "cpu_baseline": {"value": value, "unit": "Mqueries/s", "cores": threads, "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": "Mqueries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}

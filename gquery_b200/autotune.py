@@ -44,8 +44,9 @@ def candidates(kind: str, dim: int, has_wide: bool, exact_stack: int, wide_stack
             if has_wide:
                 out.append(dict(variant="wide8", packet=0, persist=1, budget=32, block=b))
                 if dim == 3:
-                    out.append(dict(variant="wide8", packet=1, sorted=1, block=b))
-                    out.append(dict(variant="wide8", packet=1, sorted=0, block=b))
+                    for packet in (1, 2):  # 2: with the warp-level child cull
+                        out.append(dict(variant="wide8", packet=packet, sorted=1, block=b))
+                        out.append(dict(variant="wide8", packet=packet, sorted=0, block=b))
     elif kind == "ray":
         for b in blocks:
             out.append(dict(variant="exact", persist=1, budget=32, block=b))

@@ -606,9 +606,26 @@ int64_t gq_order_scratch_bytes(int64_t n) {
     return (int64_t)gqd::morton_scratch_bytes(n);
 }
 
+static gq_status order_impl(const gq_scene *s, gq_vecs points, int64_t n, int32_t *order, void *scratch,
+                            int64_t scratch_bytes, void *stream, int ray_mode, gq_vecs dirs);
+
+gq_status gq_ray_order(const gq_scene *s, gq_vecs origins, gq_vecs dirs, int64_t n, int32_t mode, int32_t *order,
+                       void *scratch, int64_t scratch_bytes, void *stream) {
+    if (!s || !order) return fail(GQ_ERR_INVALID, "null scene or order");
+    if (mode < 0 || mode > 2) return fail(GQ_ERR_INVALID, "ray order mode must be 0, 1 or 2");
+    if (mode > 0 && s->dim != 3) return fail(GQ_ERR_UNSUPPORTED, "direction keys are for 3D scenes");
+    if (n > 0 && mode > 0 && !vecs_ok(dirs)) return fail(GQ_ERR_INVALID, "null direction array");
+    return order_impl(s, origins, n, order, scratch, scratch_bytes, stream, mode, dirs);
+}
+
 gq_status gq_query_order(const gq_scene *s, gq_vecs points, int64_t n, int32_t *order, void *scratch,
                          int64_t scratch_bytes, void *stream) {
     if (!s || !order) return fail(GQ_ERR_INVALID, "null scene or order");
+    return order_impl(s, points, n, order, scratch, scratch_bytes, stream, 0, gq_vecs{});
+}
+
+static gq_status order_impl(const gq_scene *s, gq_vecs points, int64_t n, int32_t *order, void *scratch,
+                            int64_t scratch_bytes, void *stream, int ray_mode, gq_vecs dirs) {
     if (n < 0) return fail(GQ_ERR_INVALID, "negative count");
     if (n == 0) return GQ_OK;
     if (!vecs_ok(points)) return fail(GQ_ERR_INVALID, "null point array");
@@ -627,7 +644,7 @@ gq_status gq_query_order(const gq_scene *s, gq_vecs points, int64_t n, int32_t *
         scr.owned = true;
         scr.st = cs;
     }
-    cudaError_t e = gqd::morton_order(s->dev, points, n, order, scr.p, need, cs);
+    cudaError_t e = gqd::morton_order(s->dev, points, n, order, scr.p, need, cs, ray_mode, dirs);
     if (e != cudaSuccess) return fail_cuda(e, "morton_order");
     return GQ_OK;
 }

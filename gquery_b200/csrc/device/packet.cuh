@@ -34,6 +34,14 @@ __device__ __forceinline__ float qf(uint32_t lo4, uint32_t hi4, int k) {
 __device__ __forceinline__ float warp_min(float x) {
     return __uint_as_float(__reduce_min_sync(0xffffffffu, __float_as_uint(x)));
 }
+// order-preserving map of any float to an unsigned word, and back
+__device__ __forceinline__ uint32_t ford(float f) {
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float funord(uint32_t u) {
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
 __device__ __forceinline__ void pcas(float &ka, int &ra, float &kb, int &rb) {
     const bool sw = kb < ka;
     const float k0 = sw ? kb : ka, k1 = sw ? ka : kb;
@@ -109,11 +117,27 @@ __device__ __forceinline__ void leaf(const DevScene &s, int ref, bool act, const
 // ignored), idx: its best item slot (-1: none).  LAYOUT 0: binary pairs,
 // 1: quantised 8-wide nodes (3D only).  STK: entries of the caller's stack `stk`; the
 // warp stops with `ovf` set rather than overflow it.
-template <int D, int LAYOUT, bool MINFIRST, int STK = kPStack>
+// CULL (8-wide nodes): before the lanes test a node's children against their own
+// queries, lanes 0..7 test one child each against the box around the warp's queries
+// and the largest search radius of the lanes that need the node; a child that is
+// farther than that from the whole box (with a 2^-17 relative margin, far above the
+// rounding of either test) fails every lane's own test, so it is dropped for all of
+// them before any lane decodes it.  The decisions, and so the answers, are those of
+// the walk without it.
+template <int D, int LAYOUT, bool MINFIRST, int STK = kPStack, bool CULL = false>
 __device__ __forceinline__ void closest_point(const DevScene &s, unsigned mask, const float *p, float &r, int &idx,
                                               bool &ovf, int2 *stk) {
     const unsigned lane = threadIdx.x & 31u;
     const bool mine = (mask >> lane) & 1u;
+    // the box around the warp's queries (lanes outside `mask` do not count)
+    float qlo[3] = {0.f, 0.f, 0.f}, qhi[3] = {0.f, 0.f, 0.f};
+    if (CULL && LAYOUT == 1) {
+#pragma unroll
+        for (int c = 0; c < D; ++c) {
+            qlo[c] = funord(__reduce_min_sync(0xffffffffu, ford(mine ? p[c] : kInf)));
+            qhi[c] = funord(__reduce_max_sync(0xffffffffu, ford(mine ? p[c] : -kInf)));
+        }
+    }
     if (!mine) r = 0.f;  // never needs a node
     int cur = LAYOUT ? s.wroot_ref : s.root_ref;
     unsigned cmask = mask;
@@ -200,10 +224,32 @@ __device__ __forceinline__ void closest_point(const DevScene &s, unsigned mask, 
             float key[8];
             int ref[8] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
             float shrink = kInf;
+            unsigned far = 0;  // children no lane can need (CULL)
+            if (CULL) {
+                // the largest radius among the lanes that need this node (r >= 0, so the
+                // float order is the unsigned order)
+                const float r2 = __uint_as_float(__reduce_max_sync(0xffffffffu, act ? __float_as_uint(r) : 0u));
+                bool cut = false;
+                if ((int)lane < nc) {
+                    const int k = (int)lane;
+                    const float clo[3] = {__fmaf_rn(qf(q0.x, q0.y, k), sx, h.x), __fmaf_rn(qf(q0.z, q0.w, k), sy, h.y),
+                                          __fmaf_rn(qf(q1.x, q1.y, k), sz, h.z)};
+                    const float chi[3] = {__fmaf_rn(qf(q1.z, q1.w, k), sx, h.x), __fmaf_rn(qf(q2.x, q2.y, k), sy, h.y),
+                                          __fmaf_rn(qf(q2.z, q2.w, k), sz, h.z)};
+                    float d2 = 0.f;
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const float g = fmaxf(fmaxf(clo[c] - qhi[c], qlo[c] - chi[c]), 0.f);
+                        d2 = __fmaf_rn(g, g, d2);
+                    }
+                    cut = d2 > r2 * (kSlack * kSlack);
+                }
+                far = __ballot_sync(0xffffffffu, cut);
+            }
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
                 float a2 = kInf, b2 = kInf;
-                if (act && k < nc) {
+                if (act && k < nc && !((far >> k) & 1u)) {
                     const float lo3[3] = {__fmaf_rn(qf(q0.x, q0.y, k), sx, h.x), __fmaf_rn(qf(q0.z, q0.w, k), sy, h.y),
                                           __fmaf_rn(qf(q1.x, q1.y, k), sz, h.z)};
                     const float hi3[3] = {__fmaf_rn(qf(q1.z, q1.w, k), sx, h.x), __fmaf_rn(qf(q2.x, q2.y, k), sy, h.y),

@@ -604,6 +604,53 @@ __global__ void k_morton_keys(int dim, float lo0, float lo1, float lo2, float sc
     vals[i] = (int32_t)i;
 }
 
+// Ray keys: the origin's cell on the same grid as k_morton_keys and the direction.
+// mode 1: the direction's octant (3 bits) above a 27-bit Morton code of the origin
+//         (9 bits per axis): each warp of sorted rays shares an octant and a region.
+// mode 2: the origin (6 bits per axis) and the direction's octahedral coordinates
+//         (6 bits each) interleaved coarse to fine, 30 bits.
+__device__ __forceinline__ uint32_t spread5(uint32_t v) {  // 6 bits -> every fifth bit
+    uint32_t r = 0;
+#pragma unroll
+    for (int b = 0; b < 6; ++b) r |= ((v >> b) & 1u) << (5 * b);
+    return r;
+}
+
+__global__ void k_ray_keys(int mode, float lo0, float lo1, float lo2, float sc0, float sc1, float sc2, gq_vecs o,
+                           gq_vecs d, int64_t n, uint32_t *keys, int32_t *vals) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float lo[3] = {lo0, lo1, lo2}, sc[3] = {sc0, sc1, sc2};
+    float dir[3];
+    uint32_t c[3];
+    for (int k = 0; k < 3; ++k) {
+        float f = (qget(o, i, k) - lo[k]) * sc[k];  // 0 .. 1024 over the grid
+        f = fminf(fmaxf(f, 0.f), 1023.f);
+        c[k] = (uint32_t)f;
+        dir[k] = qget(d, i, k);
+    }
+    uint32_t key;
+    if (mode == 1) {
+        const uint32_t oct = (dir[0] < 0.f ? 4u : 0u) | (dir[1] < 0.f ? 2u : 0u) | (dir[2] < 0.f ? 1u : 0u);
+        key = (oct << 27) | (spread3(c[0] >> 1) << 2) | (spread3(c[1] >> 1) << 1) | spread3(c[2] >> 1);
+    } else {
+        // octahedral map of the direction onto [-1, 1]^2
+        const float l1 = fabsf(dir[0]) + fabsf(dir[1]) + fabsf(dir[2]);
+        float u = l1 > 0.f ? dir[0] / l1 : 0.f, v = l1 > 0.f ? dir[1] / l1 : 0.f;
+        if (dir[2] < 0.f) {
+            const float uu = (1.f - fabsf(v)) * (u < 0.f ? -1.f : 1.f);
+            v = (1.f - fabsf(u)) * (v < 0.f ? -1.f : 1.f);
+            u = uu;
+        }
+        const uint32_t qu = (uint32_t)fminf(fmaxf((u + 1.f) * 32.f, 0.f), 63.f);
+        const uint32_t qv = (uint32_t)fminf(fmaxf((v + 1.f) * 32.f, 0.f), 63.f);
+        key = (spread5(c[0] >> 4) << 4) | (spread5(c[1] >> 4) << 3) | (spread5(c[2] >> 4) << 2) | (spread5(qu) << 1) |
+              spread5(qv);
+    }
+    keys[i] = key;
+    vals[i] = (int32_t)i;
+}
+
 inline dim3 grid_for(int64_t n) { return dim3((unsigned)((n + kBlock - 1) / kBlock)); }
 inline size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
@@ -621,7 +668,7 @@ size_t morton_scratch_bytes(int64_t n) {
 }
 
 cudaError_t morton_order(const DevScene &s, gq_vecs q, int64_t n, int32_t *perm, void *scratch, size_t scratch_bytes,
-                         cudaStream_t st) {
+                         cudaStream_t st, int ray_mode, gq_vecs ray_dir) {
     if (n <= 0) return cudaSuccess;
     if (scratch_bytes < morton_scratch_bytes(n)) return cudaErrorInvalidValue;
     char *p = (char *)scratch;
@@ -641,10 +688,15 @@ cudaError_t morton_order(const DevScene &s, gq_vecs q, int64_t n, int32_t *perm,
         lo[k] = c - ext;
         sc[k] = (float)bits / (2.f * ext);
     }
-    k_morton_keys<<<grid_for(n), kBlock, 0, st>>>(s.dim, lo[0], lo[1], lo[2], sc[0], sc[1], sc[2], q, n, k_in, v_in);
+    if (ray_mode > 0 && s.dim == 3)
+        k_ray_keys<<<grid_for(n), kBlock, 0, st>>>(ray_mode, lo[0], lo[1], lo[2], sc[0], sc[1], sc[2], q, ray_dir, n,
+                                                   k_in, v_in);
+    else
+        k_morton_keys<<<grid_for(n), kBlock, 0, st>>>(s.dim, lo[0], lo[1], lo[2], sc[0], sc[1], sc[2], q, n, k_in,
+                                                      v_in);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    const int end_bit = s.dim == 3 ? 30 : 30;
+    const int end_bit = 30;
     return cub::DeviceRadixSort::SortPairs(p, tb, k_in, k_out, v_in, perm, (int)n, 0, end_bit, st);
 }
 

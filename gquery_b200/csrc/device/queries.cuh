@@ -35,8 +35,9 @@ struct DevScene {
 // Morton reordering: writes perm[0..n) (a permutation of 0..n-1) using `scratch`.
 // Returns the scratch bytes needed when scratch == nullptr.
 size_t morton_scratch_bytes(int64_t n);
+// ray_mode > 0 (3D): keys from the ray origins q and directions ray_dir (see k_ray_keys).
 cudaError_t morton_order(const DevScene &s, gq_vecs q, int64_t n, int32_t *perm, void *scratch, size_t scratch_bytes,
-                         cudaStream_t st);
+                         cudaStream_t st, int ray_mode = 0, gq_vecs ray_dir = gq_vecs{});
 
 // Launch choices for one query kind (picked by the autotuner or the defaults).
 struct Tune {

@@ -196,6 +196,19 @@ class Scene:
         L.check(L.lib().gq_query_order(self._h, vq, n, perm.data_ptr(), sp, sb, _stream_handle(stream)))
         return perm
 
+    def ray_order(self, origins, dirs, mode: int = 1, *, stream=None, scratch=None, out=None):
+        """Permutation of rays (int32 [n] on the device) keyed by origin and direction:
+        mode 0 origin Morton order, 1 direction octant then origin, 2 origin and direction
+        interleaved."""
+        t, n, vo = self._points(origins)
+        td, n2, vd = self._points(dirs)
+        if n2 != n:
+            raise ValueError("origins and directions differ in length")
+        perm = out if out is not None else self._alloc(n, torch.int32)
+        sp, sb = (None, 0) if scratch is None else (scratch.data_ptr(), scratch.numel() * scratch.element_size())
+        L.check(L.lib().gq_ray_order(self._h, vo, vd, n, int(mode), perm.data_ptr(), sp, sb, _stream_handle(stream)))
+        return perm
+
     def get_tuning(self, kind: str) -> dict:
         t = L.Tuning()
         L.check(L.lib().gq_scene_get_tuning(self._h, KINDS[kind], C.byref(t)))

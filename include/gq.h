@@ -60,8 +60,9 @@ typedef int32_t gq_status;
 
 typedef struct {
     int32_t variant;  /* variant used when a query asks for GQ_VARIANT_AUTO */
-    int32_t packet;   /* WIDE8 closest point (3D): warp-coherent traversal; WARP silhouettes: switch to
-                         the coherent traversal from 2^18 queries on */
+    int32_t packet;   /* WIDE8 closest point (3D): 1 = warp-coherent traversal, 2 = the same with a
+                         warp-level cull of children no lane can need (same answers); WARP
+                         silhouettes: switch to the coherent traversal from 2^18 queries on */
     int32_t sorted;   /* warp-coherent wide nodes: children in distance order (else nearest first) */
     int32_t persist;  /* per-thread kernels: persistent warps, finished lanes take new queries */
     int32_t budget;   /* node visits between refills */
@@ -199,6 +200,12 @@ int64_t gq_query_scratch_bytes(int64_t n);
 int64_t gq_order_scratch_bytes(int64_t n);
 gq_status gq_query_order(const gq_scene *scene, gq_vecs points, int64_t n, int32_t *order, void *scratch,
                          int64_t scratch_bytes, void *stream);
+/* The same for rays (3D scenes), keyed by origin and direction so that the rays of one warp
+ * also point alike: mode 0 = the origins' Morton order (gq_query_order), 1 = direction
+ * octant, then the origins' Morton code, 2 = origin cell and octahedral direction cell
+ * interleaved.  No counterpart in the reference (DrJit runs rays in input order). */
+gq_status gq_ray_order(const gq_scene *scene, gq_vecs origins, gq_vecs dirs, int64_t n, int32_t mode, int32_t *order,
+                       void *scratch, int64_t scratch_bytes, void *stream);
 
 /* closest_point_bvh (Polyline: polyline.py:171 -> bvh.py:127; Mesh: mesh.py:119 -> bvh3d.py:108) */
 gq_status gq_closest_point(const gq_scene *scene, gq_vecs q, int64_t n, const gq_cp_out *out,
