@@ -38,13 +38,14 @@ def candidates(kind: str, dim: int, has_wide: bool, exact_stack: int, wide_stack
         for b in blocks:
             out.append(dict(variant="exact", persist=0, block=b))
             out.append(dict(variant="exact", persist=1, budget=32, block=b))
-            out.append(dict(variant="coherent", block=b, stack=0))
-            if exact_stack <= 32:
-                out.append(dict(variant="coherent", block=b, stack=32))
+            for packet in (1, 2):  # 2: the compact stack
+                out.append(dict(variant="coherent", packet=packet, block=b, stack=0))
+                if exact_stack <= 32:
+                    out.append(dict(variant="coherent", packet=packet, block=b, stack=32))
             if has_wide:
                 out.append(dict(variant="wide8", packet=0, persist=1, budget=32, block=b))
                 if dim == 3:
-                    for packet in (1, 2):  # 2: with the warp-level child cull
+                    for packet in (1, 2):  # 2: the compact stack
                         out.append(dict(variant="wide8", packet=packet, sorted=1, block=b))
                         out.append(dict(variant="wide8", packet=packet, sorted=0, block=b))
     elif kind == "ray":

@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(kBlock) k_batch(const DevScene *scenes, int n_
                 float r = kInf;
                 int idx = -1;
                 bool o = false;
-                pkt::closest_point<D, 0, false>(scenes[s0], m, p, r, idx, o, stk);
+                pkt::closest_point<D, 0, false>(scenes[s0], m, p, r, idx, o, pkt::PStack<false>(stk));
                 if ((m >> lane) & 1u) {
                     best_idx = idx;
                     ovf = o;

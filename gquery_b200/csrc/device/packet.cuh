@@ -14,6 +14,8 @@
 // recomputes the winner's record exactly.
 #pragma once
 
+#include <cuda_fp16.h>
+
 #include "prim.cuh"
 #include "queries.cuh"
 
@@ -34,14 +36,6 @@ __device__ __forceinline__ float qf(uint32_t lo4, uint32_t hi4, int k) {
 __device__ __forceinline__ float warp_min(float x) {
     return __uint_as_float(__reduce_min_sync(0xffffffffu, __float_as_uint(x)));
 }
-// order-preserving map of any float to an unsigned word, and back
-__device__ __forceinline__ uint32_t ford(float f) {
-    const uint32_t u = __float_as_uint(f);
-    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-}
-__device__ __forceinline__ float funord(uint32_t u) {
-    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
-}
 __device__ __forceinline__ void pcas(float &ka, int &ra, float &kb, int &rb) {
     const bool sw = kb < ka;
     const float k0 = sw ? kb : ka, k1 = sw ? ka : kb;
@@ -56,6 +50,40 @@ __device__ __forceinline__ void psort8(float (&k)[8], int (&r)[8]) {  // Batcher
     pcas(k[2], r[2], k[4], r[4]); pcas(k[3], r[3], k[5], r[5]);
     pcas(k[1], r[1], k[2], r[2]); pcas(k[3], r[3], k[4], r[4]); pcas(k[5], r[5], k[6], r[6]);
 }
+
+// The walk's stack of (node, this lane's key) entries.
+// Plain: each lane keeps both words of every entry in its local memory.
+// Compact: the node of each entry is kept once per warp in shared memory (every lane
+// writes the same word and reads back its own write, so no lane depends on another's
+// store), and the lane's key is rounded down to FP16 in its local memory: 10 bytes per
+// entry and warp instead of 256.  A key rounded down admits every entry the exact key
+// admits, and at worst a few more, which cost a visit and change no answer.
+template <bool COMPACT>
+struct PStack;
+template <>
+struct PStack<false> {
+    int2 *e;
+    __device__ __forceinline__ PStack(int2 *p) : e(p) {}
+    __device__ __forceinline__ void put(int i, int ref, float key) { e[i] = make_int2(ref, fbits(key)); }
+    __device__ __forceinline__ void get(int i, int &ref, float &key) const {
+        const int2 x = e[i];
+        ref = x.x;
+        key = __int_as_float(x.y);
+    }
+};
+template <>
+struct PStack<true> {
+    int *refs;     // this warp's row (shared memory)
+    __half *keys;  // this lane's keys (local memory)
+    __device__ __forceinline__ void put(int i, int ref, float key) {
+        refs[i] = ref;
+        keys[i] = __float2half_rd(key);
+    }
+    __device__ __forceinline__ void get(int i, int &ref, float &key) const {
+        ref = refs[i];
+        key = __half2float(keys[i]);
+    }
+};
 
 // squared distances from p to the nearest / farthest point of a box
 template <int D>
@@ -117,27 +145,12 @@ __device__ __forceinline__ void leaf(const DevScene &s, int ref, bool act, const
 // ignored), idx: its best item slot (-1: none).  LAYOUT 0: binary pairs,
 // 1: quantised 8-wide nodes (3D only).  STK: entries of the caller's stack `stk`; the
 // warp stops with `ovf` set rather than overflow it.
-// CULL (8-wide nodes): before the lanes test a node's children against their own
-// queries, lanes 0..7 test one child each against the box around the warp's queries
-// and the largest search radius of the lanes that need the node; a child that is
-// farther than that from the whole box (with a 2^-17 relative margin, far above the
-// rounding of either test) fails every lane's own test, so it is dropped for all of
-// them before any lane decodes it.  The decisions, and so the answers, are those of
-// the walk without it.
-template <int D, int LAYOUT, bool MINFIRST, int STK = kPStack, bool CULL = false>
+// COMPACT: the stack of PStack<true> (FP16 keys, one node word per warp).
+template <int D, int LAYOUT, bool MINFIRST, int STK = kPStack, bool COMPACT = false>
 __device__ __forceinline__ void closest_point(const DevScene &s, unsigned mask, const float *p, float &r, int &idx,
-                                              bool &ovf, int2 *stk) {
+                                              bool &ovf, PStack<COMPACT> stk) {
     const unsigned lane = threadIdx.x & 31u;
     const bool mine = (mask >> lane) & 1u;
-    // the box around the warp's queries (lanes outside `mask` do not count)
-    float qlo[3] = {0.f, 0.f, 0.f}, qhi[3] = {0.f, 0.f, 0.f};
-    if (CULL && LAYOUT == 1) {
-#pragma unroll
-        for (int c = 0; c < D; ++c) {
-            qlo[c] = funord(__reduce_min_sync(0xffffffffu, ford(mine ? p[c] : kInf)));
-            qhi[c] = funord(__reduce_max_sync(0xffffffffu, ford(mine ? p[c] : -kInf)));
-        }
-    }
     if (!mine) r = 0.f;  // never needs a node
     int cur = LAYOUT ? s.wroot_ref : s.root_ref;
     unsigned cmask = mask;
@@ -146,10 +159,12 @@ __device__ __forceinline__ void closest_point(const DevScene &s, unsigned mask, 
         if (cur == kNone) {
             bool found = false;
             while (sp >= 0) {
-                const int2 e = stk[sp--];
-                const unsigned m = __ballot_sync(0xffffffffu, __int_as_float(e.y) <= r * kSlack);
+                int eref;
+                float ekey;
+                stk.get(sp--, eref, ekey);
+                const unsigned m = __ballot_sync(0xffffffffu, ekey <= r * kSlack);
                 if (m) {
-                    cur = e.x;
+                    cur = eref;
                     cmask = m;
                     found = true;
                     break;
@@ -198,7 +213,8 @@ __device__ __forceinline__ void closest_point(const DevScene &s, unsigned mask, 
                     ovf = true;
                     break;
                 }
-                stk[++sp] = right_first ? make_int2(rl, fbits(hl ? a2l : kInf)) : make_int2(rr, fbits(hr ? a2r : kInf));
+                ++sp;
+                stk.put(sp, right_first ? rl : rr, right_first ? (hl ? a2l : kInf) : (hr ? a2r : kInf));
                 cur = right_first ? rr : rl;
                 cmask = right_first ? mr : ml;
             } else if (ml) {
@@ -224,32 +240,10 @@ __device__ __forceinline__ void closest_point(const DevScene &s, unsigned mask, 
             float key[8];
             int ref[8] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
             float shrink = kInf;
-            unsigned far = 0;  // children no lane can need (CULL)
-            if (CULL) {
-                // the largest radius among the lanes that need this node (r >= 0, so the
-                // float order is the unsigned order)
-                const float r2 = __uint_as_float(__reduce_max_sync(0xffffffffu, act ? __float_as_uint(r) : 0u));
-                bool cut = false;
-                if ((int)lane < nc) {
-                    const int k = (int)lane;
-                    const float clo[3] = {__fmaf_rn(qf(q0.x, q0.y, k), sx, h.x), __fmaf_rn(qf(q0.z, q0.w, k), sy, h.y),
-                                          __fmaf_rn(qf(q1.x, q1.y, k), sz, h.z)};
-                    const float chi[3] = {__fmaf_rn(qf(q1.z, q1.w, k), sx, h.x), __fmaf_rn(qf(q2.x, q2.y, k), sy, h.y),
-                                          __fmaf_rn(qf(q2.z, q2.w, k), sz, h.z)};
-                    float d2 = 0.f;
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        const float g = fmaxf(fmaxf(clo[c] - qhi[c], qlo[c] - chi[c]), 0.f);
-                        d2 = __fmaf_rn(g, g, d2);
-                    }
-                    cut = d2 > r2 * (kSlack * kSlack);
-                }
-                far = __ballot_sync(0xffffffffu, cut);
-            }
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
                 float a2 = kInf, b2 = kInf;
-                if (act && k < nc && !((far >> k) & 1u)) {
+                if (act && k < nc) {
                     const float lo3[3] = {__fmaf_rn(qf(q0.x, q0.y, k), sx, h.x), __fmaf_rn(qf(q0.z, q0.w, k), sy, h.y),
                                           __fmaf_rn(qf(q1.x, q1.y, k), sz, h.z)};
                     const float hi3[3] = {__fmaf_rn(qf(q1.z, q1.w, k), sx, h.x), __fmaf_rn(qf(q2.x, q2.y, k), sy, h.y),
@@ -297,7 +291,7 @@ __device__ __forceinline__ void closest_point(const DevScene &s, unsigned mask, 
                         c0 = ref[k];
                         m0 = wmask[k];
                     } else if (wmask[k]) {
-                        stk[++sp] = make_int2(ref[k], fbits(key[k]));
+                        stk.put(++sp, ref[k], key[k]);
                     }
                 }
                 cur = c0;
@@ -320,7 +314,7 @@ __device__ __forceinline__ void closest_point(const DevScene &s, unsigned mask, 
                         sref = (slot[k] == m) ? ref[m] : sref;
                         skey = (slot[k] == m) ? key[m] : skey;
                     }
-                    stk[++sp] = make_int2(sref, fbits(skey));
+                    stk.put(++sp, sref, skey);
                 }
             }
             int c0 = ref[0];

@@ -63,7 +63,10 @@ class Polyline(_Shape):
         p = _as_tensor(p).to(self.scene.torch_device, torch.float32)
         if n is not None and on_boundary is not None:
             n = _as_tensor(n).to(p.device, torch.float32)
-            ob = _as_tensor(on_boundary).to(p.device, torch.bool)
+            ob = _as_tensor(on_boundary).to(p.device, torch.bool).reshape(-1)
+            # one flag per ray: along the last axis of [D, n] points, the first of [n, D]
+            soa = p.dim() == 2 and p.shape[0] == self.dim and p.shape[1] == ob.numel()
+            ob = ob[None, :] if soa else ob[:, None]
             p = torch.where(ob, p - 1e-5 * n, p)
         return self.intersect_baseline(p, v, r_max)
 

@@ -60,9 +60,10 @@ typedef int32_t gq_status;
 
 typedef struct {
     int32_t variant;  /* variant used when a query asks for GQ_VARIANT_AUTO */
-    int32_t packet;   /* WIDE8 closest point (3D): 1 = warp-coherent traversal, 2 = the same with a
-                         warp-level cull of children no lane can need (same answers); WARP
-                         silhouettes: switch to the coherent traversal from 2^18 queries on */
+    int32_t packet;   /* WIDE8 closest point (3D): 1 = warp-coherent traversal; warp-coherent closest
+                         points (COHERENT, and WIDE8 with packet): 2 = the compact stack (keys rounded
+                         down to FP16, one node word per warp; same answers); WARP silhouettes:
+                         switch to the coherent traversal from 2^18 queries on */
     int32_t sorted;   /* warp-coherent wide nodes: children in distance order (else nearest first) */
     int32_t persist;  /* per-thread kernels: persistent warps, finished lanes take new queries */
     int32_t budget;   /* node visits between refills */

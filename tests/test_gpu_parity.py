@@ -329,3 +329,22 @@ def test_sil3d_fast_variants_against_oracle_small(mesh_small, variant):
     assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0, rep
     with pytest.raises(L.GQError, match="exact, coherent or warp"):
         mesh_small.closest_silhouette(x, variant="wide8")
+
+
+@pytest.mark.parametrize("variant,tuning", [("coherent", dict(stack=0)), ("wide8", dict(packet=1, sorted=0)),
+                                            ("wide8", dict(packet=1, sorted=1))])
+def test_compact_stack_bitwise(mesh_c1, variant, tuning):
+    """The warp-coherent walks with the compact stack (keys rounded down to FP16, one node
+    word per warp) give the same records as with the plain stack, bit for bit: a key
+    rounded down only admits entries whose triangles are all farther than the lane's
+    radius."""
+    q = torch.as_tensor(W.uniform_points(200_000, 3, seed=57)).cuda()
+    try:
+        mesh_c1.set_tuning("cp", variant, **tuning)
+        plain = to_np(mesh_c1.closest_point(q, variant=variant))
+        mesh_c1.set_tuning("cp", variant, **dict(tuning, packet=2))
+        compact = to_np(mesh_c1.closest_point(q, variant=variant))
+    finally:
+        mesh_c1.set_tuning("cp", "coherent", packet=1, persist=0)
+    assert_bitwise(compact, plain, CP_FIELDS_3D, f"{variant} compact ")
+    assert mesh_c1.device_error() == 0
