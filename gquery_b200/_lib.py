@@ -158,6 +158,7 @@ SIGNATURES = {
                                  C.c_void_p]),
     "gq_scene_device_error": (C.c_int32, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)]),
     "gq_scene_set_stack_limit": (C.c_int32, [C.c_void_p, C.c_int32]),
+    "gq_read_probe": (C.c_int32, [C.c_void_p, C.c_int64, C.c_int32, C.c_void_p, C.c_void_p]),
     "gq_ray_order": (C.c_int32, [C.c_void_p, Vecs, Vecs, C.c_int64, C.c_int32, C.c_void_p, C.c_void_p, C.c_int64,
                                  C.c_void_p]),
     "gq_batch_create": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int64, C.c_int32, C.POINTER(C.c_void_p)]),

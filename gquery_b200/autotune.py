@@ -56,6 +56,8 @@ def candidates(kind: str, dim: int, has_wide: bool, exact_stack: int, wide_stack
                     out.append(dict(variant="wide8", persist=1, budget=budget, block=b))
                 out.append(dict(variant="wide8", persist=0, block=b))
         out.append(dict(variant="exact", persist=0, block=128))
+        if has_wide:
+            out.append(dict(variant="wide8", packet=1))  # one ray per group of 8 lanes
     elif kind == "sil":
         if not has_snch:
             return []

@@ -20,7 +20,8 @@ BUILD = ROOT / "_build" / "gq"
 LIB = PKG / "lib" / "libgq.so"
 
 HOST_SOURCES = ["host/scene_build.cpp", "host/flatten.cpp", "capi.cpp", "server.cpp"]
-DEVICE_SOURCES = ["device/queries.cu", "device/traverse.cu", "device/packet.cu", "device/noalloc.cu", "device/batch.cu", "device/gpu_build.cu"]
+DEVICE_SOURCES = ["device/queries.cu", "device/traverse.cu", "device/packet.cu", "device/ray_group.cu",
+                  "device/noalloc.cu", "device/batch.cu", "device/gpu_build.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -1042,6 +1042,16 @@ gq_status gq_scene_load(const char *path, int32_t device, gq_scene **out) {
     return GQ_OK;
 }
 
+gq_status gq_read_probe(const void *buf, int64_t bytes, int32_t reps, uint32_t *sink, void *stream) {
+    if (!buf || !sink) return fail(GQ_ERR_INVALID, "null buffer or sink");
+    if (bytes <= 0 || bytes % 16 != 0 || ((uintptr_t)buf & 15u) != 0)
+        return fail(GQ_ERR_INVALID, "the probe reads a 16-byte aligned buffer of a positive multiple of 16 bytes");
+    if (reps < 1) return fail(GQ_ERR_INVALID, "reps must be >= 1");
+    cudaError_t e = gqd::launch_read_probe(buf, bytes, reps, sink, (cudaStream_t)stream);
+    if (e != cudaSuccess) return fail_cuda(e, "read probe launch");
+    return GQ_OK;
+}
+
 gq_status gq_scene_set_stack_limit(gq_scene *s, int32_t entries) {
     if (!s) return fail(GQ_ERR_INVALID, "null scene");
     if (entries < 0) return fail(GQ_ERR_INVALID, "stack limit must be >= 0");

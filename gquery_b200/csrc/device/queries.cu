@@ -651,6 +651,21 @@ __global__ void k_ray_keys(int mode, float lo0, float lo1, float lo2, float sc0,
     vals[i] = (int32_t)i;
 }
 
+// Bandwidth probe: every thread reads its 16-byte words of the buffer `reps` times
+// with loads that are cached in L2 only, folding them into one word so that the loads
+// cannot be dropped; one word per warp goes to `sink`.
+__global__ void __launch_bounds__(256) k_read_probe(const uint4 *buf, int64_t n16, int reps, unsigned *sink) {
+    unsigned acc = 0;
+    const int64_t step = (int64_t)gridDim.x * blockDim.x;
+    for (int r = 0; r < reps; ++r)
+        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n16; i += step) {
+            const uint4 v = __ldcg(buf + i);
+            acc ^= v.x ^ v.y ^ v.z ^ v.w;
+        }
+    acc = __reduce_xor_sync(0xffffffffu, acc);
+    if ((threadIdx.x & 31u) == 0) atomicXor(sink, acc);
+}
+
 inline dim3 grid_for(int64_t n) { return dim3((unsigned)((n + kBlock - 1) / kBlock)); }
 inline size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
@@ -796,6 +811,14 @@ cudaError_t launch_sil_brute(const DevScene &s, const void *sils, int64_t n_sil,
         k_sil_brute<3><<<grid_for(n), kBlock, 0, st>>>(b, n_sil, x, r_max, n, o);
     else
         k_sil_brute<2><<<grid_for(n), kBlock, 0, st>>>(b, n_sil, x, r_max, n, o);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_read_probe(const void *buf, int64_t bytes, int reps, unsigned *sink, cudaStream_t st) {
+    int dev = 0, n_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    k_read_probe<<<dim3((unsigned)(8 * n_sm)), 256, 0, st>>>((const uint4 *)buf, bytes / 16, reps, sink);
     return cudaGetLastError();
 }
 

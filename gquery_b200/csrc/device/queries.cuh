@@ -56,6 +56,9 @@ inline int block_slot(int block) { return block == 64 ? 0 : block == 128 ? 1 : b
 // (may be null: one query per thread then).
 cudaError_t launch_cp(const DevScene &s, int variant, const Tune &t, gq_vecs q, int64_t n, const int32_t *perm,
                       const gq_cp_out &o, unsigned long long *counter, cudaStream_t st);
+// Rays over the quantised 8-wide BVH, one ray per group of 8 lanes (ray_group.cu).
+cudaError_t launch_ray_group(const DevScene &s, gq_vecs x, gq_vecs v, const float *r_max, int64_t n,
+                             const int32_t *perm, const gq_ray_out &o, unsigned long long *counter, cudaStream_t st);
 cudaError_t launch_ray(const DevScene &s, int variant, const Tune &t, gq_vecs x, gq_vecs v, const float *r_max,
                        int64_t n, const int32_t *perm, const gq_ray_out &o, unsigned long long *counter,
                        cudaStream_t st);
@@ -74,6 +77,8 @@ cudaError_t launch_sil_brute(const DevScene &s, const void *sils, int64_t n_sil,
                              int64_t n, const gq_sil_out &o, cudaStream_t st);
 cudaError_t launch_ray_brute(const DevScene &s, gq_vecs x, gq_vecs v, const float *r_max, int64_t n,
                              const gq_ray_out &o, cudaStream_t st);
+// Reads `bytes` (a multiple of 16) of device memory `reps` times with L2-only loads.
+cudaError_t launch_read_probe(const void *buf, int64_t bytes, int reps, unsigned *sink, cudaStream_t st);
 // FP64 nearest silhouette over raw records (2D: 8 floats, 3D: 16 floats each).
 cudaError_t launch_sil_f64(int dim, const float *recs, int64_t n_sil, gq_vecs x, int64_t n, double *out_d,
                            int32_t *out_id, cudaStream_t st);

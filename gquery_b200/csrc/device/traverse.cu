@@ -141,6 +141,8 @@ cudaError_t launch_ray(const DevScene &s, int variant, const Tune &t, gq_vecs x,
     if (n <= 0) return cudaSuccess;
     const gq_cp_out none{};
     const bool wide = variant == GQ_VARIANT_WIDE8;
+    if (wide && t.packet && counter && n >= 32)  // one ray per group of 8 lanes (ray_group.cu)
+        return launch_ray_group(s, x, v, r_max, n, perm, o, counter, st);
     if (s.dim == 3)
         return wide ? launch_kind<3, true, true>(s, t, x, v, r_max, n, perm, none, o, counter, st)
                     : launch_kind<3, true, false>(s, t, x, v, r_max, n, perm, none, o, counter, st);

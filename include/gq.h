@@ -62,8 +62,9 @@ typedef struct {
     int32_t variant;  /* variant used when a query asks for GQ_VARIANT_AUTO */
     int32_t packet;   /* WIDE8 closest point (3D): 1 = warp-coherent traversal; warp-coherent closest
                          points (COHERENT, and WIDE8 with packet): 2 = the compact stack (keys rounded
-                         down to FP16, one node word per warp; same answers); WARP silhouettes:
-                         switch to the coherent traversal from 2^18 queries on */
+                         down to FP16, one node word per warp; same answers); WIDE8 rays: 1 = one ray
+                         per group of 8 lanes, one child or item per lane; WARP silhouettes: switch
+                         to the coherent traversal from 2^18 queries on */
     int32_t sorted;   /* warp-coherent wide nodes: children in distance order (else nearest first) */
     int32_t persist;  /* per-thread kernels: persistent warps, finished lanes take new queries */
     int32_t budget;   /* node visits between refills */
@@ -261,6 +262,13 @@ gq_status gq_closest_silhouette_brute(const gq_scene *scene, gq_vecs x, const fl
  * directions (kind 1 only). */
 gq_status gq_brute_f64(const gq_scene *scene, int32_t kind /*0 closest point, 1 ray, 2 silhouette*/, gq_vecs a,
                        gq_vecs b, int64_t n, double *out_d, int32_t *out_id, void *stream);
+
+/* Bandwidth probe for the roofline: reads `bytes` (a multiple of 16, 16-byte aligned) of
+ * device memory `reps` times in one launch with 16-byte loads that are cached in L2 only,
+ * and xors what it read into the device word `sink`.  Timed on a buffer that fits in L2 it
+ * gives the L2 read bandwidth, on a larger one the HBM read bandwidth.  No counterpart in
+ * the reference. */
+gq_status gq_read_probe(const void *buf, int64_t bytes, int32_t reps, uint32_t *sink, void *stream);
 
 /* Reads and clears the scene's device error word (stack overflow etc.); synchronises `stream`. */
 gq_status gq_scene_device_error(const gq_scene *scene, void *stream, int32_t *flags);

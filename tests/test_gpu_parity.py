@@ -333,11 +333,14 @@ def test_sil3d_fast_variants_against_oracle_small(mesh_small, variant):
 
 @pytest.mark.parametrize("variant,tuning", [("coherent", dict(stack=0)), ("wide8", dict(packet=1, sorted=0)),
                                             ("wide8", dict(packet=1, sorted=1))])
-def test_compact_stack_bitwise(mesh_c1, variant, tuning):
+def test_compact_stack_same_answers(mesh_c1, variant, tuning):
     """The warp-coherent walks with the compact stack (keys rounded down to FP16, one node
-    word per warp) give the same records as with the plain stack, bit for bit: a key
-    rounded down only admits entries whose triangles are all farther than the lane's
-    radius."""
+    word per warp).  A key rounded down only admits entries whose triangles are all
+    farther than the lane's radius, so no lane's best changes: the binary walk gives the
+    same records bit for bit.  In the 8-wide walk an extra lane that enters a node also
+    takes part in choosing the order of its children, so a query may end on the other
+    triangle of an exact distance tie: validity and distances bit for bit, primitives up
+    to exact ties."""
     q = torch.as_tensor(W.uniform_points(200_000, 3, seed=57)).cuda()
     try:
         mesh_c1.set_tuning("cp", variant, **tuning)
@@ -346,5 +349,37 @@ def test_compact_stack_bitwise(mesh_c1, variant, tuning):
         compact = to_np(mesh_c1.closest_point(q, variant=variant))
     finally:
         mesh_c1.set_tuning("cp", "coherent", packet=1, persist=0)
-    assert_bitwise(compact, plain, CP_FIELDS_3D, f"{variant} compact ")
+    if variant == "coherent":
+        assert_bitwise(compact, plain, CP_FIELDS_3D, "coherent compact ")
+    else:
+        assert_bitwise(compact, plain, ["valid", "d"], f"{variant} compact ")
+        rep = tie_report(compact, plain)
+        assert rep["prim_mismatch"] == rep["prim_mismatch_exact_tie"], rep
     assert mesh_c1.device_error() == 0
+
+
+def test_ray_group_matches_exact(mesh_c1, star):
+    """Rays over the 8-wide nodes with one ray per group of 8 lanes against the exact
+    traversal: the same hits, the same primitive except at FP32 distance ties, and
+    against the per-lane 8-wide traversal."""
+    for scene, dim, fields, n in ((mesh_c1, 3, RAY_FIELDS_3D, 262_144), (star, 2, RAY_FIELDS_2D, 65_536)):
+        o, d = W.rays(n, dim, seed=58 + dim)
+        rm = torch.as_tensor(np.random.default_rng(59).uniform(0.2, 3.0, n).astype(np.float32))
+        for r_max in (math.inf, rm):
+            exact = to_np(scene.intersect(o, d, r_max, variant="exact"))
+            try:
+                scene.set_tuning("ray", "wide8", packet=1)
+                group = to_np(scene.intersect(o, d, r_max, variant="wide8"))
+                scene.set_tuning("ray", "wide8", packet=0)
+                lane = to_np(scene.intersect(o, d, r_max, variant="wide8"))
+            finally:
+                scene.set_tuning("ray", "wide8", packet=0)
+            for other, what in ((exact, "exact"), (lane, "per-lane wide8")):
+                rep = tie_report(group, other)
+                assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0, (dim, what, rep)
+                assert rep["max_rel_d"] <= REL_TOL, (dim, what, rep)
+            same = group["prim_id"] == exact["prim_id"]
+            assert_bitwise({k: np.asarray(v)[..., same] for k, v in group.items()},
+                           {k: np.asarray(v)[..., same] for k, v in exact.items()}, fields, f"{dim}D group ")
+            assert group["valid"].any()
+        assert scene.device_error() == 0

@@ -37,6 +37,12 @@ def queries():
 
 def _call(s, kind, variant, qs):
     q, o, d = qs
+    if variant == "wide8_group":  # one ray per group of 8 lanes
+        s.set_tuning("ray", "wide8", packet=1)
+        try:
+            return to_np(s.intersect(o, d, variant="wide8"))
+        finally:
+            s.set_tuning("ray", "wide8", packet=0)
     if kind == "cp":
         return to_np(s.closest_point(q, variant=variant))
     if kind == "ray":
@@ -57,7 +63,8 @@ def _check_stopped(capped, free, fields, what):
 
 
 @pytest.mark.parametrize("kind,variant", [("cp", "exact"), ("cp", "coherent"), ("cp", "wide8"), ("ray", "exact"),
-                                          ("ray", "wide8"), ("sil", "exact"), ("sil", "coherent")])
+                                          ("ray", "wide8"), ("ray", "wide8_group"), ("sil", "exact"),
+                                          ("sil", "coherent")])
 def test_single_scene_overflow_is_flagged_and_zeroed(mesh, queries, kind, variant):
     mesh.set_stack_limit(0)
     free = _call(mesh, kind, variant, queries)
