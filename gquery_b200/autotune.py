@@ -58,6 +58,8 @@ def candidates(kind: str, dim: int, has_wide: bool, exact_stack: int, wide_stack
         out.append(dict(variant="exact", persist=0, block=128))
         if has_wide:
             out.append(dict(variant="wide8", packet=1))  # one ray per group of 8 lanes
+            for packet in (0, 2):  # per lane; 2: while-while scheduling
+                out.append(dict(variant="wide8", packet=packet, sorted=0, persist=1, budget=32))  # nearest first
     elif kind == "sil":
         if not has_snch:
             return []

@@ -88,11 +88,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_trav_persist(DevScene s, gq_vecs 
     }
 }
 
-template <int D, bool RAY, bool WIDE>
-cudaError_t launch_kind(const DevScene &s, const Tune &t, gq_vecs a, gq_vecs b, const float *rmax, int64_t n,
-                        const int32_t *perm, const gq_cp_out &oc, const gq_ray_out &orr, unsigned long long *counter,
-                        cudaStream_t st) {
-    constexpr int CFG = 0;
+template <int D, bool RAY, bool WIDE, int CFG>
+cudaError_t launch_cfg(const DevScene &s, const Tune &t, gq_vecs a, gq_vecs b, const float *rmax, int64_t n,
+                       const int32_t *perm, const gq_cp_out &oc, const gq_ray_out &orr, unsigned long long *counter,
+                       cudaStream_t st) {
     int slot = block_slot(t.block), block = t.block;
     if (slot < 0) slot = 1, block = 128;
     if (t.persist && counter && n > 4096) {
@@ -114,6 +113,23 @@ cudaError_t launch_kind(const DevScene &s, const Tune &t, gq_vecs a, gq_vecs b, 
             <<<dim3((unsigned)((n + block - 1) / block)), block, 0, st>>>(s, a, b, rmax, n, perm, oc, orr);
     }
     return cudaGetLastError();
+}
+
+// Per-lane traversal configuration.  Rays over the 8-wide nodes may take the nearest hit
+// child first with the other hits pushed in child order (tuning sorted = 0) instead of
+// sorting all hits by entry distance, and while-while scheduling (packet = 2).
+template <int D, bool RAY, bool WIDE>
+cudaError_t launch_kind(const DevScene &s, const Tune &t, gq_vecs a, gq_vecs b, const float *rmax, int64_t n,
+                        const int32_t *perm, const gq_cp_out &oc, const gq_ray_out &orr, unsigned long long *counter,
+                        cudaStream_t st) {
+    if constexpr (RAY && WIDE) {
+        const bool minfirst = !t.sorted, ww = t.packet == 2;
+        if (minfirst && ww)
+            return launch_cfg<D, RAY, WIDE, CFG_MINFIRST | CFG_WW>(s, t, a, b, rmax, n, perm, oc, orr, counter, st);
+        if (minfirst) return launch_cfg<D, RAY, WIDE, CFG_MINFIRST>(s, t, a, b, rmax, n, perm, oc, orr, counter, st);
+        if (ww) return launch_cfg<D, RAY, WIDE, CFG_WW>(s, t, a, b, rmax, n, perm, oc, orr, counter, st);
+    }
+    return launch_cfg<D, RAY, WIDE, 0>(s, t, a, b, rmax, n, perm, oc, orr, counter, st);
 }
 
 }  // namespace
@@ -141,7 +157,7 @@ cudaError_t launch_ray(const DevScene &s, int variant, const Tune &t, gq_vecs x,
     if (n <= 0) return cudaSuccess;
     const gq_cp_out none{};
     const bool wide = variant == GQ_VARIANT_WIDE8;
-    if (wide && t.packet && counter && n >= 32)  // one ray per group of 8 lanes (ray_group.cu)
+    if (wide && t.packet == 1 && counter && n >= 32)  // one ray per group of 8 lanes (ray_group.cu)
         return launch_ray_group(s, x, v, r_max, n, perm, o, counter, st);
     if (s.dim == 3)
         return wide ? launch_kind<3, true, true>(s, t, x, v, r_max, n, perm, none, o, counter, st)
