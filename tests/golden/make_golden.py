@@ -9,9 +9,11 @@ stand-in applies this project's fixed rules, the same as the kernels and the ora
 
     python tests/golden/make_golden.py <gQuery checkout>      (or GQ_REFERENCE=<checkout>)
 
-Writes golden_<case>.npz: scene, queries and the reference's record fields, and
+Writes golden_<case>.npz: scene, queries and the reference's record fields;
 baseline_<case>.npz: the records of the reference's brute-force methods
-(Polyline/Mesh closest_point_baseline and intersect_baseline, Polyline.intersect).
+(Polyline/Mesh closest_point_baseline and intersect_baseline, Polyline.intersect); and
+deep_<case>.npz: the traversals on deep trees (scenes named by their generator in
+gquery_b200.workloads and a checksum of the generated arrays).
 """
 from __future__ import annotations
 
@@ -179,9 +181,56 @@ def baselines():
         baseline_3d(name, v, f, q, o, d, _rmax(96, 607))
 
 
+def geometry_checksum(v, ix):
+    """sha256 of the float32 vertices and int32 indices (the deep fixtures store the
+    generator of their scene and this checksum instead of the arrays)."""
+    import hashlib
+    h = hashlib.sha256(np.ascontiguousarray(v, np.float32).tobytes())
+    h.update(np.ascontiguousarray(ix, np.int32).tobytes())
+    return h.hexdigest()
+
+
+DEEP = {  # name: (generator in gquery_b200.workloads, keyword arguments)
+    "c2_icosphere7": ("config2_mesh", {}),
+    "star262144": ("star_polyline", {"n": 262144, "seed": 1}),
+}
+
+
+def deep_cases(nq=256):
+    """The reference's traversal on deep trees: the 327,680-triangle mesh of the
+    silhouette workload (tree depth 25) and a 262,144-segment star (depth 29)."""
+    from drjit_scalar import Array2i, Array3i
+    for name, (gen, kw) in DEEP.items():
+        v, ix = getattr(W, gen)(**kw)
+        dim = v.shape[1]
+        q = W.uniform_points(nq, dim, seed=710)
+        o, d = W.rays(nq, dim, seed=711)
+        rmax_sil = np.float32(np.inf) if dim == 3 else np.float32(0.5)
+        if dim == 3:
+            V, F = soa(v, Array3), soa(ix, Array3i)
+            bvh, snch = BVH3D(V, F), SNCH3D(V, F)
+            cpf, rayf = ["valid", "p", "n", "uv", "d", "prim_id"], ["valid", "p", "n", "uv", "d", "prim_id", "on_boundary"]
+        else:
+            V, F = soa(v, Array2), soa(ix, Array2i)
+            bvh, snch = BVH(V, F), SNCH(V, F)
+            cpf, rayf = ["valid", "p", "n", "t", "d", "prim_id"], ["valid", "p", "n", "t", "d", "prim_id", "on_boundary"]
+        cp = run(bvh.closest_point, [(vec(p),) for p in q], cpf)
+        ray = run(bvh.intersect, [(vec(a), vec(b), Float(dr.inf)) for a, b in zip(o, d)], rayf)
+        sil = run(snch.closest_silhouette, [(vec(p), Float(rmax_sil)) for p in q], ["valid", "p", "d", "prim_id"])
+        np.savez_compressed(HERE / f"deep_{name}.npz", dim=dim, generator=gen, params=str(sorted(kw.items())),
+                            checksum=geometry_checksum(v, ix), q=q, o=o, d=d, rmax_sil=rmax_sil,
+                            **{f"cp_{k}": x for k, x in cp.items()}, **{f"ray_{k}": x for k, x in ray.items()},
+                            **{f"sil_{k}": x for k, x in sil.items()})
+        print("deep", name, "cp valid", cp["valid"].mean(), "ray valid", ray["valid"].mean(),
+              "sil valid", sil["valid"].mean())
+
+
 def main():
     if "--baselines-only" in sys.argv:
         baselines()
+        return
+    if "--deep-only" in sys.argv:
+        deep_cases()
         return
     # README pentagon (examples/example_2d.py) and tetrahedron (examples/example_3d.py)
     pv = np.array([[0.0, 0.0], [1.0, 0.0], [1.5, 1.0], [0.5, 1.5], [-0.5, 1.0]], np.float32)
@@ -210,6 +259,7 @@ def main():
     o, d = W.rays(300, 3, seed=508)
     case_3d("icosphere2", iv, iff, q, o, d, np.inf)
     baselines()
+    deep_cases()
 
 
 if __name__ == "__main__":

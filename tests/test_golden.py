@@ -107,3 +107,52 @@ def test_brute_kernels_match_reference_baselines(path):
         got = shape.intersect(torch.as_tensor(z["o"]).cuda(), z["d"], torch.as_tensor(z["n"]).cuda(),
                               torch.as_tensor(z["on_boundary"]).cuda(), torch.as_tensor(z["rmax"]))
         assert_bitwise(to_np(got), expected(z, "off", RAY[dim]), RAY[dim], "Polyline.intersect ")
+
+
+# ---------------------------------------------------------------- deep trees
+
+DEEP = sorted((Path(__file__).resolve().parent / "golden").glob("deep_*.npz"))
+
+
+def _deep_scene(z, device):
+    """The fixture's scene, regenerated by its generator; skipped when the regenerated
+    arrays do not match the checksum recorded with the fixture."""
+    import ast
+    import hashlib
+    from gquery_b200 import workloads as W
+    v, ix = getattr(W, str(z["generator"]))(**dict(ast.literal_eval(str(z["params"]))))
+    h = hashlib.sha256(np.ascontiguousarray(v, np.float32).tobytes())
+    h.update(np.ascontiguousarray(ix, np.int32).tobytes())
+    if h.hexdigest() != str(z["checksum"]):
+        pytest.skip("the scene generator does not reproduce the fixture's geometry on this machine")
+    return Scene(v, ix, int(z["dim"]), device=device)
+
+
+def test_deep_fixtures_exist():
+    assert {"deep_c2_icosphere7", "deep_star262144"} <= {p.stem for p in DEEP}
+
+
+@pytest.mark.parametrize("path", DEEP, ids=[p.stem for p in DEEP])
+def test_oracle_matches_reference_traversal_deep(path):
+    dim, z = load(path)
+    s = _deep_scene(z, None)
+    nodes, prims = s.ref_array(L.ARRAY_BVH_NODES), s.ref_array(L.ARRAY_PRIMITIVES)
+    snodes, sils = s.ref_array(L.ARRAY_SNCH_NODES), s.ref_array(L.ARRAY_SILHOUETTES)
+    rmax = float(z["rmax_sil"])
+    assert_bitwise(oracle.closest_point(dim, nodes, prims, z["q"]), expected(z, "cp", CP[dim]), CP[dim], "cp ")
+    assert_bitwise(oracle.intersect(dim, nodes, prims, z["o"], z["d"]), expected(z, "ray", RAY[dim]), RAY[dim],
+                   "ray ")
+    got = oracle.closest_silhouette(dim, snodes, sils, z["q"], None if np.isinf(rmax) else rmax)
+    assert_bitwise(got, expected(z, "sil", SIL), SIL, "sil ")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", DEEP, ids=[p.stem for p in DEEP])
+def test_exact_kernels_match_reference_traversal_deep(path):
+    dim, z = load(path)
+    s = _deep_scene(z, 0)
+    rmax = float(z["rmax_sil"])
+    assert_bitwise(to_np(s.closest_point(z["q"], variant="exact")), expected(z, "cp", CP[dim]), CP[dim], "cp ")
+    assert_bitwise(to_np(s.intersect(z["o"], z["d"], variant="exact")), expected(z, "ray", RAY[dim]), RAY[dim],
+                   "ray ")
+    assert_bitwise(to_np(s.closest_silhouette(z["q"], rmax, variant="exact")), expected(z, "sil", SIL), SIL, "sil ")
