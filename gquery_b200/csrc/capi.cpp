@@ -143,6 +143,7 @@ gq_status build_on_device(gq_scene *s, const gq_build_opts &o) {
         d.sroot_ref = s->np > 1 ? 0 : ~0;  // a single primitive: its leaf, records 0..D-1
         s->has_snch = true;
         s->n_sil = D * s->np;
+        d.n_sils = s->n_sil;
         s->image_bytes[4] = s->np > 1 ? spair_bytes : 0;
         s->image_bytes[5] = sil_bytes;
     }
@@ -241,6 +242,7 @@ gq_status build_scene(const float *vertices, int64_t nv, const int32_t *prims, i
     default_tuning(s.get());
     s->n_wide = (int64_t)img.wnodes.size();
     s->n_sil = (int64_t)img.sils.size();
+    s->dev.n_sils = s->n_sil;
     gqd::DevScene &d = s->dev;
     d.dim = D;
     for (int k = 0; k < 3; ++k) {
@@ -992,6 +994,7 @@ gq_status gq_scene_load(const char *path, int32_t device, gq_scene **out) {
     s->n_nodes = h.n_nodes;
     s->n_wide = h.n_wide;
     s->n_sil = h.n_sil;
+    s->dev.n_sils = h.n_sil;
     s->trees_ready = false;
     s->gpu_built = h.gpu_built != 0;
     try {

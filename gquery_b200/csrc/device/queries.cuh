@@ -20,6 +20,7 @@ struct DevScene {
     int32_t wroot_ref;
     const void *spairs;  // gq_spair2_t / gq_spair3_t (may be null)
     const void *sils;    // gq_silv_t / gq_sile_t
+    int64_t n_sils = 0;  // records in sils
     int32_t sroot_ref;
     const float *verts;  // original vertices [nv][D] (brute force)
     const int32_t *index;  // original primitives [np][D]
