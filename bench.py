@@ -620,6 +620,7 @@ def summary(line):
             x = x[k]
         return x
     s = {"mqps": {"plain_exact": line.get("plain_exact_mqps"), "quantised_wide8": line.get("quantised_wide8_mqps"),
+                  "quantised_wide16": line.get("quantised_wide16_mqps"),
                   "tuned": line.get("value"), "e2e": get("e2e", "value"),
                   "cpu_port": get("cpu_baseline", "value")},
          "quantised_wide8_vs_plain": line.get("quantised_wide8_vs_plain"), "tuned_vs_plain": line.get("tuned_vs_plain"),
@@ -666,7 +667,7 @@ def main():
 
     n = args.n
     V, F = W.config1_mesh()
-    scene = Scene(V, F, 3, device=local, build_snch=False, build_wide=True)
+    scene = Scene(V, F, 3, device=local, build_snch=False, build_wide=2)  # 8- and 16-bit child bounds
     # disjoint query shards per rank (weak scaling)
     q_h = W.uniform_points(n, 3, seed=shard_seed(1, rank))
     o_h, d_h = W.rays(n, 3, seed=shard_seed(2, rank))
@@ -727,10 +728,21 @@ def main():
         return res, clk
 
     if args.no_compare:
-        plain = quant = None
+        plain = quant = quant16 = None
     else:
+        saved = {k: scene.get_tuning(k) for k in ("cp", "ray")}
         plain, _ = timed("exact", max(2, args.steps // 2), 2)
+        # each quantised form in its fastest measured configuration: 8-bit closest points
+        # warp-coherent (nearest child first), 16-bit ones and all rays one lane per query
+        scene.set_tuning("cp", "wide8", packet=1, sorted=0)
+        scene.set_tuning("ray", "wide8", packet=0, sorted=1, persist=1)
         quant, _ = timed("wide8", max(2, args.steps // 2), 2)
+        scene.set_tuning("cp", "wide16", persist=1)
+        scene.set_tuning("ray", "wide16", persist=1)
+        quant16, _ = timed("wide16", max(2, args.steps // 2), 2)
+        for k, t in saved.items():
+            scene.set_tuning(k, t["variant"], **{f: t[f] for f in ("packet", "sorted", "persist", "budget", "block",
+                                                                  "stack")})
     tuning_report = None
     if args.variant == "auto" and not args.no_autotune:
         # the project's autotuner picks node width, stack depth and block shape on this
@@ -755,7 +767,7 @@ def main():
         scene.intersect(o, d, variant="exact", out=ex_ray)
         parity = {"note": "answers on all queries of this rank against the exact traversal (gQuery's visit "
                           "order); ties: exact = the same FP32 distance, loose = within 2e-6 relative"}
-        for name, variant in (("quantised_wide8", "wide8"), ("tuned", args.variant)):
+        for name, variant in (("quantised_wide8", "wide8"), ("quantised_wide16", "wide16"), ("tuned", args.variant)):
             scene.closest_point(q, variant=variant, out=cp_out)
             scene.intersect(o, d, variant=variant, out=ray_out)
             parity[name] = {"cp": tie_stats(cp_out, ex_cp), "ray": tie_stats(ray_out, ex_ray)}
@@ -781,6 +793,7 @@ def main():
     value = total_q / (main_res["step_ms"] / 1e3) / 1e6
     plain_value = total_q / (plain["step_ms"] / 1e3) / 1e6 if plain else None
     quant_value = total_q / (quant["step_ms"] / 1e3) / 1e6 if quant else None
+    quant16_value = total_q / (quant16["step_ms"] / 1e3) / 1e6 if quant16 else None
 
     # ---- end to end through the public API with host buffers ----
     # Every step copies its inputs from pinned host memory, answers them and copies every
@@ -917,12 +930,17 @@ def main():
             "quantised_wide8": quant and {"value": quant_value, "ms_per_step": quant["step_ms"],
                                           "cp_ms": quant["cp_ms"], "ray_ms": quant["ray_ms"],
                                           "vs_plain": quant_value / plain_value},
+            "quantised_wide16": quant16 and {"value": quant16_value, "ms_per_step": quant16["step_ms"],
+                                             "cp_ms": quant16["cp_ms"], "ray_ms": quant16["ray_ms"],
+                                             "vs_plain": quant16_value / plain_value},
             "tuned": {"cp": scene.get_tuning("cp"), "ray": scene.get_tuning("ray"),
                       "vs_plain": value / plain_value if plain else None, "autotune": tuning_report},
             "breakdown_ms": {k: main_res[k] for k in ("order_cp_ms", "cp_ms", "order_ray_ms", "ray_ms",
                                                       "wall_ms_per_step")},
             "plain_exact_mqps": plain_value, "quantised_wide8_mqps": quant_value,
+            "quantised_wide16_mqps": quant16_value,
             "quantised_wide8_vs_plain": quant_value / plain_value if plain else None,
+            "quantised_wide16_vs_plain": quant16_value / plain_value if plain else None,
             "tuned_vs_plain": value / plain_value if plain else None,
             "parity": parity, "fp64_error": fp64,
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,

@@ -24,6 +24,7 @@ VARIANT_WIDE8 = 1
 VARIANT_AUTO = 2
 VARIANT_COHERENT = 3
 VARIANT_WARP = 4
+VARIANT_WIDE16 = 5
 
 KIND_CLOSEST_POINT = 0
 KIND_INTERSECT = 1
@@ -37,6 +38,7 @@ ARRAY_RAW_SILHOUETTES = 4
 ARRAY_WIDE_NODES = 5
 ARRAY_SNCH_PAIRS = 6
 ARRAY_SIL_RECORDS = 7
+ARRAY_WIDE16_BOUNDS = 8
 
 DEVERR_STACK = 1
 

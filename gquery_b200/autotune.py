@@ -30,7 +30,7 @@ KINDS = ("cp", "ray", "sil")
 
 
 def candidates(kind: str, dim: int, has_wide: bool, exact_stack: int, wide_stack: int,
-               has_snch: bool = True) -> List[dict]:
+               has_snch: bool = True, has_wide16: bool = False) -> List[dict]:
     """Launch configurations worth timing for one query kind of one scene."""
     out: List[dict] = []
     blocks = (64, 128, 256)
@@ -48,7 +48,13 @@ def candidates(kind: str, dim: int, has_wide: bool, exact_stack: int, wide_stack
                     for packet in (1, 2):  # 2: the compact stack
                         out.append(dict(variant="wide8", packet=packet, sorted=1, block=b))
                         out.append(dict(variant="wide8", packet=packet, sorted=0, block=b))
+        if has_wide16:
+            for b in blocks:
+                out.append(dict(variant="wide16", persist=1, budget=32, block=b))
     elif kind == "ray":
+        if has_wide16:
+            for b in blocks:
+                out.append(dict(variant="wide16", persist=1, budget=32, block=b))
         for b in blocks:
             out.append(dict(variant="exact", persist=1, budget=32, block=b))
             if has_wide:
@@ -188,7 +194,7 @@ def tune(scene, kind: str, inputs: Sequence, *, cands: Optional[List[dict]] = No
             return TuneResult(kind, hit, [], True)
     if cands is None:
         cands = candidates(kind, scene.dim, info["n_wide_nodes"] > 0, info["exact_stack"], info["wide_stack"],
-                           info["n_silhouettes"] > 0)
+                           info["n_silhouettes"] > 0, getattr(scene, "has_wide16", False))
     saved = scene.get_tuning(kind)
     ref = None
     if verify:

@@ -208,8 +208,9 @@ gq_status build_scene(const float *vertices, int64_t nv, const int32_t *prims, i
         BvhTree<D> tree = build_bvh<D>(src, o.max_prims_in_node, nt);
         flatten_bvh<D>(src, tree, img);
         if (o.build_wide) {
-            flatten_wide<D>(tree, img);
+            flatten_wide<D>(tree, img, o.build_wide >= 2);
             s->has_wide = true;
+            s->has_wide16 = o.build_wide >= 2;
         }
         if (o.build_snch) {
             SnchTree<D> sn = build_snch<D>(src, tree, nt);
@@ -255,6 +256,7 @@ gq_status build_scene(const float *vertices, int64_t nv, const int32_t *prims, i
             if (bytes) std::memcpy(dst.data(), src, bytes);
         };
         keep(s->wide_words, img.wnodes.data(), img.wnodes.size() * sizeof(img.wnodes[0]));
+        keep(s->wide16_words, img.wq16.data(), img.wq16.size() * sizeof(img.wq16[0]));
         keep(s->spair_words, img.spairs.data(), img.spairs.size() * sizeof(img.spairs[0]));
         keep(s->sil_words, img.sils.data(), img.sils.size() * sizeof(img.sils[0]));
         *out = s.release();
@@ -269,6 +271,7 @@ gq_status build_scene(const float *vertices, int64_t nv, const int32_t *prims, i
     if ((st = s->upload(img.spheres, &psph)) != GQ_OK) return st;
     d.spheres = (const gq_tsph_t *)psph;
     if ((st = s->upload(img.wnodes, &d.wnodes)) != GQ_OK) return st;
+    if ((st = s->upload(img.wq16, &d.wq16)) != GQ_OK) return st;
     if ((st = s->upload(img.spairs, &d.spairs)) != GQ_OK) return st;
     if ((st = s->upload(img.sils, &d.sils)) != GQ_OK) return st;
     const void *pv = nullptr, *pi = nullptr, *pe = nullptr;
@@ -344,7 +347,7 @@ gqd::Tune to_tune(const gq_scene *s, int kind, int variant) {
     r.persist = t.persist;
     r.budget = t.budget > 0 ? t.budget : 32;
     r.block = t.block > 0 ? t.block : 128;
-    const int need = variant == GQ_VARIANT_WIDE8 ? s->wide_stack : s->exact_stack;
+    const int need = (variant == GQ_VARIANT_WIDE8 || variant == GQ_VARIANT_WIDE16) ? s->wide_stack : s->exact_stack;
     r.stack = (t.stack == 32 && need <= 32) ? 32 : 0;
     return r;
 }
@@ -354,6 +357,7 @@ int resolve_variant(const gq_scene *s, const gq_query_opts *opts, int kind) {
     if (v == GQ_VARIANT_AUTO) {
         v = s->tune[kind].variant;
         if (v == GQ_VARIANT_WIDE8 && !s->has_wide) v = GQ_VARIANT_EXACT;
+        if (v == GQ_VARIANT_WIDE16 && !s->has_wide16) v = GQ_VARIANT_EXACT;
     }
     return v;
 }
@@ -362,8 +366,10 @@ gq_status check_variant(const gq_scene *s, int v) {
     if (v == GQ_VARIANT_COHERENT) {
         if (s->exact_stack > GQ_STACK_EXACT)
             return fail(GQ_ERR_DEPTH, "tree deeper than the 64-entry traversal stack");
-    } else if (v == GQ_VARIANT_WIDE8) {
+    } else if (v == GQ_VARIANT_WIDE8 || v == GQ_VARIANT_WIDE16) {
         if (!s->has_wide) return fail(GQ_ERR_UNSUPPORTED, "scene was built without the wide BVH");
+        if (v == GQ_VARIANT_WIDE16 && !s->has_wide16)
+            return fail(GQ_ERR_UNSUPPORTED, "scene was built without the 16-bit child bounds (build_wide = 2)");
         if (s->wide_stack > GQ_STACK_WIDE) return fail(GQ_ERR_DEPTH, "wide tree needs a deeper stack than 96");
     } else if (v == GQ_VARIANT_EXACT) {
         if (s->exact_stack > GQ_STACK_EXACT)
@@ -481,8 +487,10 @@ gq_status gq_scene_free(gq_scene *scene) {
 gq_status gq_scene_set_tuning(gq_scene *s, int32_t kind, const gq_tuning *t) {
     if (!s || !t) return fail(GQ_ERR_INVALID, "null argument");
     if (kind < 0 || kind > 2) return fail(GQ_ERR_INVALID, "unknown query kind");
-    if (t->variant < 0 || t->variant > 4 || t->variant == GQ_VARIANT_AUTO)
-        return fail(GQ_ERR_INVALID, "tuning variant must be EXACT, WIDE8, COHERENT or WARP");
+    if (t->variant < 0 || t->variant > 5 || t->variant == GQ_VARIANT_AUTO)
+        return fail(GQ_ERR_INVALID, "tuning variant must be EXACT, WIDE8, COHERENT, WARP or WIDE16");
+    if (t->variant == GQ_VARIANT_WIDE16 && (kind == GQ_KIND_SILHOUETTE || !s->has_wide16))
+        return fail(GQ_ERR_UNSUPPORTED, "WIDE16 answers closest points and rays of scenes built with build_wide = 2");
     if (t->variant == GQ_VARIANT_WARP && kind != GQ_KIND_SILHOUETTE)
         return fail(GQ_ERR_INVALID, "the WARP variant answers silhouette queries only");
     if (t->variant == GQ_VARIANT_WIDE8 && !s->has_wide) return fail(GQ_ERR_UNSUPPORTED, "scene has no wide BVH");
@@ -524,11 +532,13 @@ gq_status gq_scene_get_info(const gq_scene *s, gq_scene_info *info) {
 gq_status gq_scene_ref_array(const gq_scene *s, int32_t which, float *dst, int64_t cap, int64_t *len) {
     if (!s || !len) return fail(GQ_ERR_INVALID, "null argument");
     std::vector<float> v;
-    if (which == GQ_ARRAY_WIDE_NODES || which == GQ_ARRAY_SNCH_PAIRS || which == GQ_ARRAY_SIL_RECORDS) {
+    if (which == GQ_ARRAY_WIDE_NODES || which == GQ_ARRAY_SNCH_PAIRS || which == GQ_ARRAY_SIL_RECORDS ||
+        which == GQ_ARRAY_WIDE16_BOUNDS) {
         if (s->device >= 0) return fail(GQ_ERR_UNSUPPORTED, "device record dumps are kept for host-only scenes");
-        const std::vector<float> &w = which == GQ_ARRAY_WIDE_NODES   ? s->wide_words
-                                      : which == GQ_ARRAY_SNCH_PAIRS ? s->spair_words
-                                                                     : s->sil_words;
+        const std::vector<float> &w = which == GQ_ARRAY_WIDE_NODES     ? s->wide_words
+                                      : which == GQ_ARRAY_SNCH_PAIRS   ? s->spair_words
+                                      : which == GQ_ARRAY_WIDE16_BOUNDS ? s->wide16_words
+                                                                       : s->sil_words;
         *len = (int64_t)w.size();
         if (dst && cap > 0) std::memcpy(dst, w.data(), sizeof(float) * (size_t)std::min<int64_t>(cap, *len));
         return GQ_OK;

@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(kMaxBlock, 4) k_sil_packet(DevScene s, gq_vecs
 
 // One query per warp (sil_warp.cuh): persistent warps take the next query of the
 // sorted order; the stack lives in dynamic shared memory (kWarpStack entries per warp).
-template <int D, bool COOP = false>
+template <int D>
 __global__ void __launch_bounds__(kMaxBlock, 4) k_sil_warp(DevScene s, gq_vecs xq, const float *rmax_in, int64_t n,
                                                      const int32_t *perm, gq_sil_out o, unsigned long long *counter) {
     extern __shared__ int2 wstk[];
@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(kMaxBlock, 4) k_sil_warp(DevScene s, gq_vecs x
 #pragma unroll
         for (int k = 0; k < D; ++k) x[k] = qget(xq, qi, k);
         snch::Lane<D> L;
-        wsil::closest_silhouette<D, COOP>(s, x, rmax_in ? rmax_in[qi] : kInf, L, stk);
+        wsil::closest_silhouette<D>(s, x, rmax_in ? rmax_in[qi] : kInf, L, stk);
         if (lane == 0) sil_write<D>(s, L, qi, n, o);
     }
 }
@@ -724,14 +724,11 @@ cudaError_t launch_sil(const DevScene &s, int variant, const Tune &t, gq_vecs x,
     if (slot < 0) slot = 1, block = 128;
     if (variant == GQ_VARIANT_WARP && counter) {
         const size_t smem = (size_t)(block / 32) * wsil::kWarpStack * sizeof(int2);
-        // sorted = 0: leaves scanned by the whole warp (sil_warp.cuh COOP)
-        const int ci = t.sorted ? 0 : 1;
         using Fn = void (*)(DevScene, gq_vecs, const float *, int64_t, const int32_t *, gq_sil_out,
                             unsigned long long *);
-        const Fn fn = s.dim == 3 ? (ci ? k_sil_warp<3, true> : k_sil_warp<3, false>)
-                                 : (ci ? k_sil_warp<2, true> : k_sil_warp<2, false>);
-        static int wb[2][2][3] = {}, w_sm = 0;
-        if (!wb[ci][di][slot]) {
+        const Fn fn = s.dim == 3 ? k_sil_warp<3> : k_sil_warp<2>;
+        static int wb[2][3] = {}, w_sm = 0;
+        if (!wb[di][slot]) {
             int dev = 0, b = 0;
             cudaGetDevice(&dev);
             cudaDeviceGetAttribute(&w_sm, cudaDevAttrMultiProcessorCount, dev);
@@ -739,9 +736,9 @@ cudaError_t launch_sil(const DevScene &s, int variant, const Tune &t, gq_vecs x,
             const int most = (kMaxBlock / 32) * wsil::kWarpStack * (int)sizeof(int2);
             cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (const void *)fn, block, smem);
-            wb[ci][di][slot] = b < 1 ? 1 : b;
+            wb[di][slot] = b < 1 ? 1 : b;
         }
-        const int64_t want = std::min<int64_t>((int64_t)wb[ci][di][slot] * w_sm, (n * 32 + block - 1) / block);
+        const int64_t want = std::min<int64_t>((int64_t)wb[di][slot] * w_sm, (n * 32 + block - 1) / block);
         cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
         if (e != cudaSuccess) return e;
         fn<<<dim3((unsigned)want), block, smem, st>>>(s, x, r_max, n, perm, o, counter);

@@ -17,6 +17,7 @@ struct DevScene {
     int32_t root_ref;
     float root_lo[3], root_hi[3];
     const void *wnodes;  // gq_wnode2_t / gq_wnode3_t (may be null)
+    const void *wq16 = nullptr;  // gq_wq16_2_t / gq_wq16_3_t: 16-bit bounds of the same nodes (may be null)
     int32_t wroot_ref;
     const void *spairs;  // gq_spair2_t / gq_spair3_t (may be null)
     const void *sils;    // gq_silv_t / gq_sile_t

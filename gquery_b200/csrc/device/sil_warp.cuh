@@ -41,22 +41,9 @@ __device__ __forceinline__ void warp_argmin(float v, float &m, int &who) {
     who = __ffs(hit) - 1;
 }
 
-// Whether silhouette record j is the last of its leaf.
-template <int D>
-__device__ __forceinline__ bool item_last(const DevScene &s, int64_t j) {
-    if (D == 2) return fbits(ldg4(s.sils, 2 * j + 1).w) & GQ_ITEM_LAST;
-    return fbits(ldg4(s.sils, 4 * j + 3).y) & GQ_ITEM_LAST;
-}
-
 // All 32 lanes call with the same query (x, r_max); stk: this warp's kWarpStack entries
 // of shared memory.  On return every lane holds the answer in L (found, bp, bd, bid, ovf).
-// COOP: the leaves a step takes are scanned by the whole warp, one leaf at a time, lane l
-// testing the leaf's l-th silhouette (and the (l+32)-th, ... for longer leaves), before
-// the lanes that took interior nodes test their children against the warp's new r_max.
-// Each lane keeps what it accepts under the reference's rule (valid and d < its r_max);
-// within a leaf the lowest lane among equal distances wins at the end, which is the
-// leaf order of the per-lane scan.  Without COOP each lane scans its own leaf.
-template <int D, bool COOP = false>
+template <int D>
 __device__ __forceinline__ void closest_silhouette(const DevScene &s, const float *x, float r_max, snch::Lane<D> &L,
                                                    int2 *stk) {
     const unsigned lane = threadIdx.x & 31u;
@@ -94,30 +81,7 @@ __device__ __forceinline__ void closest_silhouette(const DevScene &s, const floa
         L.r = R;
         int2 push0 = make_int2(0, 0), push1 = make_int2(0, 0);  // the lane's entries, push1 on top
         int np = 0;
-        if (COOP) {
-            const bool leaf = mine && __int_as_float(e.y) <= R && e.x < 0 && e.x != INT32_MIN;
-            unsigned lm = __ballot_sync(0xffffffffu, leaf);
-            while (lm) {
-                const int src = __ffs(lm) - 1;
-                lm &= lm - 1u;
-                int64_t first = ~(int64_t)__shfl_sync(0xffffffffu, e.x, src);
-                for (;;) {
-                    const int64_t j = first + (int64_t)lane;
-                    const bool in = j < s.n_sils;
-                    const unsigned lb = __ballot_sync(0xffffffffu, !in || item_last<D>(s, j));
-                    const int upto = lb ? __ffs(lb) - 1 : 31;  // lanes past the leaf's last record drop out
-                    if (in && (int)lane <= upto) snch::test_silhouette<D>(s, L, (int)j);
-                    if (lb) break;
-                    first += 32;
-                }
-            }
-            // interior nodes against the warp's r_max after the leaves
-            float m;
-            int who;
-            warp_argmin(L.r, m, who);
-            L.r = m;
-        }
-        if (mine && __int_as_float(e.y) <= R && !(COOP && e.x < 0)) {
+        if (mine && __int_as_float(e.y) <= R) {
             if (e.x < 0) {
                 if (e.x != INT32_MIN)
                     for (int j = ~e.x;; ++j)

@@ -121,7 +121,10 @@ cudaError_t launch_cfg(const DevScene &s, const Tune &t, gq_vecs a, gq_vecs b, c
 template <int D, bool RAY, bool WIDE>
 cudaError_t launch_kind(const DevScene &s, const Tune &t, gq_vecs a, gq_vecs b, const float *rmax, int64_t n,
                         const int32_t *perm, const gq_cp_out &oc, const gq_ray_out &orr, unsigned long long *counter,
-                        cudaStream_t st) {
+                        cudaStream_t st, bool q16 = false) {
+    if constexpr (WIDE) {  // 16-bit child bounds
+        if (q16) return launch_cfg<D, RAY, WIDE, CFG_Q16>(s, t, a, b, rmax, n, perm, oc, orr, counter, st);
+    }
     if constexpr (RAY && WIDE) {
         const bool minfirst = !t.sorted, ww = t.packet == 2;
         if (minfirst && ww)
@@ -138,16 +141,17 @@ cudaError_t launch_cp(const DevScene &s, int variant, const Tune &t, gq_vecs q, 
                       const gq_cp_out &o, unsigned long long *counter, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
     const gq_ray_out none{};
-    const bool wide = variant == GQ_VARIANT_WIDE8;
+    const bool q16 = variant == GQ_VARIANT_WIDE16;
+    const bool wide = variant == GQ_VARIANT_WIDE8 || q16;
     if (counter && n >= 32) {
         if (variant == GQ_VARIANT_COHERENT) return launch_cp_packet(s, 0, t, q, n, perm, o, counter, st);
-        if (wide && t.packet && s.dim == 3)
+        if (variant == GQ_VARIANT_WIDE8 && t.packet && s.dim == 3)
             return launch_cp_packet(s, t.sorted ? 1 : 2, t, q, n, perm, o, counter, st);
     }
     if (s.dim == 3)
-        return wide ? launch_kind<3, false, true>(s, t, q, q, nullptr, n, perm, o, none, counter, st)
+        return wide ? launch_kind<3, false, true>(s, t, q, q, nullptr, n, perm, o, none, counter, st, q16)
                     : launch_kind<3, false, false>(s, t, q, q, nullptr, n, perm, o, none, counter, st);
-    return wide ? launch_kind<2, false, true>(s, t, q, q, nullptr, n, perm, o, none, counter, st)
+    return wide ? launch_kind<2, false, true>(s, t, q, q, nullptr, n, perm, o, none, counter, st, q16)
                 : launch_kind<2, false, false>(s, t, q, q, nullptr, n, perm, o, none, counter, st);
 }
 
@@ -156,13 +160,14 @@ cudaError_t launch_ray(const DevScene &s, int variant, const Tune &t, gq_vecs x,
                        cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
     const gq_cp_out none{};
-    const bool wide = variant == GQ_VARIANT_WIDE8;
-    if (wide && t.packet == 1 && counter && n >= 32)  // one ray per group of 8 lanes (ray_group.cu)
+    const bool q16 = variant == GQ_VARIANT_WIDE16;
+    const bool wide = variant == GQ_VARIANT_WIDE8 || q16;
+    if (variant == GQ_VARIANT_WIDE8 && t.packet == 1 && counter && n >= 32)  // one ray per group of 8 lanes
         return launch_ray_group(s, x, v, r_max, n, perm, o, counter, st);
     if (s.dim == 3)
-        return wide ? launch_kind<3, true, true>(s, t, x, v, r_max, n, perm, none, o, counter, st)
+        return wide ? launch_kind<3, true, true>(s, t, x, v, r_max, n, perm, none, o, counter, st, q16)
                     : launch_kind<3, true, false>(s, t, x, v, r_max, n, perm, none, o, counter, st);
-    return wide ? launch_kind<2, true, true>(s, t, x, v, r_max, n, perm, none, o, counter, st)
+    return wide ? launch_kind<2, true, true>(s, t, x, v, r_max, n, perm, none, o, counter, st, q16)
                 : launch_kind<2, true, false>(s, t, x, v, r_max, n, perm, none, o, counter, st);
 }
 

@@ -20,6 +20,7 @@ constexpr int CFG_SPHERE = 1;     // triangle bounding-sphere rejection (closest
 constexpr int CFG_SQRTSKIP = 2;   // exact: skip square roots decided by squared distances
 constexpr int CFG_WW = 4;         // while-while scheduling
 constexpr int CFG_MINFIRST = 8;   // wide: nearest child first, other hits unsorted
+constexpr int CFG_Q16 = 16;       // wide: child bounds from the 16-bit records (s.wq16)
 
 __device__ __forceinline__ float qget(const gq_vecs &v, int64_t i, int k) {
     return v.ptr[(int64_t)k * v.comp_stride + i * v.elem_stride];
@@ -30,6 +31,12 @@ __device__ __forceinline__ float exp_scale(uint32_t meta, int ax) {
 // 2^23 + byte k of the 8-byte row (lo4, hi4), built with one byte permute.
 __device__ __forceinline__ float qf(uint32_t lo4, uint32_t hi4, int k) {
     return __int_as_float((int)__byte_perm((k < 4) ? lo4 : hi4, 0x4B000000u, 0x7540u + (unsigned)(k & 3)));
+}
+// 2^23 + the 16-bit step k of a 16-byte row of eight steps, built with one byte permute
+// (bytes 2(k&1), 2(k&1)+1 of word k/2 below the exponent byte 0x4B).
+__device__ __forceinline__ float qf16(const uint4 &row, int k) {
+    const uint32_t w = (k >> 1) == 0 ? row.x : (k >> 1) == 1 ? row.y : (k >> 1) == 2 ? row.z : row.w;
+    return __int_as_float((int)__byte_perm(w, 0x4B000000u, (k & 1) ? 0x7432u : 0x7410u));
 }
 __device__ __forceinline__ void cas(float &ka, int &ra, float &kb, int &rb) {
     const bool sw = kb < ka;
@@ -255,15 +262,26 @@ __device__ __forceinline__ void visit_pair(const DevScene &s, Lane<D, RAY, false
 
 template <int D, bool RAY, int CFG>
 __device__ __forceinline__ void visit_wide(const DevScene &s, Lane<D, RAY, true> &L, int2 *stk, int node) {
-    constexpr int F4 = (D == 3) ? 6 : 5;
+    constexpr bool Q16 = (CFG & CFG_Q16) != 0;
+    constexpr int F4 = (D == 3) ? 6 : 5;           // 16-byte words per 8-bit node
+    constexpr int G4 = (D == 3) ? 7 : 5;           // 16-byte words per 16-bit bounds record
     const int64_t base = F4 * (int64_t)node;
-    const float4 h = ldg4(s.wnodes, base);
+    const int64_t base16 = G4 * (int64_t)node;
+    // the children's references are in the 8-bit node; the header (origin, exponents,
+    // child count) and the bounds come from the 16-bit record when Q16
+    const float4 h = Q16 ? ldg4(s.wq16, base16) : ldg4(s.wnodes, base);
     const int4 r0 = __ldg(reinterpret_cast<const int4 *>(s.wnodes) + base + 1);
     const int4 r1 = __ldg(reinterpret_cast<const int4 *>(s.wnodes) + base + 2);
-    const uint4 q0 = __ldg(reinterpret_cast<const uint4 *>(s.wnodes) + base + 3);
-    const uint4 q1 = __ldg(reinterpret_cast<const uint4 *>(s.wnodes) + base + 4);
-    uint4 q2 = make_uint4(0, 0, 0, 0);
-    if (D == 3) q2 = __ldg(reinterpret_cast<const uint4 *>(s.wnodes) + base + 5);
+    uint4 q0 = make_uint4(0, 0, 0, 0), q1 = q0, q2 = q0;
+    uint4 w16[2 * D];  // Q16: one row of eight 16-bit steps per bound (lo_x.., hi_x..)
+    if (Q16) {
+#pragma unroll
+        for (int rr = 0; rr < 2 * D; ++rr) w16[rr] = __ldg(reinterpret_cast<const uint4 *>(s.wq16) + base16 + 1 + rr);
+    } else {
+        q0 = __ldg(reinterpret_cast<const uint4 *>(s.wnodes) + base + 3);
+        q1 = __ldg(reinterpret_cast<const uint4 *>(s.wnodes) + base + 4);
+        if (D == 3) q2 = __ldg(reinterpret_cast<const uint4 *>(s.wnodes) + base + 5);
+    }
     const uint32_t meta = (uint32_t)fbits(D == 3 ? h.w : h.z);
     const int nc = (int)(meta >> 24);
     const float sx = exp_scale(meta, 0), sy = exp_scale(meta, 1), sz = exp_scale(meta, 2);
@@ -274,7 +292,14 @@ __device__ __forceinline__ void visit_wide(const DevScene &s, Lane<D, RAY, true>
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
         float lo[D], hi[D];
-        if (D == 3) {
+        if (Q16) {
+            const float sc[3] = {sx, sy, sz}, org[3] = {h.x, h.y, D == 3 ? h.z : 0.f};
+#pragma unroll
+            for (int c = 0; c < D; ++c) {
+                lo[c] = __fmaf_rn(qf16(w16[c], k), sc[c], org[c]);
+                hi[c] = __fmaf_rn(qf16(w16[D + c], k), sc[c], org[c]);
+            }
+        } else if (D == 3) {
             lo[0] = __fmaf_rn(qf(q0.x, q0.y, k), sx, h.x);
             lo[1] = __fmaf_rn(qf(q0.z, q0.w, k), sy, h.y);
             lo[D - 1] = __fmaf_rn(qf(q1.x, q1.y, k), sz, h.z);

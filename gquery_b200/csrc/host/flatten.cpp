@@ -158,12 +158,12 @@ void flatten_bvh(const PrimSource<D> &src, const BvhTree<D> &t, DeviceImage<D> &
 // Quantised 8-wide collapse
 // ---------------------------------------------------------------------------
 
-int quant_exponent(float lo, float hi) {
+int quant_exponent(float lo, float hi, int qmax) {
     double ext = (double)hi - (double)lo;
     if (!(ext > 0.0)) return -126;
-    int e = (int)std::ceil(std::log2(ext / 255.0));
-    while (255.0 * std::ldexp(1.0, e) < ext) ++e;
-    while (e > -126 && 255.0 * std::ldexp(1.0, e - 1) >= ext) --e;
+    int e = (int)std::ceil(std::log2(ext / qmax));
+    while (qmax * std::ldexp(1.0, e) < ext) ++e;
+    while (e > -126 && qmax * std::ldexp(1.0, e - 1) >= ext) --e;
     if (e < -126) e = -126;
     if (e > 127) e = 127;
     return e;
@@ -178,15 +178,15 @@ float dequant(float biased, int e, int q) {
 }
 
 // Biased origin and exponent for the parent box [lo, hi] such that decode(0) <= lo
-// and decode(255) >= hi hold exactly in fp32.
-static void quant_axis(float lo, float hi, float *biased, int *e_out) {
-    int e = quant_exponent(lo, hi);
+// and decode(qmax) >= hi hold exactly in fp32.
+void quant_axis(float lo, float hi, int qmax, float *biased, int *e_out) {
+    int e = quant_exponent(lo, hi, qmax);
     for (;;) {
         float s = std::ldexp(1.0f, e);
         float b = std::fma(-8388608.0f, s, lo);
         int guard = 0;
         while (!(dequant(b, e, 0) <= lo) && guard++ < 64) b = std::nextafter(b, -INFINITY);
-        if (dequant(b, e, 255) >= hi || e >= 127) {
+        if (dequant(b, e, qmax) >= hi || e >= 127) {
             *biased = b;
             *e_out = e;
             return;
@@ -195,20 +195,34 @@ static void quant_axis(float lo, float hi, float *biased, int *e_out) {
     }
 }
 
-void quantise_bounds(float origin, int e, float clo, float chi, uint8_t *qlo, uint8_t *qhi) {
+// Outward rounding on a grid of qmax steps: the largest q with decode(q) <= clo and the
+// smallest with decode(q) >= chi, checked in the kernels' fp32 decode.
+static void quantise_steps(float origin, int e, float clo, float chi, int qmax, int *qlo, int *qhi) {
     const double base = (double)dequant(origin, e, 0);
-    // largest q with decode(q) <= clo
     int a = (int)std::floor(((double)clo - base) / std::ldexp(1.0, e));
-    a = std::max(0, std::min(255, a));
+    a = std::max(0, std::min(qmax, a));
     while (a > 0 && !(dequant(origin, e, a) <= clo)) --a;
-    while (a < 255 && dequant(origin, e, a + 1) <= clo) ++a;
-    // smallest q with decode(q) >= chi
+    while (a < qmax && dequant(origin, e, a + 1) <= clo) ++a;
     int b = (int)std::ceil(((double)chi - base) / std::ldexp(1.0, e));
-    b = std::max(0, std::min(255, b));
-    while (b < 255 && !(dequant(origin, e, b) >= chi)) ++b;
+    b = std::max(0, std::min(qmax, b));
+    while (b < qmax && !(dequant(origin, e, b) >= chi)) ++b;
     while (b > 0 && dequant(origin, e, b - 1) >= chi) --b;
+    *qlo = a;
+    *qhi = b;
+}
+
+void quantise_bounds(float origin, int e, float clo, float chi, uint8_t *qlo, uint8_t *qhi) {
+    int a, b;
+    quantise_steps(origin, e, clo, chi, 255, &a, &b);
     *qlo = (uint8_t)a;
     *qhi = (uint8_t)b;
+}
+
+void quantise_bounds16(float origin, int e, float clo, float chi, uint16_t *qlo, uint16_t *qhi) {
+    int a, b;
+    quantise_steps(origin, e, clo, chi, 65535, &a, &b);
+    *qlo = (uint16_t)a;
+    *qhi = (uint16_t)b;
 }
 
 namespace {
@@ -217,6 +231,7 @@ template <int D>
 struct WideBuilder {
     const BvhTree<D> &t;
     DeviceImage<D> &img;
+    bool with16 = false;
 
     // Returns the stack entries a traversal of this subtree needs once its node is popped.
     int build(uint32_t b, int32_t *ref_out) {
@@ -242,11 +257,35 @@ struct WideBuilder {
         }
         const size_t me = img.wnodes.size();
         img.wnodes.emplace_back();
+        if (with16) img.wq16.emplace_back();
         *ref_out = (int32_t)me;
 
         int e[D];
         float org[D];
-        for (int k = 0; k < D; ++k) quant_axis(bn.box.lo.v[k], bn.box.hi.v[k], &org[k], &e[k]);
+        for (int k = 0; k < D; ++k) quant_axis(bn.box.lo.v[k], bn.box.hi.v[k], 255, &org[k], &e[k]);
+        if (with16) {
+            // the same children's bounds on a grid of 65,535 steps over the node's box
+            typename DeviceImage<D>::WQ16 w16;
+            std::memset(&w16, 0, sizeof w16);
+            int e16[D];
+            float o16[D];
+            for (int k = 0; k < D; ++k) quant_axis(bn.box.lo.v[k], bn.box.hi.v[k], 65535, &o16[k], &e16[k]);
+            w16.ox = o16[0];
+            w16.oy = o16[1];
+            uint32_t meta = (uint32_t)(e16[0] + 127) | ((uint32_t)(e16[1] + 127) << 8) | ((uint32_t)kids.size() << 24);
+            if constexpr (D == 3) {
+                w16.oz = o16[2];
+                meta |= (uint32_t)(e16[2] + 127) << 16;
+            }
+            w16.meta = meta;
+            for (size_t k = 0; k < kids.size(); ++k) {
+                const auto &kn = t.nodes[kids[k]];
+                for (int ax = 0; ax < D; ++ax)
+                    quantise_bounds16(o16[ax], e16[ax], kn.box.lo.v[ax], kn.box.hi.v[ax], &w16.q[ax][k],
+                                      &w16.q[D + ax][k]);
+            }
+            img.wq16[me] = w16;
+        }
         typename DeviceImage<D>::WNode w;
         std::memset(&w, 0, sizeof w);
         if constexpr (D == 2) {
@@ -284,14 +323,15 @@ struct WideBuilder {
 }  // namespace
 
 template <int D>
-void flatten_wide(const BvhTree<D> &t, DeviceImage<D> &img) {
+void flatten_wide(const BvhTree<D> &t, DeviceImage<D> &img, bool with16) {
     img.wnodes.clear();
+    img.wq16.clear();
     if (t.nodes[0].n_prims > 0) {
         img.wroot_ref = ~t.nodes[0].prim_offset;
         img.wide_stack = 1;
         return;
     }
-    WideBuilder<D> wb{t, img};
+    WideBuilder<D> wb{t, img, with16};
     int32_t r;
     img.wide_stack = wb.build(0, &r);
     img.wroot_ref = r;
@@ -525,7 +565,7 @@ struct PairWideBuilder {
         out.emplace_back();
         int e[D];
         float org[D];
-        for (int k = 0; k < D; ++k) quant_axis(box.lo.v[k], box.hi.v[k], &org[k], &e[k]);
+        for (int k = 0; k < D; ++k) quant_axis(box.lo.v[k], box.hi.v[k], 255, &org[k], &e[k]);
         WNode w;
         std::memset(&w, 0, sizeof w);
         if constexpr (D == 2) {
@@ -612,8 +652,8 @@ void flatten_wide_from_pairs(const std::vector<typename DeviceImage<D>::Pair> &p
 
 template void flatten_bvh<2>(const PrimSource<2> &, const BvhTree<2> &, DeviceImage<2> &);
 template void flatten_bvh<3>(const PrimSource<3> &, const BvhTree<3> &, DeviceImage<3> &);
-template void flatten_wide<2>(const BvhTree<2> &, DeviceImage<2> &);
-template void flatten_wide<3>(const BvhTree<3> &, DeviceImage<3> &);
+template void flatten_wide<2>(const BvhTree<2> &, DeviceImage<2> &, bool);
+template void flatten_wide<3>(const BvhTree<3> &, DeviceImage<3> &, bool);
 template void flatten_wide_from_pairs<2>(const std::vector<gq_pair2_t> &, int32_t, const float *, const float *,
                                          DeviceImage<2> &, int);
 template void flatten_wide_from_pairs<3>(const std::vector<gq_pair3_t> &, int32_t, const float *, const float *,

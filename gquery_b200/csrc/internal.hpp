@@ -45,10 +45,11 @@ struct gq_scene {
     gqb::BvhTree<3> t3;
     gqb::SnchTree<2> s2;
     gqb::SnchTree<3> s3;
-    bool has_snch = false, has_wide = false;
+    bool has_snch = false, has_wide = false, has_wide16 = false;
     int exact_stack = 0, wide_stack = 0;
     int64_t n_wide = 0, n_sil = 0;
     std::vector<float> wide_words;  // host copy of the wide nodes (host-only scenes)
+    std::vector<float> wide16_words;  // and of their 16-bit bounds records
     std::vector<float> spair_words, sil_words;  // host copies of the SNCH pairs and silhouette records (idem)
     std::vector<void *> allocs;
     int64_t device_bytes = 0;

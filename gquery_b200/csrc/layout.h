@@ -137,6 +137,21 @@ typedef struct {
     uint8_t q[4][8];  // qlo_x, qlo_y, qhi_x, qhi_y
 } gq_wnode2_t;
 
+// 16-bit child bounds of the 8-wide node with the same index (same children, same
+// references, which stay in the 8-bit node): an origin and exponents of its own for the
+// finer grid, and the bounds as 16-bit steps (decoded as fma(2^23 + q, 2^e, origin)).
+// 3D: 112 B (seven 16-byte words); 2D: 80 B.
+typedef struct {
+    float ox, oy, oz;
+    uint32_t meta;       // exp_x | exp_y << 8 | exp_z << 16 | nchild << 24 (exps biased by 127)
+    uint16_t q[6][8];    // qlo_x, qlo_y, qlo_z, qhi_x, qhi_y, qhi_z
+} gq_wq16_3_t;
+typedef struct {
+    float ox, oy;
+    uint32_t meta, pad;  // exp_x | exp_y << 8 | nchild << 24
+    uint16_t q[4][8];    // qlo_x, qlo_y, qhi_x, qhi_y
+} gq_wq16_2_t;
+
 #ifdef __cplusplus
 }
 #endif

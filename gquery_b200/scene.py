@@ -16,7 +16,7 @@ from . import records as R
 ArrayLike = Union[torch.Tensor, np.ndarray, Sequence]
 
 VARIANTS = {"exact": L.VARIANT_EXACT, "wide8": L.VARIANT_WIDE8, "auto": L.VARIANT_AUTO,
-            "coherent": L.VARIANT_COHERENT, "warp": L.VARIANT_WARP}
+            "coherent": L.VARIANT_COHERENT, "warp": L.VARIANT_WARP, "wide16": L.VARIANT_WIDE16}
 KINDS = {"cp": L.KIND_CLOSEST_POINT, "ray": L.KIND_INTERSECT, "sil": L.KIND_SILHOUETTE}
 VARIANT_NAMES = {v: k for k, v in VARIANTS.items()}
 
@@ -84,7 +84,7 @@ class Scene:
     to FP32 ties)."""
 
     def __init__(self, vertices: ArrayLike, indices: ArrayLike, dim: int, *, device: Optional[int] = 0,
-                 build_snch: bool = True, build_wide: bool = True, max_prims_in_node: int = 10,
+                 build_snch: bool = True, build_wide: Union[bool, int] = True, max_prims_in_node: int = 10,
                  n_threads: int = 0, gpu_build: bool = False):
         if dim not in (2, 3):
             raise ValueError("dim must be 2 or 3")
@@ -105,7 +105,8 @@ class Scene:
         self.info = {k: (list(getattr(info, k)) if k.startswith("bbox") else getattr(info, k))
                      for k, _ in L.SceneInfo._fields_}
         self.has_snch = build_snch
-        self.has_wide = build_wide
+        self.has_wide = bool(build_wide)
+        self.has_wide16 = int(build_wide) >= 2 and not gpu_build
         self.torch_device = torch.device("cuda", self.device) if self.device >= 0 else None
 
     def save(self, path: str) -> None:
@@ -129,6 +130,7 @@ class Scene:
         self.device = int(device)
         self.has_snch = self.info["n_silhouettes"] > 0
         self.has_wide = self.info["n_wide_nodes"] > 0
+        self.has_wide16 = False  # scene files keep the 8-bit nodes only
         self.torch_device = torch.device("cuda", self.device)
         return self
 

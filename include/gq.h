@@ -50,6 +50,8 @@ typedef int32_t gq_status;
                                  point, closest silhouette); rays run as EXACT */
 #define GQ_VARIANT_WARP 4     /* closest silhouette only: one query per warp, its 32 lanes expanding up to
                                  32 tree nodes per step (for few, far-reaching queries) */
+#define GQ_VARIANT_WIDE16 5   /* the 8-wide nodes with 16-bit outward-rounded child bounds (scenes built with
+                                 build_wide = 2); closest points and rays, one lane per query */
 /* All variants other than EXACT give the same answers as EXACT except at FP32 distance
  * ties (distances within 2e-6 relative). */
 
@@ -78,7 +80,8 @@ typedef struct {
     int32_t max_prims_in_node; /* leaf size limit of the SAH build; gQuery's default is 10 */
     int32_t n_threads;         /* host threads for the build; 0 = all cores */
     int32_t build_snch;        /* also build silhouettes and normal cones */
-    int32_t build_wide;        /* also build the quantised 8-wide BVH */
+    int32_t build_wide;        /* also build the quantised 8-wide BVH (8-bit child bounds); 2: and the same
+                                  nodes' 16-bit child bounds (GQ_VARIANT_WIDE16) */
     int32_t device;            /* CUDA device that holds the scene */
     int32_t gpu_build;         /* build a linear BVH on the device instead (milliseconds; no SNCH, no wide
                                   nodes, no reference arrays; answers equal up to FP32 ties) */
@@ -175,6 +178,8 @@ gq_status gq_scene_get_tuning(const gq_scene *scene, int32_t kind, gq_tuning *tu
                                       host-only scenes (device < 0) only */
 #define GQ_ARRAY_SNCH_PAIRS 6      /* SNCH pair records (gq_spair2_t / gq_spair3_t) as raw 32-bit words
                                       (20 / 40 per pair; pair 0 is the root's); host-only scenes only */
+#define GQ_ARRAY_WIDE16_BOUNDS 8   /* 16-bit bounds records (gq_wq16_2_t / gq_wq16_3_t) as raw 32-bit words
+                                      (20 / 28 per node); host-only scenes built with build_wide = 2 only */
 #define GQ_ARRAY_SIL_RECORDS 7     /* silhouette records (gq_silv_t / gq_sile_t) as raw 32-bit words
                                       (8 / 16 per record, in leaf order); host-only scenes only */
 gq_status gq_scene_ref_array(const gq_scene *scene, int32_t which, float *dst, int64_t cap, int64_t *len);

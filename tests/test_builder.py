@@ -239,6 +239,67 @@ def test_quantised_boxes_contain_their_subtrees(dim):
     assert s.info["wide_stack"] <= 96
 
 
+def _decode_wide16(words, dim):
+    """The 16-bit bounds records, decoded like the kernels (fma(2^23 + q, 2^e, origin))."""
+    stride = 28 if dim == 3 else 20
+    w = words.view(np.uint32).reshape(-1, stride)
+    f = words.reshape(-1, stride)
+    origin = f[:, :dim]
+    meta = w[:, 3] if dim == 3 else w[:, 2]
+    q = w[:, 4:].copy().view(np.uint16).reshape(-1, 2 * dim, 8).astype(np.float64)
+    exps = np.stack([(meta >> (8 * k)) & 0xff for k in range(dim)], axis=1).astype(np.int32) - 127
+    nc = (meta >> 24).astype(np.int32)
+    scale = np.ldexp(1.0, exps)
+    lo = np.empty((w.shape[0], 8, dim), np.float32)
+    hi = np.empty_like(lo)
+    for k in range(dim):
+        s, o = scale[:, k:k + 1], origin[:, k:k + 1].astype(np.float64)
+        lo[:, :, k] = ((q[:, k, :] + 8388608.0) * s + o).astype(np.float32)
+        hi[:, :, k] = ((q[:, dim + k, :] + 8388608.0) * s + o).astype(np.float32)
+    return nc, lo, hi
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_16bit_bounds_contain_the_8bit_nodes_children(dim):
+    """The 16-bit bounds (build_wide = 2) describe the same children as the 8-bit nodes,
+    each decoded box contains the child's exact box (outward rounding), and the finer
+    grid leaves less slack around the exact boxes than the 8-bit one."""
+    if dim == 3:
+        v, f = W.icosphere(4, amplitude=0.3, seed=5)
+    else:
+        v, f = W.star_polyline(3000, seed=5)
+    s = _host(v, f, dim, build_wide=2)
+    refs, nc8, lo8, hi8 = _decode_wide(s.ref_array(L.ARRAY_WIDE_NODES), dim)
+    nc16, lo16, hi16 = _decode_wide16(s.ref_array(L.ARRAY_WIDE16_BOUNDS), dim)
+    assert np.array_equal(nc8, nc16)
+    # exact child boxes: the primitives below each child
+    P = s.ref_array(L.ARRAY_PRIMITIVES).reshape(-1, dim * dim + 1)
+    verts = P[:, :dim * dim].reshape(-1, dim, dim)
+    eps = np.float32(np.finfo(np.float32).eps)
+    plo, phi = verts.min(axis=1) - eps, verts.max(axis=1) + eps
+    N = _nodes(s)
+    leaf_len = {int(N[i, 2 * dim]): int(N[i, 2 * dim + 2]) for i in range(len(N)) if N[i, 2 * dim + 2] > 0}
+
+    def prim_range(ref):
+        if ref < 0:
+            o = ~ref
+            return [(o, o + leaf_len[o])]
+        out = []
+        for k in range(nc8[ref]):
+            out += prim_range(int(refs[ref, k]))
+        return out
+
+    slack8 = slack16 = 0.0
+    for node in range(refs.shape[0]):
+        for k in range(nc8[node]):
+            idx = np.concatenate([np.arange(a, b) for a, b in prim_range(int(refs[node, k]))])
+            elo, ehi = plo[idx].min(axis=0), phi[idx].max(axis=0)
+            assert (lo16[node, k] <= elo).all() and (hi16[node, k] >= ehi).all()
+            slack8 += float(np.sum(elo - lo8[node, k]) + np.sum(hi8[node, k] - ehi))
+            slack16 += float(np.sum(elo - lo16[node, k]) + np.sum(hi16[node, k] - ehi))
+    assert slack16 < 0.05 * slack8, (slack16, slack8)
+
+
 def test_invalid_inputs_are_rejected():
     v = np.zeros((3, 3), np.float32)
     with pytest.raises(L.GQError) as ei:

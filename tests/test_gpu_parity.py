@@ -383,3 +383,41 @@ def test_ray_group_matches_exact(mesh_c1, star):
                            {k: np.asarray(v)[..., same] for k, v in exact.items()}, fields, f"{dim}D group ")
             assert group["valid"].any()
         assert scene.device_error() == 0
+
+
+@pytest.fixture(scope="module")
+def mesh_c1_16():
+    v, f = W.config1_mesh()
+    return Scene(v, f, 3, device=0, build_snch=False, build_wide=2)
+
+
+def test_wide16_matches_exact(mesh_c1_16, star):
+    """Closest points and rays over the 8-wide nodes with 16-bit child bounds against the
+    exact traversal: the same validity everywhere, the same primitive except at FP32
+    distance ties, distances within 2e-6 relative; and the same answers as the 8-bit
+    bounds up to ties."""
+    v, e = W.star_polyline(4096, seed=0)
+    star16 = Scene(v, e, 2, device=0, build_snch=False, build_wide=2)
+    for scene, dim, n in ((mesh_c1_16, 3, 200_000), (star16, 2, 100_000)):
+        q = torch.as_tensor(W.uniform_points(n, dim, seed=60 + dim)).cuda()
+        o, d = W.rays(n, dim, seed=62 + dim)
+        ex_cp = to_np(scene.closest_point(q, variant="exact"))
+        w16_cp = to_np(scene.closest_point(q, variant="wide16"))
+        ex_ray = to_np(scene.intersect(o, d, variant="exact"))
+        w16_ray = to_np(scene.intersect(o, d, variant="wide16"))
+        for a, b, what in ((w16_cp, ex_cp, "cp"), (w16_ray, ex_ray, "ray")):
+            rep = tie_report(a, b)
+            assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0, (dim, what, rep)
+            assert rep["max_rel_d"] <= REL_TOL, (dim, what, rep)
+        scene.set_tuning("cp", "wide8", packet=0, persist=1)
+        w8_cp = to_np(scene.closest_point(q, variant="wide8"))
+        scene.set_tuning("cp", "coherent", packet=1, persist=0)
+        rep = tie_report(w16_cp, w8_cp)
+        assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0, (dim, rep)
+        assert scene.device_error() == 0
+
+
+def test_wide16_needs_the_16bit_build(mesh_c1):
+    with pytest.raises(L.GQError) as ei:
+        mesh_c1.closest_point(torch.zeros(64, 3, device="cuda"), variant="wide16")
+    assert ei.value.status == L.GQ_ERR_UNSUPPORTED
