@@ -4,8 +4,8 @@
 Headline (the JSON line's `value`): 3D closest point + ray intersection on the
 displaced icosphere of level 8 (1,310,720 triangles), 8,388,608 closest-point queries
 U[-2,2]^3 and 8,388,608 rays (origins U[-2,2]^3, directions uniform on S^2, r_max =
-inf).  One step = Morton order + closest_point over all points, then Morton order +
-intersect over all rays, each with the scene's tuned variant; the exact binary kernel
+inf).  One step = Morton order + closest_point over all points, then the rays' order (origin
+and direction) + intersect over all rays, each with the scene's tuned variant; the exact binary kernel
 (gQuery's visit order) and the quantised 8-wide kernel are measured beside it.
 
 At one GPU the same line also carries (see --sections): c0 2D closest point on the
@@ -59,9 +59,14 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the exact and wide8 side-by-side runs")
     ap.add_argument("--no-autotune", action="store_true", help="use the built-in tuning table as it is")
-    ap.add_argument("--sections", default="fp64,c0,build,c2,c3,c4",
+    ap.add_argument("--sections-only", action="store_true",
+                    help="run the listed sections alone, without the headline step (for profiling them)")
+    ap.add_argument("--ray-n", type=int, default=1 << 23, help="rays of the rays section")
+    ap.add_argument("--sections", default="fp64,rays,c0,build,c2,c3,c4",
                     help="beside the headline (cp + rays on the level-8 mesh): fp64 FP32-vs-FP64 error on "
-                         "65,536 of the headline's closest points and rays, c0 2D closest point on the "
+                         "65,536 of the headline's closest points and rays, rays: the 8-wide ray kernels (one "
+                         "ray per lane or per group of 8 lanes) in origin and origin+direction order, "
+                         "c0 2D closest point on the "
                          "4,096-vertex star (GPU and CPU), build host SAH vs device build of the "
                          "level-8 mesh, c2 silhouettes on the level-7 "
                          "mesh, c3 512 uneven 2D scenes in one batched launch, c4 serving 64 meshes; "
@@ -258,6 +263,37 @@ def tie_stats(a, b, rel=2e-6):
             "prim_mismatch_loose_tie": int((diff & ~exact & (reld <= rel)).sum()),
             "prim_mismatch_not_tie": int((diff & (reld > rel)).sum()),
             "max_rel_d": float(reld[both].max()) if bool(both.any()) else 0.0}
+
+
+def section_rays(args, dev, flush):
+    """Rays of the headline workload over the quantised 8-wide nodes: one ray per lane and
+    one ray per group of 8 lanes, each in the origins' Morton order (mode 0) and in the
+    origin + direction order (mode 2); the records of all four must be the same."""
+    import torch
+    from gquery_b200 import workloads as W
+    from gquery_b200.scene import Scene
+    V, F = W.config1_mesh()
+    s = Scene(V, F, 3, device=dev.index or 0, build_snch=False, build_wide=True)
+    n = args.ray_n
+    o, d = (torch.as_tensor(a).to(dev) for a in W.rays(n, 3, seed=2))
+    res = {"workload": f"{n} rays U[-2,2]^3 x S^2 on the level-8 mesh, 8-wide nodes"}
+    ref = None
+    same = True
+    for mode in (0, 2):
+        order = s.ray_order(o, d, mode)
+        for name, packet in (("per_lane", 0), ("group_of_8", 1)):
+            s.set_tuning("ray", "wide8", packet=packet, sorted=1, persist=1)
+            out = s.alloc_ray(n)
+            ms = dev_ms(lambda: s.intersect(o, d, variant="wide8", out=out, order=order),
+                        steps=max(1, min(args.steps, 5)), warmup=1, flush=flush)
+            res[f"{name}_order{mode}"] = {"ms": ms, "mrays_per_s": n / ms / 1e3}
+            rec = {k: v.clone() for k, v in vars(out).items()}
+            if ref is None:
+                ref = rec
+            same = same and all(torch.equal(rec[k], ref[k]) for k in rec)
+    res["records_identical"] = bool(same)
+    assert s.device_error() == 0
+    return res
 
 
 def section_c0(args, dev, flush):
@@ -660,6 +696,14 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     dev = torch.device("cuda", local)
+    if args.sections_only:  # the listed sections alone (one GPU), e.g. to profile one of them
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+        fns = {"rays": section_rays, "c0": section_c0, "build": section_build, "c2": section_c2, "c3": section_c3}
+        out = {}
+        for name in [x for x in args.sections.split(",") if x and x != "none"]:
+            out[name] = section_c4(args, dev) if name == "c4" else fns[name](args, dev, flush)
+        print(json.dumps({"sections": out}), flush=True)
+        return 0
 
     def barrier():
         if world > 1:
@@ -691,7 +735,7 @@ def main():
         scene.closest_point(q, variant=variant, out=cp_out, order=perm_q)
         if ev:
             ev[2].record()
-        scene.order(o, out=perm_o, scratch=scratch)
+        scene.ray_order(o, d, 2, out=perm_o, scratch=scratch)
         if ev:
             ev[3].record()
         scene.intersect(o, d, variant=variant, out=ray_out, order=perm_o)
@@ -847,7 +891,7 @@ def main():
             scene.closest_point(ln.qd, variant=args.variant, out=ln.cp, order=ln.perm_q, scratch=ln.scratch, stream=r)
             ev["cp"].record(r)
             r.wait_event(ev["od"])
-            scene.order(ln.od, out=ln.perm_o, scratch=ln.scratch, stream=r)
+            scene.ray_order(ln.od, ln.dd, 2, out=ln.perm_o, scratch=ln.scratch, stream=r)
             scene.intersect(ln.od, ln.dd, variant=args.variant, out=ln.ray, order=ln.perm_o, scratch=ln.scratch,
                             stream=r)
             ev["ray"].record(r)
@@ -945,17 +989,18 @@ def main():
             "parity": parity, "fp64_error": fp64,
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
             "gpu_launches": 4 * args.steps,
-            "gpu_launches_note": "own kernels per step: 2 Morton-key + 2 traversal (CUB radix-sort kernels extra)",
+            "gpu_launches_note": "own kernels per step: 1 Morton-key + 1 ray-key + 2 traversal (CUB radix-sort kernels extra)",
         }
         sections = sections_on
         flush_buf = flush
-        for name, fn in (("c0", lambda: section_c0(args, dev, flush_buf)),
+        for name, fn in (("rays", lambda: section_rays(args, dev, flush_buf)),
+                         ("c0", lambda: section_c0(args, dev, flush_buf)),
                          ("build", lambda: section_build(args, dev, flush_buf)),
                          ("c2", lambda: section_c2(args, dev, flush_buf)), ("c3", lambda: section_c3(args, dev, flush_buf)),
                          ("c4", lambda: section_c4(args, dev))):
             if name in sections:
-                key = {"c0": "closest_point_2d_c0", "build": "scene_build", "c2": "silhouette_c2",
-                       "c3": "batched_c3", "c4": "serving_c4"}[name]
+                key = {"rays": "rays_8wide", "c0": "closest_point_2d_c0", "build": "scene_build",
+                       "c2": "silhouette_c2", "c3": "batched_c3", "c4": "serving_c4"}[name]
                 t_sec = time.perf_counter()
                 line[key] = fn()
                 line[key]["section_wall_s"] = time.perf_counter() - t_sec

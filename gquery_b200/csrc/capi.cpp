@@ -398,8 +398,11 @@ struct Scratch {
 // Per-call scratch: [work counter, 256 B][permutation, n int32][Morton sort workspace].
 // The counter feeds the persistent wide kernels; the rest is used when sorting.
 
+// ray_dirs (3D rays): the rays are keyed by origin and direction (gq_ray_order mode 2),
+// which keeps the rays of a warp pointing alike.
 gq_status prepare_order(const gq_scene *s, gq_vecs keys_from, int64_t n, const gq_query_opts *opts,
-                        cudaStream_t st, Scratch &scr, const int32_t **perm, unsigned long long **counter) {
+                        cudaStream_t st, Scratch &scr, const int32_t **perm, unsigned long long **counter,
+                        const gq_vecs *ray_dirs = nullptr) {
     *perm = nullptr;
     *counter = nullptr;
     const bool sorting = opts && !opts->order && opts->sort && n >= 2;
@@ -421,7 +424,9 @@ gq_status prepare_order(const gq_scene *s, gq_vecs keys_from, int64_t n, const g
     if (!sorting) return GQ_OK;
     int32_t *pp = (int32_t *)((char *)scr.p + kCounterBytes);
     char *rest = (char *)pp + align256((size_t)n * 4);
-    cudaError_t e = gqd::morton_order(s->dev, keys_from, n, pp, rest, gqd::morton_scratch_bytes(n), st);
+    const bool ray_keys = ray_dirs && s->dim == 3;
+    cudaError_t e = gqd::morton_order(s->dev, keys_from, n, pp, rest, gqd::morton_scratch_bytes(n), st,
+                                      ray_keys ? 2 : 0, ray_keys ? *ray_dirs : gq_vecs{});
     if (e != cudaSuccess) return fail_cuda(e, "morton_order");
     *perm = pp;
     return GQ_OK;
@@ -724,7 +729,7 @@ gq_status gq_intersect(const gq_scene *s, gq_vecs origin, gq_vecs dir, const flo
     Scratch scr;
     const int32_t *perm = nullptr;
     unsigned long long *counter = nullptr;
-    if ((st = prepare_order(s, origin, n, opts, cs, scr, &perm, &counter)) != GQ_OK) return st;
+    if ((st = prepare_order(s, origin, n, opts, cs, scr, &perm, &counter, &dir)) != GQ_OK) return st;
     cudaError_t e = gqd::launch_ray(s->dev, v, to_tune(s, GQ_KIND_INTERSECT, v), origin, dir, r_max, n, perm,
                                     *out, counter, cs);
     if (e != cudaSuccess) return fail_cuda(e, "intersect launch");
