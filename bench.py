@@ -35,6 +35,8 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
+# hardware work queues for the serving runtime's streams (read when the CUDA context is created)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 METRIC = "Mqueries/s (cp/ray/silhouette) quantised+batched vs plain GPU; serving p50/p99 ms"
 WORKLOAD = ("closest point + ray intersection, displaced icosphere level 8 (1,310,720 triangles), "
@@ -564,6 +566,18 @@ def section_c4(args, dev):
         return {k: {"p50_ms": float(np.percentile(lat[kind_of == k], 50)),
                     "p99_ms": float(np.percentile(lat[kind_of == k], 99))} for k in ("cp", "ray", "sil")}
 
+    level_of = np.array([levels[r.scene] for r in reqs])
+
+    def tail(res):
+        """The slowest 1% of the requests: kind, size, mesh level and where the time went
+        (admission wait, wait for a step slot, step run to results in the host arrays)."""
+        lat = (res["t_done"] - res["t_submit"]) * 1e3
+        idx = np.argsort(-lat)[:max(1, len(lat) // 100)]
+        ms = lambda a, b, i: round(float(res[b][i] - res[a][i]) * 1e3, 3)
+        return [{"kind": str(kind_of[i]), "n": int(res["n"][i]), "level": int(level_of[i]),
+                 "latency_ms": round(float(lat[i]), 3), "admit_ms": ms("t_submit", "t_admit", i),
+                 "slot_wait_ms": ms("t_admit", "t_launch", i), "run_ms": ms("t_launch", "t_done", i)} for i in idx]
+
     out = {"workload": f"64 icospheres levels 4-8 ({sum(20 * 4 ** x for x in levels)} triangles), "
                        f"{len(reqs)} requests, {int(counts.sum())} queries", "build_s": build_s,
            "note": "loads are fractions of the batched server's saturation arrival rate; the plain "
@@ -584,7 +598,8 @@ def section_c4(args, dev):
             sm = summarize(r)
             entry["loads"].append({"load_of_batched_peak": frac, "arrivals_per_s": frac * sat_rate,
                                    "mqueries_per_s": sm["mqueries_per_s"], "p50_ms": sm["p50_ms"],
-                                   "p99_ms": sm["p99_ms"], "steps": sm["steps"], "by_kind": by_kind(r)})
+                                   "p99_ms": sm["p99_ms"], "steps": sm["steps"], "by_kind": by_kind(r),
+                                   "slowest_1pct": tail(r)})
         st = srv.stats()
         assert st["device_error"] == 0
         entry["ring_device_bytes"] = st["device_bytes"]

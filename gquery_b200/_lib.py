@@ -96,7 +96,8 @@ class QueryOpts(C.Structure):
 class ServerOpts(C.Structure):
     _fields_ = [("budget_bytes", C.c_int64), ("ring_queries", C.c_int64 * 3), ("step_queries", C.c_int64),
                 ("max_inflight", C.c_int32), ("flags", C.c_int32), ("sil_share", C.c_float),
-                ("sil_slots", C.c_int32), ("sil_step_queries", C.c_int64)]
+                ("sil_slots", C.c_int32), ("sil_step_queries", C.c_int64), ("large_queries", C.c_int64),
+                ("large_slots", C.c_int32), ("large_share", C.c_float), ("copy_threads", C.c_int32)]
 
 
 class Request(C.Structure):

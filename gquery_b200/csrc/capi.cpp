@@ -1179,7 +1179,7 @@ gq_status gq_batch_run(gq_batch *b, const gq_batch_queries *cp, const gq_cp_out 
     cudaError_t e = gqd::batch_run(b->dev_scenes, (int)b->scenes.size(), b->dim, kinds, co, ro, so,
                                    (b->flags & GQ_BATCH_RAY_EXACT) || !all_wide ? 0 : 1,
                                    gqd::cp_mode_of(b->flags), gqd::sil_mode_of(b->flags),
-                                   1.f,
+                                   1.f, 128, true,
                                    b->scratch, b->max_queries, b->err, (cudaStream_t)stream);
     if (e != cudaSuccess) return fail_cuda(e, "batch launch");
     return GQ_OK;

@@ -46,6 +46,17 @@ __device__ __forceinline__ uint32_t spread2(uint32_t v) {
     return v;
 }
 
+// Identity order for the three kinds (steps answered without sorting) and the phases'
+// claim counters zeroed, in one launch.
+__global__ void k_batch_ident(int32_t *perm0, int64_t n0, int32_t *perm1, int64_t n1, int32_t *perm2, int64_t n2,
+                              unsigned long long *counter, int n_counters) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n0) perm0[i] = (int32_t)i;
+    if (i < n1) perm1[i] = (int32_t)i;
+    if (i < n2) perm2[i] = (int32_t)i;
+    if (i < n_counters) counter[i] = 0ull;
+}
+
 // key = scene << 32 | Morton code over twice the scene's box
 __global__ void k_batch_keys(const DevScene *scenes, int n_scenes, BatchKind k, int64_t n, uint64_t *keys,
                              int32_t *vals, int32_t *bad) {
@@ -535,10 +546,11 @@ __global__ void __launch_bounds__(32, 32) k_batch_silw1(const DevScene *scenes, 
 template <int D, bool RAYW>
 cudaError_t launch_batch(const DevScene *scenes_dev, int n_scenes, BatchKind kinds[3], const gq_cp_out &cp_out,
                          const gq_ray_out &ray_out, const gq_sil_out &sil_out, int cp_mode, int sil_mode,
-                         float grid_share, unsigned long long *counter, Handover ho, int32_t *err,
+                         float grid_share, int block, unsigned long long *counter, Handover ho, int32_t *err,
                          cudaStream_t st) {
+    const int bi = block == 32 ? 1 : 0;  // k_batch and the hand-over kernels: blocks of kBlock or 32 threads
     // the one-query-per-warp silhouette phase keeps its stacks in dynamic shared memory
-    const size_t smem = (sil_mode == 2 && kinds[2].n > 0) ? (size_t)(kBlock / 32) * wsil::kWarpStack * sizeof(int2) : 0;
+    const size_t smem = (sil_mode == 2 && kinds[2].n > 0) ? (size_t)(block / 32) * wsil::kWarpStack * sizeof(int2) : 0;
     if (smem && kinds[0].n <= 0 && kinds[1].n <= 0) {  // silhouettes only: the phase's own kernel
         if (grid_share > 0.f && grid_share < 1.f) {      // beside other work: one block per query
             if (kinds[2].n > 0x7fffffff) return cudaErrorInvalidValue;
@@ -546,17 +558,19 @@ cudaError_t launch_batch(const DevScene *scenes_dev, int n_scenes, BatchKind kin
                                                                         err);
             return cudaGetLastError();
         }
+        // persistent warps in blocks of kBlock threads, whatever `block` is
+        const size_t wsmem = (size_t)(kBlock / 32) * wsil::kWarpStack * sizeof(int2);
         static int wbps = 0, w_sm = 0;
         if (!wbps) {
             int dev = 0, b = 0;
             cudaGetDevice(&dev);
             cudaDeviceGetAttribute(&w_sm, cudaDevAttrMultiProcessorCount, dev);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_silw<D>, kBlock, smem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_silw<D>, kBlock, wsmem);
             wbps = b < 1 ? 1 : b;
         }
         const int64_t want = std::min<int64_t>((int64_t)wbps * w_sm, (kinds[2].n * 32 + kBlock - 1) / kBlock);
-        k_batch_silw<D><<<dim3((unsigned)want), kBlock, smem, st>>>(scenes_dev, n_scenes, kinds[2], sil_out, counter,
-                                                                    err);
+        k_batch_silw<D><<<dim3((unsigned)want), kBlock, wsmem, st>>>(scenes_dev, n_scenes, kinds[2], sil_out, counter,
+                                                                     err);
         return cudaGetLastError();
     }
     const int mi = smem ? 1 : 0;
@@ -566,52 +580,53 @@ cudaError_t launch_batch(const DevScene *scenes_dev, int n_scenes, BatchKind kin
                                     : (const void *)k_batch<D, RAYW, true, false>)
                              : (sil ? (const void *)k_batch<D, RAYW, false, true>
                                     : (const void *)k_batch<D, RAYW, false, false>);
-    static int bps_m[2][4] = {}, n_sm = 0;
-    if (!bps_m[mi][si]) {
+    static int bps_m[2][2][4] = {}, n_sm = 0;
+    if (!bps_m[bi][mi][si]) {
         int dev = 0, b = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, kBlock, smem);
-        bps_m[mi][si] = b < 1 ? 1 : b;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, block, smem);
+        bps_m[bi][mi][si] = b < 1 ? 1 : b;
     }
-    const int bps = bps_m[mi][si];
+    const int bps = bps_m[bi][mi][si];
     const int64_t most = std::max(kinds[0].n, std::max(kinds[1].n, kinds[2].n));
     if (most <= 0) return cudaSuccess;
     int64_t want = std::min<int64_t>((int64_t)bps * n_sm,
-                                     std::max<int64_t>((most + kBlock - 1) / kBlock, smem ? (kinds[2].n * 32 + kBlock - 1) / kBlock : 0));
+                                     std::max<int64_t>((most + block - 1) / block, smem ? (kinds[2].n * 32 + block - 1) / block : 0));
     if (grid_share > 0.f && grid_share < 1.f)
         want = std::min<int64_t>(want, std::max<int64_t>(1, (int64_t)(grid_share * (float)(bps * n_sm))));
     void *args[] = {(void *)&scenes_dev, (void *)&n_scenes, (void *)&kinds[0], (void *)&cp_out,
                     (void *)&kinds[1],   (void *)&ray_out,  (void *)&kinds[2], (void *)&sil_out,
                     (void *)&cp_mode,    (void *)&sil_mode, (void *)&kBudget,  (void *)&counter,
                     (void *)&ho,         (void *)&err};
-    cudaLaunchKernel(kern, dim3((unsigned)want), dim3(kBlock), args, smem, st);
+    cudaLaunchKernel(kern, dim3((unsigned)want), dim3((unsigned)block), args, smem, st);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     // the handed-over queries: persistent grids of one query per warp
-    const size_t hsmem = (size_t)(kBlock / 32) * wcp::kWarpStack * sizeof(int2);
-    static int hbps[2] = {0, 0};
-    if (!hbps[0]) {
+    const size_t hsmem = (size_t)(block / 32) * wcp::kWarpStack * sizeof(int2);
+    static int hbps[2][2] = {};
+    if (!hbps[bi][0]) {
         int b = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_cp_heavy<D>, kBlock, hsmem);
-        hbps[0] = b < 1 ? 1 : b;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sil_heavy<D>, kBlock, hsmem);
-        hbps[1] = b < 1 ? 1 : b;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_cp_heavy<D>, block, hsmem);
+        hbps[bi][0] = b < 1 ? 1 : b;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sil_heavy<D>, block, hsmem);
+        hbps[bi][1] = b < 1 ? 1 : b;
     }
     auto hgrid = [&](int which, int64_t n) {
-        int64_t g = std::min<int64_t>((int64_t)hbps[which] * n_sm, (n * 32 + kBlock - 1) / kBlock);
+        const int hb = hbps[bi][which];
+        int64_t g = std::min<int64_t>((int64_t)hb * n_sm, (n * 32 + block - 1) / block);
         if (grid_share > 0.f && grid_share < 1.f)
-            g = std::min<int64_t>(g, std::max<int64_t>(1, (int64_t)(grid_share * (float)(hbps[which] * n_sm))));
+            g = std::min<int64_t>(g, std::max<int64_t>(1, (int64_t)(grid_share * (float)(hb * n_sm))));
         return dim3((unsigned)g);
     };
     if (cp_mode == 2 && kinds[0].n > 0) {
-        k_cp_heavy<D><<<hgrid(0, kinds[0].n), kBlock, hsmem, st>>>(scenes_dev, kinds[0], cp_out, ho.cp_q, ho.cp_r,
-                                                                   counter);
+        k_cp_heavy<D><<<hgrid(0, kinds[0].n), block, hsmem, st>>>(scenes_dev, kinds[0], cp_out, ho.cp_q, ho.cp_r,
+                                                                  counter);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     if (sil_mode == 3 && kinds[2].n > 0) {
-        k_sil_heavy<D><<<hgrid(1, kinds[2].n), kBlock, hsmem, st>>>(scenes_dev, kinds[2], sil_out, ho.sil_q,
-                                                                    ho.sil_r, counter);
+        k_sil_heavy<D><<<hgrid(1, kinds[2].n), block, hsmem, st>>>(scenes_dev, kinds[2], sil_out, ho.sil_q,
+                                                                   ho.sil_r, counter);
         e = cudaGetLastError();
     }
     return e;
@@ -637,8 +652,10 @@ size_t batch_scratch_bytes(int64_t max_n) {
 
 cudaError_t batch_run(const DevScene *scenes_dev, int n_scenes, int dim, BatchKind kinds[3], const gq_cp_out &cp_out,
                       const gq_ray_out &ray_out, const gq_sil_out &sil_out, int ray_wide, int cp_mode,
-                      int sil_mode, float grid_share, void *scratch, int64_t max_n, int32_t *err,
-                      cudaStream_t st) {
+                      int sil_mode, float grid_share, int block, bool sort, void *scratch, int64_t max_n,
+                      int32_t *err, cudaStream_t st) {
+    block = block == 32 ? 32 : kBlock;
+    constexpr int kCounters = 7;  // claims per phase; closest points handed over, their claims; silhouettes the same
     char *p = static_cast<char *>(scratch);
     unsigned long long *counter = reinterpret_cast<unsigned long long *>(p);
     p += 256;
@@ -667,7 +684,7 @@ cudaError_t batch_run(const DevScene *scenes_dev, int n_scenes, int dim, BatchKi
             ho.sil_q = v_in;
             ho.sil_r = reinterpret_cast<int2 *>(k_in);
         }
-        if (q.n <= 0) continue;
+        if (q.n <= 0 || !sort) continue;
         k_batch_keys<<<dim3((unsigned)((q.n + kBlock - 1) / kBlock)), kBlock, 0, st>>>(scenes_dev, n_scenes, q, q.n,
                                                                                         k_in, v_in, err);
         cudaError_t e = cudaGetLastError();
@@ -676,18 +693,29 @@ cudaError_t batch_run(const DevScene *scenes_dev, int n_scenes, int dim, BatchKi
         e = cub::DeviceRadixSort::SortPairs(temp, tbk, k_in, k_out, v_in, perm, (int)q.n, 0, end_bit, st);
         if (e != cudaSuccess) return e;
     }
-    // claims per phase; closest points handed over, their claims; silhouettes the same
-    cudaError_t e = cudaMemsetAsync(counter, 0, 7 * sizeof(unsigned long long), st);
+    cudaError_t e = cudaSuccess;
+    if (sort) {
+        e = cudaMemsetAsync(counter, 0, kCounters * sizeof(unsigned long long), st);
+    } else {
+        // the identity order where the sort would have put its output (the hand-over
+        // lists of the split modes live in the sort's inputs, not here)
+        const int64_t most = std::max<int64_t>(kCounters, std::max(kinds[0].n, std::max(kinds[1].n, kinds[2].n)));
+        k_batch_ident<<<dim3((unsigned)((most + block - 1) / block)), block, 0, st>>>(
+            const_cast<int32_t *>(kinds[0].perm), std::max<int64_t>(kinds[0].n, 0), const_cast<int32_t *>(kinds[1].perm),
+            std::max<int64_t>(kinds[1].n, 0), const_cast<int32_t *>(kinds[2].perm), std::max<int64_t>(kinds[2].n, 0),
+            counter, kCounters);
+        e = cudaGetLastError();
+    }
     if (e != cudaSuccess) return e;
     if (dim == 3)
         return ray_wide ? launch_batch<3, true>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_mode,
-                                                sil_mode, grid_share, counter, ho, err, st)
+                                                sil_mode, grid_share, block, counter, ho, err, st)
                         : launch_batch<3, false>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_mode,
-                                                 sil_mode, grid_share, counter, ho, err, st);
+                                                 sil_mode, grid_share, block, counter, ho, err, st);
     return ray_wide ? launch_batch<2, true>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_mode,
-                                            sil_mode, grid_share, counter, ho, err, st)
+                                            sil_mode, grid_share, block, counter, ho, err, st)
                     : launch_batch<2, false>(scenes_dev, n_scenes, kinds, cp_out, ray_out, sil_out, cp_mode,
-                                             sil_mode, grid_share, counter, ho, err, st);
+                                             sil_mode, grid_share, block, counter, ho, err, st);
 }
 
 }  // namespace gqd

@@ -39,11 +39,15 @@ size_t batch_scratch_bytes(int64_t max_n);
 // closest points as cp_mode_of; sil_mode: silhouettes 1 warp-coherent, 2 one query per
 // warp, 0 reference order per lane, 3 the same with long traversals handed to a warp;
 // grid_share in (0, 1) caps the persistent grid at that share of the GPU's resident
-// blocks, so a launch on another stream can run beside it.  No allocation and no host
-// synchronisation: the call can be recorded in a CUDA graph.
+// blocks, so a launch on another stream can run beside it; block: threads per block of
+// the batch and hand-over kernels, 128 or 32 (one warp: a launch beside one-warp
+// silhouette blocks then fits in the room any one of them leaves); sort: queries in
+// (scene, Morton) order, else in their given order with one small launch instead of the
+// keys and the radix sort (for small steps, whose launches should need little room).
+// No allocation and no host synchronisation: the call can be recorded in a CUDA graph.
 cudaError_t batch_run(const DevScene *scenes_dev, int n_scenes, int dim, BatchKind kinds[3], const gq_cp_out &cp_out,
                       const gq_ray_out &ray_out, const gq_sil_out &sil_out, int ray_wide, int cp_mode,
-                      int sil_mode, float grid_share, void *scratch, int64_t max_n, int32_t *err,
-                      cudaStream_t st);
+                      int sil_mode, float grid_share, int block, bool sort, void *scratch, int64_t max_n,
+                      int32_t *err, cudaStream_t st);
 
 }  // namespace gqd

@@ -9,13 +9,25 @@
 // is reclaimed in allocation order, so it is first-in first-out like the admission.
 // The rings' device bytes are the admission budget.
 //
-// Step.  A step takes, for each kind it serves, the run of admitted requests that are
-// contiguous in the ring (at most step_queries queries) and answers them with one
-// batch launch; closest-point and ray requests go to the general slots, silhouette
-// requests to slots of their own whose launches hold part of the GPU only;
+// Size classes.  Requests of at least large_queries queries are "large": they have
+// rings, steps and stream slots of their own, on lower stream priorities than the
+// small requests' (small closest-point / ray steps first, then small silhouette steps,
+// large closest-point / ray steps, large silhouette steps).  A small request therefore
+// never shares a step with a large one, and the block scheduler places its blocks
+// ahead of the pending blocks of every large step.
+//
+// Step.  A step takes, for each kind it serves, the run of admitted requests of its
+// class that are contiguous in the ring (at most step_queries queries) and answers
+// them with one batch launch; closest-point and ray requests go to the general slots,
+// silhouette requests to slots of their own whose launches hold part of the GPU only;
 // inside the step a field with C components is stored component-major with stride m
 // (the step's query count) from ring offset off * C, which is where the kernel writes
 // it and what one device-to-host copy per field brings back.
+//
+// Host copies.  Staging a request's queries into the pinned ring and scattering its
+// results into its arrays are plain memory copies of up to ~10 MB a request; they are
+// split into chunks over a few helper threads, so that one large request does not hold
+// the worker (and every other request's admission and completion) for a millisecond.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -45,6 +57,114 @@ double now_s() {
     return duration<double>(steady_clock::now().time_since_epoch()).count();
 }
 
+// Memory copies and 32-bit fills, run by the calling thread and `helpers` threads
+// together on chunks of at most kChunk bytes; lists under kInline bytes run inline.
+class CopyPool {
+  public:
+    struct Job {
+        void *dst;
+        const void *src;  // nullptr: fill bytes / 4 words with `word`
+        size_t bytes;
+        uint32_t word;
+    };
+
+    ~CopyPool() { stop(); }
+
+    void start(int helpers) {
+        for (int i = 0; i < helpers; ++i) th_.emplace_back([this] { loop(); });
+    }
+
+    void stop() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            quit_ = true;
+        }
+        cv_.notify_all();
+        for (std::thread &t : th_) t.join();
+        th_.clear();
+    }
+
+    // Returns when every job is done.
+    void run(const std::vector<Job> &jobs) {
+        size_t total = 0;
+        for (const Job &j : jobs) total += j.bytes;
+        if (th_.empty() || total < kInline) {
+            for (const Job &j : jobs) exec(j);
+            return;
+        }
+        {
+            std::unique_lock<std::mutex> lk(mu_);
+            idle_cv_.wait(lk, [&] { return active_ == 0; });  // a helper still leaving the previous list
+            chunks_.clear();
+            for (const Job &j : jobs)
+                for (size_t o = 0; o < j.bytes; o += kChunk)
+                    chunks_.push_back(Job{static_cast<char *>(j.dst) + o,
+                                          j.src ? static_cast<const char *>(j.src) + o : nullptr,
+                                          std::min(kChunk, j.bytes - o), j.word});
+            next_.store(0, std::memory_order_relaxed);
+            done_.store(0, std::memory_order_relaxed);
+            ++gen_;
+        }
+        cv_.notify_all();
+        work();
+        const size_t n = chunks_.size();
+        while (done_.load(std::memory_order_acquire) < n) std::this_thread::yield();
+    }
+
+  private:
+    static constexpr size_t kChunk = 256 << 10, kInline = 512 << 10;  // kChunk: a multiple of 4 (fills)
+
+    static void exec(const Job &j) {
+        if (j.src) {
+            std::memcpy(j.dst, j.src, j.bytes);
+        } else {
+            uint32_t *d = static_cast<uint32_t *>(j.dst);
+            std::fill(d, d + j.bytes / 4, j.word);
+        }
+    }
+
+    // chunks_ does not change while a thread is in here (run() waits for active_ == 0)
+    void work() {
+        const size_t n = chunks_.size();
+        for (;;) {
+            const size_t i = next_.fetch_add(1, std::memory_order_relaxed);
+            if (i >= n) return;
+            exec(chunks_[i]);
+            done_.fetch_add(1, std::memory_order_release);
+        }
+    }
+
+    void loop() {
+        uint64_t seen = 0;
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return quit_ || gen_ != seen; });
+                if (quit_) return;
+                seen = gen_;
+                ++active_;
+            }
+            work();
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                --active_;
+            }
+            idle_cv_.notify_all();
+        }
+    }
+
+    std::vector<std::thread> th_;
+    std::mutex mu_;
+    std::condition_variable cv_, idle_cv_;
+    uint64_t gen_ = 0;
+    int active_ = 0;
+    bool quit_ = false;
+    std::vector<Job> chunks_;
+    std::atomic<size_t> next_{0}, done_{0};
+};
+
+constexpr int kSmall = 0, kLarge = 1;  // request size classes
+
 // Component counts of the fields of one query kind in dimension D.
 struct Fields {
     int a = 0, b = 0, r = 0;                 // inputs: floats per query
@@ -73,6 +193,7 @@ struct Req {
     double t_submit = 0, t_admit = 0, t_launch = 0;
     int64_t phys = 0;  // first ring slot
     size_t alloc = 0;  // allocation sequence number in its ring
+    int cls = kSmall;  // size class: which of its kind's rings it is in
     int step = -1;
 };
 
@@ -125,6 +246,7 @@ struct Slot {
     int32_t *err = nullptr;
     bool busy = false;
     bool sil_only = false;  // batch mode: this slot answers silhouette requests only
+    int cls = kSmall;       // size class of the requests it takes
     int step = -1;
     gq_status status = GQ_OK;
     std::vector<Req *> reqs;
@@ -136,14 +258,17 @@ struct Slot {
 struct gq_server {
     int dim = 0, device = 0, flags = 0;
     int64_t step_queries = 0, ring_bytes = 0, sil_step_queries = 0;
-    float sil_share = 0.8f;  // per silhouette slot
+    int64_t large_queries = 0;  // requests of at least this many queries are large (0: one class)
+    float sil_share = 0.8f;     // per silhouette slot
+    float large_share = 1.f;    // share of the GPU a large closest-point / ray step's persistent grid may hold
     std::vector<gq_scene *> scenes;
     gqd::DevScene *dev_scenes = nullptr;
-    Ring ring[3];
+    Ring ring[3][2];  // [kind][size class]
     std::vector<Slot> slots;
     cudaStream_t copy_st = nullptr;
     cudaEvent_t copy_evt = nullptr;
     std::vector<void *> dev_allocs, host_allocs;
+    CopyPool pool;
 
     std::thread worker;
     std::mutex mu;  // guards `submitted` and `completed`
@@ -154,7 +279,8 @@ struct gq_server {
     std::atomic<int64_t> outstanding{0};
 
     // worker-only state
-    std::deque<Req *> pending[3], admitted[3];
+    std::deque<Req *> pending[3][2], admitted[3][2];
+    std::vector<CopyPool::Job> jobs;
     int next_step = 0;
     int64_t admitted_bytes = 0;
     std::atomic<int64_t> admitted_peak{0}, requests_done{0}, queries_done{0}, steps{0};
@@ -164,6 +290,7 @@ struct gq_server {
         stop = true;
         cv.notify_all();
         if (worker.joinable()) worker.join();
+        pool.stop();
         DeviceGuard g(device);
         for (Slot &s : slots) {
             if (s.st) cudaStreamSynchronize(s.st);
@@ -175,14 +302,17 @@ struct gq_server {
         if (copy_st) cudaStreamDestroy(copy_st);
         for (void *p : dev_allocs) cudaFree(p);
         for (void *p : host_allocs) cudaFreeHost(p);
-        for (int k = 0; k < 3; ++k) {
-            for (Req *r : pending[k]) delete r;
-            for (Req *r : admitted[k]) delete r;
-        }
+        for (int k = 0; k < 3; ++k)
+            for (int c = 0; c < 2; ++c) {
+                for (Req *r : pending[k][c]) delete r;
+                for (Req *r : admitted[k][c]) delete r;
+            }
         for (Slot &s : slots)
             for (Req *r : s.reqs) delete r;
         for (Req *r : submitted) delete r;
     }
+
+    int class_of(int64_t n) const { return large_queries > 0 && n >= large_queries ? kLarge : kSmall; }
 
     template <typename T>
     cudaError_t dalloc(T **p, int64_t count) {
@@ -250,64 +380,60 @@ struct gq_server {
     bool intake() {
         std::lock_guard<std::mutex> lk(mu);
         if (submitted.empty()) return false;
-        for (Req *r : submitted) pending[r->q.kind].push_back(r);
+        for (Req *r : submitted) pending[r->q.kind][r->cls].push_back(r);
         submitted.clear();
         return true;
     }
 
-    // Admits pending requests while their ring has room and copies their inputs up.
+    // Admits pending requests while their ring has room, stages their queries in the
+    // pinned mirror and copies them up (one copy per field and contiguous run).
     bool admit() {
-        bool any = false;
         const int D = dim;
-        for (int k = 0; k < 3; ++k) {
-            Ring &R = ring[k];
-            int64_t run_lo = -1, run_hi = -1;  // contiguous run of new slots to copy up
-            auto flush = [&]() {
-                if (run_lo < 0) return;
-                const int64_t lo = run_lo, cnt = run_hi - run_lo;
-                cudaMemcpyAsync(R.a + lo * D, R.ha + lo * D, (size_t)cnt * D * 4, cudaMemcpyHostToDevice, copy_st);
-                if (R.f.b)
-                    cudaMemcpyAsync(R.b + lo * D, R.hb + lo * D, (size_t)cnt * D * 4, cudaMemcpyHostToDevice,
-                                    copy_st);
-                if (R.f.r) cudaMemcpyAsync(R.r + lo, R.hr + lo, (size_t)cnt * 4, cudaMemcpyHostToDevice, copy_st);
-                cudaMemcpyAsync(R.sid + lo, R.hsid + lo, (size_t)cnt * 4, cudaMemcpyHostToDevice, copy_st);
-                run_lo = run_hi = -1;
-            };
-            while (!pending[k].empty()) {
-                Req *r = pending[k].front();
-                int64_t phys;
-                size_t seq;
-                if (!R.alloc(r->q.n, &phys, &seq)) break;
-                pending[k].pop_front();
-                r->phys = phys;
-                r->alloc = seq;
-                r->t_admit = now_s();
-                const int64_t n = r->q.n;
-                std::memcpy(R.ha + phys * D, r->q.a, (size_t)n * D * 4);
-                if (R.f.b) std::memcpy(R.hb + phys * D, r->q.b, (size_t)n * D * 4);
-                if (R.f.r) {
-                    if (r->q.r_max)
-                        std::memcpy(R.hr + phys, r->q.r_max, (size_t)n * 4);
+        struct Run {
+            Ring *R;
+            int64_t lo, hi;
+        };
+        std::vector<Run> runs;
+        jobs.clear();
+        for (int k = 0; k < 3; ++k)
+            for (int c = 0; c < 2; ++c) {
+                Ring &R = ring[k][c];
+                while (!pending[k][c].empty()) {
+                    Req *r = pending[k][c].front();
+                    int64_t phys;
+                    size_t seq;
+                    if (!R.alloc(r->q.n, &phys, &seq)) break;
+                    pending[k][c].pop_front();
+                    r->phys = phys;
+                    r->alloc = seq;
+                    r->t_admit = now_s();
+                    const int64_t n = r->q.n;
+                    jobs.push_back({R.ha + phys * D, r->q.a, (size_t)n * D * 4, 0});
+                    if (R.f.b) jobs.push_back({R.hb + phys * D, r->q.b, (size_t)n * D * 4, 0});
+                    if (R.f.r) jobs.push_back({R.hr + phys, r->q.r_max, (size_t)n * 4, 0x7f800000u});  // NULL: +inf
+                    jobs.push_back({R.hsid + phys, nullptr, (size_t)n * 4, (uint32_t)r->q.scene});
+                    if (!runs.empty() && runs.back().R == &R && runs.back().hi == phys)
+                        runs.back().hi += n;
                     else
-                        std::fill(R.hr + phys, R.hr + phys + n, __builtin_inff());
+                        runs.push_back({&R, phys, phys + n});
+                    admitted_bytes += n * R.f.bytes_per_query();
+                    if (admitted_bytes > admitted_peak) admitted_peak = admitted_bytes;
+                    admitted[k][c].push_back(r);
                 }
-                std::fill(R.hsid + phys, R.hsid + phys + n, r->q.scene);
-                if (run_lo >= 0 && phys == run_hi) {
-                    run_hi += n;
-                } else {
-                    flush();
-                    run_lo = phys;
-                    run_hi = phys + n;
-                }
-                admitted_bytes += n * R.f.bytes_per_query();
-                if (admitted_bytes > admitted_peak) admitted_peak = admitted_bytes;
-                admitted[k].push_back(r);
-                any = true;
             }
-            flush();
+        if (runs.empty()) return false;
+        pool.run(jobs);
+        for (const Run &u : runs) {
+            Ring &R = *u.R;
+            const int64_t lo = u.lo, cnt = u.hi - u.lo;
+            cudaMemcpyAsync(R.a + lo * D, R.ha + lo * D, (size_t)cnt * D * 4, cudaMemcpyHostToDevice, copy_st);
+            if (R.f.b)
+                cudaMemcpyAsync(R.b + lo * D, R.hb + lo * D, (size_t)cnt * D * 4, cudaMemcpyHostToDevice, copy_st);
+            if (R.f.r) cudaMemcpyAsync(R.r + lo, R.hr + lo, (size_t)cnt * 4, cudaMemcpyHostToDevice, copy_st);
+            cudaMemcpyAsync(R.sid + lo, R.hsid + lo, (size_t)cnt * 4, cudaMemcpyHostToDevice, copy_st);
         }
-        if (any) cudaEventRecord(copy_evt, copy_st);
-        return any;
+        cudaEventRecord(copy_evt, copy_st);
+        return true;
     }
 
     // Device output record of one kind for a step range; fields component-major with stride m.
@@ -334,39 +460,40 @@ struct gq_server {
 
     bool launch() {
         bool any = false;
+        const bool per_req = (flags & GQ_SERVER_PER_REQUEST) != 0;
         for (Slot &S : slots) {
             if (S.busy) continue;
+            auto serves = [&](int k) { return per_req || (k == GQ_KIND_SILHOUETTE) == S.sil_only; };
             bool have = false;
-            for (int k = 0; k < 3; ++k)
-                if (!(flags & GQ_SERVER_PER_REQUEST) && (k == GQ_KIND_SILHOUETTE) != S.sil_only) continue;
-                else have |= !admitted[k].empty();
+            for (int k = 0; k < 3; ++k) have |= serves(k) && !admitted[k][S.cls].empty();
             if (!have) continue;
             S.reqs.clear();
             for (int k = 0; k < 3; ++k) S.off[k] = 0, S.m[k] = 0;
-            if (flags & GQ_SERVER_PER_REQUEST) {
+            if (per_req) {
                 int kb = -1;  // oldest admitted request of any kind
                 for (int k = 0; k < 3; ++k)
-                    if (!admitted[k].empty() &&
-                        (kb < 0 || admitted[k].front()->t_admit < admitted[kb].front()->t_admit))
+                    if (!admitted[k][S.cls].empty() &&
+                        (kb < 0 || admitted[k][S.cls].front()->t_admit < admitted[kb][S.cls].front()->t_admit))
                         kb = k;
-                Req *r = admitted[kb].front();
-                admitted[kb].pop_front();
+                Req *r = admitted[kb][S.cls].front();
+                admitted[kb][S.cls].pop_front();
                 S.off[kb] = r->phys;
                 S.m[kb] = r->q.n;
                 S.reqs.push_back(r);
             } else {
                 for (int k = 0; k < 3; ++k) {
-                    if ((k == GQ_KIND_SILHOUETTE) != S.sil_only) continue;
-                    const int64_t cap = S.sil_only ? sil_step_queries : step_queries;
-                    while (!admitted[k].empty()) {
-                        Req *r = admitted[k].front();
+                    if (!serves(k)) continue;
+                    const int64_t cap = S.sil_only && S.cls == kSmall ? sil_step_queries : step_queries;
+                    std::deque<Req *> &q = admitted[k][S.cls];
+                    while (!q.empty()) {
+                        Req *r = q.front();
                         if (S.m[k] == 0)
                             S.off[k] = r->phys;
                         else if (r->phys != S.off[k] + S.m[k] || S.m[k] + r->q.n > cap)
                             break;
                         S.m[k] += r->q.n;
                         S.reqs.push_back(r);
-                        admitted[k].pop_front();
+                        q.pop_front();
                     }
                 }
             }
@@ -376,7 +503,7 @@ struct gq_server {
             cudaStreamWaitEvent(S.st, copy_evt, 0);
             S.status = run_step(S);
             for (int k = 0; k < 3; ++k)
-                if (S.m[k]) copy_down(ring[k], S.off[k], S.m[k], S.st);
+                if (S.m[k]) copy_down(ring[k][S.cls], S.off[k], S.m[k], S.st);
             cudaEventRecord(S.done, S.st);
             S.busy = true;
             ++steps;
@@ -390,7 +517,7 @@ struct gq_server {
         if (flags & GQ_SERVER_PER_REQUEST) {
             Req *r = S.reqs.front();
             const int k = r->q.kind;
-            Ring &R = ring[k];
+            Ring &R = ring[k][S.cls];
             const int64_t off = r->phys, n = r->q.n;
             const gq_scene *sc = scenes[(size_t)r->q.scene];
             gq_query_opts o{GQ_VARIANT_AUTO, 1, nullptr, S.scratch, (int64_t)S.scratch_bytes};
@@ -415,7 +542,7 @@ struct gq_server {
         gq_sil_out so{};
         for (int k = 0; k < 3; ++k) {
             if (!S.m[k]) continue;
-            Ring &R = ring[k];
+            Ring &R = ring[k][S.cls];
             const int64_t off = S.off[k];
             kinds[k].a = gq_vecs{R.a + off * D, 1, D};
             if (R.f.b) kinds[k].b = gq_vecs{R.b + off * D, 1, D};
@@ -423,31 +550,38 @@ struct gq_server {
             kinds[k].scene = R.sid + off;
             kinds[k].n = S.m[k];
         }
-        if (S.m[0]) step_outputs(ring[0], S.off[0], &co, nullptr, nullptr);
-        if (S.m[1]) step_outputs(ring[1], S.off[1], nullptr, &ro, nullptr);
-        if (S.m[2]) step_outputs(ring[2], S.off[2], nullptr, nullptr, &so);
+        if (S.m[0]) step_outputs(ring[0][S.cls], S.off[0], &co, nullptr, nullptr);
+        if (S.m[1]) step_outputs(ring[1][S.cls], S.off[1], nullptr, &ro, nullptr);
+        if (S.m[2]) step_outputs(ring[2][S.cls], S.off[2], nullptr, nullptr, &so);
         bool all_wide = true;
         for (const gq_scene *sc : scenes) all_wide &= sc->has_wide;
+        const float share = S.sil_only ? sil_share : S.cls == kLarge ? large_share : 1.f;
+        // One-warp blocks: the silhouette steps' one-warp blocks end all the time, and a
+        // block of this step fits in the room any one of them leaves (a 128-thread block
+        // would wait for four to end on the same SM while lower-priority one-warp blocks
+        // take each single slot).  Small steps are not sorted: the keys and the radix
+        // sort are launches of large blocks that would wait the same way, and a small
+        // step's requests are contiguous runs of one scene each already.
         cudaError_t e = gqd::batch_run(dev_scenes, (int)scenes.size(), D, kinds, co, ro, so,
                                        (flags & GQ_BATCH_RAY_EXACT) || !all_wide ? 0 : 1,
-                                       gqd::cp_mode_of(flags), gqd::sil_mode_of(flags),
-                                       S.sil_only ? sil_share : 1.f, S.scratch, step_queries, S.err, S.st);
+                                       gqd::cp_mode_of(flags), gqd::sil_mode_of(flags), share, 32,
+                                       S.cls == kLarge || !large_queries, S.scratch, step_queries, S.err, S.st);
         return e == cudaSuccess ? GQ_OK : fail_cuda(e, "server step");
     }
 
-    // Copies one request's results from the pinned ring to its host buffers.
+    // Queues the copies of one request's results from the pinned ring to its host buffers.
     void scatter(const Slot &S, const Req *r) {
         const int k = r->q.kind;
-        const Ring &R = ring[k];
+        const Ring &R = ring[k][r->cls];
         const Fields &f = R.f;
         const int64_t off = S.off[k], m = S.m[k], n = r->q.n, i0 = r->phys - off;
         auto vec = [&](float *dst, const float *h, int comps) {
             if (!dst) return;
             for (int c = 0; c < comps; ++c)
-                std::memcpy(dst + (int64_t)c * n, h + off * comps + (int64_t)c * m + i0, (size_t)n * 4);
+                jobs.push_back({dst + (int64_t)c * n, h + off * comps + (int64_t)c * m + i0, (size_t)n * 4, 0});
         };
         auto one = [&](void *dst, const void *h, size_t es) {
-            if (dst) std::memcpy(dst, static_cast<const char *>(h) + (size_t)(off + i0) * es, (size_t)n * es);
+            if (dst) jobs.push_back({dst, static_cast<const char *>(h) + (size_t)(off + i0) * es, (size_t)n * es, 0});
         };
         if (k == GQ_KIND_CLOSEST_POINT) {
             const gq_cp_out &o = r->q.cp_out;
@@ -484,11 +618,15 @@ struct gq_server {
             gq_status st = S.status;
             if (q != cudaSuccess) st = fail_cuda(q, "server step");
             if (st != GQ_OK) launch_error = st;
+            if (st == GQ_OK) {
+                jobs.clear();
+                for (Req *r : S.reqs) scatter(S, r);
+                pool.run(jobs);
+            }
             const double t = now_s();
             for (Req *r : S.reqs) {
-                if (st == GQ_OK) scatter(S, r);
-                admitted_bytes -= r->q.n * ring[r->q.kind].f.bytes_per_query();
-                ring[r->q.kind].release(r->alloc);
+                admitted_bytes -= r->q.n * ring[r->q.kind][r->cls].f.bytes_per_query();
+                ring[r->q.kind][r->cls].release(r->alloc);
                 finish(r, t, st);
             }
             S.reqs.clear();
@@ -508,7 +646,8 @@ struct gq_server {
             if (did) continue;
             bool busy = false;
             for (const Slot &S : slots) busy |= S.busy;
-            for (int k = 0; k < 3; ++k) busy |= !pending[k].empty() || !admitted[k].empty();
+            for (int k = 0; k < 3; ++k)
+                for (int c = 0; c < 2; ++c) busy |= !pending[k][c].empty() || !admitted[k][c].empty();
             if (busy) {
                 std::this_thread::yield();
             } else {
@@ -524,7 +663,8 @@ struct gq_server {
     gq_status submit(const gq_request &q, double t_submit) {
         if (q.kind < 0 || q.kind > 2) return fail(GQ_ERR_INVALID, "unknown query kind");
         if (q.scene < 0 || q.scene >= (int32_t)scenes.size()) return fail(GQ_ERR_INVALID, "scene index out of range");
-        if (q.n < 1 || q.n > step_queries || q.n > ring[q.kind].cap)
+        const int cls = q.n >= 1 ? class_of(q.n) : kSmall;
+        if (q.n < 1 || q.n > step_queries || q.n > ring[q.kind][cls].cap)
             return fail(GQ_ERR_INVALID, "request size must be in [1, step_queries] and fit its ring (" +
                                             std::to_string(q.n) + " queries)");
         if (!q.a || (q.kind == GQ_KIND_INTERSECT && !q.b)) return fail(GQ_ERR_INVALID, "null query array");
@@ -533,6 +673,7 @@ struct gq_server {
         Req *r = new (std::nothrow) Req();
         if (!r) return fail(GQ_ERR_NOMEM, "host allocation");
         r->q = q;
+        r->cls = cls;
         r->t_submit = t_submit;
         ++outstanding;
         {
@@ -574,12 +715,22 @@ gq_status gq_server_create(gq_scene *const *scenes, int32_t n_scenes, const gq_s
         views[(size_t)i] = sc->dev;
         s->scenes.push_back(sc);
     }
+    const bool per_request = (s->flags & GQ_SERVER_PER_REQUEST) != 0;
+    // the large class: on by default, off in the plain per-request mode or when no
+    // request can reach it
+    const int64_t lq = o.large_queries != 0 ? o.large_queries : (1 << 15);
+    s->large_queries = (!per_request && lq > 0 && lq <= s->step_queries) ? lq : 0;
+    s->large_share = o.large_share > 0.f ? std::min(1.f, o.large_share) : 1.f;
     int64_t ring_bytes = 0;
     for (int k = 0; k < 3; ++k) {
-        Ring &R = s->ring[k];
-        R.f = fields_of(k, s->dim);
-        R.cap = o.ring_queries[k] > 0 ? o.ring_queries[k] : (1 << 22);
-        ring_bytes += R.cap * R.f.bytes_per_query();
+        const int64_t cap = o.ring_queries[k] > 0 ? o.ring_queries[k] : (1 << 22);
+        const int64_t large = s->large_queries ? cap / 2 : 0;
+        for (int c = 0; c < 2; ++c) {
+            Ring &R = s->ring[k][c];
+            R.f = fields_of(k, s->dim);
+            R.cap = c == kLarge ? large : cap - large;
+            ring_bytes += R.cap * R.f.bytes_per_query();
+        }
     }
     s->ring_bytes = ring_bytes;
     if (o.budget_bytes > 0 && ring_bytes > o.budget_bytes)
@@ -589,38 +740,54 @@ gq_status gq_server_create(gq_scene *const *scenes, int32_t n_scenes, const gq_s
     cudaError_t e = s->dalloc(&s->dev_scenes, n_scenes);
     if (e == cudaSuccess)
         e = cudaMemcpy(s->dev_scenes, views.data(), views.size() * sizeof(gqd::DevScene), cudaMemcpyHostToDevice);
-    for (int k = 0; k < 3 && e == cudaSuccess; ++k) e = s->make_ring(s->ring[k]);
-    // closest-point / ray steps and the copies on the highest stream priority, silhouette
-    // steps (long, persistent launches) on the lowest: when both wait for SMs, the short
-    // kinds' blocks are scheduled first
+    for (int k = 0; k < 3 && e == cudaSuccess; ++k)
+        for (int c = 0; c < 2 && e == cudaSuccess; ++c) e = s->make_ring(s->ring[k][c]);
+    // Stream priorities, highest first: the copies and small closest-point / ray steps,
+    // small silhouette steps, large closest-point / ray steps, large silhouette steps
+    // (clamped to the device's range).  When several launches wait for SMs, the blocks
+    // of the shorter requests are scheduled first.
     int prio_low = 0, prio_high = 0;
     if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+    auto level = [&](int i) { return std::min(prio_low, prio_high + i); };  // prio_high <= prio_low
     if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&s->copy_st, cudaStreamNonBlocking, prio_high);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->copy_evt, cudaEventDisableTiming);
-    const bool per_request = (s->flags & GQ_SERVER_PER_REQUEST) != 0;
     const int sil_slots = per_request ? 0 : (o.sil_slots > 0 ? o.sil_slots : 3);
+    const int large_slots = s->large_queries ? (o.large_slots > 0 ? o.large_slots : 2) : 0;
     s->sil_share = std::min(1.f, s->sil_share / (float)std::max(sil_slots, 1));
     s->sil_step_queries = std::min<int64_t>(s->step_queries, o.sil_step_queries > 0 ? o.sil_step_queries : (1 << 15));
-    s->slots.resize((size_t)(inflight + sil_slots));
-    for (int i = 0; i < sil_slots; ++i) s->slots[(size_t)(inflight + i)].sil_only = true;
-    for (Slot &S : s->slots) {
-        if (e == cudaSuccess)
-            e = cudaStreamCreateWithPriority(&S.st, cudaStreamNonBlocking, S.sil_only ? prio_low : prio_high);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S.done, cudaEventDisableTiming);
-        S.scratch_bytes = (s->flags & GQ_SERVER_PER_REQUEST) ? (size_t)gq_query_scratch_bytes(s->step_queries)
-                                                             : gqd::batch_scratch_bytes(s->step_queries);
-        char *sp = nullptr;
-        if (e == cudaSuccess) e = s->dalloc(&sp, (int64_t)S.scratch_bytes);
-        S.scratch = sp;
-        if (e == cudaSuccess) e = s->dalloc(&S.err, 64);
-        if (e == cudaSuccess) e = cudaMemset(S.err, 0, 64 * sizeof(int32_t));
-    }
+    struct Group {
+        int count;
+        bool sil;
+        int cls, prio;
+    };
+    const Group groups[4] = {{inflight, false, kSmall, level(0)},
+                             {sil_slots, true, kSmall, level(1)},
+                             {large_slots, false, kLarge, level(2)},
+                             {large_slots, true, kLarge, prio_low}};
+    for (const Group &gr : groups)
+        for (int i = 0; i < gr.count && e == cudaSuccess; ++i) {
+            s->slots.emplace_back();
+            Slot &S = s->slots.back();
+            S.sil_only = gr.sil;
+            S.cls = gr.cls;
+            e = cudaStreamCreateWithPriority(&S.st, cudaStreamNonBlocking, gr.prio);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S.done, cudaEventDisableTiming);
+            S.scratch_bytes = per_request ? (size_t)gq_query_scratch_bytes(s->step_queries)
+                                          : gqd::batch_scratch_bytes(s->step_queries);
+            char *sp = nullptr;
+            if (e == cudaSuccess) e = s->dalloc(&sp, (int64_t)S.scratch_bytes);
+            S.scratch = sp;
+            if (e == cudaSuccess) e = s->dalloc(&S.err, 64);
+            if (e == cudaSuccess) e = cudaMemset(S.err, 0, 64 * sizeof(int32_t));
+        }
     if (e != cudaSuccess) return fail(GQ_ERR_NOMEM, std::string("server allocation: ") + cudaGetErrorString(e));
     gq_server *raw = s.get();
     try {
+        const int hw = (int)std::thread::hardware_concurrency();
+        s->pool.start(o.copy_threads > 0 ? o.copy_threads - 1 : std::max(0, std::min(7, hw / 2 - 1)));
         s->worker = std::thread([raw] { raw->run(); });
     } catch (...) {
-        return fail(GQ_ERR_NOMEM, "cannot start the worker thread");
+        return fail(GQ_ERR_NOMEM, "cannot start the worker or copy threads");
     }
     *out = s.release();
     return GQ_OK;

@@ -109,12 +109,21 @@ class Server:
     reference order with long traversals taken over one per warp ("split": cheaper than
     a warp-coherent walk when neighbours are far apart, and the slowest query no longer
     sets the step time) and silhouettes to one query per warp ("warp": bounds the
-    latency of far-reaching ones)."""
+    latency of far-reaching ones).
+
+    large_queries: requests of at least this many queries form a second size class
+    (half of each kind's ring, large_slots slots per kind group, lower stream
+    priorities), so small requests never share a step with large ones and their blocks
+    are placed first; a negative value keeps one class.  large_share caps the
+    persistent grid of a large closest-point / ray step; copy_threads: host threads
+    for staging queries and scattering results (0: about half the cores, at most 8)."""
 
     def __init__(self, scenes: Sequence[Scene], *, budget_bytes: int = 0, ring_queries=(1 << 22,) * 3,
                  step_queries: int = 1 << 19, max_inflight: int = 3, per_request: bool = False,
                  cp_variant: str = "split", ray_variant: str = "wide8", sil_variant: str = "warp",
-                 sil_share: float = 1.5, sil_slots: int = 3, sil_step_queries: int = 1 << 15):
+                 sil_share: float = 1.5, sil_slots: int = 3, sil_step_queries: int = 1 << 15,
+                 large_queries: int = 1 << 15, large_slots: int = 2, large_share: float = 1.0,
+                 copy_threads: int = 0):
         self.scenes = list(scenes)
         self.dim = self.scenes[0].dim
         flags = (L.SERVER_PER_REQUEST if per_request else 0) | \
@@ -124,7 +133,8 @@ class Server:
              L.BATCH_SIL_SPLIT if sil_variant == "split" else 0)
         rq = [int(ring_queries)] * 3 if isinstance(ring_queries, int) else [int(x) for x in ring_queries]
         opts = L.ServerOpts(int(budget_bytes), (C.c_int64 * 3)(*rq), int(step_queries), int(max_inflight), flags,
-                            float(sil_share), int(sil_slots), int(sil_step_queries))
+                            float(sil_share), int(sil_slots), int(sil_step_queries), int(large_queries),
+                            int(large_slots), float(large_share), int(copy_threads))
         arr = (C.c_void_p * len(self.scenes))(*[s.handle.value for s in self.scenes])
         h = C.c_void_p()
         L.check(L.lib().gq_server_create(arr, len(self.scenes), C.byref(opts), C.byref(h)))

@@ -346,16 +346,25 @@ gq_status gq_batch_device_error(gq_batch *batch, void *stream, int32_t *flags);
  * a step slot is free: one gq_batch launch for all scenes (or, with
  * GQ_SERVER_PER_REQUEST, one single-scene call per request, the scene's tuned
  * variant).  Closest-point and ray requests share max_inflight slots; silhouette
- * requests, whose traversals are far longer, have sil_slots slots of their own on the
- * lowest stream priority, taking at most sil_step_queries queries each, so the other
- * kinds never queue behind them and a small silhouette request does not wait for a
- * large one.  Silhouette steps in the default one-query-per-warp form launch one block
- * per query that exits when its query is answered, so the blocks of the higher-priority
- * closest-point / ray steps are placed first and silhouettes fill the rest of the GPU;
- * the other silhouette forms run persistent launches that together hold at most
- * sil_share of the GPU.
+ * requests, whose traversals are far longer, have sil_slots slots of their own on a
+ * lower stream priority, taking at most sil_step_queries queries each, so the other
+ * kinds never queue behind them.  Requests of at least large_queries queries form a
+ * second size class with rings and slots of its own (large_slots for closest points /
+ * rays and as many for silhouettes) on still lower priorities, so a small request
+ * never shares a step with a large one and its blocks are placed ahead of a large
+ * step's pending blocks.  Silhouette steps in the default one-query-per-warp form launch
+ * one block per query that exits when its query is answered, so the blocks of
+ * higher-priority steps are placed first and silhouettes fill the rest of the GPU; the
+ * other silhouette forms run persistent launches that together hold at most sil_share
+ * of the GPU.  Staging queries into the pinned rings and scattering results into the
+ * requests' arrays run on copy_threads host threads.
  * Each slot has its own stream, so the results of one step go back to the host while
- * the next computes.  Results are those of gq_batch_run. */
+ * the next computes.  Results are those of gq_batch_run.
+ * Streams: 1 + max_inflight + sil_slots + 2 * large_slots (11 by default).  CUDA maps
+ * streams onto CUDA_DEVICE_MAX_CONNECTIONS hardware queues (8 unless the variable is
+ * set before the CUDA context is created) and runs the work of streams that share a
+ * queue in order, so a process that serves should set it to 32: otherwise a short step
+ * can wait for a long one on its queue. */
 typedef struct gq_server gq_server;
 
 #define GQ_SERVER_PER_REQUEST 4 /* one single-scene launch per request instead of batched steps */
@@ -369,7 +378,14 @@ typedef struct {
     float sil_share;          /* share of the GPU's resident blocks all persistent silhouette steps together may hold (0: 1.5;
                                  above 1 they may oversubscribe it, each slot capped at 1) */
     int32_t sil_slots;        /* silhouette step slots (0: 3) */
-    int64_t sil_step_queries; /* most silhouette queries in one step, unless one request is larger (0: 1<<15) */
+    int64_t sil_step_queries; /* most silhouette queries in one small-class step, unless one request is larger (0: 1<<15) */
+    int64_t large_queries;    /* requests of at least this many queries are large (0: 1<<15; negative: one class;
+                                 also one class when above step_queries or with GQ_SERVER_PER_REQUEST).  With two
+                                 classes each kind's ring is split in halves, one per class */
+    int32_t large_slots;      /* step slots of the large class, for closest points / rays and for silhouettes each (0: 2) */
+    float large_share;        /* share of the GPU's resident blocks a large closest-point / ray step's persistent grid
+                                 may hold (0: 1) */
+    int32_t copy_threads;     /* host threads for staging and scattering, the worker included (0: min(8, cores / 2)) */
 } gq_server_opts;
 
 typedef struct {

@@ -2,6 +2,9 @@ import os
 import sys
 from pathlib import Path
 
+# hardware work queues for the serving runtime's streams (read when the CUDA context is created)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 import pytest
 
 ROOT = Path(__file__).resolve().parent.parent

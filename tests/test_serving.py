@@ -87,6 +87,32 @@ def test_results_same_alone_and_in_the_mix(scenes):
     _check_same_as_alone(scenes, reqs)
 
 
+def test_large_class_steps_hold_one_class(scenes):
+    # requests of >= 1000 queries are large: their own rings, steps and slots; a few of
+    # 40-70 K queries make the host copies run on the copy threads
+    reqs = _requests(150, len(scenes), seed=12)
+    rng = np.random.default_rng(14)
+    for i, kind in enumerate(("cp", "ray", "sil", "cp", "sil", "ray")):
+        c = int(rng.integers(40_000, 70_000))
+        pts = rng.uniform(-2.0, 2.0, size=(c, 3)).astype(np.float32)
+        d = rng.standard_normal((c, 3))
+        d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+        reqs.insert(20 * i + 5, HostRequest.make(i % len(scenes), kind, pts, d if kind == "ray" else None))
+    srv = Server(scenes, ring_queries=(1 << 18,) * 3, step_queries=1 << 17, max_inflight=2, large_queries=1000)
+    res = srv.run_trace(reqs, poisson_arrivals(60_000.0, len(reqs), np.random.default_rng(13)))
+    st = srv.stats()
+    assert st["device_error"] == 0 and st["requests_done"] == len(reqs)
+    large = res["n"] >= 1000
+    assert large.any() and (~large).any()
+    steps, per_step = np.unique(res["step"], return_counts=True)
+    for s in steps:
+        m = res["step"] == s
+        assert large[m].all() or not large[m].any(), f"step {s} mixes size classes"
+    assert per_step.max() > 1, "no step served more than one request"
+    _check_same_as_alone(scenes, reqs)
+    srv.close()
+
+
 def test_per_request_mode_same_as_alone(scenes):
     reqs = _requests(40, len(scenes), seed=3)
     srv = Server(scenes, ring_queries=(1 << 16,) * 3, step_queries=1 << 14, per_request=True)
