@@ -593,7 +593,7 @@ def section_c4(args, dev):
                  "loads": []}
         if sat_rate is None:
             sat_rate = sat["requests_per_s"]
-        for frac in ((0.5, 0.8) if mode == "batched" else (0.8,)):
+        for frac in ((0.3, 0.5, 0.65, 0.8) if mode == "batched" else (0.8,)):
             r = srv.run_trace(reqs, poisson_arrivals(frac * sat_rate, len(reqs), np.random.default_rng(9)))
             sm = summarize(r)
             entry["loads"].append({"load_of_batched_peak": frac, "arrivals_per_s": frac * sat_rate,
