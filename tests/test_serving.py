@@ -87,9 +87,11 @@ def test_results_same_alone_and_in_the_mix(scenes):
     _check_same_as_alone(scenes, reqs)
 
 
-def test_large_class_steps_hold_one_class(scenes):
+@pytest.mark.parametrize("cp_variant,sil_variant", [("split", "warp"), ("coherent", "coherent")])
+def test_large_class_steps_hold_one_class(scenes, cp_variant, sil_variant):
     # requests of >= 1000 queries are large: their own rings, steps and slots; a few of
-    # 40-70 K queries make the host copies run on the copy threads
+    # 40-70 K queries make the host copies run on the copy threads.  Small steps are not
+    # sorted, so the warp-coherent forms see queries of several scenes in one tile.
     reqs = _requests(150, len(scenes), seed=12)
     rng = np.random.default_rng(14)
     for i, kind in enumerate(("cp", "ray", "sil", "cp", "sil", "ray")):
@@ -98,7 +100,8 @@ def test_large_class_steps_hold_one_class(scenes):
         d = rng.standard_normal((c, 3))
         d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
         reqs.insert(20 * i + 5, HostRequest.make(i % len(scenes), kind, pts, d if kind == "ray" else None))
-    srv = Server(scenes, ring_queries=(1 << 18,) * 3, step_queries=1 << 17, max_inflight=2, large_queries=1000)
+    srv = Server(scenes, ring_queries=(1 << 18,) * 3, step_queries=1 << 17, max_inflight=2, large_queries=1000,
+                 cp_variant=cp_variant, sil_variant=sil_variant)
     res = srv.run_trace(reqs, poisson_arrivals(60_000.0, len(reqs), np.random.default_rng(13)))
     st = srv.stats()
     assert st["device_error"] == 0 and st["requests_done"] == len(reqs)
