@@ -114,7 +114,8 @@ class Completion(C.Structure):
 
 class ServerStats(C.Structure):
     _fields_ = [("requests_done", C.c_int64), ("queries_done", C.c_int64), ("steps", C.c_int64),
-                ("admitted_bytes_peak", C.c_int64), ("device_bytes", C.c_int64), ("device_error", C.c_int32)]
+                ("admitted_bytes_peak", C.c_int64), ("device_bytes", C.c_int64), ("device_error", C.c_int32),
+                ("large_queries", C.c_int64)]
 
 
 class BatchQueries(C.Structure):

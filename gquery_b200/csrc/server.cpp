@@ -716,10 +716,14 @@ gq_status gq_server_create(gq_scene *const *scenes, int32_t n_scenes, const gq_s
         s->scenes.push_back(sc);
     }
     const bool per_request = (s->flags & GQ_SERVER_PER_REQUEST) != 0;
-    // the large class: on by default, off in the plain per-request mode or when no
-    // request can reach it
+    // the large class: on by default; off in the plain per-request mode, when no request
+    // can reach it, or when half of a kind's ring could not hold a largest request (the
+    // split would refuse requests one ring admits)
     const int64_t lq = o.large_queries != 0 ? o.large_queries : (1 << 15);
-    s->large_queries = (!per_request && lq > 0 && lq <= s->step_queries) ? lq : 0;
+    bool halves_fit = true;
+    for (int k = 0; k < 3; ++k)
+        halves_fit &= (o.ring_queries[k] > 0 ? o.ring_queries[k] : (1 << 22)) / 2 >= s->step_queries;
+    s->large_queries = (!per_request && lq > 0 && lq <= s->step_queries && halves_fit) ? lq : 0;
     s->large_share = o.large_share > 0.f ? std::min(1.f, o.large_share) : 1.f;
     int64_t ring_bytes = 0;
     for (int k = 0; k < 3; ++k) {
@@ -833,6 +837,7 @@ gq_status gq_server_get_stats(gq_server *s, gq_server_stats *st) {
     st->steps = s->steps.load();
     st->admitted_bytes_peak = s->admitted_peak.load();
     st->device_bytes = s->ring_bytes;
+    st->large_queries = s->large_queries;
     if (s->outstanding.load() == 0) {  // error words are read only while nothing runs
         DeviceGuard g(s->device);
         if (!g.ok) return fail(GQ_ERR_CUDA, "cannot select the server's CUDA device");

@@ -380,8 +380,9 @@ typedef struct {
     int32_t sil_slots;        /* silhouette step slots (0: 3) */
     int64_t sil_step_queries; /* most silhouette queries in one small-class step, unless one request is larger (0: 1<<15) */
     int64_t large_queries;    /* requests of at least this many queries are large (0: 1<<15; negative: one class;
-                                 also one class when above step_queries or with GQ_SERVER_PER_REQUEST).  With two
-                                 classes each kind's ring is split in halves, one per class */
+                                 also one class when above step_queries, with GQ_SERVER_PER_REQUEST, or when half
+                                 of a kind's ring is below step_queries).  With two classes each kind's ring is
+                                 split in halves, one per class */
     int32_t large_slots;      /* step slots of the large class, for closest points / rays and for silhouettes each (0: 2) */
     float large_share;        /* share of the GPU's resident blocks a large closest-point / ray step's persistent grid
                                  may hold (0: 1) */
@@ -413,6 +414,7 @@ typedef struct {
 typedef struct {
     int64_t requests_done, queries_done, steps, admitted_bytes_peak, device_bytes;
     int32_t device_error; /* or-ed error words of the step slots and scenes (gq_batch_device_error bits) */
+    int64_t large_queries; /* size of the smallest large request, 0 when the server keeps one class */
 } gq_server_stats;
 
 double gq_server_clock(void);

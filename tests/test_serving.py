@@ -107,6 +107,7 @@ def test_large_class_steps_hold_one_class(scenes, cp_variant, sil_variant):
     assert st["device_error"] == 0 and st["requests_done"] == len(reqs)
     large = res["n"] >= 1000
     assert large.any() and (~large).any()
+    assert st["large_queries"] == 1000
     steps, per_step = np.unique(res["step"], return_counts=True)
     for s in steps:
         m = res["step"] == s
@@ -114,6 +115,23 @@ def test_large_class_steps_hold_one_class(scenes, cp_variant, sil_variant):
     assert per_step.max() > 1, "no step served more than one request"
     _check_same_as_alone(scenes, reqs)
     srv.close()
+
+
+def test_size_classes_only_where_half_rings_hold_a_largest_request(scenes):
+    # halves of 2,048 slots cannot hold a 4,096-query request: one class, all of the ring
+    one = Server(scenes, ring_queries=(4096,) * 3, step_queries=4096, large_queries=1000)
+    two = Server(scenes, ring_queries=(8192,) * 3, step_queries=4096, large_queries=1000)
+    plain = Server(scenes, ring_queries=(8192,) * 3, step_queries=4096, large_queries=1000, per_request=True)
+    try:
+        assert one.stats()["large_queries"] == 0
+        assert two.stats()["large_queries"] == 1000
+        assert plain.stats()["large_queries"] == 0
+        big = HostRequest.make(0, "cp", np.zeros((4096, 3), np.float32))
+        one.submit(big)  # fits the single ring
+        assert len(one.wait_idle(60.0)) == 1 and big.completion["status"] == 0
+    finally:
+        for s in (one, two, plain):
+            s.close()
 
 
 def test_per_request_mode_same_as_alone(scenes):
