@@ -23,6 +23,10 @@ namespace gqd {
 namespace pkt {
 
 constexpr int kNone = 0x7fffffff;
+// Largest key of a hit child of a wide node: unused and missed child slots sort as +inf,
+// and a hit whose key overflowed to +inf (a query with an infinite or huge coordinate)
+// is clamped so that the hits stay ahead of them in the sorted order.
+constexpr float kMaxHitKey = 3.40282347e38f;
 constexpr float kSlack = 1.0000038f;  // 1 + 2^-18
 constexpr int kPStack = 96;
 
@@ -260,8 +264,9 @@ __device__ __forceinline__ void closest_point(const DevScene &s, unsigned mask, 
             int cnt = 0;
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
-                const bool hit = act && key[k] <= lim;
-                key[k] = hit ? key[k] : kInf;
+                // k < nc: an unused slot's key (+inf) passes `<= lim` while lim is +inf too
+                const bool hit = act && k < nc && key[k] <= lim;
+                key[k] = hit ? fminf(key[k], kMaxHitKey) : kInf;
                 wmask[k] = __ballot_sync(0xffffffffu, hit);
                 wkey[k] = wmask[k] ? warp_min(key[k]) : kInf;
                 cnt += wmask[k] ? 1 : 0;

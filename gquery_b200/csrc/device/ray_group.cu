@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(kBlockG) k_ray_g8(DevScene s, gq_vecs a, gq_ve
                     tf = fminf(tf, fmaxf(t0, t1));
                 }
                 hit = tn <= fminf(tf * trav::kFar, r * trav::kFar);
-                key = hit ? tn : kInf;
+                key = hit ? fminf(tn, trav::kMaxHitKey) : kInf;  // hits stay below the others' +inf
             }
             const unsigned hm = (__ballot_sync(gmask, hit) >> g0) & 0xffu;
             if (hm == 0) {

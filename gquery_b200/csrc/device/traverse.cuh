@@ -14,6 +14,11 @@ constexpr float kSlack = 1.0000038f;  // 1 + 2^-18 (wide, squared space)
 constexpr float kSq20 = 1.00000095f;  // 1 + 2^-20
 constexpr float kSq21 = 1.00000048f;  // 1 + 2^-21
 constexpr float kFar = 1.000000477f;  // slab widening of the wide ray test
+// Largest key a hit child of a wide node carries.  Unused child slots (and missed
+// children) sort as +inf; a hit whose key is +inf too (a query with an infinite or
+// overflowing coordinate) is clamped here, so the sorted hits always come first and an
+// unused slot, whose reference names no node, is never pushed.
+constexpr float kMaxHitKey = 3.40282347e38f;
 
 // CFG bits
 constexpr int CFG_SPHERE = 1;     // triangle bounding-sphere rejection (closest point, 3D)
@@ -332,7 +337,7 @@ __device__ __forceinline__ void visit_wide(const DevScene &s, Lane<D, RAY, true>
                 tf = fminf(tf, fmaxf(t0, t1));
             }
             const bool hit = (k < nc) && (tn <= fminf(tf * kFar, L.r * kFar));
-            key[k] = hit ? tn : kInf;
+            key[k] = hit ? fminf(tn, kMaxHitKey) : kInf;
             cnt += hit ? 1 : 0;
         }
     }
@@ -342,7 +347,7 @@ __device__ __forceinline__ void visit_wide(const DevScene &s, Lane<D, RAY, true>
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
             const bool hit = (k < nc) && (key[k] <= lim);
-            key[k] = hit ? key[k] : kInf;
+            key[k] = hit ? fminf(key[k], kMaxHitKey) : kInf;
             cnt += hit ? 1 : 0;
         }
     }
