@@ -112,3 +112,38 @@ def test_nonfinite_silhouettes(dim):
         assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0 and rep["max_rel_d"] <= REL_TOL, (
             variant, rep)
     assert s.device_error() == 0
+
+
+@pytest.mark.parametrize("forms", [("coherent", "wide8", "coherent"), ("split", "wide8", "warp"),
+                                   ("exact", "exact", "split")])
+def test_nonfinite_in_a_batch(forms):
+    from gquery_b200.batch import SceneBatch
+    scenes = [_scene(3), Scene(*W.icosphere(2, amplitude=0.1, seed=23), 3, device=0, build_snch=True)]
+    n = 3000
+    _, q, _ = _mixed(3, n, 5)
+    _, o, _ = _mixed(3, n, 6)
+    d = np.random.default_rng(7).standard_normal((n, 3)).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    ids = np.random.default_rng(8).integers(0, len(scenes), n).astype(np.int32)
+    nonfin = ~np.all(np.isfinite(q), axis=1)
+    nonfin_o = ~np.all(np.isfinite(o), axis=1)
+    qd, od, dd, idd = (torch.as_tensor(x).cuda() for x in (q, o, d, ids))
+    cp_v, ray_v, sil_v = forms
+    batch = SceneBatch(scenes, n, cp_variant=cp_v, ray_variant=ray_v, sil_variant=sil_v)
+    res = batch.run(cp=(qd, idd), ray=(od, dd, idd), sil=(qd, idd))
+    torch.cuda.synchronize()
+    assert batch.device_error() == 0
+    cp, ray, sil = to_np(res.cp), to_np(res.ray), to_np(res.sil)
+    assert not np.asarray(cp["valid"])[nonfin].any() and not np.asarray(sil["valid"])[nonfin].any()
+    assert not np.asarray(ray["valid"])[nonfin_o].any()
+    # the ordinary queries against the single-scene exact calls on their own scene
+    for sid, sc in enumerate(scenes):
+        sel = np.nonzero((ids == sid) & ~nonfin)[0]
+        for name, got, ref in (("cp", cp, to_np(sc.closest_point(q[sel], variant="exact"))),
+                               ("sil", sil, to_np(sc.closest_silhouette(q[sel], variant="exact")))):
+            rep = tie_report(_keep(got, sel), ref)
+            assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0 and rep["max_rel_d"] <= REL_TOL, (
+                forms, name, sid, rep)
+        sel = np.nonzero((ids == sid) & ~nonfin_o)[0]
+        rep = tie_report(_keep(ray, sel), to_np(sc.intersect(o[sel], d[sel], variant="exact")))
+        assert rep["valid_mismatch"] == 0 and rep["prim_mismatch_not_tie"] == 0, (forms, "ray", sid, rep)
