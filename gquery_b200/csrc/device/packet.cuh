@@ -23,9 +23,9 @@ namespace gqd {
 namespace pkt {
 
 constexpr int kNone = 0x7fffffff;
-// Largest key of a hit child of a wide node: unused and missed child slots sort as +inf,
-// and a hit whose key overflowed to +inf (a query with an infinite or huge coordinate)
-// is clamped so that the hits stay ahead of them in the sorted order.
+// Largest sort key of a hit child of a wide node: unused and missed child slots sort as
+// +inf, and a hit whose key overflowed to +inf (a query with an infinite or huge
+// coordinate) is clamped so that the hits stay ahead of them in the sorted order.
 constexpr float kMaxHitKey = 3.40282347e38f;
 constexpr float kSlack = 1.0000038f;  // 1 + 2^-18
 constexpr int kPStack = 96;
@@ -246,7 +246,9 @@ __device__ __forceinline__ void closest_point(const DevScene &s, unsigned mask, 
             float shrink = kInf;
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
-                float a2 = kInf, b2 = kInf;
+                // NaN for inactive lanes and unused slots: it fails every `<= lim`, also while
+                // lim is +inf (an unused slot holds no node)
+                float a2 = __int_as_float(0x7fc00000), b2 = kInf;
                 if (act && k < nc) {
                     const float lo3[3] = {__fmaf_rn(qf(q0.x, q0.y, k), sx, h.x), __fmaf_rn(qf(q0.z, q0.w, k), sy, h.y),
                                           __fmaf_rn(qf(q1.x, q1.y, k), sz, h.z)};
@@ -264,11 +266,12 @@ __device__ __forceinline__ void closest_point(const DevScene &s, unsigned mask, 
             int cnt = 0;
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
-                // k < nc: an unused slot's key (+inf) passes `<= lim` while lim is +inf too
-                const bool hit = act && k < nc && key[k] <= lim;
-                key[k] = hit ? fminf(key[k], kMaxHitKey) : kInf;
+                const bool hit = key[k] <= lim;
+                key[k] = hit ? key[k] : kInf;
                 wmask[k] = __ballot_sync(0xffffffffu, hit);
-                wkey[k] = wmask[k] ? warp_min(key[k]) : kInf;
+                // hits clamped below the others' +inf: they sort first, and the nearest-first
+                // choice is a hit, so that it pushes at most cnt - 1 entries
+                wkey[k] = wmask[k] ? fminf(warp_min(key[k]), kMaxHitKey) : kInf;
                 cnt += wmask[k] ? 1 : 0;
             }
             if (cnt == 0) {
