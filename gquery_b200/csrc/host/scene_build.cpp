@@ -42,6 +42,10 @@ std::string validate_source(const PrimSource<D> &src) {
         int32_t k = src.index[i];
         if (k < 0 || k >= src.nv) return "primitive index out of range";
     }
+    // the SAH bins centroids with int(12 * offset), which a NaN or an infinite
+    // coordinate turns into an out-of-range bucket (bvh.cpp:44-46 has no guard)
+    for (int64_t i = 0; i < src.nv * D; ++i)
+        if (!std::isfinite(src.verts[i])) return "vertex coordinates must be finite";
     return std::string();
 }
 

@@ -98,7 +98,7 @@ struct PrimSource {
     int64_t np;
 };
 
-// Validates the inputs (index range, counts); returns an empty string when fine.
+// Validates the inputs (index range, counts, finite coordinates); returns an empty string when fine.
 template <int D>
 std::string validate_source(const PrimSource<D> &src);
 

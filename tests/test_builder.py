@@ -309,3 +309,17 @@ def test_invalid_inputs_are_rejected():
         Scene(v, np.zeros((0, 3), np.int32), 3, device=None)
     with pytest.raises(ValueError):
         Scene(v, np.zeros((4, 4), np.int32), 3, device=None)
+
+
+@pytest.mark.parametrize("bad", [np.nan, np.inf, -np.inf])
+@pytest.mark.parametrize("dim", [2, 3])
+def test_non_finite_vertices_are_rejected(dim, bad):
+    if dim == 3:
+        v, f = W.icosphere(1, seed=0)
+    else:
+        v, f = W.star_polyline(40, seed=0)
+    v = v.copy()
+    v[3, dim - 1] = bad
+    with pytest.raises(L.GQError) as ei:
+        Scene(v, f, dim, device=None)
+    assert ei.value.status == L.GQ_ERR_INVALID and "finite" in str(ei.value)
