@@ -143,7 +143,8 @@ const char *gq_status_string(gq_status s);
 
 /* ---- scene build (replaces gquery_ext.BVH / BVH3D / SNCH / SNCH3D constructors,
  *      src/gquery.cpp:184-185, 196-197, 227-228, 239-240) ----
- * vertices: host [nv][D] float32; prims: host [np][D] int32 (edges in 2D, faces in 3D). */
+ * vertices: host [nv][D] float32, finite; prims: host [np][D] int32 (edges in 2D, faces in
+ * 3D) in [0, nv).  Other input is GQ_ERR_INVALID. */
 gq_status gq_scene_build_2d(const float *vertices, int64_t nv, const int32_t *edges, int64_t ne,
                             const gq_build_opts *opts, gq_scene **out);
 gq_status gq_scene_build_3d(const float *vertices, int64_t nv, const int32_t *faces, int64_t nf,
