@@ -2,7 +2,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -921,6 +923,7 @@ struct SceneFileHeader {
     float root_lo[3], root_hi[3], coord_bound, pad2;
     uint64_t image_bytes[6];
 };
+static_assert(sizeof(SceneFileHeader) == 176, "the scene file header is 176 bytes");
 constexpr char kSceneMagic[8] = {'G', 'Q', 'S', 'C', 'E', 'N', 'E', '1'};
 // 2: 3D silhouette edges carry the pre-test spans (gq_sile_t.span0 / span1)
 // 3: 3D SNCH pairs carry the node bounds of both children (gq_spair3_t.l_b / r_b)
@@ -983,6 +986,85 @@ gq_status gq_scene_save(const gq_scene *s, const char *path) {
     return GQ_OK;
 }
 
+// Structure of a loaded scene image, checked on the host before anything reaches the
+// device: the kernels follow its references without bounds checks.  Returns an empty
+// string when the arrays agree with the header and with each other: every interior
+// reference names a record of its own array that no other reference and not the root
+// names (each node has at most one parent, so no walk meets a node twice and every
+// walk ends, whatever the numbering: host trees are in preorder, device-built ones in
+// the order of the sorted keys), every leaf starts inside its item array and the
+// array's last item ends a leaf (so every leaf scan ends), the roots are valid, and
+// the wide nodes' used slots follow the same rules.
+static std::string check_image(const SceneFileHeader &h, const std::vector<char> (&a)[6]) {
+    const bool d3 = h.dim == 3;
+    const size_t s_pair = d3 ? sizeof(gq_pair3_t) : sizeof(gq_pair2_t);
+    const size_t s_prim = d3 ? sizeof(gq_tri_t) : sizeof(gq_seg_t);
+    const size_t s_wide = d3 ? sizeof(gq_wnode3_t) : sizeof(gq_wnode2_t);
+    const size_t s_spair = d3 ? sizeof(gq_spair3_t) : sizeof(gq_spair2_t);
+    const size_t s_sil = d3 ? sizeof(gq_sile_t) : sizeof(gq_silv_t);
+    auto i32 = [&](int k, size_t byte) {
+        int32_t v;
+        std::memcpy(&v, a[k].data() + byte, 4);
+        return v;
+    };
+    if (a[0].size() % s_pair || a[1].size() != (size_t)h.np * s_prim || a[3].size() % s_wide ||
+        a[4].size() % s_spair || a[5].size() % s_sil)
+        return "array sizes do not match the record sizes";
+    if (d3 && !a[2].empty() && a[2].size() != (size_t)h.np * sizeof(gq_tsph_t)) return "sphere array size";
+    const int64_t n_pair = (int64_t)(a[0].size() / s_pair), n_wide = (int64_t)(a[3].size() / s_wide);
+    const int64_t n_spair = (int64_t)(a[4].size() / s_spair), n_sil = (int64_t)(a[5].size() / s_sil);
+    if (n_wide != (h.has_wide ? h.n_wide : 0) || n_sil != h.n_sil) return "record counts differ from the header";
+    if (h.np < 1) return "no primitives";
+    const size_t f_prim = d3 ? offsetof(gq_tri_t, flags) : offsetof(gq_seg_t, flags);
+    if (!(i32(1, (size_t)(h.np - 1) * s_prim + f_prim) & (int32_t)GQ_ITEM_LAST)) return "the last primitive ends no leaf";
+    if (d3 && !a[2].empty()) {
+        float r;
+        std::memcpy(&r, a[2].data() + (size_t)(h.np - 1) * sizeof(gq_tsph_t) + offsetof(gq_tsph_t, r), 4);
+        if (!std::signbit(r)) return "the last bounding sphere ends no leaf";
+    }
+    const size_t f_sil = d3 ? offsetof(gq_sile_t, flags) : offsetof(gq_silv_t, flags);
+    if (n_sil > 0 && !(i32(5, (size_t)(n_sil - 1) * s_sil + f_sil) & (int32_t)GQ_ITEM_LAST))
+        return "the last silhouette ends no leaf";
+    // a reference into an array of n records over n_items items; `parents` counts the
+    // references each record has had
+    auto ref_ok = [](int32_t ref, int64_t n, int64_t n_items, bool empty_ok, std::vector<uint8_t> &parents) {
+        if (ref >= 0) return (int64_t)ref < n && parents[(size_t)ref]++ == 0;
+        if (ref == INT32_MIN) return empty_ok;
+        return (int64_t)~ref < n_items;
+    };
+    std::vector<uint8_t> parents;
+    const size_t o_pref = d3 ? offsetof(gq_pair3_t, ref_l) : offsetof(gq_pair2_t, ref_l);
+    parents.assign((size_t)n_pair, 0);
+    if (!ref_ok(h.root_ref, n_pair, h.np, false, parents)) return "BVH root";
+    for (int64_t i = 0; i < n_pair; ++i)
+        for (int c = 0; c < 2; ++c)
+            if (!ref_ok(i32(0, (size_t)i * s_pair + o_pref + 4 * c), n_pair, h.np, false, parents))
+                return "a BVH pair references outside its arrays or a node twice";
+    if (h.has_wide) {
+        const size_t o_meta = d3 ? offsetof(gq_wnode3_t, meta) : offsetof(gq_wnode2_t, meta);
+        const size_t o_ref = d3 ? offsetof(gq_wnode3_t, ref) : offsetof(gq_wnode2_t, ref);
+        parents.assign((size_t)n_wide, 0);
+        if (!ref_ok(h.wroot_ref, n_wide, h.np, false, parents)) return "wide root";
+        for (int64_t i = 0; i < n_wide; ++i) {
+            const uint32_t nc = (uint32_t)i32(3, (size_t)i * s_wide + o_meta) >> 24;
+            if (nc < 1 || nc > GQ_WIDTH) return "a wide node's child count";
+            for (uint32_t k = 0; k < nc; ++k)
+                if (!ref_ok(i32(3, (size_t)i * s_wide + o_ref + 4 * k), n_wide, h.np, false, parents))
+                    return "a wide node references outside its arrays or a node twice";
+        }
+    }
+    if (h.has_snch) {
+        const size_t o_sref = d3 ? offsetof(gq_spair3_t, ref_l) : offsetof(gq_spair2_t, ref_l);
+        parents.assign((size_t)n_spair, 0);
+        if (!ref_ok(h.sroot_ref, n_spair, n_sil, true, parents)) return "SNCH root";
+        for (int64_t i = 0; i < n_spair; ++i)
+            for (int c = 0; c < 2; ++c)
+                if (!ref_ok(i32(4, (size_t)i * s_spair + o_sref + 4 * c), n_spair, n_sil, true, parents))
+                    return "an SNCH pair references outside its arrays or a node twice";
+    }
+    return std::string();
+}
+
 gq_status gq_scene_load(const char *path, int32_t device, gq_scene **out) {
     if (!path || !out) return fail(GQ_ERR_INVALID, "null argument");
     *out = nullptr;
@@ -1027,6 +1109,14 @@ gq_status gq_scene_load(const char *path, int32_t device, gq_scene **out) {
         ok = std::fread(arrays[k].data(), 1, arrays[k].size(), in.f) == arrays[k].size();
     }
     if (!ok) return fail(GQ_ERR_INVALID, std::string(path) + " is truncated");
+    std::string bad = check_image(h, arrays);
+    if (bad.empty()) {
+        if (h.dim == 3)
+            bad = gqb::validate_source<3>(gqb::PrimSource<3>{s->verts.data(), h.nv, s->index.data(), h.np});
+        else
+            bad = gqb::validate_source<2>(gqb::PrimSource<2>{s->verts.data(), h.nv, s->index.data(), h.np});
+    }
+    if (!bad.empty()) return fail(GQ_ERR_INVALID, std::string(path) + " is corrupt: " + bad);
     default_tuning(s.get());
     gqd::DevScene &d = s->dev;
     d.dim = h.dim;
