@@ -155,7 +155,10 @@ gq_status gq_scene_free(gq_scene *scene);
  * Mesh / Polyline is constructed): save writes the input geometry and the flattened
  * device arrays of a scene that has a device copy; load uploads them to `device` without
  * building anything.  The host trees behind gq_scene_ref_array are rebuilt on first use
- * (the build is deterministic).  The format is native-endian and versioned. */
+ * (the build is deterministic).  The format is native-endian and versioned.  Load checks
+ * the arrays on the host before uploading them (sizes, every reference inside its array
+ * with at most one parent, leaf ends, finite vertices) and refuses a file that fails
+ * with GQ_ERR_INVALID ("... is corrupt: ..."). */
 gq_status gq_scene_save(const gq_scene *scene, const char *path);
 gq_status gq_scene_load(const char *path, int32_t device, gq_scene **out);
 gq_status gq_scene_get_info(const gq_scene *scene, gq_scene_info *info);
