@@ -1036,10 +1036,16 @@ static std::string check_image(const SceneFileHeader &h, const std::vector<char>
     const size_t o_pref = d3 ? offsetof(gq_pair3_t, ref_l) : offsetof(gq_pair2_t, ref_l);
     parents.assign((size_t)n_pair, 0);
     if (!ref_ok(h.root_ref, n_pair, h.np, false, parents)) return "BVH root";
+    const size_t o_sub = d3 ? offsetof(gq_pair3_t, sub_l) : offsetof(gq_pair2_t, sub_l);
     for (int64_t i = 0; i < n_pair; ++i)
-        for (int c = 0; c < 2; ++c)
+        for (int c = 0; c < 2; ++c) {
             if (!ref_ok(i32(0, (size_t)i * s_pair + o_pref + 4 * c), n_pair, h.np, false, parents))
                 return "a BVH pair references outside its arrays or a node twice";
+            // a collapsed subtree's run: 1..GQ_COLLAPSE_MAX items inside the primitives
+            const uint32_t sub = (uint32_t)i32(0, (size_t)i * s_pair + o_sub + 4 * c), cnt = sub >> 24;
+            if (sub != 0 && (cnt < 1 || cnt > GQ_COLLAPSE_MAX || (int64_t)(sub & 0xffffffu) + cnt > h.np))
+                return "a BVH pair's collapsed run lies outside the primitives";
+        }
     if (h.has_wide) {
         const size_t o_meta = d3 ? offsetof(gq_wnode3_t, meta) : offsetof(gq_wnode2_t, meta);
         const size_t o_ref = d3 ? offsetof(gq_wnode3_t, ref) : offsetof(gq_wnode2_t, ref);

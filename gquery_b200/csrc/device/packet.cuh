@@ -106,13 +106,18 @@ __device__ __forceinline__ void box_sq(const float *lo, const float *hi, const f
 // Leaf: every lane that needs it tests the leaf's items against its query.
 template <int D>
 __device__ __forceinline__ void leaf(const DevScene &s, int ref, bool act, const float *p, float &r, int &idx) {
-    int j = ~ref;
+    // a run of a collapsed subtree (bit 30 clear): first in bits 0-23, count in 24-29;
+    // an ordinary leaf ~first (first < 2^30, so bit 30 set) runs to its last item
+    const bool run = (ref & 0x40000000) == 0;
+    int j = run ? (ref & 0xffffff) : ~ref;
+    const int end = run ? j + ((ref >> 24) & 0x3f) : 0;
+    if (run && end == j) return;  // an empty run (INT32_MIN, an unused wide slot): nothing to test
     for (;;) {
         bool last;
         if (D == 3) {
             const float4 t0 = ldg4(s.prims, 3 * (int64_t)j), t1 = ldg4(s.prims, 3 * (int64_t)j + 1),
                          t2 = ldg4(s.prims, 3 * (int64_t)j + 2);
-            last = fbits(t2.z) & GQ_ITEM_LAST;
+            last = run ? j + 1 == end : (fbits(t2.z) & GQ_ITEM_LAST) != 0;
             if (act) {
                 float pt[3], u, v;
                 tri_closest<true>(p[0], p[1], p[D - 1], t0.x, t0.y, t0.z, t0.w, t1.x, t1.y, t1.z, t1.w, t2.x, pt, &u,
@@ -127,7 +132,7 @@ __device__ __forceinline__ void leaf(const DevScene &s, int ref, bool act, const
         } else {
             const float4 a = ldg4(s.prims, 2 * (int64_t)j);
             const int4 f = __ldg(reinterpret_cast<const int4 *>(s.prims) + 2 * (int64_t)j + 1);
-            last = f.y & GQ_ITEM_LAST;
+            last = run ? j + 1 == end : (f.y & GQ_ITEM_LAST) != 0;
             if (act) {
                 const float ux = a.z - a.x, uy = a.w - a.y, vx = p[0] - a.x, vy = p[D - 1] - a.y;
                 const float t = gq_clamp(gq_div(gq_dot2(vx, vy, ux, uy), gq_dot2(ux, uy, ux, uy)), 0.f, 1.f);
@@ -191,15 +196,16 @@ __device__ __forceinline__ void closest_point(const DevScene &s, unsigned mask, 
                 const int4 rf = __ldg(reinterpret_cast<const int4 *>(s.pairs) + 4 * (int64_t)cur + 3);
                 lo[0][0] = a.x; lo[0][1] = a.y; lo[0][D - 1] = a.z; hi[0][0] = a.w; hi[0][1] = b.x; hi[0][D - 1] = b.y;
                 lo[1][0] = b.z; lo[1][1] = b.w; lo[1][D - 1] = c.x; hi[1][0] = c.y; hi[1][1] = c.z; hi[1][D - 1] = c.w;
-                rl = rf.x;
-                rr = rf.y;
+                // a small subtree is tested as one run (sub_l / sub_r of the pair record)
+                rl = rf.z ? (int)(0x80000000u | (unsigned)rf.z) : rf.x;
+                rr = rf.w ? (int)(0x80000000u | (unsigned)rf.w) : rf.y;
             } else {
                 const float4 a = ldg4(s.pairs, 3 * (int64_t)cur), b = ldg4(s.pairs, 3 * (int64_t)cur + 1);
                 const int4 rf = __ldg(reinterpret_cast<const int4 *>(s.pairs) + 3 * (int64_t)cur + 2);
                 lo[0][0] = a.x; lo[0][D - 1] = a.y; hi[0][0] = a.z; hi[0][D - 1] = a.w;
                 lo[1][0] = b.x; lo[1][D - 1] = b.y; hi[1][0] = b.z; hi[1][D - 1] = b.w;
-                rl = rf.x;
-                rr = rf.y;
+                rl = rf.z ? (int)(0x80000000u | (unsigned)rf.z) : rf.x;
+                rr = rf.w ? (int)(0x80000000u | (unsigned)rf.w) : rf.y;
             }
             float a2l = kInf, b2l = kInf, a2r = kInf, b2r = kInf;
             if (act) {

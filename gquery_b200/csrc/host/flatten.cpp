@@ -61,6 +61,25 @@ void flatten_bvh(const PrimSource<D> &src, const BvhTree<D> &t, DeviceImage<D> &
         const auto &n = t.nodes[i];
         return n.n_prims > 0 ? ~n.prim_offset : rank[i];
     };
+    // every node's run of ordered primitives, children after parents in preorder; a
+    // subtree of at most GQ_COLLAPSE_MAX primitives is also written as one run
+    std::vector<int64_t> first(t.nodes.size()), count(t.nodes.size());
+    for (size_t i = t.nodes.size(); i-- > 0;) {
+        const auto &n = t.nodes[i];
+        if (n.n_prims > 0) {
+            first[i] = n.prim_offset;
+            count[i] = n.n_prims;
+        } else {
+            const size_t l = i + 1, r = i + (size_t)n.second_child;
+            first[i] = first[l];
+            // contiguous runs (always so in this preorder; -1 turns the collapse off above)
+            count[i] = (count[l] >= 0 && count[r] >= 0 && first[r] == first[l] + count[l]) ? count[l] + count[r] : -1;
+        }
+    }
+    auto sub_of = [&](uint32_t i) -> int32_t {
+        if (count[i] < 1 || count[i] > GQ_COLLAPSE_MAX || first[i] + count[i] > (int64_t(1) << 24)) return 0;
+        return (int32_t)(first[i] | (count[i] << 24));
+    };
     img.pairs.clear();
     for (uint32_t i = 0; i < t.nodes.size(); ++i) {
         const auto &n = t.nodes[i];
@@ -93,6 +112,8 @@ void flatten_bvh(const PrimSource<D> &src, const BvhTree<D> &t, DeviceImage<D> &
         }
         p.ref_l = ref_of(l);
         p.ref_r = ref_of(r);
+        p.sub_l = sub_of(l);
+        p.sub_r = sub_of(r);
         img.pairs.push_back(p);
     }
     img.root_ref = ref_of(0);

@@ -76,18 +76,23 @@ typedef struct {
     float span0, span1;
 } gq_sile_t;
 
-// Binary BVH pair records.
+// Binary BVH pair records.  sub_l / sub_r: a child whose subtree holds at most
+// GQ_COLLAPSE_MAX primitives (in one run of the ordered primitives, as every subtree's
+// are) is described again as first | count << 24 (first < 2^24), and the warp-coherent
+// closest-point walk tests that run as one leaf instead of walking the subtree; 0 for
+// larger subtrees (and in device-built trees).  The exact walks keep the references.
+#define GQ_COLLAPSE_MAX 8
 typedef struct {  // 2D, 48 B: left box, right box, refs
     float l_lox, l_loy, l_hix, l_hiy;
     float r_lox, r_loy, r_hix, r_hiy;
-    int32_t ref_l, ref_r, pad0, pad1;
+    int32_t ref_l, ref_r, sub_l, sub_r;
 } gq_pair2_t;
 
 typedef struct {  // 3D, 64 B
     float l_lox, l_loy, l_loz, l_hix;
     float l_hiy, l_hiz, r_lox, r_loy;
     float r_loz, r_hix, r_hiy, r_hiz;
-    int32_t ref_l, ref_r, pad0, pad1;
+    int32_t ref_l, ref_r, sub_l, sub_r;
 } gq_pair3_t;
 
 // Binary SNCH pair records: child box + cone (axis, half angle, radius).
