@@ -81,7 +81,7 @@ typedef struct {
 // are) is described again as first | count << 24 (first < 2^24), and the warp-coherent
 // closest-point walk tests that run as one leaf instead of walking the subtree; 0 for
 // larger subtrees (and in device-built trees).  The exact walks keep the references.
-#define GQ_COLLAPSE_MAX 8
+#define GQ_COLLAPSE_MAX 6
 typedef struct {  // 2D, 48 B: left box, right box, refs
     float l_lox, l_loy, l_hix, l_hiy;
     float r_lox, r_loy, r_hix, r_hiy;
