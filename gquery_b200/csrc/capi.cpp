@@ -928,7 +928,9 @@ constexpr char kSceneMagic[8] = {'G', 'Q', 'S', 'C', 'E', 'N', 'E', '1'};
 // 2: 3D silhouette edges carry the pre-test spans (gq_sile_t.span0 / span1)
 // 3: 3D SNCH pairs carry the node bounds of both children (gq_spair3_t.l_b / r_b)
 // 5: the node bounds hold the delta and cone forms and the pair record is 160 B
-constexpr int32_t kSceneFileVersion = 5;
+// 6: wide nodes hold run children (small subtrees as one leaf); files of version 5 have
+//    none and load unchanged
+constexpr int32_t kSceneFileVersion = 6;
 
 struct File {
     FILE *f = nullptr;
@@ -1027,9 +1029,14 @@ static std::string check_image(const SceneFileHeader &h, const std::vector<char>
         return "the last silhouette ends no leaf";
     // a reference into an array of n records over n_items items; `parents` counts the
     // references each record has had
-    auto ref_ok = [](int32_t ref, int64_t n, int64_t n_items, bool empty_ok, std::vector<uint8_t> &parents) {
+    auto ref_ok = [](int32_t ref, int64_t n, int64_t n_items, bool empty_ok, std::vector<uint8_t> &parents,
+                     bool runs_ok = false) {
         if (ref >= 0) return (int64_t)ref < n && parents[(size_t)ref]++ == 0;
         if (ref == INT32_MIN) return empty_ok;
+        if (runs_ok && (ref & 0x40000000) == 0) {  // a run child: 1..GQ_COLLAPSE_MAX items
+            const int64_t first = ref & 0xffffff, cnt = (ref >> 24) & 0x3f;
+            return cnt >= 1 && cnt <= GQ_COLLAPSE_MAX && first + cnt <= n_items;
+        }
         return (int64_t)~ref < n_items;
     };
     std::vector<uint8_t> parents;
@@ -1050,12 +1057,12 @@ static std::string check_image(const SceneFileHeader &h, const std::vector<char>
         const size_t o_meta = d3 ? offsetof(gq_wnode3_t, meta) : offsetof(gq_wnode2_t, meta);
         const size_t o_ref = d3 ? offsetof(gq_wnode3_t, ref) : offsetof(gq_wnode2_t, ref);
         parents.assign((size_t)n_wide, 0);
-        if (!ref_ok(h.wroot_ref, n_wide, h.np, false, parents)) return "wide root";
+        if (!ref_ok(h.wroot_ref, n_wide, h.np, false, parents, true)) return "wide root";
         for (int64_t i = 0; i < n_wide; ++i) {
             const uint32_t nc = (uint32_t)i32(3, (size_t)i * s_wide + o_meta) >> 24;
             if (nc < 1 || nc > GQ_WIDTH) return "a wide node's child count";
             for (uint32_t k = 0; k < nc; ++k)
-                if (!ref_ok(i32(3, (size_t)i * s_wide + o_ref + 4 * k), n_wide, h.np, false, parents))
+                if (!ref_ok(i32(3, (size_t)i * s_wide + o_ref + 4 * k), n_wide, h.np, false, parents, true))
                     return "a wide node references outside its arrays or a node twice";
         }
     }
@@ -1079,7 +1086,7 @@ gq_status gq_scene_load(const char *path, int32_t device, gq_scene **out) {
     in.f = std::fopen(path, "rb");
     if (!in.f) return fail(GQ_ERR_INVALID, std::string("cannot open ") + path);
     SceneFileHeader h{};
-    if (std::fread(&h, sizeof h, 1, in.f) != 1 || std::memcmp(h.magic, kSceneMagic, 8) != 0 || h.version != kSceneFileVersion ||
+    if (std::fread(&h, sizeof h, 1, in.f) != 1 || std::memcmp(h.magic, kSceneMagic, 8) != 0 || (h.version != kSceneFileVersion && h.version != 5) ||
         (h.dim != 2 && h.dim != 3) || h.nv < 0 || h.np < 0)
         return fail(GQ_ERR_INVALID, std::string(path) + " is not a saved scene of this version");
     std::unique_ptr<gq_scene> s(new (std::nothrow) gq_scene());

@@ -177,24 +177,27 @@ __global__ void __launch_bounds__(kBlockG) k_ray_g8(DevScene s, gq_vecs a, gq_ve
             cur = __shfl_sync(gmask, myref, (int)g0 + bj);
             __syncwarp(gmask);  // the group's pushes are visible to its later pops
         } else {
-            // leaf: up to eight items at once, the first nearest in leaf order kept
-            int64_t j0 = ~(int64_t)cur;
+            // leaf: up to eight items at once, the first nearest in leaf order kept; a run
+            // child (bit 30 clear) ends after its count, an ordinary leaf at its last item
+            const bool run = (cur & 0x40000000) == 0;
+            int64_t j0 = run ? (int64_t)(cur & 0xffffff) : ~(int64_t)cur;
+            const int64_t end = run ? j0 + ((cur >> 24) & 0x3f) : s.n_prims;
             for (;;) {
                 const int64_t it = j0 + j;
-                const bool in = it < s.n_prims;
+                const bool in = it < end;
                 bool last = !in;
                 float key = kInf;
                 if (in) {
                     if (D == 3) {
                         const float4 t0 = ldg4(s.prims, 3 * it), t1 = ldg4(s.prims, 3 * it + 1),
                                      t2 = ldg4(s.prims, 3 * it + 2);
-                        last = fbits(t2.z) & GQ_ITEM_LAST;
+                        last = run ? it + 1 == end : (fbits(t2.z) & GQ_ITEM_LAST) != 0;
                         key = tri_ray(p[0], p[1], p[D - 1], v[0], v[1], v[D - 1], t0.x, t0.y, t0.z, t0.w, t1.x, t1.y,
                                       t1.z, t1.w, t2.x, kInf);
                     } else {
                         const float4 e = ldg4(s.prims, 2 * it);
                         const int4 f = __ldg(reinterpret_cast<const int4 *>(s.prims) + 2 * it + 1);
-                        last = f.y & GQ_ITEM_LAST;
+                        last = run ? it + 1 == end : (f.y & GQ_ITEM_LAST) != 0;
                         key = seg_ray(p[0], p[D - 1], v[0], v[D - 1], e.x, e.y, e.z, e.w);
                     }
                 }

@@ -85,14 +85,19 @@ __device__ __forceinline__ float best_key(const Lane<D, RAY, WIDE> &L) {
 
 template <int D, bool RAY, bool WIDE, int CFG>
 __device__ __forceinline__ void visit_leaf(const DevScene &s, Lane<D, RAY, WIDE> &L, int ref) {
-    int j = ~ref;
+    // wide nodes: a run child (bit 30 clear, layout.h) ends after its count, an ordinary
+    // leaf ~first (bit 30 set) at its last item
+    const bool run = WIDE && (ref & 0x40000000) == 0;
+    int j = run ? (ref & 0xffffff) : ~ref;
+    const int end = run ? j + ((ref >> 24) & 0x3f) : 0;
+    if (run && end == j) return;
     if constexpr (D == 3 && !RAY) {
         float rl = WIDE ? gq_sqrt(L.r) : L.r;
         for (;;) {
             bool last, test = true;
             if (CFG & CFG_SPHERE) {
                 const float4 sp = __ldg(reinterpret_cast<const float4 *>(s.spheres) + j);
-                last = signbit(sp.w);
+                last = run ? j + 1 == end : signbit(sp.w);
                 const float lim = (rl + fabsf(sp.w) + L.eps) * kSq20;
                 const float dx = L.p[0] - sp.x, dy = L.p[1] - sp.y, dz = L.p[D - 1] - sp.z;
                 test = !(gq_dot3(dx, dy, dz, dx, dy, dz) > lim * lim * kSq20);
@@ -100,7 +105,7 @@ __device__ __forceinline__ void visit_leaf(const DevScene &s, Lane<D, RAY, WIDE>
             if (test) {
                 const float4 t0 = ldg4(s.prims, 3 * (int64_t)j), t1 = ldg4(s.prims, 3 * (int64_t)j + 1),
                              t2 = ldg4(s.prims, 3 * (int64_t)j + 2);
-                if (!(CFG & CFG_SPHERE)) last = fbits(t2.z) & GQ_ITEM_LAST;
+                if (!(CFG & CFG_SPHERE)) last = run ? j + 1 == end : (fbits(t2.z) & GQ_ITEM_LAST) != 0;
                 float key;
                 if (WIDE) {
                     float pt[3], u, v;
@@ -129,13 +134,13 @@ __device__ __forceinline__ void visit_leaf(const DevScene &s, Lane<D, RAY, WIDE>
         if (D == 3) {
             const float4 t0 = ldg4(s.prims, 3 * (int64_t)j), t1 = ldg4(s.prims, 3 * (int64_t)j + 1),
                          t2 = ldg4(s.prims, 3 * (int64_t)j + 2);
-            last = fbits(t2.z) & GQ_ITEM_LAST;
+            last = run ? j + 1 == end : (fbits(t2.z) & GQ_ITEM_LAST) != 0;
             key = tri_ray(L.p[0], L.p[1], L.p[D - 1], L.v[0], L.v[1], L.v[D - 1], t0.x, t0.y, t0.z, t0.w, t1.x, t1.y,
                           t1.z, t1.w, t2.x, kInf);
         } else {
             const float4 a = ldg4(s.prims, 2 * (int64_t)j);
             const int4 f = __ldg(reinterpret_cast<const int4 *>(s.prims) + 2 * (int64_t)j + 1);
-            last = f.y & GQ_ITEM_LAST;
+            last = run ? j + 1 == end : (f.y & GQ_ITEM_LAST) != 0;
             if (RAY) {
                 key = seg_ray(L.p[0], L.p[D - 1], L.v[0], L.v[D - 1], a.x, a.y, a.z, a.w);
             } else if (WIDE) {

@@ -253,6 +253,12 @@ struct WideBuilder {
     const BvhTree<D> &t;
     DeviceImage<D> &img;
     bool with16 = false;
+    // every binary node's run of ordered primitives (children after parents in preorder);
+    // a subtree of at most GQ_COLLAPSE_MAX primitives becomes one run child (GQ_RUN_REF)
+    std::vector<int64_t> sfirst, scount;
+    bool small(uint32_t i) const {
+        return scount[i] >= 1 && scount[i] <= GQ_COLLAPSE_MAX && sfirst[i] + scount[i] <= (int64_t(1) << 24);
+    }
 
     // Returns the stack entries a traversal of this subtree needs once its node is popped.
     int build(uint32_t b, int32_t *ref_out) {
@@ -263,7 +269,7 @@ struct WideBuilder {
             float best = -1.f;
             for (size_t k = 0; k < kids.size(); ++k) {
                 const auto &kn = t.nodes[kids[k]];
-                if (kn.n_prims == 0) {
+                if (kn.n_prims == 0 && !small(kids[k])) {  // runs are not expanded
                     float a = kn.box.area();
                     if (a > best) {
                         best = a;
@@ -328,6 +334,8 @@ struct WideBuilder {
                 quantise_bounds(org[ax], e[ax], kn.box.lo.v[ax], kn.box.hi.v[ax], &w.q[ax][k], &w.q[D + ax][k]);
             if (kn.n_prims > 0) {
                 w.ref[k] = ~kn.prim_offset;
+            } else if (small(kids[k])) {
+                w.ref[k] = (int32_t)(0x80000000u | (uint32_t)(sfirst[kids[k]] | (scount[kids[k]] << 24)));
             } else {
                 int32_t r;
                 int need = build(kids[k], &r);
@@ -353,6 +361,20 @@ void flatten_wide(const BvhTree<D> &t, DeviceImage<D> &img, bool with16) {
         return;
     }
     WideBuilder<D> wb{t, img, with16};
+    wb.sfirst.assign(t.nodes.size(), 0);
+    wb.scount.assign(t.nodes.size(), 0);
+    for (size_t i = t.nodes.size(); i-- > 0;) {
+        const auto &n = t.nodes[i];
+        if (n.n_prims > 0) {
+            wb.sfirst[i] = n.prim_offset;
+            wb.scount[i] = n.n_prims;
+        } else {
+            const size_t l = i + 1, r = i + (size_t)n.second_child;
+            wb.sfirst[i] = wb.sfirst[l];
+            const bool joined = wb.scount[l] >= 0 && wb.scount[r] >= 0 && wb.sfirst[r] == wb.sfirst[l] + wb.scount[l];
+            wb.scount[i] = joined ? wb.scount[l] + wb.scount[r] : -1;
+        }
+    }
     int32_t r;
     img.wide_stack = wb.build(0, &r);
     img.wroot_ref = r;

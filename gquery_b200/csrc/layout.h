@@ -124,7 +124,9 @@ static_assert(sizeof(gq_spair3_t) == 160, "gq_spair3_t is five 32-byte sectors")
 
 // Quantised 8-wide node, 3D: 96 B (three 32-byte sectors).
 //   origin.xyz, meta = exp_x | exp_y << 8 | exp_z << 16 | nchild << 24 (exps biased by 127)
-//   ref[8]      child references (same encoding as pair refs)
+//   ref[8]      child references (same encoding as pair refs), or a run child: a binary
+//               subtree of at most GQ_COLLAPSE_MAX primitives as 0x80000000 | first |
+//               count << 24 (bit 30 clear, where ~first has it set), tested as one leaf
 //   q[6][8]     qlo_x, qlo_y, qlo_z, qhi_x, qhi_y, qhi_z (8 bits each)
 typedef struct {
     float ox, oy, oz;

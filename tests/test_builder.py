@@ -222,6 +222,10 @@ def test_quantised_boxes_contain_their_subtrees(dim):
     leaf_len = {int(N[i, 2 * dim]): int(N[i, 2 * dim + 2]) for i in range(len(N)) if N[i, 2 * dim + 2] > 0}
 
     def prim_range(ref):
+        if ref < 0 and (ref & 0x40000000) == 0:  # a run child: first | count << 24
+            first, cnt = ref & 0xffffff, (ref >> 24) & 0x3f
+            assert 1 <= cnt <= 6
+            return [(first, first + cnt)]
         if ref < 0:
             o = ~ref
             return [(o, o + leaf_len[o])]
@@ -230,6 +234,8 @@ def test_quantised_boxes_contain_their_subtrees(dim):
             out += prim_range(int(refs[ref, k]))
         return out
 
+    used = np.concatenate([refs[i, :nc[i]] for i in range(refs.shape[0])]).astype(np.int64)
+    assert ((used < 0) & ((used & 0x40000000) == 0)).any(), "no run children"
     for node in range(refs.shape[0]):
         for k in range(nc[node]):
             rng = prim_range(int(refs[node, k]))
@@ -281,6 +287,10 @@ def test_16bit_bounds_contain_the_8bit_nodes_children(dim):
     leaf_len = {int(N[i, 2 * dim]): int(N[i, 2 * dim + 2]) for i in range(len(N)) if N[i, 2 * dim + 2] > 0}
 
     def prim_range(ref):
+        if ref < 0 and (ref & 0x40000000) == 0:  # a run child: first | count << 24
+            first, cnt = ref & 0xffffff, (ref >> 24) & 0x3f
+            assert 1 <= cnt <= 6
+            return [(first, first + cnt)]
         if ref < 0:
             o = ~ref
             return [(o, o + leaf_len[o])]
