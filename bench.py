@@ -4,7 +4,7 @@
 Headline (the JSON line's `value`): 3D closest point + ray intersection on the
 displaced icosphere of level 8 (1,310,720 triangles), 8,388,608 closest-point queries
 U[-2,2]^3 and 8,388,608 rays (origins U[-2,2]^3, directions uniform on S^2, r_max =
-inf).  One step = Morton order + closest_point over all points and the rays' order (origin
+inf).  One step = point order + closest_point over all points and the rays' order (origin
 and direction) + intersect over all rays, each with the scene's tuned variant, the two
 kinds on two streams side by side; the same step kind after kind on one stream gives the
 per-kind breakdown, and the exact binary kernel (gQuery's visit order) and the quantised
@@ -271,7 +271,7 @@ def tie_stats(a, b, rel=2e-6):
 
 def section_rays(args, dev, flush):
     """Rays of the headline workload over the quantised 8-wide nodes: one ray per lane and
-    one ray per group of 8 lanes, each in the origins' Morton order (mode 0) and in the
+    one ray per group of 8 lanes, each in the origins' point order (mode 0) and in the
     origin + direction order (mode 2); the records of all four must be the same."""
     import torch
     from gquery_b200 import workloads as W
@@ -1064,7 +1064,7 @@ def main():
             "parity": parity, "fp64_error": fp64,
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
             "gpu_launches": 4 * args.steps,
-            "gpu_launches_note": "own kernels per step: 1 Morton-key + 1 ray-key + 2 traversal (CUB radix-sort kernels extra)",
+            "gpu_launches_note": "own kernels per step: 1 point-key + 1 ray-key + 2 traversal (CUB radix-sort kernels extra)",
         }
         sections = sections_on
         flush_buf = flush

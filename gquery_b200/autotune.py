@@ -3,7 +3,7 @@
 The reference has no launch choices to make (DrJit traces one kernel per call).  Here
 each scene carries a tuning table (``gq_scene_set_tuning``): per query kind the
 traversal variant - binary nodes in the reference order (``exact``), binary nodes walked
-once per warp of Morton-adjacent queries (``coherent``), quantised 8-wide nodes
+once per warp of queries adjacent in the sort order (``coherent``), quantised 8-wide nodes
 (``wide8``, per lane or warp-coherent) or, for silhouettes, one query per warp
 (``warp``) - plus the persistent-refill budget, the threads
 per block and, for the warp-coherent closest point, a 32-entry traversal stack when the

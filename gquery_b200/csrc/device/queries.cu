@@ -1,5 +1,5 @@
 // Query kernels for sm_100a: the binary SNCH traversal (gQuery's visit order),
-// brute-force scans and the Morton reordering of queries.  Closest-point and ray
+// brute-force scans and the reordering of queries along space-filling curves.  Closest-point and ray
 // traversals live in traverse.cu.  Compiled with --fmad=false (see gq_fmath.h).
 #include <cub/cub.cuh>
 
@@ -556,7 +556,7 @@ __global__ void __launch_bounds__(kBlock) k_sil_f64(const float *recs, int64_t n
 }
 
 // ===========================================================================
-// Morton reordering
+// Reordering along a space-filling curve
 // ===========================================================================
 
 __device__ __forceinline__ uint32_t spread3(uint32_t v) {  // 10 bits -> every third bit
@@ -576,8 +576,43 @@ __device__ __forceinline__ uint32_t spread2(uint32_t v) {  // 15 bits -> every s
     return v;
 }
 
-// Keys on a grid over the scene box grown to twice its extent about its centre.
-__global__ void k_morton_keys(int dim, float lo0, float lo1, float lo2, float sc0, float sc1, float sc2, gq_vecs q,
+// Index of a cell of the 1024^3 grid along a 3D Hilbert curve: consecutive indices are
+// face-adjacent cells, so a run of sorted points (a warp's queries) spans a more compact
+// region than along a Morton curve, whose runs jump between distant octants.  Skilling's
+// method (J. Skilling, "Programming the Hilbert curve", AIP Conf. Proc. 707, 2004):
+// axes to the transposed index by inverse undo and Gray encoding, then the transposed
+// bits interleaved like a Morton code.
+__device__ __forceinline__ uint32_t hilbert3(uint32_t x0, uint32_t x1, uint32_t x2) {
+    uint32_t x[3] = {x0, x1, x2};
+#pragma unroll
+    for (uint32_t q = 1u << 9; q > 1; q >>= 1) {
+        const uint32_t p = q - 1;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            if (x[i] & q) {
+                x[0] ^= p;
+            } else {
+                const uint32_t t = (x[0] ^ x[i]) & p;
+                x[0] ^= t;
+                x[i] ^= t;
+            }
+        }
+    }
+    x[1] ^= x[0];
+    x[2] ^= x[1];
+    uint32_t t = 0;
+#pragma unroll
+    for (uint32_t q = 1u << 9; q > 1; q >>= 1)
+        if (x[2] & q) t ^= q - 1;
+    x[0] ^= t;
+    x[1] ^= t;
+    x[2] ^= t;
+    return (spread3(x[0]) << 2) | (spread3(x[1]) << 1) | spread3(x[2]);
+}
+
+// Keys on a grid over the scene box grown to twice its extent about its centre: the
+// cell's index along a Hilbert curve in 3D (1024 cells per axis), its Morton code in 2D.
+__global__ void k_point_keys(int dim, float lo0, float lo1, float lo2, float sc0, float sc1, float sc2, gq_vecs q,
                               int64_t n, uint32_t *keys, int32_t *vals) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -590,7 +625,7 @@ __global__ void k_morton_keys(int dim, float lo0, float lo1, float lo2, float sc
             f = fminf(fmaxf(f, 0.f), 1023.f);
             c[k] = (uint32_t)f;
         }
-        key = (spread3(c[0]) << 2) | (spread3(c[1]) << 1) | spread3(c[2]);
+        key = hilbert3(c[0], c[1], c[2]);
     } else {
         uint32_t c[2];
         for (int k = 0; k < 2; ++k) {
@@ -604,7 +639,7 @@ __global__ void k_morton_keys(int dim, float lo0, float lo1, float lo2, float sc
     vals[i] = (int32_t)i;
 }
 
-// Ray keys: the origin's cell on the same grid as k_morton_keys and the direction.
+// Ray keys: the origin's cell on the same grid as k_point_keys and the direction.
 // mode 1: the direction's octant (3 bits) above a 27-bit Morton code of the origin
 //         (9 bits per axis): each warp of sorted rays shares an octant and a region.
 // mode 2: the origin (6 bits per axis) and the direction's octahedral coordinates
@@ -707,7 +742,7 @@ cudaError_t morton_order(const DevScene &s, gq_vecs q, int64_t n, int32_t *perm,
         k_ray_keys<<<grid_for(n), kBlock, 0, st>>>(ray_mode, lo[0], lo[1], lo[2], sc[0], sc[1], sc[2], q, ray_dir, n,
                                                    k_in, v_in);
     else
-        k_morton_keys<<<grid_for(n), kBlock, 0, st>>>(s.dim, lo[0], lo[1], lo[2], sc[0], sc[1], sc[2], q, n, k_in,
+        k_point_keys<<<grid_for(n), kBlock, 0, st>>>(s.dim, lo[0], lo[1], lo[2], sc[0], sc[1], sc[2], q, n, k_in,
                                                       v_in);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;

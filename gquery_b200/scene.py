@@ -191,7 +191,8 @@ class Scene:
         return L.QueryOpts(v, int(sort), o, None, 0)
 
     def order(self, points, *, stream=None, scratch=None, out=None):
-        """Morton permutation of the points (int32 [n] on the device)."""
+        """Permutation of the points along a space-filling curve (Hilbert in 3D, Morton in
+        2D; int32 [n] on the device)."""
         t, n, vq = self._points(points)
         perm = out if out is not None else self._alloc(n, torch.int32)
         sp, sb = (None, 0) if scratch is None else (scratch.data_ptr(), scratch.numel() * scratch.element_size())
@@ -200,7 +201,7 @@ class Scene:
 
     def ray_order(self, origins, dirs, mode: int = 1, *, stream=None, scratch=None, out=None):
         """Permutation of rays (int32 [n] on the device) keyed by origin and direction:
-        mode 0 origin Morton order, 1 direction octant then origin, 2 origin and direction
+        mode 0 the origins' point order, 1 direction octant then origin, 2 origin and direction
         interleaved."""
         t, n, vo = self._points(origins)
         td, n2, vd = self._points(dirs)

@@ -46,7 +46,7 @@ typedef int32_t gq_status;
 #define GQ_VARIANT_EXACT 0    /* binary tree, gQuery's visit order: reference-identical answers */
 #define GQ_VARIANT_WIDE8 1    /* 8-wide nodes, 8-bit outward-rounded child boxes */
 #define GQ_VARIANT_AUTO 2     /* the scene's tuned choice for the query kind (gq_scene_set_tuning) */
-#define GQ_VARIANT_COHERENT 3 /* binary tree walked once per warp of Morton-adjacent queries (closest
+#define GQ_VARIANT_COHERENT 3 /* binary tree walked once per warp of queries adjacent in the sort order (closest
                                  point, closest silhouette); rays run as EXACT */
 #define GQ_VARIANT_WARP 4     /* closest silhouette only: one query per warp, its 32 lanes expanding up to
                                  32 tree nodes per step (for few, far-reaching queries) */
@@ -130,7 +130,7 @@ typedef struct {
 
 typedef struct {
     int32_t variant;        /* GQ_VARIANT_* */
-    int32_t sort;           /* 1: reorder queries along a Morton curve before traversal */
+    int32_t sort;           /* 1: reorder queries along a space-filling curve before traversal (gq_query_order) */
     const int32_t *order;   /* optional device permutation from gq_query_order(); replaces `sort` */
     void *scratch;          /* optional device scratch (see gq_query_scratch_bytes); NULL = stream-ordered allocation */
     int64_t scratch_bytes;
@@ -204,7 +204,8 @@ gq_status gq_flat_silhouette_edges_device(const float *vertices, int64_t nv, con
 /* Device scratch a query of n items needs when opts->scratch is supplied. */
 int64_t gq_query_scratch_bytes(int64_t n);
 
-/* Morton order of n query points (or ray origins) over the scene's box: writes a
+/* Order of n query points (or ray origins) along a space-filling curve over twice the
+ * scene's box (a Hilbert curve in 3D, 1024 cells per axis; a Morton curve in 2D): writes a
  * permutation of 0..n-1 to device `order`.  `scratch` (device, gq_order_scratch_bytes(n)
  * bytes) may be NULL for a stream-ordered allocation.  Several queries on the same
  * points can share one order through gq_query_opts.order. */
@@ -212,7 +213,7 @@ int64_t gq_order_scratch_bytes(int64_t n);
 gq_status gq_query_order(const gq_scene *scene, gq_vecs points, int64_t n, int32_t *order, void *scratch,
                          int64_t scratch_bytes, void *stream);
 /* The same for rays (3D scenes), keyed by origin and direction so that the rays of one warp
- * also point alike: mode 0 = the origins' Morton order (gq_query_order), 1 = direction
+ * also point alike: mode 0 = the origins' order of gq_query_order, 1 = direction
  * octant, then the origins' Morton code, 2 = origin cell and octahedral direction cell
  * interleaved.  No counterpart in the reference (DrJit runs rays in input order). */
 gq_status gq_ray_order(const gq_scene *scene, gq_vecs origins, gq_vecs dirs, int64_t n, int32_t mode, int32_t *order,
@@ -227,7 +228,7 @@ gq_status gq_closest_point(const gq_scene *scene, gq_vecs q, int64_t n, const gq
  * application owns every device allocation and hands it only input and output buffers,
  * a real-time loop that must not enter an allocator, since cudaMalloc may synchronise the
  * device and take unbounded time).  The per-call scratch (work counter and
- * Morton-sort buffers) comes from a fixed device array inside the library, which every
+ * sort buffers) comes from a fixed device array inside the library, which every
  * device that loads the library holds until the process exits; hence at most
  * gq_noalloc_max_queries() queries per call (larger n is rejected with GQ_ERR_INVALID).
  * Same answers as gq_closest_point with the same variant and sort flag.  All calls on a
