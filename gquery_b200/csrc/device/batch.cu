@@ -1,6 +1,6 @@
 // Many scenes, three query kinds, one persistent launch.
 //
-// Queries of each kind are sorted by (scene, Morton code inside the scene's box).
+// Queries of each kind are sorted by (scene, Hilbert index inside the scene's box).
 // Persistent warps work through the kinds in the order closest point, rays,
 // silhouettes (a warp-uniform phase).  Closest points run as tiles of 32 sorted
 // queries with the warp-coherent traversal once per distinct scene in the tile
@@ -12,6 +12,7 @@
 
 #include "batch.cuh"
 #include "cp_warp.cuh"
+#include "curves.cuh"
 #include "packet.cuh"
 #include "records.cuh"
 #include "sil_packet.cuh"
@@ -29,23 +30,6 @@ __device__ __forceinline__ float qget(const gq_vecs &v, int64_t i, int k) {
     return v.ptr[(int64_t)k * v.comp_stride + i * v.elem_stride];
 }
 
-__device__ __forceinline__ uint32_t spread3(uint32_t v) {
-    v &= 0x3ffu;
-    v = (v | (v << 16)) & 0x030000ffu;
-    v = (v | (v << 8)) & 0x0300f00fu;
-    v = (v | (v << 4)) & 0x030c30c3u;
-    v = (v | (v << 2)) & 0x09249249u;
-    return v;
-}
-__device__ __forceinline__ uint32_t spread2(uint32_t v) {
-    v &= 0x7fffu;
-    v = (v | (v << 8)) & 0x00ff00ffu;
-    v = (v | (v << 4)) & 0x0f0f0f0fu;
-    v = (v | (v << 2)) & 0x33333333u;
-    v = (v | (v << 1)) & 0x55555555u;
-    return v;
-}
-
 // Identity order for the three kinds (steps answered without sorting) and the phases'
 // claim counters zeroed, in one launch.
 __global__ void k_batch_ident(int32_t *perm0, int64_t n0, int32_t *perm1, int64_t n1, int32_t *perm2, int64_t n2,
@@ -57,7 +41,7 @@ __global__ void k_batch_ident(int32_t *perm0, int64_t n0, int32_t *perm1, int64_
     if (i < n_counters) counter[i] = 0ull;
 }
 
-// key = scene << 32 | Morton code over twice the scene's box
+// key = scene << 32 | Hilbert index of the query's cell on a grid over twice the scene's box
 __global__ void k_batch_keys(const DevScene *scenes, int n_scenes, BatchKind k, int64_t n, uint64_t *keys,
                              int32_t *vals, int32_t *bad) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -84,7 +68,7 @@ __global__ void k_batch_keys(const DevScene *scenes, int n_scenes, BatchKind k, 
             float f = (qget(k.a, i, a) - (mid - ext)) * (1024.f / (2.f * ext));
             c[a] = (uint32_t)fminf(fmaxf(f, 0.f), 1023.f);
         }
-        code = (spread3(c[0]) << 2) | (spread3(c[1]) << 1) | spread3(c[2]);
+        code = hilbert3(c[0], c[1], c[2]);
     } else {
         uint32_t c[2];
         for (int a = 0; a < 2; ++a) {
@@ -94,7 +78,7 @@ __global__ void k_batch_keys(const DevScene *scenes, int n_scenes, BatchKind k, 
             float f = (qget(k.a, i, a) - (mid - ext)) * (32768.f / (2.f * ext));
             c[a] = (uint32_t)fminf(fmaxf(f, 0.f), 32767.f);
         }
-        code = (spread2(c[0]) << 1) | spread2(c[1]);
+        code = hilbert2(c[0], c[1]);
     }
     keys[i] = ((uint64_t)(uint32_t)sid << 32) | code;
     vals[i] = (int32_t)i;

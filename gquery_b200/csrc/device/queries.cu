@@ -5,6 +5,7 @@
 
 #include <algorithm>
 
+#include "curves.cuh"
 #include "prim.cuh"
 #include "queries.cuh"
 #include "records.cuh"
@@ -559,59 +560,8 @@ __global__ void __launch_bounds__(kBlock) k_sil_f64(const float *recs, int64_t n
 // Reordering along a space-filling curve
 // ===========================================================================
 
-__device__ __forceinline__ uint32_t spread3(uint32_t v) {  // 10 bits -> every third bit
-    v &= 0x3ffu;
-    v = (v | (v << 16)) & 0x030000ffu;
-    v = (v | (v << 8)) & 0x0300f00fu;
-    v = (v | (v << 4)) & 0x030c30c3u;
-    v = (v | (v << 2)) & 0x09249249u;
-    return v;
-}
-__device__ __forceinline__ uint32_t spread2(uint32_t v) {  // 15 bits -> every second bit
-    v &= 0x7fffu;
-    v = (v | (v << 8)) & 0x00ff00ffu;
-    v = (v | (v << 4)) & 0x0f0f0f0fu;
-    v = (v | (v << 2)) & 0x33333333u;
-    v = (v | (v << 1)) & 0x55555555u;
-    return v;
-}
-
-// Index of a cell of the 1024^3 grid along a 3D Hilbert curve: consecutive indices are
-// face-adjacent cells, so a run of sorted points (a warp's queries) spans a more compact
-// region than along a Morton curve, whose runs jump between distant octants.  Skilling's
-// method (J. Skilling, "Programming the Hilbert curve", AIP Conf. Proc. 707, 2004):
-// axes to the transposed index by inverse undo and Gray encoding, then the transposed
-// bits interleaved like a Morton code.
-__device__ __forceinline__ uint32_t hilbert3(uint32_t x0, uint32_t x1, uint32_t x2) {
-    uint32_t x[3] = {x0, x1, x2};
-#pragma unroll
-    for (uint32_t q = 1u << 9; q > 1; q >>= 1) {
-        const uint32_t p = q - 1;
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            if (x[i] & q) {
-                x[0] ^= p;
-            } else {
-                const uint32_t t = (x[0] ^ x[i]) & p;
-                x[0] ^= t;
-                x[i] ^= t;
-            }
-        }
-    }
-    x[1] ^= x[0];
-    x[2] ^= x[1];
-    uint32_t t = 0;
-#pragma unroll
-    for (uint32_t q = 1u << 9; q > 1; q >>= 1)
-        if (x[2] & q) t ^= q - 1;
-    x[0] ^= t;
-    x[1] ^= t;
-    x[2] ^= t;
-    return (spread3(x[0]) << 2) | (spread3(x[1]) << 1) | spread3(x[2]);
-}
-
 // Keys on a grid over the scene box grown to twice its extent about its centre: the
-// cell's index along a Hilbert curve in 3D (1024 cells per axis), its Morton code in 2D.
+// cell's index along a Hilbert curve (1024 cells per axis in 3D, 32768 in 2D).
 __global__ void k_point_keys(int dim, float lo0, float lo1, float lo2, float sc0, float sc1, float sc2, gq_vecs q,
                               int64_t n, uint32_t *keys, int32_t *vals) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -633,7 +583,7 @@ __global__ void k_point_keys(int dim, float lo0, float lo1, float lo2, float sc0
             f = fminf(fmaxf(f, 0.f), 32767.f);
             c[k] = (uint32_t)f;
         }
-        key = (spread2(c[0]) << 1) | spread2(c[1]);
+        key = hilbert2(c[0], c[1]);
     }
     keys[i] = key;
     vals[i] = (int32_t)i;

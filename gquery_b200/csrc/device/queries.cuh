@@ -34,8 +34,8 @@ struct DevScene {
 
 #define GQ_DEVERR_STACK 1
 
-// Reordering along a space-filling curve (Hilbert in 3D, Morton in 2D; rays by origin and
-// direction): writes perm[0..n) (a permutation of 0..n-1) using `scratch`.
+// Reordering along a space-filling curve (points: Hilbert; rays by origin and direction):
+// writes perm[0..n) (a permutation of 0..n-1) using `scratch`.
 // Returns the scratch bytes needed when scratch == nullptr.
 size_t morton_scratch_bytes(int64_t n);
 // ray_mode > 0 (3D): keys from the ray origins q and directions ray_dir (see k_ray_keys).

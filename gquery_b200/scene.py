@@ -191,8 +191,8 @@ class Scene:
         return L.QueryOpts(v, int(sort), o, None, 0)
 
     def order(self, points, *, stream=None, scratch=None, out=None):
-        """Permutation of the points along a space-filling curve (Hilbert in 3D, Morton in
-        2D; int32 [n] on the device)."""
+        """Permutation of the points along a Hilbert curve over twice the scene's box (int32
+        [n] on the device)."""
         t, n, vq = self._points(points)
         perm = out if out is not None else self._alloc(n, torch.int32)
         sp, sb = (None, 0) if scratch is None else (scratch.data_ptr(), scratch.numel() * scratch.element_size())

@@ -205,7 +205,7 @@ gq_status gq_flat_silhouette_edges_device(const float *vertices, int64_t nv, con
 int64_t gq_query_scratch_bytes(int64_t n);
 
 /* Order of n query points (or ray origins) along a space-filling curve over twice the
- * scene's box (a Hilbert curve in 3D, 1024 cells per axis; a Morton curve in 2D): writes a
+ * scene's box (a Hilbert curve, 1024 cells per axis in 3D, 32768 in 2D): writes a
  * permutation of 0..n-1 to device `order`.  `scratch` (device, gq_order_scratch_bytes(n)
  * bytes) may be NULL for a stream-ordered allocation.  Several queries on the same
  * points can share one order through gq_query_opts.order. */
