@@ -422,6 +422,10 @@ void snch_node_bounds(const BvhTree<D> &t, const SnchTree<D> &s, DeviceImage<D> 
             split[i] = 1;
         }
     }
+    // each record's orientation, read once in record order (a node's bound reads its
+    // records up to ten times, and the raw edges lie in another order)
+    std::vector<float> orient(img.sils.size());
+    for (size_t j = 0; j < orient.size(); ++j) orient[j] = (float)s.raw[s.ordered[j]].orient;
     auto edge = [&](long long j) {
         const gq_sile_t &r = img.sils[(size_t)j];
         SilEdgeGeom g;
@@ -429,7 +433,7 @@ void snch_node_bounds(const BvhTree<D> &t, const SnchTree<D> &s, DeviceImage<D> 
         g.b[0] = r.bx; g.b[1] = r.by; g.b[2] = r.bz;
         g.n0[0] = r.n0x; g.n0[1] = r.n0y; g.n0[2] = r.n0z;
         g.n1[0] = r.n1x; g.n1[1] = r.n1y; g.n1[2] = r.n1z;
-        g.orient = (float)s.raw[s.ordered[(size_t)j]].orient;
+        g.orient = orient[(size_t)j];
         g.usable = (r.flags & (GQ_ITEM_VALID | GQ_SIL_FILTER)) == GQ_SIL_FILTER;
         return g;
     };

@@ -462,6 +462,30 @@ SnchTree<D> build_snch(const PrimSource<D> &src, const BvhTree<D> &bvh, int n_th
         }
     }
 
+    // What the cones read of each listed silhouette, in list order: a node's cone reads
+    // every silhouette of its range twice, and the raw silhouettes lie in another order.
+    struct ConeIn {
+        Vec<D> normal, centroid, n0, n1;  // normal(), centroid, unit face normals
+        bool closed;
+    };
+    const int nt = std::max(1, n_threads);
+    std::vector<ConeIn> cin(out.ordered.size());
+    auto fill = [&](size_t j0, size_t j1) {
+        for (size_t j = j0; j < j1; ++j) {
+            const SilOf<D> &s = out.raw[out.ordered[j]];
+            cin[j] = ConeIn{sil_normal(s), sil_centroid(s), sil_n0(s, true), sil_n1(s, true), sil_closed(s)};
+        }
+    };
+    if (nt == 1 || cin.size() < 65536) {
+        fill(0, cin.size());
+    } else {
+        std::vector<std::thread> pool;
+        const size_t per = (cin.size() + (size_t)nt - 1) / (size_t)nt;
+        for (int t = 0; t < nt; ++t)
+            pool.emplace_back(fill, std::min(cin.size(), (size_t)t * per), std::min(cin.size(), (size_t)(t + 1) * per));
+        for (auto &th : pool) th.join();
+    }
+
     // Cone of every node from all silhouettes below it (snch.cpp:103-154).
     auto cone_of = [&](size_t i) {
         Cone<D> &cone = out.nodes[i].cone;
@@ -470,10 +494,10 @@ SnchTree<D> build_snch(const PrimSource<D> &src, const BvhTree<D> &bvh, int n_th
         for (size_t k = i; k < end[i]; ++k) {
             const SnchNode<D> &sn = out.nodes[k];
             for (int32_t j = 0; j < sn.n_sil; ++j) {
-                const SilOf<D> &s = out.raw[out.ordered[(size_t)(sn.sil_offset + j)]];
-                cone.axis = cone.axis + sil_normal(s);
-                cone.radius = std::max(cone.radius, norm(sil_centroid(s) - c));
-                all_closed = all_closed && sil_closed(s);
+                const ConeIn &s = cin[(size_t)(sn.sil_offset + j)];
+                cone.axis = cone.axis + s.normal;
+                cone.radius = std::max(cone.radius, norm(s.centroid - c));
+                all_closed = all_closed && s.closed;
                 any = true;
             }
         }
@@ -489,16 +513,15 @@ SnchTree<D> build_snch(const PrimSource<D> &src, const BvhTree<D> &bvh, int n_th
                 for (size_t k = i; k < end[i]; ++k) {
                     const SnchNode<D> &sn = out.nodes[k];
                     for (int32_t j = 0; j < sn.n_sil; ++j) {
-                        const SilOf<D> &s = out.raw[out.ordered[(size_t)(sn.sil_offset + j)]];
-                        float a0 = std::acos(std::clamp(dot(cone.axis, sil_n0(s, true)), -1.f, 1.f));
-                        float a1 = std::acos(std::clamp(dot(cone.axis, sil_n1(s, true)), -1.f, 1.f));
+                        const ConeIn &s = cin[(size_t)(sn.sil_offset + j)];
+                        float a0 = std::acos(std::clamp(dot(cone.axis, s.n0), -1.f, 1.f));
+                        float a1 = std::acos(std::clamp(dot(cone.axis, s.n1), -1.f, 1.f));
                         cone.half_angle = std::max(cone.half_angle, std::max(a0, a1));
                     }
                 }
             }
         }
     };
-    const int nt = std::max(1, n_threads);
     if (nt == 1 || nn < 4096) {
         for (size_t i = 0; i < nn; ++i) cone_of(i);
     } else {
