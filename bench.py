@@ -664,7 +664,8 @@ def run_reference(args):
 
 
 def summary(line):
-    """The figures the north star names, side by side, at the end of the line."""
+    """The headline figures (variants against plain, error, serving tail), side by side,
+    at the end of the line."""
     def get(*path):
         x = line
         for k in path:
