@@ -13,7 +13,9 @@ Writes golden_<case>.npz: scene, queries and the reference's record fields;
 baseline_<case>.npz: the records of the reference's brute-force methods
 (Polyline/Mesh closest_point_baseline and intersect_baseline, Polyline.intersect); and
 deep_<case>.npz: the traversals on deep trees (scenes named by their generator in
-gquery_b200.workloads and a checksum of the generated arrays).
+gquery_b200.workloads and a checksum of the generated arrays); rmax_<case>.npz: rays and
+silhouettes with a per-query finite r_max.  --baselines-only, --deep-only and
+--rmax-only write one group alone.
 """
 from __future__ import annotations
 
@@ -225,9 +227,54 @@ def deep_cases(nq=256):
               "sil valid", sil["valid"].mean())
 
 
+def _rmax_ladder(n, seed):
+    """Per-query radii: 0, tiny, small, medium, large and +inf in turn, every third
+    query a random radius in [0.01, 1.5] instead."""
+    ladder = np.float32([0.0, 1e-3, 0.05, 0.2, 0.5, 1.0, 2.0, np.inf])
+    r = ladder[np.arange(n) % len(ladder)].copy()
+    rnd = np.random.default_rng(seed).uniform(0.01, 1.5, n).astype(np.float32)
+    r[2::3] = rnd[2::3]
+    return r
+
+
+def rmax_cases(nq=240):
+    """The reference's rays and silhouettes with a per-query finite r_max (bvh.py:201,
+    bvh3d.py:177, snch.py:107, snch3d.py:144): the radius bounds the walk from the first
+    node on, and a ray hit at t >= r_max is no hit.  Queries include the scene's own
+    vertices (distance 0 to the nearest primitive)."""
+    from drjit_scalar import Array2i, Array3i
+    cases = {"star4096": ("star_polyline", {"n": 4096, "seed": 3}),
+             "icosphere3": ("icosphere", {"level": 3, "amplitude": 0.3, "seed": 5})}
+    for name, (gen, kw) in cases.items():
+        v, ix = getattr(W, gen)(**kw)
+        dim = v.shape[1]
+        q = W.uniform_points(nq, dim, seed=801)
+        q[: nq // 8] = v[np.random.default_rng(802).choice(len(v), nq // 8, replace=False)]
+        o, d = W.rays(nq, dim, seed=803)
+        r_ray, r_sil = _rmax_ladder(nq, 804), _rmax_ladder(nq, 805)[::-1].copy()
+        if dim == 3:
+            V, F = soa(v, Array3), soa(ix, Array3i)
+            bvh, snch = BVH3D(V, F), SNCH3D(V, F)
+            rayf = ["valid", "p", "n", "uv", "d", "prim_id", "on_boundary"]
+        else:
+            V, F = soa(v, Array2), soa(ix, Array2i)
+            bvh, snch = BVH(V, F), SNCH(V, F)
+            rayf = ["valid", "p", "n", "t", "d", "prim_id", "on_boundary"]
+        ray = run(bvh.intersect, [(vec(a), vec(b), Float(r)) for a, b, r in zip(o, d, r_ray)], rayf)
+        sil = run(snch.closest_silhouette, [(vec(p), Float(r)) for p, r in zip(q, r_sil)],
+                  ["valid", "p", "d", "prim_id"])
+        np.savez_compressed(HERE / f"rmax_{name}.npz", dim=dim, vertices=v, indices=ix, q=q, o=o, d=d,
+                            r_ray=r_ray, r_sil=r_sil, **{f"ray_{k}": x for k, x in ray.items()},
+                            **{f"sil_{k}": x for k, x in sil.items()})
+        print("rmax", name, "ray valid", ray["valid"].mean(), "sil valid", sil["valid"].mean())
+
+
 def main():
     if "--baselines-only" in sys.argv:
         baselines()
+        return
+    if "--rmax-only" in sys.argv:
+        rmax_cases()
         return
     if "--deep-only" in sys.argv:
         deep_cases()
@@ -260,6 +307,7 @@ def main():
     case_3d("icosphere2", iv, iff, q, o, d, np.inf)
     baselines()
     deep_cases()
+    rmax_cases()
 
 
 if __name__ == "__main__":

@@ -156,3 +156,38 @@ def test_exact_kernels_match_reference_traversal_deep(path):
     assert_bitwise(to_np(s.intersect(z["o"], z["d"], variant="exact")), expected(z, "ray", RAY[dim]), RAY[dim],
                    "ray ")
     assert_bitwise(to_np(s.closest_silhouette(z["q"], rmax, variant="exact")), expected(z, "sil", SIL), SIL, "sil ")
+
+
+# ---------------------------------------------------------------- per-query finite r_max
+
+RMAX = sorted((Path(__file__).resolve().parent / "golden").glob("rmax_*.npz"))
+
+
+def test_rmax_fixtures_exist():
+    assert {"rmax_star4096", "rmax_icosphere3"} <= {p.stem for p in RMAX}
+
+
+@pytest.mark.parametrize("path", RMAX, ids=[p.stem for p in RMAX])
+def test_oracle_matches_reference_traversal_rmax(path):
+    """Rays and silhouettes with one radius per query (0, tiny, finite, +inf): the
+    reference's records from bvh.py:201 / bvh3d.py:177 / snch.py:107 / snch3d.py:144."""
+    dim, z = load(path)
+    s = Scene(z["vertices"], z["indices"], dim, device=None)
+    nodes, prims = s.ref_array(L.ARRAY_BVH_NODES), s.ref_array(L.ARRAY_PRIMITIVES)
+    snodes, sils = s.ref_array(L.ARRAY_SNCH_NODES), s.ref_array(L.ARRAY_SILHOUETTES)
+    assert_bitwise(oracle.intersect(dim, nodes, prims, z["o"], z["d"], z["r_ray"]), expected(z, "ray", RAY[dim]),
+                   RAY[dim], "ray ")
+    assert_bitwise(oracle.closest_silhouette(dim, snodes, sils, z["q"], z["r_sil"]), expected(z, "sil", SIL), SIL,
+                   "sil ")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", RMAX, ids=[p.stem for p in RMAX])
+def test_exact_kernels_match_reference_traversal_rmax(path):
+    dim, z = load(path)
+    s = Scene(z["vertices"], z["indices"], dim, device=0)
+    assert_bitwise(to_np(s.intersect(z["o"], z["d"], z["r_ray"], variant="exact")), expected(z, "ray", RAY[dim]),
+                   RAY[dim], "ray ")
+    assert_bitwise(to_np(s.closest_silhouette(z["q"], z["r_sil"], variant="exact")), expected(z, "sil", SIL), SIL,
+                   "sil ")
+    assert s.device_error() == 0
