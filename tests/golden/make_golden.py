@@ -14,8 +14,9 @@ baseline_<case>.npz: the records of the reference's brute-force methods
 (Polyline/Mesh closest_point_baseline and intersect_baseline, Polyline.intersect); and
 deep_<case>.npz: the traversals on deep trees (scenes named by their generator in
 gquery_b200.workloads and a checksum of the generated arrays); rmax_<case>.npz: rays and
-silhouettes with a per-query finite r_max.  --baselines-only, --deep-only and
---rmax-only write one group alone.
+silhouettes with a per-query finite r_max; degenerate_<case>.npz: all three traversals
+on degenerate geometry.  --baselines-only, --deep-only, --rmax-only and
+--degenerate-only write one group alone.
 """
 from __future__ import annotations
 
@@ -269,9 +270,56 @@ def rmax_cases(nq=240):
         print("rmax", name, "ray valid", ray["valid"].mean(), "sil valid", sil["valid"].mean())
 
 
+def degenerate_cases(nq=320):
+    """The reference's traversals on degenerate geometry: a mesh with a zero-area face
+    (a repeated vertex), an edge collapsed to a point in several faces, repeated faces and
+    a segment-like face; a polyline with a zero-length segment, repeated segments and a
+    point segment.  A quarter of the queries sit on vertices, a quarter on the midpoints
+    of vertex pairs."""
+    v, f = W.icosphere(3, amplitude=0.2, seed=12)
+    v, f = v.copy(), f.copy()
+    f[10] = [f[10][0], f[10][0], f[10][1]]
+    v[f[20][2]] = v[f[20][1]]
+    f = np.concatenate([f, f[30:60], [[f[5][0], f[5][1], f[5][1]]]]).astype(np.int32)
+    pv, pe = W.star_polyline(500, seed=3)
+    pv = pv.copy()
+    pv[7] = pv[6]
+    pe = np.concatenate([pe, pe[100:140], [[3, 3]]]).astype(np.int32)
+    for name, (vv, ix) in (("mesh", (v, f)), ("polyline", (pv, pe))):
+        dim = vv.shape[1]
+        rng = np.random.default_rng(901)
+        k = nq // 4
+        q = np.concatenate([vv[rng.integers(0, len(vv), k)],
+                            0.5 * (vv[rng.integers(0, len(vv), k)] + vv[rng.integers(0, len(vv), k)]),
+                            rng.uniform(-2, 2, (nq - 2 * k, dim))]).astype(np.float32)
+        o, d = W.rays(nq, dim, seed=902)
+        o[:k] = q[:k]  # rays leaving from vertices
+        if dim == 3:
+            from drjit_scalar import Array3i
+            V, F = soa(vv, Array3), soa(ix, Array3i)
+            bvh, snch = BVH3D(V, F), SNCH3D(V, F)
+        else:
+            from drjit_scalar import Array2i
+            V, F = soa(vv, Array2), soa(ix, Array2i)
+            bvh, snch = BVH(V, F), SNCH(V, F)
+        uv = "uv" if dim == 3 else "t"
+        cp = run(bvh.closest_point, [(vec(p),) for p in q], ["valid", "p", "n", uv, "d", "prim_id"])
+        ray = run(bvh.intersect, [(vec(a), vec(b), Float(dr.inf)) for a, b in zip(o, d)],
+                  ["valid", "p", "n", uv, "d", "prim_id", "on_boundary"])
+        sil = run(snch.closest_silhouette, [(vec(p), Float(dr.inf)) for p in q], ["valid", "p", "d", "prim_id"])
+        np.savez_compressed(HERE / f"degenerate_{name}.npz", dim=dim, vertices=vv, indices=ix, q=q, o=o, d=d,
+                            **{f"cp_{k}": x for k, x in cp.items()}, **{f"ray_{k}": x for k, x in ray.items()},
+                            **{f"sil_{k}": x for k, x in sil.items()})
+        print("degenerate", name, "cp valid", cp["valid"].mean(), "ray valid", ray["valid"].mean(),
+              "sil valid", sil["valid"].mean())
+
+
 def main():
     if "--baselines-only" in sys.argv:
         baselines()
+        return
+    if "--degenerate-only" in sys.argv:
+        degenerate_cases()
         return
     if "--rmax-only" in sys.argv:
         rmax_cases()
@@ -308,6 +356,7 @@ def main():
     baselines()
     deep_cases()
     rmax_cases()
+    degenerate_cases()
 
 
 if __name__ == "__main__":

@@ -191,3 +191,38 @@ def test_exact_kernels_match_reference_traversal_rmax(path):
     assert_bitwise(to_np(s.closest_silhouette(z["q"], z["r_sil"], variant="exact")), expected(z, "sil", SIL), SIL,
                    "sil ")
     assert s.device_error() == 0
+
+
+# ---------------------------------------------------------------- degenerate geometry
+
+DEGENERATE = sorted((Path(__file__).resolve().parent / "golden").glob("degenerate_*.npz"))
+
+
+def test_degenerate_fixtures_exist():
+    assert {"degenerate_mesh", "degenerate_polyline"} <= {p.stem for p in DEGENERATE}
+
+
+@pytest.mark.parametrize("path", DEGENERATE, ids=[p.stem for p in DEGENERATE])
+def test_oracle_matches_reference_traversal_degenerate(path):
+    """Zero-area and segment-like faces, collapsed edges, repeated primitives, point
+    segments; queries and ray origins on vertices: every record field of the reference."""
+    dim, z = load(path)
+    s = Scene(z["vertices"], z["indices"], dim, device=None)
+    nodes, prims = s.ref_array(L.ARRAY_BVH_NODES), s.ref_array(L.ARRAY_PRIMITIVES)
+    snodes, sils = s.ref_array(L.ARRAY_SNCH_NODES), s.ref_array(L.ARRAY_SILHOUETTES)
+    assert_bitwise(oracle.closest_point(dim, nodes, prims, z["q"]), expected(z, "cp", CP[dim]), CP[dim], "cp ")
+    assert_bitwise(oracle.intersect(dim, nodes, prims, z["o"], z["d"]), expected(z, "ray", RAY[dim]), RAY[dim],
+                   "ray ")
+    assert_bitwise(oracle.closest_silhouette(dim, snodes, sils, z["q"]), expected(z, "sil", SIL), SIL, "sil ")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", DEGENERATE, ids=[p.stem for p in DEGENERATE])
+def test_exact_kernels_match_reference_traversal_degenerate(path):
+    dim, z = load(path)
+    s = Scene(z["vertices"], z["indices"], dim, device=0)
+    assert_bitwise(to_np(s.closest_point(z["q"], variant="exact")), expected(z, "cp", CP[dim]), CP[dim], "cp ")
+    assert_bitwise(to_np(s.intersect(z["o"], z["d"], variant="exact")), expected(z, "ray", RAY[dim]), RAY[dim],
+                   "ray ")
+    assert_bitwise(to_np(s.closest_silhouette(z["q"], variant="exact")), expected(z, "sil", SIL), SIL, "sil ")
+    assert s.device_error() == 0
