@@ -14,9 +14,9 @@ baseline_<case>.npz: the records of the reference's brute-force methods
 (Polyline/Mesh closest_point_baseline and intersect_baseline, Polyline.intersect); and
 deep_<case>.npz: the traversals on deep trees (scenes named by their generator in
 gquery_b200.workloads and a checksum of the generated arrays); rmax_<case>.npz: rays and
-silhouettes with a per-query finite r_max; degenerate_<case>.npz: all three traversals
-on degenerate geometry.  --baselines-only, --deep-only, --rmax-only and
---degenerate-only write one group alone.
+silhouettes with a per-query finite r_max; degenerate_<case>.npz and open_<case>.npz: all three
+traversals on degenerate and on open geometry.  --baselines-only, --deep-only,
+--rmax-only, --degenerate-only and --open-only write one group alone.
 """
 from __future__ import annotations
 
@@ -314,9 +314,47 @@ def degenerate_cases(nq=320):
               "sil valid", sil["valid"].mean())
 
 
+def open_cases(nq=320):
+    """The reference's traversals on open geometry, whose boundary edges (3D) and chain
+    ends (2D) are silhouettes from every side: a 700-vertex random-walk chain and a
+    level-4 icosphere with a cap cut off.  Silhouettes within r_max = 0.6 (2D) and
+    unbounded (3D)."""
+    rng = np.random.default_rng(9)
+    cv = np.cumsum(rng.uniform(-0.05, 0.05, (700, 2)), axis=0).astype(np.float32)
+    ce = np.stack([np.arange(699), np.arange(1, 700)], 1).astype(np.int32)
+    mv, mf = W.icosphere(4, amplitude=0.25, seed=4)
+    mf = mf[mv[mf[:, 0], 2] > -0.3]
+    for name, (vv, ix, rmax_sil) in (("chain", (cv, ce, 0.6)), ("cut_icosphere4", (mv, mf, np.inf))):
+        dim = vv.shape[1]
+        q = W.uniform_points(nq, dim, seed=911)
+        q[: nq // 8] = vv[ix[np.random.default_rng(912).integers(0, len(ix), nq // 8), 0]]
+        o, d = W.rays(nq, dim, seed=913)
+        if dim == 3:
+            from drjit_scalar import Array3i
+            V, F = soa(vv, Array3), soa(ix, Array3i)
+            bvh, snch = BVH3D(V, F), SNCH3D(V, F)
+        else:
+            from drjit_scalar import Array2i
+            V, F = soa(vv, Array2), soa(ix, Array2i)
+            bvh, snch = BVH(V, F), SNCH(V, F)
+        uv = "uv" if dim == 3 else "t"
+        cp = run(bvh.closest_point, [(vec(p),) for p in q], ["valid", "p", "n", uv, "d", "prim_id"])
+        ray = run(bvh.intersect, [(vec(a), vec(b), Float(dr.inf)) for a, b in zip(o, d)],
+                  ["valid", "p", "n", uv, "d", "prim_id", "on_boundary"])
+        sil = run(snch.closest_silhouette, [(vec(p), Float(rmax_sil)) for p in q], ["valid", "p", "d", "prim_id"])
+        np.savez_compressed(HERE / f"open_{name}.npz", dim=dim, vertices=vv, indices=ix, q=q, o=o, d=d,
+                            rmax_sil=np.float32(rmax_sil), **{f"cp_{k}": x for k, x in cp.items()},
+                            **{f"ray_{k}": x for k, x in ray.items()}, **{f"sil_{k}": x for k, x in sil.items()})
+        print("open", name, "cp valid", cp["valid"].mean(), "ray valid", ray["valid"].mean(),
+              "sil valid", sil["valid"].mean())
+
+
 def main():
     if "--baselines-only" in sys.argv:
         baselines()
+        return
+    if "--open-only" in sys.argv:
+        open_cases()
         return
     if "--degenerate-only" in sys.argv:
         degenerate_cases()
@@ -357,6 +395,7 @@ def main():
     deep_cases()
     rmax_cases()
     degenerate_cases()
+    open_cases()
 
 
 if __name__ == "__main__":

@@ -226,3 +226,28 @@ def test_exact_kernels_match_reference_traversal_degenerate(path):
                    "ray ")
     assert_bitwise(to_np(s.closest_silhouette(z["q"], variant="exact")), expected(z, "sil", SIL), SIL, "sil ")
     assert s.device_error() == 0
+
+
+# ---------------------------------------------------------------- open geometry
+
+OPEN = sorted((Path(__file__).resolve().parent / "golden").glob("open_*.npz"))
+
+
+def test_open_fixtures_exist():
+    assert {"open_chain", "open_cut_icosphere4"} <= {p.stem for p in OPEN}
+
+
+@pytest.mark.parametrize("path", OPEN, ids=[p.stem for p in OPEN])
+def test_oracle_matches_reference_traversal_open(path):
+    """An open chain (its two ends are silhouettes from every side) and a mesh with a cap
+    cut off (its boundary edges are silhouettes from every side)."""
+    dim, z = load(path)
+    s = Scene(z["vertices"], z["indices"], dim, device=None)
+    nodes, prims = s.ref_array(L.ARRAY_BVH_NODES), s.ref_array(L.ARRAY_PRIMITIVES)
+    snodes, sils = s.ref_array(L.ARRAY_SNCH_NODES), s.ref_array(L.ARRAY_SILHOUETTES)
+    rmax = float(z["rmax_sil"])
+    assert_bitwise(oracle.closest_point(dim, nodes, prims, z["q"]), expected(z, "cp", CP[dim]), CP[dim], "cp ")
+    assert_bitwise(oracle.intersect(dim, nodes, prims, z["o"], z["d"]), expected(z, "ray", RAY[dim]), RAY[dim],
+                   "ray ")
+    got = oracle.closest_silhouette(dim, snodes, sils, z["q"], None if np.isinf(rmax) else rmax)
+    assert_bitwise(got, expected(z, "sil", SIL), SIL, "sil ")
