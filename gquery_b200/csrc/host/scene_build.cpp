@@ -278,29 +278,56 @@ std::vector<SilEdge> build_silhouette_edges(const PrimSource<3> &src,
                                             std::vector<uint32_t> *face_edge_out) {
     // Edge ids follow the order in which an undirected edge is first met while
     // scanning faces f = 0.. and their edges k = 0..2 (silhouette_edge.cpp:5-19).
+    // Half-edges are bucketed by their smaller vertex (a counting sort, each bucket in
+    // half-edge order); within a bucket the half-edges with the same larger vertex form
+    // one edge, whose first member is its first appearance.  A bucket holds about a
+    // vertex's degree; a large one (a fan around one vertex) is sorted instead of
+    // scanned, which keeps the pass O(n log n) for any mesh.
     const size_t nh = (size_t)src.np * 3;
-    std::vector<std::pair<uint64_t, uint32_t>> keyed(nh);
+    std::vector<uint32_t> lo_of(nh), hi_of(nh);
+    uint32_t top = 0;
     for (size_t h = 0; h < nh; ++h) {
-        size_t f = h / 3, k = h % 3;
-        uint64_t i0 = (uint32_t)src.index[f * 3 + k];
-        uint64_t i1 = (uint32_t)src.index[f * 3 + (k + 1) % 3];
+        const size_t f = h / 3, k = h % 3;
+        uint32_t i0 = (uint32_t)src.index[f * 3 + k];
+        uint32_t i1 = (uint32_t)src.index[f * 3 + (k + 1) % 3];
         if (i0 > i1) std::swap(i0, i1);
-        keyed[h] = {(i0 << 32) | i1, (uint32_t)h};
+        lo_of[h] = i0;
+        hi_of[h] = i1;
+        top = std::max(top, i0);
     }
-    std::sort(keyed.begin(), keyed.end());
-    // groups of equal keys: the first half-edge of each group is its first appearance
-    std::vector<std::pair<uint32_t, uint32_t>> firsts;  // (first half-edge, group start in keyed)
-    for (size_t i = 0; i < nh; ++i)
-        if (i == 0 || keyed[i].first != keyed[i - 1].first) firsts.push_back({keyed[i].second, (uint32_t)i});
-    std::sort(firsts.begin(), firsts.end());
+    std::vector<uint32_t> start(nh ? (size_t)top + 2 : 1, 0);
+    for (size_t h = 0; h < nh; ++h) ++start[(size_t)lo_of[h] + 1];
+    for (size_t b = 1; b < start.size(); ++b) start[b] += start[b - 1];
+    std::vector<uint32_t> slot(nh), fill(start.begin(), start.end() - 1);
+    for (size_t h = 0; h < nh; ++h) slot[fill[lo_of[h]]++] = (uint32_t)h;
+    std::vector<uint32_t> rep(nh);  // the first half-edge of the same edge
+    std::vector<std::pair<uint32_t, uint32_t>> big;
+    for (size_t b = 0; b + 1 < start.size(); ++b) {
+        const uint32_t j0 = start[b], j1 = start[b + 1];
+        if (j1 - j0 <= 32) {
+            for (uint32_t j = j0; j < j1; ++j) {
+                const uint32_t h = slot[j];
+                rep[h] = h;
+                for (uint32_t i = j0; i < j; ++i)
+                    if (hi_of[slot[i]] == hi_of[h]) {
+                        rep[h] = slot[i];
+                        break;
+                    }
+            }
+        } else {
+            big.clear();
+            for (uint32_t j = j0; j < j1; ++j) big.push_back({hi_of[slot[j]], slot[j]});
+            std::sort(big.begin(), big.end());
+            for (size_t i = 0; i < big.size(); ++i)
+                rep[big[i].second] = (i > 0 && big[i].first == big[i - 1].first) ? rep[big[i - 1].second] : big[i].second;
+        }
+    }
+    // edge ids in order of first appearance
     std::vector<uint32_t> face_edge(nh);
-    for (uint32_t e = 0; e < firsts.size(); ++e) {
-        size_t i = firsts[e].second;
-        uint64_t key = keyed[i].first;
-        for (; i < nh && keyed[i].first == key; ++i) face_edge[keyed[i].second] = e;
-    }
+    uint32_t n_edges = 0;
+    for (size_t h = 0; h < nh; ++h) face_edge[h] = rep[h] == h ? n_edges++ : face_edge[rep[h]];
 
-    std::vector<SilEdge> sil(firsts.size());
+    std::vector<SilEdge> sil(n_edges);
     for (int64_t f = 0; f < src.np; ++f) {  // silhouette_edge.cpp:28-53
         for (int k = 0; k < 3; ++k) {
             uint64_t i0 = (uint32_t)src.index[f * 3 + k];

@@ -36,6 +36,19 @@ def _open_mesh():
     return v, f[v[f[:, 0], 2] > -0.3]  # a cap cut off: boundary edges
 
 
+def _cone():
+    """A closed cone whose apex (vertex 0) meets 200 edges, plus a repeated face and a
+    face with a repeated vertex: the edge pass sorts a bucket this large."""
+    n = 200
+    a = 2 * np.pi * np.arange(n) / n
+    ring = np.stack([np.cos(a), np.sin(a), np.zeros(n)], 1)
+    v = np.concatenate([[[0.0, 0.0, 1.0]], ring, [[0.0, 0.0, 0.0]]]).astype(np.float32)
+    i = np.arange(n)
+    side = np.stack([np.zeros(n, int), 1 + i, 1 + (i + 1) % n], 1)
+    base = np.stack([np.full(n, n + 1), 1 + (i + 1) % n, 1 + i], 1)
+    return v, np.concatenate([side, base, side[:1], [[0, 0, 5]]]).astype(np.int32)
+
+
 CASES = {
     "pentagon": lambda: (np.array([[0, 0], [1, 0], [1.5, 1], [0.5, 1.5], [-0.5, 1]], np.float32),
                          np.array([[0, 1], [1, 2], [2, 3], [3, 4], [4, 0]], np.int32)),
@@ -46,6 +59,7 @@ CASES = {
     "icosphere3": lambda: W.icosphere(3, amplitude=0.3, seed=3),
     "icosphere4_open": _open_mesh,
     "icosphere5": lambda: W.icosphere(5, amplitude=0.15, seed=1),
+    "cone200": _cone,
 }
 
 
@@ -75,7 +89,7 @@ def test_reference_arrays_other_leaf_sizes(max_prims):
 
 
 def test_flat_silhouette_edges_bitwise():
-    for v, f in (W.icosphere(4, amplitude=0.3, seed=3), _open_mesh()):
+    for v, f in (W.icosphere(4, amplitude=0.3, seed=3), _open_mesh(), _cone()):
         _assert_same(oracle.reference_flat_silhouette_edges(v, f), gx.build_flat_silhouette_edges(v, f), "edges")
 
 
