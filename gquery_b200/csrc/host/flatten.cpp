@@ -437,6 +437,14 @@ void snch_node_bounds(const BvhTree<D> &t, const SnchTree<D> &s, DeviceImage<D> 
         g.usable = (r.flags & (GQ_ITEM_VALID | GQ_SIL_FILTER)) == GQ_SIL_FILTER;
         return g;
     };
+    // each record's two normal lengths, computed once (every enclosing node's bound reads them)
+    std::vector<double> nlen(2 * img.sils.size());
+    for (size_t j = 0; j < img.sils.size(); ++j) {
+        const SilEdgeGeom g = edge((long long)j);
+        nlen[2 * j] = sil_normal_len(g, 0);
+        nlen[2 * j + 1] = sil_normal_len(g, 1);
+    }
+    auto len = [&](long long j, int f, const SilEdgeGeom &) { return nlen[2 * (size_t)j + (size_t)f]; };
     auto bound = [&](size_t i, float out[kSilNodeBound]) {
         const auto &bx = t.nodes[i].box;
         const float cx = sil_node_centre(bx.lo.v[0], bx.hi.v[0]), cy = sil_node_centre(bx.lo.v[1], bx.hi.v[1]),
@@ -447,7 +455,7 @@ void snch_node_bounds(const BvhTree<D> &t, const SnchTree<D> &s, DeviceImage<D> 
                                                __builtin_inff()};
             std::memcpy(out, open, sizeof open);
         } else {
-            sil_node_bound(cx, cy, cz, beg[i], end[i], edge, out);
+            sil_node_bound(cx, cy, cz, beg[i], end[i], edge, len, out);
         }
     };
     std::vector<uint32_t> interior;  // pair k belongs to interior node interior[k]

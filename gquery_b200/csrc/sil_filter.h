@@ -164,11 +164,32 @@ GQ_HD bool sil_node_excluded_cone(float cx, float cy, float cz, const float *b, 
 }
 
 #if !defined(__CUDA_ARCH__)
+// Length of an edge's face normal f (0: n0, 1: n1) times its orientation sign, in double:
+// sqrt((s0 * s0 + s1 * s1) + s2 * s2).
+inline double sil_normal_len(const SilEdgeGeom &e, int f) {
+    const float *n = f ? e.n1 : e.n0;
+    const double s0 = (double)e.orient * n[0], s1 = (double)e.orient * n[1], s2 = (double)e.orient * n[2];
+    return sqrt(s0 * s0 + s1 * s1 + s2 * s2);
+}
+
 // Node bound over the edges begin..end-1 (edge(j) returns their SilEdgeGeom) for a node
-// whose box centre is c: out[kSilNodeBound] as above.
+// whose box centre is c: out[kSilNodeBound] as above.  len(j, f, e) returns
+// sil_normal_len(e, f) of edge j, computed here or read from a table filled once: a
+// record's normals are read by the bound of every node above it, several times each.
+template <class EdgeAt, class NormalLen>
+inline void sil_node_bound(float cx, float cy, float cz, long long begin, long long end, EdgeAt edge,
+                           NormalLen len, float out[kSilNodeBound]);
+
 template <class EdgeAt>
 inline void sil_node_bound(float cx, float cy, float cz, long long begin, long long end, EdgeAt edge,
                            float out[kSilNodeBound]) {
+    sil_node_bound(cx, cy, cz, begin, end, edge,
+                   [](long long, int f, const SilEdgeGeom &e) { return sil_normal_len(e, f); }, out);
+}
+
+template <class EdgeAt, class NormalLen>
+inline void sil_node_bound(float cx, float cy, float cz, long long begin, long long end, EdgeAt edge,
+                           NormalLen len, float out[kSilNodeBound]) {
     out[0] = out[1] = out[2] = 0.f;
     out[3] = 0.f;
     out[4] = 1.f;
@@ -202,7 +223,7 @@ inline void sil_node_bound(float cx, float cy, float cz, long long begin, long l
             for (int f = 0; f < 2; ++f) {
                 const float *n = f ? e.n1 : e.n0;
                 const double sn[3] = {(double)e.orient * n[0], (double)e.orient * n[1], (double)e.orient * n[2]};
-                const double nl = sqrt(sn[0] * sn[0] + sn[1] * sn[1] + sn[2] * sn[2]);
+                const double nl = len(j, f, e);
                 const double cs = (sn[0] * ax[0] + sn[1] * ax[1] + sn[2] * ax[2]) / nl;
                 if (cs < cmin_it) {
                     cmin_it = cs;
@@ -233,17 +254,16 @@ inline void sil_node_bound(float cx, float cy, float cz, long long begin, long l
         const SilEdgeGeom e = edge(j);
         for (int f = 0; f < 2; ++f) {
             const float *n = f ? e.n1 : e.n0;
-            double d2 = 0.0, cs = 0.0, nl = 0.0, ac = 0.0, sp = 0.0;
+            double d2 = 0.0, cs = 0.0, ac = 0.0, sp = 0.0;
             for (int k = 0; k < 3; ++k) {
                 const double sn = (double)e.orient * (double)n[k];
                 d2 += (sn - A[k]) * (sn - A[k]);
                 cs += sn * A[k];
-                nl += sn * sn;
                 ac += sn * ((double)e.a[k] - c[k]);
                 sp += sn * ((double)e.b[k] - (double)e.a[k]);
             }
             dmax = fmax(dmax, sqrt(d2));
-            cmin = fmin(cmin, cs / (sqrt(nl) * al));  // the angle between the directions
+            cmin = fmin(cmin, cs / (len(j, f, e) * al));  // the angle between the directions
             lo = fmin(lo, ac + fmin(0.0, sp));
             hi = fmax(hi, ac + fmax(0.0, sp));
         }
